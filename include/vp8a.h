@@ -1,0 +1,338 @@
+/*
+ * vp8a.h — C ABI of the B200 VP8 encoder-analysis path.
+ *
+ * This is the drop-in boundary a Rust (or any FFI) caller binds in place of
+ * the pure-Rust encoder-analysis functions of oxideav-vp8 0.2.9. Every entry
+ * point below cites the reference function it replaces (file:line inside the
+ * oxideav-vp8 crate). Signatures use only plain C types: pointers, sizes and
+ * the POD structs declared here. No torch or CUDA type crosses the ABI except
+ * the opaque `void*` returned by vp8a_ctx_stream().
+ *
+ * Memory: every buffer argument may live in host memory (pageable or pinned)
+ * or in device memory of the context's GPU; the library inspects each pointer.
+ * Host buffers are staged through context-owned device buffers and the call
+ * returns after its host outputs are written. A call whose buffers are all
+ * device memory is asynchronous on the context stream (vp8a_ctx_synchronize
+ * waits for it). One context = one GPU + one CUDA stream; a context must not
+ * be used from two threads at once (the reference's per-call `threads` budget
+ * becomes the GPU's own parallelism).
+ *
+ * Errors: every function returns a vp8a_status. The codes mirror the
+ * reference's EncodeError (src/encoder.rs:69) plus device conditions. Caller
+ * bugs the reference panics on (e.g. ARNR centre out of range,
+ * src/arnr.rs:494) return VP8A_E_INVALID_ARGUMENT instead of aborting.
+ */
+#ifndef VP8A_H
+#define VP8A_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+
+typedef enum vp8a_status {
+  VP8A_OK = 0,
+  /* EncodeError::InvalidDimensions — width/height 0 or > 0x3FFF. */
+  VP8A_E_INVALID_DIMENSIONS = 1,
+  /* EncodeError::QuantIndexOutOfRange (> 127). */
+  VP8A_E_QUANT_INDEX_OUT_OF_RANGE = 2,
+  /* EncodeError::LoopFilterLevelOutOfRange (> 63). */
+  VP8A_E_LOOP_FILTER_LEVEL_OUT_OF_RANGE = 3,
+  /* EncodeError::SharpnessLevelOutOfRange (> 7). */
+  VP8A_E_SHARPNESS_LEVEL_OUT_OF_RANGE = 4,
+  /* EncodeError::ReferenceDimensionsMismatch. */
+  VP8A_E_REFERENCE_DIMENSIONS_MISMATCH = 5,
+  /* A precondition the reference asserts or panics on (null pointer, count
+   * mismatch, centre index out of range, MV outside [-1023, 1023]). */
+  VP8A_E_INVALID_ARGUMENT = 6,
+  /* A CUDA runtime call failed; vp8a_last_error() has the text. */
+  VP8A_E_CUDA = 7,
+  /* A device-side bounded wait ran out (a wavefront producer never
+   * advanced); the context stays usable. */
+  VP8A_E_DEVICE_TIMEOUT = 8,
+  VP8A_E_OUT_OF_MEMORY = 9,
+  VP8A_E_NO_DEVICE = 10
+} vp8a_status;
+
+/* ------------------------------------------------------------------ types */
+
+/* Mv (src/motion_vector.rs:65): quarter-pel luma vector, components in
+ * [-1023, 1023] on the wire. */
+typedef struct vp8a_mv {
+  int16_t row;
+  int16_t col;
+} vp8a_mv;
+
+/* SearchResult (src/motion_search.rs:248). */
+typedef struct vp8a_search_result {
+  vp8a_mv mv;
+  uint32_t sad;
+} vp8a_search_result;
+
+/* LumaRef (src/motion_search.rs:230): a reference luma plane. For encoder
+ * searches width/height are the MB-padded plane (mb_cols*16 x mb_rows*16,
+ * src/encoder/inter.rs:545-550). Fetches outside replicate the edge pixel. */
+typedef struct vp8a_luma_ref {
+  const uint8_t* plane;
+  uint64_t stride;
+  uint32_t width;
+  uint32_t height;
+} vp8a_luma_ref;
+
+/* I420Frame (src/encoder.rs:5419): visible-size source picture; chroma is
+ * ceil(w/2) x ceil(h/2). */
+typedef struct vp8a_i420 {
+  uint32_t width;
+  uint32_t height;
+  const uint8_t* y;
+  const uint8_t* u;
+  const uint8_t* v;
+  uint64_t y_stride;
+  uint64_t uv_stride;
+} vp8a_i420;
+
+/* KeyframePlanes (src/frame.rs:123): MB-padded reconstruction planes,
+ * luma (mb_cols*16) x (mb_rows*16), chroma (mb_cols*8) x (mb_rows*8). */
+typedef struct vp8a_planes {
+  uint8_t* y;
+  uint8_t* u;
+  uint8_t* v;
+  uint64_t y_stride;
+  uint64_t uv_stride;
+  uint32_t mb_cols;
+  uint32_t mb_rows;
+} vp8a_planes;
+
+/* RefFrame (src/motion_comp.rs) as used by the census and the §9.4 deltas. */
+enum { VP8A_REF_INTRA = 0, VP8A_REF_LAST = 1, VP8A_REF_GOLDEN = 2, VP8A_REF_ALTREF = 3 };
+
+/* InterMode (src/near_mv.rs:68). */
+enum { VP8A_MODE_ZERO = 0, VP8A_MODE_NEAREST = 1, VP8A_MODE_NEAR = 2, VP8A_MODE_NEW = 3,
+       VP8A_MODE_SPLIT = 4, VP8A_MODE_NONE = 255 };
+
+/* MvPartition (src/near_mv.rs:539), in partition_id order. */
+enum { VP8A_PART_TOP_BOTTOM = 0, VP8A_PART_LEFT_RIGHT = 1, VP8A_PART_QUARTERS = 2,
+       VP8A_PART_MV16 = 3, VP8A_PART_NONE = 255 };
+
+/* SubMvRefMode (src/near_mv.rs). */
+enum { VP8A_SUBMV_LEFT = 0, VP8A_SUBMV_ABOVE = 1, VP8A_SUBMV_ZERO = 2, VP8A_SUBMV_NEW = 3 };
+
+/* MvContexts (src/motion_vector.rs:79): two 19-entry probability vectors,
+ * row then column. */
+typedef struct vp8a_mv_contexts {
+  uint8_t p[2][19];
+} vp8a_mv_contexts;
+
+/* The per-MB outcome of the exhaustive inter analysis (MbDecision,
+ * src/encoder/inter.rs, with PickedMbForRef's search fields,
+ * src/encoder.rs:8470-8514). */
+typedef struct vp8a_mb_decision {
+  uint8_t ref_frame;   /* VP8A_REF_* of the winning reference */
+  uint8_t mode;        /* VP8A_MODE_* */
+  uint8_t partition;   /* VP8A_PART_* (SPLIT only) */
+  uint8_t reserved;
+  vp8a_mv mv;          /* chosen MV (SPLIT: split_mvs[15]) */
+  double j;            /* winning per-ref J (without ref_frame_tree bits) */
+  double total;        /* j + lambda * ref_frame_tree_bits */
+  vp8a_mv split_mvs[16];
+  uint8_t submv_modes[16];
+} vp8a_mb_decision;
+
+/* Search trace of one (MB, reference) pick (the search part of
+ * pick_mb_for_ref, src/encoder.rs:8546-8652). Optional output. */
+typedef struct vp8a_ref_search {
+  vp8a_mv best_predictor;
+  vp8a_mv nearest_mv;
+  vp8a_mv near_mv;
+  uint32_t sad_zero;
+  vp8a_search_result whole;
+  vp8a_search_result half;
+  vp8a_search_result quarter;
+  uint32_t sad_nearest;
+  uint32_t sad_near;
+  uint8_t chosen_mode;
+  uint8_t split_partition;
+  uint8_t reserved[2];
+  double j;
+} vp8a_ref_search;
+
+/* Per-MB side information the §15 pass consults (MacroblockModes +
+ * has_coeffs + InterFilterInfo, src/loop_filter.rs:1364-1489). */
+typedef struct vp8a_mb_lf_info {
+  uint8_t y_mode_is_bpred; /* y_mode == B_PRED (SPLITMV MBs are recorded as B_PRED) */
+  uint8_t has_coeffs;      /* mb_has_coeffs (src/loop_filter.rs:1497) */
+  uint8_t ref_frame;       /* VP8A_REF_*; VP8A_REF_INTRA for intra MBs */
+  uint8_t inter_mode;      /* VP8A_MODE_*; VP8A_MODE_NONE for intra MBs */
+  int8_t segment_id;       /* -1 = None */
+  uint8_t reserved[3];
+} vp8a_mb_lf_info;
+
+/* FrameFilterConfig (src/loop_filter.rs:891). */
+typedef struct vp8a_filter_config {
+  uint8_t simple;
+  uint8_t key_frame;
+  uint8_t loop_filter_level;
+  uint8_t sharpness_level;
+  uint8_t segmentation_enabled;
+  uint8_t segment_abs;
+  uint8_t delta_enabled;
+  uint8_t reserved;
+  int16_t segment_lf_level[4];
+  int16_t ref_delta_current;
+  int16_t bpred_mode_delta;
+  int16_t ref_delta_last;
+  int16_t ref_delta_golden;
+  int16_t ref_delta_altref;
+  int16_t zero_mv_mode_delta;
+  int16_t other_mv_mode_delta;
+  int16_t split_mv_mode_delta;
+} vp8a_filter_config;
+
+/* SourcePlanes (src/loop_filter.rs:1916): the visible source window. */
+typedef struct vp8a_source {
+  uint32_t width;
+  uint32_t height;
+  const uint8_t* y;
+  const uint8_t* u;
+  const uint8_t* v;
+  uint64_t y_stride;
+  uint64_t uv_stride;
+} vp8a_source;
+
+/* --------------------------------------------------------------- context */
+
+typedef struct vp8a_ctx vp8a_ctx;
+
+/* Create a context on CUDA device `device` with its own non-blocking stream.
+ * Fails with VP8A_E_NO_DEVICE when no GPU is visible: there is no CPU
+ * fallback. */
+vp8a_status vp8a_ctx_create(int device, vp8a_ctx** out);
+vp8a_status vp8a_ctx_destroy(vp8a_ctx* ctx);
+/* The context's cudaStream_t, as an opaque pointer. */
+void* vp8a_ctx_stream(vp8a_ctx* ctx);
+vp8a_status vp8a_ctx_synchronize(vp8a_ctx* ctx);
+/* Kernel launches issued by this context since creation. */
+uint64_t vp8a_ctx_launch_count(const vp8a_ctx* ctx);
+/* Text of the last error on this thread ("" if none). */
+const char* vp8a_last_error(void);
+/* ABI version of this header (major << 16 | minor). */
+uint32_t vp8a_abi_version(void);
+
+/* ------------------------------------------------- motion search (§17/§18) */
+
+/* Batched mb_luma_sad_at_mv (src/motion_search.rs:470) — the §18 six-tap
+ * sub-pel SAD; a whole-pel MV takes the copy path, which equals
+ * mb_luma_sad_at_whole_mv (src/motion_search.rs:291). Item i scores the
+ * source MB src_mbs[256*i] (16x16, stride 16) at MB position
+ * (mb_xy[2i], mb_xy[2i+1]) = (mb_col, mb_row) against `ref` at mvs[i]. */
+vp8a_status vp8a_mb_luma_sad_at_mv(vp8a_ctx* ctx, const vp8a_luma_ref* ref,
+                                   const uint8_t* src_mbs, const uint32_t* mb_xy,
+                                   const vp8a_mv* mvs, uint32_t n, uint32_t* sad_out);
+
+/* Batched small_diamond_search_luma (src/motion_search.rs:381). */
+vp8a_status vp8a_small_diamond_search_luma(vp8a_ctx* ctx, const vp8a_luma_ref* ref,
+                                           const uint8_t* src_mbs, const uint32_t* mb_xy,
+                                           const vp8a_mv* centers, uint32_t max_iters,
+                                           uint32_t n, vp8a_search_result* out);
+
+/* Batched half_pixel_refine_luma (src/motion_search.rs:564). Centres must
+ * be whole-pel and inside [-1023, 1023]. */
+vp8a_status vp8a_half_pixel_refine_luma(vp8a_ctx* ctx, const vp8a_luma_ref* ref,
+                                        const uint8_t* src_mbs, const uint32_t* mb_xy,
+                                        const vp8a_mv* whole_centers, uint32_t n,
+                                        vp8a_search_result* out);
+
+/* Batched quarter_pixel_refine_luma (src/motion_search.rs:666). Centres
+ * must be half-pel and inside [-1023, 1023]. */
+vp8a_status vp8a_quarter_pixel_refine_luma(vp8a_ctx* ctx, const vp8a_luma_ref* ref,
+                                           const uint8_t* src_mbs, const uint32_t* mb_xy,
+                                           const vp8a_mv* half_centers, uint32_t n,
+                                           vp8a_search_result* out);
+
+/* The full descent pick_mb_for_ref runs per (MB, ref)
+ * (src/encoder.rs:8576-8596): diamond(center, max_iters) -> half -> quarter,
+ * fused in one kernel. Any of the three outputs may be NULL. */
+vp8a_status vp8a_motion_descent(vp8a_ctx* ctx, const vp8a_luma_ref* ref,
+                                const uint8_t* src_mbs, const uint32_t* mb_xy,
+                                const vp8a_mv* centers, uint32_t max_iters, uint32_t n,
+                                vp8a_search_result* whole_out, vp8a_search_result* half_out,
+                                vp8a_search_result* quarter_out);
+
+/* ------------------------------------- exhaustive inter analysis (§16/§17) */
+
+/* The exhaustive per-MB analysis of a P frame with intra picking off:
+ * analyse_inter_frame (src/encoder/inter.rs:263) with
+ * decide_mb_exhaustive (src/encoder/inter.rs:537) and pick_mb_for_ref's
+ * search and mode decision (src/encoder.rs:8516-8702, SPLITMV
+ * src/encoder.rs:7573-8246). `refs[k]` (k < n_refs) are MB-padded
+ * reference planes in scoring order with ids `ref_ids[k]` (VP8A_REF_*);
+ * `mv_contexts` NULL means the §17.2 defaults; `lambda` is the RD
+ * multiplier (rd_lambda, src/encoder.rs:3742). Writes mb_cols*mb_rows
+ * decisions in raster order; `trace` (optional) receives n_refs entries
+ * per MB. The MB-row wavefront of the reference (row r waits for row r-1
+ * to be two MBs ahead) runs on the device. */
+vp8a_status vp8a_analyse_inter_frame(vp8a_ctx* ctx, const vp8a_i420* frame,
+                                     const vp8a_planes* refs, const uint8_t* ref_ids,
+                                     uint32_t n_refs, const vp8a_mv_contexts* mv_contexts,
+                                     double lambda, vp8a_mb_decision* decisions,
+                                     vp8a_ref_search* trace);
+
+/* rd_lambda (src/encoder.rs:3742) for a luma AC quantiser index 0..=127. */
+double vp8a_rd_lambda(uint32_t y_ac_qi);
+
+/* ------------------------------------------------------------ ARNR filter */
+
+/* build_arnr_altref (src/arnr.rs:476): temporally filtered altref anchor of
+ * `n` frames aligned to frames[center]. Outputs are tightly packed:
+ * y_out width*height, u_out/v_out ceil(w/2)*ceil(h/2). `strength` is
+ * clamped to 0..=6 (ArnrConfig::new, src/arnr.rs:76). */
+vp8a_status vp8a_build_arnr_altref(vp8a_ctx* ctx, const vp8a_i420* frames, uint32_t n,
+                                   uint32_t center, uint32_t strength, uint8_t* y_out,
+                                   uint8_t* u_out, uint8_t* v_out);
+
+/* ------------------------------------------------------- §15 loop filter */
+
+/* filter_inter_frame_flags (src/loop_filter.rs:1364) / filter_frame_flags
+ * (src/loop_filter.rs:2506) in place on `planes`. Key frames pass every MB
+ * with ref_frame = VP8A_REF_INTRA and config->key_frame = 1. */
+vp8a_status vp8a_filter_frame(vp8a_ctx* ctx, vp8a_planes* planes, const vp8a_mb_lf_info* mbs,
+                              const vp8a_filter_config* config);
+
+/* reconstruction_ssd (src/loop_filter.rs:1965). */
+vp8a_status vp8a_reconstruction_ssd(vp8a_ctx* ctx, const vp8a_planes* planes,
+                                    const vp8a_source* src, uint64_t* ssd_out);
+
+/* The whole §9.4 candidate grid: ssd_out[level * 8 + sharpness] is
+ * score_filter_candidate (src/loop_filter.rs:2062) for every level 0..=63
+ * and sharpness 0..=7 (level 0 is the unfiltered SSD for every sharpness).
+ * `every_rows` = 0 scores whole frames; > 0 scores the two-MB-row bands of
+ * select_filter_params_sampled (src/loop_filter.rs:2288). */
+vp8a_status vp8a_filter_sweep(vp8a_ctx* ctx, const vp8a_planes* planes,
+                              const vp8a_mb_lf_info* mbs, const vp8a_filter_config* base,
+                              const vp8a_source* src, uint32_t every_rows, uint64_t* ssd_out);
+
+/* select_filter_params (src/loop_filter.rs:2047): the reference's coarse
+ * grid + refine + sharpness search, replayed over the device sweep. */
+vp8a_status vp8a_select_filter_params(vp8a_ctx* ctx, const vp8a_planes* planes,
+                                      const vp8a_mb_lf_info* mbs,
+                                      const vp8a_filter_config* base, const vp8a_source* src,
+                                      uint8_t* level_out, uint8_t* sharpness_out);
+
+/* select_filter_params_sampled (src/loop_filter.rs:2288) with
+ * FilterSampling { every_rows, sweep_sharpness }. */
+vp8a_status vp8a_select_filter_params_sampled(vp8a_ctx* ctx, const vp8a_planes* planes,
+                                              const vp8a_mb_lf_info* mbs,
+                                              const vp8a_filter_config* base,
+                                              const vp8a_source* src, uint32_t every_rows,
+                                              uint32_t sweep_sharpness, uint8_t* level_out,
+                                              uint8_t* sharpness_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VP8A_H */

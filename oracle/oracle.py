@@ -1,0 +1,332 @@
+"""Python face of the oracle (liboracle.so) — TEST INFRASTRUCTURE ONLY.
+
+The oracle is the CPU restatement of the reference's encoder-analysis path
+(see vp8a_oracle.h). Only tests/, __graft_entry__.smoke() and the
+cpu_baseline / reference legs of bench.py use it, as the checker or as the
+timed CPU baseline; the product (libvp8a.so, package vp8a) never loads it.
+
+Function names and argument meanings match the product API in vp8a.api
+(without the GPU context), so a parity test calls both the same way.
+"""
+import ctypes as C
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+PKG_DIR = os.path.join(ROOT, "oxideav-vp8_b200")
+if PKG_DIR not in sys.path:
+    sys.path.insert(0, PKG_DIR)
+
+from vp8a import abi  # noqa: E402  (ABI record layouts only)
+from vp8a.frames import i420, luma_ref, planes, ptr, source  # noqa: E402
+
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+_lib = None
+P = C.c_void_p
+U32 = C.c_uint32
+
+
+def build(force=False):
+    """Compile liboracle.so with the Makefile beside this file."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-C", HERE, "-B" if force else "liboracle.so"], check=True, capture_output=True)
+    else:
+        subprocess.run(["make", "-C", HERE], check=True, capture_output=True)
+    return LIB_PATH
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        build()
+    lib = C.CDLL(LIB_PATH)
+    sig = {
+        "vo_block_sad_16x16": (U32, [P, P]),
+        "vo_mb_luma_sad_at_mv_batch": (None, [C.POINTER(abi.LumaRef), P, P, P, U32, P]),
+        "vo_small_diamond_batch": (None, [C.POINTER(abi.LumaRef), P, P, P, U32, U32, P]),
+        "vo_half_refine_batch": (None, [C.POINTER(abi.LumaRef), P, P, P, U32, P]),
+        "vo_quarter_refine_batch": (None, [C.POINTER(abi.LumaRef), P, P, P, U32, P]),
+        "vo_motion_descent_batch": (None, [C.POINTER(abi.LumaRef), P, P, P, U32, U32, P, P, P, U32]),
+        "vo_sixtap_mb_luma": (None, [P, C.c_int, C.c_int, P]),
+        "vo_bool_bits": (C.c_double, [C.c_uint8, C.c_int]),
+        "vo_mv_component_bits": (C.c_double, [P, C.c_int32]),
+        "vo_rd_lambda": (C.c_double, [U32]),
+        "vo_analyse_inter_frame": (C.c_int, [C.POINTER(abi.I420), P, P, U32, C.POINTER(abi.MvContexts),
+                                             C.c_double, P, P, U32]),
+        "vo_build_arnr_altref": (C.c_int, [P, U32, U32, U32, P, P, P, U32]),
+        "vo_lf_derive": (None, [C.c_uint8, C.c_uint8, C.c_int, P]),
+        "vo_common_adjust": (C.c_int32, [C.c_int, P]),
+        "vo_simple_segment": (None, [C.c_uint8, P]),
+        "vo_subblock_filter": (None, [C.c_uint8, C.c_uint8, C.c_uint8, P]),
+        "vo_mb_filter": (None, [C.c_uint8, C.c_uint8, C.c_uint8, P]),
+        "vo_mb_filter_level": (C.c_uint8, [C.POINTER(abi.FilterConfig), P]),
+        "vo_filter_frame": (C.c_int, [C.POINTER(abi.Planes), P, C.POINTER(abi.FilterConfig)]),
+        "vo_reconstruction_ssd": (C.c_uint64, [C.POINTER(abi.Planes), C.POINTER(abi.Source)]),
+        "vo_score_filter_candidate": (C.c_uint64, [C.POINTER(abi.Planes), P, C.POINTER(abi.FilterConfig),
+                                                   C.POINTER(abi.Source), C.c_uint8, C.c_uint8, U32]),
+        "vo_filter_sweep": (None, [C.POINTER(abi.Planes), P, C.POINTER(abi.FilterConfig), C.POINTER(abi.Source),
+                                   U32, P, U32]),
+        "vo_select_filter_params": (None, [C.POINTER(abi.Planes), P, C.POINTER(abi.FilterConfig),
+                                           C.POINTER(abi.Source), P, P, U32]),
+        "vo_select_filter_params_sampled": (None, [C.POINTER(abi.Planes), P, C.POINTER(abi.FilterConfig),
+                                                   C.POINTER(abi.Source), U32, U32, P, P, U32]),
+        "vo_select_from_table_full": (None, [P, C.c_uint8, P, P]),
+        "vo_select_from_table_sampled": (None, [P, C.c_uint8, C.c_int, P, P]),
+        "vo_type_size": (C.c_size_t, [C.c_int]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _mvs(a):
+    a = np.ascontiguousarray(a)
+    if a.dtype != abi.MV_DTYPE:
+        a = np.ascontiguousarray(a.astype(np.int16).reshape(-1, 2)).view(abi.MV_DTYPE).reshape(-1)
+    return a
+
+
+def _xy(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint32).reshape(-1, 2))
+
+
+def _src(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint8).reshape(-1, 256))
+
+
+def type_sizes():
+    lib = load()
+    names = ["vp8a_mv", "vp8a_search_result", "vp8a_luma_ref", "vp8a_i420", "vp8a_planes", "vp8a_mv_contexts",
+             "vp8a_mb_decision", "vp8a_ref_search", "vp8a_mb_lf_info", "vp8a_filter_config", "vp8a_source"]
+    return {n: int(lib.vo_type_size(i)) for i, n in enumerate(names)}
+
+
+def block_sad_16x16(src, pred):
+    s = np.ascontiguousarray(src, np.uint8)
+    p = np.ascontiguousarray(pred, np.uint8)
+    return int(load().vo_block_sad_16x16(ptr(s), ptr(p)))
+
+
+def sixtap_mb_luma(halo441, mx, my):
+    h = np.ascontiguousarray(halo441, np.uint8).reshape(-1)
+    out = np.zeros(256, np.uint8)
+    load().vo_sixtap_mb_luma(ptr(h), mx, my, ptr(out))
+    return out.reshape(16, 16)
+
+
+def mb_luma_sad_at_mv(ref_plane, src_mbs, mb_xy, mvs, width=None, height=None):
+    r = luma_ref(ref_plane, width, height)
+    src, xy, mv = _src(src_mbs), _xy(mb_xy), _mvs(mvs)
+    out = np.zeros(len(mv), np.uint32)
+    load().vo_mb_luma_sad_at_mv_batch(C.byref(r), ptr(src), ptr(xy), ptr(mv), len(mv), ptr(out))
+    return out
+
+
+def small_diamond_search_luma(ref_plane, src_mbs, mb_xy, centers, max_iters, width=None, height=None):
+    r = luma_ref(ref_plane, width, height)
+    src, xy, c = _src(src_mbs), _xy(mb_xy), _mvs(centers)
+    out = np.zeros(len(c), abi.SEARCH_RESULT_DTYPE)
+    load().vo_small_diamond_batch(C.byref(r), ptr(src), ptr(xy), ptr(c), max_iters, len(c), ptr(out))
+    return out
+
+
+def half_pixel_refine_luma(ref_plane, src_mbs, mb_xy, centers, width=None, height=None):
+    r = luma_ref(ref_plane, width, height)
+    src, xy, c = _src(src_mbs), _xy(mb_xy), _mvs(centers)
+    out = np.zeros(len(c), abi.SEARCH_RESULT_DTYPE)
+    load().vo_half_refine_batch(C.byref(r), ptr(src), ptr(xy), ptr(c), len(c), ptr(out))
+    return out
+
+
+def quarter_pixel_refine_luma(ref_plane, src_mbs, mb_xy, centers, width=None, height=None):
+    r = luma_ref(ref_plane, width, height)
+    src, xy, c = _src(src_mbs), _xy(mb_xy), _mvs(centers)
+    out = np.zeros(len(c), abi.SEARCH_RESULT_DTYPE)
+    load().vo_quarter_refine_batch(C.byref(r), ptr(src), ptr(xy), ptr(c), len(c), ptr(out))
+    return out
+
+
+def motion_descent(ref_plane, src_mbs, mb_xy, centers, max_iters=8, width=None, height=None, threads=1):
+    r = luma_ref(ref_plane, width, height)
+    src, xy, c = _src(src_mbs), _xy(mb_xy), _mvs(centers)
+    n = len(c)
+    w, h, q = (np.zeros(n, abi.SEARCH_RESULT_DTYPE) for _ in range(3))
+    load().vo_motion_descent_batch(C.byref(r), ptr(src), ptr(xy), ptr(c), max_iters, n, ptr(w), ptr(h), ptr(q),
+                                   threads)
+    return w, h, q
+
+
+def bool_bits(prob, value):
+    return load().vo_bool_bits(prob, int(bool(value)))
+
+
+def mv_component_bits(ctx19, value):
+    p = np.ascontiguousarray(ctx19, np.uint8)
+    return load().vo_mv_component_bits(ptr(p), value)
+
+
+def rd_lambda(qi):
+    return load().vo_rd_lambda(qi)
+
+
+def _check(status, where):
+    if status != 0:
+        raise RuntimeError(f"{where}: {abi.STATUS_NAMES.get(status, status)}")
+
+
+def analyse_inter_frame(frame, refs, ref_ids, lam, mv_contexts=None, trace=False, threads=1):
+    f = i420(*frame)
+    prs = [planes(*p) for p in refs]
+    parr = (abi.Planes * len(prs))(*prs)
+    ids = np.ascontiguousarray(np.asarray(ref_ids, np.uint8))
+    mbr, mbc = (f.height + 15) // 16, (f.width + 15) // 16
+    dec = np.zeros(mbr * mbc, abi.MB_DECISION_DTYPE)
+    tr = np.zeros(mbr * mbc * len(prs), abi.REF_SEARCH_DTYPE) if trace else None
+    ctxs = mv_contexts if mv_contexts is not None else abi.default_mv_contexts()
+    st = load().vo_analyse_inter_frame(C.byref(f), C.cast(parr, C.c_void_p), ptr(ids), len(prs), C.byref(ctxs), lam,
+                                       ptr(dec), ptr(tr), threads)
+    _check(st, "vo_analyse_inter_frame")
+    dec = dec.reshape(mbr, mbc)
+    if trace:
+        return dec, tr.reshape(mbr, mbc, len(prs))
+    return dec
+
+
+def build_arnr_altref(frames, center, strength=3, threads=1):
+    recs = [i420(*f) for f in frames]
+    arr = (abi.I420 * len(recs))(*recs)
+    h, w = frames[center][0].shape
+    ch, cw = (h + 1) // 2, (w + 1) // 2
+    y = np.zeros((h, w), np.uint8)
+    u = np.zeros((ch, cw), np.uint8)
+    v = np.zeros((ch, cw), np.uint8)
+    st = load().vo_build_arnr_altref(C.cast(arr, C.c_void_p), len(recs), center, strength, ptr(y), ptr(u), ptr(v),
+                                     threads)
+    _check(st, "vo_build_arnr_altref")
+    return y, u, v
+
+
+def lf_derive(level, sharpness, key_frame):
+    out = np.zeros(4, np.uint8)
+    load().vo_lf_derive(level, sharpness, int(bool(key_frame)), ptr(out))
+    return tuple(int(v) for v in out)  # interior, hev, mbedge, subedge
+
+
+def common_adjust(use_outer_taps, seg4):
+    s = np.ascontiguousarray(seg4, np.uint8).copy()
+    a = load().vo_common_adjust(int(bool(use_outer_taps)), ptr(s))
+    return int(a), s
+
+
+def simple_segment(edge_limit, seg4):
+    s = np.ascontiguousarray(seg4, np.uint8).copy()
+    load().vo_simple_segment(edge_limit, ptr(s))
+    return s
+
+
+def subblock_filter(hev, interior, edge, seg8):
+    s = np.ascontiguousarray(seg8, np.uint8).copy()
+    load().vo_subblock_filter(hev, interior, edge, ptr(s))
+    return s
+
+
+def mb_filter(hev, interior, edge, seg8):
+    s = np.ascontiguousarray(seg8, np.uint8).copy()
+    load().vo_mb_filter(hev, interior, edge, ptr(s))
+    return s
+
+
+def mb_filter_level(config, mb):
+    m = np.ascontiguousarray(np.asarray(mb, abi.MB_LF_INFO_DTYPE).reshape(1))
+    return int(load().vo_mb_filter_level(C.byref(config), ptr(m)))
+
+
+def filter_frame(recon, mbs, config):
+    y, u, v = (np.array(p, np.uint8, copy=True) for p in recon)
+    p = planes(y, u, v)
+    m = np.ascontiguousarray(mbs, abi.MB_LF_INFO_DTYPE)
+    _check(load().vo_filter_frame(C.byref(p), ptr(m), C.byref(config)), "vo_filter_frame")
+    return y, u, v
+
+
+def reconstruction_ssd(recon, src):
+    return int(load().vo_reconstruction_ssd(C.byref(planes(*recon)), C.byref(source(*src))))
+
+
+def score_filter_candidate(recon, mbs, base, src, level, sharpness, every_rows=0):
+    m = np.ascontiguousarray(mbs, abi.MB_LF_INFO_DTYPE)
+    return int(load().vo_score_filter_candidate(C.byref(planes(*recon)), ptr(m), C.byref(base),
+                                                C.byref(source(*src)), level, sharpness, every_rows))
+
+
+def filter_sweep(recon, mbs, base, src, every_rows=0, threads=1):
+    m = np.ascontiguousarray(mbs, abi.MB_LF_INFO_DTYPE)
+    out = np.zeros(512, np.uint64)
+    load().vo_filter_sweep(C.byref(planes(*recon)), ptr(m), C.byref(base), C.byref(source(*src)), every_rows,
+                           ptr(out), threads)
+    return out.reshape(64, 8)
+
+
+def select_filter_params(recon, mbs, base, src, threads=1):
+    m = np.ascontiguousarray(mbs, abi.MB_LF_INFO_DTYPE)
+    lv, sh = C.c_uint8(), C.c_uint8()
+    load().vo_select_filter_params(C.byref(planes(*recon)), ptr(m), C.byref(base), C.byref(source(*src)),
+                                   C.byref(lv), C.byref(sh), threads)
+    return lv.value, sh.value
+
+
+def select_filter_params_sampled(recon, mbs, base, src, every_rows, sweep_sharpness, threads=1):
+    m = np.ascontiguousarray(mbs, abi.MB_LF_INFO_DTYPE)
+    lv, sh = C.c_uint8(), C.c_uint8()
+    load().vo_select_filter_params_sampled(C.byref(planes(*recon)), ptr(m), C.byref(base), C.byref(source(*src)),
+                                           every_rows, int(bool(sweep_sharpness)), C.byref(lv), C.byref(sh), threads)
+    return lv.value, sh.value
+
+
+def select_from_table(table, base_sharp, sampled=False, sweep=True):
+    t = np.ascontiguousarray(np.asarray(table, np.uint64).reshape(512))
+    lv, sh = C.c_uint8(), C.c_uint8()
+    if sampled:
+        load().vo_select_from_table_sampled(ptr(t), base_sharp, int(bool(sweep)), C.byref(lv), C.byref(sh))
+    else:
+        load().vo_select_from_table_full(ptr(t), base_sharp, C.byref(lv), C.byref(sh))
+    return lv.value, sh.value
+
+
+class MbInfo(C.Structure):
+    """vo_mb_info (MbInfo, src/near_mv.rs:127)."""
+
+    _fields_ = [("ref_frame", C.c_uint8), ("is_split", C.c_uint8), ("has_split_mvs", C.c_uint8),
+                ("reserved", C.c_uint8), ("mv", abi.Mv), ("split_mvs", abi.Mv * 16)]
+
+
+def mb_info(ref_frame=0, mv=(0, 0), is_split=False, split_mvs=None):
+    m = MbInfo()
+    m.ref_frame = ref_frame
+    m.mv.row, m.mv.col = mv
+    m.is_split = int(bool(is_split))
+    if split_mvs is not None:
+        m.has_split_mvs = 1
+        for i, (r, c) in enumerate(split_mvs):
+            m.split_mvs[i].row, m.split_mvs[i].col = r, c
+    return m
+
+
+def find_near_mvs(above, left, aboveleft, current_ref=1):
+    lib = load()
+    fn = lib.vo_find_near_mvs
+    fn.restype = None
+    fn.argtypes = [C.POINTER(MbInfo)] * 3 + [C.c_uint8, P, P]
+    mvs = np.zeros(3, abi.MV_DTYPE)
+    cnt = np.zeros(4, np.int32)
+    fn(C.byref(above), C.byref(left), C.byref(aboveleft), current_ref, ptr(mvs), ptr(cnt))
+    return [(int(m["row"]), int(m["col"])) for m in mvs], [int(c) for c in cnt]

@@ -1,0 +1,854 @@
+// lf.cu — §15 loop filter and the §9.4 (level, sharpness) search.
+//
+// Entry points:
+//   vp8a_filter_frame                  filter_inter_frame_flags / filter_frame_flags
+//                                      (src/loop_filter.rs:1364, :2506), in place
+//   vp8a_reconstruction_ssd            (src/loop_filter.rs:1965)
+//   vp8a_filter_sweep                  score_filter_candidate (:2062) for all 64 x 8
+//   vp8a_select_filter_params          select_filter_params_threaded (:2133)
+//   vp8a_select_filter_params_sampled  select_filter_params_sampled (:2288)
+//
+// Kernel design. One CTA filters the whole picture for one (level,
+// sharpness) candidate and returns its visible-window SSD against the
+// source. The §15 raster order makes MB (r, c) depend on (r, c-1) and
+// (r-1, c+1) (the filter never writes right of or below the MB it
+// processes), so MB (r, c) runs at wavefront step t = t0(r) + c with
+// t0(r) = 2r. Warps own MB rows; at each step every active row filters one
+// MB, and one __syncthreads separates steps. A row keeps its last four MBs
+// in a ring of shared-memory slots (Y 16x16 + U 8x8 + V 8x8 = 384 B): an MB
+// is loaded from the unfiltered reconstruction when its step comes and is
+// final — no later MB writes it — two steps later, when it is scored
+// against the source (or written back) and its slot reused. The picture
+// therefore crosses HBM once per candidate (all CTAs read the same
+// reconstruction, which stays L2-resident), and no candidate copy of the
+// planes is ever materialised. Within an MB a lane owns one pixel row for
+// the four vertical edges, then one pixel column for the four horizontal
+// edges (luma lanes 0-15, U 16-23, V 24-31), matching the reference's
+// step order (left MB edge, inner vertical, top MB edge, inner horizontal).
+// The sampled search's two-row bands are rows whose t0 restarts at 0 and
+// whose first row has no top edge.
+#include <algorithm>
+
+#include "vp8a_internal.cuh"
+
+namespace {
+using namespace vp8a_dev;
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int SLOT = 384;  // Y 256 + U 64 + V 64
+
+struct LfArgs {
+  const uint8_t* y;
+  const uint8_t* u;
+  const uint8_t* v;
+  uint64_t ys, cs;
+  int mb_cols, mb_rows;
+  const vp8a_mb_lf_info* mbs;
+  vp8a_filter_config base;
+  const uint8_t* sy;
+  const uint8_t* su;
+  const uint8_t* sv;
+  uint64_t sys, scs;
+  int width, height;
+  const uint8_t* cands;    // [n][2] (level, sharpness)
+  const int16_t* row_t0;   // per MB row: first step, -1 = row not scored
+  const uint8_t* row_top;  // per MB row: has a top MB edge
+  int steps;
+  uint64_t* ssd_out;  // [64 * 8], indexed level * 8 + sharpness
+  uint8_t* oy;        // write-back planes (apply mode) or null
+  uint8_t* ou;
+  uint8_t* ov;
+  uint8_t* gslots;  // global slot storage when shared memory is too small
+  int smem_slots;
+  // Sweep mode: a level-0 candidate scores the unfiltered planes
+  // (score_filter_candidate's short cut, src/loop_filter.rs:2071). Apply
+  // mode runs the pass with the base level as given, since per-MB
+  // segment overrides and deltas can still filter MBs at base level 0.
+  int level0_unfiltered;
+};
+
+__device__ __forceinline__ int c8(int v) { return min(max(v, -128), 127); }
+__device__ __forceinline__ int iabs(int v) { return v < 0 ? -v : v; }
+
+// LoopFilterParams::derive (src/loop_filter.rs:99-148).
+struct Prm {
+  int interior, hev, mbedge, subedge;
+};
+__device__ __forceinline__ Prm derive(int level, int sharp, bool key) {
+  int interior = level;
+  if (sharp != 0) {
+    interior >>= (sharp > 4) ? 2 : 1;
+    int cap = max(9 - sharp, 0);
+    if (interior > cap) interior = cap;
+  }
+  if (interior == 0) interior = 1;
+  int hev = key ? (level >= 40 ? 2 : (level >= 15 ? 1 : 0))
+                : (level >= 40 ? 3 : (level >= 20 ? 2 : (level >= 15 ? 1 : 0)));
+  Prm p;
+  p.interior = interior;
+  p.hev = hev;
+  p.mbedge = min((level + 2) * 2 + interior, 255);
+  p.subedge = min(level * 2 + interior, 255);
+  return p;
+}
+
+// calculate_mb_filter_level_inter (src/loop_filter.rs:1280-1331).
+__device__ __forceinline__ int mb_level(const vp8a_filter_config& c, int level0, const vp8a_mb_lf_info& m) {
+  int level = level0;
+  if (c.segmentation_enabled) {
+    int seg = m.segment_id < 0 ? 0 : min((int)m.segment_id, 3);
+    if (c.segment_abs) level = c.segment_lf_level[seg];
+    else level += c.segment_lf_level[seg];
+  }
+  level = clampi(level, 0, 63);
+  if (c.delta_enabled) {
+    int rd = m.ref_frame == VP8A_REF_LAST     ? c.ref_delta_last
+             : m.ref_frame == VP8A_REF_GOLDEN ? c.ref_delta_golden
+             : m.ref_frame == VP8A_REF_ALTREF ? c.ref_delta_altref
+                                              : c.ref_delta_current;
+    level += rd;
+    if (m.ref_frame == VP8A_REF_INTRA) {
+      if (m.y_mode_is_bpred) level += c.bpred_mode_delta;
+    } else if (m.inter_mode == VP8A_MODE_ZERO) {
+      level += c.zero_mv_mode_delta;
+    } else if (m.inter_mode == VP8A_MODE_SPLIT) {
+      level += c.split_mv_mode_delta;
+    } else {
+      level += c.other_mv_mode_delta;
+    }
+  }
+  return clampi(level, 0, 63);
+}
+
+// §15.3 MBfilter (src/loop_filter.rs:331-371) on signed taps p[o..o+8).
+template <int O, int N>
+__device__ __forceinline__ void mb_filter(int (&p)[N], const Prm& q) {
+  const int p3 = p[O], p2 = p[O + 1], p1 = p[O + 2], p0 = p[O + 3];
+  const int q0 = p[O + 4], q1 = p[O + 5], q2 = p[O + 6], q3 = p[O + 7];
+  const bool yes = (iabs(p0 - q0) * 2 + (iabs(p1 - q1) >> 1)) <= q.mbedge && iabs(p3 - p2) <= q.interior &&
+                   iabs(p2 - p1) <= q.interior && iabs(p1 - p0) <= q.interior && iabs(q3 - q2) <= q.interior &&
+                   iabs(q2 - q1) <= q.interior && iabs(q1 - q0) <= q.interior;
+  const bool hv = iabs(p1 - p0) > q.hev || iabs(q1 - q0) > q.hev;
+  const int w = c8(c8(p1 - q1) + 3 * (q0 - p0));
+  if (yes) {
+    if (!hv) {
+      int a = c8((27 * w + 63) >> 7);
+      p[O + 4] = c8(q0 - a);
+      p[O + 3] = c8(p0 + a);
+      a = c8((18 * w + 63) >> 7);
+      p[O + 5] = c8(q1 - a);
+      p[O + 2] = c8(p1 + a);
+      a = c8((9 * w + 63) >> 7);
+      p[O + 6] = c8(q2 - a);
+      p[O + 1] = c8(p2 + a);
+    } else {
+      const int a = c8(w + 4) >> 3, b = c8(w + 3) >> 3;
+      p[O + 4] = c8(q0 - a);
+      p[O + 3] = c8(p0 + b);
+    }
+  }
+}
+
+// §15.3 subblock_filter (src/loop_filter.rs:292-318).
+template <int O, int N>
+__device__ __forceinline__ void sb_filter(int (&p)[N], const Prm& q) {
+  const int p3 = p[O], p2 = p[O + 1], p1 = p[O + 2], p0 = p[O + 3];
+  const int q0 = p[O + 4], q1 = p[O + 5], q2 = p[O + 6], q3 = p[O + 7];
+  const bool yes = (iabs(p0 - q0) * 2 + (iabs(p1 - q1) >> 1)) <= q.subedge && iabs(p3 - p2) <= q.interior &&
+                   iabs(p2 - p1) <= q.interior && iabs(p1 - p0) <= q.interior && iabs(q3 - q2) <= q.interior &&
+                   iabs(q2 - q1) <= q.interior && iabs(q1 - q0) <= q.interior;
+  const bool hv = iabs(p1 - p0) > q.hev || iabs(q1 - q0) > q.hev;
+  int a = c8((hv ? c8(p1 - q1) : 0) + 3 * (q0 - p0));
+  const int b = c8(a + 3) >> 3;
+  a = c8(a + 4) >> 3;
+  if (yes) {
+    p[O + 4] = c8(q0 - a);
+    p[O + 3] = c8(p0 + b);
+    if (!hv) {
+      const int a2 = (a + 1) >> 1;
+      p[O + 5] = c8(q1 - a2);
+      p[O + 2] = c8(p1 + a2);
+    }
+  }
+}
+
+// §15.2 simple_segment (src/loop_filter.rs:235-247) on signed taps.
+template <int O, int N>
+__device__ __forceinline__ void simple_filter(int (&p)[N], int edge) {
+  const int p1 = p[O], p0 = p[O + 1], q0 = p[O + 2], q1 = p[O + 3];
+  if (iabs(p0 - q0) * 2 + (iabs(p1 - q1) >> 1) <= edge) {
+    int a = c8(c8(p1 - q1) + 3 * (q0 - p0));
+    const int b = c8(a + 3) >> 3;
+    a = c8(a + 4) >> 3;
+    p[O + 2] = c8(q0 - a);
+    p[O + 1] = c8(p0 + b);
+  }
+}
+
+__device__ __forceinline__ void unpack4(uint32_t w, int* o) {
+#pragma unroll
+  for (int k = 0; k < 4; k++) o[k] = (int)((w >> (8 * k)) & 0xffu) - 128;
+}
+__device__ __forceinline__ uint32_t pack4(const int* o) {
+  return (uint32_t)(o[0] + 128) | ((uint32_t)(o[1] + 128) << 8) | ((uint32_t)(o[2] + 128) << 16) |
+         ((uint32_t)(o[3] + 128) << 24);
+}
+
+__device__ __forceinline__ uint8_t* slot_ptr(uint8_t* slots, int r, int c) {
+  return slots + ((size_t)r * 4 + (c & 3)) * SLOT;
+}
+
+// Filter MB (r, c) held in its slot; neighbours in their slots.
+__device__ __forceinline__ void filter_mb(const LfArgs& a, uint8_t* slots, int level0, int sharp, int r, int c,
+                                          bool has_top, int lane) {
+  const vp8a_mb_lf_info m = a.mbs[(size_t)r * a.mb_cols + c];
+  const int level = mb_level(a.base, level0, m);
+  if (level == 0) return;
+  const Prm q = derive(level, sharp, a.base.key_frame != 0);
+  const bool sub = m.y_mode_is_bpred || m.has_coeffs;
+  const bool has_left = c > 0;
+  uint8_t* me = slot_ptr(slots, r, c);
+  uint8_t* left = slot_ptr(slots, r, c - 1);
+  uint8_t* above = has_top ? slot_ptr(slots, r - 1, c) : nullptr;
+
+  if (a.base.simple) {
+    // §20.6 filter_row_simple: luma only.
+    if (lane < 16) {
+      uint32_t* rw = (uint32_t*)(me + lane * 16);
+      int p[20];
+      unpack4(has_left ? *(const uint32_t*)(left + lane * 16 + 12) : 0x80808080u, p);
+#pragma unroll
+      for (int k = 0; k < 4; k++) unpack4(rw[k], p + 4 + 4 * k);
+      if (has_left) simple_filter<2>(p, q.mbedge);
+      if (sub) {
+        simple_filter<6>(p, q.subedge);
+        simple_filter<10>(p, q.subedge);
+        simple_filter<14>(p, q.subedge);
+      }
+      if (has_left) *(uint32_t*)(left + lane * 16 + 12) = pack4(p);
+#pragma unroll
+      for (int k = 0; k < 4; k++) rw[k] = pack4(p + 4 + 4 * k);
+    }
+    __syncwarp();
+    if (lane < 16) {
+      int p[20];
+#pragma unroll
+      for (int k = 0; k < 4; k++) p[k] = has_top ? (int)above[(12 + k) * 16 + lane] - 128 : 0;
+#pragma unroll
+      for (int k = 0; k < 16; k++) p[4 + k] = (int)me[k * 16 + lane] - 128;
+      if (has_top) simple_filter<2>(p, q.mbedge);
+      if (sub) {
+        simple_filter<6>(p, q.subedge);
+        simple_filter<10>(p, q.subedge);
+        simple_filter<14>(p, q.subedge);
+      }
+      if (has_top)
+#pragma unroll
+        for (int k = 2; k < 4; k++) above[(12 + k) * 16 + lane] = (uint8_t)(p[k] + 128);
+#pragma unroll
+      for (int k = 0; k < 16; k++) me[k * 16 + lane] = (uint8_t)(p[4 + k] + 128);
+    }
+    __syncwarp();
+    return;
+  }
+
+  // ---- vertical edges (steps 1 and 2) ----
+  if (lane < 16) {
+    uint32_t* rw = (uint32_t*)(me + lane * 16);
+    int p[20];
+    unpack4(has_left ? *(const uint32_t*)(left + lane * 16 + 12) : 0x80808080u, p);
+#pragma unroll
+    for (int k = 0; k < 4; k++) unpack4(rw[k], p + 4 + 4 * k);
+    if (has_left) mb_filter<0>(p, q);
+    if (sub) {
+      sb_filter<4>(p, q);
+      sb_filter<8>(p, q);
+      sb_filter<12>(p, q);
+    }
+    if (has_left) *(uint32_t*)(left + lane * 16 + 12) = pack4(p);
+#pragma unroll
+    for (int k = 0; k < 4; k++) rw[k] = pack4(p + 4 + 4 * k);
+  } else {
+    const int pl = lane < 24 ? 256 : 320, row = (lane - 16) & 7;
+    uint32_t* rw = (uint32_t*)(me + pl + row * 8);
+    int p[12];
+    unpack4(has_left ? *(const uint32_t*)(left + pl + row * 8 + 4) : 0x80808080u, p);
+    unpack4(rw[0], p + 4);
+    unpack4(rw[1], p + 8);
+    if (has_left) mb_filter<0>(p, q);
+    if (sub) sb_filter<4>(p, q);
+    if (has_left) *(uint32_t*)(left + pl + row * 8 + 4) = pack4(p);
+    rw[0] = pack4(p + 4);
+    rw[1] = pack4(p + 8);
+  }
+  __syncwarp();
+  // ---- horizontal edges (steps 3 and 4) ----
+  if (lane < 16) {
+    int p[20];
+#pragma unroll
+    for (int k = 0; k < 4; k++) p[k] = has_top ? (int)above[(12 + k) * 16 + lane] - 128 : 0;
+#pragma unroll
+    for (int k = 0; k < 16; k++) p[4 + k] = (int)me[k * 16 + lane] - 128;
+    if (has_top) mb_filter<0>(p, q);
+    if (sub) {
+      sb_filter<4>(p, q);
+      sb_filter<8>(p, q);
+      sb_filter<12>(p, q);
+    }
+    if (has_top)
+#pragma unroll
+      for (int k = 1; k < 4; k++) above[(12 + k) * 16 + lane] = (uint8_t)(p[k] + 128);
+#pragma unroll
+    for (int k = 0; k < 16; k++) me[k * 16 + lane] = (uint8_t)(p[4 + k] + 128);
+  } else {
+    const int pl = lane < 24 ? 256 : 320, col = (lane - 16) & 7;
+    int p[12];
+#pragma unroll
+    for (int k = 0; k < 4; k++) p[k] = has_top ? (int)above[pl + (4 + k) * 8 + col] - 128 : 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) p[4 + k] = (int)me[pl + k * 8 + col] - 128;
+    if (has_top) mb_filter<0>(p, q);
+    if (sub) sb_filter<4>(p, q);
+    if (has_top)
+#pragma unroll
+      for (int k = 1; k < 4; k++) above[pl + (4 + k) * 8 + col] = (uint8_t)(p[k] + 128);
+#pragma unroll
+    for (int k = 0; k < 8; k++) me[pl + k * 8 + col] = (uint8_t)(p[4 + k] + 128);
+  }
+  __syncwarp();
+}
+
+// Load MB (r, c) of the unfiltered reconstruction into its slot.
+__device__ __forceinline__ void load_mb(const LfArgs& a, uint8_t* slots, int r, int c, int lane) {
+  uint8_t* s = slot_ptr(slots, r, c);
+  const size_t yo = (size_t)r * 16 * a.ys + (size_t)c * 16;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    int i = lane + 32 * k, rr = i >> 4, cc = i & 15;
+    s[i] = a.y[yo + rr * a.ys + cc];
+  }
+  const size_t co = (size_t)r * 8 * a.cs + (size_t)c * 8;
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    int i = lane + 32 * k, rr = i >> 3, cc = i & 7;
+    s[256 + i] = a.u[co + rr * a.cs + cc];
+    s[320 + i] = a.v[co + rr * a.cs + cc];
+  }
+  __syncwarp();
+}
+
+// Score (or write back) final MB (r, c): visible-window SSD vs the source.
+__device__ __forceinline__ uint64_t finish_mb(const LfArgs& a, const uint8_t* slots, int r, int c, int lane) {
+  const uint8_t* s = slot_ptr(const_cast<uint8_t*>(slots), r, c);
+  if (a.oy) {
+    const size_t yo = (size_t)r * 16 * a.ys + (size_t)c * 16;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      int i = lane + 32 * k;
+      a.oy[yo + (i >> 4) * a.ys + (i & 15)] = s[i];
+    }
+    const size_t co = (size_t)r * 8 * a.cs + (size_t)c * 8;
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      int i = lane + 32 * k;
+      a.ou[co + (i >> 3) * a.cs + (i & 7)] = s[256 + i];
+      a.ov[co + (i >> 3) * a.cs + (i & 7)] = s[320 + i];
+    }
+  }
+  if (!a.ssd_out) return 0;
+  uint32_t acc = 0;
+  const int y0 = r * 16, x0 = c * 16;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    int i = lane + 32 * k, rr = i >> 4, cc = i & 15;
+    if (y0 + rr < a.height && x0 + cc < a.width) {
+      int d = (int)s[i] - (int)a.sy[(size_t)(y0 + rr) * a.sys + x0 + cc];
+      acc += (uint32_t)(d * d);
+    }
+  }
+  const int cw = (a.width + 1) >> 1, ch = (a.height + 1) >> 1;
+  const int cy0 = r * 8, cx0 = c * 8;
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    int i = lane + 32 * k, rr = i >> 3, cc = i & 7;
+    if (cy0 + rr < ch && cx0 + cc < cw) {
+      size_t so = (size_t)(cy0 + rr) * a.scs + cx0 + cc;
+      int du = (int)s[256 + i] - (int)a.su[so];
+      int dv = (int)s[320 + i] - (int)a.sv[so];
+      acc += (uint32_t)(du * du) + (uint32_t)(dv * dv);
+    }
+  }
+  return acc;
+}
+
+__device__ __forceinline__ void block_sum_store(uint64_t v, uint64_t* dst) {
+  __shared__ unsigned long long red[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    v = lane < (int)(blockDim.x >> 5) ? red[lane] : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    if (lane == 0) *dst = v;
+  }
+}
+
+__global__ void __launch_bounds__(1024) lf_sweep_kernel(LfArgs a) {
+  extern __shared__ __align__(16) uint8_t smem_slots[];
+  const int level0 = a.cands[2 * blockIdx.x], sharp = a.cands[2 * blockIdx.x + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  uint64_t acc = 0;
+  if (level0 == 0 && a.level0_unfiltered) {
+    // score_filter_candidate level 0: the unfiltered reconstruction.
+    for (int r = warp; r < a.mb_rows; r += nwarps) {
+      if (a.row_t0[r] < 0) continue;
+      for (int c = 0; c < a.mb_cols; c++) {
+        const int y0 = r * 16, x0 = c * 16;
+        uint32_t s32 = 0;
+        for (int k = 0; k < 8; k++) {
+          int i = lane + 32 * k, rr = i >> 4, cc = i & 15;
+          if (y0 + rr < a.height && x0 + cc < a.width) {
+            int d = (int)a.y[(size_t)(y0 + rr) * a.ys + x0 + cc] - (int)a.sy[(size_t)(y0 + rr) * a.sys + x0 + cc];
+            s32 += (uint32_t)(d * d);
+          }
+        }
+        const int cw = (a.width + 1) >> 1, ch = (a.height + 1) >> 1;
+        for (int k = 0; k < 2; k++) {
+          int i = lane + 32 * k, rr = i >> 3, cc = i & 7, cy = r * 8 + rr, cx = c * 8 + cc;
+          if (cy < ch && cx < cw) {
+            int du = (int)a.u[(size_t)cy * a.cs + cx] - (int)a.su[(size_t)cy * a.scs + cx];
+            int dv = (int)a.v[(size_t)cy * a.cs + cx] - (int)a.sv[(size_t)cy * a.scs + cx];
+            s32 += (uint32_t)(du * du) + (uint32_t)(dv * dv);
+          }
+        }
+        acc += s32;
+      }
+    }
+    block_sum_store(acc, &a.ssd_out[level0 * 8 + sharp]);
+    return;
+  }
+  uint8_t* slots = a.smem_slots ? smem_slots : a.gslots + (size_t)blockIdx.x * a.mb_rows * 4 * SLOT;
+  for (int t = 0; t < a.steps; t++) {
+    for (int r = warp; r < a.mb_rows; r += nwarps) {
+      const int t0 = a.row_t0[r];
+      if (t0 < 0) continue;
+      const int c = t - t0;
+      if (c < 0 || c >= a.mb_cols) continue;
+      if (c >= 4) acc += finish_mb(a, slots, r, c - 4, lane);
+      __syncwarp();
+      load_mb(a, slots, r, c, lane);
+      filter_mb(a, slots, level0, sharp, r, c, a.row_top[r] != 0, lane);
+    }
+    __syncthreads();
+  }
+  for (int r = warp; r < a.mb_rows; r += nwarps) {
+    if (a.row_t0[r] < 0) continue;
+    for (int c = max(0, a.mb_cols - 4); c < a.mb_cols; c++) acc += finish_mb(a, slots, r, c, lane);
+  }
+  if (a.ssd_out) block_sum_store(acc, &a.ssd_out[level0 * 8 + sharp]);
+}
+
+// Plain visible-window SSD of a reconstruction (reconstruction_ssd).
+__global__ void __launch_bounds__(256) ssd_kernel(const uint8_t* rec, uint64_t rs, const uint8_t* src, uint64_t ss,
+                                                  int w, int h, unsigned long long* out) {
+  uint64_t acc = 0;
+  const size_t n = (size_t)w * h;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    int y = (int)(i / w), x = (int)(i % w);
+    int d = (int)rec[(size_t)y * rs + x] - (int)src[(size_t)y * ss + x];
+    acc += (uint64_t)(d * d);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(FULL, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, (unsigned long long)acc);
+}
+
+// ------------------------------------------------------------------- host
+
+struct LfInputs {
+  LfArgs a{};
+  int max_steps = 0;
+};
+
+vp8a_status validate_config(const vp8a_filter_config* c) {
+  if (c->loop_filter_level > 63) {
+    vp8a::set_error("loop_filter_level > 63");
+    return VP8A_E_LOOP_FILTER_LEVEL_OUT_OF_RANGE;
+  }
+  if (c->sharpness_level > 7) {
+    vp8a::set_error("sharpness_level > 7");
+    return VP8A_E_SHARPNESS_LEVEL_OUT_OF_RANGE;
+  }
+  return VP8A_OK;
+}
+
+// Stages planes, per-MB info and (optionally) the source; fills the row
+// schedule for whole frames (every_rows = 0) or sampled bands.
+vp8a_status stage_lf(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_planes* planes, const vp8a_mb_lf_info* mbs,
+                     const vp8a_filter_config* base, const vp8a_source* src, uint32_t every_rows, bool write_back,
+                     LfInputs* L) {
+  if (!planes || !mbs || !base) {
+    vp8a::set_error("null argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (planes->mb_cols == 0 || planes->mb_rows == 0 || planes->mb_cols > 1024 || planes->mb_rows > 1024) {
+    vp8a::set_error("plane MB grid out of range");
+    return VP8A_E_INVALID_DIMENSIONS;
+  }
+  if (planes->y_stride < (uint64_t)planes->mb_cols * 16 || planes->uv_stride < (uint64_t)planes->mb_cols * 8) {
+    vp8a::set_error("plane stride below the MB-padded width");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  vp8a_status s = validate_config(base);
+  if (s != VP8A_OK) return s;
+  LfArgs& a = L->a;
+  const int cols = (int)planes->mb_cols, rows = (int)planes->mb_rows;
+  const size_t yb = planes->y_stride * (size_t)rows * 16, cb = planes->uv_stride * (size_t)rows * 8;
+  const void* d;
+  void* dm;
+  if (write_back) {
+    if ((s = st.inout(planes->y, yb, &dm)) != VP8A_OK) return s;
+    a.y = (const uint8_t*)dm;
+    a.oy = (uint8_t*)dm;
+    if ((s = st.inout(planes->u, cb, &dm)) != VP8A_OK) return s;
+    a.u = (const uint8_t*)dm;
+    a.ou = (uint8_t*)dm;
+    if ((s = st.inout(planes->v, cb, &dm)) != VP8A_OK) return s;
+    a.v = (const uint8_t*)dm;
+    a.ov = (uint8_t*)dm;
+  } else {
+    if ((s = st.in(planes->y, yb, &d)) != VP8A_OK) return s;
+    a.y = (const uint8_t*)d;
+    if ((s = st.in(planes->u, cb, &d)) != VP8A_OK) return s;
+    a.u = (const uint8_t*)d;
+    if ((s = st.in(planes->v, cb, &d)) != VP8A_OK) return s;
+    a.v = (const uint8_t*)d;
+  }
+  a.ys = planes->y_stride;
+  a.cs = planes->uv_stride;
+  a.mb_cols = cols;
+  a.mb_rows = rows;
+  if ((s = st.in(mbs, sizeof(vp8a_mb_lf_info) * (size_t)cols * rows, &d)) != VP8A_OK) return s;
+  a.mbs = (const vp8a_mb_lf_info*)d;
+  a.base = *base;
+  if (src) {
+    if (src->width == 0 || src->height == 0 || src->width > (uint32_t)cols * 16 ||
+        src->height > (uint32_t)rows * 16) {
+      vp8a::set_error("source size does not fit the MB grid");
+      return VP8A_E_REFERENCE_DIMENSIONS_MISMATCH;
+    }
+    const uint32_t w = src->width, h = src->height, cw = (w + 1) / 2, ch = (h + 1) / 2;
+    if (src->y_stride < w || src->uv_stride < cw) {
+      vp8a::set_error("source stride below width");
+      return VP8A_E_INVALID_ARGUMENT;
+    }
+    if ((s = st.in(src->y, src->y_stride * (size_t)(h - 1) + w, &d)) != VP8A_OK) return s;
+    a.sy = (const uint8_t*)d;
+    if ((s = st.in(src->u, src->uv_stride * (size_t)(ch - 1) + cw, &d)) != VP8A_OK) return s;
+    a.su = (const uint8_t*)d;
+    if ((s = st.in(src->v, src->uv_stride * (size_t)(ch - 1) + cw, &d)) != VP8A_OK) return s;
+    a.sv = (const uint8_t*)d;
+    a.sys = src->y_stride;
+    a.scs = src->uv_stride;
+    a.width = (int)w;
+    a.height = (int)h;
+  }
+  // Row schedule.
+  std::vector<int16_t> t0(rows, -1);
+  std::vector<uint8_t> top(rows, 0);
+  int max_t0 = 0;
+  if (every_rows == 0) {
+    for (int r = 0; r < rows; r++) {
+      t0[r] = (int16_t)(2 * r);
+      top[r] = r > 0;
+    }
+    max_t0 = 2 * (rows - 1);
+  } else {
+    const int step = every_rows < 2 ? 2 : (int)every_rows;
+    for (int fr = 0; fr < rows; fr += step)
+      for (int k = 0; k < 2 && fr + k < rows; k++) {
+        t0[fr + k] = (int16_t)(2 * k);
+        top[fr + k] = k > 0;
+        max_t0 = std::max(max_t0, 2 * k);
+      }
+  }
+  void* dt0;
+  void* dtop;
+  if ((s = st.scratch(sizeof(int16_t) * rows, &dt0)) != VP8A_OK) return s;
+  if ((s = st.scratch(rows, &dtop)) != VP8A_OK) return s;
+  VP8A_CUDA(cudaMemcpyAsync(dt0, t0.data(), sizeof(int16_t) * rows, cudaMemcpyHostToDevice, ctx->stream));
+  VP8A_CUDA(cudaMemcpyAsync(dtop, top.data(), rows, cudaMemcpyHostToDevice, ctx->stream));
+  VP8A_CUDA(cudaStreamSynchronize(ctx->stream));  // host vectors go out of scope
+  a.row_t0 = (const int16_t*)dt0;
+  a.row_top = (const uint8_t*)dtop;
+  a.steps = max_t0 + cols;
+  L->max_steps = a.steps;
+  return VP8A_OK;
+}
+
+// Launch the sweep over `n` candidates (pairs of level, sharpness).
+vp8a_status launch_sweep(vp8a_ctx* ctx, vp8a::Stager& st, LfArgs a, const uint8_t* cands, int n) {
+  if (n == 0) return VP8A_OK;
+  void* dc;
+  vp8a_status s;
+  if ((s = st.scratch((size_t)n * 2, &dc)) != VP8A_OK) return s;
+  VP8A_CUDA(cudaMemcpyAsync(dc, cands, (size_t)n * 2, cudaMemcpyHostToDevice, ctx->stream));
+  a.cands = (const uint8_t*)dc;
+  const size_t slot_bytes = (size_t)a.mb_rows * 4 * SLOT;
+  int max_smem = 0;
+  VP8A_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+  int threads = std::min(1024, 32 * a.mb_rows);
+  if (slot_bytes + 1024 <= (size_t)max_smem) {
+    a.smem_slots = 1;
+    a.gslots = nullptr;
+    VP8A_CUDA(cudaFuncSetAttribute(lf_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slot_bytes));
+    lf_sweep_kernel<<<n, threads, slot_bytes, ctx->stream>>>(a);
+  } else {
+    void* g;
+    if ((s = st.scratch(slot_bytes * n, &g)) != VP8A_OK) return s;
+    a.smem_slots = 0;
+    a.gslots = (uint8_t*)g;
+    lf_sweep_kernel<<<n, threads, 0, ctx->stream>>>(a);
+  }
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
+  return VP8A_OK;
+}
+
+// Score `cands` into `table` (host, 512 entries indexed level * 8 + sharp).
+vp8a_status score_candidates(vp8a_ctx* ctx, vp8a::Stager& st, const LfArgs& a, void* dtable,
+                             const std::vector<uint8_t>& cands, uint64_t* table) {
+  vp8a_status s = launch_sweep(ctx, st, a, cands.data(), (int)(cands.size() / 2));
+  if (s != VP8A_OK) return s;
+  VP8A_CUDA(cudaMemcpyAsync(table, dtable, 512 * sizeof(uint64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  VP8A_CUDA(cudaStreamSynchronize(ctx->stream));
+  return VP8A_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+vp8a_status vp8a_filter_frame(vp8a_ctx* ctx, vp8a_planes* planes, const vp8a_mb_lf_info* mbs,
+                              const vp8a_filter_config* config) {
+  if (!ctx) return VP8A_E_INVALID_ARGUMENT;
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  LfInputs L;
+  vp8a_status s = stage_lf(ctx, st, planes, mbs, config, nullptr, 0, true, &L);
+  if (s != VP8A_OK) return s;
+  const uint8_t cand[2] = {config->loop_filter_level, config->sharpness_level};
+  L.a.level0_unfiltered = 0;
+  if ((s = launch_sweep(ctx, st, L.a, cand, 1)) != VP8A_OK) return s;
+  st.force_sync();  // `cand` must outlive its async copy
+  return st.finish();
+}
+
+vp8a_status vp8a_reconstruction_ssd(vp8a_ctx* ctx, const vp8a_planes* planes, const vp8a_source* src,
+                                    uint64_t* ssd_out) {
+  if (!ctx || !planes || !src || !ssd_out) return VP8A_E_INVALID_ARGUMENT;
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  const uint32_t w = src->width, h = src->height, cw = (w + 1) / 2, ch = (h + 1) / 2;
+  if (w == 0 || h == 0 || w > planes->mb_cols * 16 || h > planes->mb_rows * 16) {
+    vp8a::set_error("source size does not fit the MB grid");
+    return VP8A_E_REFERENCE_DIMENSIONS_MISMATCH;
+  }
+  vp8a_status s;
+  const void *ry, *ru, *rv, *sy, *su, *sv;
+  if ((s = st.in(planes->y, planes->y_stride * (size_t)(h - 1) + w, &ry)) != VP8A_OK) return s;
+  if ((s = st.in(planes->u, planes->uv_stride * (size_t)(ch - 1) + cw, &ru)) != VP8A_OK) return s;
+  if ((s = st.in(planes->v, planes->uv_stride * (size_t)(ch - 1) + cw, &rv)) != VP8A_OK) return s;
+  if ((s = st.in(src->y, src->y_stride * (size_t)(h - 1) + w, &sy)) != VP8A_OK) return s;
+  if ((s = st.in(src->u, src->uv_stride * (size_t)(ch - 1) + cw, &su)) != VP8A_OK) return s;
+  if ((s = st.in(src->v, src->uv_stride * (size_t)(ch - 1) + cw, &sv)) != VP8A_OK) return s;
+  void* acc;
+  if ((s = st.out(ssd_out, sizeof(uint64_t), &acc)) != VP8A_OK) return s;
+  VP8A_CUDA(cudaMemsetAsync(acc, 0, sizeof(uint64_t), ctx->stream));
+  unsigned grid = (unsigned)std::max(1, ctx->sm_count * 4);
+  ssd_kernel<<<grid, 256, 0, ctx->stream>>>((const uint8_t*)ry, planes->y_stride, (const uint8_t*)sy, src->y_stride,
+                                            (int)w, (int)h, (unsigned long long*)acc);
+  ssd_kernel<<<grid, 256, 0, ctx->stream>>>((const uint8_t*)ru, planes->uv_stride, (const uint8_t*)su,
+                                            src->uv_stride, (int)cw, (int)ch, (unsigned long long*)acc);
+  ssd_kernel<<<grid, 256, 0, ctx->stream>>>((const uint8_t*)rv, planes->uv_stride, (const uint8_t*)sv,
+                                            src->uv_stride, (int)cw, (int)ch, (unsigned long long*)acc);
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches += 3;
+  return st.finish();
+}
+
+vp8a_status vp8a_filter_sweep(vp8a_ctx* ctx, const vp8a_planes* planes, const vp8a_mb_lf_info* mbs,
+                              const vp8a_filter_config* base, const vp8a_source* src, uint32_t every_rows,
+                              uint64_t* ssd_out) {
+  if (!ctx || !src || !ssd_out) return VP8A_E_INVALID_ARGUMENT;
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  LfInputs L;
+  vp8a_status s = stage_lf(ctx, st, planes, mbs, base, src, every_rows, false, &L);
+  if (s != VP8A_OK) return s;
+  void* dt;
+  if ((s = st.out(ssd_out, 512 * sizeof(uint64_t), &dt)) != VP8A_OK) return s;
+  L.a.ssd_out = (uint64_t*)dt;
+  L.a.level0_unfiltered = 1;
+  // One level-0 candidate plus every (level 1..63, sharpness 0..7).
+  std::vector<uint8_t> c;
+  c.reserve(2 * 505);
+  c.push_back(0);
+  c.push_back(0);
+  for (int l = 1; l < 64; l++)
+    for (int sh = 0; sh < 8; sh++) {
+      c.push_back((uint8_t)l);
+      c.push_back((uint8_t)sh);
+    }
+  if ((s = launch_sweep(ctx, st, L.a, c.data(), (int)(c.size() / 2))) != VP8A_OK) return s;
+  // Level 0 scores the same for every sharpness.
+  for (int sh = 1; sh < 8; sh++)
+    VP8A_CUDA(cudaMemcpyAsync((uint64_t*)dt + sh, dt, sizeof(uint64_t), cudaMemcpyDeviceToDevice, ctx->stream));
+  st.force_sync();  // the candidate vector must outlive its async copy
+  return st.finish();
+}
+
+vp8a_status vp8a_select_filter_params(vp8a_ctx* ctx, const vp8a_planes* planes, const vp8a_mb_lf_info* mbs,
+                                      const vp8a_filter_config* base, const vp8a_source* src, uint8_t* level_out,
+                                      uint8_t* sharpness_out) {
+  if (!ctx || !src || !level_out || !sharpness_out) return VP8A_E_INVALID_ARGUMENT;
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  LfInputs L;
+  vp8a_status s = stage_lf(ctx, st, planes, mbs, base, src, 0, false, &L);
+  if (s != VP8A_OK) return s;
+  void* dt;
+  if ((s = st.scratch(512 * sizeof(uint64_t), &dt)) != VP8A_OK) return s;
+  VP8A_CUDA(cudaMemsetAsync(dt, 0, 512 * sizeof(uint64_t), ctx->stream));
+  L.a.ssd_out = (uint64_t*)dt;
+  L.a.level0_unfiltered = 1;
+  std::vector<uint64_t> t(512, 0);
+  const uint8_t bs = base->sharpness_level > 7 ? 7 : base->sharpness_level;
+  // Stage 1: grid 0, 4, ..., 60, 63 at the base sharpness.
+  std::vector<uint8_t> c;
+  for (int l = 0; l <= 60; l += 4) {
+    c.push_back((uint8_t)l);
+    c.push_back(bs);
+  }
+  c.push_back(63);
+  c.push_back(bs);
+  if ((s = score_candidates(ctx, st, L.a, dt, c, t.data())) != VP8A_OK) return s;
+  uint8_t best_level = 0;
+  uint64_t best = t[0 * 8 + bs];
+  for (size_t i = 2; i < c.size(); i += 2)
+    if (t[c[i] * 8 + bs] < best) {
+      best = t[c[i] * 8 + bs];
+      best_level = c[i];
+    }
+  // Refine +/-3 around the grid winner, excluding it.
+  const int lo = best_level >= 3 ? best_level - 3 : 0, hi = std::min(63, best_level + 3);
+  c.clear();
+  for (int l = lo; l <= hi; l++)
+    if (l != best_level) {
+      c.push_back((uint8_t)l);
+      c.push_back(bs);
+    }
+  if ((s = score_candidates(ctx, st, L.a, dt, c, t.data())) != VP8A_OK) return s;
+  for (size_t i = 0; i < c.size(); i += 2)
+    if (t[c[i] * 8 + bs] < best) {
+      best = t[c[i] * 8 + bs];
+      best_level = c[i];
+    }
+  if (best_level == 0) {
+    *level_out = 0;
+    *sharpness_out = bs;
+    return st.finish();
+  }
+  // Stage 2: the other sharpness values at the chosen level.
+  c.clear();
+  for (int sh = 0; sh < 8; sh++)
+    if (sh != bs) {
+      c.push_back(best_level);
+      c.push_back((uint8_t)sh);
+    }
+  if ((s = score_candidates(ctx, st, L.a, dt, c, t.data())) != VP8A_OK) return s;
+  uint8_t best_sharp = bs;
+  for (size_t i = 0; i < c.size(); i += 2)
+    if (t[best_level * 8 + c[i + 1]] < best) {
+      best = t[best_level * 8 + c[i + 1]];
+      best_sharp = c[i + 1];
+    }
+  *level_out = best_level;
+  *sharpness_out = best_sharp;
+  return st.finish();
+}
+
+vp8a_status vp8a_select_filter_params_sampled(vp8a_ctx* ctx, const vp8a_planes* planes, const vp8a_mb_lf_info* mbs,
+                                              const vp8a_filter_config* base, const vp8a_source* src,
+                                              uint32_t every_rows, uint32_t sweep_sharpness, uint8_t* level_out,
+                                              uint8_t* sharpness_out) {
+  if (!ctx || !src || !level_out || !sharpness_out) return VP8A_E_INVALID_ARGUMENT;
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  LfInputs L;
+  const uint32_t er = every_rows < 2 ? 2 : every_rows;
+  vp8a_status s = stage_lf(ctx, st, planes, mbs, base, src, er, false, &L);
+  if (s != VP8A_OK) return s;
+  void* dt;
+  if ((s = st.scratch(512 * sizeof(uint64_t), &dt)) != VP8A_OK) return s;
+  VP8A_CUDA(cudaMemsetAsync(dt, 0, 512 * sizeof(uint64_t), ctx->stream));
+  L.a.ssd_out = (uint64_t*)dt;
+  L.a.level0_unfiltered = 1;
+  std::vector<uint64_t> t(512, 0);
+  const uint8_t bs = base->sharpness_level > 7 ? 7 : base->sharpness_level;
+  static const uint8_t coarse[9] = {0, 8, 16, 24, 32, 40, 48, 56, 63};
+  std::vector<uint8_t> c;
+  for (uint8_t l : coarse) {
+    c.push_back(l);
+    c.push_back(bs);
+  }
+  if ((s = score_candidates(ctx, st, L.a, dt, c, t.data())) != VP8A_OK) return s;
+  uint8_t best_level = 0;
+  uint64_t best = t[0 * 8 + bs];
+  for (int i = 1; i < 9; i++)
+    if (t[coarse[i] * 8 + bs] < best) {
+      best = t[coarse[i] * 8 + bs];
+      best_level = coarse[i];
+    }
+  for (uint8_t stp : {4, 2, 1}) {
+    c.clear();
+    if (best_level >= stp) {
+      c.push_back((uint8_t)(best_level - stp));
+      c.push_back(bs);
+    }
+    if (best_level + stp <= 63) {
+      c.push_back((uint8_t)(best_level + stp));
+      c.push_back(bs);
+    }
+    if ((s = score_candidates(ctx, st, L.a, dt, c, t.data())) != VP8A_OK) return s;
+    uint8_t bl = best_level;
+    for (size_t i = 0; i < c.size(); i += 2)
+      if (t[c[i] * 8 + bs] < best) {
+        best = t[c[i] * 8 + bs];
+        bl = c[i];
+      }
+    best_level = bl;
+  }
+  uint8_t best_sharp = bs;
+  if (sweep_sharpness && best_level != 0) {
+    c.clear();
+    for (int sh = 0; sh < 8; sh++)
+      if (sh != bs) {
+        c.push_back(best_level);
+        c.push_back((uint8_t)sh);
+      }
+    if ((s = score_candidates(ctx, st, L.a, dt, c, t.data())) != VP8A_OK) return s;
+    for (size_t i = 0; i < c.size(); i += 2)
+      if (t[best_level * 8 + c[i + 1]] < best) {
+        best = t[best_level * 8 + c[i + 1]];
+        best_sharp = c[i + 1];
+      }
+  }
+  *level_out = best_level;
+  *sharpness_out = best_sharp;
+  return st.finish();
+}
+
+}  // extern "C"

@@ -1,0 +1,102 @@
+// vp8a_internal.cuh — shared internals of libvp8a (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/vp8a.h"
+
+#define VP8A_ABI_VERSION ((1u << 16) | 0u)
+
+// ----------------------------------------------------------------- context
+struct vp8a_ctx {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  uint64_t launches = 0;
+  // Device-resident status word shared by kernels with bounded waits.
+  uint32_t* d_status = nullptr;
+  // Device copy of the 256-entry -log2(p/256) bit-cost table (f64).
+  double* d_bit_cost = nullptr;
+};
+
+namespace vp8a {
+
+void set_error(const std::string& msg);
+vp8a_status cuda_fail(cudaError_t e, const char* what);
+
+#define VP8A_CUDA(call)                                        \
+  do {                                                         \
+    cudaError_t _e = (call);                                   \
+    if (_e != cudaSuccess) return ::vp8a::cuda_fail(_e, #call); \
+  } while (0)
+
+// Device status codes written by kernels (host maps them to vp8a_status).
+enum : uint32_t { DEV_OK = 0, DEV_TIMEOUT = 1, DEV_BAD_INPUT = 2 };
+
+// Host/device staging of ABI buffers. Each buffer passed through the ABI may
+// be host or device memory; host buffers get a stream-ordered device copy.
+class Stager {
+ public:
+  explicit Stager(vp8a_ctx* ctx) : ctx_(ctx) {}
+  ~Stager();
+  // Device view of a read-only input of `bytes` bytes.
+  vp8a_status in(const void* p, size_t bytes, const void** dev);
+  // Device view of an output; host outputs are copied back in finish().
+  vp8a_status out(void* p, size_t bytes, void** dev);
+  // Device view of an in/out buffer.
+  vp8a_status inout(void* p, size_t bytes, void** dev);
+  // Scratch device memory owned by this call.
+  vp8a_status scratch(size_t bytes, void** dev);
+  // Copies host outputs back and synchronises when any host buffer was
+  // involved (otherwise the call stays asynchronous on the stream).
+  vp8a_status finish();
+  bool touched_host() const { return host_; }
+  void force_sync() { host_ = true; }
+
+ private:
+  vp8a_status classify(const void* p, bool* is_device);
+  vp8a_ctx* ctx_;
+  bool host_ = false;
+  struct Back {
+    void* host;
+    void* dev;
+    size_t bytes;
+  };
+  std::vector<Back> backs_;
+  std::vector<void*> owned_;
+};
+
+inline unsigned grid_for(size_t n, unsigned block) {
+  return (unsigned)((n + block - 1) / block);
+}
+
+// Reads the device status word after the call's kernels and maps it.
+vp8a_status check_device_status(vp8a_ctx* ctx);
+
+}  // namespace vp8a
+
+// ------------------------------------------------------------ device helpers
+namespace vp8a_dev {
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// §18.3 six-tap filter table (SIXTAP_FILTERS, src/motion_comp.rs:294;
+// RFC 6386 §18.3 filters[8][6]). One copy per translation unit.
+static __constant__ int c_sixtap[8][6] = {
+    {0, 0, 128, 0, 0, 0},     {0, -6, 123, 12, -1, 0}, {2, -11, 108, 36, -8, 1},
+    {0, -9, 93, 50, -6, 0},   {3, -16, 77, 77, -16, 3}, {0, -6, 50, 93, -9, 0},
+    {1, -8, 36, 108, -11, 2}, {0, -1, 12, 123, -6, 0},
+};
+
+// interp (src/motion_comp.rs:396): dot product, (a + 64) >> 7, clamp255.
+__device__ __forceinline__ int interp6(const int* f, int s0, int s1, int s2, int s3, int s4, int s5) {
+  int a = s0 * f[0] + s1 * f[1] + s2 * f[2] + s3 * f[3] + s4 * f[4] + s5 * f[5];
+  return clampi((a + 64) >> 7, 0, 255);
+}
+
+}  // namespace vp8a_dev

@@ -1,0 +1,222 @@
+"""ctypes / numpy mirrors of the POD types declared in include/vp8a.h.
+
+The C header is the contract; these definitions repeat its layouts so that
+Python callers (and the tests) can pass numpy arrays or torch tensors of
+these records straight through the C ABI. `check_layouts()` asserts the
+sizes against the C compiler's view (exported by the library itself).
+"""
+import ctypes as C
+
+import numpy as np
+
+# vp8a_status (include/vp8a.h)
+OK = 0
+E_INVALID_DIMENSIONS = 1
+E_QUANT_INDEX_OUT_OF_RANGE = 2
+E_LOOP_FILTER_LEVEL_OUT_OF_RANGE = 3
+E_SHARPNESS_LEVEL_OUT_OF_RANGE = 4
+E_REFERENCE_DIMENSIONS_MISMATCH = 5
+E_INVALID_ARGUMENT = 6
+E_CUDA = 7
+E_DEVICE_TIMEOUT = 8
+E_OUT_OF_MEMORY = 9
+E_NO_DEVICE = 10
+
+STATUS_NAMES = {
+    0: "OK",
+    1: "InvalidDimensions",
+    2: "QuantIndexOutOfRange",
+    3: "LoopFilterLevelOutOfRange",
+    4: "SharpnessLevelOutOfRange",
+    5: "ReferenceDimensionsMismatch",
+    6: "InvalidArgument",
+    7: "Cuda",
+    8: "DeviceTimeout",
+    9: "OutOfMemory",
+    10: "NoDevice",
+}
+
+REF_INTRA, REF_LAST, REF_GOLDEN, REF_ALTREF = 0, 1, 2, 3
+MODE_ZERO, MODE_NEAREST, MODE_NEAR, MODE_NEW, MODE_SPLIT, MODE_NONE = 0, 1, 2, 3, 4, 255
+PART_TOP_BOTTOM, PART_LEFT_RIGHT, PART_QUARTERS, PART_MV16, PART_NONE = 0, 1, 2, 3, 255
+
+
+class Mv(C.Structure):
+    _fields_ = [("row", C.c_int16), ("col", C.c_int16)]
+
+
+class SearchResult(C.Structure):
+    _fields_ = [("mv", Mv), ("sad", C.c_uint32)]
+
+
+class LumaRef(C.Structure):
+    _fields_ = [("plane", C.c_void_p), ("stride", C.c_uint64), ("width", C.c_uint32), ("height", C.c_uint32)]
+
+
+class I420(C.Structure):
+    _fields_ = [
+        ("width", C.c_uint32),
+        ("height", C.c_uint32),
+        ("y", C.c_void_p),
+        ("u", C.c_void_p),
+        ("v", C.c_void_p),
+        ("y_stride", C.c_uint64),
+        ("uv_stride", C.c_uint64),
+    ]
+
+
+class Planes(C.Structure):
+    _fields_ = [
+        ("y", C.c_void_p),
+        ("u", C.c_void_p),
+        ("v", C.c_void_p),
+        ("y_stride", C.c_uint64),
+        ("uv_stride", C.c_uint64),
+        ("mb_cols", C.c_uint32),
+        ("mb_rows", C.c_uint32),
+    ]
+
+
+class MvContexts(C.Structure):
+    _fields_ = [("p", (C.c_uint8 * 19) * 2)]
+
+
+class FilterConfig(C.Structure):
+    _fields_ = [
+        ("simple", C.c_uint8),
+        ("key_frame", C.c_uint8),
+        ("loop_filter_level", C.c_uint8),
+        ("sharpness_level", C.c_uint8),
+        ("segmentation_enabled", C.c_uint8),
+        ("segment_abs", C.c_uint8),
+        ("delta_enabled", C.c_uint8),
+        ("reserved", C.c_uint8),
+        ("segment_lf_level", C.c_int16 * 4),
+        ("ref_delta_current", C.c_int16),
+        ("bpred_mode_delta", C.c_int16),
+        ("ref_delta_last", C.c_int16),
+        ("ref_delta_golden", C.c_int16),
+        ("ref_delta_altref", C.c_int16),
+        ("zero_mv_mode_delta", C.c_int16),
+        ("other_mv_mode_delta", C.c_int16),
+        ("split_mv_mode_delta", C.c_int16),
+    ]
+
+
+class Source(C.Structure):
+    _fields_ = [
+        ("width", C.c_uint32),
+        ("height", C.c_uint32),
+        ("y", C.c_void_p),
+        ("u", C.c_void_p),
+        ("v", C.c_void_p),
+        ("y_stride", C.c_uint64),
+        ("uv_stride", C.c_uint64),
+    ]
+
+
+MV_DTYPE = np.dtype([("row", "<i2"), ("col", "<i2")])
+SEARCH_RESULT_DTYPE = np.dtype([("mv", MV_DTYPE), ("sad", "<u4")])
+MB_DECISION_DTYPE = np.dtype(
+    [
+        ("ref_frame", "u1"),
+        ("mode", "u1"),
+        ("partition", "u1"),
+        ("reserved", "u1"),
+        ("mv", MV_DTYPE),
+        ("j", "<f8"),
+        ("total", "<f8"),
+        ("split_mvs", MV_DTYPE, (16,)),
+        ("submv_modes", "u1", (16,)),
+    ],
+    align=True,
+)
+REF_SEARCH_DTYPE = np.dtype(
+    [
+        ("best_predictor", MV_DTYPE),
+        ("nearest_mv", MV_DTYPE),
+        ("near_mv", MV_DTYPE),
+        ("sad_zero", "<u4"),
+        ("whole", SEARCH_RESULT_DTYPE),
+        ("half", SEARCH_RESULT_DTYPE),
+        ("quarter", SEARCH_RESULT_DTYPE),
+        ("sad_nearest", "<u4"),
+        ("sad_near", "<u4"),
+        ("chosen_mode", "u1"),
+        ("split_partition", "u1"),
+        ("reserved", "u1", (2,)),
+        ("j", "<f8"),
+    ],
+    align=True,
+)
+MB_LF_INFO_DTYPE = np.dtype(
+    [
+        ("y_mode_is_bpred", "u1"),
+        ("has_coeffs", "u1"),
+        ("ref_frame", "u1"),
+        ("inter_mode", "u1"),
+        ("segment_id", "i1"),
+        ("reserved", "u1", (3,)),
+    ]
+)
+
+# Sizes the C compiler gives these records (x86-64 and the CUDA host ABI).
+C_SIZES = {
+    "vp8a_mv": 4,
+    "vp8a_search_result": 8,
+    "vp8a_luma_ref": 24,
+    "vp8a_i420": 48,
+    "vp8a_planes": 48,
+    "vp8a_mv_contexts": 38,
+    "vp8a_mb_decision": 104,
+    "vp8a_ref_search": 64,
+    "vp8a_mb_lf_info": 8,
+    "vp8a_filter_config": 32,
+    "vp8a_source": 48,
+}
+
+
+def check_layouts():
+    """Assert that the Python mirrors match the C record sizes."""
+    got = {
+        "vp8a_mv": C.sizeof(Mv),
+        "vp8a_search_result": C.sizeof(SearchResult),
+        "vp8a_luma_ref": C.sizeof(LumaRef),
+        "vp8a_i420": C.sizeof(I420),
+        "vp8a_planes": C.sizeof(Planes),
+        "vp8a_mv_contexts": C.sizeof(MvContexts),
+        "vp8a_mb_decision": MB_DECISION_DTYPE.itemsize,
+        "vp8a_ref_search": REF_SEARCH_DTYPE.itemsize,
+        "vp8a_mb_lf_info": MB_LF_INFO_DTYPE.itemsize,
+        "vp8a_filter_config": C.sizeof(FilterConfig),
+        "vp8a_source": C.sizeof(Source),
+    }
+    assert got == C_SIZES, (got, C_SIZES)
+    return got
+
+
+def default_mv_contexts():
+    """DEFAULT_MV_CONTEXT (RFC 6386 §17.2 default MV probabilities)."""
+    ctx = MvContexts()
+    row = [162, 128, 225, 146, 172, 147, 214, 39, 156, 128, 129, 132, 75, 145, 178, 206, 239, 254, 254]
+    col = [164, 128, 204, 170, 119, 235, 140, 230, 228, 128, 130, 130, 74, 148, 180, 203, 236, 254, 254]
+    for i in range(19):
+        ctx.p[0][i] = row[i]
+        ctx.p[1][i] = col[i]
+    return ctx
+
+
+def filter_config(level=0, sharpness=0, simple=False, key_frame=False, **kw):
+    """A FrameFilterConfig (src/loop_filter.rs:891) with keyword overrides."""
+    c = FilterConfig()
+    c.loop_filter_level = level
+    c.sharpness_level = sharpness
+    c.simple = int(bool(simple))
+    c.key_frame = int(bool(key_frame))
+    for k, v in kw.items():
+        if k == "segment_lf_level":
+            for i, x in enumerate(v):
+                c.segment_lf_level[i] = x
+        else:
+            setattr(c, k, v)
+    return c

@@ -1,0 +1,231 @@
+"""Python mirror of the reference's encoder-analysis entry points.
+
+Each function keeps the name and argument meaning of the oxideav-vp8
+function it replaces (cited) and calls the matching C-ABI entry point of
+libvp8a.so, which runs CUDA kernels on the context's GPU. Inputs may be
+numpy arrays (host) or torch CUDA tensors (device); outputs are numpy unless
+an `out=` buffer is given. Errors raise Vp8aError carrying the vp8a_status,
+the counterpart of the reference's EncodeError.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from .frames import i420, luma_ref, planes, ptr, source
+from .lib import check, load
+
+
+class Context:
+    """One GPU + one CUDA stream (vp8a_ctx_create)."""
+
+    def __init__(self, device=0):
+        self._lib = load()
+        h = C.c_void_p()
+        check(self._lib.vp8a_ctx_create(device, C.byref(h)), "vp8a_ctx_create")
+        self.handle = h.value
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            self._lib.vp8a_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def stream(self):
+        return self._lib.vp8a_ctx_stream(self.handle)
+
+    @property
+    def launches(self):
+        return int(self._lib.vp8a_ctx_launch_count(self.handle))
+
+    def synchronize(self):
+        check(self._lib.vp8a_ctx_synchronize(self.handle), "vp8a_ctx_synchronize")
+
+
+def _mvs(a):
+    a = np.ascontiguousarray(a)
+    if a.dtype != abi.MV_DTYPE:
+        a = np.ascontiguousarray(a.astype(np.int16).reshape(-1, 2)).view(abi.MV_DTYPE).reshape(-1)
+    return a
+
+
+def _xy(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint32).reshape(-1, 2))
+
+
+def _src(a):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.uint8).reshape(-1, 256))
+    return a
+
+
+def mb_luma_sad_at_mv(ctx, ref_plane, src_mbs, mb_xy, mvs, width=None, height=None):
+    """mb_luma_sad_at_mv (src/motion_search.rs:470) over a batch."""
+    r = luma_ref(ref_plane, width, height)
+    src, xy, mv = _src(src_mbs), _xy(mb_xy), _mvs(mvs)
+    n = len(mv)
+    out = np.zeros(n, np.uint32)
+    check(ctx._lib.vp8a_mb_luma_sad_at_mv(ctx.handle, C.byref(r), ptr(src), ptr(xy), ptr(mv), n, ptr(out)),
+          "vp8a_mb_luma_sad_at_mv")
+    return out
+
+
+def small_diamond_search_luma(ctx, ref_plane, src_mbs, mb_xy, centers, max_iters, width=None, height=None):
+    """small_diamond_search_luma (src/motion_search.rs:381) over a batch."""
+    r = luma_ref(ref_plane, width, height)
+    src, xy, c = _src(src_mbs), _xy(mb_xy), _mvs(centers)
+    out = np.zeros(len(c), abi.SEARCH_RESULT_DTYPE)
+    check(ctx._lib.vp8a_small_diamond_search_luma(ctx.handle, C.byref(r), ptr(src), ptr(xy), ptr(c), max_iters,
+                                                  len(c), ptr(out)), "vp8a_small_diamond_search_luma")
+    return out
+
+
+def half_pixel_refine_luma(ctx, ref_plane, src_mbs, mb_xy, centers, width=None, height=None):
+    """half_pixel_refine_luma (src/motion_search.rs:564) over a batch."""
+    r = luma_ref(ref_plane, width, height)
+    src, xy, c = _src(src_mbs), _xy(mb_xy), _mvs(centers)
+    out = np.zeros(len(c), abi.SEARCH_RESULT_DTYPE)
+    check(ctx._lib.vp8a_half_pixel_refine_luma(ctx.handle, C.byref(r), ptr(src), ptr(xy), ptr(c), len(c), ptr(out)),
+          "vp8a_half_pixel_refine_luma")
+    return out
+
+
+def quarter_pixel_refine_luma(ctx, ref_plane, src_mbs, mb_xy, centers, width=None, height=None):
+    """quarter_pixel_refine_luma (src/motion_search.rs:666) over a batch."""
+    r = luma_ref(ref_plane, width, height)
+    src, xy, c = _src(src_mbs), _xy(mb_xy), _mvs(centers)
+    out = np.zeros(len(c), abi.SEARCH_RESULT_DTYPE)
+    check(ctx._lib.vp8a_quarter_pixel_refine_luma(ctx.handle, C.byref(r), ptr(src), ptr(xy), ptr(c), len(c),
+                                                  ptr(out)), "vp8a_quarter_pixel_refine_luma")
+    return out
+
+
+def motion_descent(ctx, ref_plane, src_mbs, mb_xy, centers, max_iters=8, width=None, height=None):
+    """Diamond -> half -> quarter as pick_mb_for_ref runs it
+    (src/encoder.rs:8576-8596). Returns (whole, half, quarter)."""
+    r = luma_ref(ref_plane, width, height)
+    src, xy, c = _src(src_mbs), _xy(mb_xy), _mvs(centers)
+    n = len(c)
+    w, h, q = (np.zeros(n, abi.SEARCH_RESULT_DTYPE) for _ in range(3))
+    check(ctx._lib.vp8a_motion_descent(ctx.handle, C.byref(r), ptr(src), ptr(xy), ptr(c), max_iters, n, ptr(w),
+                                       ptr(h), ptr(q)), "vp8a_motion_descent")
+    return w, h, q
+
+
+def rd_lambda(y_ac_qi):
+    """rd_lambda (src/encoder.rs:3742) for a luma AC quantiser index."""
+    return load().vp8a_rd_lambda(y_ac_qi)
+
+
+def analyse_inter_frame(ctx, frame, refs, ref_ids, lam, mv_contexts=None, trace=False):
+    """The exhaustive inter analysis (analyse_inter_frame,
+    src/encoder/inter.rs:263, intra picking off). `frame` = (y, u, v)
+    visible planes; `refs` = list of MB-padded (y, u, v). Returns the
+    decisions as a (mb_rows, mb_cols) structured array (and the per-ref
+    search trace when `trace`)."""
+    f = i420(*frame)
+    prs = [planes(*p) for p in refs]
+    parr = (abi.Planes * len(prs))(*prs)
+    ids = np.ascontiguousarray(np.asarray(ref_ids, np.uint8))
+    mbr, mbc = (f.height + 15) // 16, (f.width + 15) // 16
+    dec = np.zeros(mbr * mbc, abi.MB_DECISION_DTYPE)
+    tr = np.zeros(mbr * mbc * len(prs), abi.REF_SEARCH_DTYPE) if trace else None
+    ctxs = mv_contexts if mv_contexts is not None else abi.default_mv_contexts()
+    check(ctx._lib.vp8a_analyse_inter_frame(ctx.handle, C.byref(f), C.cast(parr, C.c_void_p), ptr(ids), len(prs),
+                                            C.byref(ctxs), lam, ptr(dec), ptr(tr)), "vp8a_analyse_inter_frame")
+    dec = dec.reshape(mbr, mbc)
+    if trace:
+        return dec, tr.reshape(mbr, mbc, len(prs))
+    return dec
+
+
+def build_arnr_altref(ctx, frames, center, strength=3):
+    """build_arnr_altref (src/arnr.rs:476). `frames` = list of (y, u, v).
+    Returns the packed (y, u, v) anchor."""
+    recs = [i420(*f) for f in frames]
+    arr = (abi.I420 * len(recs))(*recs)
+    h, w = frames[center][0].shape[0], frames[center][0].shape[1]
+    ch, cw = (h + 1) // 2, (w + 1) // 2
+    y = np.zeros((h, w), np.uint8)
+    u = np.zeros((ch, cw), np.uint8)
+    v = np.zeros((ch, cw), np.uint8)
+    check(ctx._lib.vp8a_build_arnr_altref(ctx.handle, C.cast(arr, C.c_void_p), len(recs), center, strength, ptr(y),
+                                          ptr(u), ptr(v)), "vp8a_build_arnr_altref")
+    return y, u, v
+
+
+def filter_frame(ctx, recon, mbs, config):
+    """filter_inter_frame_flags / filter_frame_flags
+    (src/loop_filter.rs:1364, :2506) on a copy of `recon` (MB-padded
+    (y, u, v)); returns the filtered planes."""
+    y, u, v = (np.array(p, np.uint8, copy=True) for p in recon)
+    p = planes(y, u, v)
+    m = np.ascontiguousarray(mbs, abi.MB_LF_INFO_DTYPE)
+    check(ctx._lib.vp8a_filter_frame(ctx.handle, C.byref(p), ptr(m), C.byref(config)), "vp8a_filter_frame")
+    return y, u, v
+
+
+def reconstruction_ssd(ctx, recon, src):
+    """reconstruction_ssd (src/loop_filter.rs:1965)."""
+    p, s = planes(*recon), source(*src)
+    out = np.zeros(1, np.uint64)
+    check(ctx._lib.vp8a_reconstruction_ssd(ctx.handle, C.byref(p), C.byref(s), ptr(out)), "vp8a_reconstruction_ssd")
+    return int(out[0])
+
+
+def filter_sweep(ctx, recon, mbs, base, src, every_rows=0):
+    """score_filter_candidate (src/loop_filter.rs:2062) for every (level,
+    sharpness); returns a (64, 8) uint64 table."""
+    p, s = planes(*recon), source(*src)
+    m = np.ascontiguousarray(mbs, abi.MB_LF_INFO_DTYPE)
+    out = np.zeros(512, np.uint64)
+    check(ctx._lib.vp8a_filter_sweep(ctx.handle, C.byref(p), ptr(m), C.byref(base), C.byref(s), every_rows,
+                                     ptr(out)), "vp8a_filter_sweep")
+    return out.reshape(64, 8)
+
+
+def select_filter_params(ctx, recon, mbs, base, src):
+    """select_filter_params (src/loop_filter.rs:2047) -> (level, sharpness)."""
+    p, s = planes(*recon), source(*src)
+    m = np.ascontiguousarray(mbs, abi.MB_LF_INFO_DTYPE)
+    lv, sh = C.c_uint8(), C.c_uint8()
+    check(ctx._lib.vp8a_select_filter_params(ctx.handle, C.byref(p), ptr(m), C.byref(base), C.byref(s),
+                                             C.byref(lv), C.byref(sh)), "vp8a_select_filter_params")
+    return lv.value, sh.value
+
+
+def select_filter_params_sampled(ctx, recon, mbs, base, src, every_rows, sweep_sharpness):
+    """select_filter_params_sampled (src/loop_filter.rs:2288)."""
+    p, s = planes(*recon), source(*src)
+    m = np.ascontiguousarray(mbs, abi.MB_LF_INFO_DTYPE)
+    lv, sh = C.c_uint8(), C.c_uint8()
+    check(ctx._lib.vp8a_select_filter_params_sampled(ctx.handle, C.byref(p), ptr(m), C.byref(base), C.byref(s),
+                                                     every_rows, int(bool(sweep_sharpness)), C.byref(lv),
+                                                     C.byref(sh)), "vp8a_select_filter_params_sampled")
+    return lv.value, sh.value
+
+
+def lf_info_from_decisions(dec, has_coeffs=None):
+    """Per-MB §15 side information from inter decisions: SPLITMV MBs are
+    recorded as B_PRED (src/loop_filter.rs:1258-1266)."""
+    d = np.asarray(dec).reshape(-1)
+    m = np.zeros(len(d), abi.MB_LF_INFO_DTYPE)
+    m["ref_frame"] = d["ref_frame"]
+    m["inter_mode"] = d["mode"]
+    m["y_mode_is_bpred"] = (d["mode"] == abi.MODE_SPLIT).astype(np.uint8)
+    m["segment_id"] = -1
+    if has_coeffs is not None:
+        m["has_coeffs"] = np.asarray(has_coeffs, np.uint8).reshape(-1)
+    return m

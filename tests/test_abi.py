@@ -1,0 +1,55 @@
+"""The C-ABI library loads and exports exactly what include/vp8a.h declares,
+and the Python record mirrors match the C layouts (no GPU needed)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+import vp8a
+from vp8a import abi
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "vp8a.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(vp8a_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_prototyped_functions():
+    assert declared_functions() == sorted(vp8a.PROTOTYPES)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = vp8a.load()
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+    assert lib.vp8a_abi_version() >> 16 == 1
+
+
+def test_record_layouts_match_c(oracle):
+    assert abi.check_layouts() == oracle.type_sizes()
+
+
+def test_no_cpu_fallback_without_gpu():
+    try:
+        import torch
+
+        has_gpu = torch.cuda.is_available()
+    except Exception:
+        has_gpu = False
+    if has_gpu:
+        pytest.skip("a GPU is visible")
+    lib = vp8a.load()
+    h = C.c_void_p()
+    assert lib.vp8a_ctx_create(0, C.byref(h)) == abi.E_NO_DEVICE
+    assert b"no CPU fallback" in lib.vp8a_last_error()
+    with pytest.raises(vp8a.Vp8aError):
+        vp8a.Context(0)
+
+
+def test_rd_lambda_host_helper(oracle):
+    for qi in (0, 44, 100, 127):
+        assert vp8a.rd_lambda(qi) == oracle.rd_lambda(qi)
