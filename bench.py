@@ -1,0 +1,526 @@
+"""Benchmark of the B200 encoder-analysis path on the 1080p P-frame workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Workload (one step = one 1920x1080 P frame, synthetic seeded I420 input):
+  1. ARNR anchor over a 7-frame lookahead window, centre anchor
+     (vp8a_build_arnr_altref);
+  2. exhaustive inter analysis of the frame against LAST (k-1), GOLDEN
+     (k-8) and ALTREF (the fresh anchor, edge-padded) with full sub-pel
+     search and SPLITMV per MB per reference (vp8a_analyse_inter_frame);
+  3. the loop-filter sweep over all 64 levels x 8 sharpness values of a
+     qi-44-style reconstruction, SSD vs source per candidate
+     (vp8a_filter_sweep), and the reference's (level, sharpness) walk.
+Metric: 1080p macroblocks per second through those three stages.
+
+`value` times the step with every input resident in HBM (device pointers);
+`e2e` times the same step through the C ABI with pinned host buffers, the
+host->device copies and the device->host reads of the results inside the
+timed region. L2 is flushed (256 MiB write) between timed steps. With N>1
+ranks each GPU analyses its own frames (replicas, no collective on the data
+path); `value` is all ranks' MBs over the slowest rank's time.
+
+`--impl reference` times the reference path's CPU restatement (the oracle,
+C, all host threads) on the same workload and metric.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "oxideav-vp8_b200"))
+
+W, H = 1920, 1080
+MB_COLS, MB_ROWS = 120, 68
+N_MB = MB_COLS * MB_ROWS
+LOOKAHEAD = 7
+QI = 44
+SEED = 20261203
+METRIC = "1080p MBs/s (ME+ARNR+LF search)"
+WORKLOAD = "1080p P frame: ARNR(7, centre) + exhaustive ME/SPLITMV vs LAST/GOLDEN/ALTREF + LF 64x8 sweep"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_inputs(seed):
+    """Frames 0..15 of the seeded sequence; the P frame is frame 8
+    (LAST = 7, GOLDEN = 0); the ARNR window is frames 9..15 (centre 12)."""
+    from vp8a import synth
+
+    frames, _ = synth.make_sequence(W, H, 16, seed)
+    return frames, synth.digest(frames)
+
+
+def pad_planes(f):
+    import vp8a
+
+    return vp8a.pad_to_mb(*f)
+
+
+class Clocks:
+    """nvidia-smi sampler (clocks and throttle reasons) over the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            p = [x.strip() for x in l.split(",")]
+            if len(p) < 7:
+                continue
+            try:
+                sm.append(float(p[0]))
+                mx.append(float(p[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# --------------------------------------------------------------- GPU arm
+
+
+class GpuStep:
+    """Device-resident buffers and the C-ABI calls of one step."""
+
+    def __init__(self, ctx, frames, lib, torch, device):
+        import vp8a
+        from vp8a import abi, synth
+
+        self.vp8a, self.abi, self.lib, self.torch, self.ctx = vp8a, abi, lib, torch, ctx
+        dev = torch.device("cuda", device)
+        # Torch work of the step runs on the library's stream, in order.
+        self.stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+        cur = frames[8]
+        self.cur = [t(p) for p in cur]
+        self.last = [t(p) for p in pad_planes(frames[7])]
+        self.golden = [t(p) for p in pad_planes(frames[0])]
+        self.window = [[t(p) for p in frames[9 + i]] for i in range(LOOKAHEAD)]
+        self.alt = [torch.zeros((MB_ROWS * 16, MB_COLS * 16), dtype=torch.uint8, device=dev),
+                    torch.zeros((MB_ROWS * 8, MB_COLS * 8), dtype=torch.uint8, device=dev),
+                    torch.zeros((MB_ROWS * 8, MB_COLS * 8), dtype=torch.uint8, device=dev)]
+        recon, has = synth.quantised_recon(pad_planes(cur))
+        self.recon = [t(p) for p in recon]
+        self.has = has
+        self.dec = torch.zeros(N_MB * abi.MB_DECISION_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+        self.table = torch.zeros(512, dtype=torch.int64, device=dev)
+        self.lam = vp8a.rd_lambda(QI)
+        self.ids = torch.tensor([1, 2, 3], dtype=torch.uint8, device=dev)
+        self.ctxs = abi.default_mv_contexts()
+        self.base = abi.filter_config(0, 0)
+        # Per-MB loop-filter side information from the frame's decisions.
+        self.run_arnr()
+        self.run_analysis()
+        ctx.synchronize()
+        torch.cuda.synchronize(dev)
+        dec = np.frombuffer(self.dec.cpu().numpy().tobytes(), abi.MB_DECISION_DTYPE)
+        self.decisions = dec
+        self.mbs = t(vp8a.lf_info_from_decisions(dec, has).view(np.uint8))
+        self.i420_window = (abi.I420 * LOOKAHEAD)(*[vp8a.i420(*f) for f in self.window])
+        self.i420_cur = vp8a.i420(*self.cur)
+        self.planes = (abi.Planes * 3)(vp8a.planes(*self.last), vp8a.planes(*self.golden), vp8a.planes(*self.alt))
+        self.recon_planes = vp8a.planes(*self.recon)
+        self.src = vp8a.source(*self.cur)
+
+    def run_arnr(self):
+        v = self.vp8a
+        win = (self.abi.I420 * LOOKAHEAD)(*[v.i420(*f) for f in self.window])
+        st = self.lib.vp8a_build_arnr_altref(self.ctx.handle, C.cast(win, C.c_void_p), LOOKAHEAD, 3, 3,
+                                             self.alt[0].data_ptr(), self.alt[1].data_ptr(), self.alt[2].data_ptr())
+        assert st == 0, v.load().vp8a_last_error()
+        # Edge-replicate the anchor into the MB-padded ALTREF planes.
+        with self.torch.cuda.stream(self.stream):
+            self.alt[0][H:] = self.alt[0][H - 1]
+            ch = (H + 1) // 2
+            self.alt[1][ch:] = self.alt[1][ch - 1]
+            self.alt[2][ch:] = self.alt[2][ch - 1]
+
+    def run_analysis(self):
+        v = self.vp8a
+        f = v.i420(*self.cur)
+        pl = (self.abi.Planes * 3)(v.planes(*self.last), v.planes(*self.golden), v.planes(*self.alt))
+        st = self.lib.vp8a_analyse_inter_frame(self.ctx.handle, C.byref(f), C.cast(pl, C.c_void_p),
+                                               self.ids.data_ptr(), 3, C.byref(self.ctxs), self.lam,
+                                               self.dec.data_ptr(), None)
+        assert st == 0, v.load().vp8a_last_error()
+
+    def run_lf(self):
+        st = self.lib.vp8a_filter_sweep(self.ctx.handle, C.byref(self.recon_planes), self.mbs.data_ptr(),
+                                        C.byref(self.base), C.byref(self.src), 0, self.table.data_ptr())
+        assert st == 0, self.vp8a.load().vp8a_last_error()
+        # The reference's coarse-grid / refine / sharpness walk over the table.
+        self.ctx.synchronize()
+        t = self.table.cpu().numpy().view(np.uint64)
+        return select_full(t, 0)
+
+    def step(self):
+        self.run_arnr()
+        self.run_analysis()
+        return self.run_lf()
+
+
+def select_full(t, bs):
+    """select_filter_params_threaded's walk (src/loop_filter.rs:2133-2199)
+    over a 64 x 8 candidate table."""
+    best_level, best = 0, int(t[bs])
+    for lv in list(range(4, 61, 4)) + [63]:
+        if int(t[lv * 8 + bs]) < best:
+            best, best_level = int(t[lv * 8 + bs]), lv
+    g = best_level
+    for lv in range(max(0, g - 3), min(63, g + 3) + 1):
+        if lv != g and int(t[lv * 8 + bs]) < best:
+            best, best_level = int(t[lv * 8 + bs]), lv
+    if best_level == 0:
+        return 0, bs
+    best_sharp = bs
+    for sh in range(8):
+        if sh != bs and int(t[best_level * 8 + sh]) < best:
+            best, best_sharp = int(t[best_level * 8 + sh]), sh
+    return best_level, best_sharp
+
+
+class HostStep:
+    """The same step through the C ABI with pinned host buffers (e2e)."""
+
+    def __init__(self, gs, torch):
+        self.gs, self.torch = gs, torch
+        pin = lambda x: x.cpu().pin_memory()  # noqa: E731
+        self.cur = [pin(p) for p in gs.cur]
+        self.last = [pin(p) for p in gs.last]
+        self.golden = [pin(p) for p in gs.golden]
+        self.window = [[pin(p) for p in f] for f in gs.window]
+        self.alt = [pin(p) for p in gs.alt]
+        self.recon = [pin(p) for p in gs.recon]
+        self.mbs = pin(gs.mbs)
+        self.dec = torch.zeros(N_MB * gs.abi.MB_DECISION_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+        self.table = torch.zeros(512, dtype=torch.int64).pin_memory()
+        self.ids = np.array([1, 2, 3], np.uint8)
+        nb = lambda ts: sum(x.numel() * x.element_size() for x in ts)  # noqa: E731
+        # Bytes the library copies in per step (what each call stages).
+        self.h2d = (sum(nb(f) for f in self.window) + self.cur[0].numel() + self.last[0].numel() +
+                    self.golden[0].numel() + self.alt[0].numel() + nb(self.recon) + nb([self.mbs]) + nb(self.cur))
+        self.d2h = nb(self.alt) - (self.alt[0][H:].numel() + 2 * self.alt[1][(H + 1) // 2:].numel()) + \
+            nb([self.dec]) + nb([self.table])
+
+    def step(self):
+        gs, v, abi, lib = self.gs, self.gs.vp8a, self.gs.abi, self.gs.lib
+        win = (abi.I420 * LOOKAHEAD)(*[v.i420(*f) for f in self.window])
+        st = lib.vp8a_build_arnr_altref(gs.ctx.handle, C.cast(win, C.c_void_p), LOOKAHEAD, 3, 3,
+                                        self.alt[0].data_ptr(), self.alt[1].data_ptr(), self.alt[2].data_ptr())
+        assert st == 0
+        self.alt[0][H:] = self.alt[0][H - 1]
+        ch = (H + 1) // 2
+        self.alt[1][ch:] = self.alt[1][ch - 1]
+        self.alt[2][ch:] = self.alt[2][ch - 1]
+        f = v.i420(*self.cur)
+        pl = (abi.Planes * 3)(v.planes(*self.last), v.planes(*self.golden), v.planes(*self.alt))
+        st = lib.vp8a_analyse_inter_frame(gs.ctx.handle, C.byref(f), C.cast(pl, C.c_void_p),
+                                          self.ids.ctypes.data, 3, C.byref(gs.ctxs), gs.lam, self.dec.data_ptr(),
+                                          None)
+        assert st == 0
+        rp, src = v.planes(*self.recon), v.source(*self.cur)
+        st = lib.vp8a_filter_sweep(gs.ctx.handle, C.byref(rp), self.mbs.data_ptr(), C.byref(gs.base), C.byref(src),
+                                   0, self.table.data_ptr())
+        assert st == 0
+        return select_full(self.table.numpy().view(np.uint64), 0)
+
+
+def gpu_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    import vp8a
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = vp8a.load()
+    ctx = vp8a.Context(local)
+    # Each rank analyses its own frames (replicas): seed by rank.
+    frames, digest = make_inputs(SEED + rank)
+    gs = GpuStep(ctx, frames, lib, torch, local)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # Warm-up.
+    for _ in range(args.warmup):
+        gs.step()
+    torch.cuda.synchronize(dev)
+    # Timed region (device-resident inputs).
+    times = []
+    launches0 = ctx.launches
+    barrier()
+    torch.cuda.synchronize(dev)
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            choice = gs.step()
+            e.record(stream)
+            e.synchronize()
+            times.append(s.elapsed_time(e))
+        torch.cuda.synchronize(dev)
+    barrier()
+    launches = ctx.launches - launches0
+    ms = float(np.sum(times))
+    # Per-kernel-stage timing for the roofline (separate, after the timed run).
+    stage = stage_times(gs, stream, torch, flush)
+    # End-to-end through host buffers.
+    hs = HostStep(gs, torch)
+    for _ in range(max(1, args.warmup)):
+        hs.step()
+    e_times = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        torch.cuda.synchronize(dev)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        hs.step()
+        e.record(stream)
+        e.synchronize()
+        e_times.append(s.elapsed_time(e))
+    e_ms = float(np.sum(e_times))
+    if world > 1:
+        t = torch.tensor([ms, e_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e_ms = float(t[0]), float(t[1])
+    result = None
+    if rank == 0:
+        value = N_MB * args.steps * world / (ms / 1000.0)
+        e2e = N_MB * args.steps * world / (e_ms / 1000.0)
+        peak, peak_kind = peaks()
+        dom = max(stage, key=lambda k: stage[k]["ms"])
+        d = stage[dom]
+        achieved = d["bytes"] / (d["ms"] / 1000.0) / 1e9
+        result = {
+            "metric": METRIC,
+            "value": round(value, 1),
+            "unit": "MB/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(ms / args.steps, 4),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "u8",
+            "data": "synthetic (seeded gratings + quarter-pel six-tap translation + noise)",
+            "config": {
+                "workload": WORKLOAD,
+                "width": W,
+                "height": H,
+                "refs": 3,
+                "lookahead": LOOKAHEAD,
+                "lf_candidates": 512,
+                "qi": QI,
+                "seed": SEED,
+                "input_sha256": digest[:16],
+                "l2": "flushed between timed steps (256 MiB write)",
+                "parallelism": f"replicas x{world}",
+                "lf_choice": list(choice),
+            },
+            "e2e": {"value": round(e2e, 1), "unit": "MB/s", "h2d_bytes_per_step": int(hs.h2d),
+                    "d2h_bytes_per_step": int(hs.d2h)},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 5), "traffic": None,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                         else "fallback 6.65 TB/s",
+                         "stage_ms": {k: round(v["ms"], 4) for k, v in stage.items()},
+                         "stage_alg_bytes": {k: int(v["bytes"]) for k, v in stage.items()}},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+        if args.gpus == 1 and world == 1 and not args.no_cpu_baseline:
+            result["cpu_baseline"] = cpu_baseline(frames, budget_s=args.cpu_budget)
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+def stage_times(gs, stream, torch, flush, reps=3):
+    """Mean device time per stage (CUDA events on the context stream) and
+    each stage's algorithmic bytes (inputs read once + outputs written)."""
+    out = {}
+    luma = W * H
+    pic = luma + 2 * ((W + 1) // 2) * ((H + 1) // 2)
+    padded = MB_COLS * 16 * MB_ROWS * 16
+    padded_pic = padded + 2 * MB_COLS * 8 * MB_ROWS * 8
+    fns = {
+        "arnr": (gs.run_arnr, LOOKAHEAD * pic + pic),
+        "analysis": (gs.run_analysis, luma + 3 * padded + N_MB * gs.abi.MB_DECISION_DTYPE.itemsize),
+        "lf_sweep": (lambda: gs.run_lf(), padded_pic + pic + N_MB * 8 + 512 * 8),
+    }
+    for name, (fn, nbytes) in fns.items():
+        ts = []
+        for _ in range(reps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            torch.cuda.synchronize()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            fn()
+            e.record(stream)
+            e.synchronize()
+            ts.append(s.elapsed_time(e))
+        out[name] = {"ms": float(np.mean(ts)), "bytes": nbytes}
+    return out
+
+
+# ----------------------------------------------------------- CPU baseline
+
+
+def cpu_step(oracle, frames, threads, pieces=("arnr", "analysis", "lf")):
+    import vp8a
+    from vp8a import synth
+
+    anchor = oracle.build_arnr_altref([frames[9 + i] for i in range(LOOKAHEAD)], 3, 3, threads=threads)
+    refs = [pad_planes(frames[7]), pad_planes(frames[0]), pad_planes(anchor)]
+    lam = oracle.rd_lambda(QI)
+    dec = oracle.analyse_inter_frame(frames[8], refs, [1, 2, 3], lam, threads=threads)
+    recon, has = synth.quantised_recon(pad_planes(frames[8]))
+    mbs = vp8a.lf_info_from_decisions(dec, has)
+    table = oracle.filter_sweep(recon, mbs, vp8a.abi.filter_config(0, 0), frames[8], 0, threads=threads)
+    return select_full(table.reshape(-1), 0)
+
+
+def cpu_baseline(frames, budget_s=30.0):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    oracle.build()
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        cpu_step(oracle, frames, threads)
+        n += 1
+        if time.perf_counter() - t0 > min(budget_s, 30.0) or n >= 3:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": round(N_MB * n / dt, 1), "unit": "MB/s", "cores": threads, "kind": "port",
+            "sample": f"{n} full 1080p step(s) (ARNR + 3-ref analysis + 505-candidate LF sweep) "
+                      f"by the C oracle on {threads} threads in {dt:.2f} s"}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    oracle.build()
+    frames, digest = make_inputs(SEED)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_step(oracle, frames, threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cpu_step(oracle, frames, threads)
+    dt = time.perf_counter() - t0
+    value = N_MB * args.steps / dt
+    return {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": round(value, 1),
+        "unit": "MB/s",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(dt * 1000.0 / args.steps, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u8",
+        "data": "synthetic (seeded gratings + quarter-pel six-tap translation + noise)",
+        "config": {"workload": WORKLOAD, "width": W, "height": H, "refs": 3, "lookahead": LOOKAHEAD,
+                   "lf_candidates": 512, "qi": QI, "seed": SEED, "input_sha256": digest[:16]},
+        "cpu_baseline": {"value": round(value, 1), "unit": "MB/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full 1080p steps after {args.warmup} warm-up, C oracle "
+                                   f"(restatement of the Rust reference, which has no toolchain here) "
+                                   f"on {threads} threads"},
+        "e2e": {"value": round(value, 1), "unit": "MB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="vp8a", choices=["vp8a", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl != "reference":
+        log("note: fewer than 3 warm-up steps")
+    res = reference_arm(args) if args.impl == "reference" else gpu_arm(args)
+    if res is not None:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

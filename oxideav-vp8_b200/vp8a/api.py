@@ -156,7 +156,10 @@ def build_arnr_altref(ctx, frames, center, strength=3):
     Returns the packed (y, u, v) anchor."""
     recs = [i420(*f) for f in frames]
     arr = (abi.I420 * len(recs))(*recs)
-    h, w = frames[center][0].shape[0], frames[center][0].shape[1]
+    # Output size follows the centre frame; an out-of-range centre is
+    # rejected by the library (VP8A_E_INVALID_ARGUMENT).
+    shape_src = frames[center] if 0 <= center < len(frames) else frames[0]
+    h, w = shape_src[0].shape[0], shape_src[0].shape[1]
     ch, cw = (h + 1) // 2, (w + 1) // 2
     y = np.zeros((h, w), np.uint8)
     u = np.zeros((ch, cw), np.uint8)
