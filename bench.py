@@ -157,6 +157,7 @@ class GpuStep:
         self.ids = torch.tensor([1, 2, 3], dtype=torch.uint8, device=dev)
         self.ctxs = abi.default_mv_contexts()
         self.base = abi.filter_config(0, 0)
+        torch.cuda.synchronize(dev)  # uploads (torch stream) before library calls
         # Per-MB loop-filter side information from the frame's decisions.
         self.run_arnr()
         self.run_analysis()
@@ -165,6 +166,7 @@ class GpuStep:
         dec = np.frombuffer(self.dec.cpu().numpy().tobytes(), abi.MB_DECISION_DTYPE)
         self.decisions = dec
         self.mbs = t(vp8a.lf_info_from_decisions(dec, has).view(np.uint8))
+        torch.cuda.synchronize(dev)
         self.i420_window = (abi.I420 * LOOKAHEAD)(*[vp8a.i420(*f) for f in self.window])
         self.i420_cur = vp8a.i420(*self.cur)
         self.planes = (abi.Planes * 3)(vp8a.planes(*self.last), vp8a.planes(*self.golden), vp8a.planes(*self.alt))
