@@ -572,6 +572,13 @@ extern "C" vp8a_status vp8a_analyse_inter_frame(vp8a_ctx* ctx, const vp8a_i420* 
     return VP8A_E_INVALID_ARGUMENT;
   }
   const int mb_cols = (int)((frame->width + 15) / 16), mb_rows = (int)((frame->height + 15) / 16);
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  vp8a_status s;
+  // The reference ids steer host-side validation; fetch them wherever they live.
+  uint8_t ids[MAX_REFS];
+  if ((s = st.read_to_host(ref_ids, n_refs, ids)) != VP8A_OK) return s;
+  ref_ids = ids;
   for (uint32_t k = 0; k < n_refs; k++) {
     if ((int)refs[k].mb_cols != mb_cols || (int)refs[k].mb_rows != mb_rows) {
       vp8a::set_error("reference planes do not match the frame's MB grid");
@@ -587,9 +594,6 @@ extern "C" vp8a_status vp8a_analyse_inter_frame(vp8a_ctx* ctx, const vp8a_i420* 
     vp8a::set_error("bad source plane");
     return VP8A_E_INVALID_ARGUMENT;
   }
-  VP8A_CUDA(cudaSetDevice(ctx->device));
-  vp8a::Stager st(ctx);
-  vp8a_status s;
   AnArgs a{};
   const void* d;
   if ((s = st.in(frame->y, frame->y_stride * (size_t)(frame->height - 1) + frame->width, &d)) != VP8A_OK) return s;

@@ -56,6 +56,40 @@ vp8a_status Stager::scratch(size_t bytes, void** dev) {
   return VP8A_OK;
 }
 
+vp8a_status Stager::read_to_host(const void* p, size_t bytes, void* host_dst) {
+  if (!p) {
+    set_error("null input buffer");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  bool is_dev = false;
+  vp8a_status st = classify(p, &is_dev);
+  if (st != VP8A_OK) return st;
+  if (!is_dev) {
+    memcpy(host_dst, p, bytes);
+    return VP8A_OK;
+  }
+  VP8A_CUDA(cudaMemcpyAsync(host_dst, p, bytes, cudaMemcpyDeviceToHost, ctx_->stream));
+  VP8A_CUDA(cudaStreamSynchronize(ctx_->stream));
+  return VP8A_OK;
+}
+
+vp8a_status Stager::write_from_host(void* dst, const void* host_src, size_t bytes) {
+  if (!dst) {
+    set_error("null output buffer");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  bool is_dev = false;
+  vp8a_status st = classify(dst, &is_dev);
+  if (st != VP8A_OK) return st;
+  if (!is_dev) {
+    memcpy(dst, host_src, bytes);
+    return VP8A_OK;
+  }
+  VP8A_CUDA(cudaMemcpyAsync(dst, host_src, bytes, cudaMemcpyHostToDevice, ctx_->stream));
+  VP8A_CUDA(cudaStreamSynchronize(ctx_->stream));
+  return VP8A_OK;
+}
+
 vp8a_status Stager::in(const void* p, size_t bytes, const void** dev) {
   if (!p) {
     set_error("null input buffer");

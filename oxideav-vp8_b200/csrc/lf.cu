@@ -757,8 +757,9 @@ vp8a_status vp8a_select_filter_params(vp8a_ctx* ctx, const vp8a_planes* planes, 
       best_level = c[i];
     }
   if (best_level == 0) {
-    *level_out = 0;
-    *sharpness_out = bs;
+    const uint8_t zero = 0;
+    if ((s = st.write_from_host(level_out, &zero, 1)) != VP8A_OK) return s;
+    if ((s = st.write_from_host(sharpness_out, &bs, 1)) != VP8A_OK) return s;
     return st.finish();
   }
   // Stage 2: the other sharpness values at the chosen level.
@@ -775,8 +776,8 @@ vp8a_status vp8a_select_filter_params(vp8a_ctx* ctx, const vp8a_planes* planes, 
       best = t[best_level * 8 + c[i + 1]];
       best_sharp = c[i + 1];
     }
-  *level_out = best_level;
-  *sharpness_out = best_sharp;
+  if ((s = st.write_from_host(level_out, &best_level, 1)) != VP8A_OK) return s;
+  if ((s = st.write_from_host(sharpness_out, &best_sharp, 1)) != VP8A_OK) return s;
   return st.finish();
 }
 
@@ -846,8 +847,8 @@ vp8a_status vp8a_select_filter_params_sampled(vp8a_ctx* ctx, const vp8a_planes* 
         best_sharp = c[i + 1];
       }
   }
-  *level_out = best_level;
-  *sharpness_out = best_sharp;
+  if ((s = st.write_from_host(level_out, &best_level, 1)) != VP8A_OK) return s;
+  if ((s = st.write_from_host(sharpness_out, &best_sharp, 1)) != VP8A_OK) return s;
   return st.finish();
 }
 

@@ -52,6 +52,12 @@ class Stager {
   vp8a_status inout(void* p, size_t bytes, void** dev);
   // Scratch device memory owned by this call.
   vp8a_status scratch(size_t bytes, void** dev);
+  // Host copy of a small buffer that may be host or device memory (for
+  // metadata the host logic itself reads, e.g. reference ids).
+  vp8a_status read_to_host(const void* p, size_t bytes, void* host_dst);
+  // Store a small host value into an output that may be host or device
+  // memory.
+  vp8a_status write_from_host(void* dst, const void* host_src, size_t bytes);
   // Copies host outputs back and synchronises when any host buffer was
   // involved (otherwise the call stays asynchronous on the stream).
   vp8a_status finish();

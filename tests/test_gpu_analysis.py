@@ -79,3 +79,44 @@ def test_analysis_errors(ctx):
         vp8a.analyse_inter_frame(ctx, frames[1], [bad], [1], 72.0)
     with pytest.raises(vp8a.Vp8aError, match="InvalidArgument"):
         vp8a.analyse_inter_frame(ctx, frames[1], [vp8a.pad_to_mb(*frames[0])], [7], 72.0)
+
+
+def test_analysis_and_lf_device_resident(ctx, oracle):
+    # Every buffer (planes, ids, outputs) in device memory: the calls are
+    # stream-ordered and must match the host-buffer results.
+    import ctypes as C
+
+    torch = pytest.importorskip("torch")
+    frames, _ = synth.make_sequence(96, 64, 4, seed=77, pieces=2, occluders=1)
+    refs = refs_for(frames, 2)
+    host = vp8a.analyse_inter_frame(ctx, frames[2], refs, [1, 2, 3], 72.0)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    cur = [d(p) for p in frames[2]]
+    drefs = [[d(p) for p in r] for r in refs]
+    ids = d(np.array([1, 2, 3], np.uint8))
+    out = torch.zeros(host.size * abi.MB_DECISION_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    lib = vp8a.load()
+    f = vp8a.i420(*cur)
+    pl = (abi.Planes * 3)(*[vp8a.planes(*r) for r in drefs])
+    ctxs = abi.default_mv_contexts()
+    st = lib.vp8a_analyse_inter_frame(ctx.handle, C.byref(f), C.cast(pl, C.c_void_p), ids.data_ptr(), 3,
+                                      C.byref(ctxs), 72.0, out.data_ptr(), None)
+    assert st == 0, lib.vp8a_last_error()
+    ctx.synchronize()
+    got = np.frombuffer(out.cpu().numpy().tobytes(), abi.MB_DECISION_DTYPE).reshape(host.shape)
+    assert_same(got, host)
+    recon, has = synth.quantised_recon(vp8a.pad_to_mb(*frames[2]))
+    mbs = vp8a.lf_info_from_decisions(host, has)
+    base = abi.filter_config(0, 0)
+    want = vp8a.select_filter_params(ctx, recon, mbs, base, frames[2])
+    drec = [d(p) for p in recon]
+    dm = d(mbs.view(np.uint8))
+    lv = torch.zeros(1, dtype=torch.uint8, device="cuda")
+    sh = torch.zeros(1, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    st = lib.vp8a_select_filter_params(ctx.handle, C.byref(vp8a.planes(*drec)), dm.data_ptr(), C.byref(base),
+                                       C.byref(vp8a.source(*cur)), lv.data_ptr(), sh.data_ptr())
+    assert st == 0, lib.vp8a_last_error()
+    ctx.synchronize()
+    assert (int(lv.item()), int(sh.item())) == want
