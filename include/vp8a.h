@@ -160,6 +160,36 @@ typedef struct vp8a_ref_search {
   double j;
 } vp8a_ref_search;
 
+/* MbInfo (src/near_mv.rs:127): the §16.3 census record one MB leaves for
+ * its neighbours. Border / intra MBs have ref_frame = VP8A_REF_INTRA. */
+typedef struct vp8a_mb_info {
+  uint8_t ref_frame;
+  uint8_t is_split;
+  uint8_t has_split_mvs;
+  uint8_t reserved;
+  vp8a_mv mv;
+  vp8a_mv split_mvs[16];
+} vp8a_mb_info;
+
+/* EncodeEffort (src/encoder/effort.rs), the RD inter search shapes
+ * (SearchShape, src/encoder/inter_search.rs:62-162). */
+enum { VP8A_EFFORT_FASTEST = 0, VP8A_EFFORT_FAST = 1, VP8A_EFFORT_BALANCED = 2, VP8A_EFFORT_THOROUGH = 3 };
+
+/* The inter candidate decide_mb_rd's search selects for one MB
+ * (src/encoder/inter_search.rs:881-1060), before its transform-model,
+ * SPLITMV and intra comparisons. */
+typedef struct vp8a_rd_inter {
+  uint8_t ref_frame;   /* VP8A_REF_* of the winner */
+  uint8_t mode;        /* VP8A_MODE_ZERO / NEAREST / NEAR / NEW */
+  uint8_t n_searched;  /* references whole-pel searched before the early stop */
+  uint8_t leader;      /* index (into refs) of the cheapest whole-pel result */
+  vp8a_mv mv;
+  uint32_t sad;
+  double cost;         /* sad + sqrt(lambda) * bits */
+  double bits;         /* ref_frame_tree_bits + mode bits (+ MV differential) */
+  vp8a_search_result found[3]; /* whole-pel result per reference, in refs order */
+} vp8a_rd_inter;
+
 /* Per-MB side information the §15 pass consults (MacroblockModes +
  * has_coeffs + InterFilterInfo, src/loop_filter.rs:1364-1489). */
 typedef struct vp8a_mb_lf_info {
@@ -280,6 +310,20 @@ vp8a_status vp8a_analyse_inter_frame(vp8a_ctx* ctx, const vp8a_i420* frame,
                                      uint32_t n_refs, const vp8a_mv_contexts* mv_contexts,
                                      double lambda, vp8a_mb_decision* decisions,
                                      vp8a_ref_search* trace);
+
+/* The RD-effort inter search of decide_mb_rd for every MB of a frame
+ * (whole_pixel_search, sub_pixel_refine and the free ZERO/NEAREST/NEAR
+ * candidates, src/encoder/inter_search.rs:198-552, :846-1060), given each
+ * MB's census neighbours: `neighbours[3*i + k]` is the above (k=0), left
+ * (k=1) and above-left (k=2) record of MB i (raster order). `y1_ac` is the
+ * luma AC dequantisation factor (good_enough threshold), `effort` one of
+ * VP8A_EFFORT_*. Every MB is independent given its neighbours, so all MBs
+ * run in parallel. */
+vp8a_status vp8a_rd_inter_search(vp8a_ctx* ctx, const vp8a_i420* frame, const vp8a_planes* refs,
+                                 const uint8_t* ref_ids, uint32_t n_refs,
+                                 const vp8a_mv_contexts* mv_contexts, double lambda,
+                                 uint32_t y1_ac, uint32_t effort,
+                                 const vp8a_mb_info* neighbours, vp8a_rd_inter* out);
 
 /* rd_lambda (src/encoder.rs:3742) for a luma AC quantiser index 0..=127. */
 double vp8a_rd_lambda(uint32_t y_ac_qi);

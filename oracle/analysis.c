@@ -197,6 +197,15 @@ static vp8a_mv clamp_mv_rect(vp8a_mv mv, int mb_col, int mb_row, int mb_cols, in
   return o;
 }
 
+/* mv_ref_probs (src/near_mv.rs:404). */
+void vo_mv_ref_probs(const int32_t cnt[4], uint8_t out[4]) {
+  for (int i = 0; i < 4; i++) out[i] = MV_COUNTS_TO_PROBS[cnt[i]][i];
+}
+
+vp8a_mv vo_clamp_mv_rect(vp8a_mv mv, int mb_col, int mb_row, int mb_cols, int mb_rows) {
+  return clamp_mv_rect(mv, mb_col, mb_row, mb_cols, mb_rows);
+}
+
 /* ------------------------------------------------------------------ SPLITMV */
 
 /* MV_PARTITIONS (src/near_mv.rs, RFC 6386 §20.13 mbsplits). */

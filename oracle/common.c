@@ -66,6 +66,8 @@ size_t vo_type_size(int which) {
     case 8: return sizeof(vp8a_mb_lf_info);
     case 9: return sizeof(vp8a_filter_config);
     case 10: return sizeof(vp8a_source);
+    case 11: return sizeof(vp8a_mb_info);
+    case 12: return sizeof(vp8a_rd_inter);
     default: return 0;
   }
 }

@@ -79,6 +79,8 @@ def load():
         "vo_select_from_table_full": (None, [P, C.c_uint8, P, P]),
         "vo_select_from_table_sampled": (None, [P, C.c_uint8, C.c_int, P, P]),
         "vo_type_size": (C.c_size_t, [C.c_int]),
+        "vo_rd_inter_search": (C.c_int, [C.POINTER(abi.I420), P, P, U32, C.POINTER(abi.MvContexts), C.c_double,
+                                         U32, U32, P, P, U32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -106,7 +108,8 @@ def _src(a):
 def type_sizes():
     lib = load()
     names = ["vp8a_mv", "vp8a_search_result", "vp8a_luma_ref", "vp8a_i420", "vp8a_planes", "vp8a_mv_contexts",
-             "vp8a_mb_decision", "vp8a_ref_search", "vp8a_mb_lf_info", "vp8a_filter_config", "vp8a_source"]
+             "vp8a_mb_decision", "vp8a_ref_search", "vp8a_mb_lf_info", "vp8a_filter_config", "vp8a_source",
+             "vp8a_mb_info", "vp8a_rd_inter"]
     return {n: int(lib.vo_type_size(i)) for i, n in enumerate(names)}
 
 
@@ -330,3 +333,39 @@ def find_near_mvs(above, left, aboveleft, current_ref=1):
     cnt = np.zeros(4, np.int32)
     fn(C.byref(above), C.byref(left), C.byref(aboveleft), current_ref, ptr(mvs), ptr(cnt))
     return [(int(m["row"]), int(m["col"])) for m in mvs], [int(c) for c in cnt]
+
+
+def neighbours_from_decisions(dec):
+    """The (above, left, above-left) census records of every MB, built from
+    a frame's decisions the way analyse_row forwards them
+    (src/encoder/inter.rs:458-480); border slots are intra records."""
+    d = np.asarray(dec)
+    mbr, mbc = d.shape
+    info = np.zeros((mbr + 1, mbc + 1), abi.MB_INFO_DTYPE)  # row/col 0 = border
+    inner = info[1:, 1:]
+    inner["ref_frame"] = d["ref_frame"]
+    inner["mv"] = d["mv"]
+    split = d["mode"] == abi.MODE_SPLIT
+    inner["is_split"] = split
+    inner["has_split_mvs"] = split
+    inner["split_mvs"] = np.where(split[..., None], d["split_mvs"], np.zeros_like(d["split_mvs"]))
+    nb = np.zeros((mbr, mbc, 3), abi.MB_INFO_DTYPE)
+    nb[:, :, 0] = info[:-1, 1:]   # above
+    nb[:, :, 1] = info[1:, :-1]   # left
+    nb[:, :, 2] = info[:-1, :-1]  # above-left
+    return np.ascontiguousarray(nb.reshape(-1))
+
+
+def rd_inter_search(frame, refs, ref_ids, lam, y1_ac, effort, neighbours, mv_contexts=None, threads=1):
+    f = i420(*frame)
+    prs = [planes(*p) for p in refs]
+    parr = (abi.Planes * len(prs))(*prs)
+    ids = np.ascontiguousarray(np.asarray(ref_ids, np.uint8))
+    nb = np.ascontiguousarray(neighbours, abi.MB_INFO_DTYPE)
+    mbr, mbc = (f.height + 15) // 16, (f.width + 15) // 16
+    out = np.zeros(mbr * mbc, abi.RD_INTER_DTYPE)
+    ctxs = mv_contexts if mv_contexts is not None else abi.default_mv_contexts()
+    st = load().vo_rd_inter_search(C.byref(f), C.cast(parr, C.c_void_p), ptr(ids), len(prs), C.byref(ctxs), lam,
+                                   y1_ac, effort, ptr(nb), ptr(out), threads)
+    _check(st, "vo_rd_inter_search")
+    return out.reshape(mbr, mbc)

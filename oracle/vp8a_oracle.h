@@ -29,14 +29,7 @@ extern "C" {
 #endif
 
 /* §16.3 per-MB census record (MbInfo, src/near_mv.rs:127). */
-typedef struct vo_mb_info {
-  uint8_t ref_frame; /* VP8A_REF_INTRA (= None) or LAST/GOLDEN/ALTREF */
-  uint8_t is_split;
-  uint8_t has_split_mvs;
-  uint8_t reserved;
-  vp8a_mv mv;
-  vp8a_mv split_mvs[16];
-} vo_mb_info;
+typedef vp8a_mb_info vo_mb_info;
 
 /* ---- motion search primitives (src/motion_search.rs, src/motion_comp.rs) */
 uint32_t vo_block_sad_16x16(const uint8_t* src, const uint8_t* pred);
@@ -83,6 +76,8 @@ void vo_find_near_mvs(const vo_mb_info* above, const vo_mb_info* left,
                       const vo_mb_info* aboveleft, uint8_t current_ref, vp8a_mv mvs_out[3],
                       int32_t cnt_out[4]);
 void vo_default_mv_contexts(vp8a_mv_contexts* out);
+void vo_mv_ref_probs(const int32_t cnt[4], uint8_t out[4]);
+vp8a_mv vo_clamp_mv_rect(vp8a_mv mv, int mb_col, int mb_row, int mb_cols, int mb_rows);
 double vo_rd_lambda(uint32_t y_ac_qi);
 
 /* ---- exhaustive analysis (src/encoder/inter.rs, src/encoder.rs) */
@@ -93,6 +88,14 @@ int vo_analyse_inter_frame(const vp8a_i420* frame, const vp8a_planes* refs,
                            const vp8a_mv_contexts* mv_contexts, double lambda,
                            vp8a_mb_decision* decisions, vp8a_ref_search* trace,
                            uint32_t threads);
+
+/* The RD-effort inter search (decide_mb_rd's search part,
+ * src/encoder/inter_search.rs:198-552, :846-1060) for every MB given its
+ * census neighbours (3 records per MB: above, left, above-left). */
+int vo_rd_inter_search(const vp8a_i420* frame, const vp8a_planes* refs, const uint8_t* ref_ids,
+                       uint32_t n_refs, const vp8a_mv_contexts* mv_contexts, double lambda,
+                       uint32_t y1_ac, uint32_t effort, const vp8a_mb_info* neighbours,
+                       vp8a_rd_inter* out, uint32_t threads);
 
 /* ---- ARNR (src/arnr.rs) */
 int vo_build_arnr_altref(const vp8a_i420* frames, uint32_t n, uint32_t center,

@@ -23,18 +23,11 @@
 // partition), all reading the reference window the main warp staged. The
 // f64 RD decision runs on one thread with the reference's operation order;
 // the library is built with -fmad=false so no multiply-add is fused.
-#include "me_common.cuh"
+#include "census.cuh"
 
 namespace {
 using namespace vp8a_dev;
 
-struct MbInfoDev {
-  uint8_t ref_frame;  // VP8A_REF_INTRA = None
-  uint8_t is_split;
-  uint8_t pad[2];
-  vp8a_mv mv;
-  vp8a_mv split_mvs[16];
-};
 
 constexpr int MAX_REFS = 3;
 constexpr int WARPS_PER_REF = 5;
@@ -57,126 +50,6 @@ struct AnArgs {
   vp8a_ref_search* trace;
   unsigned long long spin_limit;
 };
-
-__constant__ uint8_t c_counts_to_probs[6][4] = {{7, 1, 1, 143},    {14, 18, 14, 107}, {135, 64, 57, 68},
-                                                {60, 56, 128, 65}, {159, 134, 128, 34}, {234, 188, 128, 28}};
-__constant__ uint8_t c_partitions[4][16] = {{0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 1, 1, 1, 1},
-                                            {0, 0, 1, 1, 0, 0, 1, 1, 0, 0, 1, 1, 0, 0, 1, 1},
-                                            {0, 0, 1, 1, 0, 0, 1, 1, 2, 2, 3, 3, 2, 2, 3, 3},
-                                            {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15}};
-__constant__ uint8_t c_partition_probs[3] = {110, 111, 150};
-__constant__ uint8_t c_submv_probs[5][3] = {{147, 136, 18}, {106, 145, 1}, {179, 121, 1}, {223, 1, 34}, {208, 1, 1}};
-__constant__ int8_t c_small_mvtree[14] = {2, 8, 4, 6, -0, -1, -2, -3, 10, 12, -4, -5, -6, -7};
-
-__device__ __forceinline__ bool mv_eq(vp8a_mv a, vp8a_mv b) { return a.row == b.row && a.col == b.col; }
-__device__ __forceinline__ bool mv_zero(vp8a_mv a) { return a.row == 0 && a.col == 0; }
-
-// bool_bits (src/encoder.rs:2229).
-__device__ __forceinline__ double bb(const double* t, int prob, int v) {
-  if (v) {
-    int idx = 256 - prob;
-    return t[idx > 255 ? 255 : idx];
-  }
-  return t[prob];
-}
-
-// mv_component_bits (src/motion_vector.rs:345), same summation order.
-__device__ double mv_component_bits(const double* t, const uint8_t* p, int value) {
-  const int a = value < 0 ? -value : value;
-  double bits = 0.0;
-  if (a > 7) {
-    bits += bb(t, p[0], 1);
-    for (int i = 0; i < 3; i++) bits += bb(t, p[9 + i], (a >> i) & 1);
-    int i = 9;
-    for (;;) {
-      bits += bb(t, p[9 + i], (a >> i) & 1);
-      i -= 1;
-      if (i <= 3) break;
-    }
-    if ((a & 0xfff0) != 0) bits += bb(t, p[9 + 3], (a >> 3) & 1);
-  } else {
-    bits += bb(t, p[0], 0);
-    double s = 0.0;
-    int i = 0;
-    for (int k = 2; k >= 0; k--) {
-      int bit = (a >> k) & 1;
-      s += bb(t, p[2 + (i >> 1)], bit);
-      int next = c_small_mvtree[i + bit];
-      if (next <= 0) break;
-      i = next;
-    }
-    bits += s;
-  }
-  if (a != 0) bits += bb(t, p[1], value < 0);
-  return bits;
-}
-
-struct Census {
-  vp8a_mv best_predictor, nearest, near_;
-  uint8_t p[4];
-};
-
-// find_near_mvs (src/near_mv.rs:310-402; default SignBias) + clamps
-// (MvClampRect::for_mb / clamp_mv, :236-283) + mv_ref_probs (:404).
-__device__ Census census(const MbInfoDev& above, const MbInfoDev& left, const MbInfoDev& al, int mb_col, int mb_row,
-                         int mb_cols, int mb_rows) {
-  vp8a_mv nm[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
-  int cnt[4] = {0, 0, 0, 0};
-  int mi = 0, ci = 0;
-  if (above.ref_frame != VP8A_REF_INTRA) {
-    if (!mv_zero(above.mv)) {
-      mi++;
-      nm[mi] = above.mv;
-      ci++;
-    }
-    cnt[ci] += 2;
-  }
-  if (left.ref_frame != VP8A_REF_INTRA) {
-    if (!mv_zero(left.mv)) {
-      if (!mv_eq(left.mv, nm[mi])) {
-        mi++;
-        nm[mi] = left.mv;
-        ci++;
-      }
-      cnt[ci] += 2;
-    } else {
-      cnt[0] += 2;
-    }
-  }
-  if (al.ref_frame != VP8A_REF_INTRA) {
-    if (!mv_zero(al.mv)) {
-      if (!mv_eq(al.mv, nm[mi])) {
-        mi++;
-        nm[mi] = al.mv;
-        ci++;
-      }
-      cnt[ci] += 1;
-    } else {
-      cnt[0] += 1;
-    }
-  }
-  if (cnt[3] != 0 && mv_eq(nm[mi], nm[1])) cnt[1] += 1;
-  cnt[3] = (above.is_split + left.is_split) * 2 + al.is_split;
-  if (cnt[2] > cnt[1]) {
-    int t = cnt[1];
-    cnt[1] = cnt[2];
-    cnt[2] = t;
-    vp8a_mv tm = nm[1];
-    nm[1] = nm[2];
-    nm[2] = tm;
-  }
-  if (cnt[1] >= cnt[0]) nm[0] = nm[1];
-  const int to_left = -((mb_col + 1) << 6), to_right = (mb_cols - mb_col) << 6;
-  const int to_top = -((mb_row + 1) << 6), to_bottom = (mb_rows - mb_row) << 6;
-  Census c;
-  vp8a_mv* outs[3] = {&c.best_predictor, &c.nearest, &c.near_};
-  for (int k = 0; k < 3; k++) {
-    outs[k]->col = (int16_t)clampi(nm[k].col, to_left, to_right);
-    outs[k]->row = (int16_t)clampi(nm[k].row, to_top, to_bottom);
-  }
-  for (int k = 0; k < 4; k++) c.p[k] = c_counts_to_probs[cnt[k]][k];
-  return c;
-}
 
 // group_sad_at_whole_mv(_shaped) (src/encoder.rs:7650-7797): SAD over the
 // group rectangle at the integer part of the eighth-pel vector.
@@ -369,7 +242,7 @@ __global__ void __launch_bounds__(MAX_REFS* WARPS_PER_REF * 32) analysis_kernel(
   const int ref = warp / WARPS_PER_REF, role = warp % WARPS_PER_REF;  // role 0 = main, 1..4 = split pid
   for (int i = threadIdx.x; i < 256; i += blockDim.x) bit_cost[i] = a.bit_cost[i];
   __syncthreads();
-  const MbInfoDev border = {VP8A_REF_INTRA, 0, {0, 0}, {0, 0}, {}};
+  const MbInfoDev border = {VP8A_REF_INTRA, 0, 0, 0, {0, 0}, {}};
 
   for (int r = blockIdx.x; r < a.mb_rows; r += gridDim.x) {
     for (int c = 0; c < a.mb_cols; c++) {

@@ -149,6 +149,31 @@ REF_SEARCH_DTYPE = np.dtype(
     ],
     align=True,
 )
+MB_INFO_DTYPE = np.dtype(
+    [
+        ("ref_frame", "u1"),
+        ("is_split", "u1"),
+        ("has_split_mvs", "u1"),
+        ("reserved", "u1"),
+        ("mv", MV_DTYPE),
+        ("split_mvs", MV_DTYPE, (16,)),
+    ]
+)
+RD_INTER_DTYPE = np.dtype(
+    [
+        ("ref_frame", "u1"),
+        ("mode", "u1"),
+        ("n_searched", "u1"),
+        ("leader", "u1"),
+        ("mv", MV_DTYPE),
+        ("sad", "<u4"),
+        ("cost", "<f8"),
+        ("bits", "<f8"),
+        ("found", SEARCH_RESULT_DTYPE, (3,)),
+    ],
+    align=True,
+)
+EFFORT_FASTEST, EFFORT_FAST, EFFORT_BALANCED, EFFORT_THOROUGH = 0, 1, 2, 3
 MB_LF_INFO_DTYPE = np.dtype(
     [
         ("y_mode_is_bpred", "u1"),
@@ -173,6 +198,8 @@ C_SIZES = {
     "vp8a_mb_lf_info": 8,
     "vp8a_filter_config": 32,
     "vp8a_source": 48,
+    "vp8a_mb_info": 72,
+    "vp8a_rd_inter": 56,
 }
 
 
@@ -190,6 +217,8 @@ def check_layouts():
         "vp8a_mb_lf_info": MB_LF_INFO_DTYPE.itemsize,
         "vp8a_filter_config": C.sizeof(FilterConfig),
         "vp8a_source": C.sizeof(Source),
+        "vp8a_mb_info": MB_INFO_DTYPE.itemsize,
+        "vp8a_rd_inter": RD_INTER_DTYPE.itemsize,
     }
     assert got == C_SIZES, (got, C_SIZES)
     return got
