@@ -18,11 +18,15 @@
 // still bounded, and a wait that runs out sets the device status word and
 // the whole grid returns (VP8A_E_DEVICE_TIMEOUT on the host).
 //
-// Inside a CTA, each reference gets one "main" warp (ZEROMV, diamond,
-// half, quarter, NEAREST, NEAR) and four SPLITMV warps (one per
-// partition), all reading the reference window the main warp staged. The
-// f64 RD decision runs on one thread with the reference's operation order;
-// the library is built with -fmad=false so no multiply-add is fused.
+// Per MB, one staging phase fetches (edge-clamped, all loads in flight
+// together) everything the searches read: per reference the search window
+// around the predictor, the NEAREST/NEAR six-tap halos and the 16x16
+// blocks at the ZERO and neighbour vectors. Then each reference gets one
+// "main" warp (ZEROMV, diamond, half via shared half-pel planes, quarter,
+// NEAREST, NEAR) and four SPLITMV warps (one per partition, groups in
+// parallel across lanes). The f64 RD decision runs on one thread with the
+// reference's operation order; the library is built with -fmad=false so no
+// multiply-add is fused.
 #include "census.cuh"
 
 namespace {
@@ -51,26 +55,29 @@ struct AnArgs {
   unsigned long long spin_limit;
 };
 
-// group_sad_at_whole_mv(_shaped) (src/encoder.rs:7650-7797): SAD over the
-// group rectangle at the integer part of the eighth-pel vector.
-__device__ uint32_t group_sad(const MePlane& P, const uint8_t* win, int wx0, int wy0, int mbx, int mby,
-                              const uint8_t* src, int row0, int col0, int gw, int gh, vp8a_mv mv, int lane) {
-  const int bx = mbx + (eighth(mv.col) >> 3), by = mby + (eighth(mv.row) >> 3);
-  const int lx = bx + col0 - wx0, ly = by + row0 - wy0;
-  const bool inwin = lx >= 0 && ly >= 0 && lx + gw <= WS && ly + gh <= WS;
-  uint32_t s = 0;
-  const int n = gw * gh;
-  for (int i = lane; i < n; i += 32) {
-    const int rr = i / gw, cc = i - rr * gw;
-    int ref;
-    if (inwin) ref = win[(ly + rr) * WS + lx + cc];
-    else
-      ref = P.plane[(size_t)clampi(by + row0 + rr, 0, P.height - 1) * P.stride + clampi(bx + col0 + cc, 0, P.width - 1)];
-    int d = (int)src[(row0 + rr) * 16 + col0 + cc] - ref;
-    s += (uint32_t)(d < 0 ? -d : d);
-  }
-  return __reduce_add_sync(FULL, s);
-}
+// ------------------------------------------------------------- staging
+
+// Regions staged per (MB, reference) before any search runs: the 40x40
+// search window around the predictor, the 21x21 six-tap halos of the
+// NEAREST and NEAR vectors, and 16x16 blocks at the integer offsets of the
+// ZERO vector and of the left/above neighbours' vectors (the SPLITMV
+// LEFT4X4 / ABOVE4X4 / ZERO4X4 candidates). Every byte is fetched
+// edge-clamped, so later reads need no bounds checks.
+constexpr int HS = 24;        // halo stride
+constexpr int MAX_BLOCKS = 9; // zero + 4 left + 4 above offsets
+constexpr int CMAX = 25;      // SPLITMV candidate vectors per partition
+
+struct RefSmem {
+  WarpScratch ws;                       // window + six-tap scratch + half planes
+  uint8_t halo_nearest[21 * HS + 8];
+  uint8_t halo_near[21 * HS + 8];
+  uint8_t blocks[MAX_BLOCKS][256];
+};
+
+struct MainOut {
+  uint32_t sad_zero, sad_nearest, sad_near;
+  vp8a_search_result whole, half, quarter;
+};
 
 struct SplitOut {
   double j;
@@ -78,6 +85,162 @@ struct SplitOut {
   uint8_t modes[16];
   int valid;
 };
+
+struct SplitScratch {
+  uint32_t table[16 * CMAX];  // group SAD per candidate vector
+  int16_t cox[CMAX], coy[CMAX];
+  vp8a_mv cmv[CMAX];
+  vp8a_mv split[16];
+  int nc;
+};
+
+struct Plan {
+  int wx0, wy0;        // window origin (plane pixels)
+  int hn_x, hn_y;      // NEAREST halo origin
+  int hr_x, hr_y;      // NEAR halo origin
+  int nblocks;
+  int box[MAX_BLOCKS], boy[MAX_BLOCKS];  // block integer offsets
+};
+
+// Geometry of SPLITMV group g of partition p (PartitionGroups::build,
+// src/encoder.rs:7912-7980): row0, col0, width, height, anchor.
+__constant__ int8_t c_geom[4][16][5] = {
+    {{0, 0, 16, 8, 0}, {8, 0, 16, 8, 8}},
+    {{0, 0, 8, 16, 0}, {0, 8, 8, 16, 2}},
+    {{0, 0, 8, 8, 0}, {0, 8, 8, 8, 2}, {8, 0, 8, 8, 8}, {8, 8, 8, 8, 10}},
+    {{0, 0, 4, 4, 0},   {0, 4, 4, 4, 1},   {0, 8, 4, 4, 2},   {0, 12, 4, 4, 3},
+     {4, 0, 4, 4, 4},   {4, 4, 4, 4, 5},   {4, 8, 4, 4, 6},   {4, 12, 4, 4, 7},
+     {8, 0, 4, 4, 8},   {8, 4, 4, 4, 9},   {8, 8, 4, 4, 10},  {8, 12, 4, 4, 11},
+     {12, 0, 4, 4, 12}, {12, 4, 4, 4, 13}, {12, 8, 4, 4, 14}, {12, 12, 4, 4, 15}}};
+
+__device__ __forceinline__ int int_off(int16_t v) { return eighth(v) >> 3; }
+
+// External LEFT4X4 / ABOVE4X4 vectors (left_block_mv / above_block_mv for
+// anchors on the MB's left column / top row, src/near_mv.rs:722-760).
+__device__ __forceinline__ vp8a_mv ext_left(const MbInfoDev& l, int anchor) {
+  if (l.ref_frame == VP8A_REF_INTRA) return vp8a_mv{0, 0};
+  return l.is_split ? l.split_mvs[anchor + 3] : l.mv;
+}
+__device__ __forceinline__ vp8a_mv ext_above(const MbInfoDev& a, int anchor) {
+  if (a.ref_frame == VP8A_REF_INTRA) return vp8a_mv{0, 0};
+  return a.is_split ? a.split_mvs[anchor + 12] : a.mv;
+}
+
+// Stage every region of every reference; each thread keeps up to BATCH
+// loads in flight before storing.
+template <int BATCH>
+__device__ void stage(const AnArgs& a, RefSmem* rs, const Plan& pl, int mbx, int mby, int tid, int nthreads) {
+  const int per_ref = 40 * 40 + 2 * 441 + pl.nblocks * 256;
+  const int total = a.n_refs * per_ref;
+  for (int base = tid; base < total; base += nthreads * BATCH) {
+    uint8_t v[BATCH];
+    uint8_t* d[BATCH];
+#pragma unroll
+    for (int j = 0; j < BATCH; j++) {
+      const int e = base + j * nthreads;
+      d[j] = nullptr;
+      if (e < total) {
+        const int k = e < per_ref ? 0 : (e < 2 * per_ref ? 1 : 2);
+        const int rem = e - k * per_ref;
+        const MePlane& P = a.refs[k];
+        int x, y;
+        if (rem < 1600) {
+          const int r = rem / 40, c = rem - r * 40;
+          x = pl.wx0 + c;
+          y = pl.wy0 + r;
+          d[j] = rs[k].ws.win + r * WS + c;
+        } else if (rem < 1600 + 2 * 441) {
+          const int q = rem - 1600, h = q >= 441, qq = q - h * 441;
+          const int r = qq / 21, c = qq - r * 21;
+          x = (h ? pl.hr_x : pl.hn_x) + c;
+          y = (h ? pl.hr_y : pl.hn_y) + r;
+          d[j] = (h ? rs[k].halo_near : rs[k].halo_nearest) + r * HS + c;
+        } else {
+          const int q = rem - 1600 - 2 * 441, b = q >> 8, r = (q >> 4) & 15, c = q & 15;
+          x = mbx + pl.box[b] + c;
+          y = mby + pl.boy[b] + r;
+          d[j] = rs[k].blocks[b] + r * 16 + c;
+        }
+        v[j] = P.plane[(size_t)clampi(y, 0, P.height - 1) * P.stride + clampi(x, 0, P.width - 1)];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < BATCH; j++)
+      if (d[j]) *d[j] = v[j];
+  }
+}
+
+// -------------------------------------------------------------- SPLITMV
+
+// This lane's 8 pixels of its group rectangle as (row, col) runs: groups
+// have 8*L pixels for L lanes per group, so each lane owns 8.
+struct LanePix {
+  int r0, c0, r1, c1, n0;  // two runs; n0 = pixels in the first run (8 or 4)
+};
+
+__device__ __forceinline__ LanePix lane_pixels(int row0, int col0, int gw, int s) {
+  LanePix p;
+  if (gw == 16) {
+    p.r0 = row0 + (s >> 1);
+    p.c0 = col0 + (s & 1) * 8;
+    p.n0 = 8;
+  } else if (gw == 8) {
+    p.r0 = row0 + s;
+    p.c0 = col0;
+    p.n0 = 8;
+  } else {
+    p.r0 = row0 + 2 * s;
+    p.c0 = col0;
+    p.n0 = 4;
+  }
+  p.r1 = p.r0 + 1;
+  p.c1 = p.c0;
+  return p;
+}
+
+// Partial group SAD of this lane's pixels for the MB-extent block whose
+// top-left is plane pixel (bx, by): from the window, a staged block, or
+// clamped global loads.
+__device__ __forceinline__ uint32_t lane_gsad(const MePlane& P, const RefSmem& R, const Plan& pl, int mbx, int mby,
+                                              const uint8_t* src, const LanePix& q, int bx, int by) {
+  const int lx = bx - pl.wx0, ly = by - pl.wy0;
+  const uint8_t* base = nullptr;
+  int st = 0;
+  if (lx >= 0 && ly >= 0 && lx + 16 <= WS && ly + 16 <= WS) {
+    base = R.ws.win + ly * WS + lx;
+    st = WS;
+  } else {
+    for (int b = 0; b < pl.nblocks; b++)
+      if (mbx + pl.box[b] == bx && mby + pl.boy[b] == by) {
+        base = R.blocks[b];
+        st = 16;
+        break;
+      }
+  }
+  uint32_t s = 0;
+  if (base) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int rr = i < q.n0 ? q.r0 : q.r1, cc = i < q.n0 ? q.c0 + i : q.c1 + i - q.n0;
+      const int d = (int)src[rr * 16 + cc] - (int)base[rr * st + cc];
+      s += (uint32_t)(d < 0 ? -d : d);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int rr = i < q.n0 ? q.r0 : q.r1, cc = i < q.n0 ? q.c0 + i : q.c1 + i - q.n0;
+      const int ref = P.plane[(size_t)clampi(by + rr, 0, P.height - 1) * P.stride + clampi(bx + cc, 0, P.width - 1)];
+      const int d = (int)src[rr * 16 + cc] - ref;
+      s += (uint32_t)(d < 0 ? -d : d);
+    }
+  }
+  return s;
+}
+
+__device__ __forceinline__ uint32_t group_reduce(uint32_t v, int L) {
+  for (int o = L >> 1; o >= 1; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  return v;
+}
 
 __device__ __forceinline__ double submv_ref_bits(const double* t, const uint8_t* p, int mode) {
   switch (mode) {
@@ -98,77 +261,115 @@ __device__ __forceinline__ double mv_partition_bits(const double* t, int pid) {
   }
 }
 
-// score_split_partition (src/encoder.rs:8080-8246) on one warp.
-__device__ void split_partition(const AnArgs& a, const double* t, const MePlane& P, const uint8_t* win, int wx0,
-                                int wy0, int mbx, int mby, const uint8_t* src, vp8a_mv bp, const MbInfoDev& above,
-                                const MbInfoDev& left, int pid, SplitOut* out, int lane) {
+// score_split_partition (src/encoder.rs:8080-8246) on one warp. Groups run
+// in parallel (32/G lanes each) for their NEW4X4 diamonds and for a table
+// of group SADs at every vector the sub-MV choice can consider (ZERO, the
+// external neighbours' vectors, every group's NEW result); the sequential
+// LEFT/ABOVE/ZERO/NEW choice over groups then reads that table.
+__device__ void split_partition(const AnArgs& a, const double* t, const MePlane& P, const RefSmem& R, const Plan& pl,
+                                int mbx, int mby, const uint8_t* src, vp8a_mv bp, const MbInfoDev& above,
+                                const MbInfoDev& left, int pid, SplitScratch& W, SplitOut* out, int lane) {
+  const int G = pid == 3 ? 16 : (pid == 2 ? 4 : 2);
+  const int L = 32 / G, g = lane / L, s = lane - g * L;
+  const int row0 = c_geom[pid][g][0], col0 = c_geom[pid][g][1], gw = c_geom[pid][g][2];
+  const LanePix q = lane_pixels(row0, col0, gw, s);
+  // group_small_diamond_search (src/encoder.rs:7812-7879) for every group
+  // at once: snap then clamp the centre; N, S, W, E clamped, not snapped.
+  vp8a_mv best;
+  best.row = (int16_t)clampi((bp.row / 4) * 4, -1023, 1023);
+  best.col = (int16_t)clampi((bp.col / 4) * 4, -1023, 1023);
+  uint32_t bs =
+      group_reduce(lane_gsad(P, R, pl, mbx, mby, src, q, mbx + int_off(best.col), mby + int_off(best.row)), L);
+  bool active = true;
+  for (int it = 0; it < 4; it++) {
+    bool improved = false;
+    const int dr[4] = {-4, 4, 0, 0}, dc[4] = {0, 0, -4, 4};
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+      vp8a_mv c;
+      c.row = (int16_t)clampi(best.row + dr[d], -1023, 1023);
+      c.col = (int16_t)clampi(best.col + dc[d], -1023, 1023);
+      const uint32_t sv =
+          group_reduce(lane_gsad(P, R, pl, mbx, mby, src, q, mbx + int_off(c.col), mby + int_off(c.row)), L);
+      if (active && !mv_eq(c, best) && sv < bs) {
+        bs = sv;
+        best = c;
+        improved = true;
+      }
+    }
+    if (!improved) active = false;
+  }
+  // Candidate vectors (unique integer offsets): ZERO, external LEFT/ABOVE,
+  // then every group's NEW result.
+  if (lane == 0) W.nc = 0;
+  __syncwarp();
+  auto add = [&](vp8a_mv m) {
+    const int ox = int_off(m.col), oy = int_off(m.row);
+    for (int i = 0; i < W.nc; i++)
+      if (W.cox[i] == ox && W.coy[i] == oy) return;
+    const int n = W.nc;
+    __syncwarp();
+    if (lane == 0) {
+      W.cox[n] = (int16_t)ox;
+      W.coy[n] = (int16_t)oy;
+      W.cmv[n] = m;
+      W.nc = n + 1;
+    }
+    __syncwarp();
+  };
+  add(vp8a_mv{0, 0});
+  for (int gg = 0; gg < G; gg++) {
+    const int anc = c_geom[pid][gg][4];
+    if ((anc & 3) == 0) add(ext_left(left, anc));
+    if (anc < 4) add(ext_above(above, anc));
+  }
+  for (int gg = 0; gg < G; gg++) {
+    vp8a_mv m;
+    m.row = (int16_t)__shfl_sync(FULL, (int)best.row, gg * L);
+    m.col = (int16_t)__shfl_sync(FULL, (int)best.col, gg * L);
+    add(m);
+  }
+  const int nc = W.nc;
+  for (int m = 0; m < nc; m++) {
+    const uint32_t sv = group_reduce(lane_gsad(P, R, pl, mbx, mby, src, q, mbx + W.cox[m], mby + W.coy[m]), L);
+    if (s == 0) W.table[g * CMAX + m] = sv;
+  }
+  // NEW4X4 results per group.
+  if (s == 0) W.split[g] = best;  // temporary: group g's NEW vector
+  __syncwarp();
+  vp8a_mv news[16];
+  uint32_t new_sad[16];
+  for (int gg = 0; gg < G; gg++) {
+    news[gg] = W.split[gg];
+    new_sad[gg] = (uint32_t)__shfl_sync(FULL, (int)bs, gg * L);
+  }
+  __syncwarp();
+  // The sequential sub-MV choice (uniform on every lane).
   vp8a_mv split[16];
   for (int i = 0; i < 16; i++) split[i] = vp8a_mv{0, 0};
   uint8_t modes[16];
   for (int i = 0; i < 16; i++) modes[i] = VP8A_SUBMV_ZERO;
+  auto lookup = [&](int gg, vp8a_mv m) -> uint32_t {
+    const int ox = int_off(m.col), oy = int_off(m.row);
+    for (int i = 0; i < nc; i++)
+      if (W.cox[i] == ox && W.coy[i] == oy) return W.table[gg * CMAX + i];
+    return 0xffffffffu;  // unreachable: every candidate vector is tabled
+  };
   uint32_t total_sad = 0;
   double total_bits = 0.0;
-  const int ngroups = pid == 3 ? 16 : (pid == 2 ? 4 : 2);
-  for (int g = 0; g < ngroups; g++) {
-    // Members (ascending) and bounding rectangle (PartitionGroups::build).
-    int anchor = -1, min_r = 3, max_r = 0, min_c = 3, max_c = 0;
-    for (int b = 0; b < 16; b++)
-      if (c_partitions[pid][b] == g) {
-        if (anchor < 0) anchor = b;
-        min_r = min(min_r, b >> 2);
-        max_r = max(max_r, b >> 2);
-        min_c = min(min_c, b & 3);
-        max_c = max(max_c, b & 3);
-      }
-    const int row0 = min_r * 4, col0 = min_c * 4, gw = (max_c + 1 - min_c) * 4, gh = (max_r + 1 - min_r) * 4;
-    // left_block_mv / above_block_mv (src/near_mv.rs:722-760).
-    vp8a_mv lmv, amv;
-    if ((anchor & 3) == 0) {
-      lmv = left.ref_frame == VP8A_REF_INTRA ? vp8a_mv{0, 0} : (left.is_split ? left.split_mvs[anchor + 3] : left.mv);
-    } else {
-      lmv = split[anchor - 1];
-    }
-    if (anchor < 4) {
-      amv = above.ref_frame == VP8A_REF_INTRA ? vp8a_mv{0, 0} : (above.is_split ? above.split_mvs[anchor + 12] : above.mv);
-    } else {
-      amv = split[anchor - 4];
-    }
-    int ctxi;
-    {
-      const bool lez = mv_zero(lmv), aez = mv_zero(amv), lea = mv_eq(lmv, amv);
-      ctxi = (lea && lez) ? 4 : (lea ? 3 : (aez ? 2 : (lez ? 1 : 0)));
-    }
+  for (int gg = 0; gg < G; gg++) {
+    const int anchor = c_geom[pid][gg][4];
+    const vp8a_mv lmv = (anchor & 3) == 0 ? ext_left(left, anchor) : split[anchor - 1];
+    const vp8a_mv amv = anchor < 4 ? ext_above(above, anchor) : split[anchor - 4];
+    const bool lez = mv_zero(lmv), aez = mv_zero(amv), lea = mv_eq(lmv, amv);
+    const int ctxi = (lea && lez) ? 4 : (lea ? 3 : (aez ? 2 : (lez ? 1 : 0)));
     const uint8_t* probs = c_submv_probs[ctxi];
-    // group_small_diamond_search (src/encoder.rs:7812-7879).
-    vp8a_mv best;
-    best.row = (int16_t)clampi((bp.row / 4) * 4, -1023, 1023);
-    best.col = (int16_t)clampi((bp.col / 4) * 4, -1023, 1023);
-    uint32_t best_sad = group_sad(P, win, wx0, wy0, mbx, mby, src, row0, col0, gw, gh, best, lane);
-    for (int it = 0; it < 4; it++) {
-      bool improved = false;
-      const int dr[4] = {-4, 4, 0, 0}, dc[4] = {0, 0, -4, 4};
-#pragma unroll
-      for (int d = 0; d < 4; d++) {
-        vp8a_mv c;
-        c.row = (int16_t)clampi(best.row + dr[d], -1023, 1023);
-        c.col = (int16_t)clampi(best.col + dc[d], -1023, 1023);
-        if (mv_eq(c, best)) continue;
-        uint32_t s = group_sad(P, win, wx0, wy0, mbx, mby, src, row0, col0, gw, gh, c, lane);
-        if (s < best_sad) {
-          best_sad = s;
-          best = c;
-          improved = true;
-        }
-      }
-      if (!improved) break;
-    }
-    // Score LEFT4X4, ABOVE4X4, ZERO4X4, NEW4X4.
     int best_mode = VP8A_SUBMV_ZERO;
     vp8a_mv best_mv = {0, 0}, best_diff = {0, 0};
     double best_j = __longlong_as_double(0x7ff0000000000000LL);
     const vp8a_mv cm[3] = {lmv, amv, vp8a_mv{0, 0}};
     for (int m = 0; m < 3; m++) {
-      const double sad = (double)group_sad(P, win, wx0, wy0, mbx, mby, src, row0, col0, gw, gh, cm[m], lane);
+      const double sad = (double)lookup(gg, cm[m]);
       const double mode_bits = submv_ref_bits(t, probs, m);
       const double j = sad + a.lambda * (mode_bits + 0.0);
       if (j < best_j) {
@@ -178,15 +379,16 @@ __device__ void split_partition(const AnArgs& a, const double* t, const MePlane&
         best_diff = vp8a_mv{0, 0};
       }
     }
-    const int dr = (int)best.row - bp.row, dc = (int)best.col - bp.col;
+    const vp8a_mv nm = news[gg];
+    const int dr = (int)nm.row - bp.row, dc = (int)nm.col - bp.col;
     if (dr >= -1023 && dr <= 1023 && dc >= -1023 && dc <= 1023) {
       const double diff_bits = mv_component_bits(t, a.ctx.p[0], dr) + mv_component_bits(t, a.ctx.p[1], dc);
       const double mode_bits = submv_ref_bits(t, probs, VP8A_SUBMV_NEW);
-      const double j = (double)best_sad + a.lambda * (mode_bits + diff_bits);
+      const double j = (double)new_sad[gg] + a.lambda * (mode_bits + diff_bits);
       if (j < best_j) {
         best_j = j;
         best_mode = VP8A_SUBMV_NEW;
-        best_mv = best;
+        best_mv = nm;
         best_diff.row = (int16_t)dr;
         best_diff.col = (int16_t)dc;
       }
@@ -195,14 +397,14 @@ __device__ void split_partition(const AnArgs& a, const double* t, const MePlane&
       if (lane == 0) out->valid = 0;
       return;
     }
-    const uint32_t gs = group_sad(P, win, wx0, wy0, mbx, mby, src, row0, col0, gw, gh, best_mv, lane);
+    const uint32_t gs = lookup(gg, best_mv);
     for (int b = 0; b < 16; b++)
-      if (c_partitions[pid][b] == g) split[b] = best_mv;
+      if (c_partitions[pid][b] == gg) split[b] = best_mv;
     total_sad += gs;
     total_bits += submv_ref_bits(t, probs, best_mode);
     if (best_mode == VP8A_SUBMV_NEW)
       total_bits += mv_component_bits(t, a.ctx.p[0], best_diff.row) + mv_component_bits(t, a.ctx.p[1], best_diff.col);
-    modes[g] = (uint8_t)best_mode;
+    modes[gg] = (uint8_t)best_mode;
   }
   const double partition_bits = mv_partition_bits(t, pid);
   if (lane == 0) {
@@ -215,11 +417,6 @@ __device__ void split_partition(const AnArgs& a, const double* t, const MePlane&
   }
 }
 
-struct MainOut {
-  uint32_t sad_zero, sad_nearest, sad_near;
-  vp8a_search_result whole, half, quarter;
-};
-
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   unsigned v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -229,24 +426,35 @@ __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// SAD of the 16x16 source against a staged 16x16 block.
+__device__ __forceinline__ uint32_t sad_block16(const uint8_t* blk, const uint8_t* src, int lane) {
+  const int row = lane >> 1, c0 = (lane & 1) * 8;
+  const uint32_t* b = (const uint32_t*)(blk + row * 16 + c0);
+  const uint32_t* sp = (const uint32_t*)(src + row * 16 + c0);
+  return __reduce_add_sync(FULL, __vsadu4(b[0], sp[0]) + __vsadu4(b[1], sp[1]));
+}
+
 __global__ void __launch_bounds__(MAX_REFS* WARPS_PER_REF * 32) analysis_kernel(AnArgs a) {
-  __shared__ WarpScratch scratch[MAX_REFS];
+  __shared__ RefSmem rs[MAX_REFS];
+  __shared__ SplitScratch ss[MAX_REFS * 4];
   __shared__ __align__(16) uint8_t src[256];
   __shared__ double bit_cost[256];
   __shared__ MainOut mains[MAX_REFS];
   __shared__ SplitOut splits[MAX_REFS][4];
   __shared__ MbInfoDev nb[3];  // above, left, aboveleft
   __shared__ Census cen;
+  __shared__ Plan plan;
   __shared__ int s_abort;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tid = threadIdx.x, nthreads = blockDim.x;
+  const int warp = tid >> 5, lane = tid & 31;
   const int ref = warp / WARPS_PER_REF, role = warp % WARPS_PER_REF;  // role 0 = main, 1..4 = split pid
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) bit_cost[i] = a.bit_cost[i];
+  for (int i = tid; i < 256; i += nthreads) bit_cost[i] = a.bit_cost[i];
   __syncthreads();
   const MbInfoDev border = {VP8A_REF_INTRA, 0, 0, 0, {0, 0}, {}};
 
   for (int r = blockIdx.x; r < a.mb_rows; r += gridDim.x) {
     for (int c = 0; c < a.mb_cols; c++) {
-      if (threadIdx.x == 0) {
+      if (tid == 0) {
         int abort = 0;
         if (r > 0) {
           const unsigned need = (unsigned)min(c + 2, a.mb_cols);
@@ -257,7 +465,7 @@ __global__ void __launch_bounds__(MAX_REFS* WARPS_PER_REF * 32) analysis_kernel(
               abort = 1;
               break;
             }
-            __nanosleep(128);
+            __nanosleep(64);
           }
         } else if (*(volatile unsigned*)a.status != 0u) {
           abort = 1;
@@ -268,46 +476,70 @@ __global__ void __launch_bounds__(MAX_REFS* WARPS_PER_REF * 32) analysis_kernel(
       if (s_abort) return;
       // Neighbour records and the edge-replicated source MB
       // (extract_mb, src/encoder.rs:5549).
-      if (threadIdx.x < 3) {
-        const int k = threadIdx.x;
-        const int nr = k == 1 ? r : r - 1, nc = k == 0 ? c : c - 1;
-        nb[k] = (nr >= 0 && nc >= 0) ? a.infos[(size_t)nr * a.mb_cols + nc] : border;
+      if (tid < 3) {
+        const int nr = tid == 1 ? r : r - 1, nc = tid == 0 ? c : c - 1;
+        nb[tid] = (nr >= 0 && nc >= 0) ? a.infos[(size_t)nr * a.mb_cols + nc] : border;
       }
-      for (int i = threadIdx.x; i < 256; i += blockDim.x) {
-        const int y = min(r * 16 + (i >> 4), a.fh - 1), x = min(c * 16 + (i & 15), a.fw - 1);
-        src[i] = a.fy[(size_t)y * a.fys + x];
+      if (tid < 256) {
+        const int y = min(r * 16 + (tid >> 4), a.fh - 1), x = min(c * 16 + (tid & 15), a.fw - 1);
+        src[tid] = a.fy[(size_t)y * a.fys + x];
       }
-      __syncthreads();
-      if (threadIdx.x == 0) cen = census(nb[0], nb[1], nb[2], c, r, a.mb_cols, a.mb_rows);
       __syncthreads();
       const int mbx = c * 16, mby = r * 16;
-      const vp8a_mv bp = cen.best_predictor;
-      const int cx = snap_whole(clamp_component(bp.col)) / 4, cy = snap_whole(clamp_component(bp.row)) / 4;
-      const int wx0 = mbx + cx - WIN_LEAD, wy0 = mby + cy - WIN_LEAD;
-      if (ref < a.n_refs && role == 0) load_window(a.refs[ref], scratch[ref].win, wx0, wy0, lane);
+      if (tid == 0) {
+        cen = census(nb[0], nb[1], nb[2], c, r, a.mb_cols, a.mb_rows);
+        Plan p;
+        const vp8a_mv bp = cen.best_predictor;
+        p.wx0 = mbx + snap_whole(clamp_component(bp.col)) / 4 - WIN_LEAD;
+        p.wy0 = mby + snap_whole(clamp_component(bp.row)) / 4 - WIN_LEAD;
+        p.hn_x = mbx + int_off(cen.nearest.col) - 2;
+        p.hn_y = mby + int_off(cen.nearest.row) - 2;
+        p.hr_x = mbx + int_off(cen.near_.col) - 2;
+        p.hr_y = mby + int_off(cen.near_.row) - 2;
+        p.nblocks = 0;
+        auto addb = [&](vp8a_mv m) {
+          const int ox = int_off(m.col), oy = int_off(m.row);
+          for (int i = 0; i < p.nblocks; i++)
+            if (p.box[i] == ox && p.boy[i] == oy) return;
+          p.box[p.nblocks] = ox;
+          p.boy[p.nblocks] = oy;
+          p.nblocks++;
+        };
+        addb(vp8a_mv{0, 0});
+        for (int anc = 0; anc < 16; anc += 4) addb(ext_left(nb[1], anc));
+        for (int anc = 0; anc < 4; anc++) addb(ext_above(nb[0], anc));
+        plan = p;
+      }
+      __syncthreads();
+      stage<24>(a, rs, plan, mbx, mby, tid, nthreads);
       __syncthreads();
       if (ref < a.n_refs) {
         const MePlane& P = a.refs[ref];
-        WarpScratch& S = scratch[ref];
+        RefSmem& R = rs[ref];
+        const vp8a_mv bp = cen.best_predictor;
         if (role == 0) {
           MainOut m;
-          m.sad_zero = sad_whole_at(P, S.win, wx0, wy0, mbx, mby, src, lane);
-          m.whole = diamond(P, S, wx0, wy0, mbx, mby, bp, 8, src, lane);
-          m.half = refine(P, S, wx0, wy0, mbx, mby, m.whole.mv, 2, src, lane);
-          m.quarter = refine(P, S, wx0, wy0, mbx, mby, m.half.mv, 1, src, lane);
-          m.sad_nearest = sad_at_mv(P, S, wx0, wy0, mbx, mby, cen.nearest.row, cen.nearest.col, src, lane);
-          m.sad_near = sad_at_mv(P, S, wx0, wy0, mbx, mby, cen.near_.row, cen.near_.col, src, lane);
+          m.sad_zero = sad_block16(R.blocks[0], src, lane);
+          m.whole = diamond(P, R.ws, plan.wx0, plan.wy0, mbx, mby, bp, 8, src, lane);
+          if (!half_refine_planes(R.ws, plan.wx0, plan.wy0, mbx, mby, m.whole.mv, src, lane, &m.half))
+            m.half = refine(P, R.ws, plan.wx0, plan.wy0, mbx, mby, m.whole.mv, 2, src, lane);
+          m.quarter = refine(P, R.ws, plan.wx0, plan.wy0, mbx, mby, m.half.mv, 1, src, lane);
+          const int en_r = eighth(cen.nearest.row), en_c = eighth(cen.nearest.col);
+          m.sad_nearest = subpel_sad(R.halo_nearest, HS, en_c & 7, en_r & 7, src, R.ws.temp, lane);
+          const int er_r = eighth(cen.near_.row), er_c = eighth(cen.near_.col);
+          m.sad_near = subpel_sad(R.halo_near, HS, er_c & 7, er_r & 7, src, R.ws.temp, lane);
           if (lane == 0) mains[ref] = m;
         } else {
-          split_partition(a, bit_cost, P, S.win, wx0, wy0, mbx, mby, src, bp, nb[0], nb[1], role - 1,
-                          &splits[ref][role - 1], lane);
+          split_partition(a, bit_cost, P, R, plan, mbx, mby, src, bp, nb[0], nb[1], role - 1,
+                          ss[ref * 4 + role - 1], &splits[ref][role - 1], lane);
         }
       }
       __syncthreads();
-      if (threadIdx.x == 0) {
+      if (tid == 0) {
         const double* t = bit_cost;
         const double lambda = a.lambda;
         const uint8_t* p = cen.p;
+        const vp8a_mv bp = cen.best_predictor;
         double best_total = __longlong_as_double(0x7ff0000000000000LL);
         int best_k = -1, best_mode = 0, best_pid = VP8A_PART_NONE;
         vp8a_mv best_mv = {0, 0};
@@ -347,14 +579,14 @@ __global__ void __launch_bounds__(MAX_REFS* WARPS_PER_REF * 32) analysis_kernel(
           const double bits_split = bb(t, p[0], 1) + bb(t, p[1], 1) + bb(t, p[2], 1) + bb(t, p[3], 1);
           int have = 0, sp = -1;
           double sj = 0.0;
-          for (int q = 0; q < 4; q++) {
-            if (!splits[k][q].valid) continue;
-            const double total_j = splits[k][q].j + lambda * bits_split;
+          for (int qq = 0; qq < 4; qq++) {
+            if (!splits[k][qq].valid) continue;
+            const double total_j = splits[k][qq].j + lambda * bits_split;
             // The stored best already includes bits_split and the
             // comparison adds it again (src/encoder.rs:8679-8683).
             if (!have || total_j < sj + lambda * bits_split) {
               sj = total_j;
-              sp = q;
+              sp = qq;
               have = 1;
             }
           }
@@ -414,6 +646,7 @@ __global__ void __launch_bounds__(MAX_REFS* WARPS_PER_REF * 32) analysis_kernel(
           info.ref_frame = d.ref_frame;
           info.mv = best_mv;
           info.is_split = best_mode == VP8A_MODE_SPLIT;
+          info.has_split_mvs = info.is_split;
           for (int i = 0; i < 16; i++) info.split_mvs[i] = d.split_mvs[i];
         }
         a.dec[(size_t)r * a.mb_cols + c] = d;

@@ -66,14 +66,18 @@ __global__ void __launch_bounds__(ME_WARPS * 32) me_batch_kernel(MeBatch a) {
     vp8a_search_result r = diamond(a.P, S, wx0, wy0, mbx, mby, c, a.max_iters, src, lane);
     if (lane == 0) a.out0[item] = r;
   } else if (MODE == MODE_HALF) {
-    vp8a_search_result r = refine(a.P, S, wx0, wy0, mbx, mby, c, 2, src, lane);
+    vp8a_search_result r;
+    if (!half_refine_planes(S, wx0, wy0, mbx, mby, c, src, lane, &r))
+      r = refine(a.P, S, wx0, wy0, mbx, mby, c, 2, src, lane);
     if (lane == 0) a.out0[item] = r;
   } else if (MODE == MODE_QUARTER) {
     vp8a_search_result r = refine(a.P, S, wx0, wy0, mbx, mby, c, 1, src, lane);
     if (lane == 0) a.out0[item] = r;
   } else {
     vp8a_search_result w = diamond(a.P, S, wx0, wy0, mbx, mby, c, a.max_iters, src, lane);
-    vp8a_search_result h = refine(a.P, S, wx0, wy0, mbx, mby, w.mv, 2, src, lane);
+    vp8a_search_result h;
+    if (!half_refine_planes(S, wx0, wy0, mbx, mby, w.mv, src, lane, &h))
+      h = refine(a.P, S, wx0, wy0, mbx, mby, w.mv, 2, src, lane);
     vp8a_search_result q = refine(a.P, S, wx0, wy0, mbx, mby, h.mv, 1, src, lane);
     if (lane == 0) {
       if (a.out0) a.out0[item] = w;

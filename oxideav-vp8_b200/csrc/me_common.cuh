@@ -31,6 +31,10 @@ struct WarpScratch {
   uint8_t win[WIN_BYTES];
   uint8_t temp[21 * 16 + 16];
   uint8_t halo[21 * 24 + 16];
+  // Half-pel planes around a whole-pel centre: H 22x17, V 17x16, D 17x17.
+  uint8_t hp[22 * 17 + 4];
+  uint8_t vp[17 * 16 + 4];
+  uint8_t dp[17 * 17 + 4];
 };
 
 __device__ __forceinline__ int16_t clamp_component(int v) { return (int16_t)clampi(v, -1023, 1023); }
@@ -256,6 +260,85 @@ __device__ __forceinline__ vp8a_search_result refine(const MePlane& P, WarpScrat
   res.mv = best;
   res.sad = best_sad;
   return res;
+}
+
+// half_pixel_refine_luma around a whole-pel centre whose neighbourhood
+// the window covers. The eight half-pel candidates share three planes —
+// horizontal (H), vertical (V) and horizontal-then-vertical (D) half-pel
+// samples — so each six-tap output is computed once per MB instead of once
+// per candidate; every candidate's prediction is a 16x16 sub-block of one
+// plane, byte-identical to its own two-pass synthesis (same taps, same
+// 8-bit intermediate, same edge-clamped source). Returns false when the
+// window does not cover the planes (the caller then uses refine()).
+__device__ __forceinline__ bool half_refine_planes(WarpScratch& S, int wx0, int wy0, int mbx, int mby,
+                                                   vp8a_mv center, const uint8_t* src, int lane,
+                                                   vp8a_search_result* out) {
+  if ((center.row & 3) || (center.col & 3) || center.row < -1020 || center.row > 1020 || center.col < -1020 ||
+      center.col > 1020)
+    return false;
+  const int bx = mbx + center.col / 4 - wx0, by = mby + center.row / 4 - wy0;  // block origin in window
+  if (bx < 3 || by < 3 || bx + 19 > WS || by + 19 > WS) return false;
+  const int* f = c_sixtap[4];
+  // H: 22 rows (window rows by-3 .. by+18), 17 outputs at x = bx + i - 0.5.
+  for (int o = lane; o < 22 * 17; o += 32) {
+    const int r = o / 17, i = o - r * 17;
+    const uint8_t* p = S.win + (by - 3 + r) * WS + bx + i - 3;
+    S.hp[o] = (uint8_t)interp6(f, p[0], p[1], p[2], p[3], p[4], p[5]);
+  }
+  // V: 17 rows at y = by + r - 0.5, 16 columns.
+  for (int o = lane; o < 17 * 16; o += 32) {
+    const int r = o >> 4, c = o & 15;
+    const uint8_t* p = S.win + (by + r - 3) * WS + bx + c;
+    S.vp[o] = (uint8_t)interp6(f, p[0], p[WS], p[2 * WS], p[3 * WS], p[4 * WS], p[5 * WS]);
+  }
+  __syncwarp();
+  // D: vertical half-pel over H (rows r..r+5 of H), 17 x 17.
+  for (int o = lane; o < 17 * 17; o += 32) {
+    const int r = o / 17, i = o - r * 17;
+    const uint8_t* p = S.hp + r * 17 + i;
+    S.dp[o] = (uint8_t)interp6(f, p[0], p[17], p[34], p[51], p[68], p[85]);
+  }
+  __syncwarp();
+  // Centre SAD (whole pel, the copy path) and the eight candidates in the
+  // reference's order (-1,-1) (-1,0) (-1,1) (0,-1) (0,1) (1,-1) (1,0) (1,1).
+  vp8a_mv best = center;
+  uint32_t best_sad = sad_win16(S.win, bx, by, src, lane);
+  const int c = lane & 15, r0 = (lane >> 4) * 8;
+#pragma unroll 1
+  for (int k = 0; k < 8; k++) {
+    const int dy = (k < 3) ? -1 : (k < 5 ? 0 : 1);
+    const int dx = (k == 0 || k == 3 || k == 5) ? -1 : ((k == 1 || k == 6) ? 0 : 1);
+    const int cx = dx > 0, cy = dy > 0;
+    const uint8_t* pl;
+    int st;
+    if (dy == 0) {
+      pl = S.hp + 3 * 17 + cx;
+      st = 17;
+    } else if (dx == 0) {
+      pl = S.vp + cy * 16;
+      st = 16;
+    } else {
+      pl = S.dp + cy * 17 + cx;
+      st = 17;
+    }
+    uint32_t s = 0;
+#pragma unroll
+    for (int r = r0; r < r0 + 8; r++) {
+      const int d = (int)pl[r * st + c] - (int)src[r * 16 + c];
+      s += (uint32_t)(d < 0 ? -d : d);
+    }
+    s = __reduce_add_sync(FULL, s);
+    vp8a_mv cand;
+    cand.row = (int16_t)(center.row + 2 * dy);
+    cand.col = (int16_t)(center.col + 2 * dx);
+    if (s < best_sad) {
+      best_sad = s;
+      best = cand;
+    }
+  }
+  out->mv = best;
+  out->sad = best_sad;
+  return true;
 }
 
 }  // namespace vp8a_dev
