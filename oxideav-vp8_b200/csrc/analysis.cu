@@ -27,6 +27,8 @@
 // parallel across lanes). The f64 RD decision runs on one thread with the
 // reference's operation order; the library is built with -fmad=false so no
 // multiply-add is fused.
+#include <cstddef>
+
 #include "census.cuh"
 
 namespace {
@@ -67,12 +69,13 @@ constexpr int HS = 24;        // halo stride
 constexpr int MAX_BLOCKS = 9; // zero + 4 left + 4 above offsets
 constexpr int CMAX = 25;      // SPLITMV candidate vectors per partition
 
-struct RefSmem {
+struct __align__(16) RefSmem {
   WarpScratch ws;                       // window + six-tap scratch + half planes
-  uint8_t halo_nearest[21 * HS + 8];
-  uint8_t halo_near[21 * HS + 8];
-  uint8_t blocks[MAX_BLOCKS][256];
+  uint8_t halo_nearest[21 * HS + 8];    // 512
+  uint8_t halo_near[21 * HS + 8];       // 512
+  uint8_t blocks[MAX_BLOCKS][256];      // read as 32-bit words (sad_block16)
 };
+static_assert(sizeof(RefSmem) % 16 == 0 && offsetof(RefSmem, blocks) % 16 == 0, "RefSmem alignment");
 
 struct MainOut {
   uint32_t sad_zero, sad_nearest, sad_near;

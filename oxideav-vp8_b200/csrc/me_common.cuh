@@ -27,15 +27,18 @@ struct MePlane {
   int height;
 };
 
-struct WarpScratch {
-  uint8_t win[WIN_BYTES];
-  uint8_t temp[21 * 16 + 16];
-  uint8_t halo[21 * 24 + 16];
+// Every member is a multiple of 16 bytes and the struct is 16-byte aligned,
+// so arrays of it (and structs embedding it) keep word access aligned.
+struct __align__(16) WarpScratch {
+  uint8_t win[WIN_BYTES];        // 1616
+  uint8_t temp[21 * 16 + 16];    // 352
+  uint8_t halo[21 * 24 + 24];    // 528
   // Half-pel planes around a whole-pel centre: H 22x17, V 17x16, D 17x17.
-  uint8_t hp[22 * 17 + 4];
-  uint8_t vp[17 * 16 + 4];
-  uint8_t dp[17 * 17 + 4];
+  uint8_t hp[22 * 17 + 10];      // 384
+  uint8_t vp[17 * 16 + 16];      // 288
+  uint8_t dp[17 * 17 + 15];      // 304
 };
+static_assert(sizeof(WarpScratch) % 16 == 0, "WarpScratch must keep 16-byte multiples");
 
 __device__ __forceinline__ int16_t clamp_component(int v) { return (int16_t)clampi(v, -1023, 1023); }
 __device__ __forceinline__ int16_t snap_whole(int v) { return (int16_t)((v / 4) * 4); }
@@ -262,20 +265,20 @@ __device__ __forceinline__ vp8a_search_result refine(const MePlane& P, WarpScrat
   return res;
 }
 
-// half_pixel_refine_luma around a whole-pel centre whose neighbourhood
-// the window covers. The eight half-pel candidates share three planes —
-// horizontal (H), vertical (V) and horizontal-then-vertical (D) half-pel
-// samples — so each six-tap output is computed once per MB instead of once
-// per candidate; every candidate's prediction is a 16x16 sub-block of one
-// plane, byte-identical to its own two-pass synthesis (same taps, same
-// 8-bit intermediate, same edge-clamped source). Returns false when the
-// window does not cover the planes (the caller then uses refine()).
-__device__ __forceinline__ bool half_refine_planes(WarpScratch& S, int wx0, int wy0, int mbx, int mby,
-                                                   vp8a_mv center, const uint8_t* src, int lane,
-                                                   vp8a_search_result* out) {
-  if ((center.row & 3) || (center.col & 3) || center.row < -1020 || center.row > 1020 || center.col < -1020 ||
-      center.col > 1020)
-    return false;
+// The eight half-pel candidates around a whole-pel centre share three
+// planes — horizontal (H), vertical (V) and horizontal-then-vertical (D)
+// half-pel samples — so each six-tap output is computed once per MB instead
+// of once per candidate; every candidate's prediction is a 16x16 sub-block
+// of one plane, byte-identical to its own two-pass synthesis (same taps,
+// same 8-bit intermediate, same edge-clamped source). half_plane_sads fills
+// sads[k] for the offsets (row, col) = (-1,-1) (-1,0) (-1,1) (0,-1) (0,1)
+// (1,-1) (1,0) (1,1) half-pels, in that order (the order of
+// half_pixel_refine_luma, src/motion_search.rs:589-598, and of
+// sub_pixel_refine, src/encoder/inter_search.rs:520-535), and returns false
+// when the window does not cover the planes.
+__device__ __forceinline__ bool half_plane_sads(WarpScratch& S, int wx0, int wy0, int mbx, int mby, vp8a_mv center,
+                                                const uint8_t* src, int lane, uint32_t* sads) {
+  if ((center.row & 3) || (center.col & 3)) return false;
   const int bx = mbx + center.col / 4 - wx0, by = mby + center.row / 4 - wy0;  // block origin in window
   if (bx < 3 || by < 3 || bx + 19 > WS || by + 19 > WS) return false;
   const int* f = c_sixtap[4];
@@ -299,10 +302,6 @@ __device__ __forceinline__ bool half_refine_planes(WarpScratch& S, int wx0, int 
     S.dp[o] = (uint8_t)interp6(f, p[0], p[17], p[34], p[51], p[68], p[85]);
   }
   __syncwarp();
-  // Centre SAD (whole pel, the copy path) and the eight candidates in the
-  // reference's order (-1,-1) (-1,0) (-1,1) (0,-1) (0,1) (1,-1) (1,0) (1,1).
-  vp8a_mv best = center;
-  uint32_t best_sad = sad_win16(S.win, bx, by, src, lane);
   const int c = lane & 15, r0 = (lane >> 4) * 8;
 #pragma unroll 1
   for (int k = 0; k < 8; k++) {
@@ -327,13 +326,31 @@ __device__ __forceinline__ bool half_refine_planes(WarpScratch& S, int wx0, int 
       const int d = (int)pl[r * st + c] - (int)src[r * 16 + c];
       s += (uint32_t)(d < 0 ? -d : d);
     }
-    s = __reduce_add_sync(FULL, s);
-    vp8a_mv cand;
-    cand.row = (int16_t)(center.row + 2 * dy);
-    cand.col = (int16_t)(center.col + 2 * dx);
-    if (s < best_sad) {
-      best_sad = s;
-      best = cand;
+    sads[k] = __reduce_add_sync(FULL, s);
+  }
+  return true;
+}
+
+// half_pixel_refine_luma (src/motion_search.rs:564-627) over the shared
+// planes; for a whole-pel centre inside [-1020, 1020] no candidate is
+// clamped or collapses, so the reference walk is the first strict minimum.
+__device__ __forceinline__ bool half_refine_planes(WarpScratch& S, int wx0, int wy0, int mbx, int mby,
+                                                   vp8a_mv center, const uint8_t* src, int lane,
+                                                   vp8a_search_result* out) {
+  if (center.row < -1020 || center.row > 1020 || center.col < -1020 || center.col > 1020) return false;
+  uint32_t sads[8];
+  if (!half_plane_sads(S, wx0, wy0, mbx, mby, center, src, lane, sads)) return false;
+  const int bx = mbx + center.col / 4 - wx0, by = mby + center.row / 4 - wy0;
+  vp8a_mv best = center;
+  uint32_t best_sad = sad_win16(S.win, bx, by, src, lane);
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const int dy = (k < 3) ? -1 : (k < 5 ? 0 : 1);
+    const int dx = (k == 0 || k == 3 || k == 5) ? -1 : ((k == 1 || k == 6) ? 0 : 1);
+    if (sads[k] < best_sad) {
+      best_sad = sads[k];
+      best.row = (int16_t)(center.row + 2 * dy);
+      best.col = (int16_t)(center.col + 2 * dx);
     }
   }
   out->mv = best;

@@ -15,6 +15,8 @@ from .api import (
     lf_info_from_decisions,
     mb_luma_sad_at_mv,
     motion_descent,
+    neighbours_from_decisions,
+    rd_inter_search,
     quarter_pixel_refine_luma,
     rd_lambda,
     reconstruction_ssd,
@@ -40,6 +42,8 @@ __all__ = [
     "half_pixel_refine_luma",
     "lf_info_from_decisions",
     "mb_luma_sad_at_mv",
+    "neighbours_from_decisions",
+    "rd_inter_search",
     "motion_descent",
     "quarter_pixel_refine_luma",
     "rd_lambda",

@@ -151,6 +151,45 @@ def analyse_inter_frame(ctx, frame, refs, ref_ids, lam, mv_contexts=None, trace=
     return dec
 
 
+def rd_inter_search(ctx, frame, refs, ref_ids, lam, y1_ac, effort, neighbours, mv_contexts=None):
+    """decide_mb_rd's inter search (src/encoder/inter_search.rs:846-1060)
+    for every MB given its census neighbours (3 vp8a_mb_info records per MB:
+    above, left, above-left). Returns a (mb_rows, mb_cols) RD_INTER_DTYPE
+    array."""
+    f = i420(*frame)
+    prs = [planes(*p) for p in refs]
+    parr = (abi.Planes * len(prs))(*prs)
+    ids = np.ascontiguousarray(np.asarray(ref_ids, np.uint8))
+    nb = np.ascontiguousarray(neighbours, abi.MB_INFO_DTYPE)
+    mbr, mbc = (f.height + 15) // 16, (f.width + 15) // 16
+    out = np.zeros(mbr * mbc, abi.RD_INTER_DTYPE)
+    ctxs = mv_contexts if mv_contexts is not None else abi.default_mv_contexts()
+    check(ctx._lib.vp8a_rd_inter_search(ctx.handle, C.byref(f), C.cast(parr, C.c_void_p), ptr(ids), len(prs),
+                                        C.byref(ctxs), lam, y1_ac, effort, ptr(nb), ptr(out)), "vp8a_rd_inter_search")
+    return out.reshape(mbr, mbc)
+
+
+def neighbours_from_decisions(dec):
+    """The (above, left, above-left) census records of every MB, built from
+    a frame's decisions the way analyse_row forwards them
+    (src/encoder/inter.rs:458-480); border slots are intra records."""
+    d = np.asarray(dec)
+    mbr, mbc = d.shape
+    info = np.zeros((mbr + 1, mbc + 1), abi.MB_INFO_DTYPE)
+    inner = info[1:, 1:]
+    inner["ref_frame"] = d["ref_frame"]
+    inner["mv"] = d["mv"]
+    split = d["mode"] == abi.MODE_SPLIT
+    inner["is_split"] = split
+    inner["has_split_mvs"] = split
+    inner["split_mvs"] = np.where(split[..., None], d["split_mvs"], np.zeros_like(d["split_mvs"]))
+    nb = np.zeros((mbr, mbc, 3), abi.MB_INFO_DTYPE)
+    nb[:, :, 0] = info[:-1, 1:]
+    nb[:, :, 1] = info[1:, :-1]
+    nb[:, :, 2] = info[:-1, :-1]
+    return np.ascontiguousarray(nb.reshape(-1))
+
+
 def build_arnr_altref(ctx, frames, center, strength=3):
     """build_arnr_altref (src/arnr.rs:476). `frames` = list of (y, u, v).
     Returns the packed (y, u, v) anchor."""
