@@ -325,6 +325,7 @@ def gpu_arm(args):
     barrier()
     launches = ctx.launches - launches0
     ms = float(np.sum(times))
+    step_ms = [round(x, 3) for x in times]
     # Per-kernel-stage timing for the roofline (separate, after the timed run).
     stage = stage_times(gs, stream, torch, flush)
     # End-to-end through host buffers.
@@ -389,8 +390,11 @@ def gpu_arm(args):
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6.65 TB/s",
                          "stage_ms": {k: round(v["ms"], 4) for k, v in stage.items()},
+                         "stage_reps_ms": {k: v["reps"] for k, v in stage.items()},
                          "stage_alg_bytes": {k: int(v["bytes"]) for k, v in stage.items()}},
             "gpu_launches": int(launches),
+            "step_ms": step_ms,
+            "e2e_step_ms": [round(x, 3) for x in e_times],
             "clocks": clk.summary(),
         }
         if args.gpus == 1 and world == 1 and not args.no_cpu_baseline:
@@ -427,7 +431,7 @@ def stage_times(gs, stream, torch, flush, reps=3):
             e.record(stream)
             e.synchronize()
             ts.append(s.elapsed_time(e))
-        out[name] = {"ms": float(np.mean(ts)), "bytes": nbytes}
+        out[name] = {"ms": float(np.median(ts)), "bytes": nbytes, "reps": [round(x, 3) for x in ts]}
     return out
 
 
@@ -508,6 +512,38 @@ def reference_arm(args):
     }
 
 
+def case_arm(args):
+    """One stage alone on a WxH frame, for profiling captures: runs
+    `--warmup` + `--steps` calls of the stage and prints its mean device ms."""
+    import torch
+
+    import vp8a
+    from vp8a import synth
+
+    w, h = (int(v) for v in args.size.split("x"))
+    global W, H, MB_COLS, MB_ROWS, N_MB
+    W, H = w, h
+    MB_COLS, MB_ROWS = (w + 15) // 16, (h + 15) // 16
+    N_MB = MB_COLS * MB_ROWS
+    ctx = vp8a.Context(0)
+    frames, _ = synth.make_sequence(w, h, 16, SEED, pieces=4, occluders=4)
+    gs = GpuStep(ctx, frames, vp8a.load(), torch, 0)
+    fn = {"arnr": gs.run_arnr, "analysis": gs.run_analysis, "lf": gs.run_lf}[args.case]
+    for _ in range(args.warmup):
+        fn()
+    ctx.synchronize()
+    ts = []
+    for _ in range(args.steps):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(gs.stream)
+        fn()
+        e.record(gs.stream)
+        e.synchronize()
+        ts.append(s.elapsed_time(e))
+    ctx.close()
+    return {"case": args.case, "size": args.size, "ms": [round(x, 4) for x in ts]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -516,10 +552,15 @@ def main():
     ap.add_argument("--impl", default="vp8a", choices=["vp8a", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--case", choices=["arnr", "analysis", "lf"], help="profile one stage alone")
+    ap.add_argument("--size", default="1920x1080", help="frame size for --case")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl != "reference":
         log("note: fewer than 3 warm-up steps")
-    res = reference_arm(args) if args.impl == "reference" else gpu_arm(args)
+    if args.case:
+        res = case_arm(args)
+    else:
+        res = reference_arm(args) if args.impl == "reference" else gpu_arm(args)
     if res is not None:
         print(json.dumps(res), flush=True)
 

@@ -203,6 +203,17 @@ vp8a_status vp8a_ctx_create(int device, vp8a_ctx** out) {
     return cuda_fail(pe, "cudaGetDeviceProperties");
   }
   c->sm_count = prop.multiProcessorCount;
+  // Keep freed stream-ordered staging memory in the device pool instead of
+  // returning it to the driver at every synchronisation, so per-call
+  // staging allocations stay cheap.
+  {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t keep = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+  }
   cudaError_t se = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (se != cudaSuccess) {
     delete c;
