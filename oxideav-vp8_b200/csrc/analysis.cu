@@ -49,6 +49,7 @@ struct AnArgs {
   vp8a_mv_contexts ctx;
   double lambda;
   const double* bit_cost;
+  const double* mvbits;  // mv_component_bits per context and value (2 x 2047)
   MbInfoDev* infos;
   unsigned* progress;
   unsigned* status;
@@ -89,14 +90,16 @@ struct SplitOut {
   int valid;
 };
 
+// SPLITMV scratch of one warp. Candidate column layout (fixed, no
+// de-duplication): 0 = ZERO, 1..4 = LEFT vectors of the MB's left column
+// anchors 0/4/8/12, 5..8 = ABOVE vectors of the top-row anchors 0..3,
+// 9..24 = the NEW4X4 result of group 0..15.
 struct SplitScratch {
-  uint32_t table[16 * CMAX];  // group SAD per candidate vector
-  int16_t cox[CMAX], coy[CMAX];
+  uint32_t table[16 * CMAX];  // group g's SAD at column m: table[g * CMAX + m]
   vp8a_mv cmv[CMAX];
-  vp8a_mv split[16];
-  int nc;
+  uint32_t new_sad[16];
+  uint8_t chosen[16];         // column each group chose
 };
-
 struct Plan {
   int wx0, wy0;        // window origin (plane pixels)
   int hn_x, hn_y;      // NEAREST halo origin
@@ -175,37 +178,58 @@ __device__ void stage(const AnArgs& a, RefSmem* rs, const Plan& pl, int mbx, int
 
 // -------------------------------------------------------------- SPLITMV
 
-// This lane's 8 pixels of its group rectangle as (row, col) runs: groups
-// have 8*L pixels for L lanes per group, so each lane owns 8.
+// Columns of the candidate table each partition needs (see SplitScratch):
+// ZERO, the LEFT/ABOVE vectors of its left-column / top-row anchors, and
+// its groups' NEW results.
+__constant__ uint32_t c_need_cols[4] = {
+    (1u << 0) | (1u << 1) | (1u << 3) | (1u << 5) | (0x3u << 9),   // TopBottom: anchors 0, 8
+    (1u << 0) | (1u << 1) | (1u << 5) | (1u << 7) | (0x3u << 9),   // LeftRight: anchors 0, 2
+    (1u << 0) | (1u << 1) | (1u << 3) | (1u << 5) | (1u << 7) | (0xfu << 9),  // Quarters: 0, 2, 8, 10
+    0x1ffffffu};                                                   // Mv16: every column
+
+// Unaligned 4-byte read from shared memory.
+__device__ __forceinline__ uint32_t load4u(const uint8_t* p) {
+  uintptr_t a = (uintptr_t)p;
+  const uint32_t* w = (const uint32_t*)(a & ~(uintptr_t)3);
+  return __funnelshift_r(w[0], w[1], (unsigned)(a & 3) * 8u);
+}
+
+// This lane's 8 pixels of its group: one run of 8 (groups 8 or 16 wide) or
+// two rows of 4 (4x4 groups). off0/off1 are (row*stride + col) with the
+// row/col in MB coordinates.
 struct LanePix {
-  int r0, c0, r1, c1, n0;  // two runs; n0 = pixels in the first run (8 or 4)
+  int r0, c0, r1, c1;
+  bool wide;
+  uint32_t s0, s1;  // the source bytes as two little-endian words
 };
 
-__device__ __forceinline__ LanePix lane_pixels(int row0, int col0, int gw, int s) {
+__device__ __forceinline__ LanePix lane_pixels(int row0, int col0, int gw, int s, const uint8_t* src) {
   LanePix p;
   if (gw == 16) {
     p.r0 = row0 + (s >> 1);
     p.c0 = col0 + (s & 1) * 8;
-    p.n0 = 8;
+    p.wide = true;
   } else if (gw == 8) {
     p.r0 = row0 + s;
     p.c0 = col0;
-    p.n0 = 8;
+    p.wide = true;
   } else {
     p.r0 = row0 + 2 * s;
     p.c0 = col0;
-    p.n0 = 4;
+    p.wide = false;
   }
-  p.r1 = p.r0 + 1;
-  p.c1 = p.c0;
+  p.r1 = p.wide ? p.r0 : p.r0 + 1;
+  p.c1 = p.wide ? p.c0 + 4 : p.c0;
+  p.s0 = *(const uint32_t*)(src + p.r0 * 16 + p.c0);
+  p.s1 = *(const uint32_t*)(src + p.r1 * 16 + p.c1);
   return p;
 }
 
-// Partial group SAD of this lane's pixels for the MB-extent block whose
-// top-left is plane pixel (bx, by): from the window, a staged block, or
-// clamped global loads.
+// Partial SAD of this lane's pixels for the MB-extent block whose top-left
+// is plane pixel (bx, by): from the window, a staged block, or clamped
+// global loads.
 __device__ __forceinline__ uint32_t lane_gsad(const MePlane& P, const RefSmem& R, const Plan& pl, int mbx, int mby,
-                                              const uint8_t* src, const LanePix& q, int bx, int by) {
+                                              const LanePix& q, int bx, int by) {
   const int lx = bx - pl.wx0, ly = by - pl.wy0;
   const uint8_t* base = nullptr;
   int st = 0;
@@ -220,24 +244,23 @@ __device__ __forceinline__ uint32_t lane_gsad(const MePlane& P, const RefSmem& R
         break;
       }
   }
-  uint32_t s = 0;
+  uint32_t r0, r1;
   if (base) {
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-      const int rr = i < q.n0 ? q.r0 : q.r1, cc = i < q.n0 ? q.c0 + i : q.c1 + i - q.n0;
-      const int d = (int)src[rr * 16 + cc] - (int)base[rr * st + cc];
-      s += (uint32_t)(d < 0 ? -d : d);
-    }
+    r0 = load4u(base + q.r0 * st + q.c0);
+    r1 = load4u(base + q.r1 * st + q.c1);
   } else {
+    r0 = r1 = 0;
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-      const int rr = i < q.n0 ? q.r0 : q.r1, cc = i < q.n0 ? q.c0 + i : q.c1 + i - q.n0;
-      const int ref = P.plane[(size_t)clampi(by + rr, 0, P.height - 1) * P.stride + clampi(bx + cc, 0, P.width - 1)];
-      const int d = (int)src[rr * 16 + cc] - ref;
-      s += (uint32_t)(d < 0 ? -d : d);
+    for (int i = 0; i < 4; i++) {
+      const uint32_t b0 =
+          P.plane[(size_t)clampi(by + q.r0, 0, P.height - 1) * P.stride + clampi(bx + q.c0 + i, 0, P.width - 1)];
+      const uint32_t b1 =
+          P.plane[(size_t)clampi(by + q.r1, 0, P.height - 1) * P.stride + clampi(bx + q.c1 + i, 0, P.width - 1)];
+      r0 |= b0 << (8 * i);
+      r1 |= b1 << (8 * i);
     }
   }
-  return s;
+  return __vsadu4(r0, q.s0) + __vsadu4(r1, q.s1);
 }
 
 __device__ __forceinline__ uint32_t group_reduce(uint32_t v, int L) {
@@ -275,14 +298,13 @@ __device__ void split_partition(const AnArgs& a, const double* t, const MePlane&
   const int G = pid == 3 ? 16 : (pid == 2 ? 4 : 2);
   const int L = 32 / G, g = lane / L, s = lane - g * L;
   const int row0 = c_geom[pid][g][0], col0 = c_geom[pid][g][1], gw = c_geom[pid][g][2];
-  const LanePix q = lane_pixels(row0, col0, gw, s);
+  const LanePix q = lane_pixels(row0, col0, gw, s, src);
   // group_small_diamond_search (src/encoder.rs:7812-7879) for every group
   // at once: snap then clamp the centre; N, S, W, E clamped, not snapped.
   vp8a_mv best;
   best.row = (int16_t)clampi((bp.row / 4) * 4, -1023, 1023);
   best.col = (int16_t)clampi((bp.col / 4) * 4, -1023, 1023);
-  uint32_t bs =
-      group_reduce(lane_gsad(P, R, pl, mbx, mby, src, q, mbx + int_off(best.col), mby + int_off(best.row)), L);
+  uint32_t bs = group_reduce(lane_gsad(P, R, pl, mbx, mby, q, mbx + int_off(best.col), mby + int_off(best.row)), L);
   bool active = true;
   for (int it = 0; it < 4; it++) {
     bool improved = false;
@@ -293,7 +315,7 @@ __device__ void split_partition(const AnArgs& a, const double* t, const MePlane&
       c.row = (int16_t)clampi(best.row + dr[d], -1023, 1023);
       c.col = (int16_t)clampi(best.col + dc[d], -1023, 1023);
       const uint32_t sv =
-          group_reduce(lane_gsad(P, R, pl, mbx, mby, src, q, mbx + int_off(c.col), mby + int_off(c.row)), L);
+          group_reduce(lane_gsad(P, R, pl, mbx, mby, q, mbx + int_off(c.col), mby + int_off(c.row)), L);
       if (active && !mv_eq(c, best) && sv < bs) {
         bs = sv;
         best = c;
@@ -302,122 +324,86 @@ __device__ void split_partition(const AnArgs& a, const double* t, const MePlane&
     }
     if (!improved) active = false;
   }
-  // Candidate vectors (unique integer offsets): ZERO, external LEFT/ABOVE,
-  // then every group's NEW result.
-  if (lane == 0) W.nc = 0;
+  // Candidate columns.
+  if (s == 0) {
+    W.cmv[9 + g] = best;
+    W.new_sad[g] = bs;
+  }
+  if (lane == 0) {
+    W.cmv[0] = vp8a_mv{0, 0};
+    for (int k = 0; k < 4; k++) W.cmv[1 + k] = ext_left(left, 4 * k);
+    for (int k = 0; k < 4; k++) W.cmv[5 + k] = ext_above(above, k);
+  }
   __syncwarp();
-  auto add = [&](vp8a_mv m) {
-    const int ox = int_off(m.col), oy = int_off(m.row);
-    for (int i = 0; i < W.nc; i++)
-      if (W.cox[i] == ox && W.coy[i] == oy) return;
-    const int n = W.nc;
-    __syncwarp();
-    if (lane == 0) {
-      W.cox[n] = (int16_t)ox;
-      W.coy[n] = (int16_t)oy;
-      W.cmv[n] = m;
-      W.nc = n + 1;
-    }
-    __syncwarp();
-  };
-  add(vp8a_mv{0, 0});
-  for (int gg = 0; gg < G; gg++) {
-    const int anc = c_geom[pid][gg][4];
-    if ((anc & 3) == 0) add(ext_left(left, anc));
-    if (anc < 4) add(ext_above(above, anc));
-  }
-  for (int gg = 0; gg < G; gg++) {
-    vp8a_mv m;
-    m.row = (int16_t)__shfl_sync(FULL, (int)best.row, gg * L);
-    m.col = (int16_t)__shfl_sync(FULL, (int)best.col, gg * L);
-    add(m);
-  }
-  const int nc = W.nc;
-  for (int m = 0; m < nc; m++) {
-    const uint32_t sv = group_reduce(lane_gsad(P, R, pl, mbx, mby, src, q, mbx + W.cox[m], mby + W.coy[m]), L);
+  const uint32_t need = c_need_cols[pid];
+  for (int m = 0; m < CMAX; m++) {
+    if (!((need >> m) & 1u)) continue;
+    const vp8a_mv mv = W.cmv[m];
+    const uint32_t sv = group_reduce(lane_gsad(P, R, pl, mbx, mby, q, mbx + int_off(mv.col), mby + int_off(mv.row)), L);
     if (s == 0) W.table[g * CMAX + m] = sv;
   }
-  // NEW4X4 results per group.
-  if (s == 0) W.split[g] = best;  // temporary: group g's NEW vector
   __syncwarp();
-  vp8a_mv news[16];
-  uint32_t new_sad[16];
-  for (int gg = 0; gg < G; gg++) {
-    news[gg] = W.split[gg];
-    new_sad[gg] = (uint32_t)__shfl_sync(FULL, (int)bs, gg * L);
-  }
-  __syncwarp();
-  // The sequential sub-MV choice (uniform on every lane).
-  vp8a_mv split[16];
-  for (int i = 0; i < 16; i++) split[i] = vp8a_mv{0, 0};
-  uint8_t modes[16];
-  for (int i = 0; i < 16; i++) modes[i] = VP8A_SUBMV_ZERO;
-  auto lookup = [&](int gg, vp8a_mv m) -> uint32_t {
-    const int ox = int_off(m.col), oy = int_off(m.row);
-    for (int i = 0; i < nc; i++)
-      if (W.cox[i] == ox && W.coy[i] == oy) return W.table[gg * CMAX + i];
-    return 0xffffffffu;  // unreachable: every candidate vector is tabled
-  };
+  // The sequential sub-MV choice (uniform on every lane; lane 0 records).
   uint32_t total_sad = 0;
   double total_bits = 0.0;
   for (int gg = 0; gg < G; gg++) {
     const int anchor = c_geom[pid][gg][4];
-    const vp8a_mv lmv = (anchor & 3) == 0 ? ext_left(left, anchor) : split[anchor - 1];
-    const vp8a_mv amv = anchor < 4 ? ext_above(above, anchor) : split[anchor - 4];
+    const int lidx = (anchor & 3) == 0 ? 1 + (anchor >> 2) : W.chosen[c_partitions[pid][anchor - 1]];
+    const int aidx = anchor < 4 ? 5 + anchor : W.chosen[c_partitions[pid][anchor - 4]];
+    const vp8a_mv lmv = W.cmv[lidx], amv = W.cmv[aidx];
     const bool lez = mv_zero(lmv), aez = mv_zero(amv), lea = mv_eq(lmv, amv);
     const int ctxi = (lea && lez) ? 4 : (lea ? 3 : (aez ? 2 : (lez ? 1 : 0)));
     const uint8_t* probs = c_submv_probs[ctxi];
-    int best_mode = VP8A_SUBMV_ZERO;
-    vp8a_mv best_mv = {0, 0}, best_diff = {0, 0};
+    const uint32_t* trow = W.table + gg * CMAX;
+    int best_mode = VP8A_SUBMV_ZERO, best_col = 0;
+    int diff_r = 0, diff_c = 0;
     double best_j = __longlong_as_double(0x7ff0000000000000LL);
-    const vp8a_mv cm[3] = {lmv, amv, vp8a_mv{0, 0}};
+    const int cols[3] = {lidx, aidx, 0};
     for (int m = 0; m < 3; m++) {
-      const double sad = (double)lookup(gg, cm[m]);
+      const double sad = (double)trow[cols[m]];
       const double mode_bits = submv_ref_bits(t, probs, m);
       const double j = sad + a.lambda * (mode_bits + 0.0);
       if (j < best_j) {
         best_j = j;
         best_mode = m;
-        best_mv = cm[m];
-        best_diff = vp8a_mv{0, 0};
+        best_col = cols[m];
       }
     }
-    const vp8a_mv nm = news[gg];
+    const vp8a_mv nm = W.cmv[9 + gg];
     const int dr = (int)nm.row - bp.row, dc = (int)nm.col - bp.col;
     if (dr >= -1023 && dr <= 1023 && dc >= -1023 && dc <= 1023) {
-      const double diff_bits = mv_component_bits(t, a.ctx.p[0], dr) + mv_component_bits(t, a.ctx.p[1], dc);
+      const double diff_bits = mv_bits_lookup(a.mvbits, 0, dr) + mv_bits_lookup(a.mvbits, 1, dc);
       const double mode_bits = submv_ref_bits(t, probs, VP8A_SUBMV_NEW);
-      const double j = (double)new_sad[gg] + a.lambda * (mode_bits + diff_bits);
+      const double j = (double)W.new_sad[gg] + a.lambda * (mode_bits + diff_bits);
       if (j < best_j) {
         best_j = j;
         best_mode = VP8A_SUBMV_NEW;
-        best_mv = nm;
-        best_diff.row = (int16_t)dr;
-        best_diff.col = (int16_t)dc;
+        best_col = 9 + gg;
+        diff_r = dr;
+        diff_c = dc;
       }
     }
     if (!isfinite(best_j)) {
       if (lane == 0) out->valid = 0;
       return;
     }
-    const uint32_t gs = lookup(gg, best_mv);
-    for (int b = 0; b < 16; b++)
-      if (c_partitions[pid][b] == gg) split[b] = best_mv;
-    total_sad += gs;
+    total_sad += trow[best_col];
     total_bits += submv_ref_bits(t, probs, best_mode);
-    if (best_mode == VP8A_SUBMV_NEW)
-      total_bits += mv_component_bits(t, a.ctx.p[0], best_diff.row) + mv_component_bits(t, a.ctx.p[1], best_diff.col);
-    modes[gg] = (uint8_t)best_mode;
+    if (best_mode == VP8A_SUBMV_NEW) total_bits += mv_bits_lookup(a.mvbits, 0, diff_r) + mv_bits_lookup(a.mvbits, 1, diff_c);
+    __syncwarp();
+    if (lane == 0) {
+      W.chosen[gg] = (uint8_t)best_col;
+      out->modes[gg] = (uint8_t)best_mode;
+    }
+    __syncwarp();
   }
   const double partition_bits = mv_partition_bits(t, pid);
   if (lane == 0) {
     out->j = (double)total_sad + a.lambda * (partition_bits + total_bits);
-    for (int i = 0; i < 16; i++) {
-      out->split_mvs[i] = split[i];
-      out->modes[i] = modes[i];
-    }
+    for (int i = G; i < 16; i++) out->modes[i] = VP8A_SUBMV_ZERO;
     out->valid = 1;
   }
+  if (lane < 16) out->split_mvs[lane] = W.cmv[W.chosen[c_partitions[pid][lane]]];
 }
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
@@ -555,7 +541,7 @@ __global__ void __launch_bounds__(MAX_REFS* WARPS_PER_REF * 32) analysis_kernel(
           const double bits_new = bb(t, p[0], 1) + bb(t, p[1], 1) + bb(t, p[2], 1) + bb(t, p[3], 0);
           const int dr = (int)m.quarter.mv.row - bp.row, dc = (int)m.quarter.mv.col - bp.col;
           const bool in_range = dr >= -1023 && dr <= 1023 && dc >= -1023 && dc <= 1023;
-          const double bits_mv = in_range ? mv_component_bits(t, a.ctx.p[0], dr) + mv_component_bits(t, a.ctx.p[1], dc)
+          const double bits_mv = in_range ? mv_bits_lookup(a.mvbits, 0, dr) + mv_bits_lookup(a.mvbits, 1, dc)
                                           : __longlong_as_double(0x7ff0000000000000LL);
           const double j_zero = (double)m.sad_zero + lambda * bits_zero;
           const double j_nearest = (double)m.sad_nearest + lambda * bits_nearest;
@@ -733,7 +719,13 @@ extern "C" vp8a_status vp8a_analyse_inter_frame(vp8a_ctx* ctx, const vp8a_i420* 
   a.lambda = lambda;
   a.bit_cost = ctx->d_bit_cost;
   const size_t nmb = (size_t)mb_cols * mb_rows;
-  void *dinfo, *dprog, *ddec, *dtr = nullptr;
+  void *dinfo, *dprog, *ddec, *dtr = nullptr, *dmvb;
+  if ((s = st.scratch(sizeof(double) * 2 * MV_BITS_SPAN, &dmvb)) != VP8A_OK) return s;
+  mv_bits_table_kernel<<<(2 * MV_BITS_SPAN + 255) / 256, 256, 0, ctx->stream>>>(ctx->d_bit_cost, a.ctx,
+                                                                               (double*)dmvb);
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
+  a.mvbits = (const double*)dmvb;
   if ((s = st.scratch(sizeof(MbInfoDev) * nmb, &dinfo)) != VP8A_OK) return s;
   if ((s = st.scratch(sizeof(unsigned) * mb_rows, &dprog)) != VP8A_OK) return s;
   VP8A_CUDA(cudaMemsetAsync(dprog, 0, sizeof(unsigned) * mb_rows, ctx->stream));

@@ -72,6 +72,23 @@ static __device__ double mv_component_bits(const double* t, const uint8_t* p, in
   return bits;
 }
 
+// mv_component_bits of both components for every value -1023..1023,
+// written to out[k * 2047 + value + 1023]: the searches read the table
+// instead of walking the tree per candidate. The entries come from the
+// same device function, so they are bit-identical.
+constexpr int MV_BITS_SPAN = 2047;
+static __global__ void mv_bits_table_kernel(const double* t, vp8a_mv_contexts ctx, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 2 * MV_BITS_SPAN) return;
+  const int k = i >= MV_BITS_SPAN, v = i - k * MV_BITS_SPAN - 1023;
+  out[i] = mv_component_bits(t, ctx.p[k], v);
+}
+
+// Table lookup; value must lie in -1023..1023.
+static __device__ __forceinline__ double mv_bits_lookup(const double* tab, int k, int v) {
+  return __ldg(tab + k * MV_BITS_SPAN + v + 1023);
+}
+
 struct Census {
   vp8a_mv best_predictor, nearest, near_;
   uint8_t p[4];

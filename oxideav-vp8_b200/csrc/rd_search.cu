@@ -51,6 +51,7 @@ struct RdArgs {
   uint32_t good_enough;
   Shape shape;
   const double* bit_cost;
+  const double* mvbits;  // mv_component_bits per context and value (2 x 2047)
   const MbInfoDev* nb;
   vp8a_rd_inter* out;
 };
@@ -68,11 +69,10 @@ struct RdCensus {
 
 // MvCostTable::bits: f32 component costs summed in f32; false when the
 // differential leaves [-1023, 1023].
-__device__ __forceinline__ bool cost_bits(const double* t, const vp8a_mv_contexts& c, vp8a_mv mv, vp8a_mv base,
-                                          double* out) {
+__device__ __forceinline__ bool cost_bits(const double* mvb, vp8a_mv mv, vp8a_mv base, double* out) {
   const int dr = mv.row - base.row, dc = mv.col - base.col;
   if (dr < -1023 || dr > 1023 || dc < -1023 || dc > 1023) return false;
-  const float s = (float)mv_component_bits(t, c.p[0], dr) + (float)mv_component_bits(t, c.p[1], dc);
+  const float s = (float)mv_bits_lookup(mvb, 0, dr) + (float)mv_bits_lookup(mvb, 1, dc);
   *out = (double)s;
   return true;
 }
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(RD_WARPS * 32) rd_search_kernel(RdArgs a) {
       mv.row = (int16_t)(py * 4);
       mv.col = (int16_t)(px * 4);
       double bits;
-      if (!cost_bits(t, a.ctx, mv, cs.best, &bits)) return false;
+      if (!cost_bits(a.mvbits, mv, cs.best, &bits)) return false;
       const double rate = ls * bits;
       if (rate >= best.cost) return false;
       const uint32_t sad = whole_sad_g(P, ox + px, oy + py, src, lane);
@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(RD_WARPS * 32) rd_search_kernel(RdArgs a) {
         mv.col = (int16_t)(start.mv.col + 2 * dx);
         if (abs((int)mv.row) > 1020 || abs((int)mv.col) > 1020) continue;
         double bits;
-        if (cost_bits(t, a.ctx, mv, cs.best, &bits)) {
+        if (cost_bits(a.mvbits, mv, cs.best, &bits)) {
           const double cost = (double)hs[k] + ls * bits;
           if (cost < f.cost) f = Found{mv, hs[k], cost};
         }
@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(RD_WARPS * 32) rd_search_kernel(RdArgs a) {
           if (abs((int)mv.row) > 1022 || abs((int)mv.col) > 1022) continue;
           const uint32_t sad = sad_at_mv(P, S, wx0, wy0, ox, oy, mv.row, mv.col, src, lane);
           double bits;
-          if (cost_bits(t, a.ctx, mv, cs.best, &bits)) {
+          if (cost_bits(a.mvbits, mv, cs.best, &bits)) {
             const double cost = (double)sad + ls * bits;
             if (cost < f.cost) f = Found{mv, sad, cost};
           }
@@ -287,7 +287,7 @@ __global__ void __launch_bounds__(RD_WARPS * 32) rd_search_kernel(RdArgs a) {
       mode_bits = cs.mode_bits[2];
     } else {
       double diff = 0.0;
-      cost_bits(t, a.ctx, f.mv, cs.best, &diff);
+      cost_bits(a.mvbits, f.mv, cs.best, &diff);
       mode = VP8A_MODE_NEW;
       mode_bits = cs.mode_bits[3] + diff;
     }
@@ -392,9 +392,15 @@ extern "C" vp8a_status vp8a_rd_inter_search(vp8a_ctx* ctx, const vp8a_i420* fram
   const size_t nmb = (size_t)mb_cols * mb_rows;
   if ((s = st.in(neighbours, sizeof(vp8a_mb_info) * nmb * 3, &d)) != VP8A_OK) return s;
   a.nb = (const MbInfoDev*)d;
-  void* dout;
+  void *dout, *dmvb;
   if ((s = st.out(out, sizeof(vp8a_rd_inter) * nmb, &dout)) != VP8A_OK) return s;
   a.out = (vp8a_rd_inter*)dout;
+  if ((s = st.scratch(sizeof(double) * 2 * MV_BITS_SPAN, &dmvb)) != VP8A_OK) return s;
+  mv_bits_table_kernel<<<(2 * MV_BITS_SPAN + 255) / 256, 256, 0, ctx->stream>>>(ctx->d_bit_cost, a.ctx,
+                                                                               (double*)dmvb);
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
+  a.mvbits = (const double*)dmvb;
   rd_search_kernel<<<vp8a::grid_for(nmb, RD_WARPS), RD_WARPS * 32, 0, ctx->stream>>>(a);
   VP8A_CUDA(cudaGetLastError());
   ctx->launches++;
