@@ -34,7 +34,9 @@
 namespace {
 using namespace vp8a_dev;
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int SLOT = 384;  // Y 256 + U 64 + V 64
+// An MB slot holds Y 16x16 + U 8x8 + V 8x8 = 384 bytes, padded to 400 so
+// that the slots of neighbouring rows start on different banks.
+constexpr int SLOT_STRIDE = 400;
 
 struct LfArgs {
   const uint8_t* y;
@@ -53,6 +55,11 @@ struct LfArgs {
   const int16_t* row_t0;   // per MB row: first step, -1 = row not scored
   const uint8_t* row_top;  // per MB row: has a top MB edge
   int steps;
+  const int32_t* sched_off;  // [steps + 1]: rows active at step t are
+  const uint16_t* sched_row; //   sched_row[sched_off[t] .. sched_off[t + 1])
+  int max_active;            // most rows active at one step
+  int recon_words;           // planes and strides allow 4-byte accesses
+  int source_words;
   uint64_t* ssd_out;  // [64 * 8], indexed level * 8 + sharpness
   uint8_t* oy;        // write-back planes (apply mode) or null
   uint8_t* ou;
@@ -194,12 +201,139 @@ __device__ __forceinline__ uint32_t pack4(const int* o) {
 }
 
 __device__ __forceinline__ uint8_t* slot_ptr(uint8_t* slots, int r, int c) {
-  return slots + ((size_t)r * 4 + (c & 3)) * SLOT;
+  return slots + ((size_t)r * 4 + (c & 3)) * SLOT_STRIDE;
 }
 
-// Filter MB (r, c) held in its slot; neighbours in their slots.
+// One half-warp handles one MB: lane l (0-15) owns luma row l and chroma
+// row l & 7 of U (l < 8) or V (l >= 8) for the vertical edges, then the
+// same-numbered columns for the horizontal edges, so luma and chroma run on
+// the same instructions.
+struct MbWords {
+  uint32_t y[4], c[2];
+};
+
+// This lane's 24 bytes of MB (r, c) of the unfiltered reconstruction.
+__device__ __forceinline__ MbWords fetch_recon(const LfArgs& a, int r, int c, int l) {
+  MbWords w;
+  const uint8_t* gy = a.y + (size_t)(r * 16 + l) * a.ys + (size_t)c * 16;
+  const uint8_t* gc = (l < 8 ? a.u : a.v) + (size_t)(r * 8 + (l & 7)) * a.cs + (size_t)c * 8;
+  if (a.recon_words) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) w.y[k] = ((const uint32_t*)gy)[k];
+    w.c[0] = ((const uint32_t*)gc)[0];
+    w.c[1] = ((const uint32_t*)gc)[1];
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      w.y[k] = (uint32_t)gy[4 * k] | ((uint32_t)gy[4 * k + 1] << 8) | ((uint32_t)gy[4 * k + 2] << 16) |
+               ((uint32_t)gy[4 * k + 3] << 24);
+#pragma unroll
+    for (int k = 0; k < 2; k++)
+      w.c[k] = (uint32_t)gc[4 * k] | ((uint32_t)gc[4 * k + 1] << 8) | ((uint32_t)gc[4 * k + 2] << 16) |
+               ((uint32_t)gc[4 * k + 3] << 24);
+  }
+  return w;
+}
+
+__device__ __forceinline__ void store_slot(uint8_t* s, const MbWords& w, int l) {
+  uint32_t* sy = (uint32_t*)(s + l * 16);
+#pragma unroll
+  for (int k = 0; k < 4; k++) sy[k] = w.y[k];
+  uint32_t* sc = (uint32_t*)(s + (l < 8 ? 256 : 320) + (l & 7) * 8);
+  sc[0] = w.c[0];
+  sc[1] = w.c[1];
+}
+
+// The source under this lane's rows of MB (r, c), restricted to the
+// visible window: bytes outside it read as 0 and their mask bytes are 0.
+struct SrcWords {
+  uint32_t y[4], c[2], my[4], mc[2];
+};
+
+__device__ __forceinline__ uint32_t vis_mask(int n, int k) {
+  const int v = n - 4 * k;
+  return v >= 4 ? 0xffffffffu : (v <= 0 ? 0u : (1u << (8 * v)) - 1u);
+}
+
+__device__ __forceinline__ SrcWords fetch_source(const LfArgs& a, int r, int c, int l) {
+  SrcWords w;
+  const int yy = r * 16 + l, x0 = c * 16;
+  const int ny = yy < a.height ? clampi(a.width - x0, 0, 16) : 0;
+  const int cw = (a.width + 1) >> 1, ch = (a.height + 1) >> 1;
+  const int cy = r * 8 + (l & 7), cx0 = c * 8;
+  const int nc = cy < ch ? clampi(cw - cx0, 0, 8) : 0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    w.my[k] = vis_mask(ny, k);
+    w.y[k] = 0;
+  }
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    w.mc[k] = vis_mask(nc, k);
+    w.c[k] = 0;
+  }
+  if (ny > 0) {
+    const uint8_t* p = a.sy + (size_t)yy * a.sys + x0;
+    if (ny == 16 && a.source_words) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) w.y[k] = ((const uint32_t*)p)[k];
+    } else {
+#pragma unroll
+      for (int i = 0; i < 16; i++)
+        if (i < ny) w.y[i >> 2] |= (uint32_t)p[i] << (8 * (i & 3));
+    }
+  }
+  if (nc > 0) {
+    const uint8_t* p = (l < 8 ? a.su : a.sv) + (size_t)cy * a.scs + cx0;
+    if (nc == 8 && a.source_words) {
+      w.c[0] = ((const uint32_t*)p)[0];
+      w.c[1] = ((const uint32_t*)p)[1];
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+        if (i < nc) w.c[i >> 2] |= (uint32_t)p[i] << (8 * (i & 3));
+    }
+  }
+  return w;
+}
+
+// Sum of squared differences of four byte pairs, masked bytes excluded.
+__device__ __forceinline__ uint32_t ssd4(uint32_t x, uint32_t y, uint32_t m) {
+  const uint32_t d = __vabsdiffu4(x, y) & m;
+  return (uint32_t)__dp4a(d, d, 0u);
+}
+
+// Finish final MB (r, c): write it back (apply mode) and return this lane's
+// share of its visible-window SSD.
+__device__ __forceinline__ uint32_t finish_mb(const LfArgs& a, const uint8_t* slots, int r, int c, int l,
+                                              const SrcWords& sw) {
+  const uint8_t* s = slot_ptr(const_cast<uint8_t*>(slots), r, c);
+  const uint32_t* sy = (const uint32_t*)(s + l * 16);
+  const uint32_t* sc = (const uint32_t*)(s + (l < 8 ? 256 : 320) + (l & 7) * 8);
+  if (a.oy) {
+    uint8_t* gy = a.oy + (size_t)(r * 16 + l) * a.ys + (size_t)c * 16;
+    uint8_t* gc = (l < 8 ? a.ou : a.ov) + (size_t)(r * 8 + (l & 7)) * a.cs + (size_t)c * 8;
+    if (a.recon_words) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) ((uint32_t*)gy)[k] = sy[k];
+      ((uint32_t*)gc)[0] = sc[0];
+      ((uint32_t*)gc)[1] = sc[1];
+    } else {
+      for (int i = 0; i < 16; i++) gy[i] = s[l * 16 + i];
+      for (int i = 0; i < 8; i++) gc[i] = s[(l < 8 ? 256 : 320) + (l & 7) * 8 + i];
+    }
+  }
+  uint32_t acc = 0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) acc += ssd4(sy[k], sw.y[k], sw.my[k]);
+  acc += ssd4(sc[0], sw.c[0], sw.mc[0]) + ssd4(sc[1], sw.c[1], sw.mc[1]);
+  return acc;
+}
+
+// Filter MB (r, c) held in its slot; neighbours in their slots. The
+// caller's half-warp (mask hm) runs this together.
 __device__ __forceinline__ void filter_mb(const LfArgs& a, uint8_t* slots, int level0, int sharp, int r, int c,
-                                          bool has_top, int lane) {
+                                          bool has_top, int l, unsigned hm) {
   const vp8a_mb_lf_info m = a.mbs[(size_t)r * a.mb_cols + c];
   const int level = mb_level(a.base, level0, m);
   if (level == 0) return;
@@ -212,10 +346,10 @@ __device__ __forceinline__ void filter_mb(const LfArgs& a, uint8_t* slots, int l
 
   if (a.base.simple) {
     // §20.6 filter_row_simple: luma only.
-    if (lane < 16) {
-      uint32_t* rw = (uint32_t*)(me + lane * 16);
+    {
+      uint32_t* rw = (uint32_t*)(me + l * 16);
       int p[20];
-      unpack4(has_left ? *(const uint32_t*)(left + lane * 16 + 12) : 0x80808080u, p);
+      unpack4(has_left ? *(const uint32_t*)(left + l * 16 + 12) : 0x80808080u, p);
 #pragma unroll
       for (int k = 0; k < 4; k++) unpack4(rw[k], p + 4 + 4 * k);
       if (has_left) simple_filter<2>(p, q.mbedge);
@@ -224,17 +358,17 @@ __device__ __forceinline__ void filter_mb(const LfArgs& a, uint8_t* slots, int l
         simple_filter<10>(p, q.subedge);
         simple_filter<14>(p, q.subedge);
       }
-      if (has_left) *(uint32_t*)(left + lane * 16 + 12) = pack4(p);
+      if (has_left) *(uint32_t*)(left + l * 16 + 12) = pack4(p);
 #pragma unroll
       for (int k = 0; k < 4; k++) rw[k] = pack4(p + 4 + 4 * k);
     }
-    __syncwarp();
-    if (lane < 16) {
+    __syncwarp(hm);
+    {
       int p[20];
 #pragma unroll
-      for (int k = 0; k < 4; k++) p[k] = has_top ? (int)above[(12 + k) * 16 + lane] - 128 : 0;
+      for (int k = 0; k < 4; k++) p[k] = has_top ? (int)above[(12 + k) * 16 + l] - 128 : 0;
 #pragma unroll
-      for (int k = 0; k < 16; k++) p[4 + k] = (int)me[k * 16 + lane] - 128;
+      for (int k = 0; k < 16; k++) p[4 + k] = (int)me[k * 16 + l] - 128;
       if (has_top) simple_filter<2>(p, q.mbedge);
       if (sub) {
         simple_filter<6>(p, q.subedge);
@@ -243,19 +377,20 @@ __device__ __forceinline__ void filter_mb(const LfArgs& a, uint8_t* slots, int l
       }
       if (has_top)
 #pragma unroll
-        for (int k = 2; k < 4; k++) above[(12 + k) * 16 + lane] = (uint8_t)(p[k] + 128);
+        for (int k = 2; k < 4; k++) above[(12 + k) * 16 + l] = (uint8_t)(p[k] + 128);
 #pragma unroll
-      for (int k = 0; k < 16; k++) me[k * 16 + lane] = (uint8_t)(p[4 + k] + 128);
+      for (int k = 0; k < 16; k++) me[k * 16 + l] = (uint8_t)(p[4 + k] + 128);
     }
-    __syncwarp();
+    __syncwarp(hm);
     return;
   }
 
-  // ---- vertical edges (steps 1 and 2) ----
-  if (lane < 16) {
-    uint32_t* rw = (uint32_t*)(me + lane * 16);
+  const int pl = l < 8 ? 256 : 320, cl = l & 7;  // this lane's chroma plane offset and row/column
+  // ---- vertical edges (steps 1 and 2): luma row l, then chroma row cl ----
+  {
+    uint32_t* rw = (uint32_t*)(me + l * 16);
     int p[20];
-    unpack4(has_left ? *(const uint32_t*)(left + lane * 16 + 12) : 0x80808080u, p);
+    unpack4(has_left ? *(const uint32_t*)(left + l * 16 + 12) : 0x80808080u, p);
 #pragma unroll
     for (int k = 0; k < 4; k++) unpack4(rw[k], p + 4 + 4 * k);
     if (has_left) mb_filter<0>(p, q);
@@ -264,30 +399,30 @@ __device__ __forceinline__ void filter_mb(const LfArgs& a, uint8_t* slots, int l
       sb_filter<8>(p, q);
       sb_filter<12>(p, q);
     }
-    if (has_left) *(uint32_t*)(left + lane * 16 + 12) = pack4(p);
+    if (has_left) *(uint32_t*)(left + l * 16 + 12) = pack4(p);
 #pragma unroll
     for (int k = 0; k < 4; k++) rw[k] = pack4(p + 4 + 4 * k);
-  } else {
-    const int pl = lane < 24 ? 256 : 320, row = (lane - 16) & 7;
-    uint32_t* rw = (uint32_t*)(me + pl + row * 8);
+  }
+  {
+    uint32_t* rw = (uint32_t*)(me + pl + cl * 8);
     int p[12];
-    unpack4(has_left ? *(const uint32_t*)(left + pl + row * 8 + 4) : 0x80808080u, p);
+    unpack4(has_left ? *(const uint32_t*)(left + pl + cl * 8 + 4) : 0x80808080u, p);
     unpack4(rw[0], p + 4);
     unpack4(rw[1], p + 8);
     if (has_left) mb_filter<0>(p, q);
     if (sub) sb_filter<4>(p, q);
-    if (has_left) *(uint32_t*)(left + pl + row * 8 + 4) = pack4(p);
+    if (has_left) *(uint32_t*)(left + pl + cl * 8 + 4) = pack4(p);
     rw[0] = pack4(p + 4);
     rw[1] = pack4(p + 8);
   }
-  __syncwarp();
-  // ---- horizontal edges (steps 3 and 4) ----
-  if (lane < 16) {
+  __syncwarp(hm);
+  // ---- horizontal edges (steps 3 and 4): luma column l, chroma column cl ----
+  {
     int p[20];
 #pragma unroll
-    for (int k = 0; k < 4; k++) p[k] = has_top ? (int)above[(12 + k) * 16 + lane] - 128 : 0;
+    for (int k = 0; k < 4; k++) p[k] = has_top ? (int)above[(12 + k) * 16 + l] - 128 : 0;
 #pragma unroll
-    for (int k = 0; k < 16; k++) p[4 + k] = (int)me[k * 16 + lane] - 128;
+    for (int k = 0; k < 16; k++) p[4 + k] = (int)me[k * 16 + l] - 128;
     if (has_top) mb_filter<0>(p, q);
     if (sub) {
       sb_filter<4>(p, q);
@@ -296,88 +431,25 @@ __device__ __forceinline__ void filter_mb(const LfArgs& a, uint8_t* slots, int l
     }
     if (has_top)
 #pragma unroll
-      for (int k = 1; k < 4; k++) above[(12 + k) * 16 + lane] = (uint8_t)(p[k] + 128);
+      for (int k = 1; k < 4; k++) above[(12 + k) * 16 + l] = (uint8_t)(p[k] + 128);
 #pragma unroll
-    for (int k = 0; k < 16; k++) me[k * 16 + lane] = (uint8_t)(p[4 + k] + 128);
-  } else {
-    const int pl = lane < 24 ? 256 : 320, col = (lane - 16) & 7;
+    for (int k = 0; k < 16; k++) me[k * 16 + l] = (uint8_t)(p[4 + k] + 128);
+  }
+  {
     int p[12];
 #pragma unroll
-    for (int k = 0; k < 4; k++) p[k] = has_top ? (int)above[pl + (4 + k) * 8 + col] - 128 : 0;
+    for (int k = 0; k < 4; k++) p[k] = has_top ? (int)above[pl + (4 + k) * 8 + cl] - 128 : 0;
 #pragma unroll
-    for (int k = 0; k < 8; k++) p[4 + k] = (int)me[pl + k * 8 + col] - 128;
+    for (int k = 0; k < 8; k++) p[4 + k] = (int)me[pl + k * 8 + cl] - 128;
     if (has_top) mb_filter<0>(p, q);
     if (sub) sb_filter<4>(p, q);
     if (has_top)
 #pragma unroll
-      for (int k = 1; k < 4; k++) above[pl + (4 + k) * 8 + col] = (uint8_t)(p[k] + 128);
+      for (int k = 1; k < 4; k++) above[pl + (4 + k) * 8 + cl] = (uint8_t)(p[k] + 128);
 #pragma unroll
-    for (int k = 0; k < 8; k++) me[pl + k * 8 + col] = (uint8_t)(p[4 + k] + 128);
+    for (int k = 0; k < 8; k++) me[pl + k * 8 + cl] = (uint8_t)(p[4 + k] + 128);
   }
-  __syncwarp();
-}
-
-// Load MB (r, c) of the unfiltered reconstruction into its slot.
-__device__ __forceinline__ void load_mb(const LfArgs& a, uint8_t* slots, int r, int c, int lane) {
-  uint8_t* s = slot_ptr(slots, r, c);
-  const size_t yo = (size_t)r * 16 * a.ys + (size_t)c * 16;
-#pragma unroll
-  for (int k = 0; k < 8; k++) {
-    int i = lane + 32 * k, rr = i >> 4, cc = i & 15;
-    s[i] = a.y[yo + rr * a.ys + cc];
-  }
-  const size_t co = (size_t)r * 8 * a.cs + (size_t)c * 8;
-#pragma unroll
-  for (int k = 0; k < 2; k++) {
-    int i = lane + 32 * k, rr = i >> 3, cc = i & 7;
-    s[256 + i] = a.u[co + rr * a.cs + cc];
-    s[320 + i] = a.v[co + rr * a.cs + cc];
-  }
-  __syncwarp();
-}
-
-// Score (or write back) final MB (r, c): visible-window SSD vs the source.
-__device__ __forceinline__ uint64_t finish_mb(const LfArgs& a, const uint8_t* slots, int r, int c, int lane) {
-  const uint8_t* s = slot_ptr(const_cast<uint8_t*>(slots), r, c);
-  if (a.oy) {
-    const size_t yo = (size_t)r * 16 * a.ys + (size_t)c * 16;
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-      int i = lane + 32 * k;
-      a.oy[yo + (i >> 4) * a.ys + (i & 15)] = s[i];
-    }
-    const size_t co = (size_t)r * 8 * a.cs + (size_t)c * 8;
-#pragma unroll
-    for (int k = 0; k < 2; k++) {
-      int i = lane + 32 * k;
-      a.ou[co + (i >> 3) * a.cs + (i & 7)] = s[256 + i];
-      a.ov[co + (i >> 3) * a.cs + (i & 7)] = s[320 + i];
-    }
-  }
-  if (!a.ssd_out) return 0;
-  uint32_t acc = 0;
-  const int y0 = r * 16, x0 = c * 16;
-#pragma unroll
-  for (int k = 0; k < 8; k++) {
-    int i = lane + 32 * k, rr = i >> 4, cc = i & 15;
-    if (y0 + rr < a.height && x0 + cc < a.width) {
-      int d = (int)s[i] - (int)a.sy[(size_t)(y0 + rr) * a.sys + x0 + cc];
-      acc += (uint32_t)(d * d);
-    }
-  }
-  const int cw = (a.width + 1) >> 1, ch = (a.height + 1) >> 1;
-  const int cy0 = r * 8, cx0 = c * 8;
-#pragma unroll
-  for (int k = 0; k < 2; k++) {
-    int i = lane + 32 * k, rr = i >> 3, cc = i & 7;
-    if (cy0 + rr < ch && cx0 + cc < cw) {
-      size_t so = (size_t)(cy0 + rr) * a.scs + cx0 + cc;
-      int du = (int)s[256 + i] - (int)a.su[so];
-      int dv = (int)s[320 + i] - (int)a.sv[so];
-      acc += (uint32_t)(du * du) + (uint32_t)(dv * dv);
-    }
-  }
-  return acc;
+  __syncwarp(hm);
 }
 
 __device__ __forceinline__ void block_sum_store(uint64_t v, uint64_t* dst) {
@@ -395,10 +467,17 @@ __device__ __forceinline__ void block_sum_store(uint64_t v, uint64_t* dst) {
   }
 }
 
+// One CTA per candidate. At step t the MBs of the rows listed in
+// sched_row[sched_off[t] .. sched_off[t+1]) are independent; half-warp h
+// takes the h-th, (h + H)-th, ... of them. Per MB the global fetches (its
+// reconstruction and the source under the MB finished in its slot) are
+// issued together before the slot is touched.
 __global__ void __launch_bounds__(1024) lf_sweep_kernel(LfArgs a) {
   extern __shared__ __align__(16) uint8_t smem_slots[];
   const int level0 = a.cands[2 * blockIdx.x], sharp = a.cands[2 * blockIdx.x + 1];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int hw = threadIdx.x >> 4, nhw = blockDim.x >> 4, l = threadIdx.x & 15;
+  const unsigned hm = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
   uint64_t acc = 0;
   if (level0 == 0 && a.level0_unfiltered) {
     // score_filter_candidate level 0: the unfiltered reconstruction.
@@ -429,25 +508,32 @@ __global__ void __launch_bounds__(1024) lf_sweep_kernel(LfArgs a) {
     block_sum_store(acc, &a.ssd_out[level0 * 8 + sharp]);
     return;
   }
-  uint8_t* slots = a.smem_slots ? smem_slots : a.gslots + (size_t)blockIdx.x * a.mb_rows * 4 * SLOT;
+  uint8_t* slots = a.smem_slots ? smem_slots : a.gslots + (size_t)blockIdx.x * a.mb_rows * 4 * SLOT_STRIDE;
+  const bool score = a.ssd_out != nullptr;
   for (int t = 0; t < a.steps; t++) {
-    for (int r = warp; r < a.mb_rows; r += nwarps) {
-      const int t0 = a.row_t0[r];
-      if (t0 < 0) continue;
-      const int c = t - t0;
-      if (c < 0 || c >= a.mb_cols) continue;
-      if (c >= 4) acc += finish_mb(a, slots, r, c - 4, lane);
-      __syncwarp();
-      load_mb(a, slots, r, c, lane);
-      filter_mb(a, slots, level0, sharp, r, c, a.row_top[r] != 0, lane);
+    const int e = a.sched_off[t + 1];
+    for (int i = a.sched_off[t] + hw; i < e; i += nhw) {
+      const int r = a.sched_row[i], c = t - a.row_t0[r];
+      const MbWords rec = fetch_recon(a, r, c, l);
+      if (c >= 4) {
+        const SrcWords sw = score ? fetch_source(a, r, c - 4, l) : SrcWords{};
+        acc += finish_mb(a, slots, r, c - 4, l, sw);
+        __syncwarp(hm);
+      }
+      store_slot(slot_ptr(slots, r, c), rec, l);
+      __syncwarp(hm);
+      filter_mb(a, slots, level0, sharp, r, c, a.row_top[r] != 0, l, hm);
     }
     __syncthreads();
   }
-  for (int r = warp; r < a.mb_rows; r += nwarps) {
-    if (a.row_t0[r] < 0) continue;
-    for (int c = max(0, a.mb_cols - 4); c < a.mb_cols; c++) acc += finish_mb(a, slots, r, c, lane);
+  // The last four MBs of every scored row.
+  for (int i = hw; i < a.mb_rows * 4; i += nhw) {
+    const int r = i >> 2, c = a.mb_cols - 4 + (i & 3);
+    if (c < 0 || a.row_t0[r] < 0) continue;
+    const SrcWords sw = score ? fetch_source(a, r, c, l) : SrcWords{};
+    acc += finish_mb(a, slots, r, c, l, sw);
   }
-  if (a.ssd_out) block_sum_store(acc, &a.ssd_out[level0 * 8 + sharp]);
+  if (score) block_sum_store(acc, &a.ssd_out[level0 * 8 + sharp]);
 }
 
 // Plain visible-window SSD of a reconstruction (reconstruction_ssd).
@@ -574,16 +660,40 @@ vp8a_status stage_lf(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_planes* planes,
         max_t0 = std::max(max_t0, 2 * k);
       }
   }
-  void* dt0;
-  void* dtop;
-  if ((s = st.scratch(sizeof(int16_t) * rows, &dt0)) != VP8A_OK) return s;
-  if ((s = st.scratch(rows, &dtop)) != VP8A_OK) return s;
-  VP8A_CUDA(cudaMemcpyAsync(dt0, t0.data(), sizeof(int16_t) * rows, cudaMemcpyHostToDevice, ctx->stream));
-  VP8A_CUDA(cudaMemcpyAsync(dtop, top.data(), rows, cudaMemcpyHostToDevice, ctx->stream));
-  VP8A_CUDA(cudaStreamSynchronize(ctx->stream));  // host vectors go out of scope
-  a.row_t0 = (const int16_t*)dt0;
-  a.row_top = (const uint8_t*)dtop;
-  a.steps = max_t0 + cols;
+  // Step schedule: the rows active at step t, in increasing order.
+  const int steps = max_t0 + cols;
+  std::vector<int32_t> off(steps + 1, 0);
+  std::vector<uint16_t> sched;
+  int max_active = 0;
+  for (int t = 0; t < steps; t++) {
+    off[t] = (int32_t)sched.size();
+    for (int r = 0; r < rows; r++)
+      if (t0[r] >= 0 && t >= t0[r] && t < t0[r] + cols) sched.push_back((uint16_t)r);
+    max_active = std::max(max_active, (int)sched.size() - off[t]);
+  }
+  off[steps] = (int32_t)sched.size();
+  // One upload: t0 (int16), top (u8), offsets (int32), rows (u16).
+  const size_t o_top = sizeof(int16_t) * rows, o_off = (o_top + rows + 3) & ~(size_t)3,
+               o_row = o_off + sizeof(int32_t) * (steps + 1), total = o_row + sizeof(uint16_t) * sched.size();
+  std::vector<uint8_t> blob(total, 0);
+  memcpy(blob.data(), t0.data(), o_top);
+  memcpy(blob.data() + o_top, top.data(), rows);
+  memcpy(blob.data() + o_off, off.data(), sizeof(int32_t) * (steps + 1));
+  if (!sched.empty()) memcpy(blob.data() + o_row, sched.data(), sizeof(uint16_t) * sched.size());
+  void* dblob;
+  if ((s = st.scratch(total, &dblob)) != VP8A_OK) return s;
+  VP8A_CUDA(cudaMemcpyAsync(dblob, blob.data(), total, cudaMemcpyHostToDevice, ctx->stream));
+  VP8A_CUDA(cudaStreamSynchronize(ctx->stream));  // the host blob goes out of scope
+  const uint8_t* db = (const uint8_t*)dblob;
+  a.row_t0 = (const int16_t*)db;
+  a.row_top = db + o_top;
+  a.sched_off = (const int32_t*)(db + o_off);
+  a.sched_row = (const uint16_t*)(db + o_row);
+  a.max_active = max_active;
+  a.steps = steps;
+  auto al4 = [](const void* p, uint64_t stride) { return ((uintptr_t)p % 4 == 0) && (stride % 4 == 0); };
+  a.recon_words = al4(a.y, a.ys) && al4(a.u, a.cs) && al4(a.v, a.cs);
+  a.source_words = a.sy ? (al4(a.sy, a.sys) && al4(a.su, a.scs) && al4(a.sv, a.scs)) : 0;
   L->max_steps = a.steps;
   return VP8A_OK;
 }
@@ -596,10 +706,10 @@ vp8a_status launch_sweep(vp8a_ctx* ctx, vp8a::Stager& st, LfArgs a, const uint8_
   if ((s = st.scratch((size_t)n * 2, &dc)) != VP8A_OK) return s;
   VP8A_CUDA(cudaMemcpyAsync(dc, cands, (size_t)n * 2, cudaMemcpyHostToDevice, ctx->stream));
   a.cands = (const uint8_t*)dc;
-  const size_t slot_bytes = (size_t)a.mb_rows * 4 * SLOT;
+  const size_t slot_bytes = (size_t)a.mb_rows * 4 * SLOT_STRIDE;
   int max_smem = 0;
   VP8A_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-  int threads = std::min(1024, 32 * a.mb_rows);
+  const int threads = std::min(1024, std::max(32, (16 * a.max_active + 31) / 32 * 32));
   if (slot_bytes + 1024 <= (size_t)max_smem) {
     a.smem_slots = 1;
     a.gslots = nullptr;
