@@ -83,6 +83,13 @@ struct MainOut {
   vp8a_search_result whole, half, quarter;
 };
 
+// One reference's mode decision (pick_mb_for_ref's result).
+struct RefDec {
+  double j, total;
+  vp8a_mv mv;
+  int mode, pid;
+};
+
 struct SplitOut {
   double j;
   vp8a_mv split_mvs[16];
@@ -97,7 +104,9 @@ struct SplitOut {
 struct SplitScratch {
   uint32_t table[16 * CMAX];  // group g's SAD at column m: table[g * CMAX + m]
   vp8a_mv cmv[CMAX];
+  double new_bits[16];        // NEW4X4 vector bits of group g (when new_ok)
   uint32_t new_sad[16];
+  uint8_t new_ok[16];         // group g's NEW differential lies in [-1023, 1023]
   uint8_t chosen[16];         // column each group chose
 };
 struct Plan {
@@ -292,9 +301,15 @@ __device__ __forceinline__ double mv_partition_bits(const double* t, int pid) {
 // of group SADs at every vector the sub-MV choice can consider (ZERO, the
 // external neighbours' vectors, every group's NEW result); the sequential
 // LEFT/ABOVE/ZERO/NEW choice over groups then reads that table.
-__device__ void split_partition(const AnArgs& a, const double* t, const MePlane& P, const RefSmem& R, const Plan& pl,
-                                int mbx, int mby, const uint8_t* src, vp8a_mv bp, const MbInfoDev& above,
-                                const MbInfoDev& left, int pid, SplitScratch& W, SplitOut* out, int lane) {
+//
+// The per-group costs that do not depend on the chain are computed before
+// it: sbits[ctx * 4 + mode] = submv_ref_bits of each context and mode, and
+// each group's NEW vector bits. Every value is the same expression the
+// reference evaluates, so the chain's sums are unchanged.
+__device__ void split_partition(const AnArgs& a, const double* t, const double* sbits, const MePlane& P,
+                                const RefSmem& R, const Plan& pl, int mbx, int mby, const uint8_t* src, vp8a_mv bp,
+                                const MbInfoDev& above, const MbInfoDev& left, int pid, SplitScratch& W,
+                                SplitOut* out, int lane) {
   const int G = pid == 3 ? 16 : (pid == 2 ? 4 : 2);
   const int L = 32 / G, g = lane / L, s = lane - g * L;
   const int row0 = c_geom[pid][g][0], col0 = c_geom[pid][g][1], gw = c_geom[pid][g][2];
@@ -328,6 +343,10 @@ __device__ void split_partition(const AnArgs& a, const double* t, const MePlane&
   if (s == 0) {
     W.cmv[9 + g] = best;
     W.new_sad[g] = bs;
+    const int dr = (int)best.row - bp.row, dc = (int)best.col - bp.col;
+    const bool ok = dr >= -1023 && dr <= 1023 && dc >= -1023 && dc <= 1023;
+    W.new_ok[g] = ok;
+    W.new_bits[g] = ok ? mv_bits_lookup(a.mvbits, 0, dr) + mv_bits_lookup(a.mvbits, 1, dc) : 0.0;
   }
   if (lane == 0) {
     W.cmv[0] = vp8a_mv{0, 0};
@@ -353,34 +372,35 @@ __device__ void split_partition(const AnArgs& a, const double* t, const MePlane&
     const vp8a_mv lmv = W.cmv[lidx], amv = W.cmv[aidx];
     const bool lez = mv_zero(lmv), aez = mv_zero(amv), lea = mv_eq(lmv, amv);
     const int ctxi = (lea && lez) ? 4 : (lea ? 3 : (aez ? 2 : (lez ? 1 : 0)));
-    const uint8_t* probs = c_submv_probs[ctxi];
+    const double* mb = sbits + ctxi * 4;
     const uint32_t* trow = W.table + gg * CMAX;
-    int best_mode = VP8A_SUBMV_ZERO, best_col = 0;
-    int diff_r = 0, diff_c = 0;
+    // LEFT, ABOVE, ZERO, then NEW; strict '<' keeps the first minimum.
+    const double j0 = (double)trow[lidx] + a.lambda * (mb[0] + 0.0);
+    const double j1 = (double)trow[aidx] + a.lambda * (mb[1] + 0.0);
+    const double j2 = (double)trow[0] + a.lambda * (mb[2] + 0.0);
     double best_j = __longlong_as_double(0x7ff0000000000000LL);
-    const int cols[3] = {lidx, aidx, 0};
-    for (int m = 0; m < 3; m++) {
-      const double sad = (double)trow[cols[m]];
-      const double mode_bits = submv_ref_bits(t, probs, m);
-      const double j = sad + a.lambda * (mode_bits + 0.0);
-      if (j < best_j) {
-        best_j = j;
-        best_mode = m;
-        best_col = cols[m];
-      }
+    int best_mode = VP8A_SUBMV_ZERO, best_col = 0;
+    if (j0 < best_j) {
+      best_j = j0;
+      best_mode = VP8A_SUBMV_LEFT;
+      best_col = lidx;
     }
-    const vp8a_mv nm = W.cmv[9 + gg];
-    const int dr = (int)nm.row - bp.row, dc = (int)nm.col - bp.col;
-    if (dr >= -1023 && dr <= 1023 && dc >= -1023 && dc <= 1023) {
-      const double diff_bits = mv_bits_lookup(a.mvbits, 0, dr) + mv_bits_lookup(a.mvbits, 1, dc);
-      const double mode_bits = submv_ref_bits(t, probs, VP8A_SUBMV_NEW);
-      const double j = (double)W.new_sad[gg] + a.lambda * (mode_bits + diff_bits);
-      if (j < best_j) {
-        best_j = j;
+    if (j1 < best_j) {
+      best_j = j1;
+      best_mode = VP8A_SUBMV_ABOVE;
+      best_col = aidx;
+    }
+    if (j2 < best_j) {
+      best_j = j2;
+      best_mode = VP8A_SUBMV_ZERO;
+      best_col = 0;
+    }
+    if (W.new_ok[gg]) {
+      const double jn = (double)W.new_sad[gg] + a.lambda * (mb[3] + W.new_bits[gg]);
+      if (jn < best_j) {
+        best_j = jn;
         best_mode = VP8A_SUBMV_NEW;
         best_col = 9 + gg;
-        diff_r = dr;
-        diff_c = dc;
       }
     }
     if (!isfinite(best_j)) {
@@ -388,8 +408,8 @@ __device__ void split_partition(const AnArgs& a, const double* t, const MePlane&
       return;
     }
     total_sad += trow[best_col];
-    total_bits += submv_ref_bits(t, probs, best_mode);
-    if (best_mode == VP8A_SUBMV_NEW) total_bits += mv_bits_lookup(a.mvbits, 0, diff_r) + mv_bits_lookup(a.mvbits, 1, diff_c);
+    total_bits += mb[best_mode];
+    if (best_mode == VP8A_SUBMV_NEW) total_bits += W.new_bits[gg];
     __syncwarp();
     if (lane == 0) {
       W.chosen[gg] = (uint8_t)best_col;
@@ -428,8 +448,10 @@ __global__ void __launch_bounds__(MAX_REFS* WARPS_PER_REF * 32) analysis_kernel(
   __shared__ SplitScratch ss[MAX_REFS * 4];
   __shared__ __align__(16) uint8_t src[256];
   __shared__ double bit_cost[256];
+  __shared__ double sbits[5 * 4];  // submv_ref_bits per context and mode
   __shared__ MainOut mains[MAX_REFS];
   __shared__ SplitOut splits[MAX_REFS][4];
+  __shared__ RefDec decs[MAX_REFS];
   __shared__ MbInfoDev nb[3];  // above, left, aboveleft
   __shared__ Census cen;
   __shared__ Plan plan;
@@ -439,6 +461,7 @@ __global__ void __launch_bounds__(MAX_REFS* WARPS_PER_REF * 32) analysis_kernel(
   const int ref = warp / WARPS_PER_REF, role = warp % WARPS_PER_REF;  // role 0 = main, 1..4 = split pid
   for (int i = tid; i < 256; i += nthreads) bit_cost[i] = a.bit_cost[i];
   __syncthreads();
+  if (tid < 20) sbits[tid] = submv_ref_bits(bit_cost, c_submv_probs[tid >> 2], tid & 3);
   const MbInfoDev border = {VP8A_REF_INTRA, 0, 0, 0, {0, 0}, {}};
 
   for (int r = blockIdx.x; r < a.mb_rows; r += gridDim.x) {
@@ -512,28 +535,27 @@ __global__ void __launch_bounds__(MAX_REFS* WARPS_PER_REF * 32) analysis_kernel(
           m.whole = diamond(P, R.ws, plan.wx0, plan.wy0, mbx, mby, bp, 8, src, lane);
           if (!half_refine_planes(R.ws, plan.wx0, plan.wy0, mbx, mby, m.whole.mv, src, lane, &m.half))
             m.half = refine(P, R.ws, plan.wx0, plan.wy0, mbx, mby, m.whole.mv, 2, src, lane);
-          m.quarter = refine(P, R.ws, plan.wx0, plan.wy0, mbx, mby, m.half.mv, 1, src, lane);
+          m.quarter = refine(P, R.ws, plan.wx0, plan.wy0, mbx, mby, m.half.mv, 1, src, lane, m.half.sad);
           const int en_r = eighth(cen.nearest.row), en_c = eighth(cen.nearest.col);
           m.sad_nearest = subpel_sad(R.halo_nearest, HS, en_c & 7, en_r & 7, src, R.ws.temp, lane);
           const int er_r = eighth(cen.near_.row), er_c = eighth(cen.near_.col);
           m.sad_near = subpel_sad(R.halo_near, HS, er_c & 7, er_r & 7, src, R.ws.temp, lane);
           if (lane == 0) mains[ref] = m;
         } else {
-          split_partition(a, bit_cost, P, R, plan, mbx, mby, src, bp, nb[0], nb[1], role - 1,
+          split_partition(a, bit_cost, sbits, P, R, plan, mbx, mby, src, bp, nb[0], nb[1], role - 1,
                           ss[ref * 4 + role - 1], &splits[ref][role - 1], lane);
         }
       }
-      __syncthreads();
-      if (tid == 0) {
-        const double* t = bit_cost;
-        const double lambda = a.lambda;
-        const uint8_t* p = cen.p;
-        const vp8a_mv bp = cen.best_predictor;
-        double best_total = __longlong_as_double(0x7ff0000000000000LL);
-        int best_k = -1, best_mode = 0, best_pid = VP8A_PART_NONE;
-        vp8a_mv best_mv = {0, 0};
-        double best_j = 0.0;
-        for (int k = 0; k < a.n_refs; k++) {
+      if (ref < a.n_refs) {
+        // The reference's five warps meet; its main warp's lane 0 decides
+        // its mode (pick_mb_for_ref, src/encoder.rs:8598-8652).
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + ref), "r"(WARPS_PER_REF * 32) : "memory");
+        if (role == 0 && lane == 0) {
+          const int k = ref;
+          const double* t = bit_cost;
+          const double lambda = a.lambda;
+          const uint8_t* p = cen.p;
+          const vp8a_mv bp = cen.best_predictor;
           const MainOut& m = mains[k];
           const double bits_zero = bb(t, p[0], 0);
           const double bits_nearest = bb(t, p[0], 1) + bb(t, p[1], 0);
@@ -608,13 +630,26 @@ __global__ void __launch_bounds__(MAX_REFS* WARPS_PER_REF * 32) analysis_kernel(
             tr.j = cj;
             a.trace[((size_t)r * a.mb_cols + c) * a.n_refs + k] = tr;
           }
-          if (total < best_total) {
-            best_total = total;
+          decs[k] = RefDec{cj, total, mv, mode, pid};
+        }
+      }
+      __syncthreads();
+      if (tid == 0) {
+        // decide_mb_exhaustive's reference comparison: first strict minimum
+        // of J + ref_frame_tree_bits in reference order.
+        double best_total = __longlong_as_double(0x7ff0000000000000LL);
+        int best_k = -1, best_mode = 0, best_pid = VP8A_PART_NONE;
+        vp8a_mv best_mv = {0, 0};
+        double best_j = 0.0;
+        for (int k = 0; k < a.n_refs; k++) {
+          const RefDec& rd = decs[k];
+          if (rd.total < best_total) {
+            best_total = rd.total;
             best_k = k;
-            best_mode = mode;
-            best_mv = mv;
-            best_j = cj;
-            best_pid = pid;
+            best_mode = rd.mode;
+            best_mv = rd.mv;
+            best_j = rd.j;
+            best_pid = rd.pid;
           }
         }
         vp8a_mb_decision d;

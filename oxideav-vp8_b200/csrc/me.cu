@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(ME_WARPS * 32) me_batch_kernel(MeBatch a) {
     vp8a_search_result h;
     if (!half_refine_planes(S, wx0, wy0, mbx, mby, w.mv, src, lane, &h))
       h = refine(a.P, S, wx0, wy0, mbx, mby, w.mv, 2, src, lane);
-    vp8a_search_result q = refine(a.P, S, wx0, wy0, mbx, mby, h.mv, 1, src, lane);
+    vp8a_search_result q = refine(a.P, S, wx0, wy0, mbx, mby, h.mv, 1, src, lane, h.sad);
     if (lane == 0) {
       if (a.out0) a.out0[item] = w;
       if (a.out1) a.out1[item] = h;

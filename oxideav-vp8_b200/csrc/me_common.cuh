@@ -239,11 +239,14 @@ __device__ __forceinline__ vp8a_search_result diamond(const MePlane& P, WarpScra
 // half_pixel_refine_luma / quarter_pixel_refine_luma
 // (src/motion_search.rs:564-728): centre plus 8 offsets of `step`
 // quarter-pels in the fixed order, strict '<', collapse skips.
+// `center_sad` is the SAD at `center` when the caller already has it (the
+// previous refinement's result), else ~0u.
 __device__ __forceinline__ vp8a_search_result refine(const MePlane& P, WarpScratch& S, int wx0, int wy0, int mbx,
                                                      int mby, vp8a_mv center, int step, const uint8_t* src,
-                                                     int lane) {
+                                                     int lane, uint32_t center_sad = ~0u) {
   vp8a_mv best = center;
-  uint32_t best_sad = sad_at_mv(P, S, wx0, wy0, mbx, mby, center.row, center.col, src, lane);
+  uint32_t best_sad = center_sad != ~0u ? center_sad
+                                        : sad_at_mv(P, S, wx0, wy0, mbx, mby, center.row, center.col, src, lane);
 #pragma unroll 1
   for (int k = 0; k < 8; k++) {
     // Offsets (-1,-1) (-1,0) (-1,1) (0,-1) (0,1) (1,-1) (1,0) (1,1).
