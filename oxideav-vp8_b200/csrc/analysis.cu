@@ -27,6 +27,7 @@
 // parallel across lanes). The f64 RD decision runs on one thread with the
 // reference's operation order; the library is built with -fmad=false so no
 // multiply-add is fused.
+#include <cooperative_groups.h>
 #include <cstddef>
 
 #include "census.cuh"
@@ -36,7 +37,6 @@ using namespace vp8a_dev;
 
 
 constexpr int MAX_REFS = 3;
-constexpr int WARPS_PER_REF = 5;
 
 struct AnArgs {
   const uint8_t* fy;
@@ -56,6 +56,7 @@ struct AnArgs {
   vp8a_mb_decision* dec;
   vp8a_ref_search* trace;
   unsigned long long spin_limit;
+  int words;  // reference planes allow 32-bit loads (4-byte aligned base and stride)
 };
 
 // ------------------------------------------------------------- staging
@@ -83,12 +84,16 @@ struct MainOut {
   vp8a_search_result whole, half, quarter;
 };
 
-// One reference's mode decision (pick_mb_for_ref's result).
-struct RefDec {
+// One reference's mode decision (pick_mb_for_ref's result), with the
+// chosen partition's sub-MVs; each CTA writes its own into rank 0.
+struct __align__(16) RefDec {
   double j, total;
   vp8a_mv mv;
   int mode, pid;
+  vp8a_mv split_mvs[16];
+  uint8_t submv_modes[16];
 };
+static_assert(sizeof(RefDec) % 16 == 0, "RefDec is copied as words");
 
 struct SplitOut {
   double j;
@@ -108,7 +113,13 @@ struct SplitScratch {
   uint32_t new_sad[16];
   uint8_t new_ok[16];         // group g's NEW differential lies in [-1023, 1023]
   uint8_t chosen[16];         // column each group chose
+  double bits_a[16];          // group g's sub-MV reference bits
+  uint32_t sad[16];           // group g's SAD at its chosen vector
+  uint8_t is_new[16];         // group g chose NEW4X4 (adds new_bits[g])
+  uint8_t bad[16];            // group g had no finite choice
+  int colpos[CMAX];           // column m: field position, -(j+1) = staged block j, COL_DIRECT
 };
+constexpr int COL_DIRECT = -1000;
 struct Plan {
   int wx0, wy0;        // window origin (plane pixels)
   int hn_x, hn_y;      // NEAREST halo origin
@@ -141,48 +152,188 @@ __device__ __forceinline__ vp8a_mv ext_above(const MbInfoDev& a, int anchor) {
   return a.is_split ? a.split_mvs[anchor + 12] : a.mv;
 }
 
-// Stage every region of every reference; each thread keeps up to BATCH
-// loads in flight before storing.
-template <int BATCH>
-__device__ void stage(const AnArgs& a, RefSmem* rs, const Plan& pl, int mbx, int mby, int tid, int nthreads) {
-  const int per_ref = 40 * 40 + 2 * 441 + pl.nblocks * 256;
-  const int total = a.n_refs * per_ref;
-  for (int base = tid; base < total; base += nthreads * BATCH) {
-    uint8_t v[BATCH];
-    uint8_t* d[BATCH];
+// Stage this CTA's reference: every region row is copied as 32-bit words
+// (two aligned loads and a funnel shift per word); a word whose plane bytes
+// are not all inside the row — at the frame edges — is fetched byte by byte
+// with edge clamping. Each thread keeps up to 8 words in flight.
+__device__ void stage_ref(const MePlane& P, RefSmem& R, const Plan& pl, int mbx, int mby, bool words, int tid,
+                          int nthreads) {
+  constexpr int N_WIN = 40 * 10, N_HALO = 21 * 6;
+  const int total = N_WIN + 2 * N_HALO + pl.nblocks * 64;
+  for (int base = tid; base < total; base += nthreads * 8) {
+    uint32_t v[8];
+    uint32_t* d[8];
 #pragma unroll
-    for (int j = 0; j < BATCH; j++) {
+    for (int j = 0; j < 8; j++) {
       const int e = base + j * nthreads;
       d[j] = nullptr;
+      v[j] = 0;
       if (e < total) {
-        const int k = e < per_ref ? 0 : (e < 2 * per_ref ? 1 : 2);
-        const int rem = e - k * per_ref;
-        const MePlane& P = a.refs[k];
-        int x, y;
-        if (rem < 1600) {
-          const int r = rem / 40, c = rem - r * 40;
-          x = pl.wx0 + c;
-          y = pl.wy0 + r;
-          d[j] = rs[k].ws.win + r * WS + c;
-        } else if (rem < 1600 + 2 * 441) {
-          const int q = rem - 1600, h = q >= 441, qq = q - h * 441;
-          const int r = qq / 21, c = qq - r * 21;
-          x = (h ? pl.hr_x : pl.hn_x) + c;
-          y = (h ? pl.hr_y : pl.hn_y) + r;
-          d[j] = (h ? rs[k].halo_near : rs[k].halo_nearest) + r * HS + c;
+        int row, word, x0, y0;
+        uint8_t* dst;
+        if (e < N_WIN) {
+          row = e / 10;
+          word = e - row * 10;
+          x0 = pl.wx0;
+          y0 = pl.wy0;
+          dst = R.ws.win + row * WS;
+        } else if (e < N_WIN + 2 * N_HALO) {
+          const int q = e - N_WIN, h = q >= N_HALO, qq = q - h * N_HALO;
+          row = qq / 6;
+          word = qq - row * 6;
+          x0 = h ? pl.hr_x : pl.hn_x;
+          y0 = h ? pl.hr_y : pl.hn_y;
+          dst = (h ? R.halo_near : R.halo_nearest) + row * HS;
         } else {
-          const int q = rem - 1600 - 2 * 441, b = q >> 8, r = (q >> 4) & 15, c = q & 15;
-          x = mbx + pl.box[b] + c;
-          y = mby + pl.boy[b] + r;
-          d[j] = rs[k].blocks[b] + r * 16 + c;
+          const int q = e - N_WIN - 2 * N_HALO, b = q >> 6;
+          row = (q >> 2) & 15;
+          word = q & 3;
+          x0 = mbx + pl.box[b];
+          y0 = mby + pl.boy[b];
+          dst = R.blocks[b] + row * 16;
         }
-        v[j] = P.plane[(size_t)clampi(y, 0, P.height - 1) * P.stride + clampi(x, 0, P.width - 1)];
+        const uint8_t* rp = P.plane + (size_t)clampi(y0 + row, 0, P.height - 1) * P.stride;
+        const int x = x0 + 4 * word, sh = x & 3, xa = x - sh;
+        if (words && x >= 0 && xa + (sh ? 8 : 4) <= P.width) {
+          const uint32_t lo = *(const uint32_t*)(rp + xa);
+          const uint32_t hi = sh ? *(const uint32_t*)(rp + xa + 4) : 0u;
+          v[j] = __funnelshift_r(lo, hi, 8u * (unsigned)sh);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 4; k++) v[j] |= (uint32_t)rp[clampi(x + k, 0, P.width - 1)] << (8 * k);
+        }
+        d[j] = (uint32_t*)(dst + 4 * word);
       }
     }
 #pragma unroll
-    for (int j = 0; j < BATCH; j++)
+    for (int j = 0; j < 8; j++)
       if (d[j]) *d[j] = v[j];
   }
+}
+
+// ------------------------------------------------------ whole-pel field
+
+// Whole-pel SADs of every position within +-FR pixels of the search start
+// (the snapped, clamped best predictor), per 4x4 block: a group SAD of any
+// SPLITMV partition at such a position is the sum of its blocks, and the
+// 16x16 SAD the sum of all 16. Both diamonds (the MB's, at most 8 steps of
+// one pixel, and every SPLITMV group's, at most 4) stay inside the field,
+// so they become table walks; vectors outside it (ZERO, the neighbours'
+// vectors) are served by the staged blocks.
+constexpr int FR = 8, FN = 2 * FR + 1, FP = FN * FN;
+static_assert(WIN_LEAD - FR >= 0 && WIN_LEAD + FR + 16 <= WS, "the window covers the field");
+
+struct __align__(16) FieldSmem {
+  uint16_t blk[FP][16];  // 4x4 block SADs at each position (raster block order)
+  uint32_t full[FP];     // 16x16 SADs
+  uint16_t grp[FP][8];   // TopBottom 0,1 | LeftRight 0,1 | Quarters 0..3
+};
+
+__device__ __forceinline__ int fpos(int dx, int dy) {
+  return (dx >= -FR && dx <= FR && dy >= -FR && dy <= FR) ? (dy + FR) * FN + dx + FR : -1;
+}
+
+// Block SADs: one thread per (block, row of positions); the 17 positions
+// of a row share each window row's six words.
+__device__ __forceinline__ void field_blocks(const uint8_t* win, const uint8_t* src, FieldSmem& F, int tid) {
+  if (tid >= 16 * FN) return;
+  const int b = tid & 15, dyi = tid >> 4;
+  const int bx4 = (b & 3) * 4, by4 = (b >> 2) * 4;
+  uint32_t acc[FN];
+#pragma unroll
+  for (int i = 0; i < FN; i++) acc[i] = 0;
+#pragma unroll
+  for (int row = 0; row < 4; row++) {
+    const uint32_t sw = *(const uint32_t*)(src + (by4 + row) * 16 + bx4);
+    const uint32_t* w = (const uint32_t*)(win + (WIN_LEAD - FR + dyi + by4 + row) * WS + bx4);
+    uint32_t wd[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) wd[k] = w[k];
+#pragma unroll
+    for (int dxi = 0; dxi < FN; dxi++) {
+      constexpr int base = WIN_LEAD - FR;
+      const int o = base + dxi;
+      acc[dxi] += __vsadu4(__funnelshift_r(wd[o >> 2], wd[(o >> 2) + 1], (unsigned)(o & 3) * 8u), sw);
+    }
+  }
+#pragma unroll
+  for (int dxi = 0; dxi < FN; dxi++) F.blk[dyi * FN + dxi][b] = (uint16_t)acc[dxi];
+}
+
+// 16x16 and partition-group sums per position.
+__device__ __forceinline__ void field_sums(FieldSmem& F, int tid, int nthreads) {
+  for (int pos = tid; pos < FP; pos += nthreads) {
+    const uint32_t* v = (const uint32_t*)F.blk[pos];
+    uint32_t b[16];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const uint32_t w = v[k];
+      b[2 * k] = w & 0xffffu;
+      b[2 * k + 1] = w >> 16;
+    }
+    const uint32_t q0 = b[0] + b[1] + b[4] + b[5], q1 = b[2] + b[3] + b[6] + b[7];
+    const uint32_t q2 = b[8] + b[9] + b[12] + b[13], q3 = b[10] + b[11] + b[14] + b[15];
+    F.full[pos] = q0 + q1 + q2 + q3;
+    uint32_t* g = (uint32_t*)F.grp[pos];
+    g[0] = (q0 + q1) | ((q2 + q3) << 16);
+    g[1] = (q0 + q2) | ((q1 + q3) << 16);
+    g[2] = q0 | (q1 << 16);
+    g[3] = q2 | (q3 << 16);
+  }
+}
+
+// 4x4 block SADs of the staged 16x16 blocks (ZERO and neighbour vectors).
+__device__ __forceinline__ void staged_block_sads(const RefSmem& R, const uint8_t* src, int nblocks,
+                                                  uint16_t (*xs)[16], int tid, int nthreads) {
+  for (int t = tid; t < nblocks * 16; t += nthreads) {
+    const int j = t >> 4, b = t & 15, bx4 = (b & 3) * 4, by4 = (b >> 2) * 4;
+    uint32_t acc = 0;
+#pragma unroll
+    for (int row = 0; row < 4; row++)
+      acc += __vsadu4(*(const uint32_t*)(R.blocks[j] + (by4 + row) * 16 + bx4),
+                      *(const uint32_t*)(src + (by4 + row) * 16 + bx4));
+    xs[j][b] = (uint16_t)acc;
+  }
+}
+
+// small_diamond_search_luma (src/motion_search.rs:381-442) walked over the
+// field: N, S, W, E from the running best, strict '<', collapse skips, at
+// most max_iters rounds. Warp-uniform; a position outside the field (not
+// reachable from an in-range start) is computed from the plane.
+__device__ vp8a_search_result diamond_field(const FieldSmem& F, const MePlane& P, const uint8_t* win, int wx0,
+                                            int wy0, int mbx, int mby, int cxp, int cyp, vp8a_mv center,
+                                            int max_iters, const uint8_t* src, int lane) {
+  auto sad = [&](vp8a_mv m) -> uint32_t {
+    const int x = mbx + m.col / 4, y = mby + m.row / 4;
+    const int p = fpos(x - cxp, y - cyp);
+    return p >= 0 ? F.full[p] : sad_whole_at(P, win, wx0, wy0, x, y, src, lane);
+  };
+  vp8a_mv best;
+  best.row = snap_whole(clamp_component(center.row));
+  best.col = snap_whole(clamp_component(center.col));
+  uint32_t best_sad = sad(best);
+  for (int it = 0; it < max_iters; it++) {
+    bool improved = false;
+    const int dr[4] = {-4, 4, 0, 0}, dc[4] = {0, 0, -4, 4};
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+      vp8a_mv cand;
+      cand.row = snap_whole(clamp_component(best.row + dr[d]));
+      cand.col = snap_whole(clamp_component(best.col + dc[d]));
+      if (cand.row == best.row && cand.col == best.col) continue;
+      const uint32_t s = sad(cand);
+      if (s < best_sad) {
+        best_sad = s;
+        best = cand;
+        improved = true;
+      }
+    }
+    if (!improved) break;
+  }
+  vp8a_search_result res;
+  res.mv = best;
+  res.sad = best_sad;
+  return res;
 }
 
 // -------------------------------------------------------------- SPLITMV
@@ -196,85 +347,62 @@ __constant__ uint32_t c_need_cols[4] = {
     (1u << 0) | (1u << 1) | (1u << 3) | (1u << 5) | (1u << 7) | (0xfu << 9),  // Quarters: 0, 2, 8, 10
     0x1ffffffu};                                                   // Mv16: every column
 
-// Unaligned 4-byte read from shared memory.
-__device__ __forceinline__ uint32_t load4u(const uint8_t* p) {
-  uintptr_t a = (uintptr_t)p;
-  const uint32_t* w = (const uint32_t*)(a & ~(uintptr_t)3);
-  return __funnelshift_r(w[0], w[1], (unsigned)(a & 3) * 8u);
-}
+// 4x4 blocks of group g of partition p, as a bit mask over raster blocks.
+__constant__ uint16_t c_group_blocks[4][16] = {
+    {0x00ff, 0xff00},
+    {0x3333, 0xcccc},
+    {0x0033, 0x00cc, 0x3300, 0xcc00},
+    {0x0001, 0x0002, 0x0004, 0x0008, 0x0010, 0x0020, 0x0040, 0x0080, 0x0100, 0x0200, 0x0400, 0x0800, 0x1000,
+     0x2000, 0x4000, 0x8000}};
 
-// This lane's 8 pixels of its group: one run of 8 (groups 8 or 16 wide) or
-// two rows of 4 (4x4 groups). off0/off1 are (row*stride + col) with the
-// row/col in MB coordinates.
-struct LanePix {
-  int r0, c0, r1, c1;
-  bool wide;
-  uint32_t s0, s1;  // the source bytes as two little-endian words
-};
-
-__device__ __forceinline__ LanePix lane_pixels(int row0, int col0, int gw, int s, const uint8_t* src) {
-  LanePix p;
-  if (gw == 16) {
-    p.r0 = row0 + (s >> 1);
-    p.c0 = col0 + (s & 1) * 8;
-    p.wide = true;
-  } else if (gw == 8) {
-    p.r0 = row0 + s;
-    p.c0 = col0;
-    p.wide = true;
-  } else {
-    p.r0 = row0 + 2 * s;
-    p.c0 = col0;
-    p.wide = false;
-  }
-  p.r1 = p.wide ? p.r0 : p.r0 + 1;
-  p.c1 = p.wide ? p.c0 + 4 : p.c0;
-  p.s0 = *(const uint32_t*)(src + p.r0 * 16 + p.c0);
-  p.s1 = *(const uint32_t*)(src + p.r1 * 16 + p.c1);
-  return p;
-}
-
-// Partial SAD of this lane's pixels for the MB-extent block whose top-left
-// is plane pixel (bx, by): from the window, a staged block, or clamped
-// global loads.
-__device__ __forceinline__ uint32_t lane_gsad(const MePlane& P, const RefSmem& R, const Plan& pl, int mbx, int mby,
-                                              const LanePix& q, int bx, int by) {
-  const int lx = bx - pl.wx0, ly = by - pl.wy0;
-  const uint8_t* base = nullptr;
-  int st = 0;
-  if (lx >= 0 && ly >= 0 && lx + 16 <= WS && ly + 16 <= WS) {
-    base = R.ws.win + ly * WS + lx;
-    st = WS;
-  } else {
-    for (int b = 0; b < pl.nblocks; b++)
-      if (mbx + pl.box[b] == bx && mby + pl.boy[b] == by) {
-        base = R.blocks[b];
-        st = 16;
-        break;
-      }
-  }
-  uint32_t r0, r1;
-  if (base) {
-    r0 = load4u(base + q.r0 * st + q.c0);
-    r1 = load4u(base + q.r1 * st + q.c1);
-  } else {
-    r0 = r1 = 0;
+__device__ __forceinline__ uint32_t group_sum(const uint16_t* v16, int pid, int g) {
+  const uint32_t m = c_group_blocks[pid][g];
+  uint32_t s = 0;
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-      const uint32_t b0 =
-          P.plane[(size_t)clampi(by + q.r0, 0, P.height - 1) * P.stride + clampi(bx + q.c0 + i, 0, P.width - 1)];
-      const uint32_t b1 =
-          P.plane[(size_t)clampi(by + q.r1, 0, P.height - 1) * P.stride + clampi(bx + q.c1 + i, 0, P.width - 1)];
-      r0 |= b0 << (8 * i);
-      r1 |= b1 << (8 * i);
+  for (int b = 0; b < 16; b++)
+    if ((m >> b) & 1u) s += v16[b];
+  return s;
+}
+
+// A group's whole-pel SAD at pixel (x, y) computed from the plane with
+// edge clamping, by one lane (only for positions neither the field nor a
+// staged block covers).
+__device__ uint32_t direct_group_sad(const MePlane& P, const uint8_t* src, int x, int y, int pid, int g) {
+  const uint32_t m = c_group_blocks[pid][g];
+  uint32_t s = 0;
+  for (int b = 0; b < 16; b++) {
+    if (!((m >> b) & 1u)) continue;
+    const int bx4 = (b & 3) * 4, by4 = (b >> 2) * 4;
+    for (int r = 0; r < 4; r++) {
+      const uint8_t* row = P.plane + (size_t)clampi(y + by4 + r, 0, P.height - 1) * P.stride;
+      for (int c = 0; c < 4; c++) {
+        const int d = (int)row[clampi(x + bx4 + c, 0, P.width - 1)] - (int)src[(by4 + r) * 16 + bx4 + c];
+        s += (uint32_t)(d < 0 ? -d : d);
+      }
     }
   }
-  return __vsadu4(r0, q.s0) + __vsadu4(r1, q.s1);
+  return s;
 }
 
-__device__ __forceinline__ uint32_t group_reduce(uint32_t v, int L) {
-  for (int o = L >> 1; o >= 1; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-  return v;
+struct FieldView {
+  const FieldSmem* F;
+  const uint16_t (*xs)[16];
+  const Plan* pl;
+  int mbx, mby, cxp, cyp;
+};
+
+// Group g's SAD at integer offset of `m`: field, staged block, or plane.
+__device__ __forceinline__ uint32_t group_sad(const FieldView& v, const MePlane& P, const uint8_t* src, int pid,
+                                              int g, vp8a_mv m) {
+  const int x = v.mbx + int_off(m.col), y = v.mby + int_off(m.row);
+  const int p = fpos(x - v.cxp, y - v.cyp);
+  if (p >= 0) {
+    if (pid == 3) return v.F->blk[p][g];
+    return v.F->grp[p][(pid == 0 ? 0 : (pid == 1 ? 2 : 4)) + g];
+  }
+  for (int j = 0; j < v.pl->nblocks; j++)
+    if (v.mbx + v.pl->box[j] == x && v.mby + v.pl->boy[j] == y) return group_sum(v.xs[j], pid, g);
+  return direct_group_sad(P, src, x, y, pid, g);
 }
 
 __device__ __forceinline__ double submv_ref_bits(const double* t, const uint8_t* p, int mode) {
@@ -296,51 +424,46 @@ __device__ __forceinline__ double mv_partition_bits(const double* t, int pid) {
   }
 }
 
-// score_split_partition (src/encoder.rs:8080-8246) on one warp. Groups run
-// in parallel (32/G lanes each) for their NEW4X4 diamonds and for a table
-// of group SADs at every vector the sub-MV choice can consider (ZERO, the
-// external neighbours' vectors, every group's NEW result); the sequential
-// LEFT/ABOVE/ZERO/NEW choice over groups then reads that table.
+// score_split_partition (src/encoder.rs:8080-8246) on one warp: lane g
+// walks group g's NEW4X4 diamond over the field, the lanes then fill a
+// table of group SADs at every vector the sub-MV choice can consider (ZERO,
+// the external neighbours' vectors, every group's NEW result), and the
+// sequential LEFT/ABOVE/ZERO/NEW choice over groups reads that table.
 //
 // The per-group costs that do not depend on the chain are computed before
 // it: sbits[ctx * 4 + mode] = submv_ref_bits of each context and mode, and
 // each group's NEW vector bits. Every value is the same expression the
 // reference evaluates, so the chain's sums are unchanged.
-__device__ void split_partition(const AnArgs& a, const double* t, const double* sbits, const MePlane& P,
-                                const RefSmem& R, const Plan& pl, int mbx, int mby, const uint8_t* src, vp8a_mv bp,
-                                const MbInfoDev& above, const MbInfoDev& left, int pid, SplitScratch& W,
-                                SplitOut* out, int lane) {
+__device__ void split_partition(const AnArgs& a, const double* t, const double* sbits, const FieldView& fv,
+                                const MePlane& P, const uint8_t* src, vp8a_mv bp, const MbInfoDev& above,
+                                const MbInfoDev& left, int pid, SplitScratch& W, SplitOut* out, int lane) {
   const int G = pid == 3 ? 16 : (pid == 2 ? 4 : 2);
-  const int L = 32 / G, g = lane / L, s = lane - g * L;
-  const int row0 = c_geom[pid][g][0], col0 = c_geom[pid][g][1], gw = c_geom[pid][g][2];
-  const LanePix q = lane_pixels(row0, col0, gw, s, src);
-  // group_small_diamond_search (src/encoder.rs:7812-7879) for every group
-  // at once: snap then clamp the centre; N, S, W, E clamped, not snapped.
-  vp8a_mv best;
-  best.row = (int16_t)clampi((bp.row / 4) * 4, -1023, 1023);
-  best.col = (int16_t)clampi((bp.col / 4) * 4, -1023, 1023);
-  uint32_t bs = group_reduce(lane_gsad(P, R, pl, mbx, mby, q, mbx + int_off(best.col), mby + int_off(best.row)), L);
-  bool active = true;
-  for (int it = 0; it < 4; it++) {
-    bool improved = false;
-    const int dr[4] = {-4, 4, 0, 0}, dc[4] = {0, 0, -4, 4};
+  if (lane < G) {
+    // group_small_diamond_search (src/encoder.rs:7812-7879): snap then
+    // clamp the centre; N, S, W, E clamped, not snapped; four rounds.
+    const int g = lane;
+    vp8a_mv best;
+    best.row = (int16_t)clampi((bp.row / 4) * 4, -1023, 1023);
+    best.col = (int16_t)clampi((bp.col / 4) * 4, -1023, 1023);
+    uint32_t bs = group_sad(fv, P, src, pid, g, best);
+    for (int it = 0; it < 4; it++) {
+      bool improved = false;
+      const int dr[4] = {-4, 4, 0, 0}, dc[4] = {0, 0, -4, 4};
 #pragma unroll
-    for (int d = 0; d < 4; d++) {
-      vp8a_mv c;
-      c.row = (int16_t)clampi(best.row + dr[d], -1023, 1023);
-      c.col = (int16_t)clampi(best.col + dc[d], -1023, 1023);
-      const uint32_t sv =
-          group_reduce(lane_gsad(P, R, pl, mbx, mby, q, mbx + int_off(c.col), mby + int_off(c.row)), L);
-      if (active && !mv_eq(c, best) && sv < bs) {
-        bs = sv;
-        best = c;
-        improved = true;
+      for (int d = 0; d < 4; d++) {
+        vp8a_mv c;
+        c.row = (int16_t)clampi(best.row + dr[d], -1023, 1023);
+        c.col = (int16_t)clampi(best.col + dc[d], -1023, 1023);
+        if (mv_eq(c, best)) continue;
+        const uint32_t sv = group_sad(fv, P, src, pid, g, c);
+        if (sv < bs) {
+          bs = sv;
+          best = c;
+          improved = true;
+        }
       }
+      if (!improved) break;
     }
-    if (!improved) active = false;
-  }
-  // Candidate columns.
-  if (s == 0) {
     W.cmv[9 + g] = best;
     W.new_sad[g] = bs;
     const int dr = (int)best.row - bp.row, dc = (int)best.col - bp.col;
@@ -355,73 +478,114 @@ __device__ void split_partition(const AnArgs& a, const double* t, const double* 
   }
   __syncwarp();
   const uint32_t need = c_need_cols[pid];
-  for (int m = 0; m < CMAX; m++) {
-    if (!((need >> m) & 1u)) continue;
-    const vp8a_mv mv = W.cmv[m];
-    const uint32_t sv = group_reduce(lane_gsad(P, R, pl, mbx, mby, q, mbx + int_off(mv.col), mby + int_off(mv.row)), L);
-    if (s == 0) W.table[g * CMAX + m] = sv;
+  // Where each needed column's vector lands: the field, a staged block, or
+  // (never for in-range vectors) the plane.
+  if (lane < CMAX && ((need >> lane) & 1u)) {
+    const vp8a_mv m = W.cmv[lane];
+    const int x = fv.mbx + int_off(m.col), y = fv.mby + int_off(m.row);
+    int cp = fpos(x - fv.cxp, y - fv.cyp);
+    if (cp < 0) {
+      cp = COL_DIRECT;
+      for (int j = 0; j < fv.pl->nblocks; j++)
+        if (fv.mbx + fv.pl->box[j] == x && fv.mby + fv.pl->boy[j] == y) {
+          cp = -(j + 1);
+          break;
+        }
+    }
+    W.colpos[lane] = cp;
   }
   __syncwarp();
-  // The sequential sub-MV choice (uniform on every lane; lane 0 records).
-  uint32_t total_sad = 0;
-  double total_bits = 0.0;
-  for (int gg = 0; gg < G; gg++) {
-    const int anchor = c_geom[pid][gg][4];
-    const int lidx = (anchor & 3) == 0 ? 1 + (anchor >> 2) : W.chosen[c_partitions[pid][anchor - 1]];
-    const int aidx = anchor < 4 ? 5 + anchor : W.chosen[c_partitions[pid][anchor - 4]];
-    const vp8a_mv lmv = W.cmv[lidx], amv = W.cmv[aidx];
-    const bool lez = mv_zero(lmv), aez = mv_zero(amv), lea = mv_eq(lmv, amv);
-    const int ctxi = (lea && lez) ? 4 : (lea ? 3 : (aez ? 2 : (lez ? 1 : 0)));
-    const double* mb = sbits + ctxi * 4;
-    const uint32_t* trow = W.table + gg * CMAX;
-    // LEFT, ABOVE, ZERO, then NEW; strict '<' keeps the first minimum.
-    const double j0 = (double)trow[lidx] + a.lambda * (mb[0] + 0.0);
-    const double j1 = (double)trow[aidx] + a.lambda * (mb[1] + 0.0);
-    const double j2 = (double)trow[0] + a.lambda * (mb[2] + 0.0);
-    double best_j = __longlong_as_double(0x7ff0000000000000LL);
-    int best_mode = VP8A_SUBMV_ZERO, best_col = 0;
-    if (j0 < best_j) {
-      best_j = j0;
-      best_mode = VP8A_SUBMV_LEFT;
-      best_col = lidx;
+  const int goff = pid == 0 ? 0 : (pid == 1 ? 2 : 4);
+  for (int q = lane; q < G * CMAX; q += 32) {
+    const int g = q / CMAX, m = q - g * CMAX;
+    if (!((need >> m) & 1u)) continue;
+    const int cp = W.colpos[m];
+    uint32_t v;
+    if (cp >= 0) {
+      v = pid == 3 ? fv.F->blk[cp][g] : fv.F->grp[cp][goff + g];
+    } else if (cp != COL_DIRECT) {
+      v = pid == 3 ? fv.xs[-cp - 1][g] : group_sum(fv.xs[-cp - 1], pid, g);
+    } else {
+      const vp8a_mv mm = W.cmv[m];
+      v = direct_group_sad(P, src, fv.mbx + int_off(mm.col), fv.mby + int_off(mm.row), pid, g);
     }
-    if (j1 < best_j) {
-      best_j = j1;
-      best_mode = VP8A_SUBMV_ABOVE;
-      best_col = aidx;
-    }
-    if (j2 < best_j) {
-      best_j = j2;
-      best_mode = VP8A_SUBMV_ZERO;
-      best_col = 0;
-    }
-    if (W.new_ok[gg]) {
-      const double jn = (double)W.new_sad[gg] + a.lambda * (mb[3] + W.new_bits[gg]);
-      if (jn < best_j) {
-        best_j = jn;
-        best_mode = VP8A_SUBMV_NEW;
-        best_col = 9 + gg;
+    W.table[q] = v;
+  }
+  __syncwarp();
+  // The sub-MV choice. A group's LEFT/ABOVE come from the group to its left
+  // and above, so the groups of one anti-diagonal of the partition's group
+  // grid are independent: step s decides them in parallel, one lane each.
+  const int gh = pid == 1 ? 1 : (pid == 3 ? 4 : 2), gw = pid == 0 ? 1 : (pid == 3 ? 4 : 2);
+  for (int st = 0; st < gh + gw - 1; st++) {
+    const int gr = max(0, st - (gw - 1)) + lane, gc = st - gr;
+    if (gr <= min(gh - 1, st) && gc >= 0) {
+      const int gg = gr * gw + gc;
+      const int anchor = c_geom[pid][gg][4];
+      const int lidx = (anchor & 3) == 0 ? 1 + (anchor >> 2) : W.chosen[c_partitions[pid][anchor - 1]];
+      const int aidx = anchor < 4 ? 5 + anchor : W.chosen[c_partitions[pid][anchor - 4]];
+      const vp8a_mv lmv = W.cmv[lidx], amv = W.cmv[aidx];
+      const bool lez = mv_zero(lmv), aez = mv_zero(amv), lea = mv_eq(lmv, amv);
+      const int ctxi = (lea && lez) ? 4 : (lea ? 3 : (aez ? 2 : (lez ? 1 : 0)));
+      const double* mb = sbits + ctxi * 4;
+      const uint32_t* trow = W.table + gg * CMAX;
+      // LEFT, ABOVE, ZERO, then NEW; strict '<' keeps the first minimum.
+      const double j0 = (double)trow[lidx] + a.lambda * (mb[0] + 0.0);
+      const double j1 = (double)trow[aidx] + a.lambda * (mb[1] + 0.0);
+      const double j2 = (double)trow[0] + a.lambda * (mb[2] + 0.0);
+      double best_j = __longlong_as_double(0x7ff0000000000000LL);
+      int best_mode = VP8A_SUBMV_ZERO, best_col = 0;
+      if (j0 < best_j) {
+        best_j = j0;
+        best_mode = VP8A_SUBMV_LEFT;
+        best_col = lidx;
       }
-    }
-    if (!isfinite(best_j)) {
-      if (lane == 0) out->valid = 0;
-      return;
-    }
-    total_sad += trow[best_col];
-    total_bits += mb[best_mode];
-    if (best_mode == VP8A_SUBMV_NEW) total_bits += W.new_bits[gg];
-    __syncwarp();
-    if (lane == 0) {
+      if (j1 < best_j) {
+        best_j = j1;
+        best_mode = VP8A_SUBMV_ABOVE;
+        best_col = aidx;
+      }
+      if (j2 < best_j) {
+        best_j = j2;
+        best_mode = VP8A_SUBMV_ZERO;
+        best_col = 0;
+      }
+      if (W.new_ok[gg]) {
+        const double jn = (double)W.new_sad[gg] + a.lambda * (mb[3] + W.new_bits[gg]);
+        if (jn < best_j) {
+          best_j = jn;
+          best_mode = VP8A_SUBMV_NEW;
+          best_col = 9 + gg;
+        }
+      }
       W.chosen[gg] = (uint8_t)best_col;
+      W.bad[gg] = !isfinite(best_j);
+      W.sad[gg] = trow[best_col];
+      W.bits_a[gg] = mb[best_mode];
+      W.is_new[gg] = best_mode == VP8A_SUBMV_NEW;
       out->modes[gg] = (uint8_t)best_mode;
     }
     __syncwarp();
   }
-  const double partition_bits = mv_partition_bits(t, pid);
+  // Totals in the reference's group order (the f64 sum is order-sensitive).
   if (lane == 0) {
-    out->j = (double)total_sad + a.lambda * (partition_bits + total_bits);
-    for (int i = G; i < 16; i++) out->modes[i] = VP8A_SUBMV_ZERO;
-    out->valid = 1;
+    uint32_t total_sad = 0;
+    double total_bits = 0.0;
+    int valid = 1;
+    for (int gg = 0; gg < G; gg++) {
+      if (W.bad[gg]) {
+        valid = 0;
+        break;
+      }
+      total_sad += W.sad[gg];
+      total_bits += W.bits_a[gg];
+      if (W.is_new[gg]) total_bits += W.new_bits[gg];
+    }
+    out->valid = valid;
+    if (valid) {
+      const double partition_bits = mv_partition_bits(t, pid);
+      out->j = (double)total_sad + a.lambda * (partition_bits + total_bits);
+      for (int i = G; i < 16; i++) out->modes[i] = VP8A_SUBMV_ZERO;
+    }
   }
   if (lane < 16) out->split_mvs[lane] = W.cmv[W.chosen[c_partitions[pid][lane]]];
 }
@@ -435,38 +599,108 @@ __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// SAD of the 16x16 source against a staged 16x16 block.
-__device__ __forceinline__ uint32_t sad_block16(const uint8_t* blk, const uint8_t* src, int lane) {
-  const int row = lane >> 1, c0 = (lane & 1) * 8;
-  const uint32_t* b = (const uint32_t*)(blk + row * 16 + c0);
-  const uint32_t* sp = (const uint32_t*)(src + row * 16 + c0);
-  return __reduce_add_sync(FULL, __vsadu4(b[0], sp[0]) + __vsadu4(b[1], sp[1]));
+// ------------------------------------------------------ sub-pel stages
+
+// Offsets (row, col) of the eight refinement candidates in the reference's
+// order: (-1,-1) (-1,0) (-1,1) (0,-1) (0,1) (1,-1) (1,0) (1,1).
+__device__ __forceinline__ int cand_dr(int k) { return (k < 3) ? -1 : (k < 5 ? 0 : 1); }
+__device__ __forceinline__ int cand_dc(int k) { return (k == 0 || k == 3 || k == 5) ? -1 : ((k == 1 || k == 6) ? 0 : 1); }
+
+// The H, V and D half-pel planes around a whole-pel centre whose block
+// origin in the window is (bx, by) (the planes of half_plane_sads, filled
+// by the whole CTA).
+__device__ __forceinline__ void half_planes_cta(WarpScratch& S, int bx, int by, int tid, int nthreads) {
+  const int* f = c_sixtap[4];
+  for (int o = tid; o < 22 * 17 + 17 * 16; o += nthreads) {
+    if (o < 22 * 17) {
+      const int r = o / 17, i = o - r * 17;
+      const uint8_t* p = S.win + (by - 3 + r) * WS + bx + i - 3;
+      S.hp[o] = (uint8_t)interp6(f, p[0], p[1], p[2], p[3], p[4], p[5]);
+    } else {
+      const int q = o - 22 * 17, r = q >> 4, c = q & 15;
+      const uint8_t* p = S.win + (by + r - 3) * WS + bx + c;
+      S.vp[q] = (uint8_t)interp6(f, p[0], p[WS], p[2 * WS], p[3 * WS], p[4 * WS], p[5 * WS]);
+    }
+  }
+  __syncthreads();
+  for (int o = tid; o < 17 * 17; o += nthreads) {
+    const int r = o / 17, i = o - r * 17;
+    const uint8_t* p = S.hp + r * 17 + i;
+    S.dp[o] = (uint8_t)interp6(f, p[0], p[17], p[34], p[51], p[68], p[85]);
+  }
 }
 
-__global__ void __launch_bounds__(MAX_REFS* WARPS_PER_REF * 32) analysis_kernel(AnArgs a) {
-  __shared__ RefSmem rs[MAX_REFS];
-  __shared__ SplitScratch ss[MAX_REFS * 4];
+// SAD of half-pel candidate k against the planes (one warp).
+__device__ __forceinline__ uint32_t half_cand_sad(const WarpScratch& S, int k, const uint8_t* src, int lane) {
+  const int dy = cand_dr(k), dx = cand_dc(k);
+  const int cx = dx > 0, cy = dy > 0;
+  const uint8_t* pl;
+  int st;
+  if (dy == 0) {
+    pl = S.hp + 3 * 17 + cx;
+    st = 17;
+  } else if (dx == 0) {
+    pl = S.vp + cy * 16;
+    st = 16;
+  } else {
+    pl = S.dp + cy * 17 + cx;
+    st = 17;
+  }
+  const int c = lane & 15, r0 = (lane >> 4) * 8;
+  uint32_t s = 0;
+#pragma unroll
+  for (int r = r0; r < r0 + 8; r++) {
+    const int d = (int)pl[r * st + c] - (int)src[r * 16 + c];
+    s += (uint32_t)(d < 0 ? -d : d);
+  }
+  return __reduce_add_sync(FULL, s);
+}
+
+struct __align__(16) WarpTemp {
+  uint8_t temp[21 * 16 + 16];  // six-tap first pass
+  uint8_t halo[21 * 24 + 24];  // out-of-window halo
+};
+
+// -------------------------------------------------------------- kernel
+
+constexpr int NW = 9;                 // warps per CTA (one reference)
+constexpr int AN_THREADS = NW * 32;
+static_assert(AN_THREADS >= 16 * FN, "one thread per field task");
+
+__global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  __shared__ RefSmem R;
+  __shared__ FieldSmem F;
+  __shared__ WarpTemp wt[NW];
+  __shared__ SplitScratch ss[4];
+  __shared__ __align__(16) uint16_t xs[MAX_BLOCKS][16];
   __shared__ __align__(16) uint8_t src[256];
   __shared__ double bit_cost[256];
   __shared__ double sbits[5 * 4];  // submv_ref_bits per context and mode
-  __shared__ MainOut mains[MAX_REFS];
-  __shared__ SplitOut splits[MAX_REFS][4];
-  __shared__ RefDec decs[MAX_REFS];
-  __shared__ MbInfoDev nb[3];  // above, left, aboveleft
+  __shared__ MainOut mo;
+  __shared__ uint32_t cand_sad[8];
+  __shared__ SplitOut splits[4];
+  __shared__ RefDec mydec;
+  __shared__ RefDec decs[MAX_REFS];  // rank 0: every reference's decision
+  __shared__ __align__(16) MbInfoDev nb[3];  // above, left, aboveleft
   __shared__ Census cen;
   __shared__ Plan plan;
   __shared__ int s_abort;
-  const int tid = threadIdx.x, nthreads = blockDim.x;
-  const int warp = tid >> 5, lane = tid & 31;
-  const int ref = warp / WARPS_PER_REF, role = warp % WARPS_PER_REF;  // role 0 = main, 1..4 = split pid
-  for (int i = tid; i < 256; i += nthreads) bit_cost[i] = a.bit_cost[i];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int k = (int)cl.block_rank();  // the reference this CTA searches
+  const int cid = blockIdx.x / a.n_refs, n_clusters = gridDim.x / a.n_refs;
+  const MePlane& P = a.refs[k];
+  for (int i = tid; i < 256; i += AN_THREADS) bit_cost[i] = a.bit_cost[i];
   __syncthreads();
   if (tid < 20) sbits[tid] = submv_ref_bits(bit_cost, c_submv_probs[tid >> 2], tid & 3);
-  const MbInfoDev border = {VP8A_REF_INTRA, 0, 0, 0, {0, 0}, {}};
+  uint32_t* dec_slot = (uint32_t*)cl.map_shared_rank(&decs[k], 0);
+  const int* abort0 = cl.map_shared_rank(&s_abort, 0);
 
-  for (int r = blockIdx.x; r < a.mb_rows; r += gridDim.x) {
+  for (int r = cid; r < a.mb_rows; r += n_clusters) {
     for (int c = 0; c < a.mb_cols; c++) {
-      if (tid == 0) {
+      // Rank 0 waits for the row above; the cluster follows its verdict.
+      if (k == 0 && tid == 0) {
         int abort = 0;
         if (r > 0) {
           const unsigned need = (unsigned)min(c + 2, a.mb_cols);
@@ -484,17 +718,24 @@ __global__ void __launch_bounds__(MAX_REFS* WARPS_PER_REF * 32) analysis_kernel(
         }
         s_abort = abort;
       }
-      __syncthreads();
-      if (s_abort) return;
-      // Neighbour records and the edge-replicated source MB
-      // (extract_mb, src/encoder.rs:5549).
-      if (tid < 3) {
-        const int nr = tid == 1 ? r : r - 1, nc = tid == 0 ? c : c - 1;
-        nb[tid] = (nr >= 0 && nc >= 0) ? a.infos[(size_t)nr * a.mb_cols + nc] : border;
+      cl.sync();
+      if (*abort0) {
+        cl.sync();  // rank 0's shared memory stays live until every CTA has read it
+        return;
       }
-      if (tid < 256) {
-        const int y = min(r * 16 + (tid >> 4), a.fh - 1), x = min(c * 16 + (tid & 15), a.fw - 1);
-        src[tid] = a.fy[(size_t)y * a.fys + x];
+      // Neighbour records (read past L1: rank 0 and other clusters write
+      // them) and the edge-replicated source MB (extract_mb,
+      // src/encoder.rs:5549).
+      if (tid < 3 * 18) {
+        const int n = tid / 18, w = tid - n * 18;
+        const int nr = n == 1 ? r : r - 1, nc = n == 0 ? c : c - 1;
+        const uint32_t* g = (const uint32_t*)(a.infos + (size_t)nr * a.mb_cols + nc);
+        // Outside the frame: an intra record (ref_frame in byte 0, the rest 0).
+        ((uint32_t*)&nb[n])[w] = (nr >= 0 && nc >= 0) ? __ldcg(g + w) : (w == 0 ? (uint32_t)VP8A_REF_INTRA : 0u);
+      }
+      for (int i = tid; i < 256; i += AN_THREADS) {
+        const int y = min(r * 16 + (i >> 4), a.fh - 1), x = min(c * 16 + (i & 15), a.fw - 1);
+        src[i] = a.fy[(size_t)y * a.fys + x];
       }
       __syncthreads();
       const int mbx = c * 16, mby = r * 16;
@@ -523,153 +764,220 @@ __global__ void __launch_bounds__(MAX_REFS* WARPS_PER_REF * 32) analysis_kernel(
         plan = p;
       }
       __syncthreads();
-      stage<24>(a, rs, plan, mbx, mby, tid, nthreads);
+      stage_ref(P, R, plan, mbx, mby, a.words, tid, AN_THREADS);
       __syncthreads();
-      if (ref < a.n_refs) {
-        const MePlane& P = a.refs[ref];
-        RefSmem& R = rs[ref];
-        const vp8a_mv bp = cen.best_predictor;
-        if (role == 0) {
-          MainOut m;
-          m.sad_zero = sad_block16(R.blocks[0], src, lane);
-          m.whole = diamond(P, R.ws, plan.wx0, plan.wy0, mbx, mby, bp, 8, src, lane);
-          if (!half_refine_planes(R.ws, plan.wx0, plan.wy0, mbx, mby, m.whole.mv, src, lane, &m.half))
-            m.half = refine(P, R.ws, plan.wx0, plan.wy0, mbx, mby, m.whole.mv, 2, src, lane);
-          m.quarter = refine(P, R.ws, plan.wx0, plan.wy0, mbx, mby, m.half.mv, 1, src, lane, m.half.sad);
-          const int en_r = eighth(cen.nearest.row), en_c = eighth(cen.nearest.col);
-          m.sad_nearest = subpel_sad(R.halo_nearest, HS, en_c & 7, en_r & 7, src, R.ws.temp, lane);
-          const int er_r = eighth(cen.near_.row), er_c = eighth(cen.near_.col);
-          m.sad_near = subpel_sad(R.halo_near, HS, er_c & 7, er_r & 7, src, R.ws.temp, lane);
-          if (lane == 0) mains[ref] = m;
-        } else {
-          split_partition(a, bit_cost, sbits, P, R, plan, mbx, mby, src, bp, nb[0], nb[1], role - 1,
-                          ss[ref * 4 + role - 1], &splits[ref][role - 1], lane);
+      field_blocks(R.ws.win, src, F, tid);
+      __syncthreads();
+      field_sums(F, tid, AN_THREADS);
+      staged_block_sads(R, src, plan.nblocks, xs, tid, AN_THREADS);
+      __syncthreads();
+      const vp8a_mv bp = cen.best_predictor;
+      const int cxp = plan.wx0 + WIN_LEAD, cyp = plan.wy0 + WIN_LEAD;  // field centre (plane pixels)
+      const FieldView fv{&F, xs, &plan, mbx, mby, cxp, cyp};
+      if (warp == 0) {
+        // ZEROMV SAD and the whole-pel diamond (src/encoder.rs:8560-8576).
+        uint32_t z = 0;
+        if (lane < 16) z = xs[0][lane];
+        z = __reduce_add_sync(FULL, z);
+        const vp8a_search_result w =
+            diamond_field(F, P, R.ws.win, plan.wx0, plan.wy0, mbx, mby, cxp, cyp, bp, 8, src, lane);
+        if (lane == 0) {
+          mo.sad_zero = z;
+          mo.whole = w;
+        }
+      } else if (warp <= 4) {
+        split_partition(a, bit_cost, sbits, fv, P, src, bp, nb[0], nb[1], warp - 1, ss[warp - 1], &splits[warp - 1],
+                        lane);
+      } else if (warp == 5) {
+        const int er = eighth(cen.nearest.row), ec = eighth(cen.nearest.col);
+        const uint32_t sv = subpel_sad(R.halo_nearest, HS, ec & 7, er & 7, src, wt[5].temp, lane);
+        if (lane == 0) mo.sad_nearest = sv;
+      } else if (warp == 6) {
+        const int er = eighth(cen.near_.row), ec = eighth(cen.near_.col);
+        const uint32_t sv = subpel_sad(R.halo_near, HS, ec & 7, er & 7, src, wt[6].temp, lane);
+        if (lane == 0) mo.sad_near = sv;
+      }
+      __syncthreads();
+      // half_pixel_refine_luma around the whole-pel result: planes shared by
+      // the CTA, one candidate per warp, first strict minimum in order. For
+      // a whole-pel centre inside [-1020, 1020] no candidate is clamped.
+      {
+        const vp8a_mv hc = mo.whole.mv;
+        const int hbx = mbx + hc.col / 4 - plan.wx0, hby = mby + hc.row / 4 - plan.wy0;
+        const bool planes = hc.row >= -1020 && hc.row <= 1020 && hc.col >= -1020 && hc.col <= 1020 &&
+                            !(hc.row & 3) && !(hc.col & 3) && hbx >= 3 && hby >= 3 && hbx + 19 <= WS &&
+                            hby + 19 <= WS;
+        if (planes) {
+          half_planes_cta(R.ws, hbx, hby, tid, AN_THREADS);
+          __syncthreads();
+          if (warp < 8) {
+            const uint32_t sv = half_cand_sad(R.ws, warp, src, lane);
+            if (lane == 0) cand_sad[warp] = sv;
+          }
+          __syncthreads();
+          if (tid == 0) {
+            vp8a_mv best = hc;
+            uint32_t best_sad = mo.whole.sad;
+            for (int q = 0; q < 8; q++)
+              if (cand_sad[q] < best_sad) {
+                best_sad = cand_sad[q];
+                best.row = (int16_t)(hc.row + 2 * cand_dr(q));
+                best.col = (int16_t)(hc.col + 2 * cand_dc(q));
+              }
+            mo.half = vp8a_search_result{best, best_sad};
+          }
+        } else if (warp == 0) {
+          WarpScratch& S = R.ws;
+          const vp8a_search_result h = refine(P, S, plan.wx0, plan.wy0, mbx, mby, hc, 2, src, lane, mo.whole.sad);
+          if (lane == 0) mo.half = h;
         }
       }
-      if (ref < a.n_refs) {
-        // The reference's five warps meet; its main warp's lane 0 decides
-        // its mode (pick_mb_for_ref, src/encoder.rs:8598-8652).
-        asm volatile("bar.sync %0, %1;" ::"r"(1 + ref), "r"(WARPS_PER_REF * 32) : "memory");
-        if (role == 0 && lane == 0) {
-          const int k = ref;
-          const double* t = bit_cost;
-          const double lambda = a.lambda;
-          const uint8_t* p = cen.p;
-          const vp8a_mv bp = cen.best_predictor;
-          const MainOut& m = mains[k];
-          const double bits_zero = bb(t, p[0], 0);
-          const double bits_nearest = bb(t, p[0], 1) + bb(t, p[1], 0);
-          const double bits_near = bb(t, p[0], 1) + bb(t, p[1], 1) + bb(t, p[2], 0);
-          const double bits_new = bb(t, p[0], 1) + bb(t, p[1], 1) + bb(t, p[2], 1) + bb(t, p[3], 0);
-          const int dr = (int)m.quarter.mv.row - bp.row, dc = (int)m.quarter.mv.col - bp.col;
-          const bool in_range = dr >= -1023 && dr <= 1023 && dc >= -1023 && dc <= 1023;
-          const double bits_mv = in_range ? mv_bits_lookup(a.mvbits, 0, dr) + mv_bits_lookup(a.mvbits, 1, dc)
-                                          : __longlong_as_double(0x7ff0000000000000LL);
-          const double j_zero = (double)m.sad_zero + lambda * bits_zero;
-          const double j_nearest = (double)m.sad_nearest + lambda * bits_nearest;
-          const double j_near = (double)m.sad_near + lambda * bits_near;
-          const double j_new = (double)m.quarter.sad + lambda * (bits_new + bits_mv);
-          int mode = VP8A_MODE_ZERO, pid = VP8A_PART_NONE;
-          vp8a_mv mv = {0, 0};
-          double cj = j_zero;
-          if (!mv_zero(cen.nearest) && j_nearest < cj) {
-            mode = VP8A_MODE_NEAREST;
-            mv = cen.nearest;
-            cj = j_nearest;
-          }
-          if (!mv_zero(cen.near_) && j_near < cj) {
-            mode = VP8A_MODE_NEAR;
-            mv = cen.near_;
-            cj = j_near;
-          }
-          if (in_range && !mv_zero(m.quarter.mv) && j_new < cj) {
-            mode = VP8A_MODE_NEW;
-            mv = m.quarter.mv;
-            cj = j_new;
-          }
-          const double bits_split = bb(t, p[0], 1) + bb(t, p[1], 1) + bb(t, p[2], 1) + bb(t, p[3], 1);
-          int have = 0, sp = -1;
-          double sj = 0.0;
-          for (int qq = 0; qq < 4; qq++) {
-            if (!splits[k][qq].valid) continue;
-            const double total_j = splits[k][qq].j + lambda * bits_split;
-            // The stored best already includes bits_split and the
-            // comparison adds it again (src/encoder.rs:8679-8683).
-            if (!have || total_j < sj + lambda * bits_split) {
-              sj = total_j;
-              sp = qq;
-              have = 1;
+      __syncthreads();
+      // quarter_pixel_refine_luma around the half-pel result: one candidate
+      // per warp, the centre's SAD is the half-pel result's.
+      {
+        const vp8a_mv qc = mo.half.mv;
+        if (warp < 8) {
+          const int16_t rr = clamp_component(qc.row + cand_dr(warp)), cc = clamp_component(qc.col + cand_dc(warp));
+          const uint32_t sv = sad_at_mv(P, R.ws.win, wt[warp].temp, wt[warp].halo, plan.wx0, plan.wy0, mbx, mby, rr,
+                                        cc, src, lane);
+          if (lane == 0) cand_sad[warp] = sv;
+        }
+        __syncthreads();
+        if (tid == 0) {
+          vp8a_mv best = qc;
+          uint32_t best_sad = mo.half.sad;
+          for (int q = 0; q < 8; q++)
+            if (cand_sad[q] < best_sad) {
+              best_sad = cand_sad[q];
+              best.row = clamp_component(qc.row + cand_dr(q));
+              best.col = clamp_component(qc.col + cand_dc(q));
             }
-          }
-          if (have && sj < cj) {
-            mode = VP8A_MODE_SPLIT;
-            mv = splits[k][sp].split_mvs[15];
-            cj = sj;
-            pid = sp;
-          }
-          // ref_frame_tree_bits(ref, 128, 128) (src/encoder.rs:9108).
-          const uint8_t id = a.ref_ids[k];
-          const double rbits = id == VP8A_REF_LAST ? bb(t, 128, 0)
-                               : id == VP8A_REF_GOLDEN ? bb(t, 128, 1) + bb(t, 128, 0)
-                                                       : bb(t, 128, 1) + bb(t, 128, 1);
-          const double total = cj + lambda * rbits;
-          if (a.trace) {
-            vp8a_ref_search tr;
-            tr.best_predictor = bp;
-            tr.nearest_mv = cen.nearest;
-            tr.near_mv = cen.near_;
-            tr.sad_zero = m.sad_zero;
-            tr.whole = m.whole;
-            tr.half = m.half;
-            tr.quarter = m.quarter;
-            tr.sad_nearest = m.sad_nearest;
-            tr.sad_near = m.sad_near;
-            tr.chosen_mode = (uint8_t)mode;
-            tr.split_partition = (uint8_t)pid;
-            tr.reserved[0] = tr.reserved[1] = 0;
-            tr.j = cj;
-            a.trace[((size_t)r * a.mb_cols + c) * a.n_refs + k] = tr;
-          }
-          decs[k] = RefDec{cj, total, mv, mode, pid};
+          mo.quarter = vp8a_search_result{best, best_sad};
         }
       }
       __syncthreads();
       if (tid == 0) {
+        // pick_mb_for_ref's mode decision (src/encoder.rs:8598-8652).
+        const double* t = bit_cost;
+        const double lambda = a.lambda;
+        const uint8_t* p = cen.p;
+        const MainOut& m = mo;
+        const double bits_zero = bb(t, p[0], 0);
+        const double bits_nearest = bb(t, p[0], 1) + bb(t, p[1], 0);
+        const double bits_near = bb(t, p[0], 1) + bb(t, p[1], 1) + bb(t, p[2], 0);
+        const double bits_new = bb(t, p[0], 1) + bb(t, p[1], 1) + bb(t, p[2], 1) + bb(t, p[3], 0);
+        const int dr = (int)m.quarter.mv.row - bp.row, dc = (int)m.quarter.mv.col - bp.col;
+        const bool in_range = dr >= -1023 && dr <= 1023 && dc >= -1023 && dc <= 1023;
+        const double bits_mv = in_range ? mv_bits_lookup(a.mvbits, 0, dr) + mv_bits_lookup(a.mvbits, 1, dc)
+                                        : __longlong_as_double(0x7ff0000000000000LL);
+        const double j_zero = (double)m.sad_zero + lambda * bits_zero;
+        const double j_nearest = (double)m.sad_nearest + lambda * bits_nearest;
+        const double j_near = (double)m.sad_near + lambda * bits_near;
+        const double j_new = (double)m.quarter.sad + lambda * (bits_new + bits_mv);
+        int mode = VP8A_MODE_ZERO, pid = VP8A_PART_NONE;
+        vp8a_mv mv = {0, 0};
+        double cj = j_zero;
+        if (!mv_zero(cen.nearest) && j_nearest < cj) {
+          mode = VP8A_MODE_NEAREST;
+          mv = cen.nearest;
+          cj = j_nearest;
+        }
+        if (!mv_zero(cen.near_) && j_near < cj) {
+          mode = VP8A_MODE_NEAR;
+          mv = cen.near_;
+          cj = j_near;
+        }
+        if (in_range && !mv_zero(m.quarter.mv) && j_new < cj) {
+          mode = VP8A_MODE_NEW;
+          mv = m.quarter.mv;
+          cj = j_new;
+        }
+        const double bits_split = bb(t, p[0], 1) + bb(t, p[1], 1) + bb(t, p[2], 1) + bb(t, p[3], 1);
+        int have = 0, sp = -1;
+        double sj = 0.0;
+        for (int qq = 0; qq < 4; qq++) {
+          if (!splits[qq].valid) continue;
+          const double total_j = splits[qq].j + lambda * bits_split;
+          // The stored best already includes bits_split and the
+          // comparison adds it again (src/encoder.rs:8679-8683).
+          if (!have || total_j < sj + lambda * bits_split) {
+            sj = total_j;
+            sp = qq;
+            have = 1;
+          }
+        }
+        if (have && sj < cj) {
+          mode = VP8A_MODE_SPLIT;
+          mv = splits[sp].split_mvs[15];
+          cj = sj;
+          pid = sp;
+        }
+        // ref_frame_tree_bits(ref, 128, 128) (src/encoder.rs:9108).
+        const uint8_t id = a.ref_ids[k];
+        const double rbits = id == VP8A_REF_LAST ? bb(t, 128, 0)
+                             : id == VP8A_REF_GOLDEN ? bb(t, 128, 1) + bb(t, 128, 0)
+                                                     : bb(t, 128, 1) + bb(t, 128, 1);
+        const double total = cj + lambda * rbits;
+        if (a.trace) {
+          vp8a_ref_search tr;
+          tr.best_predictor = bp;
+          tr.nearest_mv = cen.nearest;
+          tr.near_mv = cen.near_;
+          tr.sad_zero = m.sad_zero;
+          tr.whole = m.whole;
+          tr.half = m.half;
+          tr.quarter = m.quarter;
+          tr.sad_nearest = m.sad_nearest;
+          tr.sad_near = m.sad_near;
+          tr.chosen_mode = (uint8_t)mode;
+          tr.split_partition = (uint8_t)pid;
+          tr.reserved[0] = tr.reserved[1] = 0;
+          tr.j = cj;
+          a.trace[((size_t)r * a.mb_cols + c) * a.n_refs + k] = tr;
+        }
+        mydec.j = cj;
+        mydec.total = total;
+        mydec.mv = mv;
+        mydec.mode = mode;
+        mydec.pid = pid;
+        for (int i = 0; i < 16; i++) {
+          mydec.split_mvs[i] = mode == VP8A_MODE_SPLIT ? splits[pid].split_mvs[i] : vp8a_mv{0, 0};
+          mydec.submv_modes[i] = mode == VP8A_MODE_SPLIT ? splits[pid].modes[i] : (uint8_t)VP8A_SUBMV_ZERO;
+        }
+      }
+      __syncthreads();
+      if (tid < (int)(sizeof(RefDec) / 4)) dec_slot[tid] = ((const uint32_t*)&mydec)[tid];
+      cl.sync();
+      if (k == 0 && tid == 0) {
         // decide_mb_exhaustive's reference comparison: first strict minimum
         // of J + ref_frame_tree_bits in reference order.
         double best_total = __longlong_as_double(0x7ff0000000000000LL);
-        int best_k = -1, best_mode = 0, best_pid = VP8A_PART_NONE;
-        vp8a_mv best_mv = {0, 0};
-        double best_j = 0.0;
-        for (int k = 0; k < a.n_refs; k++) {
-          const RefDec& rd = decs[k];
-          if (rd.total < best_total) {
-            best_total = rd.total;
-            best_k = k;
-            best_mode = rd.mode;
-            best_mv = rd.mv;
-            best_j = rd.j;
-            best_pid = rd.pid;
+        int best_k = -1;
+        for (int q = 0; q < a.n_refs; q++)
+          if (decs[q].total < best_total) {
+            best_total = decs[q].total;
+            best_k = q;
           }
-        }
         vp8a_mb_decision d;
         memset(&d, 0, sizeof d);
         MbInfoDev info;
         memset(&info, 0, sizeof info);
         if (best_k >= 0) {
+          const RefDec& b = decs[best_k];
           d.ref_frame = a.ref_ids[best_k];
-          d.mode = (uint8_t)best_mode;
-          d.partition = (uint8_t)best_pid;
-          d.mv = best_mv;
-          d.j = best_j;
-          d.total = best_total;
+          d.mode = (uint8_t)b.mode;
+          d.partition = (uint8_t)b.pid;
+          d.mv = b.mv;
+          d.j = b.j;
+          d.total = b.total;
           for (int i = 0; i < 16; i++) {
-            d.split_mvs[i] = best_mode == VP8A_MODE_SPLIT ? splits[best_k][best_pid].split_mvs[i] : vp8a_mv{0, 0};
-            d.submv_modes[i] = best_mode == VP8A_MODE_SPLIT ? splits[best_k][best_pid].modes[i] : (uint8_t)VP8A_SUBMV_ZERO;
+            d.split_mvs[i] = b.split_mvs[i];
+            d.submv_modes[i] = b.submv_modes[i];
           }
           info.ref_frame = d.ref_frame;
-          info.mv = best_mv;
-          info.is_split = best_mode == VP8A_MODE_SPLIT;
+          info.mv = b.mv;
+          info.is_split = b.mode == VP8A_MODE_SPLIT;
           info.has_split_mvs = info.is_split;
           for (int i = 0; i < 16; i++) info.split_mvs[i] = d.split_mvs[i];
         }
@@ -678,7 +986,7 @@ __global__ void __launch_bounds__(MAX_REFS* WARPS_PER_REF * 32) analysis_kernel(
         __threadfence();
         st_release(&a.progress[r], (unsigned)(c + 1));
       }
-      // The next MB's first barrier orders these shared results.
+      // The next MB's first cluster barrier orders these results.
     }
   }
 }
@@ -772,15 +1080,42 @@ extern "C" vp8a_status vp8a_analyse_inter_frame(vp8a_ctx* ctx, const vp8a_i420* 
   a.dec = (vp8a_mb_decision*)ddec;
   a.trace = (vp8a_ref_search*)dtr;
   a.spin_limit = 1ull << 24;
-  const int threads = MAX_REFS * WARPS_PER_REF * 32;
-  int per_sm = 0;
-  VP8A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, analysis_kernel, threads, 0));
-  if (per_sm < 1) {
+  a.words = 1;
+  for (uint32_t k = 0; k < n_refs; k++)
+    if ((uintptr_t)a.refs[k].plane % 4 != 0 || a.refs[k].stride % 4 != 0) a.words = 0;
+  // One CTA per reference, the references of one MB row in one thread-block
+  // cluster; the shared-memory request keeps one CTA per SM so that the
+  // reference searches of an MB do not compete for issue slots.
+  cudaFuncAttributes fa;
+  VP8A_CUDA(cudaFuncGetAttributes(&fa, analysis_kernel));
+  int smem_sm = 0;
+  VP8A_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
+  const int pad = std::max(0, smem_sm / 2 + 1 - (int)fa.sharedSizeBytes);
+  VP8A_CUDA(cudaFuncSetAttribute(analysis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, pad));
+  VP8A_CUDA(cudaFuncSetAttribute(analysis_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 0));
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = n_refs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.blockDim = dim3(AN_THREADS);
+  cfg.dynamicSmemBytes = (size_t)pad;
+  cfg.stream = ctx->stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cfg.gridDim = dim3(n_refs * (unsigned)mb_rows);
+  int max_clusters = 0;
+  VP8A_CUDA(cudaOccupancyMaxActiveClusters(&max_clusters, analysis_kernel, &cfg));
+  if (max_clusters < 1) {
     vp8a::set_error("analysis kernel cannot be resident");
     return VP8A_E_CUDA;
   }
-  const int grid = std::min(mb_rows, per_sm * ctx->sm_count);
-  analysis_kernel<<<grid, threads, 0, ctx->stream>>>(a);
+  // Every cluster must be resident at once: rows are handed out round-robin
+  // and a row waits on the one above it.
+  const int n_clusters = std::min(mb_rows, max_clusters);
+  cfg.gridDim = dim3(n_refs * (unsigned)n_clusters);
+  VP8A_CUDA(cudaLaunchKernelEx(&cfg, analysis_kernel, a));
   VP8A_CUDA(cudaGetLastError());
   ctx->launches++;
   if ((s = vp8a::check_device_status(ctx)) != VP8A_OK) return s;

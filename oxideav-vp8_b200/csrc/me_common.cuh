@@ -137,26 +137,33 @@ __device__ __forceinline__ uint32_t subpel_sad(const uint8_t* h, int hs, int mx,
 
 // mb_luma_sad_at_mv (src/motion_search.rs:470-529) for the MB at plane
 // pixel (mbx, mby), served from the window when it covers the candidate.
-__device__ __forceinline__ uint32_t sad_at_mv(const MePlane& P, WarpScratch& S, int wx0, int wy0, int mbx,
-                                              int mby, int16_t mv_row, int16_t mv_col, const uint8_t* src,
-                                              int lane) {
+// `temp` (21 x 16 bytes) and `halo` (21 x 24) are the warp's own scratch.
+__device__ __forceinline__ uint32_t sad_at_mv(const MePlane& P, const uint8_t* win, uint8_t* temp, uint8_t* halo,
+                                              int wx0, int wy0, int mbx, int mby, int16_t mv_row, int16_t mv_col,
+                                              const uint8_t* src, int lane) {
   int er = eighth(mv_row), ec = eighth(mv_col);
   int mx = ec & 7, my = er & 7;
   int bx = mbx + (ec >> 3), by = mby + (er >> 3);
-  if (mx == 0 && my == 0) return sad_whole_at(P, S.win, wx0, wy0, bx, by, src, lane);
+  if (mx == 0 && my == 0) return sad_whole_at(P, win, wx0, wy0, bx, by, src, lane);
   int hx = bx - 2, hy = by - 2;
   int lx = hx - wx0, ly = hy - wy0;
   if (lx >= 0 && ly >= 0 && lx <= WS - 21 && ly <= WS - 21)
-    return subpel_sad(S.win + ly * WS + lx, WS, mx, my, src, S.temp, lane);
+    return subpel_sad(win + ly * WS + lx, WS, mx, my, src, temp, lane);
   // Out-of-window halo: clamped fetch into scratch (fetch_luma_mb_halo).
   for (int r = 0; r < 21; r++) {
     int y = clampi(hy + r, 0, P.height - 1);
     const uint8_t* row = P.plane + (size_t)y * P.stride;
-    if (lane < 21) S.halo[r * 24 + lane] = row[clampi(hx + lane, 0, P.width - 1)];
+    if (lane < 21) halo[r * 24 + lane] = row[clampi(hx + lane, 0, P.width - 1)];
   }
   __syncwarp();
-  uint32_t s = subpel_sad(S.halo, 24, mx, my, src, S.temp, lane);
+  uint32_t s = subpel_sad(halo, 24, mx, my, src, temp, lane);
   return s;
+}
+
+__device__ __forceinline__ uint32_t sad_at_mv(const MePlane& P, WarpScratch& S, int wx0, int wy0, int mbx,
+                                              int mby, int16_t mv_row, int16_t mv_col, const uint8_t* src,
+                                              int lane) {
+  return sad_at_mv(P, S.win, S.temp, S.halo, wx0, wy0, mbx, mby, mv_row, mv_col, src, lane);
 }
 
 // small_diamond_search_luma (src/motion_search.rs:381-442). Each round
