@@ -107,19 +107,18 @@ struct SplitOut {
 // anchors 0/4/8/12, 5..8 = ABOVE vectors of the top-row anchors 0..3,
 // 9..24 = the NEW4X4 result of group 0..15.
 struct SplitScratch {
-  uint32_t table[16 * CMAX];  // group g's SAD at column m: table[g * CMAX + m]
-  vp8a_mv cmv[CMAX];
+  double table[16 * CMAX];    // group g's SAD at column m (exact in f64): table[g * CMAX + m]
+  double new_cost[16 * 5];    // lambda * (NEW4X4 mode bits of context x + group g's vector bits)
   double new_bits[16];        // NEW4X4 vector bits of group g (when new_ok)
+  double bits_a[16];          // group g's sub-MV reference bits
+  vp8a_mv cmv[CMAX];
   uint32_t new_sad[16];
+  uint32_t sad[16];           // group g's SAD at its chosen vector
   uint8_t new_ok[16];         // group g's NEW differential lies in [-1023, 1023]
   uint8_t chosen[16];         // column each group chose
-  double bits_a[16];          // group g's sub-MV reference bits
-  uint32_t sad[16];           // group g's SAD at its chosen vector
   uint8_t is_new[16];         // group g chose NEW4X4 (adds new_bits[g])
   uint8_t bad[16];            // group g had no finite choice
-  int colpos[CMAX];           // column m: field position, -(j+1) = staged block j, COL_DIRECT
 };
-constexpr int COL_DIRECT = -1000;
 struct Plan {
   int wx0, wy0;        // window origin (plane pixels)
   int hn_x, hn_y;      // NEAREST halo origin
@@ -127,17 +126,6 @@ struct Plan {
   int nblocks;
   int box[MAX_BLOCKS], boy[MAX_BLOCKS];  // block integer offsets
 };
-
-// Geometry of SPLITMV group g of partition p (PartitionGroups::build,
-// src/encoder.rs:7912-7980): row0, col0, width, height, anchor.
-__constant__ int8_t c_geom[4][16][5] = {
-    {{0, 0, 16, 8, 0}, {8, 0, 16, 8, 8}},
-    {{0, 0, 8, 16, 0}, {0, 8, 8, 16, 2}},
-    {{0, 0, 8, 8, 0}, {0, 8, 8, 8, 2}, {8, 0, 8, 8, 8}, {8, 8, 8, 8, 10}},
-    {{0, 0, 4, 4, 0},   {0, 4, 4, 4, 1},   {0, 8, 4, 4, 2},   {0, 12, 4, 4, 3},
-     {4, 0, 4, 4, 4},   {4, 4, 4, 4, 5},   {4, 8, 4, 4, 6},   {4, 12, 4, 4, 7},
-     {8, 0, 4, 4, 8},   {8, 4, 4, 4, 9},   {8, 8, 4, 4, 10},  {8, 12, 4, 4, 11},
-     {12, 0, 4, 4, 12}, {12, 4, 4, 4, 13}, {12, 8, 4, 4, 14}, {12, 12, 4, 4, 15}}};
 
 __device__ __forceinline__ int int_off(int16_t v) { return eighth(v) >> 3; }
 
@@ -347,7 +335,10 @@ __constant__ uint32_t c_need_cols[4] = {
     (1u << 0) | (1u << 1) | (1u << 3) | (1u << 5) | (1u << 7) | (0xfu << 9),  // Quarters: 0, 2, 8, 10
     0x1ffffffu};                                                   // Mv16: every column
 
-// 4x4 blocks of group g of partition p, as a bit mask over raster blocks.
+// 4x4 blocks of group g of partition p, as a bit mask over raster blocks
+// (PartitionGroups::build, src/encoder.rs:7912-7980). Groups are numbered
+// in raster order over the partition's gh x gw group grid: TopBottom 2x1,
+// LeftRight 1x2, Quarters 2x2, Mv16 4x4.
 __constant__ uint16_t c_group_blocks[4][16] = {
     {0x00ff, 0xff00},
     {0x3333, 0xcccc},
@@ -434,32 +425,66 @@ __device__ __forceinline__ double mv_partition_bits(const double* t, int pid) {
 // it: sbits[ctx * 4 + mode] = submv_ref_bits of each context and mode, and
 // each group's NEW vector bits. Every value is the same expression the
 // reference evaluates, so the chain's sums are unchanged.
-__device__ void split_partition(const AnArgs& a, const double* t, const double* sbits, const FieldView& fv,
-                                const MePlane& P, const uint8_t* src, vp8a_mv bp, const MbInfoDev& above,
-                                const MbInfoDev& left, int pid, SplitScratch& W, SplitOut* out, int lane) {
+__device__ void split_partition(const AnArgs& a, const double* t, const double* sbits, const double* lterm,
+                                const FieldView& fv, const MePlane& P, const uint8_t* src, vp8a_mv bp,
+                                const MbInfoDev& above, const MbInfoDev& left, int pid, SplitScratch& W,
+                                SplitOut* out, int lane) {
   const int G = pid == 3 ? 16 : (pid == 2 ? 4 : 2);
+  const int goff = pid == 0 ? 0 : (pid == 1 ? 2 : 4);
   if (lane < G) {
     // group_small_diamond_search (src/encoder.rs:7812-7879): snap then
-    // clamp the centre; N, S, W, E clamped, not snapped; four rounds.
+    // clamp the centre; N, S, W, E clamped, not snapped; four rounds. Every
+    // candidate of a round lies within one pixel of the round's start, so
+    // the round reads that 3x3 neighbourhood first and replays the walk.
     const int g = lane;
     vp8a_mv best;
     best.row = (int16_t)clampi((bp.row / 4) * 4, -1023, 1023);
     best.col = (int16_t)clampi((bp.col / 4) * 4, -1023, 1023);
     uint32_t bs = group_sad(fv, P, src, pid, g, best);
+    const uint16_t* fbase = pid == 3 ? &fv.F->blk[0][g] : &fv.F->grp[0][goff + g];
+    const int fstride = pid == 3 ? 16 : 8;  // u16 entries per field position
     for (int it = 0; it < 4; it++) {
+      const int dx0 = fv.mbx + int_off(best.col) - fv.cxp, dy0 = fv.mby + int_off(best.row) - fv.cyp;
+      const vp8a_mv b0 = best;
+      const uint32_t r11 = bs;  // the SAD at the round's start
       bool improved = false;
       const int dr[4] = {-4, 4, 0, 0}, dc[4] = {0, 0, -4, 4};
+      if (dx0 > -FR && dx0 < FR && dy0 > -FR && dy0 < FR) {
+        // The round's 3x3 neighbourhood, read together.
+        const uint16_t* c0 = fbase + fpos(dx0, dy0) * fstride;
+        const uint32_t r00 = c0[(-FN - 1) * fstride], r01 = c0[-FN * fstride], r02 = c0[(-FN + 1) * fstride];
+        const uint32_t r10 = c0[-fstride], r12 = c0[fstride];
+        const uint32_t r20 = c0[(FN - 1) * fstride], r21 = c0[FN * fstride], r22 = c0[(FN + 1) * fstride];
 #pragma unroll
-      for (int d = 0; d < 4; d++) {
-        vp8a_mv c;
-        c.row = (int16_t)clampi(best.row + dr[d], -1023, 1023);
-        c.col = (int16_t)clampi(best.col + dc[d], -1023, 1023);
-        if (mv_eq(c, best)) continue;
-        const uint32_t sv = group_sad(fv, P, src, pid, g, c);
-        if (sv < bs) {
-          bs = sv;
-          best = c;
-          improved = true;
+        for (int d = 0; d < 4; d++) {
+          vp8a_mv c;
+          c.row = (int16_t)clampi(best.row + dr[d], -1023, 1023);
+          c.col = (int16_t)clampi(best.col + dc[d], -1023, 1023);
+          if (mv_eq(c, best)) continue;
+          const int ox = int_off(c.col) - int_off(b0.col), oy = int_off(c.row) - int_off(b0.row);
+          const uint32_t top = ox < 0 ? r00 : (ox == 0 ? r01 : r02);
+          const uint32_t mid = ox < 0 ? r10 : (ox == 0 ? r11 : r12);
+          const uint32_t bot = ox < 0 ? r20 : (ox == 0 ? r21 : r22);
+          const uint32_t sv = oy < 0 ? top : (oy == 0 ? mid : bot);
+          if (sv < bs) {
+            bs = sv;
+            best = c;
+            improved = true;
+          }
+        }
+      } else {
+#pragma unroll 1
+        for (int d = 0; d < 4; d++) {
+          vp8a_mv c;
+          c.row = (int16_t)clampi(best.row + dr[d], -1023, 1023);
+          c.col = (int16_t)clampi(best.col + dc[d], -1023, 1023);
+          if (mv_eq(c, best)) continue;
+          const uint32_t sv = group_sad(fv, P, src, pid, g, c);
+          if (sv < bs) {
+            bs = sv;
+            best = c;
+            improved = true;
+          }
         }
       }
       if (!improved) break;
@@ -468,8 +493,11 @@ __device__ void split_partition(const AnArgs& a, const double* t, const double* 
     W.new_sad[g] = bs;
     const int dr = (int)best.row - bp.row, dc = (int)best.col - bp.col;
     const bool ok = dr >= -1023 && dr <= 1023 && dc >= -1023 && dc <= 1023;
+    const double nb = ok ? mv_bits_lookup(a.mvbits, 0, dr) + mv_bits_lookup(a.mvbits, 1, dc) : 0.0;
     W.new_ok[g] = ok;
-    W.new_bits[g] = ok ? mv_bits_lookup(a.mvbits, 0, dr) + mv_bits_lookup(a.mvbits, 1, dc) : 0.0;
+    W.new_bits[g] = nb;
+#pragma unroll
+    for (int x = 0; x < 5; x++) W.new_cost[g * 5 + x] = a.lambda * (sbits[x * 4 + VP8A_SUBMV_NEW] + nb);
   }
   if (lane == 0) {
     W.cmv[0] = vp8a_mv{0, 0};
@@ -477,39 +505,31 @@ __device__ void split_partition(const AnArgs& a, const double* t, const double* 
     for (int k = 0; k < 4; k++) W.cmv[5 + k] = ext_above(above, k);
   }
   __syncwarp();
+  // The table, one column per lane: where the column's vector lands (the
+  // field, a staged block, or - never for in-range vectors - the plane),
+  // then every group's SAD there.
   const uint32_t need = c_need_cols[pid];
-  // Where each needed column's vector lands: the field, a staged block, or
-  // (never for in-range vectors) the plane.
   if (lane < CMAX && ((need >> lane) & 1u)) {
-    const vp8a_mv m = W.cmv[lane];
-    const int x = fv.mbx + int_off(m.col), y = fv.mby + int_off(m.row);
-    int cp = fpos(x - fv.cxp, y - fv.cyp);
-    if (cp < 0) {
-      cp = COL_DIRECT;
-      for (int j = 0; j < fv.pl->nblocks; j++)
-        if (fv.mbx + fv.pl->box[j] == x && fv.mby + fv.pl->boy[j] == y) {
-          cp = -(j + 1);
+    const int m = lane;
+    const vp8a_mv mv = W.cmv[m];
+    const int x = fv.mbx + int_off(mv.col), y = fv.mby + int_off(mv.row);
+    const int p = fpos(x - fv.cxp, y - fv.cyp);
+    int j = -1;
+    if (p < 0)
+      for (int q = 0; q < fv.pl->nblocks; q++)
+        if (fv.mbx + fv.pl->box[q] == x && fv.mby + fv.pl->boy[q] == y) {
+          j = q;
           break;
         }
+#pragma unroll
+    for (int g = 0; g < 16; g++) {
+      if (g >= G) break;
+      uint32_t v;
+      if (p >= 0) v = pid == 3 ? fv.F->blk[p][g] : fv.F->grp[p][goff + g];
+      else if (j >= 0) v = pid == 3 ? fv.xs[j][g] : group_sum(fv.xs[j], pid, g);
+      else v = direct_group_sad(P, src, x, y, pid, g);
+      W.table[g * CMAX + m] = (double)v;
     }
-    W.colpos[lane] = cp;
-  }
-  __syncwarp();
-  const int goff = pid == 0 ? 0 : (pid == 1 ? 2 : 4);
-  for (int q = lane; q < G * CMAX; q += 32) {
-    const int g = q / CMAX, m = q - g * CMAX;
-    if (!((need >> m) & 1u)) continue;
-    const int cp = W.colpos[m];
-    uint32_t v;
-    if (cp >= 0) {
-      v = pid == 3 ? fv.F->blk[cp][g] : fv.F->grp[cp][goff + g];
-    } else if (cp != COL_DIRECT) {
-      v = pid == 3 ? fv.xs[-cp - 1][g] : group_sum(fv.xs[-cp - 1], pid, g);
-    } else {
-      const vp8a_mv mm = W.cmv[m];
-      v = direct_group_sad(P, src, fv.mbx + int_off(mm.col), fv.mby + int_off(mm.row), pid, g);
-    }
-    W.table[q] = v;
   }
   __syncwarp();
   // The sub-MV choice. A group's LEFT/ABOVE come from the group to its left
@@ -520,18 +540,22 @@ __device__ void split_partition(const AnArgs& a, const double* t, const double* 
     const int gr = max(0, st - (gw - 1)) + lane, gc = st - gr;
     if (gr <= min(gh - 1, st) && gc >= 0) {
       const int gg = gr * gw + gc;
-      const int anchor = c_geom[pid][gg][4];
-      const int lidx = (anchor & 3) == 0 ? 1 + (anchor >> 2) : W.chosen[c_partitions[pid][anchor - 1]];
-      const int aidx = anchor < 4 ? 5 + anchor : W.chosen[c_partitions[pid][anchor - 4]];
+      // The group's top-left block; the blocks left of and above it belong
+      // to the groups (gr, gc - 1) and (gr - 1, gc), or lie outside the MB.
+      const int anchor = gr * (4 / gh) * 4 + gc * (4 / gw);
+      const int lidx = gc == 0 ? 1 + (anchor >> 2) : W.chosen[gg - 1];
+      const int aidx = gr == 0 ? 5 + anchor : W.chosen[gg - gw];
       const vp8a_mv lmv = W.cmv[lidx], amv = W.cmv[aidx];
       const bool lez = mv_zero(lmv), aez = mv_zero(amv), lea = mv_eq(lmv, amv);
       const int ctxi = (lea && lez) ? 4 : (lea ? 3 : (aez ? 2 : (lez ? 1 : 0)));
-      const double* mb = sbits + ctxi * 4;
-      const uint32_t* trow = W.table + gg * CMAX;
-      // LEFT, ABOVE, ZERO, then NEW; strict '<' keeps the first minimum.
-      const double j0 = (double)trow[lidx] + a.lambda * (mb[0] + 0.0);
-      const double j1 = (double)trow[aidx] + a.lambda * (mb[1] + 0.0);
-      const double j2 = (double)trow[0] + a.lambda * (mb[2] + 0.0);
+      const double* trow = W.table + gg * CMAX;
+      const double* lt = lterm + ctxi * 4;
+      // LEFT, ABOVE, ZERO, then NEW (sad + lambda * (mode bits + vector
+      // bits), the vector bits 0 for the first three); strict '<' keeps the
+      // first minimum.
+      const double j0 = trow[lidx] + lt[0];
+      const double j1 = trow[aidx] + lt[1];
+      const double j2 = trow[0] + lt[2];
       double best_j = __longlong_as_double(0x7ff0000000000000LL);
       int best_mode = VP8A_SUBMV_ZERO, best_col = 0;
       if (j0 < best_j) {
@@ -550,7 +574,7 @@ __device__ void split_partition(const AnArgs& a, const double* t, const double* 
         best_col = 0;
       }
       if (W.new_ok[gg]) {
-        const double jn = (double)W.new_sad[gg] + a.lambda * (mb[3] + W.new_bits[gg]);
+        const double jn = (double)W.new_sad[gg] + W.new_cost[gg * 5 + ctxi];
         if (jn < best_j) {
           best_j = jn;
           best_mode = VP8A_SUBMV_NEW;
@@ -559,35 +583,38 @@ __device__ void split_partition(const AnArgs& a, const double* t, const double* 
       }
       W.chosen[gg] = (uint8_t)best_col;
       W.bad[gg] = !isfinite(best_j);
-      W.sad[gg] = trow[best_col];
-      W.bits_a[gg] = mb[best_mode];
+      W.sad[gg] = (uint32_t)trow[best_col];
+      W.bits_a[gg] = sbits[ctxi * 4 + best_mode];
       W.is_new[gg] = best_mode == VP8A_SUBMV_NEW;
       out->modes[gg] = (uint8_t)best_mode;
     }
     __syncwarp();
   }
-  // Totals in the reference's group order (the f64 sum is order-sensitive).
+  // Totals in the reference's group order (the f64 sum is order-sensitive):
+  // lane g holds group g's terms, every lane sums them in order.
+  const bool mine = lane < G;
+  const double ba = mine ? W.bits_a[lane] : 0.0;
+  const double bn = mine && W.is_new[lane] ? W.new_bits[lane] : 0.0;
+  const int isn = mine ? W.is_new[lane] : 0, bad = mine ? W.bad[lane] : 0;
+  const uint32_t sd = mine ? W.sad[lane] : 0u;
+  const uint32_t total_sad = __reduce_add_sync(FULL, sd);
+  const unsigned any_bad = __ballot_sync(FULL, bad != 0), news = __ballot_sync(FULL, isn != 0);
+  double total_bits = 0.0;
+  for (int gg = 0; gg < G; gg++) {
+    const double x = __shfl_sync(FULL, ba, gg), y = __shfl_sync(FULL, bn, gg);
+    total_bits += x;
+    if ((news >> gg) & 1u) total_bits += y;
+  }
   if (lane == 0) {
-    uint32_t total_sad = 0;
-    double total_bits = 0.0;
-    int valid = 1;
-    for (int gg = 0; gg < G; gg++) {
-      if (W.bad[gg]) {
-        valid = 0;
-        break;
-      }
-      total_sad += W.sad[gg];
-      total_bits += W.bits_a[gg];
-      if (W.is_new[gg]) total_bits += W.new_bits[gg];
-    }
-    out->valid = valid;
-    if (valid) {
+    // The reference stops at the first group without a finite choice.
+    out->valid = any_bad == 0u;
+    if (any_bad == 0u) {
       const double partition_bits = mv_partition_bits(t, pid);
       out->j = (double)total_sad + a.lambda * (partition_bits + total_bits);
       for (int i = G; i < 16; i++) out->modes[i] = VP8A_SUBMV_ZERO;
     }
   }
-  if (lane < 16) out->split_mvs[lane] = W.cmv[W.chosen[c_partitions[pid][lane]]];
+  if (lane < 16) out->split_mvs[lane] = W.cmv[W.chosen[((lane >> 2) / (4 / gh)) * gw + (lane & 3) / (4 / gw)]];
 }
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
@@ -673,11 +700,13 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
   __shared__ RefSmem R;
   __shared__ FieldSmem F;
   __shared__ WarpTemp wt[NW];
-  __shared__ SplitScratch ss[4];
+  extern __shared__ __align__(16) uint8_t dyn_smem[];
+  SplitScratch* ss = (SplitScratch*)dyn_smem;  // [4], in the dynamic allocation
   __shared__ __align__(16) uint16_t xs[MAX_BLOCKS][16];
   __shared__ __align__(16) uint8_t src[256];
   __shared__ double bit_cost[256];
   __shared__ double sbits[5 * 4];  // submv_ref_bits per context and mode
+  __shared__ double lterm[5 * 4];  // lambda * (sbits + 0.0): the LEFT/ABOVE/ZERO cost terms
   __shared__ MainOut mo;
   __shared__ uint32_t cand_sad[8];
   __shared__ SplitOut splits[4];
@@ -693,7 +722,11 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
   const MePlane& P = a.refs[k];
   for (int i = tid; i < 256; i += AN_THREADS) bit_cost[i] = a.bit_cost[i];
   __syncthreads();
-  if (tid < 20) sbits[tid] = submv_ref_bits(bit_cost, c_submv_probs[tid >> 2], tid & 3);
+  if (tid < 20) {
+    const double b = submv_ref_bits(bit_cost, c_submv_probs[tid >> 2], tid & 3);
+    sbits[tid] = b;
+    lterm[tid] = a.lambda * (b + 0.0);
+  }
   uint32_t* dec_slot = (uint32_t*)cl.map_shared_rank(&decs[k], 0);
   const int* abort0 = cl.map_shared_rank(&s_abort, 0);
 
@@ -786,7 +819,7 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
           mo.whole = w;
         }
       } else if (warp <= 4) {
-        split_partition(a, bit_cost, sbits, fv, P, src, bp, nb[0], nb[1], warp - 1, ss[warp - 1], &splits[warp - 1],
+        split_partition(a, bit_cost, sbits, lterm, fv, P, src, bp, nb[0], nb[1], warp - 1, ss[warp - 1], &splits[warp - 1],
                         lane);
       } else if (warp == 5) {
         const int er = eighth(cen.nearest.row), ec = eighth(cen.nearest.col);
@@ -1090,7 +1123,7 @@ extern "C" vp8a_status vp8a_analyse_inter_frame(vp8a_ctx* ctx, const vp8a_i420* 
   VP8A_CUDA(cudaFuncGetAttributes(&fa, analysis_kernel));
   int smem_sm = 0;
   VP8A_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
-  const int pad = std::max(0, smem_sm / 2 + 1 - (int)fa.sharedSizeBytes);
+  const int pad = std::max((int)(4 * sizeof(SplitScratch)), smem_sm / 2 + 1 - (int)fa.sharedSizeBytes);
   VP8A_CUDA(cudaFuncSetAttribute(analysis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, pad));
   VP8A_CUDA(cudaFuncSetAttribute(analysis_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 0));
   cudaLaunchAttribute attr[1];
