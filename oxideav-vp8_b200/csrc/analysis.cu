@@ -78,6 +78,8 @@ struct __align__(16) RefSmem {
   uint8_t blocks[MAX_BLOCKS][256];      // read as 32-bit words (sad_block16)
 };
 static_assert(sizeof(RefSmem) % 16 == 0 && offsetof(RefSmem, blocks) % 16 == 0, "RefSmem alignment");
+static_assert(sizeof(WarpScratch) - offsetof(WarpScratch, temp) >= 3 * 22 * 16,
+              "the quarter-pel planes fit in the window's six-tap scratch");
 
 struct MainOut {
   uint32_t sad_zero, sad_nearest, sad_near;
@@ -107,7 +109,7 @@ struct SplitOut {
 // anchors 0/4/8/12, 5..8 = ABOVE vectors of the top-row anchors 0..3,
 // 9..24 = the NEW4X4 result of group 0..15.
 struct SplitScratch {
-  double table[16 * CMAX];    // group g's SAD at column m (exact in f64): table[g * CMAX + m]
+  double table[16 * 9];       // group g's SAD at staged column m < 9 (exact in f64): table[g * 9 + m]
   double new_cost[16 * 5];    // lambda * (NEW4X4 mode bits of context x + group g's vector bits)
   double new_bits[16];        // NEW4X4 vector bits of group g (when new_ok)
   double bits_a[16];          // group g's sub-MV reference bits
@@ -118,6 +120,7 @@ struct SplitScratch {
   uint8_t chosen[16];         // column each group chose
   uint8_t is_new[16];         // group g chose NEW4X4 (adds new_bits[g])
   uint8_t bad[16];            // group g had no finite choice
+  int colpos[CMAX];           // column m < 9: staged block index; m >= 9: field position or -1
 };
 struct Plan {
   int wx0, wy0;        // window origin (plane pixels)
@@ -426,7 +429,7 @@ __device__ __forceinline__ double mv_partition_bits(const double* t, int pid) {
 // each group's NEW vector bits. Every value is the same expression the
 // reference evaluates, so the chain's sums are unchanged.
 __device__ void split_partition(const AnArgs& a, const double* t, const double* sbits, const double* lterm,
-                                const FieldView& fv, const MePlane& P, const uint8_t* src, vp8a_mv bp,
+                                const double* mvb, const FieldView& fv, const MePlane& P, const uint8_t* src, vp8a_mv bp,
                                 const MbInfoDev& above, const MbInfoDev& left, int pid, SplitScratch& W,
                                 SplitOut* out, int lane) {
   const int G = pid == 3 ? 16 : (pid == 2 ? 4 : 2);
@@ -493,7 +496,7 @@ __device__ void split_partition(const AnArgs& a, const double* t, const double* 
     W.new_sad[g] = bs;
     const int dr = (int)best.row - bp.row, dc = (int)best.col - bp.col;
     const bool ok = dr >= -1023 && dr <= 1023 && dc >= -1023 && dc <= 1023;
-    const double nb = ok ? mv_bits_lookup(a.mvbits, 0, dr) + mv_bits_lookup(a.mvbits, 1, dc) : 0.0;
+    const double nb = ok ? mvb[dr + 1023] + mvb[MV_BITS_SPAN + dc + 1023] : 0.0;
     W.new_ok[g] = ok;
     W.new_bits[g] = nb;
 #pragma unroll
@@ -505,33 +508,42 @@ __device__ void split_partition(const AnArgs& a, const double* t, const double* 
     for (int k = 0; k < 4; k++) W.cmv[5 + k] = ext_above(above, k);
   }
   __syncwarp();
-  // The table, one column per lane: where the column's vector lands (the
-  // field, a staged block, or - never for in-range vectors - the plane),
-  // then every group's SAD there.
+  // Candidate SADs. Columns 0-8 (ZERO and the neighbours' vectors) are the
+  // staged blocks: their group SADs are tabled, (group, column) pairs over
+  // the lanes. Columns 9+ (the groups' NEW results) lie in the field and
+  // are read from it when the chain needs them.
   const uint32_t need = c_need_cols[pid];
-  if (lane < CMAX && ((need >> lane) & 1u)) {
-    const int m = lane;
-    const vp8a_mv mv = W.cmv[m];
+  if (lane < 9 + G && ((need >> lane) & 1u)) {
+    const vp8a_mv mv = W.cmv[lane];
     const int x = fv.mbx + int_off(mv.col), y = fv.mby + int_off(mv.row);
-    const int p = fpos(x - fv.cxp, y - fv.cyp);
-    int j = -1;
-    if (p < 0)
+    int cp = -1;
+    if (lane < 9) {
       for (int q = 0; q < fv.pl->nblocks; q++)
         if (fv.mbx + fv.pl->box[q] == x && fv.mby + fv.pl->boy[q] == y) {
-          j = q;
+          cp = q;
           break;
         }
-#pragma unroll
-    for (int g = 0; g < 16; g++) {
-      if (g >= G) break;
-      uint32_t v;
-      if (p >= 0) v = pid == 3 ? fv.F->blk[p][g] : fv.F->grp[p][goff + g];
-      else if (j >= 0) v = pid == 3 ? fv.xs[j][g] : group_sum(fv.xs[j], pid, g);
-      else v = direct_group_sad(P, src, x, y, pid, g);
-      W.table[g * CMAX + m] = (double)v;
+    } else {
+      cp = fpos(x - fv.cxp, y - fv.cyp);
     }
+    W.colpos[lane] = cp;
   }
   __syncwarp();
+  for (int q = lane; q < G * 9; q += 32) {
+    const int g = q / 9, m = q - g * 9;
+    if (!((need >> m) & 1u)) continue;
+    const int j = W.colpos[m];  // always staged: the plan stages every one of these vectors
+    W.table[q] = (double)(pid == 3 ? fv.xs[j][g] : group_sum(fv.xs[j], pid, g));
+  }
+  __syncwarp();
+  // Group g's SAD at column m.
+  auto cand = [&](int g, int m) -> double {
+    if (m < 9) return W.table[g * 9 + m];
+    const int p = W.colpos[m];
+    if (p >= 0) return (double)(pid == 3 ? fv.F->blk[p][g] : fv.F->grp[p][goff + g]);
+    const vp8a_mv mv = W.cmv[m];
+    return (double)direct_group_sad(P, src, fv.mbx + int_off(mv.col), fv.mby + int_off(mv.row), pid, g);
+  };
   // The sub-MV choice. A group's LEFT/ABOVE come from the group to its left
   // and above, so the groups of one anti-diagonal of the partition's group
   // grid are independent: step s decides them in parallel, one lane each.
@@ -548,30 +560,34 @@ __device__ void split_partition(const AnArgs& a, const double* t, const double* 
       const vp8a_mv lmv = W.cmv[lidx], amv = W.cmv[aidx];
       const bool lez = mv_zero(lmv), aez = mv_zero(amv), lea = mv_eq(lmv, amv);
       const int ctxi = (lea && lez) ? 4 : (lea ? 3 : (aez ? 2 : (lez ? 1 : 0)));
-      const double* trow = W.table + gg * CMAX;
       const double* lt = lterm + ctxi * 4;
+      const double tl = cand(gg, lidx), ta = cand(gg, aidx), tz = W.table[gg * 9];
       // LEFT, ABOVE, ZERO, then NEW (sad + lambda * (mode bits + vector
       // bits), the vector bits 0 for the first three); strict '<' keeps the
       // first minimum.
-      const double j0 = trow[lidx] + lt[0];
-      const double j1 = trow[aidx] + lt[1];
-      const double j2 = trow[0] + lt[2];
+      const double j0 = tl + lt[0];
+      const double j1 = ta + lt[1];
+      const double j2 = tz + lt[2];
       double best_j = __longlong_as_double(0x7ff0000000000000LL);
       int best_mode = VP8A_SUBMV_ZERO, best_col = 0;
+      double best_sad = tz;
       if (j0 < best_j) {
         best_j = j0;
         best_mode = VP8A_SUBMV_LEFT;
         best_col = lidx;
+        best_sad = tl;
       }
       if (j1 < best_j) {
         best_j = j1;
         best_mode = VP8A_SUBMV_ABOVE;
         best_col = aidx;
+        best_sad = ta;
       }
       if (j2 < best_j) {
         best_j = j2;
         best_mode = VP8A_SUBMV_ZERO;
         best_col = 0;
+        best_sad = tz;
       }
       if (W.new_ok[gg]) {
         const double jn = (double)W.new_sad[gg] + W.new_cost[gg * 5 + ctxi];
@@ -579,11 +595,12 @@ __device__ void split_partition(const AnArgs& a, const double* t, const double* 
           best_j = jn;
           best_mode = VP8A_SUBMV_NEW;
           best_col = 9 + gg;
+          best_sad = (double)W.new_sad[gg];
         }
       }
       W.chosen[gg] = (uint8_t)best_col;
       W.bad[gg] = !isfinite(best_j);
-      W.sad[gg] = (uint32_t)trow[best_col];
+      W.sad[gg] = (uint32_t)best_sad;
       W.bits_a[gg] = sbits[ctxi * 4 + best_mode];
       W.is_new[gg] = best_mode == VP8A_SUBMV_NEW;
       out->modes[gg] = (uint8_t)best_mode;
@@ -635,8 +652,8 @@ __device__ __forceinline__ int cand_dc(int k) { return (k == 0 || k == 3 || k ==
 
 // The H, V and D half-pel planes around a whole-pel centre whose block
 // origin in the window is (bx, by) (the planes of half_plane_sads, filled
-// by the whole CTA).
-__device__ __forceinline__ void half_planes_cta(WarpScratch& S, int bx, int by, int tid, int nthreads) {
+// by several warps): H and V first, then D from H.
+__device__ __forceinline__ void half_planes_hv(WarpScratch& S, int bx, int by, int tid, int nthreads) {
   const int* f = c_sixtap[4];
   for (int o = tid; o < 22 * 17 + 17 * 16; o += nthreads) {
     if (o < 22 * 17) {
@@ -649,7 +666,11 @@ __device__ __forceinline__ void half_planes_cta(WarpScratch& S, int bx, int by, 
       S.vp[q] = (uint8_t)interp6(f, p[0], p[WS], p[2 * WS], p[3 * WS], p[4 * WS], p[5 * WS]);
     }
   }
-  __syncthreads();
+}
+
+// The D plane, from H (after H is complete).
+__device__ __forceinline__ void half_planes_d(WarpScratch& S, int tid, int nthreads) {
+  const int* f = c_sixtap[4];
   for (int o = tid; o < 17 * 17; o += nthreads) {
     const int r = o / 17, i = o - r * 17;
     const uint8_t* p = S.hp + r * 17 + i;
@@ -683,6 +704,92 @@ __device__ __forceinline__ uint32_t half_cand_sad(const WarpScratch& S, int k, c
   return __reduce_add_sync(FULL, s);
 }
 
+// quarter_pixel_refine_luma's eight candidates around `qc` share three
+// horizontal six-tap planes, one per candidate column (the columns are
+// qc.col - 1, qc.col, qc.col + 1 quarter-pels; a column whose eighth-pel
+// fraction is 0 keeps the unfiltered pixels, the reference's identity
+// elision). Each candidate's prediction is then its vertical pass over its
+// column's plane: the same taps, the same 8-bit intermediate and the same
+// edge-clamped source as its own two-pass synthesis.
+struct QuarterGeom {
+  int ix[3], fx[3], iy[3], fy[3], iy0;
+};
+
+// Fills the geometry; false when the window does not cover every
+// candidate's halo.
+__device__ __forceinline__ bool quarter_geom(vp8a_mv qc, int mbx, int mby, int wx0, int wy0, QuarterGeom& q) {
+  int xmin = 1 << 30, xmax = -(1 << 30), ymin = 1 << 30, ymax = -(1 << 30);
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const int ec = eighth(clamp_component(qc.col + k - 1)), er = eighth(clamp_component(qc.row + k - 1));
+    q.ix[k] = mbx + (ec >> 3) - wx0;
+    q.fx[k] = ec & 7;
+    q.iy[k] = mby + (er >> 3) - wy0;
+    q.fy[k] = er & 7;
+    xmin = min(xmin, q.ix[k]);
+    xmax = max(xmax, q.ix[k]);
+    ymin = min(ymin, q.iy[k]);
+    ymax = max(ymax, q.iy[k]);
+  }
+  q.iy0 = ymin - 2;  // first plane row (window coordinates)
+  // Planes span window rows iy0 .. iy0 + 21 and columns ix - 2 .. ix + 18.
+  return xmin >= 2 && xmax + 19 <= WS && ymin >= 2 && ymin + 20 <= WS && ymax - ymin <= 1;
+}
+
+// Horizontal planes: qh[k * 352 + rr * 16 + c], rr = 0..21 from window row iy0.
+__device__ __forceinline__ void quarter_planes_h(const uint8_t* win, uint8_t* qh, const QuarterGeom& q, int t, int n) {
+  for (int o = t; o < 3 * 22 * 16; o += n) {
+    const int k = o / 352, rem = o - k * 352, rr = rem >> 4, c = rem & 15;
+    const uint8_t* p = win + (q.iy0 + rr) * WS + q.ix[k] + c;
+    int v;
+    if (q.fx[k]) {
+      const int* f = c_sixtap[q.fx[k]];
+      v = interp6(f, p[-2], p[-1], p[0], p[1], p[2], p[3]);
+    } else {
+      v = p[0];
+    }
+    qh[o] = (uint8_t)v;
+  }
+}
+
+// Vertical pass and SAD of candidate t >> 4 at column t & 15, reduced over
+// the half-warp; the SAD is valid on lane (t & 15) == 0 of each half-warp.
+__device__ __forceinline__ uint32_t quarter_vsad(const uint8_t* qh, const QuarterGeom& q, const uint8_t* src, int t) {
+  const int k = t >> 4, c = t & 15;
+  const int kc = cand_dc(k) + 1, kr = cand_dr(k) + 1;
+  const uint8_t* pl = qh + kc * 352 + (q.iy[kr] - 2 - q.iy0) * 16 + c;  // plane row of prediction row -2
+  const int fy = q.fy[kr];
+  uint32_t s = 0;
+  if (fy) {
+    const int* fp = c_sixtap[fy];
+    const int f0 = fp[0], f1 = fp[1], f2 = fp[2], f3 = fp[3], f4 = fp[4], f5 = fp[5];
+    int w0 = pl[0], w1 = pl[16], w2 = pl[32], w3 = pl[48], w4 = pl[64];
+#pragma unroll
+    for (int r = 0; r < 16; r++) {
+      const int w5 = pl[(r + 5) * 16];
+      const int a = w0 * f0 + w1 * f1 + w2 * f2 + w3 * f3 + w4 * f4 + w5 * f5;
+      const int v = clampi((a + 64) >> 7, 0, 255);
+      const int d = v - (int)src[r * 16 + c];
+      s += (uint32_t)(d < 0 ? -d : d);
+      w0 = w1;
+      w1 = w2;
+      w2 = w3;
+      w3 = w4;
+      w4 = w5;
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < 16; r++) {
+      const int d = (int)pl[(r + 2) * 16] - (int)src[r * 16 + c];
+      s += (uint32_t)(d < 0 ? -d : d);
+    }
+  }
+  const unsigned hm = (t & 16) ? 0xffff0000u : 0x0000ffffu;
+#pragma unroll
+  for (int o = 8; o >= 1; o >>= 1) s += __shfl_xor_sync(hm, s, o);
+  return s;
+}
+
 struct __align__(16) WarpTemp {
   uint8_t temp[21 * 16 + 16];  // six-tap first pass
   uint8_t halo[21 * 24 + 24];  // out-of-window halo
@@ -692,6 +799,11 @@ struct __align__(16) WarpTemp {
 
 constexpr int NW = 9;                 // warps per CTA (one reference)
 constexpr int AN_THREADS = NW * 32;
+constexpr int MAIN_WARPS = 5;         // warps 0 and 5-8: the MB search chain
+constexpr int MAIN_THREADS = MAIN_WARPS * 32;
+
+// Barrier 1: the main group only.
+__device__ __forceinline__ void main_sync() { asm volatile("bar.sync 1, %0;" ::"n"(MAIN_THREADS) : "memory"); }
 static_assert(AN_THREADS >= 16 * FN, "one thread per field task");
 
 __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
@@ -700,8 +812,11 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
   __shared__ RefSmem R;
   __shared__ FieldSmem F;
   __shared__ WarpTemp wt[NW];
+  // Dynamic shared memory: the four SPLITMV scratch areas, then this
+  // call's mv_component_bits table (2 x 2047 doubles).
   extern __shared__ __align__(16) uint8_t dyn_smem[];
-  SplitScratch* ss = (SplitScratch*)dyn_smem;  // [4], in the dynamic allocation
+  SplitScratch* ss = (SplitScratch*)dyn_smem;
+  double* mvb = (double*)(dyn_smem + 4 * sizeof(SplitScratch));
   __shared__ __align__(16) uint16_t xs[MAX_BLOCKS][16];
   __shared__ __align__(16) uint8_t src[256];
   __shared__ double bit_cost[256];
@@ -715,12 +830,14 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
   __shared__ __align__(16) MbInfoDev nb[3];  // above, left, aboveleft
   __shared__ Census cen;
   __shared__ Plan plan;
-  __shared__ int s_abort;
+  __shared__ int s_abort, s_qok;
+  __shared__ QuarterGeom s_qg;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int k = (int)cl.block_rank();  // the reference this CTA searches
   const int cid = blockIdx.x / a.n_refs, n_clusters = gridDim.x / a.n_refs;
   const MePlane& P = a.refs[k];
   for (int i = tid; i < 256; i += AN_THREADS) bit_cost[i] = a.bit_cost[i];
+  for (int i = tid; i < 2 * MV_BITS_SPAN; i += AN_THREADS) mvb[i] = a.mvbits[i];
   __syncthreads();
   if (tid < 20) {
     const double b = submv_ref_bits(bit_cost, c_submv_probs[tid >> 2], tid & 3);
@@ -807,48 +924,54 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
       const vp8a_mv bp = cen.best_predictor;
       const int cxp = plan.wx0 + WIN_LEAD, cyp = plan.wy0 + WIN_LEAD;  // field centre (plane pixels)
       const FieldView fv{&F, xs, &plan, mbx, mby, cxp, cyp};
-      if (warp == 0) {
-        // ZEROMV SAD and the whole-pel diamond (src/encoder.rs:8560-8576).
-        uint32_t z = 0;
-        if (lane < 16) z = xs[0][lane];
-        z = __reduce_add_sync(FULL, z);
-        const vp8a_search_result w =
-            diamond_field(F, P, R.ws.win, plan.wx0, plan.wy0, mbx, mby, cxp, cyp, bp, 8, src, lane);
-        if (lane == 0) {
-          mo.sad_zero = z;
-          mo.whole = w;
+      if (warp >= 1 && warp <= 4) {
+        split_partition(a, bit_cost, sbits, lterm, mvb, fv, P, src, bp, nb[0], nb[1], warp - 1, ss[warp - 1],
+                        &splits[warp - 1], lane);
+      } else {
+        // The main group (warps 0 and 5-8) runs the MB search chain while
+        // warps 1-4 score the SPLITMV partitions.
+        const int slot = warp == 0 ? 0 : warp - 4, mt = slot * 32 + lane;
+        if (warp == 0) {
+          // ZEROMV SAD and the whole-pel diamond (src/encoder.rs:8560-8576).
+          uint32_t z = 0;
+          if (lane < 16) z = xs[0][lane];
+          z = __reduce_add_sync(FULL, z);
+          const vp8a_search_result w =
+              diamond_field(F, P, R.ws.win, plan.wx0, plan.wy0, mbx, mby, cxp, cyp, bp, 8, src, lane);
+          if (lane == 0) {
+            mo.sad_zero = z;
+            mo.whole = w;
+          }
+        } else if (warp == 5) {
+          const int er = eighth(cen.nearest.row), ec = eighth(cen.nearest.col);
+          const uint32_t sv = subpel_sad(R.halo_nearest, HS, ec & 7, er & 7, src, wt[5].temp, lane);
+          if (lane == 0) mo.sad_nearest = sv;
+        } else if (warp == 6) {
+          const int er = eighth(cen.near_.row), ec = eighth(cen.near_.col);
+          const uint32_t sv = subpel_sad(R.halo_near, HS, ec & 7, er & 7, src, wt[6].temp, lane);
+          if (lane == 0) mo.sad_near = sv;
         }
-      } else if (warp <= 4) {
-        split_partition(a, bit_cost, sbits, lterm, fv, P, src, bp, nb[0], nb[1], warp - 1, ss[warp - 1], &splits[warp - 1],
-                        lane);
-      } else if (warp == 5) {
-        const int er = eighth(cen.nearest.row), ec = eighth(cen.nearest.col);
-        const uint32_t sv = subpel_sad(R.halo_nearest, HS, ec & 7, er & 7, src, wt[5].temp, lane);
-        if (lane == 0) mo.sad_nearest = sv;
-      } else if (warp == 6) {
-        const int er = eighth(cen.near_.row), ec = eighth(cen.near_.col);
-        const uint32_t sv = subpel_sad(R.halo_near, HS, ec & 7, er & 7, src, wt[6].temp, lane);
-        if (lane == 0) mo.sad_near = sv;
-      }
-      __syncthreads();
-      // half_pixel_refine_luma around the whole-pel result: planes shared by
-      // the CTA, one candidate per warp, first strict minimum in order. For
-      // a whole-pel centre inside [-1020, 1020] no candidate is clamped.
-      {
+        main_sync();
+        // half_pixel_refine_luma around the whole-pel result: planes shared
+        // by the group, candidates spread over its warps, first strict
+        // minimum in order. For a whole-pel centre inside [-1020, 1020] no
+        // candidate is clamped.
         const vp8a_mv hc = mo.whole.mv;
         const int hbx = mbx + hc.col / 4 - plan.wx0, hby = mby + hc.row / 4 - plan.wy0;
         const bool planes = hc.row >= -1020 && hc.row <= 1020 && hc.col >= -1020 && hc.col <= 1020 &&
                             !(hc.row & 3) && !(hc.col & 3) && hbx >= 3 && hby >= 3 && hbx + 19 <= WS &&
                             hby + 19 <= WS;
         if (planes) {
-          half_planes_cta(R.ws, hbx, hby, tid, AN_THREADS);
-          __syncthreads();
-          if (warp < 8) {
-            const uint32_t sv = half_cand_sad(R.ws, warp, src, lane);
-            if (lane == 0) cand_sad[warp] = sv;
+          half_planes_hv(R.ws, hbx, hby, mt, MAIN_THREADS);
+          main_sync();
+          half_planes_d(R.ws, mt, MAIN_THREADS);
+          main_sync();
+          for (int q = slot; q < 8; q += MAIN_WARPS) {
+            const uint32_t sv = half_cand_sad(R.ws, q, src, lane);
+            if (lane == 0) cand_sad[q] = sv;
           }
-          __syncthreads();
-          if (tid == 0) {
+          main_sync();
+          if (mt == 0) {
             vp8a_mv best = hc;
             uint32_t best_sad = mo.whole.sad;
             for (int q = 0; q < 8; q++)
@@ -858,26 +981,37 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
                 best.col = (int16_t)(hc.col + 2 * cand_dc(q));
               }
             mo.half = vp8a_search_result{best, best_sad};
+            s_qok = quarter_geom(best, mbx, mby, plan.wx0, plan.wy0, s_qg);
           }
         } else if (warp == 0) {
-          WarpScratch& S = R.ws;
-          const vp8a_search_result h = refine(P, S, plan.wx0, plan.wy0, mbx, mby, hc, 2, src, lane, mo.whole.sad);
-          if (lane == 0) mo.half = h;
+          const vp8a_search_result h = refine(P, R.ws, plan.wx0, plan.wy0, mbx, mby, hc, 2, src, lane, mo.whole.sad);
+          if (lane == 0) {
+            mo.half = h;
+            s_qok = quarter_geom(h.mv, mbx, mby, plan.wx0, plan.wy0, s_qg);
+          }
         }
-      }
-      __syncthreads();
-      // quarter_pixel_refine_luma around the half-pel result: one candidate
-      // per warp, the centre's SAD is the half-pel result's.
-      {
+        main_sync();
+        // quarter_pixel_refine_luma around the half-pel result; the centre's
+        // SAD is the half-pel result's.
         const vp8a_mv qc = mo.half.mv;
-        if (warp < 8) {
-          const int16_t rr = clamp_component(qc.row + cand_dr(warp)), cc = clamp_component(qc.col + cand_dc(warp));
-          const uint32_t sv = sad_at_mv(P, R.ws.win, wt[warp].temp, wt[warp].halo, plan.wx0, plan.wy0, mbx, mby, rr,
-                                        cc, src, lane);
-          if (lane == 0) cand_sad[warp] = sv;
+        if (s_qok) {
+          uint8_t* qh = R.ws.temp;  // the six-tap scratch and half planes are free now
+          quarter_planes_h(R.ws.win, qh, s_qg, mt, MAIN_THREADS);
+          main_sync();
+          if (mt < 128) {
+            const uint32_t sv = quarter_vsad(qh, s_qg, src, mt);
+            if ((mt & 15) == 0) cand_sad[mt >> 4] = sv;
+          }
+        } else {
+          for (int q = slot; q < 8; q += MAIN_WARPS) {
+            const int16_t rr = clamp_component(qc.row + cand_dr(q)), cc = clamp_component(qc.col + cand_dc(q));
+            const uint32_t sv =
+                sad_at_mv(P, R.ws.win, wt[warp].temp, wt[warp].halo, plan.wx0, plan.wy0, mbx, mby, rr, cc, src, lane);
+            if (lane == 0) cand_sad[q] = sv;
+          }
         }
-        __syncthreads();
-        if (tid == 0) {
+        main_sync();
+        if (mt == 0) {
           vp8a_mv best = qc;
           uint32_t best_sad = mo.half.sad;
           for (int q = 0; q < 8; q++)
@@ -902,7 +1036,7 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
         const double bits_new = bb(t, p[0], 1) + bb(t, p[1], 1) + bb(t, p[2], 1) + bb(t, p[3], 0);
         const int dr = (int)m.quarter.mv.row - bp.row, dc = (int)m.quarter.mv.col - bp.col;
         const bool in_range = dr >= -1023 && dr <= 1023 && dc >= -1023 && dc <= 1023;
-        const double bits_mv = in_range ? mv_bits_lookup(a.mvbits, 0, dr) + mv_bits_lookup(a.mvbits, 1, dc)
+        const double bits_mv = in_range ? mvb[dr + 1023] + mvb[MV_BITS_SPAN + dc + 1023]
                                         : __longlong_as_double(0x7ff0000000000000LL);
         const double j_zero = (double)m.sad_zero + lambda * bits_zero;
         const double j_nearest = (double)m.sad_nearest + lambda * bits_nearest;
@@ -1123,7 +1257,8 @@ extern "C" vp8a_status vp8a_analyse_inter_frame(vp8a_ctx* ctx, const vp8a_i420* 
   VP8A_CUDA(cudaFuncGetAttributes(&fa, analysis_kernel));
   int smem_sm = 0;
   VP8A_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
-  const int pad = std::max((int)(4 * sizeof(SplitScratch)), smem_sm / 2 + 1 - (int)fa.sharedSizeBytes);
+  const int dyn = (int)(4 * sizeof(SplitScratch) + 2 * MV_BITS_SPAN * sizeof(double));
+  const int pad = std::max(dyn, smem_sm / 2 + 1 - (int)fa.sharedSizeBytes);
   VP8A_CUDA(cudaFuncSetAttribute(analysis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, pad));
   VP8A_CUDA(cudaFuncSetAttribute(analysis_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 0));
   cudaLaunchAttribute attr[1];
