@@ -66,13 +66,52 @@ def pad_planes(f):
 
 
 class Clocks:
-    """nvidia-smi sampler (clocks and throttle reasons) over the timed region."""
+    """SM clock and throttle-reason sampler over the timed region: NVML in a
+    background thread every 10 ms (the first sample is taken before the
+    region starts), else nvidia-smi at its 200 ms floor."""
+
+    REASONS = {  # NVML clocks-event reason bits
+        "sw_power_cap": 0x4,
+        "hw_slowdown": 0x8,
+        "sw_thermal_slowdown": 0x20,
+        "hw_thermal_slowdown": 0x40,
+    }
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.samples = []
+        self.nvml = None
+
+    def _nvml_loop(self):
+        nv, h = self.nvml, self.handle
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((float(sm), float(mx), int(rs)))
+            except Exception:
+                pass
+            self.first.set()
+            self.stop.wait(0.01)
 
     def __enter__(self):
+        import threading
+
+        try:
+            import pynvml as nv
+
+            nv.nvmlInit()
+            self.handle = nv.nvmlDeviceGetHandleByIndex(self.index)
+            self.nvml = nv
+            self.stop, self.first = threading.Event(), threading.Event()
+            self.thread = threading.Thread(target=self._nvml_loop, daemon=True)
+            self.thread.start()
+            self.first.wait(2.0)
+            return self
+        except Exception:
+            self.nvml = None
         q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
@@ -85,7 +124,14 @@ class Clocks:
         return self
 
     def __exit__(self, *a):
-        self.lines = []
+        if self.nvml is not None:
+            self.stop.set()
+            self.thread.join(2.0)
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
+            return
         if self.proc:
             self.proc.terminate()
             try:
@@ -93,27 +139,25 @@ class Clocks:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
                 out, _ = self.proc.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for l in out.splitlines():
+                p = [x.strip() for x in l.split(",")]
+                if len(p) < 7:
+                    continue
+                try:
+                    sm, mx = float(p[0]), float(p[1])
+                except ValueError:
+                    continue
+                bits = sum(self.REASONS[n] for n, v in zip(names, p[3:7]) if v.lower() == "active")
+                self.samples.append((sm, mx, bits))
 
     def summary(self):
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in getattr(self, "lines", []):
-            p = [x.strip() for x in l.split(",")]
-            if len(p) < 7:
-                continue
-            try:
-                sm.append(float(p[0]))
-                mx.append(float(p[1]))
-            except ValueError:
-                continue
-            for n, v in zip(names, p[3:7]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        if not sm:
+        if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        sm = [x[0] for x in self.samples]
+        reasons = sorted({n for _, _, b in self.samples for n, bit in self.REASONS.items() if b & bit})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(x[1] for x in self.samples), "reasons": reasons,
+                "samples": len(sm), "source": "nvml" if self.nvml is not None else "nvidia-smi"}
 
 
 def peaks():
