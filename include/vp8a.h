@@ -359,6 +359,34 @@ vp8a_status vp8a_filter_sweep(vp8a_ctx* ctx, const vp8a_planes* planes,
                               const vp8a_mb_lf_info* mbs, const vp8a_filter_config* base,
                               const vp8a_source* src, uint32_t every_rows, uint64_t* ssd_out);
 
+/* No counterpart in the reference. vp8a_filter_sweep for callers that may
+ * not allocate device memory once they are running — for instance a host
+ * that hands the library a pre-sized memory pool, or a real-time encoder
+ * loop where an allocation can stall or fail. It computes exactly what
+ * vp8a_filter_sweep computes and allocates nothing: no cudaMalloc, no
+ * cudaFree, no staging buffers. Therefore:
+ *  - every buffer (the planes, `mbs`, the source planes and the 512-entry
+ *    `ssd_out`) must already be device memory of the context's GPU
+ *    (VP8A_E_INVALID_ARGUMENT otherwise);
+ *  - its scratch (candidate list and step schedule) is one fixed array of
+ *    about 72 KiB compiled into the library, which every GPU that loads the
+ *    library holds until the process exits; it bounds the picture to at most
+ *    256 x 136 MBs (4096 x 2176 pixels), larger grids return
+ *    VP8A_E_INVALID_DIMENSIONS;
+ *  - the scratch is shared by every call on a device and keeps the last
+ *    call's contents (each call rewrites all it reads), so calls whose work
+ *    overlaps on the GPU — from different contexts or streams — race; keep
+ *    them ordered on one stream;
+ *  - the first call on each device looks the scratch's device address up
+ *    (cudaGetSymbolAddress); make that first call before any stream
+ *    capture.
+ * All its work is queued on the context stream (vp8a_ctx_synchronize waits
+ * for it). */
+vp8a_status vp8a_filter_sweep_noalloc(vp8a_ctx* ctx, const vp8a_planes* planes,
+                                      const vp8a_mb_lf_info* mbs, const vp8a_filter_config* base,
+                                      const vp8a_source* src, uint32_t every_rows,
+                                      uint64_t* ssd_out);
+
 /* select_filter_params (src/loop_filter.rs:2047): the reference's coarse
  * grid + refine + sharpness search, replayed over the device sweep. */
 vp8a_status vp8a_select_filter_params(vp8a_ctx* ctx, const vp8a_planes* planes,

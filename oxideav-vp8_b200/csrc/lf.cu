@@ -28,6 +28,7 @@
 // The sampled search's two-row bands are rows whose t0 restarts at 0 and
 // whose first row has no top edge.
 #include <algorithm>
+#include <mutex>
 
 #include "vp8a_internal.cuh"
 
@@ -737,6 +738,117 @@ vp8a_status score_candidates(vp8a_ctx* ctx, vp8a::Stager& st, const LfArgs& a, v
   return VP8A_OK;
 }
 
+// ----------------------------------------------- sweep without allocation
+//
+// vp8a_filter_sweep_noalloc runs the same sweep kernel as vp8a_filter_sweep
+// for callers that cannot allocate device memory while they run. Its scratch
+// (the candidate list and the step schedule) lives in one fixed array of
+// device memory owned by the library, built on the device by a small
+// kernel; every buffer the caller names must already be on the device.
+constexpr int NA_MAX_MB_COLS = 256;  // 4096 pixels
+constexpr int NA_MAX_MB_ROWS = 136;  // 2176 pixels: every row's slot ring fits in shared memory
+constexpr int NA_MAX_STEPS = 2 * (NA_MAX_MB_ROWS - 1) + NA_MAX_MB_COLS;
+constexpr int NA_CANDIDATES = 1 + 63 * 8;
+// Scratch layout (bytes).
+constexpr size_t NA_CANDS = 0;                                              // (level, sharpness) pairs
+constexpr size_t NA_T0 = 1024;                                              // int16 per MB row
+constexpr size_t NA_TOP = NA_T0 + 2 * NA_MAX_MB_ROWS;                       // u8 per MB row
+constexpr size_t NA_OFF = 1536;                                             // int32 per step + 1
+constexpr size_t NA_ROWS = (NA_OFF + 4 * (NA_MAX_STEPS + 1) + 15) & ~(size_t)15;  // u16 per scored MB
+constexpr size_t NA_BYTES = NA_ROWS + 2 * (size_t)NA_MAX_MB_ROWS * NA_MAX_MB_COLS;
+static_assert(2 * NA_CANDIDATES <= NA_T0 && NA_TOP + NA_MAX_MB_ROWS <= NA_OFF, "scratch layout");
+
+// The library's only copy; every call on a device shares it (about 72 KiB,
+// held by each device that loads the library until the process exits).
+static __device__ __align__(256) uint8_t g_sweep_scratch[NA_BYTES];
+
+// Candidates and step schedule of vp8a_filter_sweep (the host-built ones of
+// stage_lf and vp8a_filter_sweep), written on the device. One CTA of 1024
+// threads: steps <= NA_MAX_STEPS < 1024.
+__global__ void __launch_bounds__(1024) sweep_schedule_kernel(uint8_t* scr, int rows, int cols, int every_rows,
+                                                              int steps) {
+  __shared__ int16_t st0[NA_MAX_MB_ROWS];
+  __shared__ int cnt[NA_MAX_STEPS];
+  uint8_t* cands = scr + NA_CANDS;
+  int16_t* t0 = (int16_t*)(scr + NA_T0);
+  uint8_t* top = scr + NA_TOP;
+  int32_t* off = (int32_t*)(scr + NA_OFF);
+  uint16_t* srow = (uint16_t*)(scr + NA_ROWS);
+  const int tid = threadIdx.x;
+  // One level-0 candidate, then every (level 1..63, sharpness 0..7).
+  for (int i = tid; i < NA_CANDIDATES; i += blockDim.x) {
+    cands[2 * i] = (uint8_t)(i == 0 ? 0 : 1 + (i - 1) / 8);
+    cands[2 * i + 1] = (uint8_t)(i == 0 ? 0 : (i - 1) % 8);
+  }
+  for (int r = tid; r < rows; r += blockDim.x) {
+    int v, t;
+    if (every_rows == 0) {
+      v = 2 * r;
+      t = r > 0;
+    } else {
+      const int step = every_rows < 2 ? 2 : every_rows, k = r % step;
+      v = k < 2 ? 2 * k : -1;
+      t = k == 1;
+    }
+    st0[r] = (int16_t)v;
+    t0[r] = (int16_t)v;
+    top[r] = (uint8_t)t;
+  }
+  __syncthreads();
+  for (int t = tid; t < steps; t += blockDim.x) {
+    int n = 0;
+    for (int r = 0; r < rows; r++) n += st0[r] >= 0 && t >= st0[r] && t < st0[r] + cols;
+    cnt[t] = n;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int acc = 0;
+    for (int t = 0; t < steps; t++) {
+      off[t] = acc;
+      acc += cnt[t];
+      cnt[t] = off[t];
+    }
+    off[steps] = acc;
+  }
+  __syncthreads();
+  for (int t = tid; t < steps; t += blockDim.x) {
+    int o = cnt[t];
+    for (int r = 0; r < rows; r++)
+      if (st0[r] >= 0 && t >= st0[r] && t < st0[r] + cols) srow[o++] = (uint16_t)r;
+  }
+}
+
+// Device address of g_sweep_scratch on `dev` (current), looked up once per
+// device. In host code the array's name only stands in for the symbol.
+vp8a_status sweep_scratch(int dev, uint8_t** out) {
+  static std::mutex mu;
+  static void* ptr[64] = {};
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev < 0 || dev >= 64) {
+    vp8a::set_error("device index out of range");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (!ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_sweep_scratch);
+    if (e != cudaSuccess) return vp8a::cuda_fail(e, "cudaGetSymbolAddress(g_sweep_scratch)");
+    ptr[dev] = p;
+  }
+  *out = (uint8_t*)ptr[dev];
+  return VP8A_OK;
+}
+
+// True when `p` is device (or managed) memory usable on `dev`.
+bool device_resident(const void* p, int dev) {
+  if (!p) return false;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return (at.type == cudaMemoryTypeDevice && at.device == dev) || at.type == cudaMemoryTypeManaged;
+}
+
 }  // namespace
 
 extern "C" {
@@ -960,6 +1072,116 @@ vp8a_status vp8a_select_filter_params_sampled(vp8a_ctx* ctx, const vp8a_planes* 
   if ((s = st.write_from_host(level_out, &best_level, 1)) != VP8A_OK) return s;
   if ((s = st.write_from_host(sharpness_out, &best_sharp, 1)) != VP8A_OK) return s;
   return st.finish();
+}
+
+// The sweep of vp8a_filter_sweep without any allocation: see the header.
+vp8a_status vp8a_filter_sweep_noalloc(vp8a_ctx* ctx, const vp8a_planes* planes, const vp8a_mb_lf_info* mbs,
+                                      const vp8a_filter_config* base, const vp8a_source* src, uint32_t every_rows,
+                                      uint64_t* ssd_out) {
+  if (!ctx || !planes || !mbs || !base || !src || !ssd_out) {
+    vp8a::set_error("null argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  const int cols = (int)planes->mb_cols, rows = (int)planes->mb_rows;
+  if (cols < 1 || rows < 1 || cols > NA_MAX_MB_COLS || rows > NA_MAX_MB_ROWS) {
+    vp8a::set_error("vp8a_filter_sweep_noalloc: the MB grid must be 1..256 columns by 1..136 rows "
+                    "(its fixed scratch holds the schedule of at most 4096x2176 pixels)");
+    return VP8A_E_INVALID_DIMENSIONS;
+  }
+  if (planes->y_stride < (uint64_t)cols * 16 || planes->uv_stride < (uint64_t)cols * 8) {
+    vp8a::set_error("plane stride below the MB-padded width");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  vp8a_status s = validate_config(base);
+  if (s != VP8A_OK) return s;
+  if (src->width == 0 || src->height == 0 || src->width > (uint32_t)cols * 16 || src->height > (uint32_t)rows * 16) {
+    vp8a::set_error("source size does not fit the MB grid");
+    return VP8A_E_REFERENCE_DIMENSIONS_MISMATCH;
+  }
+  const uint32_t cw = (src->width + 1) / 2;
+  if (src->y_stride < src->width || src->uv_stride < cw) {
+    vp8a::set_error("source stride below width");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  const void* bufs[8] = {planes->y, planes->u, planes->v, mbs, src->y, src->u, src->v, ssd_out};
+  for (const void* b : bufs)
+    if (!device_resident(b, ctx->device)) {
+      vp8a::set_error("vp8a_filter_sweep_noalloc: every buffer must be device memory of the context's GPU "
+                      "(this entry point stages nothing)");
+      return VP8A_E_INVALID_ARGUMENT;
+    }
+  uint8_t* scr = nullptr;
+  if ((s = sweep_scratch(ctx->device, &scr)) != VP8A_OK) return s;
+  // Host-side schedule extent: steps and the busiest step's row count.
+  const int max_t0 = every_rows == 0 ? 2 * (rows - 1) : (rows >= 2 ? 2 : 0);
+  const int steps = max_t0 + cols;
+  int max_active = 0;
+  for (int t = 0; t < steps; t++) {
+    int n = 0;
+    for (int r = 0; r < rows; r++) {
+      int v;
+      if (every_rows == 0) {
+        v = 2 * r;
+      } else {
+        const int step = every_rows < 2 ? 2 : (int)every_rows, k = r % step;
+        v = k < 2 ? 2 * k : -1;
+      }
+      n += v >= 0 && t >= v && t < v + cols;
+    }
+    max_active = std::max(max_active, n);
+  }
+  sweep_schedule_kernel<<<1, 1024, 0, ctx->stream>>>(scr, rows, cols, (int)every_rows, steps);
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
+
+  LfArgs a{};
+  a.y = (const uint8_t*)planes->y;
+  a.u = (const uint8_t*)planes->u;
+  a.v = (const uint8_t*)planes->v;
+  a.ys = planes->y_stride;
+  a.cs = planes->uv_stride;
+  a.mb_cols = cols;
+  a.mb_rows = rows;
+  a.mbs = mbs;
+  a.base = *base;
+  a.sy = (const uint8_t*)src->y;
+  a.su = (const uint8_t*)src->u;
+  a.sv = (const uint8_t*)src->v;
+  a.sys = src->y_stride;
+  a.scs = src->uv_stride;
+  a.width = (int)src->width;
+  a.height = (int)src->height;
+  a.cands = scr + NA_CANDS;
+  a.row_t0 = (const int16_t*)(scr + NA_T0);
+  a.row_top = scr + NA_TOP;
+  a.sched_off = (const int32_t*)(scr + NA_OFF);
+  a.sched_row = (const uint16_t*)(scr + NA_ROWS);
+  a.steps = steps;
+  a.max_active = max_active;
+  auto al4 = [](const void* p, uint64_t stride) { return ((uintptr_t)p % 4 == 0) && (stride % 4 == 0); };
+  a.recon_words = al4(a.y, a.ys) && al4(a.u, a.cs) && al4(a.v, a.cs);
+  a.source_words = al4(a.sy, a.sys) && al4(a.su, a.scs) && al4(a.sv, a.scs);
+  a.ssd_out = ssd_out;
+  a.level0_unfiltered = 1;
+  a.smem_slots = 1;
+  a.gslots = nullptr;
+  const size_t slot_bytes = (size_t)rows * 4 * SLOT_STRIDE;
+  int max_smem = 0;
+  VP8A_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+  if (slot_bytes + 1024 > (size_t)max_smem) {
+    vp8a::set_error("vp8a_filter_sweep_noalloc: the MB rows' slot rings do not fit in shared memory");
+    return VP8A_E_INVALID_DIMENSIONS;
+  }
+  const int threads = std::min(1024, std::max(32, (16 * max_active + 31) / 32 * 32));
+  VP8A_CUDA(cudaFuncSetAttribute(lf_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slot_bytes));
+  lf_sweep_kernel<<<NA_CANDIDATES, threads, slot_bytes, ctx->stream>>>(a);
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
+  // Level 0 scores the same for every sharpness.
+  for (int sh = 1; sh < 8; sh++)
+    VP8A_CUDA(cudaMemcpyAsync(ssd_out + sh, ssd_out, sizeof(uint64_t), cudaMemcpyDeviceToDevice, ctx->stream));
+  return VP8A_OK;
 }
 
 }  // extern "C"

@@ -44,6 +44,10 @@ PROTOTYPES = {
         C.c_int,
         [P, C.POINTER(abi.Planes), P, C.POINTER(abi.FilterConfig), C.POINTER(abi.Source), U32, P],
     ),
+    "vp8a_filter_sweep_noalloc": (
+        C.c_int,
+        [P, C.POINTER(abi.Planes), P, C.POINTER(abi.FilterConfig), C.POINTER(abi.Source), U32, P],
+    ),
     "vp8a_select_filter_params": (
         C.c_int,
         [P, C.POINTER(abi.Planes), P, C.POINTER(abi.FilterConfig), C.POINTER(abi.Source), P, P],
