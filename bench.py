@@ -400,6 +400,14 @@ def gpu_arm(args):
         dom = max(stage, key=lambda k: stage[k]["ms"])
         d = stage[dom]
         achieved = d["bytes"] / (d["ms"] / 1000.0) / 1e9
+        ipeak = int32_peak_tops()
+        stages = {}
+        for k, v in stage.items():
+            gbs = v["bytes"] / (v["ms"] / 1000.0) / 1e9
+            tops = v["ops"] / (v["ms"] / 1000.0) / 1e12
+            stages[k] = {"ms": round(v["ms"], 4), "reps_ms": v["reps"], "alg_bytes": int(v["bytes"]),
+                         "dram_traffic": dram_traffic(k), "gbs": round(gbs, 2), "hbm_frac": round(gbs / peak, 5),
+                         "alg_ops": int(v["ops"]), "tops": round(tops, 3), "alu_frac": round(tops / ipeak, 4)}
         result = {
             "metric": METRIC,
             "value": round(value, 1),
@@ -430,12 +438,13 @@ def gpu_arm(args):
             "e2e": {"value": round(e2e, 1), "unit": "MB/s", "h2d_bytes_per_step": int(hs.h2d),
                     "d2h_bytes_per_step": int(hs.d2h)},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": peak,
-                         "unit": "GB/s", "frac": round(achieved / peak, 5), "traffic": None,
+                         "unit": "GB/s", "frac": round(achieved / peak, 5), "traffic": dram_traffic(dom),
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6.65 TB/s",
-                         "stage_ms": {k: round(v["ms"], 4) for k, v in stage.items()},
-                         "stage_reps_ms": {k: v["reps"] for k, v in stage.items()},
-                         "stage_alg_bytes": {k: int(v["bytes"]) for k, v in stage.items()}},
+                         "alu": {"kernel": dom, "achieved": stages[dom]["tops"], "peak": round(ipeak, 2),
+                                 "unit": "Tops/s (int32, algorithmic op model)", "frac": stages[dom]["alu_frac"],
+                                 "peak_source": "nominal: 148 SMs x 128 INT32 lanes x max SM clock"},
+                         "stages": stages},
             "gpu_launches": int(launches),
             "step_ms": step_ms,
             "e2e_step_ms": [round(x, 3) for x in e_times],
@@ -448,6 +457,38 @@ def gpu_arm(args):
         dist.barrier()
         dist.destroy_process_group()
     return result
+
+
+# Algorithmic integer operations per stage at 1080p (the op model of the
+# scope table's measurement row): ME 3 refs x ~92 k ops per (MB, ref);
+# ARNR (L-1) x MBs x 33 x 256 search abs-diffs + (L-1) x picture pixels x 4
+# blend ops; LF ~9 k ops per candidate-MB (192 edge segments x ~40 ops plus
+# a 384-pixel SSD) over 512 candidates.
+STAGE_OPS = {
+    "analysis": N_MB * 3 * 92_000,
+    "arnr": (LOOKAHEAD - 1) * N_MB * 33 * 256 + (LOOKAHEAD - 1) * (W * H * 3 // 2) * 4,
+    "lf_sweep": 512 * N_MB * 9_000,
+}
+def int32_peak_tops():
+    """Nominal INT32 issue peak: 148 SMs x 128 lanes x max SM clock (no
+    measured integer peak is available)."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            mhz = float(json.load(f).get("sm_max_mhz", 1965.0))
+    except (OSError, ValueError):
+        mhz = 1965.0
+    return 148 * 128 * mhz * 1e6 / 1e12
+
+
+def dram_traffic(stage):
+    """DRAM bytes per launch of the stage's kernels from the committed ncu
+    capture (profiles/dram_traffic_1080p.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "dram_traffic_1080p.json")) as f:
+            d = json.load(f)["bytes_per_launch"][stage]
+        return int(sum(v["read"] + v["write"] for v in d.values()))
+    except (OSError, KeyError, ValueError):
+        return None
 
 
 def stage_times(gs, stream, torch, flush, reps=3):
@@ -475,7 +516,8 @@ def stage_times(gs, stream, torch, flush, reps=3):
             e.record(stream)
             e.synchronize()
             ts.append(s.elapsed_time(e))
-        out[name] = {"ms": float(np.median(ts)), "bytes": nbytes, "reps": [round(x, 3) for x in ts]}
+        out[name] = {"ms": float(np.median(ts)), "bytes": nbytes, "ops": STAGE_OPS[name],
+                     "reps": [round(x, 3) for x in ts]}
     return out
 
 
