@@ -287,6 +287,34 @@ __device__ __forceinline__ void staged_block_sads(const RefSmem& R, const uint8_
   }
 }
 
+// One round of the N, S, W, E walk away from the +-1023 clamp, where every
+// candidate is the running best moved by one pixel and none collapses: with
+// the 3x3 neighbourhood of the round's start (r[4] = its SAD), N moves if it
+// beats the start, else S; then W from the row reached, else E (a candidate
+// that steps back onto an earlier position cannot beat it). Returns the
+// move (dx, dy) and the new best SAD; (0, 0) ends the walk.
+__device__ __forceinline__ void walk_round(const uint32_t (&r)[9], int& dx, int& dy, uint32_t& b) {
+  b = r[4];
+  dy = 0;
+  if (r[1] < b) {
+    dy = -1;
+    b = r[1];
+  } else if (r[7] < b) {
+    dy = 1;
+    b = r[7];
+  }
+  const uint32_t wv = dy < 0 ? r[0] : (dy == 0 ? r[3] : r[6]);
+  const uint32_t ev = dy < 0 ? r[2] : (dy == 0 ? r[5] : r[8]);
+  dx = 0;
+  if (wv < b) {
+    dx = -1;
+    b = wv;
+  } else if (ev < b) {
+    dx = 1;
+    b = ev;
+  }
+}
+
 // small_diamond_search_luma (src/motion_search.rs:381-442) walked over the
 // field: N, S, W, E from the running best, strict '<', collapse skips, at
 // most max_iters rounds. Warp-uniform; a position outside the field (not
@@ -302,6 +330,31 @@ __device__ vp8a_search_result diamond_field(const FieldSmem& F, const MePlane& P
   vp8a_mv best;
   best.row = snap_whole(clamp_component(center.row));
   best.col = snap_whole(clamp_component(center.col));
+  const int x0 = mbx + best.col / 4 - cxp, y0 = mby + best.row / 4 - cyp;
+  const int lim = 1020 - 4 * max_iters;
+  if (best.row >= -lim && best.row <= lim && best.col >= -lim && best.col <= lim && max_iters <= FR &&
+      x0 == 0 && y0 == 0) {
+    // No candidate of the walk is clamped and every round's neighbourhood
+    // lies in the field: read it whole, decide the round with selects.
+    int x = 0, y = 0;
+    uint32_t bs = F.full[fpos(0, 0)];
+    for (int it = 0; it < max_iters; it++) {
+      const uint32_t* c0 = F.full + fpos(x, y);
+      const uint32_t r[9] = {c0[-FN - 1], c0[-FN], c0[-FN + 1], c0[-1], bs, c0[1], c0[FN - 1], c0[FN], c0[FN + 1]};
+      int dx, dy;
+      uint32_t b;
+      walk_round(r, dx, dy, b);
+      if (dx == 0 && dy == 0) break;
+      x += dx;
+      y += dy;
+      bs = b;
+    }
+    vp8a_search_result res;
+    res.mv.row = (int16_t)(best.row + 4 * y);
+    res.mv.col = (int16_t)(best.col + 4 * x);
+    res.sad = bs;
+    return res;
+  }
   uint32_t best_sad = sad(best);
   for (int it = 0; it < max_iters; it++) {
     bool improved = false;
@@ -446,6 +499,27 @@ __device__ void split_partition(const AnArgs& a, const double* t, const double* 
     uint32_t bs = group_sad(fv, P, src, pid, g, best);
     const uint16_t* fbase = pid == 3 ? &fv.F->blk[0][g] : &fv.F->grp[0][goff + g];
     const int fstride = pid == 3 ? 16 : 8;  // u16 entries per field position
+    const int sx = fv.mbx + int_off(best.col) - fv.cxp, sy = fv.mby + int_off(best.row) - fv.cyp;
+    if (!(best.row & 3) && !(best.col & 3) && best.row >= -1007 && best.row <= 1007 && best.col >= -1007 &&
+        best.col <= 1007 && sx >= -(FR - 4) && sx <= FR - 4 && sy >= -(FR - 4) && sy <= FR - 4) {
+      // Four rounds away from the clamp, inside the field (walk_round).
+      int x = sx, y = sy;
+      for (int it = 0; it < 4; it++) {
+        const uint16_t* c0 = fbase + fpos(x, y) * fstride;
+        const uint32_t r[9] = {c0[(-FN - 1) * fstride], c0[-FN * fstride], c0[(-FN + 1) * fstride],
+                               c0[-fstride],            bs,                c0[fstride],
+                               c0[(FN - 1) * fstride],  c0[FN * fstride],  c0[(FN + 1) * fstride]};
+        int dx, dy;
+        uint32_t b;
+        walk_round(r, dx, dy, b);
+        if (dx == 0 && dy == 0) break;
+        x += dx;
+        y += dy;
+        bs = b;
+      }
+      best.row = (int16_t)(best.row + 4 * (y - sy));
+      best.col = (int16_t)(best.col + 4 * (x - sx));
+    } else
     for (int it = 0; it < 4; it++) {
       const int dx0 = fv.mbx + int_off(best.col) - fv.cxp, dy0 = fv.mby + int_off(best.row) - fv.cyp;
       const vp8a_mv b0 = best;
@@ -1150,7 +1224,7 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
         }
         a.dec[(size_t)r * a.mb_cols + c] = d;
         a.infos[(size_t)r * a.mb_cols + c] = info;
-        __threadfence();
+        // The release orders this thread's record writes before the count.
         st_release(&a.progress[r], (unsigned)(c + 1));
       }
       // The next MB's first cluster barrier orders these results.
