@@ -95,7 +95,13 @@ struct __align__(16) RefDec {
   vp8a_mv split_mvs[16];
   uint8_t submv_modes[16];
 };
-static_assert(sizeof(RefDec) % 16 == 0, "RefDec is copied as words");
+static_assert(sizeof(RefDec) == 112 && offsetof(RefDec, mv) == 16 && offsetof(RefDec, split_mvs) == 28 &&
+                  offsetof(RefDec, submv_modes) == 92,
+              "RefDec is copied as words");
+static_assert(offsetof(vp8a_mb_decision, mv) == 4 && offsetof(vp8a_mb_decision, j) == 8 &&
+                  offsetof(vp8a_mb_decision, split_mvs) == 24 && offsetof(vp8a_mb_decision, submv_modes) == 88 &&
+                  sizeof(vp8a_mb_decision) == 104,
+              "vp8a_mb_decision is written as words");
 
 struct SplitOut {
   double j;
@@ -128,6 +134,7 @@ struct Plan {
   int hr_x, hr_y;      // NEAR halo origin
   int nblocks;
   int box[MAX_BLOCKS], boy[MAX_BLOCKS];  // block integer offsets
+  int colblk[9];       // staged block of SPLITMV column m < 9 (ZERO, LEFT x4, ABOVE x4)
 };
 
 __device__ __forceinline__ int int_off(int16_t v) { return eighth(v) >> 3; }
@@ -481,7 +488,7 @@ __device__ __forceinline__ double mv_partition_bits(const double* t, int pid) {
 // it: sbits[ctx * 4 + mode] = submv_ref_bits of each context and mode, and
 // each group's NEW vector bits. Every value is the same expression the
 // reference evaluates, so the chain's sums are unchanged.
-__device__ void split_partition(const AnArgs& a, const double* t, const double* sbits, const double* lterm,
+__device__ void split_partition(const AnArgs& a, const double* pbits, const double* sbits, const double* lterm,
                                 const double* mvb, const FieldView& fv, const MePlane& P, const uint8_t* src, vp8a_mv bp,
                                 const MbInfoDev& above, const MbInfoDev& left, int pid, SplitScratch& W,
                                 SplitOut* out, int lane) {
@@ -576,11 +583,10 @@ __device__ void split_partition(const AnArgs& a, const double* t, const double* 
 #pragma unroll
     for (int x = 0; x < 5; x++) W.new_cost[g * 5 + x] = a.lambda * (sbits[x * 4 + VP8A_SUBMV_NEW] + nb);
   }
-  if (lane == 0) {
-    W.cmv[0] = vp8a_mv{0, 0};
-    for (int k = 0; k < 4; k++) W.cmv[1 + k] = ext_left(left, 4 * k);
-    for (int k = 0; k < 4; k++) W.cmv[5 + k] = ext_above(above, k);
-  }
+  // Columns 0-8: ZERO, the left neighbour's vectors at anchors 0/4/8/12,
+  // the above neighbour's at anchors 0-3 (one lane each).
+  if (lane < 9)
+    W.cmv[lane] = lane == 0 ? vp8a_mv{0, 0} : (lane < 5 ? ext_left(left, 4 * (lane - 1)) : ext_above(above, lane - 5));
   __syncwarp();
   // Candidate SADs. Columns 0-8 (ZERO and the neighbours' vectors) are the
   // staged blocks: their group SADs are tabled, (group, column) pairs over
@@ -590,17 +596,7 @@ __device__ void split_partition(const AnArgs& a, const double* t, const double* 
   if (lane < 9 + G && ((need >> lane) & 1u)) {
     const vp8a_mv mv = W.cmv[lane];
     const int x = fv.mbx + int_off(mv.col), y = fv.mby + int_off(mv.row);
-    int cp = -1;
-    if (lane < 9) {
-      for (int q = 0; q < fv.pl->nblocks; q++)
-        if (fv.mbx + fv.pl->box[q] == x && fv.mby + fv.pl->boy[q] == y) {
-          cp = q;
-          break;
-        }
-    } else {
-      cp = fpos(x - fv.cxp, y - fv.cyp);
-    }
-    W.colpos[lane] = cp;
+    W.colpos[lane] = lane < 9 ? fv.pl->colblk[lane] : fpos(x - fv.cxp, y - fv.cyp);
   }
   __syncwarp();
   for (int q = lane; q < G * 9; q += 32) {
@@ -690,18 +686,24 @@ __device__ void split_partition(const AnArgs& a, const double* t, const double* 
   const uint32_t sd = mine ? W.sad[lane] : 0u;
   const uint32_t total_sad = __reduce_add_sync(FULL, sd);
   const unsigned any_bad = __ballot_sync(FULL, bad != 0), news = __ballot_sync(FULL, isn != 0);
+  double xa[16], xn[16];
+#pragma unroll
+  for (int gg = 0; gg < 16; gg++) {
+    xa[gg] = __shfl_sync(FULL, ba, gg);
+    xn[gg] = __shfl_sync(FULL, bn, gg);
+  }
   double total_bits = 0.0;
-  for (int gg = 0; gg < G; gg++) {
-    const double x = __shfl_sync(FULL, ba, gg), y = __shfl_sync(FULL, bn, gg);
-    total_bits += x;
-    if ((news >> gg) & 1u) total_bits += y;
+#pragma unroll
+  for (int gg = 0; gg < 16; gg++) {
+    if (gg >= G) break;
+    total_bits += xa[gg];
+    if ((news >> gg) & 1u) total_bits += xn[gg];
   }
   if (lane == 0) {
     // The reference stops at the first group without a finite choice.
     out->valid = any_bad == 0u;
     if (any_bad == 0u) {
-      const double partition_bits = mv_partition_bits(t, pid);
-      out->j = (double)total_sad + a.lambda * (partition_bits + total_bits);
+      out->j = (double)total_sad + a.lambda * (pbits[pid] + total_bits);
       for (int i = G; i < 16; i++) out->modes[i] = VP8A_SUBMV_ZERO;
     }
   }
@@ -905,6 +907,10 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
   __shared__ Census cen;
   __shared__ Plan plan;
   __shared__ int s_abort, s_qok;
+  // Per-MB cost terms of the mode decision (from the census probabilities),
+  // filled during the search by warp 7; per-CTA constants below.
+  __shared__ double dz, dnearest, dnear, dnew_bits, dsplit;
+  __shared__ double lrbits, pbits[4];
   __shared__ QuarterGeom s_qg;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int k = (int)cl.block_rank();  // the reference this CTA searches
@@ -917,6 +923,16 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
     const double b = submv_ref_bits(bit_cost, c_submv_probs[tid >> 2], tid & 3);
     sbits[tid] = b;
     lterm[tid] = a.lambda * (b + 0.0);
+  } else if (tid < 24) {
+    pbits[tid - 20] = mv_partition_bits(bit_cost, tid - 20);
+  } else if (tid == 24) {
+    // lambda * ref_frame_tree_bits(ref, 128, 128) (src/encoder.rs:9108).
+    const double* t = bit_cost;
+    const uint8_t id = a.ref_ids[k];
+    const double rbits = id == VP8A_REF_LAST ? bb(t, 128, 0)
+                         : id == VP8A_REF_GOLDEN ? bb(t, 128, 1) + bb(t, 128, 0)
+                                                 : bb(t, 128, 1) + bb(t, 128, 1);
+    lrbits = a.lambda * rbits;
   }
   uint32_t* dec_slot = (uint32_t*)cl.map_shared_rank(&decs[k], 0);
   const int* abort0 = cl.map_shared_rank(&s_abort, 0);
@@ -974,17 +990,17 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
         p.hr_x = mbx + int_off(cen.near_.col) - 2;
         p.hr_y = mby + int_off(cen.near_.row) - 2;
         p.nblocks = 0;
-        auto addb = [&](vp8a_mv m) {
+        auto addb = [&](vp8a_mv m) -> int {
           const int ox = int_off(m.col), oy = int_off(m.row);
           for (int i = 0; i < p.nblocks; i++)
-            if (p.box[i] == ox && p.boy[i] == oy) return;
+            if (p.box[i] == ox && p.boy[i] == oy) return i;
           p.box[p.nblocks] = ox;
           p.boy[p.nblocks] = oy;
-          p.nblocks++;
+          return p.nblocks++;
         };
-        addb(vp8a_mv{0, 0});
-        for (int anc = 0; anc < 16; anc += 4) addb(ext_left(nb[1], anc));
-        for (int anc = 0; anc < 4; anc++) addb(ext_above(nb[0], anc));
+        p.colblk[0] = addb(vp8a_mv{0, 0});
+        for (int k = 0; k < 4; k++) p.colblk[1 + k] = addb(ext_left(nb[1], 4 * k));
+        for (int k = 0; k < 4; k++) p.colblk[5 + k] = addb(ext_above(nb[0], k));
         plan = p;
       }
       __syncthreads();
@@ -999,7 +1015,7 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
       const int cxp = plan.wx0 + WIN_LEAD, cyp = plan.wy0 + WIN_LEAD;  // field centre (plane pixels)
       const FieldView fv{&F, xs, &plan, mbx, mby, cxp, cyp};
       if (warp >= 1 && warp <= 4) {
-        split_partition(a, bit_cost, sbits, lterm, mvb, fv, P, src, bp, nb[0], nb[1], warp - 1, ss[warp - 1],
+        split_partition(a, pbits, sbits, lterm, mvb, fv, P, src, bp, nb[0], nb[1], warp - 1, ss[warp - 1],
                         &splits[warp - 1], lane);
       } else {
         // The main group (warps 0 and 5-8) runs the MB search chain while
@@ -1024,6 +1040,15 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
           const int er = eighth(cen.near_.row), ec = eighth(cen.near_.col);
           const uint32_t sv = subpel_sad(R.halo_near, HS, ec & 7, er & 7, src, wt[6].temp, lane);
           if (lane == 0) mo.sad_near = sv;
+        } else if (warp == 7 && lane == 0) {
+          // The mode tree's bits under this MB's census probabilities.
+          const double* t = bit_cost;
+          const uint8_t* p = cen.p;
+          dz = a.lambda * bb(t, p[0], 0);
+          dnearest = a.lambda * (bb(t, p[0], 1) + bb(t, p[1], 0));
+          dnear = a.lambda * (bb(t, p[0], 1) + bb(t, p[1], 1) + bb(t, p[2], 0));
+          dnew_bits = bb(t, p[0], 1) + bb(t, p[1], 1) + bb(t, p[2], 1) + bb(t, p[3], 0);
+          dsplit = a.lambda * (bb(t, p[0], 1) + bb(t, p[1], 1) + bb(t, p[2], 1) + bb(t, p[3], 1));
         }
         main_sync();
         // half_pixel_refine_luma around the whole-pel result: planes shared
@@ -1100,22 +1125,19 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
       __syncthreads();
       if (tid == 0) {
         // pick_mb_for_ref's mode decision (src/encoder.rs:8598-8652).
-        const double* t = bit_cost;
+        // Every product lambda * bits below is the reference's own; the ones
+        // that depend only on the census or the reference were formed
+        // during the search.
         const double lambda = a.lambda;
-        const uint8_t* p = cen.p;
         const MainOut& m = mo;
-        const double bits_zero = bb(t, p[0], 0);
-        const double bits_nearest = bb(t, p[0], 1) + bb(t, p[1], 0);
-        const double bits_near = bb(t, p[0], 1) + bb(t, p[1], 1) + bb(t, p[2], 0);
-        const double bits_new = bb(t, p[0], 1) + bb(t, p[1], 1) + bb(t, p[2], 1) + bb(t, p[3], 0);
         const int dr = (int)m.quarter.mv.row - bp.row, dc = (int)m.quarter.mv.col - bp.col;
         const bool in_range = dr >= -1023 && dr <= 1023 && dc >= -1023 && dc <= 1023;
         const double bits_mv = in_range ? mvb[dr + 1023] + mvb[MV_BITS_SPAN + dc + 1023]
                                         : __longlong_as_double(0x7ff0000000000000LL);
-        const double j_zero = (double)m.sad_zero + lambda * bits_zero;
-        const double j_nearest = (double)m.sad_nearest + lambda * bits_nearest;
-        const double j_near = (double)m.sad_near + lambda * bits_near;
-        const double j_new = (double)m.quarter.sad + lambda * (bits_new + bits_mv);
+        const double j_zero = (double)m.sad_zero + dz;
+        const double j_nearest = (double)m.sad_nearest + dnearest;
+        const double j_near = (double)m.sad_near + dnear;
+        const double j_new = (double)m.quarter.sad + lambda * (dnew_bits + bits_mv);
         int mode = VP8A_MODE_ZERO, pid = VP8A_PART_NONE;
         vp8a_mv mv = {0, 0};
         double cj = j_zero;
@@ -1134,15 +1156,14 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
           mv = m.quarter.mv;
           cj = j_new;
         }
-        const double bits_split = bb(t, p[0], 1) + bb(t, p[1], 1) + bb(t, p[2], 1) + bb(t, p[3], 1);
         int have = 0, sp = -1;
         double sj = 0.0;
         for (int qq = 0; qq < 4; qq++) {
           if (!splits[qq].valid) continue;
-          const double total_j = splits[qq].j + lambda * bits_split;
+          const double total_j = splits[qq].j + dsplit;
           // The stored best already includes bits_split and the
           // comparison adds it again (src/encoder.rs:8679-8683).
-          if (!have || total_j < sj + lambda * bits_split) {
+          if (!have || total_j < sj + dsplit) {
             sj = total_j;
             sp = qq;
             have = 1;
@@ -1154,12 +1175,7 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
           cj = sj;
           pid = sp;
         }
-        // ref_frame_tree_bits(ref, 128, 128) (src/encoder.rs:9108).
-        const uint8_t id = a.ref_ids[k];
-        const double rbits = id == VP8A_REF_LAST ? bb(t, 128, 0)
-                             : id == VP8A_REF_GOLDEN ? bb(t, 128, 1) + bb(t, 128, 0)
-                                                     : bb(t, 128, 1) + bb(t, 128, 1);
-        const double total = cj + lambda * rbits;
+        const double total = cj + lrbits;
         if (a.trace) {
           vp8a_ref_search tr;
           tr.best_predictor = bp;
@@ -1182,17 +1198,24 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
         mydec.mv = mv;
         mydec.mode = mode;
         mydec.pid = pid;
-        for (int i = 0; i < 16; i++) {
-          mydec.split_mvs[i] = mode == VP8A_MODE_SPLIT ? splits[pid].split_mvs[i] : vp8a_mv{0, 0};
-          mydec.submv_modes[i] = mode == VP8A_MODE_SPLIT ? splits[pid].modes[i] : (uint8_t)VP8A_SUBMV_ZERO;
-        }
       }
       __syncthreads();
-      if (tid < (int)(sizeof(RefDec) / 4)) dec_slot[tid] = ((const uint32_t*)&mydec)[tid];
+      // Into rank 0, word by word; the sub-MVs and sub-MV modes come from
+      // the chosen partition (ZERO vectors and ZERO4X4 modes otherwise).
+      if (tid < (int)(sizeof(RefDec) / 4)) {
+        const bool spl = mydec.mode == VP8A_MODE_SPLIT;
+        uint32_t w;
+        if (tid < 7) w = ((const uint32_t*)&mydec)[tid];
+        else if (tid < 23) w = spl ? ((const uint32_t*)splits[mydec.pid].split_mvs)[tid - 7] : 0u;
+        else if (tid < 27) w = spl ? ((const uint32_t*)splits[mydec.pid].modes)[tid - 23] : 0x01010101u * VP8A_SUBMV_ZERO;
+        else w = 0u;
+        dec_slot[tid] = w;
+      }
       cl.sync();
-      if (k == 0 && tid == 0) {
+      if (k == 0 && warp == 0) {
         // decide_mb_exhaustive's reference comparison: first strict minimum
-        // of J + ref_frame_tree_bits in reference order.
+        // of J + ref_frame_tree_bits in reference order (every lane), then
+        // the decision and census records written word by word.
         double best_total = __longlong_as_double(0x7ff0000000000000LL);
         int best_k = -1;
         for (int q = 0; q < a.n_refs; q++)
@@ -1200,32 +1223,30 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
             best_total = decs[q].total;
             best_k = q;
           }
-        vp8a_mb_decision d;
-        memset(&d, 0, sizeof d);
-        MbInfoDev info;
-        memset(&info, 0, sizeof info);
-        if (best_k >= 0) {
-          const RefDec& b = decs[best_k];
-          d.ref_frame = a.ref_ids[best_k];
-          d.mode = (uint8_t)b.mode;
-          d.partition = (uint8_t)b.pid;
-          d.mv = b.mv;
-          d.j = b.j;
-          d.total = b.total;
-          for (int i = 0; i < 16; i++) {
-            d.split_mvs[i] = b.split_mvs[i];
-            d.submv_modes[i] = b.submv_modes[i];
-          }
-          info.ref_frame = d.ref_frame;
-          info.mv = b.mv;
-          info.is_split = b.mode == VP8A_MODE_SPLIT;
-          info.has_split_mvs = info.is_split;
-          for (int i = 0; i < 16; i++) info.split_mvs[i] = d.split_mvs[i];
+        const uint32_t* b = (const uint32_t*)&decs[best_k < 0 ? 0 : best_k];
+        const bool ok = best_k >= 0;
+        const uint32_t mode = ok ? (uint32_t)decs[best_k].mode : 0u, pid = ok ? (uint32_t)decs[best_k].pid : 0u;
+        const uint32_t id = ok ? (uint32_t)a.ref_ids[best_k] : 0u, spl = mode == VP8A_MODE_SPLIT;
+        uint32_t* dw = (uint32_t*)(a.dec + (size_t)r * a.mb_cols + c);
+        uint32_t* iw = (uint32_t*)(a.infos + (size_t)r * a.mb_cols + c);
+        if (lane < 26) {  // vp8a_mb_decision
+          uint32_t w;
+          if (lane == 0) w = id | (mode & 0xffu) << 8 | (pid & 0xffu) << 16;
+          else if (lane == 1) w = b[4];         // mv
+          else if (lane < 6) w = b[lane - 2];   // j, total
+          else w = b[lane + 1];                 // split_mvs, submv_modes
+          dw[lane] = ok ? w : 0u;
         }
-        a.dec[(size_t)r * a.mb_cols + c] = d;
-        a.infos[(size_t)r * a.mb_cols + c] = info;
-        // The release orders this thread's record writes before the count.
-        st_release(&a.progress[r], (unsigned)(c + 1));
+        if (lane < 18) {  // the census record
+          uint32_t w;
+          if (lane == 0) w = id | spl << 8 | spl << 16;
+          else if (lane == 1) w = b[4];
+          else w = b[lane + 5];
+          iw[lane] = ok ? w : 0u;
+        }
+        __syncwarp();
+        // The release orders the warp's record writes before the count.
+        if (lane == 0) st_release(&a.progress[r], (unsigned)(c + 1));
       }
       // The next MB's first cluster barrier orders these results.
     }
