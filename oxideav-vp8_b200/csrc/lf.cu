@@ -127,33 +127,31 @@ __device__ __forceinline__ int mb_level(const vp8a_filter_config& c, int level0,
   return clampi(level, 0, 63);
 }
 
-// §15.3 MBfilter (src/loop_filter.rs:331-371) on signed taps p[o..o+8).
+// The filters below work on unsigned pixels (0..255): the reference's
+// signed taps are pixel - 128, every difference is the same, and
+// c8(x_signed + a) + 128 == u8c(x_unsigned + a). Both outcomes of each
+// per-segment test are formed and selected, so lanes never diverge.
+__device__ __forceinline__ int u8c(int v) { return min(max(v, 0), 255); }
+
+// §15.3 MBfilter (src/loop_filter.rs:331-371) on taps p[O..O+8).
 template <int O, int N>
 __device__ __forceinline__ void mb_filter(int (&p)[N], const Prm& q) {
   const int p3 = p[O], p2 = p[O + 1], p1 = p[O + 2], p0 = p[O + 3];
   const int q0 = p[O + 4], q1 = p[O + 5], q2 = p[O + 6], q3 = p[O + 7];
-  const bool yes = (iabs(p0 - q0) * 2 + (iabs(p1 - q1) >> 1)) <= q.mbedge && iabs(p3 - p2) <= q.interior &&
-                   iabs(p2 - p1) <= q.interior && iabs(p1 - p0) <= q.interior && iabs(q3 - q2) <= q.interior &&
-                   iabs(q2 - q1) <= q.interior && iabs(q1 - q0) <= q.interior;
-  const bool hv = iabs(p1 - p0) > q.hev || iabs(q1 - q0) > q.hev;
+  const int inner = max(iabs(p1 - p0), iabs(q1 - q0));
+  const int flat = max(max(iabs(p3 - p2), iabs(p2 - p1)), max(max(iabs(q3 - q2), iabs(q2 - q1)), inner));
+  const bool yes = (iabs(p0 - q0) * 2 + (iabs(p1 - q1) >> 1)) <= q.mbedge && flat <= q.interior;
+  const bool hv = inner > q.hev;
   const int w = c8(c8(p1 - q1) + 3 * (q0 - p0));
-  if (yes) {
-    if (!hv) {
-      int a = c8((27 * w + 63) >> 7);
-      p[O + 4] = c8(q0 - a);
-      p[O + 3] = c8(p0 + a);
-      a = c8((18 * w + 63) >> 7);
-      p[O + 5] = c8(q1 - a);
-      p[O + 2] = c8(p1 + a);
-      a = c8((9 * w + 63) >> 7);
-      p[O + 6] = c8(q2 - a);
-      p[O + 1] = c8(p2 + a);
-    } else {
-      const int a = c8(w + 4) >> 3, b = c8(w + 3) >> 3;
-      p[O + 4] = c8(q0 - a);
-      p[O + 3] = c8(p0 + b);
-    }
-  }
+  const int a27 = c8((27 * w + 63) >> 7), a18 = c8((18 * w + 63) >> 7), a9 = c8((9 * w + 63) >> 7);
+  const int aq = hv ? c8(w + 4) >> 3 : a27, ap = hv ? c8(w + 3) >> 3 : a27;
+  const bool wide = yes && !hv;
+  p[O + 4] = yes ? u8c(q0 - aq) : q0;
+  p[O + 3] = yes ? u8c(p0 + ap) : p0;
+  p[O + 5] = wide ? u8c(q1 - a18) : q1;
+  p[O + 2] = wide ? u8c(p1 + a18) : p1;
+  p[O + 6] = wide ? u8c(q2 - a9) : q2;
+  p[O + 1] = wide ? u8c(p2 + a9) : p2;
 }
 
 // §15.3 subblock_filter (src/loop_filter.rs:292-318).
@@ -161,44 +159,39 @@ template <int O, int N>
 __device__ __forceinline__ void sb_filter(int (&p)[N], const Prm& q) {
   const int p3 = p[O], p2 = p[O + 1], p1 = p[O + 2], p0 = p[O + 3];
   const int q0 = p[O + 4], q1 = p[O + 5], q2 = p[O + 6], q3 = p[O + 7];
-  const bool yes = (iabs(p0 - q0) * 2 + (iabs(p1 - q1) >> 1)) <= q.subedge && iabs(p3 - p2) <= q.interior &&
-                   iabs(p2 - p1) <= q.interior && iabs(p1 - p0) <= q.interior && iabs(q3 - q2) <= q.interior &&
-                   iabs(q2 - q1) <= q.interior && iabs(q1 - q0) <= q.interior;
-  const bool hv = iabs(p1 - p0) > q.hev || iabs(q1 - q0) > q.hev;
+  const int inner = max(iabs(p1 - p0), iabs(q1 - q0));
+  const int flat = max(max(iabs(p3 - p2), iabs(p2 - p1)), max(max(iabs(q3 - q2), iabs(q2 - q1)), inner));
+  const bool yes = (iabs(p0 - q0) * 2 + (iabs(p1 - q1) >> 1)) <= q.subedge && flat <= q.interior;
+  const bool hv = inner > q.hev;
   int a = c8((hv ? c8(p1 - q1) : 0) + 3 * (q0 - p0));
   const int b = c8(a + 3) >> 3;
   a = c8(a + 4) >> 3;
-  if (yes) {
-    p[O + 4] = c8(q0 - a);
-    p[O + 3] = c8(p0 + b);
-    if (!hv) {
-      const int a2 = (a + 1) >> 1;
-      p[O + 5] = c8(q1 - a2);
-      p[O + 2] = c8(p1 + a2);
-    }
-  }
+  const int a2 = (a + 1) >> 1;
+  const bool wide = yes && !hv;
+  p[O + 4] = yes ? u8c(q0 - a) : q0;
+  p[O + 3] = yes ? u8c(p0 + b) : p0;
+  p[O + 5] = wide ? u8c(q1 - a2) : q1;
+  p[O + 2] = wide ? u8c(p1 + a2) : p1;
 }
 
-// §15.2 simple_segment (src/loop_filter.rs:235-247) on signed taps.
+// §15.2 simple_segment (src/loop_filter.rs:235-247).
 template <int O, int N>
 __device__ __forceinline__ void simple_filter(int (&p)[N], int edge) {
   const int p1 = p[O], p0 = p[O + 1], q0 = p[O + 2], q1 = p[O + 3];
-  if (iabs(p0 - q0) * 2 + (iabs(p1 - q1) >> 1) <= edge) {
-    int a = c8(c8(p1 - q1) + 3 * (q0 - p0));
-    const int b = c8(a + 3) >> 3;
-    a = c8(a + 4) >> 3;
-    p[O + 2] = c8(q0 - a);
-    p[O + 1] = c8(p0 + b);
-  }
+  const bool yes = iabs(p0 - q0) * 2 + (iabs(p1 - q1) >> 1) <= edge;
+  int a = c8(c8(p1 - q1) + 3 * (q0 - p0));
+  const int b = c8(a + 3) >> 3;
+  a = c8(a + 4) >> 3;
+  p[O + 2] = yes ? u8c(q0 - a) : q0;
+  p[O + 1] = yes ? u8c(p0 + b) : p0;
 }
 
 __device__ __forceinline__ void unpack4(uint32_t w, int* o) {
 #pragma unroll
-  for (int k = 0; k < 4; k++) o[k] = (int)((w >> (8 * k)) & 0xffu) - 128;
+  for (int k = 0; k < 4; k++) o[k] = (int)((w >> (8 * k)) & 0xffu);
 }
 __device__ __forceinline__ uint32_t pack4(const int* o) {
-  return (uint32_t)(o[0] + 128) | ((uint32_t)(o[1] + 128) << 8) | ((uint32_t)(o[2] + 128) << 16) |
-         ((uint32_t)(o[3] + 128) << 24);
+  return (uint32_t)o[0] | ((uint32_t)o[1] << 8) | ((uint32_t)o[2] << 16) | ((uint32_t)o[3] << 24);
 }
 
 __device__ __forceinline__ uint8_t* slot_ptr(uint8_t* slots, int r, int c) {
@@ -333,12 +326,12 @@ __device__ __forceinline__ uint32_t finish_mb(const LfArgs& a, const uint8_t* sl
 
 // Filter MB (r, c) held in its slot; neighbours in their slots. The
 // caller's half-warp (mask hm) runs this together.
-__device__ __forceinline__ void filter_mb(const LfArgs& a, uint8_t* slots, int level0, int sharp, int r, int c,
+__device__ __forceinline__ void filter_mb(const LfArgs& a, const Prm* prm, uint8_t* slots, int level0, int r, int c,
                                           bool has_top, int l, unsigned hm) {
   const vp8a_mb_lf_info m = a.mbs[(size_t)r * a.mb_cols + c];
   const int level = mb_level(a.base, level0, m);
   if (level == 0) return;
-  const Prm q = derive(level, sharp, a.base.key_frame != 0);
+  const Prm q = prm[level];
   const bool sub = m.y_mode_is_bpred || m.has_coeffs;
   const bool has_left = c > 0;
   uint8_t* me = slot_ptr(slots, r, c);
@@ -367,9 +360,9 @@ __device__ __forceinline__ void filter_mb(const LfArgs& a, uint8_t* slots, int l
     {
       int p[20];
 #pragma unroll
-      for (int k = 0; k < 4; k++) p[k] = has_top ? (int)above[(12 + k) * 16 + l] - 128 : 0;
+      for (int k = 0; k < 4; k++) p[k] = has_top ? (int)above[(12 + k) * 16 + l] : 0;
 #pragma unroll
-      for (int k = 0; k < 16; k++) p[4 + k] = (int)me[k * 16 + l] - 128;
+      for (int k = 0; k < 16; k++) p[4 + k] = (int)me[k * 16 + l];
       if (has_top) simple_filter<2>(p, q.mbedge);
       if (sub) {
         simple_filter<6>(p, q.subedge);
@@ -378,9 +371,9 @@ __device__ __forceinline__ void filter_mb(const LfArgs& a, uint8_t* slots, int l
       }
       if (has_top)
 #pragma unroll
-        for (int k = 2; k < 4; k++) above[(12 + k) * 16 + l] = (uint8_t)(p[k] + 128);
+        for (int k = 2; k < 4; k++) above[(12 + k) * 16 + l] = (uint8_t)(p[k]);
 #pragma unroll
-      for (int k = 0; k < 16; k++) me[k * 16 + l] = (uint8_t)(p[4 + k] + 128);
+      for (int k = 0; k < 16; k++) me[k * 16 + l] = (uint8_t)(p[4 + k]);
     }
     __syncwarp(hm);
     return;
@@ -421,9 +414,9 @@ __device__ __forceinline__ void filter_mb(const LfArgs& a, uint8_t* slots, int l
   {
     int p[20];
 #pragma unroll
-    for (int k = 0; k < 4; k++) p[k] = has_top ? (int)above[(12 + k) * 16 + l] - 128 : 0;
+    for (int k = 0; k < 4; k++) p[k] = has_top ? (int)above[(12 + k) * 16 + l] : 0;
 #pragma unroll
-    for (int k = 0; k < 16; k++) p[4 + k] = (int)me[k * 16 + l] - 128;
+    for (int k = 0; k < 16; k++) p[4 + k] = (int)me[k * 16 + l];
     if (has_top) mb_filter<0>(p, q);
     if (sub) {
       sb_filter<4>(p, q);
@@ -432,23 +425,23 @@ __device__ __forceinline__ void filter_mb(const LfArgs& a, uint8_t* slots, int l
     }
     if (has_top)
 #pragma unroll
-      for (int k = 1; k < 4; k++) above[(12 + k) * 16 + l] = (uint8_t)(p[k] + 128);
+      for (int k = 1; k < 4; k++) above[(12 + k) * 16 + l] = (uint8_t)(p[k]);
 #pragma unroll
-    for (int k = 0; k < 16; k++) me[k * 16 + l] = (uint8_t)(p[4 + k] + 128);
+    for (int k = 0; k < 16; k++) me[k * 16 + l] = (uint8_t)(p[4 + k]);
   }
   {
     int p[12];
 #pragma unroll
-    for (int k = 0; k < 4; k++) p[k] = has_top ? (int)above[pl + (4 + k) * 8 + cl] - 128 : 0;
+    for (int k = 0; k < 4; k++) p[k] = has_top ? (int)above[pl + (4 + k) * 8 + cl] : 0;
 #pragma unroll
-    for (int k = 0; k < 8; k++) p[4 + k] = (int)me[pl + k * 8 + cl] - 128;
+    for (int k = 0; k < 8; k++) p[4 + k] = (int)me[pl + k * 8 + cl];
     if (has_top) mb_filter<0>(p, q);
     if (sub) sb_filter<4>(p, q);
     if (has_top)
 #pragma unroll
-      for (int k = 1; k < 4; k++) above[pl + (4 + k) * 8 + cl] = (uint8_t)(p[k] + 128);
+      for (int k = 1; k < 4; k++) above[pl + (4 + k) * 8 + cl] = (uint8_t)(p[k]);
 #pragma unroll
-    for (int k = 0; k < 8; k++) me[pl + k * 8 + cl] = (uint8_t)(p[4 + k] + 128);
+    for (int k = 0; k < 8; k++) me[pl + k * 8 + cl] = (uint8_t)(p[4 + k]);
   }
   __syncwarp(hm);
 }
@@ -511,6 +504,10 @@ __global__ void __launch_bounds__(1024) lf_sweep_kernel(LfArgs a) {
   }
   uint8_t* slots = a.smem_slots ? smem_slots : a.gslots + (size_t)blockIdx.x * a.mb_rows * 4 * SLOT_STRIDE;
   const bool score = a.ssd_out != nullptr;
+  // LoopFilterParams::derive for every level at this candidate's sharpness.
+  __shared__ Prm prm[64];
+  for (int i = threadIdx.x; i < 64; i += blockDim.x) prm[i] = derive(i, sharp, a.base.key_frame != 0);
+  __syncthreads();
   for (int t = 0; t < a.steps; t++) {
     const int e = a.sched_off[t + 1];
     for (int i = a.sched_off[t] + hw; i < e; i += nhw) {
@@ -523,7 +520,7 @@ __global__ void __launch_bounds__(1024) lf_sweep_kernel(LfArgs a) {
       }
       store_slot(slot_ptr(slots, r, c), rec, l);
       __syncwarp(hm);
-      filter_mb(a, slots, level0, sharp, r, c, a.row_top[r] != 0, l, hm);
+      filter_mb(a, prm, slots, level0, r, c, a.row_top[r] != 0, l, hm);
     }
     __syncthreads();
   }
