@@ -61,6 +61,11 @@ struct LfArgs {
   int max_active;            // most rows active at one step
   int recon_words;           // planes and strides allow 4-byte accesses
   int source_words;
+  // Next-step prefetch: each half-warp copies its next MB's reconstruction,
+  // source rows and MB record into its own staging area (dynamic shared
+  // memory at byte stage_off) while the current step runs (cp.async).
+  int prefetch;
+  int stage_off;
   uint64_t* ssd_out;  // [64 * 8], indexed level * 8 + sharpness
   uint8_t* oy;        // write-back planes (apply mode) or null
   uint8_t* ou;
@@ -326,9 +331,8 @@ __device__ __forceinline__ uint32_t finish_mb(const LfArgs& a, const uint8_t* sl
 
 // Filter MB (r, c) held in its slot; neighbours in their slots. The
 // caller's half-warp (mask hm) runs this together.
-__device__ __forceinline__ void filter_mb(const LfArgs& a, const Prm* prm, uint8_t* slots, int level0, int r, int c,
-                                          bool has_top, int l, unsigned hm) {
-  const vp8a_mb_lf_info m = a.mbs[(size_t)r * a.mb_cols + c];
+__device__ __forceinline__ void filter_mb(const LfArgs& a, const Prm* prm, const vp8a_mb_lf_info m, uint8_t* slots,
+                                          int level0, int r, int c, bool has_top, int l, unsigned hm) {
   const int level = mb_level(a.base, level0, m);
   if (level == 0) return;
   const Prm q = prm[level];
@@ -446,6 +450,47 @@ __device__ __forceinline__ void filter_mb(const LfArgs& a, const Prm* prm, uint8
   __syncwarp(hm);
 }
 
+// A half-warp's staged next MB.
+struct __align__(16) Stage {
+  uint8_t rec[384];  // Y rows 0-15, U rows 0-7, V rows 0-7 (slot layout)
+  uint8_t src[384];  // the source under the MB the step finishes, same layout
+  vp8a_mb_lf_info info;
+  uint8_t pad[8];
+};
+static_assert(sizeof(Stage) % 16 == 0, "Stage keeps 16-byte copies aligned");
+
+__device__ __forceinline__ void cp_async(void* smem, const void* g, int bytes, int src_bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+  if (bytes == 16)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(g), "r"(src_bytes) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(g), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Start copying MB (r, c)'s inputs into `g`: lane l copies luma row l and
+// chroma row l & 7 of U (l < 8) or V of the reconstruction, the same rows of
+// the source under MB (r, c - 4) when one is finished with it (bytes outside
+// the visible window are filled with zeros, never read), and lane 0 the MB
+// record.
+__device__ __forceinline__ void prefetch_mb(const LfArgs& a, Stage* g, int r, int c, int l, bool score) {
+  cp_async(g->rec + l * 16, a.y + (size_t)(r * 16 + l) * a.ys + (size_t)c * 16, 16, 16);
+  const int pl = l < 8 ? 256 : 320, cr = l & 7;
+  cp_async(g->rec + pl + cr * 8, (l < 8 ? a.u : a.v) + (size_t)(r * 8 + cr) * a.cs + (size_t)c * 8, 8, 8);
+  if (score && c >= 4) {
+    const int yy = r * 16 + l, x0 = (c - 4) * 16;
+    const int ny = yy < a.height ? clampi(a.width - x0, 0, 16) : 0;
+    cp_async(g->src + l * 16, ny > 0 ? (const void*)(a.sy + (size_t)yy * a.sys + x0) : (const void*)a.sy, 16, ny);
+    const int cw = (a.width + 1) >> 1, ch = (a.height + 1) >> 1, cy = r * 8 + cr, cx0 = (c - 4) * 8;
+    const int nc = cy < ch ? clampi(cw - cx0, 0, 8) : 0;
+    const uint8_t* sp = l < 8 ? a.su : a.sv;
+    cp_async(g->src + pl + cr * 8, nc > 0 ? (const void*)(sp + (size_t)cy * a.scs + cx0) : (const void*)sp, 8, nc);
+  }
+  if (l == 0) cp_async(&g->info, a.mbs + (size_t)r * a.mb_cols + c, 8, 8);
+  cp_async_commit();
+}
+
 __device__ __forceinline__ void block_sum_store(uint64_t v, uint64_t* dst) {
   __shared__ unsigned long long red[32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -508,19 +553,88 @@ __global__ void __launch_bounds__(1024) lf_sweep_kernel(LfArgs a) {
   __shared__ Prm prm[64];
   for (int i = threadIdx.x; i < 64; i += blockDim.x) prm[i] = derive(i, sharp, a.base.key_frame != 0);
   __syncthreads();
+  Stage* stage = a.prefetch ? (Stage*)(smem_slots + a.stage_off) + hw : nullptr;
+  // The half-warp's first MB of step t, or -1.
+  auto first_mb = [&](int t) -> int {
+    if (t >= a.steps) return -1;
+    const int i = a.sched_off[t] + hw;
+    return i < a.sched_off[t + 1] ? i : -1;
+  };
+  bool staged = false;
+  if (a.prefetch) {
+    const int i = first_mb(0);
+    if (i >= 0) {
+      const int r = a.sched_row[i];
+      prefetch_mb(a, stage, r, 0 - a.row_t0[r], l, score);
+      staged = true;
+    }
+  }
   for (int t = 0; t < a.steps; t++) {
-    const int e = a.sched_off[t + 1];
-    for (int i = a.sched_off[t] + hw; i < e; i += nhw) {
+    const int b = a.sched_off[t], e = a.sched_off[t + 1];
+    bool next_issued = false;
+    for (int i = b + hw; i < e; i += nhw) {
       const int r = a.sched_row[i], c = t - a.row_t0[r];
-      const MbWords rec = fetch_recon(a, r, c, l);
+      MbWords rec;
+      SrcWords sw{};
+      vp8a_mb_lf_info m;
+      if (staged && i == b + hw) {
+        cp_async_wait_all();
+        __syncwarp(hm);
+        const uint32_t* ry = (const uint32_t*)(stage->rec + l * 16);
+        const uint32_t* rc = (const uint32_t*)(stage->rec + (l < 8 ? 256 : 320) + (l & 7) * 8);
+#pragma unroll
+        for (int k = 0; k < 4; k++) rec.y[k] = ry[k];
+        rec.c[0] = rc[0];
+        rec.c[1] = rc[1];
+        if (score && c >= 4) {
+          const uint32_t* sy = (const uint32_t*)(stage->src + l * 16);
+          const uint32_t* sc = (const uint32_t*)(stage->src + (l < 8 ? 256 : 320) + (l & 7) * 8);
+          const int ny = r * 16 + l < a.height ? clampi(a.width - (c - 4) * 16, 0, 16) : 0;
+          const int cw = (a.width + 1) >> 1, ch = (a.height + 1) >> 1;
+          const int nc = r * 8 + (l & 7) < ch ? clampi(cw - (c - 4) * 8, 0, 8) : 0;
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            sw.y[k] = sy[k];
+            sw.my[k] = vis_mask(ny, k);
+          }
+#pragma unroll
+          for (int k = 0; k < 2; k++) {
+            sw.c[k] = sc[k];
+            sw.mc[k] = vis_mask(nc, k);
+          }
+        }
+        m = stage->info;
+        staged = false;
+      } else {
+        rec = fetch_recon(a, r, c, l);
+        if (score && c >= 4) sw = fetch_source(a, r, c - 4, l);
+        m = a.mbs[(size_t)r * a.mb_cols + c];
+      }
       if (c >= 4) {
-        const SrcWords sw = score ? fetch_source(a, r, c - 4, l) : SrcWords{};
         acc += finish_mb(a, slots, r, c - 4, l, sw);
         __syncwarp(hm);
       }
       store_slot(slot_ptr(slots, r, c), rec, l);
       __syncwarp(hm);
-      filter_mb(a, prm, slots, level0, r, c, a.row_top[r] != 0, l, hm);
+      if (a.prefetch && !next_issued) {
+        // The staging area is free again: start the next step's copies.
+        const int j = first_mb(t + 1);
+        if (j >= 0) {
+          const int r2 = a.sched_row[j];
+          prefetch_mb(a, stage, r2, t + 1 - a.row_t0[r2], l, score);
+          staged = true;
+        }
+        next_issued = true;
+      }
+      filter_mb(a, prm, m, slots, level0, r, c, a.row_top[r] != 0, l, hm);
+    }
+    if (a.prefetch && !next_issued) {
+      const int j = first_mb(t + 1);
+      if (j >= 0) {
+        const int r2 = a.sched_row[j];
+        prefetch_mb(a, stage, r2, t + 1 - a.row_t0[r2], l, score);
+        staged = true;
+      }
     }
     __syncthreads();
   }
@@ -696,6 +810,25 @@ vp8a_status stage_lf(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_planes* planes,
   return VP8A_OK;
 }
 
+// Dynamic shared memory of a sweep launch: the slot rings, then (when the
+// planes allow aligned asynchronous copies and it fits) one staging area
+// per half-warp for the next-step prefetch.
+size_t sweep_smem(LfArgs& a, int threads, size_t slot_bytes, int max_smem) {
+  auto al = [](const void* p, uint64_t stride, unsigned n) { return ((uintptr_t)p % n == 0) && (stride % n == 0); };
+  const bool score = a.ssd_out != nullptr;
+  bool ok = al(a.y, a.ys, 16) && al(a.u, a.cs, 8) && al(a.v, a.cs, 8) && (uintptr_t)a.mbs % 8 == 0;
+  if (score) ok = ok && al(a.sy, a.sys, 16) && al(a.su, a.scs, 8) && al(a.sv, a.scs, 8);
+  const size_t stage_bytes = (size_t)(threads / 16) * sizeof(Stage);
+  if (ok && slot_bytes + stage_bytes + 1024 <= (size_t)max_smem) {
+    a.prefetch = 1;
+    a.stage_off = (int)slot_bytes;
+    return slot_bytes + stage_bytes;
+  }
+  a.prefetch = 0;
+  a.stage_off = 0;
+  return slot_bytes;
+}
+
 // Launch the sweep over `n` candidates (pairs of level, sharpness).
 vp8a_status launch_sweep(vp8a_ctx* ctx, vp8a::Stager& st, LfArgs a, const uint8_t* cands, int n) {
   if (n == 0) return VP8A_OK;
@@ -711,13 +844,15 @@ vp8a_status launch_sweep(vp8a_ctx* ctx, vp8a::Stager& st, LfArgs a, const uint8_
   if (slot_bytes + 1024 <= (size_t)max_smem) {
     a.smem_slots = 1;
     a.gslots = nullptr;
-    VP8A_CUDA(cudaFuncSetAttribute(lf_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slot_bytes));
-    lf_sweep_kernel<<<n, threads, slot_bytes, ctx->stream>>>(a);
+    const size_t smem = sweep_smem(a, threads, slot_bytes, max_smem);
+    VP8A_CUDA(cudaFuncSetAttribute(lf_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    lf_sweep_kernel<<<n, threads, smem, ctx->stream>>>(a);
   } else {
     void* g;
     if ((s = st.scratch(slot_bytes * n, &g)) != VP8A_OK) return s;
     a.smem_slots = 0;
     a.gslots = (uint8_t*)g;
+    a.prefetch = 0;
     lf_sweep_kernel<<<n, threads, 0, ctx->stream>>>(a);
   }
   VP8A_CUDA(cudaGetLastError());
@@ -1171,8 +1306,9 @@ vp8a_status vp8a_filter_sweep_noalloc(vp8a_ctx* ctx, const vp8a_planes* planes, 
     return VP8A_E_INVALID_DIMENSIONS;
   }
   const int threads = std::min(1024, std::max(32, (16 * max_active + 31) / 32 * 32));
-  VP8A_CUDA(cudaFuncSetAttribute(lf_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slot_bytes));
-  lf_sweep_kernel<<<NA_CANDIDATES, threads, slot_bytes, ctx->stream>>>(a);
+  const size_t smem = sweep_smem(a, threads, slot_bytes, max_smem);
+  VP8A_CUDA(cudaFuncSetAttribute(lf_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  lf_sweep_kernel<<<NA_CANDIDATES, threads, smem, ctx->stream>>>(a);
   VP8A_CUDA(cudaGetLastError());
   ctx->launches++;
   // Level 0 scores the same for every sharpness.
