@@ -72,6 +72,37 @@ def test_sweep_table_parity(ctx, oracle, every_rows):
     assert np.array_equal(got, want)
 
 
+@pytest.mark.parametrize("size", [(64, 2048), (48, 2400)])
+def test_sweep_tall_pictures(ctx, oracle, size):
+    # Tall pictures take the sweep's other shared-memory layouts: 128 MB rows
+    # keep compact slot rings (with the next-MB prefetch), 150 rows keep the
+    # rings in global memory.
+    src, recon, m = lf_case(*size, seed=size[1])
+    base = abi.filter_config(0, 1)
+    got = vp8a.filter_sweep(ctx, recon, m, base, src, 0)
+    want = oracle.filter_sweep(recon, m, base, src, 0, threads=8)
+    assert np.array_equal(got, want)
+
+
+def test_sweep_unaligned_strides(ctx, oracle):
+    # Row strides that allow neither word nor asynchronous copies.
+    src, recon, m = lf_case(96, 72, seed=11)
+
+    def widen(planes, extra):
+        out = []
+        for p in planes:
+            w = np.zeros((p.shape[0], p.shape[1] + extra), np.uint8)
+            w[:, : p.shape[1]] = p
+            out.append(w[:, : p.shape[1]])
+        return out
+
+    rs, ss = widen(recon, 3), widen(src, 5)
+    base = abi.filter_config(0, 2)
+    got = vp8a.filter_sweep(ctx, rs, m, base, ss, 0)
+    want = oracle.filter_sweep(recon, m, base, src, 0, threads=8)
+    assert np.array_equal(got, want)
+
+
 @pytest.mark.parametrize("size,seed", [((320, 240), 3), ((72, 40), 4), ((33, 65), 5)])
 def test_selection_parity(ctx, oracle, size, seed):
     src, recon, m = lf_case(*size, seed=seed)
