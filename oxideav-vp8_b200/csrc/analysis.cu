@@ -979,29 +979,40 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
       }
       __syncthreads();
       const int mbx = c * 16, mby = r * 16;
-      if (tid == 0) {
-        cen = census(nb[0], nb[1], nb[2], c, r, a.mb_cols, a.mb_rows);
-        Plan p;
-        const vp8a_mv bp = cen.best_predictor;
-        p.wx0 = mbx + snap_whole(clamp_component(bp.col)) / 4 - WIN_LEAD;
-        p.wy0 = mby + snap_whole(clamp_component(bp.row)) / 4 - WIN_LEAD;
-        p.hn_x = mbx + int_off(cen.nearest.col) - 2;
-        p.hn_y = mby + int_off(cen.nearest.row) - 2;
-        p.hr_x = mbx + int_off(cen.near_.col) - 2;
-        p.hr_y = mby + int_off(cen.near_.row) - 2;
-        p.nblocks = 0;
-        auto addb = [&](vp8a_mv m) -> int {
-          const int ox = int_off(m.col), oy = int_off(m.row);
-          for (int i = 0; i < p.nblocks; i++)
-            if (p.box[i] == ox && p.boy[i] == oy) return i;
-          p.box[p.nblocks] = ox;
-          p.boy[p.nblocks] = oy;
-          return p.nblocks++;
-        };
-        p.colblk[0] = addb(vp8a_mv{0, 0});
-        for (int k = 0; k < 4; k++) p.colblk[1 + k] = addb(ext_left(nb[1], 4 * k));
-        for (int k = 0; k < 4; k++) p.colblk[5 + k] = addb(ext_above(nb[0], k));
-        plan = p;
+      if (warp == 0) {
+        // The census (every lane, registers only) and the staging plan: lanes
+        // 0-8 hold the SPLITMV column vectors (ZERO, the left neighbour's
+        // at anchors 0/4/8/12, the above neighbour's at 0-3); vectors with
+        // equal integer offsets share one staged block, numbered in column
+        // order of first appearance.
+        const Census cs = census(nb[0], nb[1], nb[2], c, r, a.mb_cols, a.mb_rows);
+        const vp8a_mv m = lane == 0 ? vp8a_mv{0, 0}
+                                    : (lane < 5 ? ext_left(nb[1], 4 * ((lane - 1) & 3)) : ext_above(nb[0], (lane - 5) & 3));
+        const int ox = int_off(m.col), oy = int_off(m.row);
+        const unsigned key = ((unsigned)(uint16_t)oy << 16) | (uint16_t)ox;
+        const unsigned cols9 = 0x1ffu;
+        const unsigned same = __match_any_sync(FULL, lane < 9 ? key : 0xffffffffu) & cols9;
+        const int leader = __ffs(same) - 1;
+        const unsigned leaders = __ballot_sync(FULL, lane < 9 && leader == lane);
+        if (lane < 9) {
+          const int idx = __popc(leaders & ((1u << leader) - 1u));
+          plan.colblk[lane] = idx;
+          if (leader == lane) {
+            plan.box[idx] = ox;
+            plan.boy[idx] = oy;
+          }
+        }
+        if (lane == 0) {
+          cen = cs;
+          const vp8a_mv bp = cs.best_predictor;
+          plan.wx0 = mbx + snap_whole(clamp_component(bp.col)) / 4 - WIN_LEAD;
+          plan.wy0 = mby + snap_whole(clamp_component(bp.row)) / 4 - WIN_LEAD;
+          plan.hn_x = mbx + int_off(cs.nearest.col) - 2;
+          plan.hn_y = mby + int_off(cs.nearest.row) - 2;
+          plan.hr_x = mbx + int_off(cs.near_.col) - 2;
+          plan.hr_y = mby + int_off(cs.near_.row) - 2;
+          plan.nblocks = __popc(leaders);
+        }
       }
       __syncthreads();
       stage_ref(P, R, plan, mbx, mby, a.words, tid, AN_THREADS);

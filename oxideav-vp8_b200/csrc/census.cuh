@@ -96,63 +96,70 @@ struct Census {
 
 // find_near_mvs (src/near_mv.rs:310-402; default SignBias) + clamps
 // (MvClampRect::for_mb / clamp_mv, :236-283) + mv_ref_probs (:404).
-static __device__ Census census(const MbInfoDev& above, const MbInfoDev& left, const MbInfoDev& al, int mb_col, int mb_row,
-                         int mb_cols, int mb_rows) {
-  vp8a_mv nm[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
-  int cnt[4] = {0, 0, 0, 0};
-  int mi = 0, ci = 0;
+// The reference's near-MV list index and count index always advance
+// together, so one index `mi` drives both; the list and the counts live in
+// registers (every index is resolved with selects).
+static __device__ __forceinline__ Census census(const MbInfoDev& above, const MbInfoDev& left, const MbInfoDev& al,
+                                                int mb_col, int mb_row, int mb_cols, int mb_rows) {
+  vp8a_mv n0 = {0, 0}, n1 = {0, 0}, n2 = {0, 0}, n3 = {0, 0};
+  int c0 = 0, c1 = 0, c2 = 0, c3 = 0, mi = 0;
+  auto last = [&]() { return mi == 0 ? n0 : (mi == 1 ? n1 : (mi == 2 ? n2 : n3)); };
+  auto push = [&](vp8a_mv v) {
+    mi++;
+    if (mi == 1) n1 = v;
+    else if (mi == 2) n2 = v;
+    else n3 = v;
+  };
+  auto count = [&](int w) {
+    if (mi == 0) c0 += w;
+    else if (mi == 1) c1 += w;
+    else if (mi == 2) c2 += w;
+    else c3 += w;
+  };
   if (above.ref_frame != VP8A_REF_INTRA) {
-    if (!mv_zero(above.mv)) {
-      mi++;
-      nm[mi] = above.mv;
-      ci++;
-    }
-    cnt[ci] += 2;
+    if (!mv_zero(above.mv)) push(above.mv);
+    count(2);
   }
   if (left.ref_frame != VP8A_REF_INTRA) {
     if (!mv_zero(left.mv)) {
-      if (!mv_eq(left.mv, nm[mi])) {
-        mi++;
-        nm[mi] = left.mv;
-        ci++;
-      }
-      cnt[ci] += 2;
+      if (!mv_eq(left.mv, last())) push(left.mv);
+      count(2);
     } else {
-      cnt[0] += 2;
+      c0 += 2;
     }
   }
   if (al.ref_frame != VP8A_REF_INTRA) {
     if (!mv_zero(al.mv)) {
-      if (!mv_eq(al.mv, nm[mi])) {
-        mi++;
-        nm[mi] = al.mv;
-        ci++;
-      }
-      cnt[ci] += 1;
+      if (!mv_eq(al.mv, last())) push(al.mv);
+      count(1);
     } else {
-      cnt[0] += 1;
+      c0 += 1;
     }
   }
-  if (cnt[3] != 0 && mv_eq(nm[mi], nm[1])) cnt[1] += 1;
-  cnt[3] = (above.is_split + left.is_split) * 2 + al.is_split;
-  if (cnt[2] > cnt[1]) {
-    int t = cnt[1];
-    cnt[1] = cnt[2];
-    cnt[2] = t;
-    vp8a_mv tm = nm[1];
-    nm[1] = nm[2];
-    nm[2] = tm;
+  if (c3 != 0 && mv_eq(last(), n1)) c1 += 1;
+  c3 = (above.is_split + left.is_split) * 2 + al.is_split;
+  if (c2 > c1) {
+    const int t = c1;
+    c1 = c2;
+    c2 = t;
+    const vp8a_mv tm = n1;
+    n1 = n2;
+    n2 = tm;
   }
-  if (cnt[1] >= cnt[0]) nm[0] = nm[1];
+  if (c1 >= c0) n0 = n1;
   const int to_left = -((mb_col + 1) << 6), to_right = (mb_cols - mb_col) << 6;
   const int to_top = -((mb_row + 1) << 6), to_bottom = (mb_rows - mb_row) << 6;
   Census c;
-  vp8a_mv* outs[3] = {&c.best_predictor, &c.nearest, &c.near_};
-  for (int k = 0; k < 3; k++) {
-    outs[k]->col = (int16_t)clampi(nm[k].col, to_left, to_right);
-    outs[k]->row = (int16_t)clampi(nm[k].row, to_top, to_bottom);
-  }
-  for (int k = 0; k < 4; k++) c.p[k] = c_counts_to_probs[cnt[k]][k];
+  c.best_predictor.col = (int16_t)clampi(n0.col, to_left, to_right);
+  c.best_predictor.row = (int16_t)clampi(n0.row, to_top, to_bottom);
+  c.nearest.col = (int16_t)clampi(n1.col, to_left, to_right);
+  c.nearest.row = (int16_t)clampi(n1.row, to_top, to_bottom);
+  c.near_.col = (int16_t)clampi(n2.col, to_left, to_right);
+  c.near_.row = (int16_t)clampi(n2.row, to_top, to_bottom);
+  c.p[0] = c_counts_to_probs[c0][0];
+  c.p[1] = c_counts_to_probs[c1][1];
+  c.p[2] = c_counts_to_probs[c2][2];
+  c.p[3] = c_counts_to_probs[c3][3];
   return c;
 }
 
