@@ -38,6 +38,11 @@ constexpr unsigned FULL = 0xffffffffu;
 // An MB slot holds Y 16x16 + U 8x8 + V 8x8 = 384 bytes, padded to 400 so
 // that the slots of neighbouring rows start on different banks.
 constexpr int SLOT_STRIDE = 400;
+// Slots per MB row: MB (r, c) takes slot c % 3 once MB (r, c - 3) is final
+// (its last writer, MB (r + 1, c - 3), ran the step before) and scored.
+// While MB (r, c) runs, row r - 1 runs (r - 1, c + 2) and row r + 1 runs
+// (r + 1, c - 2): the slots they touch are never the one being refilled.
+constexpr int RING = 3;
 
 struct LfArgs {
   const uint8_t* y;
@@ -66,6 +71,8 @@ struct LfArgs {
   // memory at byte stage_off) while the current step runs (cp.async).
   int prefetch;
   int stage_off;
+  int n_cands;    // candidates in `cands`; a CTA takes NC consecutive ones
+  int ring_bytes; // one candidate's slot rings
   uint64_t* ssd_out;  // [64 * 8], indexed level * 8 + sharpness
   uint8_t* oy;        // write-back planes (apply mode) or null
   uint8_t* ou;
@@ -200,7 +207,7 @@ __device__ __forceinline__ uint32_t pack4(const int* o) {
 }
 
 __device__ __forceinline__ uint8_t* slot_ptr(uint8_t* slots, int r, int c) {
-  return slots + ((size_t)r * 4 + (c & 3)) * SLOT_STRIDE;
+  return slots + ((size_t)r * RING + c % RING) * SLOT_STRIDE;
 }
 
 // One half-warp handles one MB: lane l (0-15) owns luma row l and chroma
@@ -471,18 +478,18 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // Start copying MB (r, c)'s inputs into `g`: lane l copies luma row l and
 // chroma row l & 7 of U (l < 8) or V of the reconstruction, the same rows of
-// the source under MB (r, c - 4) when one is finished with it (bytes outside
+// the source under MB (r, c - 3) when one is finished with it (bytes outside
 // the visible window are filled with zeros, never read), and lane 0 the MB
 // record.
 __device__ __forceinline__ void prefetch_mb(const LfArgs& a, Stage* g, int r, int c, int l, bool score) {
   cp_async(g->rec + l * 16, a.y + (size_t)(r * 16 + l) * a.ys + (size_t)c * 16, 16, 16);
   const int pl = l < 8 ? 256 : 320, cr = l & 7;
   cp_async(g->rec + pl + cr * 8, (l < 8 ? a.u : a.v) + (size_t)(r * 8 + cr) * a.cs + (size_t)c * 8, 8, 8);
-  if (score && c >= 4) {
-    const int yy = r * 16 + l, x0 = (c - 4) * 16;
+  if (score && c >= RING) {
+    const int yy = r * 16 + l, x0 = (c - RING) * 16;
     const int ny = yy < a.height ? clampi(a.width - x0, 0, 16) : 0;
     cp_async(g->src + l * 16, ny > 0 ? (const void*)(a.sy + (size_t)yy * a.sys + x0) : (const void*)a.sy, 16, ny);
-    const int cw = (a.width + 1) >> 1, ch = (a.height + 1) >> 1, cy = r * 8 + cr, cx0 = (c - 4) * 8;
+    const int cw = (a.width + 1) >> 1, ch = (a.height + 1) >> 1, cy = r * 8 + cr, cx0 = (c - RING) * 8;
     const int nc = cy < ch ? clampi(cw - cx0, 0, 8) : 0;
     const uint8_t* sp = l < 8 ? a.su : a.sv;
     cp_async(g->src + pl + cr * 8, nc > 0 ? (const void*)(sp + (size_t)cy * a.scs + cx0) : (const void*)sp, 8, nc);
@@ -491,67 +498,63 @@ __device__ __forceinline__ void prefetch_mb(const LfArgs& a, Stage* g, int r, in
   cp_async_commit();
 }
 
-__device__ __forceinline__ void block_sum_store(uint64_t v, uint64_t* dst) {
-  __shared__ unsigned long long red[32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-  if (lane == 0) red[warp] = v;
-  __syncthreads();
-  if (warp == 0) {
-    v = lane < (int)(blockDim.x >> 5) ? red[lane] : 0;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-    if (lane == 0) *dst = v;
-  }
-}
 
 // One CTA per candidate. At step t the MBs of the rows listed in
 // sched_row[sched_off[t] .. sched_off[t+1]) are independent; half-warp h
 // takes the h-th, (h + H)-th, ... of them. Per MB the global fetches (its
 // reconstruction and the source under the MB finished in its slot) are
 // issued together before the slot is touched.
+// SSD totals of the CTA's candidates into the table.
+template <int NC>
+__device__ __forceinline__ void block_sums_store(const uint64_t (&v)[NC], const LfArgs& a, const int (&lv)[NC],
+                                                 const int (&sh)[NC], int nc) {
+  __shared__ unsigned long long red[NC][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NC; k++) {
+    uint64_t x = v[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(FULL, x, o);
+    if (lane == 0) red[k][warp] = x;
+  }
+  __syncthreads();
+  const int nwarps = (int)(blockDim.x >> 5);
+  for (int k = warp; k < nc; k += nwarps) {
+    uint64_t x = lane < nwarps ? red[k][lane] : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(FULL, x, o);
+    if (lane == 0) a.ssd_out[lv[k] * 8 + sh[k]] = x;
+  }
+}
+
+// NC candidates per CTA over one step schedule: the MB inputs are fetched
+// (or prefetched) once and each candidate filters them in its own slot
+// rings. A sweep-mode level-0 candidate is not filtered at all: it scores
+// the unfiltered reconstruction (score_filter_candidate's short cut,
+// src/loop_filter.rs:2071).
+template <int NC>
 __global__ void __launch_bounds__(1024) lf_sweep_kernel(LfArgs a) {
   extern __shared__ __align__(16) uint8_t smem_slots[];
-  const int level0 = a.cands[2 * blockIdx.x], sharp = a.cands[2 * blockIdx.x + 1];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int hw = threadIdx.x >> 4, nhw = blockDim.x >> 4, l = threadIdx.x & 15;
   const unsigned hm = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
-  uint64_t acc = 0;
-  if (level0 == 0 && a.level0_unfiltered) {
-    // score_filter_candidate level 0: the unfiltered reconstruction.
-    for (int r = warp; r < a.mb_rows; r += nwarps) {
-      if (a.row_t0[r] < 0) continue;
-      for (int c = 0; c < a.mb_cols; c++) {
-        const int y0 = r * 16, x0 = c * 16;
-        uint32_t s32 = 0;
-        for (int k = 0; k < 8; k++) {
-          int i = lane + 32 * k, rr = i >> 4, cc = i & 15;
-          if (y0 + rr < a.height && x0 + cc < a.width) {
-            int d = (int)a.y[(size_t)(y0 + rr) * a.ys + x0 + cc] - (int)a.sy[(size_t)(y0 + rr) * a.sys + x0 + cc];
-            s32 += (uint32_t)(d * d);
-          }
-        }
-        const int cw = (a.width + 1) >> 1, ch = (a.height + 1) >> 1;
-        for (int k = 0; k < 2; k++) {
-          int i = lane + 32 * k, rr = i >> 3, cc = i & 7, cy = r * 8 + rr, cx = c * 8 + cc;
-          if (cy < ch && cx < cw) {
-            int du = (int)a.u[(size_t)cy * a.cs + cx] - (int)a.su[(size_t)cy * a.scs + cx];
-            int dv = (int)a.v[(size_t)cy * a.cs + cx] - (int)a.sv[(size_t)cy * a.scs + cx];
-            s32 += (uint32_t)(du * du) + (uint32_t)(dv * dv);
-          }
-        }
-        acc += s32;
-      }
-    }
-    block_sum_store(acc, &a.ssd_out[level0 * 8 + sharp]);
-    return;
+  const int first = blockIdx.x * NC, nc = min(NC, a.n_cands - first);
+  int lv[NC], sh[NC];
+  bool filt[NC];
+  uint64_t acc[NC];
+  uint8_t* slots[NC];
+  __shared__ Prm prm[NC][64];
+#pragma unroll
+  for (int k = 0; k < NC; k++) {
+    const int q = first + min(k, nc - 1);
+    lv[k] = a.cands[2 * q];
+    sh[k] = a.cands[2 * q + 1];
+    filt[k] = k < nc && !(lv[k] == 0 && a.level0_unfiltered);
+    acc[k] = 0;
+    slots[k] = (a.smem_slots ? smem_slots : a.gslots + (size_t)first * a.ring_bytes) + (size_t)k * a.ring_bytes;
+    // LoopFilterParams::derive for every level at this candidate's sharpness.
+    for (int i = threadIdx.x; i < 64; i += blockDim.x) prm[k][i] = derive(i, sh[k], a.base.key_frame != 0);
   }
-  uint8_t* slots = a.smem_slots ? smem_slots : a.gslots + (size_t)blockIdx.x * a.mb_rows * 4 * SLOT_STRIDE;
   const bool score = a.ssd_out != nullptr;
-  // LoopFilterParams::derive for every level at this candidate's sharpness.
-  __shared__ Prm prm[64];
-  for (int i = threadIdx.x; i < 64; i += blockDim.x) prm[i] = derive(i, sharp, a.base.key_frame != 0);
   __syncthreads();
   Stage* stage = a.prefetch ? (Stage*)(smem_slots + a.stage_off) + hw : nullptr;
   // The half-warp's first MB of step t, or -1.
@@ -560,15 +563,14 @@ __global__ void __launch_bounds__(1024) lf_sweep_kernel(LfArgs a) {
     const int i = a.sched_off[t] + hw;
     return i < a.sched_off[t + 1] ? i : -1;
   };
-  bool staged = false;
-  if (a.prefetch) {
-    const int i = first_mb(0);
-    if (i >= 0) {
-      const int r = a.sched_row[i];
-      prefetch_mb(a, stage, r, 0 - a.row_t0[r], l, score);
-      staged = true;
-    }
-  }
+  auto issue = [&](int t) -> bool {
+    const int j = first_mb(t);
+    if (j < 0) return false;
+    const int r2 = a.sched_row[j];
+    prefetch_mb(a, stage, r2, t - a.row_t0[r2], l, score);
+    return true;
+  };
+  bool staged = a.prefetch ? issue(0) : false;
   for (int t = 0; t < a.steps; t++) {
     const int b = a.sched_off[t], e = a.sched_off[t + 1];
     bool next_issued = false;
@@ -586,12 +588,12 @@ __global__ void __launch_bounds__(1024) lf_sweep_kernel(LfArgs a) {
         for (int k = 0; k < 4; k++) rec.y[k] = ry[k];
         rec.c[0] = rc[0];
         rec.c[1] = rc[1];
-        if (score && c >= 4) {
+        if (score && c >= RING) {
           const uint32_t* sy = (const uint32_t*)(stage->src + l * 16);
           const uint32_t* sc = (const uint32_t*)(stage->src + (l < 8 ? 256 : 320) + (l & 7) * 8);
-          const int ny = r * 16 + l < a.height ? clampi(a.width - (c - 4) * 16, 0, 16) : 0;
+          const int ny = r * 16 + l < a.height ? clampi(a.width - (c - RING) * 16, 0, 16) : 0;
           const int cw = (a.width + 1) >> 1, ch = (a.height + 1) >> 1;
-          const int nc = r * 8 + (l & 7) < ch ? clampi(cw - (c - 4) * 8, 0, 8) : 0;
+          const int ncv = r * 8 + (l & 7) < ch ? clampi(cw - (c - RING) * 8, 0, 8) : 0;
 #pragma unroll
           for (int k = 0; k < 4; k++) {
             sw.y[k] = sy[k];
@@ -600,52 +602,46 @@ __global__ void __launch_bounds__(1024) lf_sweep_kernel(LfArgs a) {
 #pragma unroll
           for (int k = 0; k < 2; k++) {
             sw.c[k] = sc[k];
-            sw.mc[k] = vis_mask(nc, k);
+            sw.mc[k] = vis_mask(ncv, k);
           }
         }
         m = stage->info;
-        staged = false;
+        __syncwarp(hm);
+        // The staging area is free again: start the next step's copies.
+        staged = a.prefetch && issue(t + 1);
+        next_issued = true;
       } else {
         rec = fetch_recon(a, r, c, l);
-        if (score && c >= 4) sw = fetch_source(a, r, c - 4, l);
+        if (score && c >= RING) sw = fetch_source(a, r, c - RING, l);
         m = a.mbs[(size_t)r * a.mb_cols + c];
       }
-      if (c >= 4) {
-        acc += finish_mb(a, slots, r, c - 4, l, sw);
-        __syncwarp(hm);
-      }
-      store_slot(slot_ptr(slots, r, c), rec, l);
-      __syncwarp(hm);
-      if (a.prefetch && !next_issued) {
-        // The staging area is free again: start the next step's copies.
-        const int j = first_mb(t + 1);
-        if (j >= 0) {
-          const int r2 = a.sched_row[j];
-          prefetch_mb(a, stage, r2, t + 1 - a.row_t0[r2], l, score);
-          staged = true;
+#pragma unroll
+      for (int k = 0; k < NC; k++) {
+        if (k >= nc) break;
+        if (c >= RING) {
+          acc[k] += finish_mb(a, slots[k], r, c - RING, l, sw);
+          __syncwarp(hm);
         }
-        next_issued = true;
+        store_slot(slot_ptr(slots[k], r, c), rec, l);
       }
-      filter_mb(a, prm, m, slots, level0, r, c, a.row_top[r] != 0, l, hm);
+      __syncwarp(hm);
+#pragma unroll
+      for (int k = 0; k < NC; k++)
+        if (filt[k]) filter_mb(a, prm[k], m, slots[k], lv[k], r, c, a.row_top[r] != 0, l, hm);
     }
-    if (a.prefetch && !next_issued) {
-      const int j = first_mb(t + 1);
-      if (j >= 0) {
-        const int r2 = a.sched_row[j];
-        prefetch_mb(a, stage, r2, t + 1 - a.row_t0[r2], l, score);
-        staged = true;
-      }
-    }
+    if (a.prefetch && !next_issued) staged = issue(t + 1);
     __syncthreads();
   }
-  // The last four MBs of every scored row.
-  for (int i = hw; i < a.mb_rows * 4; i += nhw) {
-    const int r = i >> 2, c = a.mb_cols - 4 + (i & 3);
+  // The last MBs of every scored row.
+  for (int i = hw; i < a.mb_rows * RING; i += nhw) {
+    const int r = i / RING, c = a.mb_cols - RING + i % RING;
     if (c < 0 || a.row_t0[r] < 0) continue;
     const SrcWords sw = score ? fetch_source(a, r, c, l) : SrcWords{};
-    acc += finish_mb(a, slots, r, c, l, sw);
+#pragma unroll
+    for (int k = 0; k < NC; k++)
+      if (k < nc) acc[k] += finish_mb(a, slots[k], r, c, l, sw);
   }
-  if (score) block_sum_store(acc, &a.ssd_out[level0 * 8 + sharp]);
+  if (score) block_sums_store<NC>(acc, a, lv, sh, nc);
 }
 
 // Plain visible-window SSD of a reconstruction (reconstruction_ssd).
@@ -810,26 +806,71 @@ vp8a_status stage_lf(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_planes* planes,
   return VP8A_OK;
 }
 
-// Dynamic shared memory of a sweep launch: the slot rings, then (when the
-// planes allow aligned asynchronous copies and it fits) one staging area
-// per half-warp for the next-step prefetch.
-size_t sweep_smem(LfArgs& a, int threads, size_t slot_bytes, int max_smem) {
-  auto al = [](const void* p, uint64_t stride, unsigned n) { return ((uintptr_t)p % n == 0) && (stride % n == 0); };
-  const bool score = a.ssd_out != nullptr;
-  bool ok = al(a.y, a.ys, 16) && al(a.u, a.cs, 8) && al(a.v, a.cs, 8) && (uintptr_t)a.mbs % 8 == 0;
-  if (score) ok = ok && al(a.sy, a.sys, 16) && al(a.su, a.scs, 8) && al(a.sv, a.scs, 8);
+// Launch the sweep over `n` candidates (pairs of level, sharpness) already
+// in device memory at a.cands. Layout, best first: two candidates per CTA
+// with the next-MB prefetch, one with the prefetch, two without, one
+// without (the slot rings and staging in shared memory); otherwise, when
+// `gslots` can provide them, the rings in global memory. The prefetch needs
+// planes whose rows allow aligned 16- and 8-byte asynchronous copies.
+vp8a_status run_sweep(vp8a_ctx* ctx, LfArgs a, int n, vp8a::Stager* gst) {
+  if (n == 0) return VP8A_OK;
+  a.n_cands = n;
+  a.ring_bytes = a.mb_rows * RING * SLOT_STRIDE;
+  int max_smem = 0;
+  VP8A_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+  const int threads = std::min(1024, std::max(32, (16 * a.max_active + 31) / 32 * 32));
+  auto al = [](const void* p, uint64_t stride, unsigned k) { return ((uintptr_t)p % k == 0) && (stride % k == 0); };
+  bool pre_ok = al(a.y, a.ys, 16) && al(a.u, a.cs, 8) && al(a.v, a.cs, 8) && (uintptr_t)a.mbs % 8 == 0;
+  if (a.ssd_out) pre_ok = pre_ok && al(a.sy, a.sys, 16) && al(a.su, a.scs, 8) && al(a.sv, a.scs, 8);
   const size_t stage_bytes = (size_t)(threads / 16) * sizeof(Stage);
-  if (ok && slot_bytes + stage_bytes + 1024 <= (size_t)max_smem) {
-    a.prefetch = 1;
-    a.stage_off = (int)slot_bytes;
-    return slot_bytes + stage_bytes;
+  cudaFuncAttributes f1, f2;
+  VP8A_CUDA(cudaFuncGetAttributes(&f1, lf_sweep_kernel<1>));
+  VP8A_CUDA(cudaFuncGetAttributes(&f2, lf_sweep_kernel<2>));
+  const struct {
+    int nc;
+    bool pre;
+  } opts[4] = {{2, true}, {1, true}, {2, false}, {1, false}};
+  for (const auto& o : opts) {
+    if ((o.nc == 2 && n < 2) || (o.pre && !pre_ok)) continue;
+    const size_t rings = (size_t)o.nc * a.ring_bytes, total = rings + (o.pre ? stage_bytes : 0);
+    const size_t stat = o.nc == 2 ? f2.sharedSizeBytes : f1.sharedSizeBytes;
+    if (total + stat + 1024 > (size_t)max_smem) continue;
+    a.smem_slots = 1;
+    a.gslots = nullptr;
+    a.prefetch = o.pre;
+    a.stage_off = (int)rings;
+    const int grid = (n + o.nc - 1) / o.nc;
+    if (o.nc == 2) {
+      VP8A_CUDA(cudaFuncSetAttribute(lf_sweep_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)total));
+      lf_sweep_kernel<2><<<grid, threads, total, ctx->stream>>>(a);
+    } else {
+      VP8A_CUDA(cudaFuncSetAttribute(lf_sweep_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)total));
+      lf_sweep_kernel<1><<<grid, threads, total, ctx->stream>>>(a);
+    }
+    VP8A_CUDA(cudaGetLastError());
+    ctx->launches++;
+    return VP8A_OK;
   }
-  a.prefetch = 0;
+  if (!gst) {
+    vp8a::set_error("the MB rows' slot rings do not fit in shared memory");
+    return VP8A_E_INVALID_DIMENSIONS;
+  }
+  // Rings in global memory, one set per candidate; staging still shared.
+  void* g;
+  vp8a_status s;
+  if ((s = gst->scratch((size_t)a.ring_bytes * n, &g)) != VP8A_OK) return s;
+  a.smem_slots = 0;
+  a.gslots = (uint8_t*)g;
+  a.prefetch = pre_ok && stage_bytes + f1.sharedSizeBytes + 1024 <= (size_t)max_smem;
   a.stage_off = 0;
-  return slot_bytes;
+  const size_t total = a.prefetch ? stage_bytes : 0;
+  VP8A_CUDA(cudaFuncSetAttribute(lf_sweep_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)total));
+  lf_sweep_kernel<1><<<n, threads, total, ctx->stream>>>(a);
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
+  return VP8A_OK;
 }
 
-// Launch the sweep over `n` candidates (pairs of level, sharpness).
 vp8a_status launch_sweep(vp8a_ctx* ctx, vp8a::Stager& st, LfArgs a, const uint8_t* cands, int n) {
   if (n == 0) return VP8A_OK;
   void* dc;
@@ -837,27 +878,7 @@ vp8a_status launch_sweep(vp8a_ctx* ctx, vp8a::Stager& st, LfArgs a, const uint8_
   if ((s = st.scratch((size_t)n * 2, &dc)) != VP8A_OK) return s;
   VP8A_CUDA(cudaMemcpyAsync(dc, cands, (size_t)n * 2, cudaMemcpyHostToDevice, ctx->stream));
   a.cands = (const uint8_t*)dc;
-  const size_t slot_bytes = (size_t)a.mb_rows * 4 * SLOT_STRIDE;
-  int max_smem = 0;
-  VP8A_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-  const int threads = std::min(1024, std::max(32, (16 * a.max_active + 31) / 32 * 32));
-  if (slot_bytes + 1024 <= (size_t)max_smem) {
-    a.smem_slots = 1;
-    a.gslots = nullptr;
-    const size_t smem = sweep_smem(a, threads, slot_bytes, max_smem);
-    VP8A_CUDA(cudaFuncSetAttribute(lf_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    lf_sweep_kernel<<<n, threads, smem, ctx->stream>>>(a);
-  } else {
-    void* g;
-    if ((s = st.scratch(slot_bytes * n, &g)) != VP8A_OK) return s;
-    a.smem_slots = 0;
-    a.gslots = (uint8_t*)g;
-    a.prefetch = 0;
-    lf_sweep_kernel<<<n, threads, 0, ctx->stream>>>(a);
-  }
-  VP8A_CUDA(cudaGetLastError());
-  ctx->launches++;
-  return VP8A_OK;
+  return run_sweep(ctx, a, n, &st);
 }
 
 // Score `cands` into `table` (host, 512 entries indexed level * 8 + sharp).
@@ -1298,19 +1319,7 @@ vp8a_status vp8a_filter_sweep_noalloc(vp8a_ctx* ctx, const vp8a_planes* planes, 
   a.level0_unfiltered = 1;
   a.smem_slots = 1;
   a.gslots = nullptr;
-  const size_t slot_bytes = (size_t)rows * 4 * SLOT_STRIDE;
-  int max_smem = 0;
-  VP8A_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-  if (slot_bytes + 1024 > (size_t)max_smem) {
-    vp8a::set_error("vp8a_filter_sweep_noalloc: the MB rows' slot rings do not fit in shared memory");
-    return VP8A_E_INVALID_DIMENSIONS;
-  }
-  const int threads = std::min(1024, std::max(32, (16 * max_active + 31) / 32 * 32));
-  const size_t smem = sweep_smem(a, threads, slot_bytes, max_smem);
-  VP8A_CUDA(cudaFuncSetAttribute(lf_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  lf_sweep_kernel<<<NA_CANDIDATES, threads, smem, ctx->stream>>>(a);
-  VP8A_CUDA(cudaGetLastError());
-  ctx->launches++;
+  if ((s = run_sweep(ctx, a, NA_CANDIDATES, nullptr)) != VP8A_OK) return s;
   // Level 0 scores the same for every sharpness.
   for (int sh = 1; sh < 8; sh++)
     VP8A_CUDA(cudaMemcpyAsync(ssd_out + sh, ssd_out, sizeof(uint64_t), cudaMemcpyDeviceToDevice, ctx->stream));
