@@ -394,6 +394,11 @@ vp8a_status vp8a_select_filter_params(vp8a_ctx* ctx, const vp8a_planes* planes,
                                       const vp8a_filter_config* base, const vp8a_source* src,
                                       uint8_t* level_out, uint8_t* sharpness_out);
 
+/* FilterSampling::for_key_frame (src/loop_filter.rs:2266): the band
+ * spacing and sharpness sweep the key-frame encoder's sampled loop-filter
+ * pick uses (src/encoder.rs:6643-6651). Host only; no context needed. */
+void vp8a_key_frame_sampling(uint32_t mb_rows, uint32_t* every_rows, uint32_t* sweep_sharpness);
+
 /* select_filter_params_sampled (src/loop_filter.rs:2288) with
  * FilterSampling { every_rows, sweep_sharpness }. */
 vp8a_status vp8a_select_filter_params_sampled(vp8a_ctx* ctx, const vp8a_planes* planes,

@@ -287,6 +287,14 @@ def select_filter_params(recon, mbs, base, src, threads=1):
     return lv.value, sh.value
 
 
+def key_frame_sampling(mb_rows):
+    """FilterSampling::for_key_frame (src/loop_filter.rs:2266-2272):
+    bands = clamp(mb_rows / 32, 3, 6); every_rows = max(mb_rows / bands, 2);
+    the sharpness sweep on."""
+    bands = min(max(mb_rows // 32, 3), 6)
+    return max(mb_rows // bands, 2), True
+
+
 def select_filter_params_sampled(recon, mbs, base, src, every_rows, sweep_sharpness, threads=1):
     m = np.ascontiguousarray(mbs, abi.MB_LF_INFO_DTYPE)
     lv, sh = C.c_uint8(), C.c_uint8()

@@ -1156,6 +1156,13 @@ vp8a_status vp8a_select_filter_params(vp8a_ctx* ctx, const vp8a_planes* planes, 
   return st.finish();
 }
 
+void vp8a_key_frame_sampling(uint32_t mb_rows, uint32_t* every_rows, uint32_t* sweep_sharpness) {
+  // bands = clamp(mb_rows / 32, 3, 6); every_rows = max(mb_rows / bands, 2).
+  const uint32_t bands = std::min<uint32_t>(std::max<uint32_t>(mb_rows / 32, 3), 6);
+  if (every_rows) *every_rows = std::max<uint32_t>(mb_rows / bands, 2);
+  if (sweep_sharpness) *sweep_sharpness = 1;
+}
+
 vp8a_status vp8a_select_filter_params_sampled(vp8a_ctx* ctx, const vp8a_planes* planes, const vp8a_mb_lf_info* mbs,
                                               const vp8a_filter_config* base, const vp8a_source* src,
                                               uint32_t every_rows, uint32_t sweep_sharpness, uint8_t* level_out,

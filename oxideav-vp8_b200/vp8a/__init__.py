@@ -12,6 +12,7 @@ from .api import (
     filter_frame,
     filter_sweep,
     half_pixel_refine_luma,
+    key_frame_sampling,
     lf_info_from_decisions,
     mb_luma_sad_at_mv,
     motion_descent,
@@ -21,6 +22,7 @@ from .api import (
     rd_lambda,
     reconstruction_ssd,
     select_filter_params,
+    select_filter_params_key_frame,
     select_filter_params_sampled,
     small_diamond_search_luma,
 )
@@ -40,6 +42,7 @@ __all__ = [
     "filter_frame",
     "filter_sweep",
     "half_pixel_refine_luma",
+    "key_frame_sampling",
     "lf_info_from_decisions",
     "mb_luma_sad_at_mv",
     "neighbours_from_decisions",
@@ -49,6 +52,7 @@ __all__ = [
     "rd_lambda",
     "reconstruction_ssd",
     "select_filter_params",
+    "select_filter_params_key_frame",
     "select_filter_params_sampled",
     "small_diamond_search_luma",
     "i420",

@@ -259,6 +259,25 @@ def select_filter_params_sampled(ctx, recon, mbs, base, src, every_rows, sweep_s
     return lv.value, sh.value
 
 
+def key_frame_sampling(mb_rows):
+    """FilterSampling::for_key_frame (src/loop_filter.rs:2266) ->
+    (every_rows, sweep_sharpness), from the library's own helper."""
+    er, sw = C.c_uint32(), C.c_uint32()
+    load().vp8a_key_frame_sampling(int(mb_rows), C.byref(er), C.byref(sw))
+    return er.value, bool(sw.value)
+
+
+def select_filter_params_key_frame(ctx, recon, mbs, base, src, sampled=True):
+    """The key-frame encoder's loop-filter pick (src/encoder.rs:6638-6655):
+    the sampled search with FilterSampling::for_key_frame, or the full
+    search. `base` is the key frame's FrameFilterConfig (key_frame set)
+    and `mbs` its intra MB side information."""
+    if not sampled:
+        return select_filter_params(ctx, recon, mbs, base, src)
+    er, sw = key_frame_sampling(recon[0].shape[0] // 16)
+    return select_filter_params_sampled(ctx, recon, mbs, base, src, er, sw)
+
+
 def lf_info_from_decisions(dec, has_coeffs=None):
     """Per-MB §15 side information from inter decisions: SPLITMV MBs are
     recorded as B_PRED (src/loop_filter.rs:1258-1266)."""

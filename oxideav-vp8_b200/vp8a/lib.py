@@ -52,6 +52,7 @@ PROTOTYPES = {
         C.c_int,
         [P, C.POINTER(abi.Planes), P, C.POINTER(abi.FilterConfig), C.POINTER(abi.Source), P, P],
     ),
+    "vp8a_key_frame_sampling": (None, [U32, C.POINTER(U32), C.POINTER(U32)]),
     "vp8a_select_filter_params_sampled": (
         C.c_int,
         [P, C.POINTER(abi.Planes), P, C.POINTER(abi.FilterConfig), C.POINTER(abi.Source), U32, U32, P, P],

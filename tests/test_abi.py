@@ -53,3 +53,9 @@ def test_no_cpu_fallback_without_gpu():
 def test_rd_lambda_host_helper(oracle):
     for qi in (0, 44, 100, 127):
         assert vp8a.rd_lambda(qi) == oracle.rd_lambda(qi)
+
+
+def test_key_frame_sampling_helper(oracle):
+    # FilterSampling::for_key_frame, host-side in the library.
+    for mb_rows in list(range(1, 300)) + [4096]:
+        assert vp8a.key_frame_sampling(mb_rows) == oracle.key_frame_sampling(mb_rows), mb_rows

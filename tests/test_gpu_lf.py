@@ -141,3 +141,29 @@ def test_lf_errors(ctx):
         vp8a.filter_frame(ctx, recon, m, abi.filter_config(64, 0))
     with pytest.raises(vp8a.Vp8aError, match="SharpnessLevelOutOfRange"):
         vp8a.filter_frame(ctx, recon, m, abi.filter_config(10, 8))
+
+
+def key_frame_case(width, height, seed):
+    """An intra picture's §15 side information: every MB intra, some B_PRED."""
+    src, recon, m = lf_case(width, height, seed)
+    rng = np.random.default_rng(seed + 1)
+    m["ref_frame"] = abi.REF_INTRA
+    m["inter_mode"] = abi.MODE_NONE
+    m["y_mode_is_bpred"] = rng.random(m.size) < 0.4
+    m["segment_id"] = -1
+    return src, recon, m
+
+
+@pytest.mark.parametrize("size", [(320, 240), (176, 144), (640, 368)])
+def test_key_frame_auto_lf(ctx, oracle, size):
+    # encode_keyframe_auto_loop_filter's pick (src/encoder.rs:6638-6655):
+    # the sampled search with FilterSampling::for_key_frame, and the full
+    # search, on key-frame hev thresholds and intra MBs.
+    src, recon, m = key_frame_case(*size, seed=size[0])
+    er, sw = oracle.key_frame_sampling(recon[0].shape[0] // 16)
+    for bs in (0, 4):
+        base = abi.filter_config(0, bs, key_frame=True)
+        assert vp8a.select_filter_params_key_frame(ctx, recon, m, base, src) == \
+            oracle.select_filter_params_sampled(recon, m, base, src, er, sw, threads=8)
+        assert vp8a.select_filter_params_key_frame(ctx, recon, m, base, src, sampled=False) == \
+            oracle.select_filter_params(recon, m, base, src, threads=8)
