@@ -328,6 +328,47 @@ vp8a_status vp8a_rd_inter_search(vp8a_ctx* ctx, const vp8a_i420* frame, const vp
 /* rd_lambda (src/encoder.rs:3742) for a luma AC quantiser index 0..=127. */
 double vp8a_rd_lambda(uint32_t y_ac_qi);
 
+/* ------------------------------------------- §18 inter prediction (MC) */
+
+/* FilterSet (src/motion_comp.rs:344). filter_set_for_version
+ * (src/motion_comp.rs:370): frame-tag version 0 uses SIXTAP, any other
+ * version BILINEAR. */
+enum { VP8A_FILTER_SIXTAP = 0, VP8A_FILTER_BILINEAR = 1 };
+
+/* Batched predict_inter_mb (src/motion_comp.rs:1986): item i predicts the
+ * MB at (mb_xy[2i], mb_xy[2i+1]) = (mb_col, mb_row) from `ref` under the
+ * quarter-pel luma vector mvs[i]. `full_pixel` is the version-3 full-pel
+ * flag (apply_full_pixel, src/motion_comp.rs:256), `filter_set` one of
+ * VP8A_FILTER_*. `out` receives 384 bytes per item in ReconstructedMb's
+ * layout (src/reconstruct.rs:178): y[256] (16x16 raster), then u[64] and
+ * v[64] (8x8 raster). Fetches outside the MB-padded planes replicate the
+ * edge pixel, as the reference's do. */
+vp8a_status vp8a_predict_inter_mb(vp8a_ctx* ctx, const vp8a_planes* ref, const uint32_t* mb_xy,
+                                  const vp8a_mv* mvs, uint32_t n, uint32_t full_pixel,
+                                  uint32_t filter_set, uint8_t* out);
+
+/* Batched predict_split_mv (src/motion_comp.rs:2228): as
+ * vp8a_predict_inter_mb with 16 quarter-pel vectors per item,
+ * split_mvs[16i + b] for luma sub-block b in raster order; chroma takes
+ * split_chroma_mvs (src/motion_comp.rs:2175). */
+vp8a_status vp8a_predict_split_mv(vp8a_ctx* ctx, const vp8a_planes* ref, const uint32_t* mb_xy,
+                                  const vp8a_mv* split_mvs, uint32_t n, uint32_t full_pixel,
+                                  uint32_t filter_set, uint8_t* out);
+
+/* The prediction pick_mb_for_ref builds for its chosen mode
+ * (src/encoder.rs:8704-8735) for every MB of a frame: predict_split_mv for
+ * a VP8A_MODE_SPLIT decision, predict_inter_mb with `mv` otherwise, from
+ * the reference of `ref_frame`, written into the MB-padded `out` planes at
+ * the MB's position. decisions holds out->mb_cols * out->mb_rows records in
+ * raster order (vp8a_analyse_inter_frame's output). `refs[k]` has id
+ * `ref_ids[k]` (VP8A_REF_LAST/GOLDEN/ALTREF) and the output's MB grid. MBs
+ * whose ref_frame is VP8A_REF_INTRA or has no plane in `refs` keep the
+ * pixels `out` already holds. */
+vp8a_status vp8a_predict_inter_frame(vp8a_ctx* ctx, const vp8a_planes* refs,
+                                     const uint8_t* ref_ids, uint32_t n_refs,
+                                     const vp8a_mb_decision* decisions, uint32_t full_pixel,
+                                     uint32_t filter_set, vp8a_planes* out);
+
 /* ------------------------------------------------------------ ARNR filter */
 
 /* build_arnr_altref (src/arnr.rs:476): temporally filtered altref anchor of

@@ -79,6 +79,12 @@ def load():
         "vo_select_from_table_full": (None, [P, C.c_uint8, P, P]),
         "vo_select_from_table_sampled": (None, [P, C.c_uint8, C.c_int, P, P]),
         "vo_type_size": (C.c_size_t, [C.c_int]),
+        "vo_chroma_mv": (abi.Mv, [abi.Mv]),
+        "vo_split_chroma_mvs": (None, [P, P]),
+        "vo_sixtap_2d": (None, [P, C.c_int, C.c_int, C.c_int, P]),
+        "vo_predict_inter_mb_batch": (None, [C.POINTER(abi.Planes), P, P, U32, C.c_int, C.c_int, P]),
+        "vo_predict_split_mv_batch": (None, [C.POINTER(abi.Planes), P, P, U32, C.c_int, C.c_int, P]),
+        "vo_predict_inter_frame": (C.c_int, [P, P, U32, P, C.c_int, C.c_int, C.POINTER(abi.Planes)]),
         "vo_rd_inter_search": (C.c_int, [C.POINTER(abi.I420), P, P, U32, C.POINTER(abi.MvContexts), C.c_double,
                                          U32, U32, P, P, U32]),
     }
@@ -377,3 +383,62 @@ def rd_inter_search(frame, refs, ref_ids, lam, y1_ac, effort, neighbours, mv_con
                                    y1_ac, effort, ptr(nb), ptr(out), threads)
     _check(st, "vo_rd_inter_search")
     return out.reshape(mbr, mbc)
+
+
+# ---- §18 inter prediction (predict.c) -----------------------------------
+
+def chroma_mv(row, col):
+    """chroma_mv (src/motion_comp.rs:232) of an eighth-pel luma vector."""
+    m = load().vo_chroma_mv(abi.Mv(row, col))
+    return (m.row, m.col)
+
+
+def split_chroma_mvs(split_mvs):
+    """split_chroma_mvs (src/motion_comp.rs:2175): 16 quarter-pel vectors ->
+    4 eighth-pel chroma vectors, as an (4, 2) int array (row, col)."""
+    mv = _mvs(split_mvs)
+    assert len(mv) == 16
+    out = np.zeros(4, abi.MV_DTYPE)
+    load().vo_split_chroma_mvs(ptr(mv), ptr(out))
+    return np.stack([out["row"], out["col"]], axis=1).astype(np.int32)
+
+
+def sixtap_2d(halo81, mx, my, filter_set=abi.FILTER_SIXTAP):
+    """sixtap_2d (src/motion_comp.rs:680) of a 9x9 halo, block origin (2, 2)."""
+    h = np.ascontiguousarray(np.asarray(halo81, np.uint8).reshape(81))
+    out = np.zeros(16, np.uint8)
+    load().vo_sixtap_2d(ptr(h), mx, my, filter_set, ptr(out))
+    return out.reshape(4, 4)
+
+
+def predict_inter_mb(ref, mb_xy, mvs, full_pixel=False, filter_set=abi.FILTER_SIXTAP):
+    """predict_inter_mb (src/motion_comp.rs:1986) over a batch; (n, 384)."""
+    p = planes(*ref)
+    xy, mv = _xy(mb_xy), _mvs(mvs)
+    out = np.zeros((len(mv), 384), np.uint8)
+    load().vo_predict_inter_mb_batch(C.byref(p), ptr(xy), ptr(mv), len(mv), int(bool(full_pixel)), filter_set,
+                                     ptr(out))
+    return out
+
+
+def predict_split_mv(ref, mb_xy, split_mvs, full_pixel=False, filter_set=abi.FILTER_SIXTAP):
+    """predict_split_mv (src/motion_comp.rs:2228) over a batch; (n, 384)."""
+    p = planes(*ref)
+    xy, mv = _xy(mb_xy), _mvs(split_mvs)
+    n = len(mv) // 16
+    out = np.zeros((n, 384), np.uint8)
+    load().vo_predict_split_mv_batch(C.byref(p), ptr(xy), ptr(mv), n, int(bool(full_pixel)), filter_set, ptr(out))
+    return out
+
+
+def predict_inter_frame(refs, ref_ids, decisions, out, full_pixel=False, filter_set=abi.FILTER_SIXTAP):
+    """The per-MB prediction of pick_mb_for_ref's chosen mode
+    (src/encoder.rs:8704-8735) into the MB-padded planes `out` in place.
+    Returns the number of MBs left untouched (no inter reference)."""
+    prs = [planes(*p) for p in refs]
+    parr = (abi.Planes * len(prs))(*prs)
+    ids = np.ascontiguousarray(np.asarray(ref_ids, np.uint8))
+    dec = np.ascontiguousarray(decisions).reshape(-1)
+    op = planes(*out)
+    return load().vo_predict_inter_frame(C.cast(parr, C.c_void_p), ptr(ids), len(prs), ptr(dec),
+                                         int(bool(full_pixel)), filter_set, C.byref(op))

@@ -136,6 +136,22 @@ void vo_select_from_table_full(const uint64_t* ssd, uint8_t base_sharp, uint8_t*
 void vo_select_from_table_sampled(const uint64_t* ssd, uint8_t base_sharp, int sweep,
                                   uint8_t* level, uint8_t* sharp);
 
+/* ---- §18 inter prediction (src/motion_comp.rs; predict.c) */
+vp8a_mv vo_chroma_mv(vp8a_mv luma_eighth);
+void vo_split_chroma_mvs(const vp8a_mv* split16, vp8a_mv* out4);
+void vo_sixtap_2d(const uint8_t* halo81, int mx, int my, int filter_set, uint8_t* out16);
+void vo_predict_inter_mb(const vp8a_planes* ref, uint32_t mb_col, uint32_t mb_row, vp8a_mv luma_mv,
+                         int full_pixel, int filter_set, uint8_t* out384);
+void vo_predict_split_mv(const vp8a_planes* ref, uint32_t mb_col, uint32_t mb_row,
+                         const vp8a_mv* split16, int full_pixel, int filter_set, uint8_t* out384);
+void vo_predict_inter_mb_batch(const vp8a_planes* ref, const uint32_t* mb_xy, const vp8a_mv* mvs,
+                               uint32_t n, int full_pixel, int filter_set, uint8_t* out);
+void vo_predict_split_mv_batch(const vp8a_planes* ref, const uint32_t* mb_xy, const vp8a_mv* mvs16,
+                               uint32_t n, int full_pixel, int filter_set, uint8_t* out);
+int vo_predict_inter_frame(const vp8a_planes* refs, const uint8_t* ref_ids, uint32_t n_refs,
+                           const vp8a_mb_decision* dec, int full_pixel, int filter_set,
+                           vp8a_planes* out);
+
 /* ---- threading helper */
 typedef void (*vo_task_fn)(void* arg, uint32_t index);
 void vo_parallel_for(uint32_t n, uint32_t threads, vo_task_fn fn, void* arg);

@@ -1,0 +1,561 @@
+// predict.cu — §18 inter prediction (motion compensation) on the GPU:
+//   vp8a_predict_inter_mb    (predict_inter_mb, src/motion_comp.rs:1986)
+//   vp8a_predict_split_mv    (predict_split_mv, src/motion_comp.rs:2228)
+//   vp8a_predict_inter_frame (the prediction pick_mb_for_ref builds for its
+//                             chosen mode, src/encoder.rs:8704-8735)
+//
+// Work decomposition. The reference interpolates a whole-MB vector as one
+// 16x16 luma and two 8x8 chroma blocks and a SPLITMV MB as 4x4 blocks; the
+// §18.3 dot product of an output sample does not depend on the tiling, so
+// every MB is cut into the same 48 tasks here: 32 luma (16 4x4 blocks x 2
+// row pairs) and 16 chroma (4 blocks of U and of V x 2 row pairs). A CTA of
+// 128 threads takes 8 MBs per step, 384 tasks = 3 per thread.
+//
+// Step: (1) 16 threads per MB derive the eighth-pel vectors of its 16 luma
+// and 4 chroma blocks (stored_luma_mv, chroma_mv or split_chroma_mvs,
+// apply_full_pixel); (2) each warp copies the edge-clamped source of two MBs
+// into shared memory — one 21x21 luma and two 13x13 chroma regions for a
+// whole-MB vector, 24 9x9 block halos for SPLITMV; (3) each task reads a
+// 12-byte-wide, 7-row window as 32-bit words and runs the horizontal pass
+// (4 outputs per row, dp4a with the tap row pre-shifted per output column),
+// packs the 8-bit intermediate with saturation, transposes it with byte
+// permutes and runs the vertical pass the same way. A zero fraction is the
+// identity filter, taken as a byte select.
+#include <algorithm>
+
+#include "vp8a_internal.cuh"
+
+namespace {
+
+constexpr int PR_THREADS = 128;
+constexpr int PR_MBS = 8;           // MBs per CTA step
+constexpr int PR_TASKS = 48;        // tasks per MB
+constexpr int SLOT_BYTES = 2592;    // 24 block halos of 9 rows x 12 bytes
+constexpr int WY_STRIDE = 24, WC_STRIDE = 16, WU_OFF = 504, WV_OFF = 712;  // whole-MB layout
+constexpr int HALO_STRIDE = 12, HALO_BYTES = 108;                          // SPLITMV layout
+constexpr int MAX_PRED_REFS = 3;
+
+// §18.3 tap tables (SIXTAP_FILTERS / BILINEAR_FILTERS, src/motion_comp.rs:294-334).
+__constant__ int c_taps[2][8][6] = {
+    {{0, 0, 128, 0, 0, 0},
+     {0, -6, 123, 12, -1, 0},
+     {2, -11, 108, 36, -8, 1},
+     {0, -9, 93, 50, -6, 0},
+     {3, -16, 77, 77, -16, 3},
+     {0, -6, 50, 93, -9, 0},
+     {1, -8, 36, 108, -11, 2},
+     {0, -1, 12, 123, -6, 0}},
+    {{0, 0, 128, 0, 0, 0},
+     {0, 0, 112, 16, 0, 0},
+     {0, 0, 96, 32, 0, 0},
+     {0, 0, 80, 48, 0, 0},
+     {0, 0, 64, 64, 0, 0},
+     {0, 0, 48, 80, 0, 0},
+     {0, 0, 32, 96, 0, 0},
+     {0, 0, 16, 112, 0, 0}},
+};
+
+enum PredMode { PRED_WHOLE = 0, PRED_SPLIT = 1, PRED_FRAME = 2 };
+
+struct PredPlanes {
+  const uint8_t* y;
+  const uint8_t* u;
+  const uint8_t* v;
+  uint64_t ys, uvs;
+};
+
+struct PredArgs {
+  PredPlanes refs[MAX_PRED_REFS];
+  uint8_t ref_ids[MAX_PRED_REFS];
+  int n_refs;
+  int lw, lh, cw, ch;  // MB-padded plane sizes of the references
+  int mb_cols;         // frame mode: raster order of decisions
+  uint32_t n;          // MBs
+  const uint32_t* mb_xy;
+  const vp8a_mv* mvs;  // whole: 1 per MB, split: 16 per MB
+  const vp8a_mb_decision* dec;
+  int full_pixel;
+  int filter_set;
+  // Output: batched -> out + 384 i; frame -> planes at the MB position.
+  uint8_t* out;
+  uint8_t *oy, *ou, *ov;
+  uint64_t oys, ouvs;
+  int aligned_out;  // every output row start is 4-byte aligned
+};
+
+struct Job {
+  const uint8_t* y;
+  const uint8_t* u;
+  const uint8_t* v;
+  uint64_t ys, uvs;
+  uint8_t *oy, *ou, *ov;
+  uint64_t oys, ouvs;
+  int x16, y16;  // MB luma origin (clamped so every offset fits int)
+  int split;
+  int skip;
+  short2 lmv[16];  // eighth-pel (row, col) per luma block
+  short2 cmv[4];   // eighth-pel per chroma block
+};
+
+__device__ __forceinline__ int dp4a_us(uint32_t a, uint32_t b, int c) {
+  int d;
+  asm("dp4a.u32.s32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+  return d;
+}
+
+// (c << 16) | (sat_u8(hi) << 8) | sat_u8(lo)
+__device__ __forceinline__ uint32_t pack2_sat(int lo, int hi, uint32_t rest) {
+  uint32_t d;
+  asm("cvt.pack.sat.u8.s32.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(hi), "r"(lo), "r"(rest));
+  return d;
+}
+
+__device__ __forceinline__ uint32_t pack4_sat(int v0, int v1, int v2, int v3) {
+  return pack2_sat(v0, v1, pack2_sat(v2, v3, 0u));
+}
+
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t s) { return __byte_perm(a, b, s); }
+
+// stored_luma_mv (src/motion_comp.rs:187): i16 wrapping doubling.
+__device__ __forceinline__ int dbl16(int v) { return (int)(short)(unsigned short)((unsigned)v * 2u); }
+// avg (src/motion_comp.rs:209).
+__device__ __forceinline__ int avg_sum(int s) { return s >= 0 ? (s + 4) >> 3 : -((-s + 4) >> 3); }
+
+// One 4-column output row pair of a 4x4 block: rows 0..6 of `win` (stride
+// ws) are the block's halo rows 2h .. 2h+6 starting at halo column 0.
+__device__ __forceinline__ void predict_pair(const uint8_t* win, int ws, int mx, int my, const uint32_t (*tw)[4][3],
+                                             uint32_t& o0, uint32_t& o1) {
+  uint32_t R[7];
+  if (mx == 0) {
+#pragma unroll
+    for (int i = 0; i < 7; i++) {
+      const uint32_t* w = reinterpret_cast<const uint32_t*>(win + i * ws);
+      R[i] = prmt(w[0], w[1], 0x5432);
+    }
+  } else {
+    const uint32_t(*T)[3] = tw[mx];
+    const uint32_t t00 = T[0][0], t01 = T[0][1], t10 = T[1][0], t11 = T[1][1];
+    const uint32_t t20 = T[2][0], t21 = T[2][1], t30 = T[3][0], t31 = T[3][1], t32 = T[3][2];
+#pragma unroll
+    for (int i = 0; i < 7; i++) {
+      const uint32_t* w = reinterpret_cast<const uint32_t*>(win + i * ws);
+      const uint32_t A = w[0], B = w[1], C = w[2];
+      const int a0 = dp4a_us(A, t00, dp4a_us(B, t01, 64));
+      const int a1 = dp4a_us(A, t10, dp4a_us(B, t11, 64));
+      const int a2 = dp4a_us(A, t20, dp4a_us(B, t21, 64));
+      const int a3 = dp4a_us(A, t30, dp4a_us(B, t31, dp4a_us(C, t32, 64)));
+      R[i] = pack4_sat(a0 >> 7, a1 >> 7, a2 >> 7, a3 >> 7);
+    }
+  }
+  if (my == 0) {
+    o0 = R[2];
+    o1 = R[3];
+    return;
+  }
+  // Column words: L[j] = column j of rows 0..3, H[j] = rows 4..6 (+ 0).
+  const uint32_t x01l = prmt(R[0], R[1], 0x5140), x01h = prmt(R[0], R[1], 0x7362);
+  const uint32_t x23l = prmt(R[2], R[3], 0x5140), x23h = prmt(R[2], R[3], 0x7362);
+  const uint32_t x45l = prmt(R[4], R[5], 0x5140), x45h = prmt(R[4], R[5], 0x7362);
+  const uint32_t x67l = prmt(R[6], 0u, 0x5140), x67h = prmt(R[6], 0u, 0x7362);
+  const uint32_t L0 = prmt(x01l, x23l, 0x5410), L1 = prmt(x01l, x23l, 0x7632);
+  const uint32_t L2 = prmt(x01h, x23h, 0x5410), L3 = prmt(x01h, x23h, 0x7632);
+  const uint32_t H0 = prmt(x45l, x67l, 0x5410), H1 = prmt(x45l, x67l, 0x7632);
+  const uint32_t H2 = prmt(x45h, x67h, 0x5410), H3 = prmt(x45h, x67h, 0x7632);
+  const uint32_t(*V)[3] = tw[my];
+  const uint32_t v00 = V[0][0], v01 = V[0][1], v10 = V[1][0], v11 = V[1][1];
+  o0 = pack4_sat(dp4a_us(L0, v00, dp4a_us(H0, v01, 64)) >> 7, dp4a_us(L1, v00, dp4a_us(H1, v01, 64)) >> 7,
+                 dp4a_us(L2, v00, dp4a_us(H2, v01, 64)) >> 7, dp4a_us(L3, v00, dp4a_us(H3, v01, 64)) >> 7);
+  o1 = pack4_sat(dp4a_us(L0, v10, dp4a_us(H0, v11, 64)) >> 7, dp4a_us(L1, v10, dp4a_us(H1, v11, 64)) >> 7,
+                 dp4a_us(L2, v10, dp4a_us(H2, v11, 64)) >> 7, dp4a_us(L3, v10, dp4a_us(H3, v11, 64)) >> 7);
+}
+
+__device__ __forceinline__ void store_row(uint8_t* p, uint32_t v, int aligned) {
+  if (aligned) {
+    *reinterpret_cast<uint32_t*>(p) = v;
+  } else {
+    p[0] = (uint8_t)v;
+    p[1] = (uint8_t)(v >> 8);
+    p[2] = (uint8_t)(v >> 16);
+    p[3] = (uint8_t)(v >> 24);
+  }
+}
+
+// Edge-clamped byte of a plane.
+__device__ __forceinline__ uint8_t fetch(const uint8_t* p, uint64_t stride, int w, int h, int x, int y) {
+  x = x < 0 ? 0 : (x >= w ? w - 1 : x);
+  y = y < 0 ? 0 : (y >= h ? h - 1 : y);
+  return __ldg(p + (uint64_t)y * stride + x);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(PR_THREADS) predict_kernel(PredArgs a) {
+  __shared__ __align__(16) uint8_t slots[PR_MBS][SLOT_BYTES];
+  __shared__ Job jobs[PR_MBS];
+  __shared__ uint32_t tw[8][4][3];  // tap words: [fraction][output shift][window word]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+  // Tap words for dp4a: byte m of word q for output column j holds tap
+  // 4q + m - j (0 outside 0..5). The identity fraction never uses them.
+  if (tid < 96) {
+    const int f = tid / 12, j = (tid / 3) & 3, q = tid % 3;
+    uint32_t w = 0;
+    if (f != 0)
+      for (int m = 0; m < 4; m++) {
+        const int k = 4 * q + m - j;
+        if (k >= 0 && k < 6) w |= (uint32_t)(uint8_t)(int8_t)c_taps[a.filter_set][f][k] << (8 * m);
+      }
+    tw[f][j][q] = w;
+  }
+
+  for (uint32_t g = blockIdx.x; (size_t)g * PR_MBS < a.n; g += gridDim.x) {
+    // ---- (1) per-MB vectors: 16 threads per MB, thread b = luma block b.
+    {
+      const int s = tid >> 4, b = tid & 15;
+      const uint32_t item = g * PR_MBS + s;
+      Job& J = jobs[s];
+      int skip = item >= a.n, split = 0, col = 0, row = 0, ridx = 0;
+      vp8a_mv mv = {0, 0};
+      if (!skip) {
+        if (MODE == PRED_FRAME) {
+          const vp8a_mb_decision& d = a.dec[item];
+          ridx = -1;
+          for (int k = 0; k < a.n_refs; k++)
+            if (d.ref_frame != VP8A_REF_INTRA && a.ref_ids[k] == d.ref_frame) ridx = k;
+          skip = ridx < 0;
+          split = d.mode == VP8A_MODE_SPLIT;
+          mv = split ? d.split_mvs[b] : d.mv;
+          col = (int)(item % (uint32_t)a.mb_cols);
+          row = (int)(item / (uint32_t)a.mb_cols);
+        } else {
+          split = MODE == PRED_SPLIT;
+          mv = a.mvs[split ? (size_t)item * 16 + b : item];
+          col = (int)min(a.mb_xy[2 * item], 0x40000u);
+          row = (int)min(a.mb_xy[2 * item + 1], 0x40000u);
+        }
+      }
+      // Luma block vector.
+      int er = dbl16(mv.row), ec = dbl16(mv.col);
+      // Chroma: the SPLITMV four-block average of the i32-doubled vectors
+      // (blocks b, b^1, b^4, b^5 share a chroma block), or the whole-MB
+      // chroma_mv of the doubled vector. The sums run in every lane so the
+      // shuffles stay converged.
+      int sr = 2 * (int)mv.row, sc = 2 * (int)mv.col;
+      sr += __shfl_xor_sync(0xffffffffu, sr, 1);
+      sc += __shfl_xor_sync(0xffffffffu, sc, 1);
+      sr += __shfl_xor_sync(0xffffffffu, sr, 4);
+      sc += __shfl_xor_sync(0xffffffffu, sc, 4);
+      int cr = (short)avg_sum(split ? sr : 4 * er);
+      int cc = (short)avg_sum(split ? sc : 4 * ec);
+      if (a.full_pixel) {
+        er &= ~7;
+        ec &= ~7;
+        cr &= ~7;
+        cc &= ~7;
+      }
+      J.lmv[b] = make_short2((short)er, (short)ec);
+      const int cidx = ((b >> 1) & 1) + ((b >> 2) & 2);
+      if ((b & 5) == 0) J.cmv[cidx] = make_short2((short)cr, (short)cc);
+      if (b == 0) {
+        J.skip = skip;
+        J.split = split;
+        // Vector offsets reach 4096 pixels in luma and in chroma, so an MB
+        // origin more than 16448 luma pixels past the plane fetches only
+        // edge pixels in both; clamping it there keeps every offset an int.
+        J.x16 = min(col * 16, a.lw + 16448);
+        J.y16 = min(row * 16, a.lh + 16448);
+        if (!skip) {
+          const PredPlanes& P = a.refs[ridx];
+          J.y = P.y;
+          J.u = P.u;
+          J.v = P.v;
+          J.ys = P.ys;
+          J.uvs = P.uvs;
+          if (MODE == PRED_FRAME) {
+            J.oy = a.oy + (uint64_t)row * 16 * a.oys + (uint64_t)col * 16;
+            J.ou = a.ou + (uint64_t)row * 8 * a.ouvs + (uint64_t)col * 8;
+            J.ov = a.ov + (uint64_t)row * 8 * a.ouvs + (uint64_t)col * 8;
+            J.oys = a.oys;
+            J.ouvs = a.ouvs;
+          } else {
+            J.oy = a.out + (size_t)item * 384;
+            J.ou = J.oy + 256;
+            J.ov = J.oy + 320;
+            J.oys = 16;
+            J.ouvs = 8;
+          }
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---- (2) edge-clamped source regions into shared memory.
+#pragma unroll 1
+    for (int s = 2 * warp; s < 2 * warp + 2; s++) {
+      const Job& J = jobs[s];
+      if (J.skip) continue;
+      uint8_t* S = slots[s];
+      const int x8 = J.x16 >> 1, y8 = J.y16 >> 1;
+      if (!J.split) {
+        const short2 lm = J.lmv[0], cm = J.cmv[0];
+        const int lx = J.x16 + (lm.y >> 3) - 2, ly = J.y16 + (lm.x >> 3) - 2;
+        const int ux = x8 + (cm.y >> 3) - 2, uy = y8 + (cm.x >> 3) - 2;
+        for (int i = lane; i < 441 + 2 * 169; i += 32) {
+          if (i < 441) {
+            const int r = i / 21, c = i - 21 * r;
+            S[r * WY_STRIDE + c] = fetch(J.y, J.ys, a.lw, a.lh, lx + c, ly + r);
+          } else {
+            const int k = i - 441, p = k >= 169, kk = k - 169 * p;
+            const int r = kk / 13, c = kk - 13 * r;
+            S[(p ? WV_OFF : WU_OFF) + r * WC_STRIDE + c] = fetch(p ? J.v : J.u, J.uvs, a.cw, a.ch, ux + c, uy + r);
+          }
+        }
+      } else {
+        for (int i = lane; i < 24 * 81; i += 32) {
+          const int blk = i / 81, k = i - 81 * blk, r = k / 9, c = k - 9 * r;
+          uint8_t v;
+          if (blk < 16) {
+            const short2 m = J.lmv[blk];
+            v = fetch(J.y, J.ys, a.lw, a.lh, J.x16 + 4 * (blk & 3) + (m.y >> 3) - 2 + c,
+                      J.y16 + 4 * (blk >> 2) + (m.x >> 3) - 2 + r);
+          } else {
+            const int cb = (blk - 16) & 3, p = (blk - 16) >> 2;
+            const short2 m = J.cmv[cb];
+            v = fetch(p ? J.v : J.u, J.uvs, a.cw, a.ch, x8 + 4 * (cb & 1) + (m.y >> 3) - 2 + c,
+                      y8 + 4 * (cb >> 1) + (m.x >> 3) - 2 + r);
+          }
+          S[blk * HALO_BYTES + r * HALO_STRIDE + c] = v;
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---- (3) tasks: 48 per MB.
+#pragma unroll 1
+    for (int t = tid; t < PR_MBS * PR_TASKS; t += PR_THREADS) {
+      const int s = t / PR_TASKS, k = t - PR_TASKS * s;
+      const Job& J = jobs[s];
+      if (J.skip) continue;
+      const uint8_t* S = slots[s];
+      const uint8_t* win;
+      int ws, sb, sc, h;
+      short2 m;
+      uint8_t* dst;
+      uint64_t ds;
+      if (k < 32) {
+        const int b = k >> 1;
+        h = k & 1;
+        sb = b >> 2;
+        sc = b & 3;
+        m = J.lmv[b];
+        if (J.split) {
+          win = S + b * HALO_BYTES + 2 * h * HALO_STRIDE;
+          ws = HALO_STRIDE;
+        } else {
+          win = S + (4 * sb + 2 * h) * WY_STRIDE + 4 * sc;
+          ws = WY_STRIDE;
+        }
+        dst = J.oy;
+        ds = J.oys;
+      } else {
+        const int kk = k - 32, p = kk >> 3, cb = (kk >> 1) & 3;
+        h = kk & 1;
+        sb = cb >> 1;
+        sc = cb & 1;
+        m = J.cmv[cb];
+        if (J.split) {
+          win = S + (16 + 4 * p + cb) * HALO_BYTES + 2 * h * HALO_STRIDE;
+          ws = HALO_STRIDE;
+        } else {
+          win = S + (p ? WV_OFF : WU_OFF) + (4 * sb + 2 * h) * WC_STRIDE + 4 * sc;
+          ws = WC_STRIDE;
+        }
+        dst = p ? J.ov : J.ou;
+        ds = J.ouvs;
+      }
+      uint32_t o0, o1;
+      predict_pair(win, ws, m.y & 7, m.x & 7, tw, o0, o1);
+      uint8_t* d0 = dst + (uint64_t)(4 * sb + 2 * h) * ds + 4 * sc;
+      store_row(d0, o0, a.aligned_out);
+      store_row(d0 + ds, o1, a.aligned_out);
+    }
+    __syncthreads();
+  }
+}
+
+int g_pred_blocks_per_sm[3] = {0, 0, 0};
+
+template <int MODE>
+vp8a_status launch(vp8a_ctx* ctx, const PredArgs& a) {
+  if (a.n == 0) return VP8A_OK;
+  if (!g_pred_blocks_per_sm[MODE]) {
+    int b = 0;
+    VP8A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, predict_kernel<MODE>, PR_THREADS, 0));
+    g_pred_blocks_per_sm[MODE] = std::max(b, 1);
+  }
+  const size_t groups = (a.n + PR_MBS - 1) / PR_MBS;
+  const unsigned grid = (unsigned)std::min<size_t>(groups, (size_t)ctx->sm_count * g_pred_blocks_per_sm[MODE]);
+  predict_kernel<MODE><<<grid, PR_THREADS, 0, ctx->stream>>>(a);
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
+  return VP8A_OK;
+}
+
+vp8a_status check_planes(const vp8a_planes* p, const char* what) {
+  if (!p || !p->y || !p->u || !p->v) {
+    vp8a::set_error(std::string(what) + ": null plane");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (p->mb_cols == 0 || p->mb_rows == 0 || p->mb_cols > 1024 || p->mb_rows > 1024) {
+    vp8a::set_error(std::string(what) + ": MB grid must be 1..1024 x 1..1024");
+    return VP8A_E_INVALID_DIMENSIONS;
+  }
+  if (p->y_stride < (uint64_t)p->mb_cols * 16 || p->uv_stride < (uint64_t)p->mb_cols * 8) {
+    vp8a::set_error(std::string(what) + ": stride below the MB-padded width");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  return VP8A_OK;
+}
+
+size_t luma_bytes(const vp8a_planes* p) { return p->y_stride * ((size_t)p->mb_rows * 16 - 1) + (size_t)p->mb_cols * 16; }
+size_t chroma_bytes(const vp8a_planes* p) { return p->uv_stride * ((size_t)p->mb_rows * 8 - 1) + (size_t)p->mb_cols * 8; }
+
+// Stages one reference's planes (read-only) into a.refs[k].
+vp8a_status stage_ref(vp8a::Stager& st, const vp8a_planes* p, PredPlanes* out) {
+  vp8a_status s;
+  const void* d;
+  if ((s = st.in(p->y, luma_bytes(p), &d)) != VP8A_OK) return s;
+  out->y = (const uint8_t*)d;
+  if ((s = st.in(p->u, chroma_bytes(p), &d)) != VP8A_OK) return s;
+  out->u = (const uint8_t*)d;
+  if ((s = st.in(p->v, chroma_bytes(p), &d)) != VP8A_OK) return s;
+  out->v = (const uint8_t*)d;
+  out->ys = p->y_stride;
+  out->uvs = p->uv_stride;
+  return VP8A_OK;
+}
+
+void set_dims(PredArgs& a, const vp8a_planes* p) {
+  a.lw = (int)p->mb_cols * 16;
+  a.lh = (int)p->mb_rows * 16;
+  a.cw = (int)p->mb_cols * 8;
+  a.ch = (int)p->mb_rows * 8;
+}
+
+vp8a_status predict_batch(vp8a_ctx* ctx, const vp8a_planes* ref, const uint32_t* mb_xy, const vp8a_mv* mvs,
+                          uint32_t n, uint32_t full_pixel, uint32_t filter_set, uint8_t* out, bool split) {
+  if (!ctx) {
+    vp8a::set_error("null context");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (filter_set > VP8A_FILTER_BILINEAR) {
+    vp8a::set_error("filter_set must be VP8A_FILTER_SIXTAP or VP8A_FILTER_BILINEAR");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  vp8a_status s;
+  if ((s = check_planes(ref, "reference")) != VP8A_OK) return s;
+  if (n == 0) return VP8A_OK;
+  if (!mb_xy || !mvs || !out) {
+    vp8a::set_error("null batch argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  PredArgs a{};
+  if ((s = stage_ref(st, ref, &a.refs[0])) != VP8A_OK) return s;
+  a.ref_ids[0] = VP8A_REF_LAST;
+  a.n_refs = 1;
+  set_dims(a, ref);
+  const void* d;
+  if ((s = st.in(mb_xy, (size_t)n * 8, &d)) != VP8A_OK) return s;
+  a.mb_xy = (const uint32_t*)d;
+  if ((s = st.in(mvs, (size_t)n * (split ? 16 : 1) * sizeof(vp8a_mv), &d)) != VP8A_OK) return s;
+  a.mvs = (const vp8a_mv*)d;
+  void* o;
+  if ((s = st.out(out, (size_t)n * 384, &o)) != VP8A_OK) return s;
+  a.out = (uint8_t*)o;
+  a.aligned_out = ((uintptr_t)o & 3) == 0;
+  a.n = n;
+  a.full_pixel = full_pixel != 0;
+  a.filter_set = (int)filter_set;
+  if ((s = split ? launch<PRED_SPLIT>(ctx, a) : launch<PRED_WHOLE>(ctx, a)) != VP8A_OK) return s;
+  return st.finish();
+}
+
+}  // namespace
+
+extern "C" {
+
+vp8a_status vp8a_predict_inter_mb(vp8a_ctx* ctx, const vp8a_planes* ref, const uint32_t* mb_xy, const vp8a_mv* mvs,
+                                  uint32_t n, uint32_t full_pixel, uint32_t filter_set, uint8_t* out) {
+  return predict_batch(ctx, ref, mb_xy, mvs, n, full_pixel, filter_set, out, false);
+}
+
+vp8a_status vp8a_predict_split_mv(vp8a_ctx* ctx, const vp8a_planes* ref, const uint32_t* mb_xy,
+                                  const vp8a_mv* split_mvs, uint32_t n, uint32_t full_pixel, uint32_t filter_set,
+                                  uint8_t* out) {
+  return predict_batch(ctx, ref, mb_xy, split_mvs, n, full_pixel, filter_set, out, true);
+}
+
+vp8a_status vp8a_predict_inter_frame(vp8a_ctx* ctx, const vp8a_planes* refs, const uint8_t* ref_ids, uint32_t n_refs,
+                                     const vp8a_mb_decision* decisions, uint32_t full_pixel, uint32_t filter_set,
+                                     vp8a_planes* out) {
+  if (!ctx || !refs || !ref_ids || !decisions) {
+    vp8a::set_error("null argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (n_refs == 0 || n_refs > (uint32_t)MAX_PRED_REFS) {
+    vp8a::set_error("n_refs must be 1..3");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (filter_set > VP8A_FILTER_BILINEAR) {
+    vp8a::set_error("filter_set must be VP8A_FILTER_SIXTAP or VP8A_FILTER_BILINEAR");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  vp8a_status s;
+  if ((s = check_planes(out, "output")) != VP8A_OK) return s;
+  for (uint32_t k = 0; k < n_refs; k++) {
+    if ((s = check_planes(&refs[k], "reference")) != VP8A_OK) return s;
+    if (refs[k].mb_cols != out->mb_cols || refs[k].mb_rows != out->mb_rows) {
+      vp8a::set_error("reference planes do not match the output MB grid");
+      return VP8A_E_REFERENCE_DIMENSIONS_MISMATCH;
+    }
+  }
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  PredArgs a{};
+  uint8_t ids[MAX_PRED_REFS];
+  if ((s = st.read_to_host(ref_ids, n_refs, ids)) != VP8A_OK) return s;
+  for (uint32_t k = 0; k < n_refs; k++) {
+    if (ids[k] < VP8A_REF_LAST || ids[k] > VP8A_REF_ALTREF) {
+      vp8a::set_error("reference ids must be VP8A_REF_LAST, _GOLDEN or _ALTREF");
+      return VP8A_E_INVALID_ARGUMENT;
+    }
+    if ((s = stage_ref(st, &refs[k], &a.refs[k])) != VP8A_OK) return s;
+    a.ref_ids[k] = ids[k];
+  }
+  a.n_refs = (int)n_refs;
+  set_dims(a, out);
+  a.mb_cols = (int)out->mb_cols;
+  const uint32_t n = out->mb_cols * out->mb_rows;
+  const void* d;
+  if ((s = st.in(decisions, (size_t)n * sizeof(vp8a_mb_decision), &d)) != VP8A_OK) return s;
+  a.dec = (const vp8a_mb_decision*)d;
+  // In/out: MBs without an inter reference keep the caller's pixels.
+  void* o;
+  if ((s = st.inout(out->y, luma_bytes(out), &o)) != VP8A_OK) return s;
+  a.oy = (uint8_t*)o;
+  if ((s = st.inout(out->u, chroma_bytes(out), &o)) != VP8A_OK) return s;
+  a.ou = (uint8_t*)o;
+  if ((s = st.inout(out->v, chroma_bytes(out), &o)) != VP8A_OK) return s;
+  a.ov = (uint8_t*)o;
+  a.oys = out->y_stride;
+  a.ouvs = out->uv_stride;
+  a.aligned_out = (((uintptr_t)a.oy | (uintptr_t)a.ou | (uintptr_t)a.ov | a.oys | a.ouvs) & 3) == 0;
+  a.n = n;
+  a.full_pixel = full_pixel != 0;
+  a.filter_set = (int)filter_set;
+  if ((s = launch<PRED_FRAME>(ctx, a)) != VP8A_OK) return s;
+  return st.finish();
+}
+
+}  // extern "C"

@@ -10,6 +10,7 @@ from .api import (
     analyse_inter_frame,
     build_arnr_altref,
     filter_frame,
+    filter_set_for_version,
     filter_sweep,
     half_pixel_refine_luma,
     key_frame_sampling,
@@ -17,6 +18,9 @@ from .api import (
     mb_luma_sad_at_mv,
     motion_descent,
     neighbours_from_decisions,
+    predict_inter_frame,
+    predict_inter_mb,
+    predict_split_mv,
     rd_inter_search,
     quarter_pixel_refine_luma,
     rd_lambda,
@@ -40,12 +44,16 @@ __all__ = [
     "analyse_inter_frame",
     "build_arnr_altref",
     "filter_frame",
+    "filter_set_for_version",
     "filter_sweep",
     "half_pixel_refine_luma",
     "key_frame_sampling",
     "lf_info_from_decisions",
     "mb_luma_sad_at_mv",
     "neighbours_from_decisions",
+    "predict_inter_frame",
+    "predict_inter_mb",
+    "predict_split_mv",
     "rd_inter_search",
     "motion_descent",
     "quarter_pixel_refine_luma",

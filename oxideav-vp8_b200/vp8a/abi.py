@@ -38,6 +38,7 @@ STATUS_NAMES = {
 
 REF_INTRA, REF_LAST, REF_GOLDEN, REF_ALTREF = 0, 1, 2, 3
 MODE_ZERO, MODE_NEAREST, MODE_NEAR, MODE_NEW, MODE_SPLIT, MODE_NONE = 0, 1, 2, 3, 4, 255
+FILTER_SIXTAP, FILTER_BILINEAR = 0, 1
 PART_TOP_BOTTOM, PART_LEFT_RIGHT, PART_QUARTERS, PART_MV16, PART_NONE = 0, 1, 2, 3, 255
 
 

@@ -190,6 +190,60 @@ def neighbours_from_decisions(dec):
     return np.ascontiguousarray(nb.reshape(-1))
 
 
+def filter_set_for_version(version):
+    """filter_set_for_version (src/motion_comp.rs:370): version 0 selects
+    the six-tap set, any other version the bilinear set."""
+    return abi.FILTER_SIXTAP if version == 0 else abi.FILTER_BILINEAR
+
+
+def _contig(a):
+    return a if hasattr(a, "data_ptr") else np.ascontiguousarray(a)
+
+
+def predict_inter_mb(ctx, ref, mb_xy, mvs, full_pixel=False, filter_set=abi.FILTER_SIXTAP, out=None):
+    """predict_inter_mb (src/motion_comp.rs:1986) over a batch: item i is the
+    MB at mb_xy[i] = (mb_col, mb_row) under the quarter-pel vector mvs[i].
+    `ref` = MB-padded (y, u, v). Returns (n, 384) uint8 ReconstructedMb
+    records: y[256], u[64], v[64] in raster order."""
+    p = planes(*ref)
+    xy, mv = _xy(mb_xy), _mvs(mvs)
+    n = len(mv)
+    o = np.zeros((n, 384), np.uint8) if out is None else out
+    check(ctx._lib.vp8a_predict_inter_mb(ctx.handle, C.byref(p), ptr(xy), ptr(mv), n, int(bool(full_pixel)),
+                                         filter_set, ptr(o)), "vp8a_predict_inter_mb")
+    return o
+
+
+def predict_split_mv(ctx, ref, mb_xy, split_mvs, full_pixel=False, filter_set=abi.FILTER_SIXTAP, out=None):
+    """predict_split_mv (src/motion_comp.rs:2228) over a batch: 16
+    quarter-pel vectors per item (raster sub-block order)."""
+    p = planes(*ref)
+    xy, mv = _xy(mb_xy), _mvs(split_mvs)
+    n = len(mv) // 16
+    assert len(mv) == 16 * n and len(xy) == n, "need 16 vectors and one position per MB"
+    o = np.zeros((n, 384), np.uint8) if out is None else out
+    check(ctx._lib.vp8a_predict_split_mv(ctx.handle, C.byref(p), ptr(xy), ptr(mv), n, int(bool(full_pixel)),
+                                         filter_set, ptr(o)), "vp8a_predict_split_mv")
+    return o
+
+
+def predict_inter_frame(ctx, refs, ref_ids, decisions, out, full_pixel=False, filter_set=abi.FILTER_SIXTAP):
+    """The prediction pick_mb_for_ref builds for each MB's chosen mode
+    (src/encoder.rs:8704-8735), written into the MB-padded planes `out` =
+    (y, u, v) in place; MBs without an inter reference keep their pixels.
+    `decisions` is vp8a_analyse_inter_frame's output (any shape, raster
+    order). Returns `out`."""
+    prs = [planes(*p) for p in refs]
+    parr = (abi.Planes * len(prs))(*prs)
+    ids = np.ascontiguousarray(np.asarray(ref_ids, np.uint8))
+    dec = _contig(decisions)
+    op = planes(*out)
+    check(ctx._lib.vp8a_predict_inter_frame(ctx.handle, C.cast(parr, C.c_void_p), ptr(ids), len(prs), ptr(dec),
+                                            int(bool(full_pixel)), filter_set, C.byref(op)),
+          "vp8a_predict_inter_frame")
+    return out
+
+
 def build_arnr_altref(ctx, frames, center, strength=3):
     """build_arnr_altref (src/arnr.rs:476). `frames` = list of (y, u, v).
     Returns the packed (y, u, v) anchor."""
