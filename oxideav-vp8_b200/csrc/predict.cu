@@ -13,9 +13,9 @@
 //
 // Step: (1) 16 threads per MB derive the eighth-pel vectors of its 16 luma
 // and 4 chroma blocks (stored_luma_mv, chroma_mv or split_chroma_mvs,
-// apply_full_pixel); (2) each warp copies the edge-clamped source of two MBs
-// into shared memory — one 21x21 luma and two 13x13 chroma regions for a
-// whole-MB vector, 24 9x9 block halos for SPLITMV; (3) each task reads a
+// apply_full_pixel); (2) the CTA copies the edge-clamped source of its MBs
+// into shared memory as 32-bit words — one 21x21 luma and two 13x13 chroma
+// regions for a whole-MB vector, 24 9x9 block halos for SPLITMV; (3) each task reads a
 // 12-byte-wide, 7-row window as 32-bit words and runs the horizontal pass
 // (4 outputs per row, dp4a with the tap row pre-shifted per output column),
 // packs the 8-bit intermediate with saturation, transposes it with byte
@@ -34,6 +34,7 @@ constexpr int SLOT_BYTES = 2592;    // 24 block halos of 9 rows x 12 bytes
 constexpr int WY_STRIDE = 24, WC_STRIDE = 16, WU_OFF = 504, WV_OFF = 712;  // whole-MB layout
 constexpr int HALO_STRIDE = 12, HALO_BYTES = 108;                          // SPLITMV layout
 constexpr int MAX_PRED_REFS = 3;
+constexpr int WHOLE_ROWS = 21 + 2 * 13, SPLIT_ROWS = 24 * 9;
 
 // §18.3 tap tables (SIXTAP_FILTERS / BILINEAR_FILTERS, src/motion_comp.rs:294-334).
 __constant__ int c_taps[2][8][6] = {
@@ -81,6 +82,7 @@ struct PredArgs {
   uint8_t *oy, *ou, *ov;
   uint64_t oys, ouvs;
   int aligned_out;  // every output row start is 4-byte aligned
+  int aligned_src;  // every reference plane base and row pitch is 4-byte aligned
 };
 
 struct Job {
@@ -180,11 +182,90 @@ __device__ __forceinline__ void store_row(uint8_t* p, uint32_t v, int aligned) {
   }
 }
 
-// Edge-clamped byte of a plane.
-__device__ __forceinline__ uint8_t fetch(const uint8_t* p, uint64_t stride, int w, int h, int x, int y) {
-  x = x < 0 ? 0 : (x >= w ? w - 1 : x);
-  y = y < 0 ? 0 : (y >= h ? h - 1 : y);
-  return __ldg(p + (uint64_t)y * stride + x);
+// Row i of MB slot S's staging list: one row of one region, copied to
+// shared memory so that smem byte c of the row is source column x0 + c of
+// source row y0 + r (edge-clamped; bytes past the region's `ncols` are
+// don't-care). A whole-MB vector has 21 luma rows of 21 bytes and 2 x 13
+// chroma rows of 13; SPLITMV has 24 x 9 block-halo rows of 9. Rows inside
+// the plane horizontally are read as aligned 32-bit words and realigned with
+// funnel shifts — the plane width is a multiple of 4, so a word that starts
+// inside it ends inside it; rows that straddle an edge take clamped bytes.
+__device__ __forceinline__ void stage_row(const Job& J, uint8_t* S, int i, const PredArgs& a) {
+  const uint8_t* plane;
+  uint64_t stride;
+  int w, h, x0, y0, r, ncols, off;
+  if (!J.split) {
+    if (i < 21) {
+      r = i;
+      plane = J.y;
+      stride = J.ys;
+      w = a.lw;
+      h = a.lh;
+      x0 = J.x16 + (J.lmv[0].y >> 3) - 2;
+      y0 = J.y16 + (J.lmv[0].x >> 3) - 2;
+      ncols = 21;
+      off = r * WY_STRIDE;
+    } else {
+      const int p = i >= 34;
+      r = i - 21 - 13 * p;
+      plane = p ? J.v : J.u;
+      stride = J.uvs;
+      w = a.cw;
+      h = a.ch;
+      x0 = (J.x16 >> 1) + (J.cmv[0].y >> 3) - 2;
+      y0 = (J.y16 >> 1) + (J.cmv[0].x >> 3) - 2;
+      ncols = 13;
+      off = (p ? WV_OFF : WU_OFF) + r * WC_STRIDE;
+    }
+  } else {
+    const int blk = i / 9;
+    r = i - 9 * blk;
+    ncols = 9;
+    off = blk * HALO_BYTES + r * HALO_STRIDE;
+    if (blk < 16) {
+      const short2 m = J.lmv[blk];
+      plane = J.y;
+      stride = J.ys;
+      w = a.lw;
+      h = a.lh;
+      x0 = J.x16 + 4 * (blk & 3) + (m.y >> 3) - 2;
+      y0 = J.y16 + 4 * (blk >> 2) + (m.x >> 3) - 2;
+    } else {
+      const int cb = (blk - 16) & 3;
+      const short2 m = J.cmv[cb];
+      plane = blk < 20 ? J.u : J.v;
+      stride = J.uvs;
+      w = a.cw;
+      h = a.ch;
+      x0 = (J.x16 >> 1) + 4 * (cb & 1) + (m.y >> 3) - 2;
+      y0 = (J.y16 >> 1) + 4 * (cb >> 1) + (m.x >> 3) - 2;
+    }
+  }
+  uint32_t* dst = reinterpret_cast<uint32_t*>(S + off);
+  const int sy = y0 + r < 0 ? 0 : (y0 + r >= h ? h - 1 : y0 + r);
+  const uint8_t* row = plane + (uint64_t)sy * stride;
+  const int nw = (ncols + 3) >> 2;  // words stored: 6, 4 or 3
+  if (a.aligned_src && x0 >= 0 && x0 + ncols <= w) {
+    const int j0 = x0 & ~3, sh = 8 * (x0 & 3);
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(row + j0);
+    const int avail = (w - j0) >> 2;  // words from j0 to the row's end
+    uint32_t wd[7];
+#pragma unroll
+    for (int k = 0; k < 7; k++) wd[k] = (k <= nw && k < avail) ? __ldg(src + k) : 0u;
+#pragma unroll
+    for (int k = 0; k < 6; k++)
+      if (k < nw) dst[k] = __funnelshift_r(wd[k], wd[k + 1], sh);
+    return;
+  }
+#pragma unroll 1
+  for (int k = 0; k < nw; k++) {
+    uint32_t v = 0;
+    for (int c = 0; c < 4 && 4 * k + c < ncols; c++) {
+      const int x = x0 + 4 * k + c;
+      v |= (uint32_t)__ldg(row + (x < 0 ? 0 : (x >= w ? w - 1 : x))) << (8 * c);
+    }
+    dst[k] = v;
+  }
 }
 
 template <int MODE>
@@ -192,7 +273,7 @@ __global__ void __launch_bounds__(PR_THREADS) predict_kernel(PredArgs a) {
   __shared__ __align__(16) uint8_t slots[PR_MBS][SLOT_BYTES];
   __shared__ Job jobs[PR_MBS];
   __shared__ uint32_t tw[8][4][3];  // tap words: [fraction][output shift][window word]
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x;
 
   // Tap words for dp4a: byte m of word q for output column j holds tap
   // 4q + m - j (0 outside 0..5). The identity fraction never uses them.
@@ -288,43 +369,25 @@ __global__ void __launch_bounds__(PR_THREADS) predict_kernel(PredArgs a) {
     }
     __syncthreads();
 
-    // ---- (2) edge-clamped source regions into shared memory.
+    // ---- (2) edge-clamped source regions into shared memory, one region
+    // row per thread and step over the 8 MBs' rows.
+    {
+      int start[PR_MBS + 1];
+      start[0] = 0;
+#pragma unroll
+      for (int q = 0; q < PR_MBS; q++)
+        start[q + 1] = start[q] + (jobs[q].skip ? 0 : (jobs[q].split ? SPLIT_ROWS : WHOLE_ROWS));
+      const int total = start[PR_MBS];
 #pragma unroll 1
-    for (int s = 2 * warp; s < 2 * warp + 2; s++) {
-      const Job& J = jobs[s];
-      if (J.skip) continue;
-      uint8_t* S = slots[s];
-      const int x8 = J.x16 >> 1, y8 = J.y16 >> 1;
-      if (!J.split) {
-        const short2 lm = J.lmv[0], cm = J.cmv[0];
-        const int lx = J.x16 + (lm.y >> 3) - 2, ly = J.y16 + (lm.x >> 3) - 2;
-        const int ux = x8 + (cm.y >> 3) - 2, uy = y8 + (cm.x >> 3) - 2;
-        for (int i = lane; i < 441 + 2 * 169; i += 32) {
-          if (i < 441) {
-            const int r = i / 21, c = i - 21 * r;
-            S[r * WY_STRIDE + c] = fetch(J.y, J.ys, a.lw, a.lh, lx + c, ly + r);
-          } else {
-            const int k = i - 441, p = k >= 169, kk = k - 169 * p;
-            const int r = kk / 13, c = kk - 13 * r;
-            S[(p ? WV_OFF : WU_OFF) + r * WC_STRIDE + c] = fetch(p ? J.v : J.u, J.uvs, a.cw, a.ch, ux + c, uy + r);
+      for (int i = tid; i < total; i += PR_THREADS) {
+        int s = 0, first = 0;
+#pragma unroll
+        for (int q = 1; q < PR_MBS; q++)
+          if (i >= start[q]) {
+            s = q;
+            first = start[q];
           }
-        }
-      } else {
-        for (int i = lane; i < 24 * 81; i += 32) {
-          const int blk = i / 81, k = i - 81 * blk, r = k / 9, c = k - 9 * r;
-          uint8_t v;
-          if (blk < 16) {
-            const short2 m = J.lmv[blk];
-            v = fetch(J.y, J.ys, a.lw, a.lh, J.x16 + 4 * (blk & 3) + (m.y >> 3) - 2 + c,
-                      J.y16 + 4 * (blk >> 2) + (m.x >> 3) - 2 + r);
-          } else {
-            const int cb = (blk - 16) & 3, p = (blk - 16) >> 2;
-            const short2 m = J.cmv[cb];
-            v = fetch(p ? J.v : J.u, J.uvs, a.cw, a.ch, x8 + 4 * (cb & 1) + (m.y >> 3) - 2 + c,
-                      y8 + 4 * (cb >> 1) + (m.x >> 3) - 2 + r);
-          }
-          S[blk * HALO_BYTES + r * HALO_STRIDE + c] = v;
-        }
+        stage_row(jobs[s], slots[s], i - first, a);
       }
     }
     __syncthreads();
@@ -434,6 +497,10 @@ vp8a_status stage_ref(vp8a::Stager& st, const vp8a_planes* p, PredPlanes* out) {
   return VP8A_OK;
 }
 
+int src_aligned(const PredPlanes& p) {
+  return (((uintptr_t)p.y | (uintptr_t)p.u | (uintptr_t)p.v | p.ys | p.uvs) & 3) == 0;
+}
+
 void set_dims(PredArgs& a, const vp8a_planes* p) {
   a.lw = (int)p->mb_cols * 16;
   a.lh = (int)p->mb_rows * 16;
@@ -464,6 +531,7 @@ vp8a_status predict_batch(vp8a_ctx* ctx, const vp8a_planes* ref, const uint32_t*
   if ((s = stage_ref(st, ref, &a.refs[0])) != VP8A_OK) return s;
   a.ref_ids[0] = VP8A_REF_LAST;
   a.n_refs = 1;
+  a.aligned_src = src_aligned(a.refs[0]);
   set_dims(a, ref);
   const void* d;
   if ((s = st.in(mb_xy, (size_t)n * 8, &d)) != VP8A_OK) return s;
@@ -534,6 +602,8 @@ vp8a_status vp8a_predict_inter_frame(vp8a_ctx* ctx, const vp8a_planes* refs, con
     a.ref_ids[k] = ids[k];
   }
   a.n_refs = (int)n_refs;
+  a.aligned_src = 1;
+  for (uint32_t k = 0; k < n_refs; k++) a.aligned_src &= src_aligned(a.refs[k]);
   set_dims(a, out);
   a.mb_cols = (int)out->mb_cols;
   const uint32_t n = out->mb_cols * out->mb_rows;

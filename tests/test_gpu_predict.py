@@ -125,8 +125,9 @@ def test_predict_inter_frame_from_analysis(ctx, oracle, w, h, seed):
 @pytest.mark.parametrize("filter_set", [abi.FILTER_SIXTAP, abi.FILTER_BILINEAR])
 def test_predict_inter_frame_mixed_decisions_device_strided(ctx, oracle, filter_set):
     # Synthetic decisions: intra MBs, a reference id with no planes, SPLIT and
-    # whole-MB vectors; output planes with a row pitch that is not a multiple
-    # of 4 (byte stores), all buffers on the device.
+    # whole-MB vectors; a reference and the output planes with a row pitch
+    # that is not a multiple of 4 (byte loads and stores), all buffers on
+    # the device.
     import torch
 
     rng = np.random.default_rng(31 + filter_set)
@@ -149,7 +150,12 @@ def test_predict_inter_frame_mixed_decisions_device_strided(ctx, oracle, filter_
     want = [padded(p, 3)[:, : p.shape[1]] for p in refs[0]]
     skipped = oracle.predict_inter_frame(refs, ids, dec, want, filter_set=filter_set)
     assert skipped == int(np.isin(dec["ref_frame"], [abi.REF_INTRA, abi.REF_ALTREF]).sum())
-    dref = [[torch.from_numpy(p).cuda() for p in r] for r in refs]
+    def strided(p):  # row pitch width + 3: word loads of the source are off
+        d = torch.zeros((p.shape[0], p.shape[1] + 3), dtype=torch.uint8, device="cuda")
+        d[:, : p.shape[1]] = torch.from_numpy(p).cuda()
+        return d[:, : p.shape[1]]
+
+    dref = [[torch.from_numpy(p).cuda() for p in refs[0]], [strided(p) for p in refs[1]]]
     dout = [torch.full((p.shape[0], p.shape[1] + 3), 200, dtype=torch.uint8, device="cuda")[:, : p.shape[1]]
             for p in refs[0]]
     ddec = torch.from_numpy(dec.view(np.uint8).copy()).cuda()
