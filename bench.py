@@ -216,6 +216,11 @@ class GpuStep:
         self.planes = (abi.Planes * 3)(vp8a.planes(*self.last), vp8a.planes(*self.golden), vp8a.planes(*self.alt))
         self.recon_planes = vp8a.planes(*self.recon)
         self.src = vp8a.source(*self.cur)
+        # §18 prediction of every MB's decision (the encoder's next step after
+        # the analysis; timed as its own stage, outside the metric's step).
+        self.pred = [torch.zeros_like(p) for p in self.last]
+        self.pred_planes = vp8a.planes(*self.pred)
+        self.host_ids = np.array([1, 2, 3], np.uint8)
 
     def run_arnr(self):
         v = self.vp8a
@@ -247,6 +252,12 @@ class GpuStep:
         self.ctx.synchronize()
         t = self.table.cpu().numpy().view(np.uint64)
         return select_full(t, 0)
+
+    def run_predict(self):
+        st = self.lib.vp8a_predict_inter_frame(self.ctx.handle, C.cast(self.planes, C.c_void_p),
+                                               self.host_ids.ctypes.data, 3, self.dec.data_ptr(), 0,
+                                               self.abi.FILTER_SIXTAP, C.byref(self.pred_planes))
+        assert st == 0, self.vp8a.load().vp8a_last_error()
 
     def step(self):
         self.run_arnr()
@@ -397,7 +408,7 @@ def gpu_arm(args):
         value = N_MB * args.steps * world / (ms / 1000.0)
         e2e = N_MB * args.steps * world / (e_ms / 1000.0)
         peak, peak_kind = peaks()
-        dom = max(stage, key=lambda k: stage[k]["ms"])
+        dom = max((k for k in stage if k not in EXTRA_STAGES), key=lambda k: stage[k]["ms"])
         d = stage[dom]
         achieved = d["bytes"] / (d["ms"] / 1000.0) / 1e9
         ipeak = int32_peak_tops()
@@ -407,7 +418,8 @@ def gpu_arm(args):
             tops = v["ops"] / (v["ms"] / 1000.0) / 1e12
             stages[k] = {"ms": round(v["ms"], 4), "reps_ms": v["reps"], "alg_bytes": int(v["bytes"]),
                          "dram_traffic": dram_traffic(k), "gbs": round(gbs, 2), "hbm_frac": round(gbs / peak, 5),
-                         "alg_ops": int(v["ops"]), "tops": round(tops, 3), "alu_frac": round(tops / ipeak, 4)}
+                         "alg_ops": int(v["ops"]), "tops": round(tops, 3), "alu_frac": round(tops / ipeak, 4),
+                         "in_step": k not in EXTRA_STAGES}
         result = {
             "metric": METRIC,
             "value": round(value, 1),
@@ -468,7 +480,12 @@ STAGE_OPS = {
     "analysis": N_MB * 3 * 92_000,
     "arnr": (LOOKAHEAD - 1) * N_MB * 33 * 256 + (LOOKAHEAD - 1) * (W * H * 3 // 2) * 4,
     "lf_sweep": 512 * N_MB * 9_000,
+    # Two-pass six-tap MACs of a sub-pel MB: luma 21x16 + 16x16, chroma
+    # 2 x (13x8 + 8x8) outputs, 6 taps each.
+    "predict": N_MB * 6 * (21 * 16 + 16 * 16 + 2 * (13 * 8 + 8 * 8)),
 }
+# Stages outside the metric's step (reported, not in `value`).
+EXTRA_STAGES = ("predict",)
 def int32_peak_tops():
     """Nominal INT32 issue peak: 148 SMs x 128 lanes x max SM clock (no
     measured integer peak is available)."""
@@ -503,8 +520,13 @@ def stage_times(gs, stream, torch, flush, reps=3):
         "arnr": (gs.run_arnr, LOOKAHEAD * pic + pic),
         "analysis": (gs.run_analysis, luma + 3 * padded + N_MB * gs.abi.MB_DECISION_DTYPE.itemsize),
         "lf_sweep": (lambda: gs.run_lf(), padded_pic + pic + N_MB * 8 + 512 * 8),
+        # Decisions read, one MB of reference pixels read and one written per
+        # MB; a short kernel, so timed over 10 back-to-back calls.
+        "predict": (gs.run_predict, N_MB * (gs.abi.MB_DECISION_DTYPE.itemsize + 2 * 384), 10),
     }
-    for name, (fn, nbytes) in fns.items():
+    for name, spec in fns.items():
+        fn, nbytes = spec[0], spec[1]
+        calls = spec[2] if len(spec) > 2 else 1
         ts = []
         for _ in range(reps):
             with torch.cuda.stream(stream):
@@ -512,10 +534,11 @@ def stage_times(gs, stream, torch, flush, reps=3):
             torch.cuda.synchronize()
             s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             s.record(stream)
-            fn()
+            for _ in range(calls):
+                fn()
             e.record(stream)
             e.synchronize()
-            ts.append(s.elapsed_time(e))
+            ts.append(s.elapsed_time(e) / calls)
         out[name] = {"ms": float(np.median(ts)), "bytes": nbytes, "ops": STAGE_OPS[name],
                      "reps": [round(x, 3) for x in ts]}
     return out
@@ -612,22 +635,53 @@ def case_arm(args):
     MB_COLS, MB_ROWS = (w + 15) // 16, (h + 15) // 16
     N_MB = MB_COLS * MB_ROWS
     ctx = vp8a.Context(0)
-    frames, _ = synth.make_sequence(w, h, 16, SEED, pieces=4, occluders=4)
-    gs = GpuStep(ctx, frames, vp8a.load(), torch, 0)
-    fn = {"arnr": gs.run_arnr, "analysis": gs.run_analysis, "lf": gs.run_lf}[args.case]
+    if args.case in ("predict_mb", "predict_split"):
+        fn = batched_predict(ctx, vp8a, torch, args.case == "predict_split")
+    else:
+        frames, _ = synth.make_sequence(w, h, 16, SEED, pieces=4, occluders=4)
+        gs = GpuStep(ctx, frames, vp8a.load(), torch, 0)
+        fn = {"arnr": gs.run_arnr, "analysis": gs.run_analysis, "lf": gs.run_lf, "predict": gs.run_predict}[args.case]
+    stream = torch.cuda.ExternalStream(ctx.stream)
     for _ in range(args.warmup):
         fn()
     ctx.synchronize()
     ts = []
     for _ in range(args.steps):
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record(gs.stream)
+        s.record(stream)
         fn()
-        e.record(gs.stream)
+        e.record(stream)
         e.synchronize()
         ts.append(s.elapsed_time(e))
     ctx.close()
     return {"case": args.case, "size": args.size, "ms": [round(x, 4) for x in ts]}
+
+
+def batched_predict(ctx, vp8a, torch, split):
+    """vp8a_predict_inter_mb (or _split_mv) over 8 frames' worth of MBs at
+    random positions of random MB-padded reference planes of the --size grid,
+    vectors within +-16 px: the batched entry points at a size that fills
+    the GPU."""
+    from vp8a.frames import planes
+
+    rng = np.random.default_rng(SEED)
+    shapes = [(MB_ROWS * 16, MB_COLS * 16), (MB_ROWS * 8, MB_COLS * 8), (MB_ROWS * 8, MB_COLS * 8)]
+    ref = [torch.from_numpy(rng.integers(0, 256, s, dtype=np.uint8)).cuda() for s in shapes]
+    n = 8 * N_MB
+    xy = np.stack([rng.integers(0, MB_COLS, n), rng.integers(0, MB_ROWS, n)], 1).astype(np.uint32)
+    mv = rng.integers(-64, 65, (n * (16 if split else 1), 2)).astype(np.int16)
+    dxy, dmv = torch.from_numpy(xy.view(np.int32)).cuda(), torch.from_numpy(mv).cuda()
+    out = torch.empty(n * 384, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    p = planes(*ref)
+    call = ctx._lib.vp8a_predict_split_mv if split else ctx._lib.vp8a_predict_inter_mb
+
+    def fn():
+        st = call(ctx.handle, C.byref(p), dxy.data_ptr(), dmv.data_ptr(), n, 0, 0, out.data_ptr())
+        assert st == 0, vp8a.load().vp8a_last_error()
+
+    fn.keep = (ref, dxy, dmv, out, p)
+    return fn
 
 
 def main():
@@ -638,7 +692,8 @@ def main():
     ap.add_argument("--impl", default="vp8a", choices=["vp8a", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
-    ap.add_argument("--case", choices=["arnr", "analysis", "lf"], help="profile one stage alone")
+    ap.add_argument("--case", choices=["arnr", "analysis", "lf", "predict", "predict_mb", "predict_split"],
+                    help="profile one stage alone")
     ap.add_argument("--size", default="1920x1080", help="frame size for --case")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl != "reference":
