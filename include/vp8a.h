@@ -330,6 +330,17 @@ double vp8a_rd_lambda(uint32_t y_ac_qi);
 
 /* ------------------------------------------- §18 inter prediction (MC) */
 
+/* QuantIndices (src/coded_header.rs:171); an absent delta is 0. */
+typedef struct vp8a_quant_indices {
+  uint8_t y_ac_qi;
+  int8_t y_dc_delta;
+  int8_t y2_dc_delta;
+  int8_t y2_ac_delta;
+  int8_t uv_dc_delta;
+  int8_t uv_ac_delta;
+  uint8_t reserved[2];
+} vp8a_quant_indices;
+
 /* FilterSet (src/motion_comp.rs:344). filter_set_for_version
  * (src/motion_comp.rs:370): frame-tag version 0 uses SIXTAP, any other
  * version BILINEAR. */
@@ -368,6 +379,45 @@ vp8a_status vp8a_predict_inter_frame(vp8a_ctx* ctx, const vp8a_planes* refs,
                                      const uint8_t* ref_ids, uint32_t n_refs,
                                      const vp8a_mb_decision* decisions, uint32_t full_pixel,
                                      uint32_t filter_set, vp8a_planes* out);
+
+/* ------------------------------------- §14 inter reconstruction (trellis off) */
+
+/* MbDequantFactors::from_quant_indices / for_segment (src/dequant.rs:169,
+ * :201): out = {y1_dc, y1_ac, y2_dc, y2_ac, uv_dc, uv_ac}. With
+ * has_segment, the base index is segment_quant (absolute) or y_ac_qi +
+ * segment_quant. Host only; no context needed. */
+void vp8a_dequant_factors(const vp8a_quant_indices* qi, uint32_t has_segment,
+                          int32_t segment_quant, uint32_t absolute, int16_t* out);
+
+/* Per-MB flags of vp8a_reconstruct_inter_frame. */
+enum { VP8A_MB_SKIP = 1, VP8A_MB_HAS_COEFFS = 2 };
+
+/* The §18 + §14 step pick_mb_for_ref runs for its chosen mode
+ * (src/encoder.rs:8704-8800) with TrellisStrength::OFF (src/encoder.rs:2677),
+ * for every MB of a frame: the prediction of vp8a_predict_inter_frame; the
+ * residual against the source MB (I420Frame::extract_mb,
+ * src/encoder.rs:5549, edge-replicated); forward DCT, Y2 WHT for non-SPLITMV
+ * MBs and plain rounding (transform_whole_block_luma_rd :3815,
+ * transform_split_mv_mb_rd :8259, transform_chroma_plane_rd :4133,
+ * enc_quantize_block :2127); §11.1 skip detection; dequantisation and
+ * reconstruct_inter_mb / reconstruct_split_mv_mb (src/motion_comp.rs:2098,
+ * :2340). `frame` is the visible source picture; `recon` (MB-padded, the
+ * references' grid) receives the reconstruction. Optional outputs:
+ * `coeffs`, 400 int16 per MB in MbCoeffs order (src/frame.rs:98: y2[16],
+ * y[16][16], u[4][16], v[4][16], raster coefficient order, quantised);
+ * `mb_flags`, VP8A_MB_SKIP | VP8A_MB_HAS_COEFFS per MB (mb_has_coeffs,
+ * src/loop_filter.rs:1500). `mb_segment` (optional, one int8 per MB, -1 =
+ * none) selects the factors of segment k from segment_quant[k]
+ * (for_segment with `segment_abs`). MBs whose ref_frame is VP8A_REF_INTRA
+ * or has no plane in `refs` keep recon's pixels and get flags 0. */
+vp8a_status vp8a_reconstruct_inter_frame(vp8a_ctx* ctx, const vp8a_i420* frame,
+                                         const vp8a_planes* refs, const uint8_t* ref_ids,
+                                         uint32_t n_refs, const vp8a_mb_decision* decisions,
+                                         const vp8a_quant_indices* quant,
+                                         const int8_t* mb_segment, const int16_t* segment_quant,
+                                         uint32_t segment_abs, uint32_t full_pixel,
+                                         uint32_t filter_set, vp8a_planes* recon,
+                                         int16_t* coeffs, uint8_t* mb_flags);
 
 /* ------------------------------------------------------------ ARNR filter */
 

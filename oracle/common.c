@@ -68,6 +68,7 @@ size_t vo_type_size(int which) {
     case 10: return sizeof(vp8a_source);
     case 11: return sizeof(vp8a_mb_info);
     case 12: return sizeof(vp8a_rd_inter);
+    case 13: return sizeof(vp8a_quant_indices);
     default: return 0;
   }
 }

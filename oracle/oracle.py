@@ -85,6 +85,16 @@ def load():
         "vo_predict_inter_mb_batch": (None, [C.POINTER(abi.Planes), P, P, U32, C.c_int, C.c_int, P]),
         "vo_predict_split_mv_batch": (None, [C.POINTER(abi.Planes), P, P, U32, C.c_int, C.c_int, P]),
         "vo_predict_inter_frame": (C.c_int, [P, P, U32, P, C.c_int, C.c_int, C.POINTER(abi.Planes)]),
+        "vo_dequant_factors": (None, [C.c_int32] * 6 + [P]),
+        "vo_segment_factors": (None, [C.POINTER(abi.QuantIndices), C.c_int, C.c_int32, C.c_int, P]),
+        "vo_forward_dct_4x4": (None, [P, P]),
+        "vo_forward_wht_4x4": (None, [P, P]),
+        "vo_inverse_dct_4x4": (None, [P, P]),
+        "vo_inverse_wht_4x4": (None, [P, P]),
+        "vo_enc_quantize_block": (None, [P, C.c_int16, C.c_int16]),
+        "vo_reconstruct_inter_mb": (C.c_int, [P, P, P, C.c_int, P]),
+        "vo_reconstruct_inter_frame": (C.c_int, [C.POINTER(abi.I420), P, P, U32, P, C.POINTER(abi.QuantIndices), P, P,
+                                                 C.c_int, C.c_int, C.c_int, C.POINTER(abi.Planes), P, P]),
         "vo_rd_inter_search": (C.c_int, [C.POINTER(abi.I420), P, P, U32, C.POINTER(abi.MvContexts), C.c_double,
                                          U32, U32, P, P, U32]),
     }
@@ -115,7 +125,7 @@ def type_sizes():
     lib = load()
     names = ["vp8a_mv", "vp8a_search_result", "vp8a_luma_ref", "vp8a_i420", "vp8a_planes", "vp8a_mv_contexts",
              "vp8a_mb_decision", "vp8a_ref_search", "vp8a_mb_lf_info", "vp8a_filter_config", "vp8a_source",
-             "vp8a_mb_info", "vp8a_rd_inter"]
+             "vp8a_mb_info", "vp8a_rd_inter", "vp8a_quant_indices"]
     return {n: int(lib.vo_type_size(i)) for i, n in enumerate(names)}
 
 
@@ -442,3 +452,83 @@ def predict_inter_frame(refs, ref_ids, decisions, out, full_pixel=False, filter_
     op = planes(*out)
     return load().vo_predict_inter_frame(C.cast(parr, C.c_void_p), ptr(ids), len(prs), ptr(dec),
                                          int(bool(full_pixel)), filter_set, C.byref(op))
+
+
+# ---- §14 inter reconstruction, trellis off (recon.c) ---------------------
+
+def dequant_factors(q, ydc=0, y2dc=0, y2ac=0, uvdc=0, uvac=0):
+    """MbDequantFactors::from_base_and_deltas (src/dequant.rs:118):
+    (y1_dc, y1_ac, y2_dc, y2_ac, uv_dc, uv_ac)."""
+    out = np.zeros(6, np.int16)
+    load().vo_dequant_factors(q, ydc, y2dc, y2ac, uvdc, uvac, ptr(out))
+    return tuple(int(x) for x in out)
+
+
+def segment_factors(qi, segment_quant=None, absolute=False):
+    """from_quant_indices / for_segment (src/dequant.rs:169, :201)."""
+    out = np.zeros(6, np.int16)
+    load().vo_segment_factors(C.byref(qi), segment_quant is not None, segment_quant or 0, int(absolute), ptr(out))
+    return tuple(int(x) for x in out)
+
+
+def _blk(fn, block):
+    a = np.ascontiguousarray(np.asarray(block, np.int16).reshape(16))
+    out = np.zeros(16, np.int16)
+    fn(ptr(a), ptr(out))
+    return out
+
+
+def forward_dct_4x4(block):
+    return _blk(load().vo_forward_dct_4x4, block)
+
+
+def forward_wht_4x4(block):
+    return _blk(load().vo_forward_wht_4x4, block)
+
+
+def inverse_dct_4x4(block):
+    return _blk(load().vo_inverse_dct_4x4, block)
+
+
+def inverse_wht_4x4(block):
+    return _blk(load().vo_inverse_wht_4x4, block)
+
+
+def enc_quantize_block(block, dc, ac):
+    a = np.ascontiguousarray(np.asarray(block, np.int16).reshape(16)).copy()
+    load().vo_enc_quantize_block(ptr(a), dc, ac)
+    return a
+
+
+def reconstruct_inter_mb(src384, pred384, factors, split):
+    """The §14 half of the chosen-mode step for one MB: returns
+    (recon 384 B, quantised coeffs (400,) int16, flags)."""
+    src = np.ascontiguousarray(np.asarray(src384, np.uint8).reshape(384))
+    rec = np.ascontiguousarray(np.asarray(pred384, np.uint8).reshape(384)).copy()
+    f = np.ascontiguousarray(np.asarray(factors, np.int16).reshape(6))
+    cf = np.zeros(400, np.int16)
+    fl = load().vo_reconstruct_inter_mb(ptr(src), ptr(rec), ptr(f), int(bool(split)), ptr(cf))
+    return rec, cf, fl
+
+
+def reconstruct_inter_frame(frame, refs, ref_ids, decisions, quant, out, mb_segment=None, segment_quant=None,
+                            segment_abs=False, full_pixel=False, filter_set=abi.FILTER_SIXTAP):
+    """pick_mb_for_ref's chosen-mode §18 + §14 step (trellis off) for a
+    frame into the MB-padded planes `out` in place. Returns
+    (coeffs (mb_rows*mb_cols, 400) int16, flags (mb_rows*mb_cols,) uint8,
+    number of MBs left untouched)."""
+    f = i420(*frame)
+    prs = [planes(*p) for p in refs]
+    parr = (abi.Planes * len(prs))(*prs)
+    ids = np.ascontiguousarray(np.asarray(ref_ids, np.uint8))
+    dec = np.ascontiguousarray(decisions).reshape(-1)
+    op = planes(*out)
+    n = op.mb_cols * op.mb_rows
+    cf = np.zeros((n, 400), np.int16)
+    fl = np.zeros(n, np.uint8)
+    seg = None if mb_segment is None else np.ascontiguousarray(np.asarray(mb_segment, np.int8).reshape(-1))
+    sq = None if segment_quant is None else np.ascontiguousarray(np.asarray(segment_quant, np.int16).reshape(4))
+    skipped = load().vo_reconstruct_inter_frame(C.byref(f), C.cast(parr, C.c_void_p), ptr(ids), len(prs), ptr(dec),
+                                                C.byref(quant), ptr(seg), ptr(sq), int(bool(segment_abs)),
+                                                int(bool(full_pixel)), filter_set, C.byref(op), ptr(cf), ptr(fl))
+    return cf, fl, skipped

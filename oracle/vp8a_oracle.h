@@ -152,6 +152,26 @@ int vo_predict_inter_frame(const vp8a_planes* refs, const uint8_t* ref_ids, uint
                            const vp8a_mb_decision* dec, int full_pixel, int filter_set,
                            vp8a_planes* out);
 
+/* ---- §14 inter reconstruction, trellis off (src/encoder.rs, src/dequant.rs,
+ * src/forward_transform.rs, src/inverse_transform.rs; recon.c) */
+void vo_dequant_factors(int32_t q, int32_t ydc, int32_t y2dc, int32_t y2ac, int32_t uvdc,
+                        int32_t uvac, int16_t* out);
+void vo_segment_factors(const vp8a_quant_indices* qi, int has_segment, int32_t segment_quant,
+                        int absolute, int16_t* out);
+void vo_forward_dct_4x4(const int16_t* in, int16_t* out);
+void vo_forward_wht_4x4(const int16_t* in, int16_t* out);
+void vo_inverse_dct_4x4(const int16_t* in, int16_t* out);
+void vo_inverse_wht_4x4(const int16_t* in, int16_t* out);
+void vo_enc_quantize_block(int16_t* blk, int16_t dc, int16_t ac);
+int vo_reconstruct_inter_mb(const uint8_t* src384, uint8_t* pred, const int16_t* f, int split,
+                            int16_t* coeffs);
+int vo_reconstruct_inter_frame(const vp8a_i420* frame, const vp8a_planes* refs,
+                               const uint8_t* ref_ids, uint32_t n_refs,
+                               const vp8a_mb_decision* dec, const vp8a_quant_indices* qi,
+                               const int8_t* mb_segment, const int16_t* segment_quant,
+                               int segment_abs, int full_pixel, int filter_set,
+                               vp8a_planes* out, int16_t* coeffs, uint8_t* flags);
+
 /* ---- threading helper */
 typedef void (*vo_task_fn)(void* arg, uint32_t index);
 void vo_parallel_for(uint32_t n, uint32_t threads, vo_task_fn fn, void* arg);

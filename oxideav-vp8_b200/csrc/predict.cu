@@ -551,32 +551,21 @@ vp8a_status predict_batch(vp8a_ctx* ctx, const vp8a_planes* ref, const uint32_t*
 
 }  // namespace
 
-extern "C" {
+namespace vp8a {
 
-vp8a_status vp8a_predict_inter_mb(vp8a_ctx* ctx, const vp8a_planes* ref, const uint32_t* mb_xy, const vp8a_mv* mvs,
-                                  uint32_t n, uint32_t full_pixel, uint32_t filter_set, uint8_t* out) {
-  return predict_batch(ctx, ref, mb_xy, mvs, n, full_pixel, filter_set, out, false);
-}
-
-vp8a_status vp8a_predict_split_mv(vp8a_ctx* ctx, const vp8a_planes* ref, const uint32_t* mb_xy,
-                                  const vp8a_mv* split_mvs, uint32_t n, uint32_t full_pixel, uint32_t filter_set,
-                                  uint8_t* out) {
-  return predict_batch(ctx, ref, mb_xy, split_mvs, n, full_pixel, filter_set, out, true);
-}
-
-vp8a_status vp8a_predict_inter_frame(vp8a_ctx* ctx, const vp8a_planes* refs, const uint8_t* ref_ids, uint32_t n_refs,
-                                     const vp8a_mb_decision* decisions, uint32_t full_pixel, uint32_t filter_set,
-                                     vp8a_planes* out) {
-  if (!ctx || !refs || !ref_ids || !decisions) {
-    vp8a::set_error("null argument");
+vp8a_status predict_frame(vp8a_ctx* ctx, Stager& st, const vp8a_planes* refs, const uint8_t* ref_ids,
+                          uint32_t n_refs, const vp8a_mb_decision* decisions, uint32_t full_pixel,
+                          uint32_t filter_set, const vp8a_planes* out, FramePrediction* fp) {
+  if (!refs || !ref_ids || !decisions) {
+    set_error("null argument");
     return VP8A_E_INVALID_ARGUMENT;
   }
   if (n_refs == 0 || n_refs > (uint32_t)MAX_PRED_REFS) {
-    vp8a::set_error("n_refs must be 1..3");
+    set_error("n_refs must be 1..3");
     return VP8A_E_INVALID_ARGUMENT;
   }
   if (filter_set > VP8A_FILTER_BILINEAR) {
-    vp8a::set_error("filter_set must be VP8A_FILTER_SIXTAP or VP8A_FILTER_BILINEAR");
+    set_error("filter_set must be VP8A_FILTER_SIXTAP or VP8A_FILTER_BILINEAR");
     return VP8A_E_INVALID_ARGUMENT;
   }
   vp8a_status s;
@@ -584,23 +573,21 @@ vp8a_status vp8a_predict_inter_frame(vp8a_ctx* ctx, const vp8a_planes* refs, con
   for (uint32_t k = 0; k < n_refs; k++) {
     if ((s = check_planes(&refs[k], "reference")) != VP8A_OK) return s;
     if (refs[k].mb_cols != out->mb_cols || refs[k].mb_rows != out->mb_rows) {
-      vp8a::set_error("reference planes do not match the output MB grid");
+      set_error("reference planes do not match the output MB grid");
       return VP8A_E_REFERENCE_DIMENSIONS_MISMATCH;
     }
   }
-  VP8A_CUDA(cudaSetDevice(ctx->device));
-  vp8a::Stager st(ctx);
   PredArgs a{};
-  uint8_t ids[MAX_PRED_REFS];
-  if ((s = st.read_to_host(ref_ids, n_refs, ids)) != VP8A_OK) return s;
+  if ((s = st.read_to_host(ref_ids, n_refs, fp->ref_ids)) != VP8A_OK) return s;
   for (uint32_t k = 0; k < n_refs; k++) {
-    if (ids[k] < VP8A_REF_LAST || ids[k] > VP8A_REF_ALTREF) {
-      vp8a::set_error("reference ids must be VP8A_REF_LAST, _GOLDEN or _ALTREF");
+    if (fp->ref_ids[k] < VP8A_REF_LAST || fp->ref_ids[k] > VP8A_REF_ALTREF) {
+      set_error("reference ids must be VP8A_REF_LAST, _GOLDEN or _ALTREF");
       return VP8A_E_INVALID_ARGUMENT;
     }
     if ((s = stage_ref(st, &refs[k], &a.refs[k])) != VP8A_OK) return s;
-    a.ref_ids[k] = ids[k];
+    a.ref_ids[k] = fp->ref_ids[k];
   }
+  fp->n_refs = n_refs;
   a.n_refs = (int)n_refs;
   a.aligned_src = 1;
   for (uint32_t k = 0; k < n_refs; k++) a.aligned_src &= src_aligned(a.refs[k]);
@@ -625,6 +612,41 @@ vp8a_status vp8a_predict_inter_frame(vp8a_ctx* ctx, const vp8a_planes* refs, con
   a.full_pixel = full_pixel != 0;
   a.filter_set = (int)filter_set;
   if ((s = launch<PRED_FRAME>(ctx, a)) != VP8A_OK) return s;
+  fp->dec = a.dec;
+  fp->planes = *out;
+  fp->planes.y = a.oy;
+  fp->planes.u = a.ou;
+  fp->planes.v = a.ov;
+  return VP8A_OK;
+}
+
+}  // namespace vp8a
+
+extern "C" {
+
+vp8a_status vp8a_predict_inter_mb(vp8a_ctx* ctx, const vp8a_planes* ref, const uint32_t* mb_xy, const vp8a_mv* mvs,
+                                  uint32_t n, uint32_t full_pixel, uint32_t filter_set, uint8_t* out) {
+  return predict_batch(ctx, ref, mb_xy, mvs, n, full_pixel, filter_set, out, false);
+}
+
+vp8a_status vp8a_predict_split_mv(vp8a_ctx* ctx, const vp8a_planes* ref, const uint32_t* mb_xy,
+                                  const vp8a_mv* split_mvs, uint32_t n, uint32_t full_pixel, uint32_t filter_set,
+                                  uint8_t* out) {
+  return predict_batch(ctx, ref, mb_xy, split_mvs, n, full_pixel, filter_set, out, true);
+}
+
+vp8a_status vp8a_predict_inter_frame(vp8a_ctx* ctx, const vp8a_planes* refs, const uint8_t* ref_ids, uint32_t n_refs,
+                                     const vp8a_mb_decision* decisions, uint32_t full_pixel, uint32_t filter_set,
+                                     vp8a_planes* out) {
+  if (!ctx) {
+    vp8a::set_error("null context");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  vp8a::FramePrediction fp;
+  vp8a_status s = vp8a::predict_frame(ctx, st, refs, ref_ids, n_refs, decisions, full_pixel, filter_set, out, &fp);
+  if (s != VP8A_OK) return s;
   return st.finish();
 }
 

@@ -1,0 +1,454 @@
+// recon.cu — the §14 inter reconstruction of the encoder's chosen mode
+// (trellis off) on the GPU:
+//   vp8a_reconstruct_inter_frame  (the §18 + §14 step of pick_mb_for_ref,
+//                                  src/encoder.rs:8704-8800, TrellisStrength::OFF)
+//   vp8a_dequant_factors          (MbDequantFactors, src/dequant.rs:118-230; host)
+//
+// The prediction is queued first (predict.cu) into the output planes; this
+// kernel then turns each MB's prediction into its reconstruction in place.
+// One warp per MB, one lane per 4x4 block: lanes 0-15 the luma blocks in
+// raster order, 16-19 U, 20-23 V, lane 24 the Y2 block of a non-SPLITMV MB.
+// A lane forms its block's residual against the source MB (edge-replicated
+// as I420Frame::extract_mb does), runs the forward DCT, hands its DC to lane
+// 24 for the forward WHT (non-SPLITMV), quantises with the plain rounding
+// quantiser, votes on the §11.1 skip decision, dequantises, takes its DC back
+// from lane 24's inverse WHT, runs the inverse DCT and adds onto the
+// prediction. All arithmetic is the reference's integer listing: the
+// forward transforms in int, the inverse DCT in wrapping 32-bit int.
+#include <algorithm>
+
+#include "vp8a_internal.cuh"
+
+namespace {
+
+constexpr int RC_WARPS = 4;
+constexpr int COS8 = 20091;  // sqrt(2) cos(pi/8) - 1, 16-bit fixed point
+constexpr int SIN8 = 35468;  // sqrt(2) sin(pi/8), 16-bit fixed point
+
+// §14.1 dc_qlookup / ac_qlookup (src/inverse_transform.rs:72-103).
+const int16_t DC_Q[128] = {
+    4,   5,   6,   7,   8,   9,   10,  10,  11,  12,  13,  14,  15,  16,  17,  17,  18,  19,  20,
+    20,  21,  21,  22,  22,  23,  23,  24,  25,  25,  26,  27,  28,  29,  30,  31,  32,  33,  34,
+    35,  36,  37,  37,  38,  39,  40,  41,  42,  43,  44,  45,  46,  46,  47,  48,  49,  50,  51,
+    52,  53,  54,  55,  56,  57,  58,  59,  60,  61,  62,  63,  64,  65,  66,  67,  68,  69,  70,
+    71,  72,  73,  74,  75,  76,  76,  77,  78,  79,  80,  81,  82,  83,  84,  85,  86,  87,  88,
+    89,  91,  93,  95,  96,  98,  100, 101, 102, 104, 106, 108, 110, 112, 114, 116, 118, 122, 124,
+    126, 128, 130, 132, 134, 136, 138, 140, 143, 145, 148, 151, 154, 157};
+const int16_t AC_Q[128] = {
+    4,   5,   6,   7,   8,   9,   10,  11,  12,  13,  14,  15,  16,  17,  18,  19,  20,  21,  22,
+    23,  24,  25,  26,  27,  28,  29,  30,  31,  32,  33,  34,  35,  36,  37,  38,  39,  40,  41,
+    42,  43,  44,  45,  46,  47,  48,  49,  50,  51,  52,  53,  54,  55,  56,  57,  58,  60,  62,
+    64,  66,  68,  70,  72,  74,  76,  78,  80,  82,  84,  86,  88,  90,  92,  94,  96,  98,  100,
+    102, 104, 106, 108, 110, 112, 114, 116, 119, 122, 125, 128, 131, 134, 137, 140, 143, 146, 149,
+    152, 155, 158, 161, 164, 167, 170, 173, 177, 181, 185, 189, 193, 197, 201, 205, 209, 213, 217,
+    221, 225, 229, 234, 239, 245, 249, 254, 259, 264, 269, 274, 279, 284};
+
+int qclamp(int64_t q) { return q < 0 ? 0 : (q > 127 ? 127 : (int)q); }
+int64_t sat32(int64_t v) { return std::max<int64_t>(INT32_MIN, std::min<int64_t>(INT32_MAX, v)); }
+
+// MbDequantFactors::from_base_and_deltas (src/dequant.rs:118-165).
+void factors_from(int64_t q, int ydc, int y2dc, int y2ac, int uvdc, int uvac, int16_t* out) {
+  int y2_ac = AC_Q[qclamp(sat32(q + y2ac))] * 155 / 100;
+  int uv_dc = DC_Q[qclamp(sat32(q + uvdc))];
+  out[0] = DC_Q[qclamp(sat32(q + ydc))];
+  out[1] = AC_Q[qclamp(q)];
+  out[2] = (int16_t)(DC_Q[qclamp(sat32(q + y2dc))] * 2);
+  out[3] = (int16_t)(y2_ac < 8 ? 8 : y2_ac);
+  out[4] = (int16_t)(uv_dc > 132 ? 132 : uv_dc);
+  out[5] = AC_Q[qclamp(sat32(q + uvac))];
+}
+
+struct RcArgs {
+  const uint8_t *fy, *fu, *fv;  // visible source
+  uint64_t fys, fuvs;
+  int fw, fh, fcw, fch;
+  uint8_t *ry, *ru, *rv;  // MB-padded planes: prediction in, reconstruction out
+  uint64_t rys, ruvs;
+  int aligned;  // recon plane bases and pitches are 4-byte aligned
+  int mb_cols;
+  uint32_t n;
+  const vp8a_mb_decision* dec;
+  uint8_t ref_ids[3];
+  int n_refs;
+  const int8_t* mb_segment;
+  int16_t f[5][6];  // frame factors, then segments 0..3
+  int16_t* coeffs;
+  uint8_t* flags;
+};
+
+__device__ __forceinline__ int cmul(int i) { return i + ((i * COS8) >> 16); }
+__device__ __forceinline__ int smul(int i) { return (i * SIN8) >> 16; }
+__device__ __forceinline__ int rdiv2(int v) {
+  const int r = v >= 0 ? (v + 1) >> 1 : -((-v + 1) >> 1);
+  return r < -32768 ? -32768 : (r > 32767 ? 32767 : r);
+}
+__device__ __forceinline__ int to16(int v) { return (int)(short)v; }
+
+// forward_dct_4x4_scalar (src/forward_transform.rs:486-604), in place.
+__device__ __forceinline__ void fdct4x4(int* b) {
+  int t[16];
+#pragma unroll
+  for (int col = 0; col < 4; col++) {
+    const int i0 = b[col], i4 = b[4 + col], i8 = b[8 + col], i12 = b[12 + col];
+    t[col] = (i0 + i12) + (i4 + i8);
+    t[4 + col] = (cmul(i0) - cmul(i12)) + (smul(i4) - smul(i8));
+    t[8 + col] = (i0 + i12) - (i4 + i8);
+    t[12 + col] = (smul(i0) - smul(i12)) - (cmul(i4) - cmul(i8));
+  }
+#pragma unroll
+  for (int row = 0; row < 4; row++) {
+    const int r0 = t[4 * row], r1 = t[4 * row + 1], r2 = t[4 * row + 2], r3 = t[4 * row + 3];
+    b[4 * row] = rdiv2((r0 + r3) + (r1 + r2));
+    b[4 * row + 1] = rdiv2((cmul(r0) - cmul(r3)) + (smul(r1) - smul(r2)));
+    b[4 * row + 2] = rdiv2((r0 + r3) - (r1 + r2));
+    b[4 * row + 3] = rdiv2((smul(r0) - smul(r3)) - (cmul(r1) - cmul(r2)));
+  }
+}
+
+// forward_wht_4x4_scalar (src/forward_transform.rs:173-260), in place.
+__device__ __forceinline__ void fwht4x4(int* b) {
+  int t[16];
+#pragma unroll
+  for (int col = 0; col < 4; col++) {
+    const int a1 = b[col] + b[12 + col], b1 = b[4 + col] + b[8 + col];
+    const int c1 = b[4 + col] - b[8 + col], d1 = b[col] - b[12 + col];
+    t[col] = a1 + b1;
+    t[4 + col] = c1 + d1;
+    t[8 + col] = a1 - b1;
+    t[12 + col] = d1 - c1;
+  }
+#pragma unroll
+  for (int row = 0; row < 4; row++) {
+    const int a1 = t[4 * row] + t[4 * row + 3], b1 = t[4 * row + 1] + t[4 * row + 2];
+    const int c1 = t[4 * row + 1] - t[4 * row + 2], d1 = t[4 * row] - t[4 * row + 3];
+    b[4 * row] = rdiv2(a1 + b1);
+    b[4 * row + 1] = rdiv2(c1 + d1);
+    b[4 * row + 2] = rdiv2(a1 - b1);
+    b[4 * row + 3] = rdiv2(d1 - c1);
+  }
+}
+
+// inverse_wht_4x4_scalar (src/inverse_transform.rs:190-252), in place.
+__device__ __forceinline__ void iwht4x4(int* b) {
+  int t[16];
+#pragma unroll
+  for (int col = 0; col < 4; col++) {
+    const int a1 = b[col] + b[12 + col], b1 = b[4 + col] + b[8 + col];
+    const int c1 = b[4 + col] - b[8 + col], d1 = b[col] - b[12 + col];
+    t[col] = a1 + b1;
+    t[4 + col] = c1 + d1;
+    t[8 + col] = a1 - b1;
+    t[12 + col] = d1 - c1;
+  }
+#pragma unroll
+  for (int row = 0; row < 4; row++) {
+    const int a1 = t[4 * row] + t[4 * row + 3], b1 = t[4 * row + 1] + t[4 * row + 2];
+    const int c1 = t[4 * row + 1] - t[4 * row + 2], d1 = t[4 * row] - t[4 * row + 3];
+    b[4 * row] = to16((a1 + b1 + 3) >> 3);
+    b[4 * row + 1] = to16((c1 + d1 + 3) >> 3);
+    b[4 * row + 2] = to16((a1 - b1 + 3) >> 3);
+    b[4 * row + 3] = to16((d1 - c1 + 3) >> 3);
+  }
+}
+
+// Two's-complement 32-bit arithmetic (the reference's wrapping_* ops).
+__device__ __forceinline__ int wa(int a, int b) { return (int)((unsigned)a + (unsigned)b); }
+__device__ __forceinline__ int ws(int a, int b) { return (int)((unsigned)a - (unsigned)b); }
+__device__ __forceinline__ int wm(int a, int b) { return (int)((unsigned)a * (unsigned)b); }
+
+// inverse_dct_4x4_scalar (src/inverse_transform.rs:609-712), in place.
+__device__ __forceinline__ void idct4x4(int* b) {
+  int t[16];
+#pragma unroll
+  for (int col = 0; col < 4; col++) {
+    const int i0 = b[col], i4 = b[4 + col], i8 = b[8 + col], i12 = b[12 + col];
+    const int a1 = wa(i0, i8), b1 = ws(i0, i8);
+    const int c1 = ws(wm(i4, SIN8) >> 16, wa(i12, wm(i12, COS8) >> 16));
+    const int d1 = wa(wa(i4, wm(i4, COS8) >> 16), wm(i12, SIN8) >> 16);
+    t[col] = wa(a1, d1);
+    t[12 + col] = ws(a1, d1);
+    t[4 + col] = wa(b1, c1);
+    t[8 + col] = ws(b1, c1);
+  }
+#pragma unroll
+  for (int row = 0; row < 4; row++) {
+    const int r0 = t[4 * row], r1 = t[4 * row + 1], r2 = t[4 * row + 2], r3 = t[4 * row + 3];
+    const int a1 = wa(r0, r2), b1 = ws(r0, r2);
+    const int c1 = ws(wm(r1, SIN8) >> 16, wa(r3, wm(r3, COS8) >> 16));
+    const int d1 = wa(wa(r1, wm(r1, COS8) >> 16), wm(r3, SIN8) >> 16);
+    b[4 * row] = to16(wa(wa(a1, d1), 4) >> 3);
+    b[4 * row + 3] = to16(wa(ws(a1, d1), 4) >> 3);
+    b[4 * row + 1] = to16(wa(wa(b1, c1), 4) >> 3);
+    b[4 * row + 2] = to16(wa(ws(b1, c1), 4) >> 3);
+  }
+}
+
+// enc_round_div (src/encoder.rs:2112): round half away from zero, as i16.
+__device__ __forceinline__ int rdiv(int num, int den) {
+  const int r = num >= 0 ? (num + den / 2) / den : -(((-num) + den / 2) / den);
+  return to16(r);
+}
+
+__global__ void __launch_bounds__(RC_WARPS * 32) recon_kernel(RcArgs a) {
+  const int lane = threadIdx.x & 31;
+  const unsigned full = 0xffffffffu;
+  for (uint32_t item = blockIdx.x * RC_WARPS + (threadIdx.x >> 5); item < a.n; item += gridDim.x * RC_WARPS) {
+    const vp8a_mb_decision& d = a.dec[item];
+    bool have = false;
+    for (int k = 0; k < a.n_refs; k++) have |= d.ref_frame != VP8A_REF_INTRA && a.ref_ids[k] == d.ref_frame;
+    if (!have) {  // warp-uniform: no inter reference, no reconstruction
+      if (a.flags && lane == 0) a.flags[item] = 0;
+      if (a.coeffs && lane < 25) {
+        int16_t* dst = a.coeffs + (size_t)item * 400 + (lane == 24 ? 0 : 16 + 16 * lane);
+#pragma unroll
+        for (int k = 0; k < 16; k += 2) *reinterpret_cast<uint32_t*>(dst + k) = 0u;
+      }
+      continue;
+    }
+    const bool split = d.mode == VP8A_MODE_SPLIT;
+    const int seg = a.mb_segment ? a.mb_segment[item] : -1;
+    const int16_t* f = a.f[(seg >= 0 && seg < 4) ? 1 + seg : 0];
+    const int mbx = (int)(item % (uint32_t)a.mb_cols), mby = (int)(item / (uint32_t)a.mb_cols);
+
+    // This lane's block: plane, top-left pixel in the plane.
+    const bool luma = lane < 16, chroma = lane >= 16 && lane < 24;
+    const int cb = (lane - 16) & 3;
+    int px = 0, py = 0;
+    uint8_t* rp = nullptr;
+    uint64_t rs = 0;
+    const uint8_t* sp = nullptr;
+    uint64_t ss = 0;
+    int sw = 1, sh = 1;
+    if (luma) {
+      px = mbx * 16 + 4 * (lane & 3);
+      py = mby * 16 + 4 * (lane >> 2);
+      rp = a.ry;
+      rs = a.rys;
+      sp = a.fy;
+      ss = a.fys;
+      sw = a.fw;
+      sh = a.fh;
+    } else if (chroma) {
+      px = mbx * 8 + 4 * (cb & 1);
+      py = mby * 8 + 4 * (cb >> 1);
+      rp = lane < 20 ? a.ru : a.rv;
+      rs = a.ruvs;
+      sp = lane < 20 ? a.fu : a.fv;
+      ss = a.fuvs;
+      sw = a.fcw;
+      sh = a.fch;
+    }
+    int blk[16];
+    uint8_t pred[16];
+    if (luma || chroma) {
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        const uint8_t* prow = rp + (uint64_t)(py + r) * rs + px;
+        if (a.aligned) {
+          const uint32_t w = *reinterpret_cast<const uint32_t*>(prow);
+#pragma unroll
+          for (int c = 0; c < 4; c++) pred[4 * r + c] = (uint8_t)(w >> (8 * c));
+        } else {
+#pragma unroll
+          for (int c = 0; c < 4; c++) pred[4 * r + c] = prow[c];
+        }
+        const int sy = min(py + r, sh - 1);
+        const uint8_t* srow = sp + (uint64_t)sy * ss;
+#pragma unroll
+        for (int c = 0; c < 4; c++) blk[4 * r + c] = (int)__ldg(srow + min(px + c, sw - 1)) - (int)pred[4 * r + c];
+      }
+      fdct4x4(blk);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; k++) blk[k] = 0;
+    }
+
+    // Y2: lane 24 collects the sixteen luma DCs (non-SPLITMV).
+    if (!split) {
+#pragma unroll
+      for (int k = 0; k < 16; k++) {
+        const int v = __shfl_sync(full, blk[0], k);
+        if (lane == 24) blk[k] = v;
+      }
+      if (lane == 24) fwht4x4(blk);
+      if (luma) blk[0] = 0;
+    }
+    // Plain quantisation (enc_quantize_block) with this block's factors.
+    int qdc = f[0], qac = f[1];
+    if (lane == 24) {
+      qdc = f[2];
+      qac = f[3];
+    } else if (chroma) {
+      qdc = f[4];
+      qac = f[5];
+    }
+    const bool active = luma || chroma || (lane == 24 && !split);
+    int nz = 0;
+    if (active) {
+      blk[0] = rdiv(blk[0], qdc);
+#pragma unroll
+      for (int k = 1; k < 16; k++) blk[k] = rdiv(blk[k], qac);
+#pragma unroll
+      for (int k = 0; k < 16; k++) nz |= blk[k];
+    }
+    // §11.1 skip: no non-zero coefficient in Y2, the Y blocks (from index 1
+    // with Y2; their DC is already 0) or the chroma blocks.
+    const bool skip = !__any_sync(full, nz != 0);
+    if (a.coeffs && (active || lane == 24)) {
+      // MbCoeffs order: y2, y[16], u[4], v[4].
+      const int off = lane == 24 ? 0 : (luma ? 16 + 16 * lane : 272 + 16 * (lane - 16));
+      int16_t* dst = a.coeffs + (size_t)item * 400 + off;
+#pragma unroll
+      for (int k = 0; k < 16; k += 2)
+        *reinterpret_cast<uint32_t*>(dst + k) = (uint32_t)(uint16_t)blk[k] | ((uint32_t)(uint16_t)blk[k + 1] << 16);
+    }
+    // Dequantise (dequant_block: (c * factor) as i16).
+    int dnz = 0;
+    if (active) {
+      blk[0] = to16(blk[0] * qdc);
+#pragma unroll
+      for (int k = 1; k < 16; k++) blk[k] = to16(blk[k] * qac);
+#pragma unroll
+      for (int k = 0; k < 16; k++) dnz |= blk[k];
+    }
+    const bool has = __any_sync(full, dnz != 0);
+    if (a.flags && lane == 0) a.flags[item] = (uint8_t)((skip ? VP8A_MB_SKIP : 0) | (has ? VP8A_MB_HAS_COEFFS : 0));
+    if (skip) continue;  // warp-uniform: the reconstruction is the prediction
+    if (!split) {
+      if (lane == 24) iwht4x4(blk);
+#pragma unroll
+      for (int k = 0; k < 16; k++) {
+        const int v = __shfl_sync(full, blk[k], 24);
+        if (lane == k) blk[0] = v;
+      }
+    }
+    if (luma || chroma) {
+      idct4x4(blk);
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        uint8_t* prow = rp + (uint64_t)(py + r) * rs + px;
+        uint32_t w = 0;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+          const int v = (int)pred[4 * r + c] + blk[4 * r + c];
+          w |= (uint32_t)(v < 0 ? 0 : (v > 255 ? 255 : v)) << (8 * c);
+        }
+        if (a.aligned) {
+          *reinterpret_cast<uint32_t*>(prow) = w;
+        } else {
+#pragma unroll
+          for (int c = 0; c < 4; c++) prow[c] = (uint8_t)(w >> (8 * c));
+        }
+      }
+    }
+  }
+}
+
+int g_rc_blocks_per_sm = 0;
+
+}  // namespace
+
+extern "C" {
+
+void vp8a_dequant_factors(const vp8a_quant_indices* qi, uint32_t has_segment, int32_t segment_quant,
+                          uint32_t absolute, int16_t* out) {
+  if (!qi || !out) return;
+  int64_t q = qi->y_ac_qi;
+  if (has_segment) q = absolute ? (int64_t)segment_quant : sat32((int64_t)qi->y_ac_qi + segment_quant);
+  factors_from(q, qi->y_dc_delta, qi->y2_dc_delta, qi->y2_ac_delta, qi->uv_dc_delta, qi->uv_ac_delta, out);
+}
+
+vp8a_status vp8a_reconstruct_inter_frame(vp8a_ctx* ctx, const vp8a_i420* frame, const vp8a_planes* refs,
+                                         const uint8_t* ref_ids, uint32_t n_refs, const vp8a_mb_decision* decisions,
+                                         const vp8a_quant_indices* quant, const int8_t* mb_segment,
+                                         const int16_t* segment_quant, uint32_t segment_abs, uint32_t full_pixel,
+                                         uint32_t filter_set, vp8a_planes* recon, int16_t* coeffs,
+                                         uint8_t* mb_flags) {
+  if (!ctx || !frame || !quant || !recon) {
+    vp8a::set_error("null argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (frame->width == 0 || frame->height == 0 || frame->width > 0x3FFF || frame->height > 0x3FFF) {
+    vp8a::set_error("invalid dimensions");
+    return VP8A_E_INVALID_DIMENSIONS;
+  }
+  if (quant->y_ac_qi > 127) {
+    vp8a::set_error("y_ac_qi must be 0..=127");
+    return VP8A_E_QUANT_INDEX_OUT_OF_RANGE;
+  }
+  if (!frame->y || !frame->u || !frame->v || frame->y_stride < frame->width ||
+      frame->uv_stride < (frame->width + 1) / 2) {
+    vp8a::set_error("bad source plane");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (recon->mb_cols != (frame->width + 15) / 16 || recon->mb_rows != (frame->height + 15) / 16) {
+    vp8a::set_error("reconstruction planes do not match the frame's MB grid");
+    return VP8A_E_REFERENCE_DIMENSIONS_MISMATCH;
+  }
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  vp8a::FramePrediction fp;
+  vp8a_status s = vp8a::predict_frame(ctx, st, refs, ref_ids, n_refs, decisions, full_pixel, filter_set, recon, &fp);
+  if (s != VP8A_OK) return s;
+
+  RcArgs a{};
+  const size_t cw = (frame->width + 1) / 2, ch = (frame->height + 1) / 2;
+  const void* d;
+  if ((s = st.in(frame->y, frame->y_stride * (size_t)(frame->height - 1) + frame->width, &d)) != VP8A_OK) return s;
+  a.fy = (const uint8_t*)d;
+  if ((s = st.in(frame->u, frame->uv_stride * (ch - 1) + cw, &d)) != VP8A_OK) return s;
+  a.fu = (const uint8_t*)d;
+  if ((s = st.in(frame->v, frame->uv_stride * (ch - 1) + cw, &d)) != VP8A_OK) return s;
+  a.fv = (const uint8_t*)d;
+  a.fys = frame->y_stride;
+  a.fuvs = frame->uv_stride;
+  a.fw = (int)frame->width;
+  a.fh = (int)frame->height;
+  a.fcw = (int)cw;
+  a.fch = (int)ch;
+  a.ry = fp.planes.y;
+  a.ru = fp.planes.u;
+  a.rv = fp.planes.v;
+  a.rys = fp.planes.y_stride;
+  a.ruvs = fp.planes.uv_stride;
+  a.aligned = (((uintptr_t)a.ry | (uintptr_t)a.ru | (uintptr_t)a.rv | a.rys | a.ruvs) & 3) == 0;
+  a.mb_cols = (int)recon->mb_cols;
+  a.n = recon->mb_cols * recon->mb_rows;
+  a.dec = fp.dec;
+  for (uint32_t k = 0; k < fp.n_refs; k++) a.ref_ids[k] = fp.ref_ids[k];
+  a.n_refs = (int)fp.n_refs;
+  int16_t sq[4] = {0, 0, 0, 0};
+  if (segment_quant && (s = st.read_to_host(segment_quant, sizeof sq, sq)) != VP8A_OK) return s;
+  vp8a_dequant_factors(quant, 0, 0, 0, a.f[0]);
+  for (int k = 0; k < 4; k++) vp8a_dequant_factors(quant, 1, sq[k], segment_abs, a.f[1 + k]);
+  if (mb_segment) {
+    if ((s = st.in(mb_segment, a.n, &d)) != VP8A_OK) return s;
+    a.mb_segment = (const int8_t*)d;
+  }
+  void* o;
+  if (coeffs) {
+    if ((s = st.out(coeffs, (size_t)a.n * 400 * sizeof(int16_t), &o)) != VP8A_OK) return s;
+    if (((uintptr_t)o & 3) != 0) {
+      vp8a::set_error("coeffs must be 4-byte aligned");
+      return VP8A_E_INVALID_ARGUMENT;
+    }
+    a.coeffs = (int16_t*)o;
+  }
+  if (mb_flags) {
+    if ((s = st.out(mb_flags, a.n, &o)) != VP8A_OK) return s;
+    a.flags = (uint8_t*)o;
+  }
+  if (!g_rc_blocks_per_sm) {
+    int b = 0;
+    VP8A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, recon_kernel, RC_WARPS * 32, 0));
+    g_rc_blocks_per_sm = std::max(b, 1);
+  }
+  const unsigned grid = (unsigned)std::min<size_t>((a.n + RC_WARPS - 1) / RC_WARPS,
+                                                   (size_t)ctx->sm_count * g_rc_blocks_per_sm);
+  recon_kernel<<<grid, RC_WARPS * 32, 0, ctx->stream>>>(a);
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
+  return st.finish();
+}
+
+}  // extern "C"

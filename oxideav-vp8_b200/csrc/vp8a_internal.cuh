@@ -84,6 +84,22 @@ inline unsigned grid_for(size_t n, unsigned block) {
 // Reads the device status word after the call's kernels and maps it.
 vp8a_status check_device_status(vp8a_ctx* ctx);
 
+// Device views left by predict_frame: the staged decisions and the output
+// planes (device pointers) now holding the prediction, plus the host copy of
+// the reference ids.
+struct FramePrediction {
+  const vp8a_mb_decision* dec = nullptr;
+  vp8a_planes planes{};
+  uint8_t ref_ids[3] = {0, 0, 0};
+  uint32_t n_refs = 0;
+};
+
+// Validates and stages the arguments of vp8a_predict_inter_frame through
+// `st` and queues the per-MB §18 prediction into `out` (predict.cu).
+vp8a_status predict_frame(vp8a_ctx* ctx, Stager& st, const vp8a_planes* refs, const uint8_t* ref_ids,
+                          uint32_t n_refs, const vp8a_mb_decision* decisions, uint32_t full_pixel,
+                          uint32_t filter_set, const vp8a_planes* out, FramePrediction* fp);
+
 }  // namespace vp8a
 
 // ------------------------------------------------------------ device helpers

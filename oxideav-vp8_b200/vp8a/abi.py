@@ -104,6 +104,21 @@ class FilterConfig(C.Structure):
     ]
 
 
+class QuantIndices(C.Structure):
+    """vp8a_quant_indices (QuantIndices, src/coded_header.rs:171); 0 = no delta."""
+
+    _fields_ = [("y_ac_qi", C.c_uint8), ("y_dc_delta", C.c_int8), ("y2_dc_delta", C.c_int8),
+                ("y2_ac_delta", C.c_int8), ("uv_dc_delta", C.c_int8), ("uv_ac_delta", C.c_int8),
+                ("reserved", C.c_uint8 * 2)]
+
+
+def quant_indices(y_ac_qi, y_dc=0, y2_dc=0, y2_ac=0, uv_dc=0, uv_ac=0):
+    return QuantIndices(y_ac_qi, y_dc, y2_dc, y2_ac, uv_dc, uv_ac)
+
+
+MB_SKIP, MB_HAS_COEFFS = 1, 2
+
+
 class Source(C.Structure):
     _fields_ = [
         ("width", C.c_uint32),
@@ -201,6 +216,7 @@ C_SIZES = {
     "vp8a_source": 48,
     "vp8a_mb_info": 72,
     "vp8a_rd_inter": 56,
+    "vp8a_quant_indices": 8,
 }
 
 
@@ -220,6 +236,7 @@ def check_layouts():
         "vp8a_source": C.sizeof(Source),
         "vp8a_mb_info": MB_INFO_DTYPE.itemsize,
         "vp8a_rd_inter": RD_INTER_DTYPE.itemsize,
+        "vp8a_quant_indices": C.sizeof(QuantIndices),
     }
     assert got == C_SIZES, (got, C_SIZES)
     return got

@@ -244,6 +244,43 @@ def predict_inter_frame(ctx, refs, ref_ids, decisions, out, full_pixel=False, fi
     return out
 
 
+def dequant_factors(quant, segment_quant=None, absolute=False):
+    """MbDequantFactors::from_quant_indices / for_segment (src/dequant.rs:169,
+    :201): (y1_dc, y1_ac, y2_dc, y2_ac, uv_dc, uv_ac)."""
+    out = np.zeros(6, np.int16)
+    load().vp8a_dequant_factors(C.byref(quant), segment_quant is not None, segment_quant or 0, int(bool(absolute)),
+                                ptr(out))
+    return tuple(int(x) for x in out)
+
+
+def reconstruct_inter_frame(ctx, frame, refs, ref_ids, decisions, quant, recon, mb_segment=None,
+                            segment_quant=None, segment_abs=False, full_pixel=False, filter_set=abi.FILTER_SIXTAP,
+                            coeffs=True, flags=True):
+    """pick_mb_for_ref's §18 prediction + §14 transform / quantise /
+    reconstruct for every MB's chosen mode with the trellis off
+    (src/encoder.rs:8704-8800). `frame` = visible (y, u, v); `recon` =
+    MB-padded (y, u, v) written in place; `quant` an abi.QuantIndices.
+    Returns (coeffs (n_mbs, 400) int16 in MbCoeffs order or None,
+    flags (n_mbs,) uint8 of abi.MB_SKIP | abi.MB_HAS_COEFFS or None)."""
+    f = i420(*frame)
+    prs = [planes(*p) for p in refs]
+    parr = (abi.Planes * len(prs))(*prs)
+    ids = np.ascontiguousarray(np.asarray(ref_ids, np.uint8))
+    dec = _contig(decisions)
+    op = planes(*recon)
+    n = op.mb_cols * op.mb_rows
+    cf = np.zeros((n, 400), np.int16) if coeffs is True else coeffs
+    fl = np.zeros(n, np.uint8) if flags is True else flags
+    seg = None if mb_segment is None else _contig(mb_segment if hasattr(mb_segment, "data_ptr")
+                                                  else np.asarray(mb_segment, np.int8))
+    sq = None if segment_quant is None else np.ascontiguousarray(np.asarray(segment_quant, np.int16).reshape(4))
+    check(ctx._lib.vp8a_reconstruct_inter_frame(ctx.handle, C.byref(f), C.cast(parr, C.c_void_p), ptr(ids), len(prs),
+                                                ptr(dec), C.byref(quant), ptr(seg), ptr(sq), int(bool(segment_abs)),
+                                                int(bool(full_pixel)), filter_set, C.byref(op), ptr(cf), ptr(fl)),
+          "vp8a_reconstruct_inter_frame")
+    return cf, fl
+
+
 def build_arnr_altref(ctx, frames, center, strength=3):
     """build_arnr_altref (src/arnr.rs:476). `frames` = list of (y, u, v).
     Returns the packed (y, u, v) anchor."""

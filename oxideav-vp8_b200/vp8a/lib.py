@@ -40,6 +40,12 @@ PROTOTYPES = {
     "vp8a_predict_inter_mb": (C.c_int, [P, C.POINTER(abi.Planes), P, P, U32, U32, U32, P]),
     "vp8a_predict_split_mv": (C.c_int, [P, C.POINTER(abi.Planes), P, P, U32, U32, U32, P]),
     "vp8a_predict_inter_frame": (C.c_int, [P, P, P, U32, P, U32, U32, C.POINTER(abi.Planes)]),
+    "vp8a_dequant_factors": (None, [C.POINTER(abi.QuantIndices), U32, C.c_int32, U32, P]),
+    "vp8a_reconstruct_inter_frame": (
+        C.c_int,
+        [P, C.POINTER(abi.I420), P, P, U32, P, C.POINTER(abi.QuantIndices), P, P, U32, U32, U32,
+         C.POINTER(abi.Planes), P, P],
+    ),
     "vp8a_build_arnr_altref": (C.c_int, [P, P, U32, U32, U32, P, P, P]),
     "vp8a_filter_frame": (C.c_int, [P, C.POINTER(abi.Planes), P, C.POINTER(abi.FilterConfig)]),
     "vp8a_reconstruction_ssd": (C.c_int, [P, C.POINTER(abi.Planes), C.POINTER(abi.Source), P]),

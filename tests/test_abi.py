@@ -59,3 +59,12 @@ def test_key_frame_sampling_helper(oracle):
     # FilterSampling::for_key_frame, host-side in the library.
     for mb_rows in list(range(1, 300)) + [4096]:
         assert vp8a.key_frame_sampling(mb_rows) == oracle.key_frame_sampling(mb_rows), mb_rows
+
+
+def test_dequant_factors_helper(oracle):
+    # MbDequantFactors::from_quant_indices / for_segment, host-side in the library.
+    for qi in (abi.quant_indices(44, y_dc=-3, y2_dc=5, y2_ac=-7, uv_dc=9, uv_ac=-2), abi.quant_indices(0),
+               abi.quant_indices(127, y_dc=15, uv_dc=-15)):
+        assert vp8a.dequant_factors(qi) == oracle.segment_factors(qi)
+        for sq, absolute in ((15, False), (-60, False), (100, True), (2**31 - 1, False), (-2**31, True)):
+            assert vp8a.dequant_factors(qi, sq, absolute) == oracle.segment_factors(qi, sq, absolute)
