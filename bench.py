@@ -8,10 +8,13 @@ Workload (one step = one 1920x1080 P frame, synthetic seeded I420 input):
   2. exhaustive inter analysis of the frame against LAST (k-1), GOLDEN
      (k-8) and ALTREF (the fresh anchor, edge-padded) with full sub-pel
      search and SPLITMV per MB per reference (vp8a_analyse_inter_frame);
-  3. the loop-filter sweep over all 64 levels x 8 sharpness values of a
-     qi-44-style reconstruction, SSD vs source per candidate
-     (vp8a_filter_sweep), and the reference's (level, sharpness) walk.
-Metric: 1080p macroblocks per second through those three stages.
+  3. the prediction, transform, quantisation (qi 44, trellis off) and
+     reconstruction of every MB's chosen mode, with its loop-filter side
+     information (vp8a_reconstruct_inter_frame);
+  4. the loop-filter sweep over all 64 levels x 8 sharpness values of that
+     reconstruction, SSD vs source per candidate (vp8a_filter_sweep), and
+     the reference's (level, sharpness) walk.
+Metric: 1080p macroblocks per second through those stages.
 
 `value` times the step with every input resident in HBM (device pointers);
 `e2e` times the same step through the C ABI with pinned host buffers, the
@@ -43,7 +46,8 @@ LOOKAHEAD = 7
 QI = 44
 SEED = 20261203
 METRIC = "1080p MBs/s (ME+ARNR+LF search)"
-WORKLOAD = "1080p P frame: ARNR(7, centre) + exhaustive ME/SPLITMV vs LAST/GOLDEN/ALTREF + LF 64x8 sweep"
+WORKLOAD = ("1080p P frame: ARNR(7, centre) + exhaustive ME/SPLITMV vs LAST/GOLDEN/ALTREF + qi-44 reconstruction "
+            "+ LF 64x8 sweep")
 
 
 def log(*a):
@@ -177,7 +181,7 @@ class GpuStep:
 
     def __init__(self, ctx, frames, lib, torch, device):
         import vp8a
-        from vp8a import abi, synth
+        from vp8a import abi
 
         self.vp8a, self.abi, self.lib, self.torch, self.ctx = vp8a, abi, lib, torch, ctx
         dev = torch.device("cuda", device)
@@ -192,9 +196,11 @@ class GpuStep:
         self.alt = [torch.zeros((MB_ROWS * 16, MB_COLS * 16), dtype=torch.uint8, device=dev),
                     torch.zeros((MB_ROWS * 8, MB_COLS * 8), dtype=torch.uint8, device=dev),
                     torch.zeros((MB_ROWS * 8, MB_COLS * 8), dtype=torch.uint8, device=dev)]
-        recon, has = synth.quantised_recon(pad_planes(cur))
-        self.recon = [t(p) for p in recon]
-        self.has = has
+        # The chosen modes' reconstruction (and the MBs' loop-filter side
+        # information) are rebuilt every step by run_recon.
+        self.recon = [torch.zeros_like(p) for p in self.last]
+        self.mbs = torch.zeros(N_MB * abi.MB_LF_INFO_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+        self.quant = abi.quant_indices(QI)
         self.dec = torch.zeros(N_MB * abi.MB_DECISION_DTYPE.itemsize, dtype=torch.uint8, device=dev)
         self.table = torch.zeros(512, dtype=torch.int64, device=dev)
         self.lam = vp8a.rd_lambda(QI)
@@ -209,7 +215,6 @@ class GpuStep:
         torch.cuda.synchronize(dev)
         dec = np.frombuffer(self.dec.cpu().numpy().tobytes(), abi.MB_DECISION_DTYPE)
         self.decisions = dec
-        self.mbs = t(vp8a.lf_info_from_decisions(dec, has).view(np.uint8))
         torch.cuda.synchronize(dev)
         self.i420_window = (abi.I420 * LOOKAHEAD)(*[vp8a.i420(*f) for f in self.window])
         self.i420_cur = vp8a.i420(*self.cur)
@@ -221,6 +226,8 @@ class GpuStep:
         self.pred = [torch.zeros_like(p) for p in self.last]
         self.pred_planes = vp8a.planes(*self.pred)
         self.host_ids = np.array([1, 2, 3], np.uint8)
+        self.run_recon()
+        ctx.synchronize()
 
     def run_arnr(self):
         v = self.vp8a
@@ -259,9 +266,17 @@ class GpuStep:
                                                self.abi.FILTER_SIXTAP, C.byref(self.pred_planes))
         assert st == 0, self.vp8a.load().vp8a_last_error()
 
+    def run_recon(self):
+        st = self.lib.vp8a_reconstruct_inter_frame(self.ctx.handle, C.byref(self.i420_cur), C.cast(self.planes, C.c_void_p),
+                                                   self.host_ids.ctypes.data, 3, self.dec.data_ptr(),
+                                                   C.byref(self.quant), None, None, 0, 0, self.abi.FILTER_SIXTAP,
+                                                   C.byref(self.recon_planes), None, None, self.mbs.data_ptr())
+        assert st == 0, self.vp8a.load().vp8a_last_error()
+
     def step(self):
         self.run_arnr()
         self.run_analysis()
+        self.run_recon()
         return self.run_lf()
 
 
@@ -302,11 +317,18 @@ class HostStep:
         self.table = torch.zeros(512, dtype=torch.int64).pin_memory()
         self.ids = np.array([1, 2, 3], np.uint8)
         nb = lambda ts: sum(x.numel() * x.element_size() for x in ts)  # noqa: E731
-        # Bytes the library copies in per step (what each call stages).
+        # Bytes the library copies in and out per step (what each call stages):
+        # ARNR window in, anchor out; analysis luma in, decisions out;
+        # reconstruction source + references + decisions + recon/LF-info
+        # (in/out) in, recon + LF info out; LF sweep recon + info + source in,
+        # table out.
+        refs = nb(self.last) + nb(self.golden) + nb(self.alt)
         self.h2d = (sum(nb(f) for f in self.window) + self.cur[0].numel() + self.last[0].numel() +
-                    self.golden[0].numel() + self.alt[0].numel() + nb(self.recon) + nb([self.mbs]) + nb(self.cur))
+                    self.golden[0].numel() + self.alt[0].numel() +
+                    nb(self.cur) + refs + nb([self.dec]) + nb(self.recon) + nb([self.mbs]) +
+                    nb(self.recon) + nb([self.mbs]) + nb(self.cur))
         self.d2h = nb(self.alt) - (self.alt[0][H:].numel() + 2 * self.alt[1][(H + 1) // 2:].numel()) + \
-            nb([self.dec]) + nb([self.table])
+            nb([self.dec]) + nb(self.recon) + nb([self.mbs]) + nb([self.table])
 
     def step(self):
         gs, v, abi, lib = self.gs, self.gs.vp8a, self.gs.abi, self.gs.lib
@@ -325,6 +347,10 @@ class HostStep:
                                           None)
         assert st == 0
         rp, src = v.planes(*self.recon), v.source(*self.cur)
+        st = lib.vp8a_reconstruct_inter_frame(gs.ctx.handle, C.byref(f), C.cast(pl, C.c_void_p), self.ids.ctypes.data,
+                                              3, self.dec.data_ptr(), C.byref(gs.quant), None, None, 0, 0,
+                                              abi.FILTER_SIXTAP, C.byref(rp), None, None, self.mbs.data_ptr())
+        assert st == 0
         st = lib.vp8a_filter_sweep(gs.ctx.handle, C.byref(rp), self.mbs.data_ptr(), C.byref(gs.base), C.byref(src),
                                    0, self.table.data_ptr())
         assert st == 0
@@ -480,6 +506,9 @@ STAGE_OPS = {
     "analysis": N_MB * 3 * 92_000,
     "arnr": (LOOKAHEAD - 1) * N_MB * 33 * 256 + (LOOKAHEAD - 1) * (W * H * 3 // 2) * 4,
     "lf_sweep": 512 * N_MB * 9_000,
+    # Prediction MACs (below) plus 25 forward and inverse 4x4 transforms
+    # (~64 ops each), quantisation and dequantisation (16 each) per MB.
+    "recon": N_MB * (6 * (21 * 16 + 16 * 16 + 2 * (13 * 8 + 8 * 8)) + 25 * (64 + 16 + 16 + 64)),
     # Two-pass six-tap MACs of a sub-pel MB: luma 21x16 + 16x16, chroma
     # 2 x (13x8 + 8x8) outputs, 6 taps each.
     "predict": N_MB * 6 * (21 * 16 + 16 * 16 + 2 * (13 * 8 + 8 * 8)),
@@ -519,6 +548,9 @@ def stage_times(gs, stream, torch, flush, reps=3):
     fns = {
         "arnr": (gs.run_arnr, LOOKAHEAD * pic + pic),
         "analysis": (gs.run_analysis, luma + 3 * padded + N_MB * gs.abi.MB_DECISION_DTYPE.itemsize),
+        # Source MB, decision and reference MB read, reconstruction and LF
+        # info written per MB.
+        "recon": (gs.run_recon, N_MB * (384 + gs.abi.MB_DECISION_DTYPE.itemsize + 384 + 384 + 8)),
         "lf_sweep": (lambda: gs.run_lf(), padded_pic + pic + N_MB * 8 + 512 * 8),
         # Decisions read, one MB of reference pixels read and one written per
         # MB; a short kernel, so timed over 10 back-to-back calls.
@@ -547,16 +579,17 @@ def stage_times(gs, stream, torch, flush, reps=3):
 # ----------------------------------------------------------- CPU baseline
 
 
-def cpu_step(oracle, frames, threads, pieces=("arnr", "analysis", "lf")):
+def cpu_step(oracle, frames, threads):
     import vp8a
-    from vp8a import synth
 
     anchor = oracle.build_arnr_altref([frames[9 + i] for i in range(LOOKAHEAD)], 3, 3, threads=threads)
     refs = [pad_planes(frames[7]), pad_planes(frames[0]), pad_planes(anchor)]
     lam = oracle.rd_lambda(QI)
     dec = oracle.analyse_inter_frame(frames[8], refs, [1, 2, 3], lam, threads=threads)
-    recon, has = synth.quantised_recon(pad_planes(frames[8]))
-    mbs = vp8a.lf_info_from_decisions(dec, has)
+    recon = tuple(np.zeros_like(p) for p in refs[0])
+    mbs = np.zeros(N_MB, vp8a.abi.MB_LF_INFO_DTYPE)
+    oracle.reconstruct_inter_frame(frames[8], refs, [1, 2, 3], dec, vp8a.abi.quant_indices(QI), recon, lf_info=mbs,
+                                   threads=threads)
     table = oracle.filter_sweep(recon, mbs, vp8a.abi.filter_config(0, 0), frames[8], 0, threads=threads)
     return select_full(table.reshape(-1), 0)
 
@@ -576,8 +609,20 @@ def cpu_baseline(frames, budget_s=30.0):
             break
     dt = time.perf_counter() - t0
     return {"value": round(N_MB * n / dt, 1), "unit": "MB/s", "cores": threads, "kind": "port",
-            "sample": f"{n} full 1080p step(s) (ARNR + 3-ref analysis + 505-candidate LF sweep) "
-                      f"by the C oracle on {threads} threads in {dt:.2f} s"}
+            "sample": f"{n} full 1080p step(s) (ARNR + 3-ref analysis + qi-44 reconstruction + 505-candidate "
+                      f"LF sweep) by the C oracle on {threads} threads in {dt:.2f} s",
+            "cpu_model": cpu_model()}
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def reference_arm(args):
@@ -616,7 +661,7 @@ def reference_arm(args):
         "cpu_baseline": {"value": round(value, 1), "unit": "MB/s", "cores": threads, "kind": "port",
                          "sample": f"{args.steps} full 1080p steps after {args.warmup} warm-up, C oracle "
                                    f"(restatement of the Rust reference, which has no toolchain here) "
-                                   f"on {threads} threads"},
+                                   f"on {threads} threads", "cpu_model": cpu_model()},
         "e2e": {"value": round(value, 1), "unit": "MB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 

@@ -406,10 +406,13 @@ enum { VP8A_MB_SKIP = 1, VP8A_MB_HAS_COEFFS = 2 };
  * `coeffs`, 400 int16 per MB in MbCoeffs order (src/frame.rs:98: y2[16],
  * y[16][16], u[4][16], v[4][16], raster coefficient order, quantised);
  * `mb_flags`, VP8A_MB_SKIP | VP8A_MB_HAS_COEFFS per MB (mb_has_coeffs,
- * src/loop_filter.rs:1500). `mb_segment` (optional, one int8 per MB, -1 =
- * none) selects the factors of segment k from segment_quant[k]
- * (for_segment with `segment_abs`). MBs whose ref_frame is VP8A_REF_INTRA
- * or has no plane in `refs` keep recon's pixels and get flags 0. */
+ * src/loop_filter.rs:1500); `lf_info`, the MB's §15 side information for
+ * vp8a_filter_frame / the loop-filter search (SPLITMV recorded as B_PRED,
+ * src/loop_filter.rs:1258-1266; segment_id from mb_segment). `mb_segment`
+ * (optional, one int8 per MB, -1 = none) selects the factors of segment k
+ * from segment_quant[k] (for_segment with `segment_abs`). MBs whose
+ * ref_frame is VP8A_REF_INTRA or has no plane in `refs` keep recon's pixels
+ * and their lf_info record, and get flags 0 and zero coefficients. */
 vp8a_status vp8a_reconstruct_inter_frame(vp8a_ctx* ctx, const vp8a_i420* frame,
                                          const vp8a_planes* refs, const uint8_t* ref_ids,
                                          uint32_t n_refs, const vp8a_mb_decision* decisions,
@@ -417,7 +420,8 @@ vp8a_status vp8a_reconstruct_inter_frame(vp8a_ctx* ctx, const vp8a_i420* frame,
                                          const int8_t* mb_segment, const int16_t* segment_quant,
                                          uint32_t segment_abs, uint32_t full_pixel,
                                          uint32_t filter_set, vp8a_planes* recon,
-                                         int16_t* coeffs, uint8_t* mb_flags);
+                                         int16_t* coeffs, uint8_t* mb_flags,
+                                         vp8a_mb_lf_info* lf_info);
 
 /* ------------------------------------------------------------ ARNR filter */
 

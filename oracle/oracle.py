@@ -94,7 +94,7 @@ def load():
         "vo_enc_quantize_block": (None, [P, C.c_int16, C.c_int16]),
         "vo_reconstruct_inter_mb": (C.c_int, [P, P, P, C.c_int, P]),
         "vo_reconstruct_inter_frame": (C.c_int, [C.POINTER(abi.I420), P, P, U32, P, C.POINTER(abi.QuantIndices), P, P,
-                                                 C.c_int, C.c_int, C.c_int, C.POINTER(abi.Planes), P, P]),
+                                                 C.c_int, C.c_int, C.c_int, C.POINTER(abi.Planes), P, P, P, U32]),
         "vo_rd_inter_search": (C.c_int, [C.POINTER(abi.I420), P, P, U32, C.POINTER(abi.MvContexts), C.c_double,
                                          U32, U32, P, P, U32]),
     }
@@ -512,11 +512,13 @@ def reconstruct_inter_mb(src384, pred384, factors, split):
 
 
 def reconstruct_inter_frame(frame, refs, ref_ids, decisions, quant, out, mb_segment=None, segment_quant=None,
-                            segment_abs=False, full_pixel=False, filter_set=abi.FILTER_SIXTAP):
+                            segment_abs=False, full_pixel=False, filter_set=abi.FILTER_SIXTAP, lf_info=None,
+                            threads=1):
     """pick_mb_for_ref's chosen-mode §18 + §14 step (trellis off) for a
     frame into the MB-padded planes `out` in place. Returns
     (coeffs (mb_rows*mb_cols, 400) int16, flags (mb_rows*mb_cols,) uint8,
-    number of MBs left untouched)."""
+    number of MBs left untouched); `lf_info` (optional MB_LF_INFO_DTYPE
+    array) receives the §15 side information."""
     f = i420(*frame)
     prs = [planes(*p) for p in refs]
     parr = (abi.Planes * len(prs))(*prs)
@@ -530,5 +532,6 @@ def reconstruct_inter_frame(frame, refs, ref_ids, decisions, quant, out, mb_segm
     sq = None if segment_quant is None else np.ascontiguousarray(np.asarray(segment_quant, np.int16).reshape(4))
     skipped = load().vo_reconstruct_inter_frame(C.byref(f), C.cast(parr, C.c_void_p), ptr(ids), len(prs), ptr(dec),
                                                 C.byref(quant), ptr(seg), ptr(sq), int(bool(segment_abs)),
-                                                int(bool(full_pixel)), filter_set, C.byref(op), ptr(cf), ptr(fl))
+                                                int(bool(full_pixel)), filter_set, C.byref(op), ptr(cf), ptr(fl),
+                                                ptr(lf_info), threads)
     return cf, fl, skipped

@@ -339,50 +339,97 @@ int vo_reconstruct_inter_mb(const uint8_t* src384, uint8_t* pred, const int16_t*
  * / predict_inter_mb from the decision's reference, then
  * vo_reconstruct_inter_mb, written into the MB-padded `out` planes.
  * mb_segment (optional) selects per-MB factors: -1 = the frame's, k = the
- * segment quant segment_quant[k] (absolute or a delta). MBs without an
- * inter reference are left untouched (flags 0). Returns their count. */
+ * segment quant segment_quant[k] (absolute or a delta). lf (optional)
+ * receives each MB's §15 side information. MBs without an inter reference
+ * are left untouched (flags 0, their lf record kept). Every MB is
+ * independent, so MB rows are spread over `threads` (same outputs for any
+ * count). Returns the number of MBs left untouched. */
+typedef struct {
+  const vp8a_i420* frame;
+  const vp8a_planes* refs;
+  const uint8_t* ref_ids;
+  uint32_t n_refs;
+  const vp8a_mb_decision* dec;
+  const int8_t* mb_segment;
+  int16_t fset[5][6];
+  int full_pixel, filter_set;
+  vp8a_planes* out;
+  int16_t* coeffs;
+  uint8_t* flags;
+  vp8a_mb_lf_info* lf;
+  _Atomic int skipped;
+} recon_job;
+
+static void recon_row(void* arg, uint32_t row) {
+  recon_job* j = (recon_job*)arg;
+  vp8a_planes* out = j->out;
+  uint8_t src[384], mb[384];
+  int16_t cf[400];
+  for (uint32_t col = 0; col < out->mb_cols; col++) {
+    const size_t idx = (size_t)row * out->mb_cols + col;
+    const vp8a_mb_decision* d = &j->dec[idx];
+    const vp8a_planes* ref = NULL;
+    for (uint32_t k = 0; k < j->n_refs; k++)
+      if (d->ref_frame != VP8A_REF_INTRA && j->ref_ids[k] == d->ref_frame) ref = &j->refs[k];
+    if (!ref) {
+      j->skipped++;
+      if (j->flags) j->flags[idx] = 0;
+      continue;
+    }
+    const int split = d->mode == VP8A_MODE_SPLIT;
+    if (split)
+      vo_predict_split_mv(ref, col, row, d->split_mvs, j->full_pixel, j->filter_set, mb);
+    else
+      vo_predict_inter_mb(ref, col, row, d->mv, j->full_pixel, j->filter_set, mb);
+    extract_mb(j->frame, row, col, src, src + 256, src + 320);
+    const int seg = j->mb_segment ? j->mb_segment[idx] : -1;
+    const int16_t* f = j->fset[(seg >= 0 && seg < 4) ? 1 + seg : 0];
+    const int fl = vo_reconstruct_inter_mb(src, mb, f, split, cf);
+    if (j->flags) j->flags[idx] = (uint8_t)fl;
+    if (j->lf) {
+      /* The §15 side information of the MB (SPLITMV as B_PRED,
+       * src/loop_filter.rs:1258-1266). */
+      memset(&j->lf[idx], 0, sizeof j->lf[idx]);
+      j->lf[idx].y_mode_is_bpred = (uint8_t)split;
+      j->lf[idx].has_coeffs = (uint8_t)(fl >> 1);
+      j->lf[idx].ref_frame = d->ref_frame;
+      j->lf[idx].inter_mode = d->mode;
+      j->lf[idx].segment_id = (int8_t)seg;
+    }
+    if (j->coeffs) memcpy(j->coeffs + idx * 400, cf, sizeof cf);
+    for (int r = 0; r < 16; r++)
+      memcpy(out->y + ((size_t)row * 16 + r) * out->y_stride + (size_t)col * 16, mb + r * 16, 16);
+    for (int r = 0; r < 8; r++) {
+      memcpy(out->u + ((size_t)row * 8 + r) * out->uv_stride + (size_t)col * 8, mb + 256 + r * 8, 8);
+      memcpy(out->v + ((size_t)row * 8 + r) * out->uv_stride + (size_t)col * 8, mb + 320 + r * 8, 8);
+    }
+  }
+}
+
 int vo_reconstruct_inter_frame(const vp8a_i420* frame, const vp8a_planes* refs,
                                const uint8_t* ref_ids, uint32_t n_refs,
                                const vp8a_mb_decision* dec, const vp8a_quant_indices* qi,
                                const int8_t* mb_segment, const int16_t* segment_quant,
                                int segment_abs, int full_pixel, int filter_set,
-                               vp8a_planes* out, int16_t* coeffs, uint8_t* flags) {
-  int16_t fset[5][6];
-  vo_segment_factors(qi, 0, 0, 0, fset[0]);
+                               vp8a_planes* out, int16_t* coeffs, uint8_t* flags,
+                               vp8a_mb_lf_info* lf, uint32_t threads) {
+  recon_job j;
+  memset(&j, 0, sizeof j);
+  j.frame = frame;
+  j.refs = refs;
+  j.ref_ids = ref_ids;
+  j.n_refs = n_refs;
+  j.dec = dec;
+  j.mb_segment = mb_segment;
+  vo_segment_factors(qi, 0, 0, 0, j.fset[0]);
   for (int k = 0; k < 4; k++)
-    vo_segment_factors(qi, 1, segment_quant ? segment_quant[k] : 0, segment_abs, fset[1 + k]);
-  int skipped = 0;
-  uint8_t src[384], mb[384];
-  int16_t cf[400];
-  for (uint32_t row = 0; row < out->mb_rows; row++)
-    for (uint32_t col = 0; col < out->mb_cols; col++) {
-      const size_t idx = (size_t)row * out->mb_cols + col;
-      const vp8a_mb_decision* d = &dec[idx];
-      const vp8a_planes* ref = NULL;
-      for (uint32_t k = 0; k < n_refs; k++)
-        if (d->ref_frame != VP8A_REF_INTRA && ref_ids[k] == d->ref_frame) ref = &refs[k];
-      if (!ref) {
-        skipped++;
-        if (flags) flags[idx] = 0;
-        continue;
-      }
-      const int split = d->mode == VP8A_MODE_SPLIT;
-      if (split)
-        vo_predict_split_mv(ref, col, row, d->split_mvs, full_pixel, filter_set, mb);
-      else
-        vo_predict_inter_mb(ref, col, row, d->mv, full_pixel, filter_set, mb);
-      extract_mb(frame, row, col, src, src + 256, src + 320);
-      const int seg = mb_segment ? mb_segment[idx] : -1;
-      const int16_t* f = fset[(seg >= 0 && seg < 4) ? 1 + seg : 0];
-      const int fl = vo_reconstruct_inter_mb(src, mb, f, split, cf);
-      if (flags) flags[idx] = (uint8_t)fl;
-      if (coeffs) memcpy(coeffs + idx * 400, cf, sizeof cf);
-      for (int r = 0; r < 16; r++)
-        memcpy(out->y + ((size_t)row * 16 + r) * out->y_stride + (size_t)col * 16, mb + r * 16, 16);
-      for (int r = 0; r < 8; r++) {
-        memcpy(out->u + ((size_t)row * 8 + r) * out->uv_stride + (size_t)col * 8, mb + 256 + r * 8, 8);
-        memcpy(out->v + ((size_t)row * 8 + r) * out->uv_stride + (size_t)col * 8, mb + 320 + r * 8, 8);
-      }
-    }
-  return skipped;
+    vo_segment_factors(qi, 1, segment_quant ? segment_quant[k] : 0, segment_abs, j.fset[1 + k]);
+  j.full_pixel = full_pixel;
+  j.filter_set = filter_set;
+  j.out = out;
+  j.coeffs = coeffs;
+  j.flags = flags;
+  j.lf = lf;
+  vo_parallel_for(out->mb_rows, threads, recon_row, &j);
+  return j.skipped;
 }

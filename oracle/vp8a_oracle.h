@@ -170,7 +170,8 @@ int vo_reconstruct_inter_frame(const vp8a_i420* frame, const vp8a_planes* refs,
                                const vp8a_mb_decision* dec, const vp8a_quant_indices* qi,
                                const int8_t* mb_segment, const int16_t* segment_quant,
                                int segment_abs, int full_pixel, int filter_set,
-                               vp8a_planes* out, int16_t* coeffs, uint8_t* flags);
+                               vp8a_planes* out, int16_t* coeffs, uint8_t* flags,
+                               vp8a_mb_lf_info* lf, uint32_t threads);
 
 /* ---- threading helper */
 typedef void (*vo_task_fn)(void* arg, uint32_t index);

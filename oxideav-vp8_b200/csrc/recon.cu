@@ -74,6 +74,7 @@ struct RcArgs {
   int16_t f[5][6];  // frame factors, then segments 0..3
   int16_t* coeffs;
   uint8_t* flags;
+  vp8a_mb_lf_info* lf;
 };
 
 __device__ __forceinline__ int cmul(int i) { return i + ((i * COS8) >> 16); }
@@ -313,6 +314,15 @@ __global__ void __launch_bounds__(RC_WARPS * 32) recon_kernel(RcArgs a) {
     }
     const bool has = __any_sync(full, dnz != 0);
     if (a.flags && lane == 0) a.flags[item] = (uint8_t)((skip ? VP8A_MB_SKIP : 0) | (has ? VP8A_MB_HAS_COEFFS : 0));
+    if (a.lf && lane == 0) {
+      vp8a_mb_lf_info m{};
+      m.y_mode_is_bpred = split;
+      m.has_coeffs = has;
+      m.ref_frame = d.ref_frame;
+      m.inter_mode = d.mode;
+      m.segment_id = (int8_t)seg;
+      a.lf[item] = m;
+    }
     if (skip) continue;  // warp-uniform: the reconstruction is the prediction
     if (!split) {
       if (lane == 24) iwht4x4(blk);
@@ -363,7 +373,7 @@ vp8a_status vp8a_reconstruct_inter_frame(vp8a_ctx* ctx, const vp8a_i420* frame, 
                                          const vp8a_quant_indices* quant, const int8_t* mb_segment,
                                          const int16_t* segment_quant, uint32_t segment_abs, uint32_t full_pixel,
                                          uint32_t filter_set, vp8a_planes* recon, int16_t* coeffs,
-                                         uint8_t* mb_flags) {
+                                         uint8_t* mb_flags, vp8a_mb_lf_info* lf_info) {
   if (!ctx || !frame || !quant || !recon) {
     vp8a::set_error("null argument");
     return VP8A_E_INVALID_ARGUMENT;
@@ -437,6 +447,11 @@ vp8a_status vp8a_reconstruct_inter_frame(vp8a_ctx* ctx, const vp8a_i420* frame, 
   if (mb_flags) {
     if ((s = st.out(mb_flags, a.n, &o)) != VP8A_OK) return s;
     a.flags = (uint8_t*)o;
+  }
+  if (lf_info) {
+    // In/out: MBs without an inter reference keep the caller's record.
+    if ((s = st.inout(lf_info, (size_t)a.n * sizeof(vp8a_mb_lf_info), &o)) != VP8A_OK) return s;
+    a.lf = (vp8a_mb_lf_info*)o;
   }
   if (!g_rc_blocks_per_sm) {
     int b = 0;

@@ -255,13 +255,15 @@ def dequant_factors(quant, segment_quant=None, absolute=False):
 
 def reconstruct_inter_frame(ctx, frame, refs, ref_ids, decisions, quant, recon, mb_segment=None,
                             segment_quant=None, segment_abs=False, full_pixel=False, filter_set=abi.FILTER_SIXTAP,
-                            coeffs=True, flags=True):
+                            coeffs=True, flags=True, lf_info=None):
     """pick_mb_for_ref's §18 prediction + §14 transform / quantise /
     reconstruct for every MB's chosen mode with the trellis off
     (src/encoder.rs:8704-8800). `frame` = visible (y, u, v); `recon` =
     MB-padded (y, u, v) written in place; `quant` an abi.QuantIndices.
     Returns (coeffs (n_mbs, 400) int16 in MbCoeffs order or None,
-    flags (n_mbs,) uint8 of abi.MB_SKIP | abi.MB_HAS_COEFFS or None)."""
+    flags (n_mbs,) uint8 of abi.MB_SKIP | abi.MB_HAS_COEFFS or None);
+    `lf_info` (optional MB_LF_INFO_DTYPE buffer) receives each inter MB's
+    §15 side information for the loop-filter calls."""
     f = i420(*frame)
     prs = [planes(*p) for p in refs]
     parr = (abi.Planes * len(prs))(*prs)
@@ -276,7 +278,8 @@ def reconstruct_inter_frame(ctx, frame, refs, ref_ids, decisions, quant, recon, 
     sq = None if segment_quant is None else np.ascontiguousarray(np.asarray(segment_quant, np.int16).reshape(4))
     check(ctx._lib.vp8a_reconstruct_inter_frame(ctx.handle, C.byref(f), C.cast(parr, C.c_void_p), ptr(ids), len(prs),
                                                 ptr(dec), C.byref(quant), ptr(seg), ptr(sq), int(bool(segment_abs)),
-                                                int(bool(full_pixel)), filter_set, C.byref(op), ptr(cf), ptr(fl)),
+                                                int(bool(full_pixel)), filter_set, C.byref(op), ptr(cf), ptr(fl),
+                                                ptr(lf_info)),
           "vp8a_reconstruct_inter_frame")
     return cf, fl
 

@@ -44,7 +44,7 @@ PROTOTYPES = {
     "vp8a_reconstruct_inter_frame": (
         C.c_int,
         [P, C.POINTER(abi.I420), P, P, U32, P, C.POINTER(abi.QuantIndices), P, P, U32, U32, U32,
-         C.POINTER(abi.Planes), P, P],
+         C.POINTER(abi.Planes), P, P, P],
     ),
     "vp8a_build_arnr_altref": (C.c_int, [P, P, U32, U32, U32, P, P, P]),
     "vp8a_filter_frame": (C.c_int, [P, C.POINTER(abi.Planes), P, C.POINTER(abi.FilterConfig)]),

@@ -24,11 +24,15 @@ def frame_case(w, h, seed):
 def run_both(ctx, oracle, frame, refs, ids, dec, quant, fill=7, **kw):
     got = tuple(np.full(p.shape, fill, np.uint8) for p in refs[0])
     want = tuple(np.full(p.shape, fill, np.uint8) for p in refs[0])
-    gcf, gfl = vp8a.reconstruct_inter_frame(ctx, frame, refs, ids, dec, quant, got, **kw)
-    wcf, wfl, _ = oracle.reconstruct_inter_frame(frame, refs, ids, dec, quant, want, **kw)
+    n = got[0].shape[0] // 16 * (got[0].shape[1] // 16)
+    glf = np.full(n, 0x55, np.uint8).repeat(abi.MB_LF_INFO_DTYPE.itemsize).view(abi.MB_LF_INFO_DTYPE)
+    wlf = glf.copy()
+    gcf, gfl = vp8a.reconstruct_inter_frame(ctx, frame, refs, ids, dec, quant, got, lf_info=glf, **kw)
+    wcf, wfl, _ = oracle.reconstruct_inter_frame(frame, refs, ids, dec, quant, want, lf_info=wlf, **kw)
     for g, w in zip(got, want):
         assert np.array_equal(g, w)
     assert np.array_equal(gfl, wfl)
+    assert np.array_equal(glf.view(np.uint8), wlf.view(np.uint8))
     bad = np.argwhere((gcf != wcf).any(axis=1)).reshape(-1)
     assert bad.size == 0, f"coefficients differ in {bad.size} MBs, first {bad[:5]}"
     return got, gcf, gfl
