@@ -685,7 +685,8 @@ def case_arm(args):
     else:
         frames, _ = synth.make_sequence(w, h, 16, SEED, pieces=4, occluders=4)
         gs = GpuStep(ctx, frames, vp8a.load(), torch, 0)
-        fn = {"arnr": gs.run_arnr, "analysis": gs.run_analysis, "lf": gs.run_lf, "predict": gs.run_predict}[args.case]
+        fn = {"arnr": gs.run_arnr, "analysis": gs.run_analysis, "lf": gs.run_lf, "predict": gs.run_predict,
+              "recon": gs.run_recon}[args.case]
     stream = torch.cuda.ExternalStream(ctx.stream)
     for _ in range(args.warmup):
         fn()
@@ -737,7 +738,7 @@ def main():
     ap.add_argument("--impl", default="vp8a", choices=["vp8a", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
-    ap.add_argument("--case", choices=["arnr", "analysis", "lf", "predict", "predict_mb", "predict_split"],
+    ap.add_argument("--case", choices=["arnr", "analysis", "lf", "recon", "predict", "predict_mb", "predict_split"],
                     help="profile one stage alone")
     ap.add_argument("--size", default="1920x1080", help="frame size for --case")
     args = ap.parse_args()

@@ -72,6 +72,7 @@ struct RcArgs {
   int n_refs;
   const int8_t* mb_segment;
   int16_t f[5][6];  // frame factors, then segments 0..3
+  uint32_t m[5][6];  // ceil(2^32 / f): the quantiser's reciprocals
   int16_t* coeffs;
   uint8_t* flags;
   vp8a_mb_lf_info* lf;
@@ -185,9 +186,14 @@ __device__ __forceinline__ void idct4x4(int* b) {
 }
 
 // enc_round_div (src/encoder.rs:2112): round half away from zero, as i16.
-__device__ __forceinline__ int rdiv(int num, int den) {
-  const int r = num >= 0 ? (num + den / 2) / den : -(((-num) + den / 2) / den);
-  return to16(r);
+// The quotient floor(a / den) of a = |num| + den / 2 < 2^17 is taken as
+// the high word of a * m with m = ceil(2^32 / den): with e = m * den - 2^32
+// in [0, den), a * m / 2^32 = a / den + a * e / (den * 2^32), and the excess
+// stays below 1 / den because a * den < 2^27 (den <= 440), so the floor is
+// exact.
+__device__ __forceinline__ int rdiv(int num, int den, uint32_t m) {
+  const uint32_t q = __umulhi((uint32_t)abs(num) + (uint32_t)(den >> 1), m);
+  return to16(num >= 0 ? (int)q : -(int)q);
 }
 
 __global__ void __launch_bounds__(RC_WARPS * 32) recon_kernel(RcArgs a) {
@@ -208,7 +214,9 @@ __global__ void __launch_bounds__(RC_WARPS * 32) recon_kernel(RcArgs a) {
     }
     const bool split = d.mode == VP8A_MODE_SPLIT;
     const int seg = a.mb_segment ? a.mb_segment[item] : -1;
-    const int16_t* f = a.f[(seg >= 0 && seg < 4) ? 1 + seg : 0];
+    const int fs = (seg >= 0 && seg < 4) ? 1 + seg : 0;
+    const int16_t* f = a.f[fs];
+    const uint32_t* fm = a.m[fs];
     const int mbx = (int)(item % (uint32_t)a.mb_cols), mby = (int)(item / (uint32_t)a.mb_cols);
 
     // This lane's block: plane, top-left pixel in the plane.
@@ -275,20 +283,15 @@ __global__ void __launch_bounds__(RC_WARPS * 32) recon_kernel(RcArgs a) {
       if (luma) blk[0] = 0;
     }
     // Plain quantisation (enc_quantize_block) with this block's factors.
-    int qdc = f[0], qac = f[1];
-    if (lane == 24) {
-      qdc = f[2];
-      qac = f[3];
-    } else if (chroma) {
-      qdc = f[4];
-      qac = f[5];
-    }
+    const int fi = lane == 24 ? 2 : (chroma ? 4 : 0);
+    const int qdc = f[fi], qac = f[fi + 1];
+    const uint32_t mdc = fm[fi], mac = fm[fi + 1];
     const bool active = luma || chroma || (lane == 24 && !split);
     int nz = 0;
     if (active) {
-      blk[0] = rdiv(blk[0], qdc);
+      blk[0] = rdiv(blk[0], qdc, mdc);
 #pragma unroll
-      for (int k = 1; k < 16; k++) blk[k] = rdiv(blk[k], qac);
+      for (int k = 1; k < 16; k++) blk[k] = rdiv(blk[k], qac, mac);
 #pragma unroll
       for (int k = 0; k < 16; k++) nz |= blk[k];
     }
@@ -431,6 +434,8 @@ vp8a_status vp8a_reconstruct_inter_frame(vp8a_ctx* ctx, const vp8a_i420* frame, 
   if (segment_quant && (s = st.read_to_host(segment_quant, sizeof sq, sq)) != VP8A_OK) return s;
   vp8a_dequant_factors(quant, 0, 0, 0, a.f[0]);
   for (int k = 0; k < 4; k++) vp8a_dequant_factors(quant, 1, sq[k], segment_abs, a.f[1 + k]);
+  for (int k = 0; k < 5; k++)
+    for (int i = 0; i < 6; i++) a.m[k][i] = (uint32_t)((((uint64_t)1 << 32) + a.f[k][i] - 1) / a.f[k][i]);
   if (mb_segment) {
     if ((s = st.in(mb_segment, a.n, &d)) != VP8A_OK) return s;
     a.mb_segment = (const int8_t*)d;
