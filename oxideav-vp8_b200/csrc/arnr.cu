@@ -2,19 +2,23 @@
 //
 // Two kernels:
 //  * arnr_search_kernel — refine_search (src/arnr.rs:264-300) for every
-//    (window frame != centre, 16x16 block): one warp per block, the +/-15 px
-//    neighbourhood of the block staged edge-clamped in shared memory, the
-//    eight candidates of each 8/4/2/1 round scored in parallel (four lanes
-//    each) and folded in the reference's candidate order with strict '<'.
+//    (window frame != centre, 16x16 block): one CTA per strip of 8 blocks
+//    of one frame, whose shared +/-15 px neighbourhood is staged
+//    edge-clamped in shared memory once; one warp per block, the eight
+//    candidates of each 8/4/2/1 round scored in parallel (four lanes each)
+//    and folded in the reference's candidate order with strict '<'.
 //  * arnr_blend_kernel — the per-pixel weighted temporal mean
-//    (accumulate_* :337-459 + resolve_plane :670): every output pixel
-//    gathers its block's alignment from each frame, applies the SAD
-//    occlusion guard (:605) and the weight table (:307-323), and resolves in
-//    one pass. Integer sums are order-free, so gathering per pixel equals
+//    (accumulate_* :337-459 + resolve_plane :670): each thread takes four
+//    horizontally adjacent output pixels of one block, gathers the block's
+//    alignment from each frame, applies the SAD occlusion guard (:605) and
+//    the weight table (:307-323) to one motion-compensated word per frame,
+//    and resolves in one pass. Integer sums are order-free, so gathering per pixel equals
 //    the reference's frame-then-raster scatter. Every chroma pixel lies in
 //    exactly one chroma block (block k covers [8k, 8k + ceil(bw/2)) and
 //    ceil((bx+bw)/2) <= ceil(w/2)), so the clamped-overhang branch of
 //    accumulate_chroma_block never adds a second contribution.
+#include <climits>
+
 #include "vp8a_internal.cuh"
 
 namespace {
@@ -36,8 +40,6 @@ struct BlockMv {
 };
 
 constexpr int AW = 46;       // window extent: 16 + 2 * 15
-constexpr int AWS = 48;      // window stride
-constexpr int ARNR_WARPS = 4;
 
 __device__ __forceinline__ void load8u(const uint8_t* p, uint32_t& o0, uint32_t& o1) {
   uintptr_t a = (uintptr_t)p;
@@ -52,39 +54,75 @@ struct SearchArgs {
   const ArnrFrame* frames;
   uint32_t n, center;
   int w, h, bcols, brows;
+  int aligned;  // every window plane base and row pitch is 4-byte aligned
   BlockMv* out;  // [n][brows][bcols]
 };
 
-__global__ void __launch_bounds__(ARNR_WARPS * 32) arnr_search_kernel(SearchArgs a) {
-  __shared__ __align__(16) uint8_t win[ARNR_WARPS][AWS * AW + 16];
-  __shared__ __align__(16) uint8_t srcb[ARNR_WARPS][256];
+constexpr int STRIP = 8;                    // blocks per CTA (one warp each)
+constexpr int SWS = 164;  // row stride: rows four apart fall four banks apart
+constexpr int SWW = SWS / 4;                // words per staged row
+
+// One CTA per (window frame != centre, strip of 8 horizontally adjacent
+// blocks). The strip's +-15 px neighbourhood in the frame (46 rows x 158
+// columns, staged 164 wide, edge-clamped to the visible plane as pel does, src/arnr.rs:149)
+// and its 16 source rows of the centre frame are staged once as 32-bit
+// words; warp j then runs refine_search for block j of the strip on the
+// staged window.
+__global__ void __launch_bounds__(STRIP * 32) arnr_search_kernel(SearchArgs a) {
+  __shared__ __align__(16) uint8_t win[AW * SWS + 16];
+  __shared__ __align__(16) uint8_t srcs[16 * STRIP * 16];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t nblk = (uint32_t)a.bcols * a.brows;
-  const uint32_t item = blockIdx.x * ARNR_WARPS + warp;
-  if (item >= nblk * (a.n - 1)) return;
-  uint32_t fi = item / nblk;
+  const int strips = (a.bcols + STRIP - 1) / STRIP;
+  uint32_t fi = blockIdx.x / ((uint32_t)strips * a.brows);
+  const uint32_t rest = blockIdx.x % ((uint32_t)strips * a.brows);
   if (fi >= a.center) fi++;  // skip the centre frame
-  const uint32_t blk = item % nblk;
-  const int bcol = (int)(blk % a.bcols), brow = (int)(blk / a.bcols);
-  const int bx = bcol * 16, by = brow * 16;
-  const int bw = min(16, a.w - bx), bh = min(16, a.h - by);
+  const int brow = (int)(rest / strips), strip = (int)(rest % strips);
+  const int bx0 = strip * STRIP * 16, by = brow * 16;
   const ArnrFrame ctr = a.frames[a.center];
   const ArnrFrame ref = a.frames[fi];
-  uint8_t* W = win[warp];
-  uint8_t* S = srcb[warp];
-  // Source block (centre frame), zero outside bw x bh.
-  for (int i = lane; i < 256; i += 32) {
-    int r = i >> 4, c = i & 15;
-    S[i] = (r < bh && c < bw) ? ctr.y[(size_t)(by + r) * ctr.y_stride + bx + c] : 0;
+  // Window: word k of row r holds columns x0 + 4k .. x0 + 4k + 3.
+  const int x0 = bx0 - 15;
+  const bool words = a.aligned && x0 >= 0 && x0 + SWS + 4 <= a.w;
+  for (int i = threadIdx.x; i < AW * SWW; i += blockDim.x) {
+    const int r = i / SWW, k = i - SWW * r;
+    const uint8_t* row = ref.y + (size_t)clampi(by - 15 + r, 0, a.h - 1) * ref.y_stride;
+    uint32_t v;
+    if (words) {
+      const int x = x0 + 4 * k;
+      const uint32_t* p = reinterpret_cast<const uint32_t*>(row + (x & ~3));
+      v = __funnelshift_r(__ldg(p), __ldg(p + 1), 8 * (x & 3));
+    } else {
+      v = 0;
+#pragma unroll
+      for (int c = 0; c < 4; c++) v |= (uint32_t)__ldg(row + clampi(x0 + 4 * k + c, 0, a.w - 1)) << (8 * c);
+    }
+    *reinterpret_cast<uint32_t*>(win + r * SWS + 4 * k) = v;
   }
-  // Reference neighbourhood, edge-clamped to the visible plane (pel,
-  // src/arnr.rs:149).
-  for (int r = 0; r < AW; r++) {
-    int yy = clampi(by - 15 + r, 0, a.h - 1);
-    const uint8_t* row = ref.y + (size_t)yy * ref.y_stride;
-    for (int c = lane; c < AW; c += 32) W[r * AWS + c] = row[clampi(bx - 15 + c, 0, a.w - 1)];
+  // Source rows of the strip (centre frame), zero outside the picture.
+  for (int i = threadIdx.x; i < 16 * STRIP * 4; i += blockDim.x) {
+    const int r = i / (STRIP * 4), k = i - STRIP * 4 * r, x = bx0 + 4 * k;
+    uint32_t v = 0;
+    if (by + r < a.h) {
+      const uint8_t* row = ctr.y + (size_t)(by + r) * ctr.y_stride;
+      if (a.aligned && x + 4 <= a.w) {
+        v = __ldg(reinterpret_cast<const uint32_t*>(row + x));
+      } else {
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+          if (x + c < a.w) v |= (uint32_t)__ldg(row + x + c) << (8 * c);
+      }
+    }
+    // Stored block-major: block j's 16 x 16 source at srcs + 256 j.
+    const int j = k >> 2, kk = k & 3;
+    *reinterpret_cast<uint32_t*>(srcs + 256 * j + 16 * r + 4 * kk) = v;
   }
-  __syncwarp();
+  __syncthreads();
+  const int bcol = strip * STRIP + warp;
+  if (bcol >= a.bcols) return;  // past the picture's last block (after the only barrier)
+  const int bx = bcol * 16;
+  const int bw = min(16, a.w - bx), bh = min(16, a.h - by);
+  const uint8_t* W = win + 16 * warp;  // this block's 46 x 46 window
+  const uint8_t* S = srcs + 256 * warp;
   const int k = lane >> 2, q = lane & 3;
   // Byte masks for the partial-width columns.
   uint32_t m[4];
@@ -99,13 +137,13 @@ __global__ void __launch_bounds__(ARNR_WARPS * 32) arnr_search_kernel(SearchArgs
   // SAD of candidate (x, y) over this lane's four rows.
   auto part = [&](int x, int y) -> uint32_t {
     uint32_t s = 0;
-    const uint8_t* base = W + (15 + y + q * 4) * AWS + 15 + x;
+    const uint8_t* base = W + (15 + y + q * 4) * SWS + 15 + x;
 #pragma unroll
     for (int r = 0; r < 4; r++) {
       if (q * 4 + r < bh) {
         uint32_t a0, a1, a2, a3;
-        load8u(base + r * AWS, a0, a1);
-        load8u(base + r * AWS + 8, a2, a3);
+        load8u(base + r * SWS, a0, a1);
+        load8u(base + r * SWS + 8, a2, a3);
         const uint32_t* sp = (const uint32_t*)(S + (q * 4 + r) * 16);
         s += __vsadu4(a0 & m[0], sp[0]) + __vsadu4(a1 & m[1], sp[1]) + __vsadu4(a2 & m[2], sp[2]) +
              __vsadu4(a3 & m[3], sp[3]);
@@ -130,18 +168,15 @@ __global__ void __launch_bounds__(ARNR_WARPS * 32) arnr_search_kernel(SearchArgs
     uint32_t s = valid ? part(x, y) : 0;
     s += __shfl_xor_sync(FULL, s, 1);
     s += __shfl_xor_sync(FULL, s, 2);
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-      uint32_t sj = __shfl_sync(FULL, s, j * 4);
-      const int jdx = (j == 0 || j == 3 || j == 5) ? -step : ((j == 1 || j == 6) ? 0 : step);
-      const int jdy = (j < 3) ? -step : (j < 5 ? 0 : step);
-      const int jx = cx + jdx, jy = cy + jdy;
-      const bool jv = jx >= -15 && jx <= 15 && jy >= -15 && jy <= 15;
-      if (jv && sj < best_sad) {
-        best_sad = sj;
-        bestx = jx;
-        besty = jy;
-      }
+    // The reference folds the eight candidates in order with a strict '<'
+    // against the running best: that is the smallest (sad, order) pair,
+    // taken when its sad beats the incumbent. SADs are < 2^17.
+    const uint32_t r = __reduce_min_sync(FULL, valid ? (s << 3) | (uint32_t)k : 0xffffffffu);
+    if (r != 0xffffffffu && (r >> 3) < best_sad) {
+      const int j = (int)(r & 7);
+      best_sad = r >> 3;
+      bestx = cx + ((j == 0 || j == 3 || j == 5) ? -step : ((j == 1 || j == 6) ? 0 : step));
+      besty = cy + ((j < 3) ? -step : (j < 5 ? 0 : step));
     }
   }
   if (lane == 0) {
@@ -158,49 +193,116 @@ struct BlendArgs {
   const BlockMv* mv;
   uint32_t n, center, s_scale;
   int w, h, cw, ch, bcols, brows;
+  int aligned_in;  // every window plane base and row pitch is 4-byte aligned
+  int aligned_out;  // the output planes' rows start 4-byte aligned
   uint8_t* y_out;
   uint8_t* u_out;
   uint8_t* v_out;
 };
 
-// One thread per output pixel of the three planes (luma first).
-__global__ void __launch_bounds__(256) arnr_blend_kernel(BlendArgs a) {
+constexpr int BLEND_BLOCKS = 2;                 // 16x16 blocks per CTA step
+constexpr int BLEND_THREADS = 96 * BLEND_BLOCKS;  // 64 luma + 2 x 16 chroma words per block
+
+// Four bytes of row `row` at columns x .. x+3, each clamped to [0, pw). The
+// word form needs a row whose base and pitch are 4-byte aligned and the
+// aligned pair [x & ~3, (x & ~3) + 8) inside [0, pw): that pair covers the
+// four bytes and never leaves the row.
+__device__ __forceinline__ uint32_t row4(const uint8_t* row, int x, int pw, bool words) {
+  if (words && x >= 0 && x + 8 <= pw) {
+    const uint32_t* p = reinterpret_cast<const uint32_t*>(row + (x & ~3));
+    return __funnelshift_r(__ldg(p), __ldg(p + 1), 8 * (x & 3));
+  }
+  uint32_t v = 0;
+#pragma unroll
+  for (int c = 0; c < 4; c++) v |= (uint32_t)__ldg(row + clampi(x + c, 0, pw - 1)) << (8 * c);
+  return v;
+}
+
+// floor(a / d) for a < 2^24, 16 <= d < 2^16: the single-precision estimate
+// is within one below the quotient; the remainder test corrects it.
+__device__ __forceinline__ uint32_t udiv_small(uint32_t a, uint32_t d) {
+  uint32_t q = __float2uint_rz(__uint2float_rn(a) * __frcp_rn(__uint2float_rn(d)));
+  const int r = (int)a - (int)(q * d);
+  if (r < 0) q--;
+  else if (r >= (int)d) q++;
+  return q;
+}
+
+// Each thread blends four horizontally adjacent output pixels of one block:
+// threads 0-63 of a block's group the 16x16 luma block (row t / 4, columns
+// 4 (t % 4) ..), 64-79 the 8x8 U block and 80-95 the 8x8 V block. The
+// block's alignment per window frame is uniform, so every frame's four
+// motion-compensated samples are one unaligned word of one row. The
+// alignments of the CTA's blocks are staged in shared memory first (frames
+// past BLEND_MAX_FRAMES are read from global memory).
+constexpr int BLEND_MAX_FRAMES = 32;
+
+__global__ void __launch_bounds__(BLEND_THREADS) arnr_blend_kernel(BlendArgs a) {
   __shared__ uint32_t wt[256];
+  __shared__ int2 smv[BLEND_BLOCKS][BLEND_MAX_FRAMES];  // (mvx, mvy); mvx = INT_MIN: frame not used
   for (int d = threadIdx.x; d < 256; d += blockDim.x)
     wt[d] = (16u * a.s_scale) / (a.s_scale + (uint32_t)(d * d));
-  __syncthreads();
-  const size_t ny = (size_t)a.w * a.h, nc = (size_t)a.cw * a.ch;
-  const size_t total = ny + 2 * nc;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+  const int g = threadIdx.x / 96, t = threadIdx.x % 96;
+  const uint32_t nblk = (uint32_t)a.bcols * a.brows;
+  const ArnrFrame c = a.frames[a.center];
+  const uint32_t nst = min(a.n, (uint32_t)BLEND_MAX_FRAMES);
+  for (uint32_t b0 = blockIdx.x * BLEND_BLOCKS; b0 < nblk; b0 += gridDim.x * BLEND_BLOCKS) {
+    const uint32_t b = b0 + g;
+    const int bcol = (int)(b % (uint32_t)a.bcols), brow = (int)(b / (uint32_t)a.bcols);
+    // Occlusion guard: sad / (bw * bh) > 12 (BLOCK_SAD_PER_PIXEL_CUTOFF)
+    // is sad >= 13 * area for integers.
+    const uint32_t area = (uint32_t)(min(16, a.w - bcol * 16) * min(16, a.h - brow * 16));
+    __syncthreads();  // the previous step's readers are done with smv
+    for (uint32_t fi = t; fi < nst && b < nblk; fi += 96) {
+      int2 v = make_int2(INT_MIN, 0);
+      if (fi != a.center) {
+        const BlockMv m = a.mv[((size_t)fi * a.brows + brow) * a.bcols + bcol];
+        if (m.sad < 13u * area) v = make_int2(m.mvx, m.mvy);
+      }
+      smv[g][fi] = v;
+    }
+    __syncthreads();
+    if (b >= nblk) continue;
     int plane, x, y, pw, ph;
-    if (i < ny) {
+    if (t < 64) {
       plane = 0;
-      y = (int)(i / a.w);
-      x = (int)(i % a.w);
+      x = bcol * 16 + 4 * (t & 3);
+      y = brow * 16 + (t >> 2);
       pw = a.w;
       ph = a.h;
     } else {
-      size_t j = i - ny;
-      plane = j < nc ? 1 : 2;
-      if (j >= nc) j -= nc;
-      y = (int)(j / a.cw);
-      x = (int)(j % a.cw);
+      const int k = t - 64;
+      plane = 1 + (k >> 4);
+      x = bcol * 8 + 4 * (k & 1);
+      y = brow * 8 + ((k >> 1) & 7);
       pw = a.cw;
       ph = a.ch;
     }
-    const int blk_x = plane ? x >> 3 : x >> 4, blk_y = plane ? y >> 3 : y >> 4;
-    const ArnrFrame c = a.frames[a.center];
+    if (x >= pw || y >= ph) continue;
+    const int nvalid = min(4, pw - x);
     const uint8_t* cp = plane == 0 ? c.y : (plane == 1 ? c.u : c.v);
     const uint64_t cs = plane == 0 ? c.y_stride : c.uv_stride;
-    const int ctr = cp[(size_t)y * cs + x];
-    uint32_t acc = 16u * (uint32_t)ctr, ws = 16u;
-    const int bw = min(16, a.w - blk_x * 16), bh = min(16, a.h - blk_y * 16);
-    const uint32_t area = (uint32_t)(bw * bh);
+    const uint32_t ctr = row4(cp + (uint64_t)y * cs, x, pw, a.aligned_in);
+    uint32_t acc[4], ws[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      acc[j] = 16u * ((ctr >> (8 * j)) & 0xffu);
+      ws[j] = 16u;
+    }
+#pragma unroll 2
     for (uint32_t fi = 0; fi < a.n; fi++) {
-      if (fi == a.center) continue;
-      const BlockMv m = a.mv[((size_t)fi * a.brows + blk_y) * a.bcols + blk_x];
-      if (m.sad / area > 12u) continue;  // BLOCK_SAD_PER_PIXEL_CUTOFF
-      int mvx = m.mvx, mvy = m.mvy;
+      int2 mv;
+      if (fi < nst) {
+        mv = smv[g][fi];
+      } else {
+        mv = make_int2(INT_MIN, 0);
+        if (fi != a.center) {
+          const BlockMv m = a.mv[((size_t)fi * a.brows + brow) * a.bcols + bcol];
+          if (m.sad < 13u * area) mv = make_int2(m.mvx, m.mvy);
+        }
+      }
+      if (mv.x == INT_MIN) continue;
+      int mvx = mv.x, mvy = mv.y;
       if (plane) {
         mvx /= 2;  // toward zero (src/arnr.rs:622)
         mvy /= 2;
@@ -208,17 +310,24 @@ __global__ void __launch_bounds__(256) arnr_blend_kernel(BlendArgs a) {
       const ArnrFrame f = a.frames[fi];
       const uint8_t* fp = plane == 0 ? f.y : (plane == 1 ? f.u : f.v);
       const uint64_t fs = plane == 0 ? f.y_stride : f.uv_stride;
-      const int rx = clampi(x + mvx, 0, pw - 1), ry = clampi(y + mvy, 0, ph - 1);
-      const int ref = fp[(size_t)ry * fs + rx];
-      const int d = ref - ctr;
-      const uint32_t wgt = wt[d < 0 ? -d : d];
-      acc += wgt * (uint32_t)ref;
-      ws += wgt;
+      const uint32_t ref = row4(fp + (uint64_t)clampi(y + mvy, 0, ph - 1) * fs, x + mvx, pw, a.aligned_in);
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int rv = (int)((ref >> (8 * j)) & 0xffu), cv = (int)((ctr >> (8 * j)) & 0xffu);
+        const uint32_t wgt = wt[rv > cv ? rv - cv : cv - rv];
+        acc[j] += wgt * (uint32_t)rv;
+        ws[j] += wgt;
+      }
     }
-    const uint8_t o = (uint8_t)((acc + ws / 2) / ws);
-    if (plane == 0) a.y_out[(size_t)y * a.w + x] = o;
-    else if (plane == 1) a.u_out[(size_t)y * a.cw + x] = o;
-    else a.v_out[(size_t)y * a.cw + x] = o;
+    uint32_t o = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) o |= udiv_small(acc[j] + ws[j] / 2, ws[j]) << (8 * j);
+    uint8_t* op = plane == 0 ? a.y_out + (size_t)y * a.w : (plane == 1 ? a.u_out : a.v_out) + (size_t)y * a.cw;
+    if (nvalid == 4 && a.aligned_out) {
+      *reinterpret_cast<uint32_t*>(op + x) = o;
+    } else {
+      for (int j = 0; j < nvalid; j++) op[x + j] = (uint8_t)(o >> (8 * j));
+    }
   }
 }
 
@@ -283,14 +392,22 @@ extern "C" vp8a_status vp8a_build_arnr_altref(vp8a_ctx* ctx, const vp8a_i420* fr
   void* dmv = nullptr;
   if ((s = st.scratch(sizeof(BlockMv) * (size_t)n * bcols * brows, &dmv)) != VP8A_OK) return s;
   if (filter) {
-    SearchArgs sa{(const ArnrFrame*)dframes, n, center, w, h, bcols, brows, (BlockMv*)dmv};
-    size_t items = (size_t)bcols * brows * (n - 1);
-    arnr_search_kernel<<<vp8a::grid_for(items, ARNR_WARPS), ARNR_WARPS * 32, 0, ctx->stream>>>(sa);
+    int aligned = 1;
+    for (uint32_t i = 0; i < n; i++) aligned &= (((uintptr_t)hf[i].y | hf[i].y_stride) & 3) == 0;
+    SearchArgs sa{(const ArnrFrame*)dframes, n, center, w, h, bcols, brows, aligned, (BlockMv*)dmv};
+    const size_t ctas = (size_t)((bcols + STRIP - 1) / STRIP) * brows * (n - 1);
+    arnr_search_kernel<<<(unsigned)ctas, STRIP * 32, 0, ctx->stream>>>(sa);
     VP8A_CUDA(cudaGetLastError());
     ctx->launches++;
   }
+  int aligned_in = 1;
+  for (uint32_t i = 0; i < n; i++)
+    aligned_in &= (((uintptr_t)hf[i].y | (uintptr_t)hf[i].u | (uintptr_t)hf[i].v | hf[i].y_stride |
+                     hf[i].uv_stride) & 3) == 0;
+  const int aligned_out = (((uintptr_t)dy | (uintptr_t)du | (uintptr_t)dv | (uintptr_t)w | (uintptr_t)cw) & 3) == 0;
   BlendArgs ba{(const ArnrFrame*)dframes, (const BlockMv*)dmv, filter ? n : 0u, filter ? center : 0u,
-               8u << str, w, h, cw, ch, bcols, brows, (uint8_t*)dy, (uint8_t*)du, (uint8_t*)dv};
+               8u << str, w, h, cw, ch, bcols, brows, aligned_in, aligned_out,
+               (uint8_t*)dy, (uint8_t*)du, (uint8_t*)dv};
   if (!filter) {
     // Pass-through (src/arnr.rs:527-529): the blend with no window frames
     // reproduces the centre exactly. The centre is frames[0] of a
@@ -299,9 +416,9 @@ extern "C" vp8a_status vp8a_build_arnr_altref(vp8a_ctx* ctx, const vp8a_i420* fr
     ba.n = 1;
     ba.center = 0;
   }
-  size_t total = (size_t)w * h + 2 * (size_t)cw * ch;
-  unsigned grid = (unsigned)std::min<size_t>(vp8a::grid_for(total, 256), (size_t)ctx->sm_count * 16);
-  arnr_blend_kernel<<<grid, 256, 0, ctx->stream>>>(ba);
+  const size_t nblk = (size_t)bcols * brows;
+  unsigned grid = (unsigned)std::min<size_t>(vp8a::grid_for(nblk, BLEND_BLOCKS), (size_t)ctx->sm_count * 16);
+  arnr_blend_kernel<<<grid, BLEND_THREADS, 0, ctx->stream>>>(ba);
   VP8A_CUDA(cudaGetLastError());
   ctx->launches++;
   return st.finish();
