@@ -86,6 +86,10 @@ def load():
         "vo_predict_split_mv_batch": (None, [C.POINTER(abi.Planes), P, P, U32, C.c_int, C.c_int, P]),
         "vo_predict_inter_frame": (C.c_int, [P, P, U32, P, C.c_int, C.c_int, C.POINTER(abi.Planes)]),
         "vo_dequant_factors": (None, [C.c_int32] * 6 + [P]),
+        "vo_vp8_decoder_new": (P, []),
+        "vo_vp8_decoder_free": (None, [P]),
+        "vo_vp8_decode_frame": (C.c_int, [P, P, C.c_size_t, P, C.POINTER(U32), C.POINTER(U32),
+                                          C.POINTER(C.c_int)]),
         "vo_segment_factors": (None, [C.POINTER(abi.QuantIndices), C.c_int, C.c_int32, C.c_int, P]),
         "vo_forward_dct_4x4": (None, [P, P]),
         "vo_forward_wht_4x4": (None, [P, P]),
@@ -535,3 +539,54 @@ def reconstruct_inter_frame(frame, refs, ref_ids, decisions, quant, out, mb_segm
                                                 int(bool(full_pixel)), filter_set, C.byref(op), ptr(cf), ptr(fl),
                                                 ptr(lf_info), threads)
     return cf, fl, skipped
+
+
+# ---- VP8 decoder restatement (decoder.c) ---------------------------------
+
+def ivf_frames(data):
+    """The frame payloads of an IVF file (32-byte header, then 12-byte frame
+    headers: 4-byte little-endian size + 8-byte timestamp)."""
+    assert data[:4] == b"DKIF", "not an IVF file"
+    hdr = int.from_bytes(data[6:8], "little")
+    pos, out = hdr, []
+    while pos + 12 <= len(data):
+        n = int.from_bytes(data[pos:pos + 4], "little")
+        out.append(bytes(data[pos + 12:pos + 12 + n]))
+        pos += 12 + n
+    return out
+
+
+class Vp8Decoder:
+    """Vp8DecoderState (src/state.rs): decode frames in order; each call
+    returns the visible I420 picture as (y, u, v) arrays."""
+
+    def __init__(self):
+        self.lib = load()
+        self.h = self.lib.vo_vp8_decoder_new()
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.vo_vp8_decoder_free(self.h)
+            self.h = None
+
+    def decode_into(self, frame, max_pixels=1 << 24):
+        buf = np.frombuffer(frame, np.uint8)
+        out = np.zeros(max_pixels * 3 // 2 + 16, np.uint8)
+        w, h, shown = U32(), U32(), C.c_int()
+        st = self.lib.vo_vp8_decode_frame(self.h, ptr(buf), len(buf), ptr(out), C.byref(w), C.byref(h),
+                                          C.byref(shown))
+        if st != 0:
+            raise RuntimeError(f"vo_vp8_decode_frame: {st}")
+        w, h = w.value, h.value
+        cw, ch = (w + 1) // 2, (h + 1) // 2
+        y = out[:w * h].reshape(h, w).copy()
+        u = out[w * h:w * h + cw * ch].reshape(ch, cw).copy()
+        v = out[w * h + cw * ch:w * h + 2 * cw * ch].reshape(ch, cw).copy()
+        return (y, u, v), bool(shown.value)
+
+
+def decode_ivf(data):
+    """Every frame of an IVF stream through the restated decoder, as a list
+    of ((y, u, v), shown)."""
+    dec = Vp8Decoder()
+    return [dec.decode_into(f) for f in ivf_frames(data)]

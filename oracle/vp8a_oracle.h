@@ -173,6 +173,13 @@ int vo_reconstruct_inter_frame(const vp8a_i420* frame, const vp8a_planes* refs,
                                vp8a_planes* out, int16_t* coeffs, uint8_t* flags,
                                vp8a_mb_lf_info* lf, uint32_t threads);
 
+/* ---- VP8 decoder restatement (decoder.c) */
+typedef struct vo_vp8_decoder vo_vp8_decoder;
+vo_vp8_decoder* vo_vp8_decoder_new(void);
+void vo_vp8_decoder_free(vo_vp8_decoder* d);
+int vo_vp8_decode_frame(vo_vp8_decoder* d, const uint8_t* data, size_t size, uint8_t* out,
+                        uint32_t* width, uint32_t* height, int* shown);
+
 /* ---- threading helper */
 typedef void (*vo_task_fn)(void* arg, uint32_t index);
 void vo_parallel_for(uint32_t n, uint32_t threads, vo_task_fn fn, void* arg);
