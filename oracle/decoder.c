@@ -156,6 +156,7 @@ enum { BT_Y_AFTER_Y2 = 0, BT_Y2 = 1, BT_UV = 2, BT_Y_NO_Y2 = 3 };
 /* ----------------------------------------------------------- decoder state */
 
 struct vo_vp8_decoder {
+  vo_vp8_capture* cap;  /* optional per-frame capture (see vo_vp8_decoder_capture) */
   int have_key;
   uint32_t width, height, mb_cols, mb_rows;
   uint8_t* slot[3][3]; /* LAST, GOLDEN, ALTREF x (y, u, v), MB-padded */
@@ -170,6 +171,13 @@ vo_vp8_decoder* vo_vp8_decoder_new(void) {
   vo_vp8_decoder* d = (vo_vp8_decoder*)calloc(1, sizeof(vo_vp8_decoder));
   return d;
 }
+
+/* Attach (or with NULL detach) caller buffers that each later decode fills
+ * with that frame's intermediate state: the references in force, every
+ * inter MB's prediction and decision, the reconstruction before and after
+ * the loop filter, the MBs' loop-filter records and the filter
+ * configuration. */
+void vo_vp8_decoder_capture(vo_vp8_decoder* d, vo_vp8_capture* cap) { d->cap = cap; }
 
 void vo_vp8_decoder_free(vo_vp8_decoder* d) {
   if (!d) return;
@@ -923,6 +931,19 @@ int vo_vp8_decode_frame(vo_vp8_decoder* d, const uint8_t* data, size_t size, uin
   refp[VP8A_REF_GOLDEN] = planes_of(d, d->slot[1][0], d->slot[1][1], d->slot[1][2]);
   refp[VP8A_REF_ALTREF] = planes_of(d, d->slot[2][0], d->slot[2][1], d->slot[2][2]);
   for (int c = 0; c < cols; c++) above_mb[c].ref = VP8A_REF_INTRA;
+  vo_vp8_capture* cap = d->cap;
+  if (cap) {
+    cap->captured = cap->mb_cols == cols && cap->mb_rows == rows;
+    if (!cap->captured) cap = NULL;
+  }
+  if (cap) {
+    for (int s = 0; s < 3; s++)
+      for (int p = 0; p < 3; p++) memcpy(cap->refs[s][p], d->slot[s][p], p ? lc : ly);
+    for (int p = 0; p < 3; p++) memset(cap->pred[p], 0, p ? lc : ly);
+    memset(cap->dec, 0, (size_t)n_mb * sizeof(vp8a_mb_decision));
+    cap->key = h.key;
+    cap->version = h.version;
+  }
 
   int16_t cf[400];
   uint8_t mb[384];
@@ -979,8 +1000,22 @@ int vo_vp8_decode_frame(vo_vp8_decoder* d, const uint8_t* data, size_t size, uin
           vo_predict_split_mv(&refp[ref], (uint32_t)col, (uint32_t)row, info.split, full_pixel, filter_set, mb);
         else
           vo_predict_inter_mb(&refp[ref], (uint32_t)col, (uint32_t)row, mv, full_pixel, filter_set, mb);
+        if (cap) {
+          vp8a_mb_decision* dd = &cap->dec[idx];
+          dd->ref_frame = (uint8_t)ref;
+          dd->mode = (uint8_t)mode;
+          dd->mv = mv;
+          if (split) memcpy(dd->split_mvs, info.split, sizeof info.split);
+          for (int r = 0; r < 16; r++)
+            memcpy(cap->pred[0] + ((size_t)row * 16 + r) * cur.y_stride + col * 16, mb + 16 * r, 16);
+          for (int r = 0; r < 8; r++) {
+            memcpy(cap->pred[1] + ((size_t)row * 8 + r) * cur.uv_stride + col * 8, mb + 256 + 8 * r, 8);
+            memcpy(cap->pred[2] + ((size_t)row * 8 + r) * cur.uv_stride + col * 8, mb + 320 + 8 * r, 8);
+          }
+        }
         if (!skip) add_residual(mb, cf, !split, 0);
       } else {
+        if (cap) cap->dec[idx].ref_frame = VP8A_REF_INTRA;
         int ymode, uvmode;
         uint8_t bm[16];
         if (h.key) {
@@ -1082,7 +1117,20 @@ int vo_vp8_decode_frame(vo_vp8_decoder* d, const uint8_t* data, size_t size, uin
   }
   memcpy(d->ref_lf_deltas, rd, sizeof rd);
   memcpy(d->mode_lf_deltas, md, sizeof md);
+  if (cap) {
+    memcpy(cap->pre[0], cur_y, ly);
+    memcpy(cap->pre[1], cur_u, lc);
+    memcpy(cap->pre[2], cur_v, lc);
+    memcpy(cap->lf, lfi, (size_t)n_mb * sizeof(vp8a_mb_lf_info));
+    *cap->cfg = lc_;
+    cap->filtered = h.level != 0;
+  }
   if (h.level != 0) vo_filter_frame(&cur, lfi, &lc_);
+  if (cap) {
+    memcpy(cap->post[0], cur_y, ly);
+    memcpy(cap->post[1], cur_u, lc);
+    memcpy(cap->post[2], cur_v, lc);
+  }
 
   /* Probability carry (src/state.rs:628-640, :1163-1171). */
   if (h.key) {

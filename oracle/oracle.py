@@ -88,6 +88,7 @@ def load():
         "vo_dequant_factors": (None, [C.c_int32] * 6 + [P]),
         "vo_vp8_decoder_new": (P, []),
         "vo_vp8_decoder_free": (None, [P]),
+        "vo_vp8_decoder_capture": (None, [P, P]),
         "vo_vp8_decode_frame": (C.c_int, [P, P, C.c_size_t, P, C.POINTER(U32), C.POINTER(U32),
                                           C.POINTER(C.c_int)]),
         "vo_segment_factors": (None, [C.POINTER(abi.QuantIndices), C.c_int, C.c_int32, C.c_int, P]),
@@ -590,3 +591,47 @@ def decode_ivf(data):
     of ((y, u, v), shown)."""
     dec = Vp8Decoder()
     return [dec.decode_into(f) for f in ivf_frames(data)]
+
+
+class _Capture(C.Structure):
+    _fields_ = [("refs", (P * 3) * 3), ("pred", P * 3), ("pre", P * 3), ("post", P * 3), ("dec", P), ("lf", P),
+                ("cfg", C.POINTER(abi.FilterConfig)), ("key", C.c_int32), ("version", C.c_int32),
+                ("filtered", C.c_int32), ("mb_cols", C.c_int32), ("mb_rows", C.c_int32), ("captured", C.c_int32)]
+
+
+def decode_ivf_captured(data):
+    """Decode an IVF stream with the restated decoder, yielding per frame a
+    dict of its intermediate state (MB-padded planes as (y, u, v)): `refs`
+    (LAST, GOLDEN, ALTREF in force), `pred` (inter MBs' prediction, intra
+    MBs 0), `dec` (MB_DECISION_DTYPE; ref_frame INTRA for intra MBs),
+    `pre` / `post` (reconstruction before / after the loop filter), `lf`
+    (MB_LF_INFO_DTYPE), `cfg` (abi.FilterConfig), `key`, `version`,
+    `filtered`, and the visible `picture`."""
+    w, h = int.from_bytes(data[12:14], "little"), int.from_bytes(data[14:16], "little")
+    mbc, mbr = (w + 15) // 16, (h + 15) // 16
+    shapes = [(mbr * 16, mbc * 16), (mbr * 8, mbc * 8), (mbr * 8, mbc * 8)]
+    new = lambda: [np.zeros(s, np.uint8) for s in shapes]  # noqa: E731
+    refs, pred, pre, post = [new() for _ in range(3)], new(), new(), new()
+    dec = np.zeros(mbc * mbr, abi.MB_DECISION_DTYPE)
+    lf = np.zeros(mbc * mbr, abi.MB_LF_INFO_DTYPE)
+    cfg = abi.FilterConfig()
+    cap = _Capture()
+    for s in range(3):
+        for p in range(3):
+            cap.refs[s][p] = ptr(refs[s][p])
+    for p in range(3):
+        cap.pred[p], cap.pre[p], cap.post[p] = ptr(pred[p]), ptr(pre[p]), ptr(post[p])
+    cap.dec, cap.lf, cap.cfg = ptr(dec), ptr(lf), C.pointer(cfg)
+    cap.mb_cols, cap.mb_rows = mbc, mbr
+    dec_obj = Vp8Decoder()
+    dec_obj.lib.vo_vp8_decoder_capture(dec_obj.h, C.byref(cap))
+    for frame in ivf_frames(data):
+        cap.captured = 0
+        picture, shown = dec_obj.decode_into(frame)
+        if not cap.captured:
+            raise ValueError("frame size differs from the IVF header's; capture needs a fixed size")
+        yield {"refs": [tuple(p.copy() for p in r) for r in refs], "pred": tuple(p.copy() for p in pred),
+               "pre": tuple(p.copy() for p in pre), "post": tuple(p.copy() for p in post), "dec": dec.copy(),
+               "lf": lf.copy(), "cfg": abi.FilterConfig.from_buffer_copy(cfg), "key": bool(cap.key),
+               "version": int(cap.version), "filtered": bool(cap.filtered), "picture": picture, "shown": shown}
+    dec_obj.lib.vo_vp8_decoder_capture(dec_obj.h, None)

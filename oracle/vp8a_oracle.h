@@ -175,8 +175,22 @@ int vo_reconstruct_inter_frame(const vp8a_i420* frame, const vp8a_planes* refs,
 
 /* ---- VP8 decoder restatement (decoder.c) */
 typedef struct vo_vp8_decoder vo_vp8_decoder;
+/* Caller buffers one decode fills (MB-padded planes of the stream's grid). */
+typedef struct vo_vp8_capture {
+  uint8_t* refs[3][3];   /* LAST, GOLDEN, ALTREF in force x (y, u, v) */
+  uint8_t* pred[3];      /* inter MBs' §18 prediction (intra MBs 0) */
+  uint8_t* pre[3];       /* reconstruction before the loop filter */
+  uint8_t* post[3];      /* reconstruction after it */
+  vp8a_mb_decision* dec; /* per MB: ref_frame (INTRA for intra), mode, mv, split_mvs */
+  vp8a_mb_lf_info* lf;
+  vp8a_filter_config* cfg;
+  int32_t key, version, filtered;
+  int32_t mb_cols, mb_rows;  /* set by the caller: the buffers' MB grid */
+  int32_t captured;          /* 1 when the last frame's grid matched and was captured */
+} vo_vp8_capture;
 vo_vp8_decoder* vo_vp8_decoder_new(void);
 void vo_vp8_decoder_free(vo_vp8_decoder* d);
+void vo_vp8_decoder_capture(vo_vp8_decoder* d, vo_vp8_capture* cap);
 int vo_vp8_decode_frame(vo_vp8_decoder* d, const uint8_t* data, size_t size, uint8_t* out,
                         uint32_t* width, uint32_t* height, int* shown);
 

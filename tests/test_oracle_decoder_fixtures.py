@@ -36,3 +36,38 @@ def test_decoder_matches_libvpx_fixture(name):
 
 def test_all_fixtures_present():
     assert len(NAMES) == 13
+
+
+def _planes_equal(a, b):
+    return all(np.array_equal(x, y) for x, y in zip(a, b))
+
+
+@pytest.mark.parametrize("name", ["i-frame-then-p-frame-64x64", "golden-update-cycle", "altref-arnr-on",
+                                  "vp8-with-loopfilter-mode-simple"])
+def test_decoder_capture_is_consistent(name):
+    # The capture hook's intermediate state re-derives the decoded pictures:
+    # the batched prediction entry point over the captured decisions
+    # reproduces the decoder's own per-MB prediction, the frame filter over
+    # the captured records reproduces the post-filter planes, and those crop
+    # to the visible picture. This is the state the device parity test
+    # feeds to the CUDA kernels.
+    from vp8a import abi
+    from vp8a.api import filter_set_for_version
+
+    data = open(os.path.join(FIX, name, "input.ivf"), "rb").read()
+    n_inter = 0
+    for f in oracle.decode_ivf_captured(data):
+        if not f["key"]:
+            n_inter += 1
+            inter = np.isin(f["dec"]["ref_frame"], [abi.REF_LAST, abi.REF_GOLDEN, abi.REF_ALTREF])
+            assert inter.any()
+            out = tuple(np.zeros_like(p) for p in f["pred"])
+            oracle.predict_inter_frame(f["refs"], [abi.REF_LAST, abi.REF_GOLDEN, abi.REF_ALTREF], f["dec"], out,
+                                       full_pixel=f["version"] == 3, filter_set=filter_set_for_version(f["version"]))
+            assert _planes_equal(out, f["pred"])
+        post = oracle.filter_frame(f["pre"], f["lf"], f["cfg"]) if f["filtered"] else f["pre"]
+        assert _planes_equal(post, f["post"])
+        y, u, v = f["picture"]
+        assert np.array_equal(f["post"][0][:y.shape[0], :y.shape[1]], y)
+        assert np.array_equal(f["post"][1][:u.shape[0], :u.shape[1]], u)
+    assert n_inter > 0 or name == "vp8-with-loopfilter-mode-simple"  # a single key frame
