@@ -703,6 +703,190 @@ def case_arm(args):
     return {"case": args.case, "size": args.size, "ms": [round(x, 4) for x in ts]}
 
 
+# ------------------------------------------------- batched streams case
+
+BATCH_RESOLUTIONS = [(176, 144), (640, 360), (1280, 720), (1920, 1080), (3840, 2160)]
+BATCH_LOOKAHEAD = 5
+
+
+class BatchStep:
+    """The batched plain path over many independent streams of uneven size:
+    per stream one P frame analysed against LAST (the previous frame) and
+    ALTREF (the ARNR anchor of a 5-frame lookahead, centre anchor), its
+    qi-44 reconstruction and the 64 x 8 loop-filter sweep over it. Each
+    stage of all streams is one call of the batched entry points
+    (vp8a_build_arnr_altrefs, vp8a_analyse_inter_frames,
+    vp8a_reconstruct_inter_frames, vp8a_filter_sweeps) on device-resident
+    buffers."""
+
+    def __init__(self, ctx, streams, torch):
+        import vp8a
+        from vp8a import abi
+
+        self.vp8a, self.abi, self.ctx, self.torch = vp8a, abi, ctx, torch
+        self.stream = torch.cuda.ExternalStream(ctx.stream)
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+        self.keep = []
+        self.s = []
+        for frames in streams:
+            h, w = frames[0][0].shape
+            mbc, mbr = (w + 15) // 16, (h + 15) // 16
+            st = {"w": w, "h": h, "mbs": mbc * mbr}
+            st["cur"] = [t(p) for p in frames[1]]
+            st["last"] = [t(p) for p in pad_planes(frames[0])]
+            st["win"] = [[t(p) for p in f] for f in frames[2:2 + BATCH_LOOKAHEAD]]
+            st["alt"] = [torch.zeros_like(p) for p in st["last"]]
+            st["recon"] = [torch.zeros_like(p) for p in st["last"]]
+            st["lf"] = torch.zeros(st["mbs"] * abi.MB_LF_INFO_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+            st["dec"] = torch.zeros(st["mbs"] * abi.MB_DECISION_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+            self.s.append(st)
+        self.tables = torch.zeros((len(streams), 512), dtype=torch.int64, device="cuda")
+        torch.cuda.synchronize()
+        ids = np.array([abi.REF_LAST, abi.REF_ALTREF], np.uint8)
+        self.ctxs = abi.default_mv_contexts()
+        lam = vp8a.rd_lambda(QI)
+        aj, anj, rj, sj = [], [], [], []
+        for i, st in enumerate(self.s):
+            win = (abi.I420 * BATCH_LOOKAHEAD)(*[vp8a.i420(*f) for f in st["win"]])
+            refs = (abi.Planes * 2)(vp8a.planes(*st["last"]), vp8a.planes(*st["alt"]))
+            self.keep += [win, refs]
+            a = st["alt"]
+            aj.append(abi.ArnrJob(C.cast(win, C.c_void_p), BATCH_LOOKAHEAD, BATCH_LOOKAHEAD // 2, 3,
+                                  a[0].data_ptr(), a[1].data_ptr(), a[2].data_ptr()))
+            cur = vp8a.i420(*st["cur"])
+            anj.append(abi.AnalysisJob(cur, C.cast(refs, C.c_void_p), ids.ctypes.data, 2,
+                                       C.cast(C.pointer(self.ctxs), C.c_void_p), lam, st["dec"].data_ptr(), None))
+            rj.append(abi.ReconJob(cur, C.cast(refs, C.c_void_p), ids.ctypes.data, 2, 0, st["dec"].data_ptr(),
+                                   abi.quant_indices(QI), None, None, 0, abi.FILTER_SIXTAP, vp8a.planes(*st["recon"]),
+                                   None, None, st["lf"].data_ptr()))
+            sj.append(abi.SweepJob(vp8a.planes(*st["recon"]), st["lf"].data_ptr(), abi.filter_config(0, 0),
+                                   vp8a.source(*st["cur"]), 0, self.tables[i].data_ptr()))
+        self.ids = ids
+        self.jobs = {k: (type(v[0]) * len(v))(*v) for k, v in
+                     (("arnr", aj), ("analysis", anj), ("recon", rj), ("lf", sj))}
+        self.n_mb = sum(st["mbs"] for st in self.s)
+
+    def _call(self, fn, key):
+        arr = self.jobs[key]
+        st = getattr(self.ctx._lib, fn)(self.ctx.handle, C.cast(arr, C.c_void_p), len(arr))
+        assert st == 0, self.vp8a.load().vp8a_last_error()
+
+    def run_arnr(self):
+        self._call("vp8a_build_arnr_altrefs", "arnr")
+        # Edge-replicate each anchor into its MB-padded ALTREF planes.
+        with self.torch.cuda.stream(self.stream):
+            for st in self.s:
+                h, ch = st["h"], (st["h"] + 1) // 2
+                a = st["alt"]
+                if a[0].shape[0] > h:
+                    a[0][h:] = a[0][h - 1]
+                if a[1].shape[0] > ch:
+                    a[1][ch:] = a[1][ch - 1]
+                    a[2][ch:] = a[2][ch - 1]
+
+    def run_analysis(self):
+        self._call("vp8a_analyse_inter_frames", "analysis")
+
+    def run_recon(self):
+        self._call("vp8a_reconstruct_inter_frames", "recon")
+
+    def run_lf(self):
+        self._call("vp8a_filter_sweeps", "lf")
+        self.ctx.synchronize()
+        t = self.tables.cpu().numpy().view(np.uint64)
+        return [select_full(row, 0) for row in t]
+
+    def step(self):
+        self.run_arnr()
+        self.run_analysis()
+        self.run_recon()
+        return self.run_lf()
+
+
+def batch_streams(n_streams, seed):
+    """`n_streams` streams with resolutions drawn from BATCH_RESOLUTIONS by
+    `seed`; each stream is 2 + BATCH_LOOKAHEAD consecutive frames of one
+    seeded sequence per resolution (streams of one resolution start at
+    different frames)."""
+    from vp8a import synth
+
+    rng = np.random.default_rng(seed)
+    pick = rng.integers(0, len(BATCH_RESOLUTIONS), n_streams)
+    need = 2 + BATCH_LOOKAHEAD
+    seqs = {}
+    for r in sorted(set(int(x) for x in pick)):
+        w, h = BATCH_RESOLUTIONS[r]
+        seqs[r], _ = synth.make_sequence(w, h, need - 1 + int((pick == r).sum()), seed + 17 * r, pieces=4,
+                                         occluders=4)
+    used = {r: 0 for r in seqs}
+    streams = []
+    for r in pick:
+        r = int(r)
+        streams.append(seqs[r][used[r]:used[r] + need])
+        used[r] += 1
+    return streams, pick
+
+
+def batch_arm(args):
+    """The batched plain path (48 streams of uneven size by default): MBs
+    per second through ARNR + analysis + reconstruction + LF sweep, every
+    stage one batched launch, inputs resident on the device, L2 flushed
+    between timed steps."""
+    import torch
+
+    import vp8a
+
+    streams, pick = batch_streams(args.streams, SEED)
+    ctx = vp8a.Context(0)
+    bs = BatchStep(ctx, streams, torch)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = bs.stream
+    for _ in range(args.warmup):
+        bs.step()
+    ctx.synchronize()
+    ts = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        bs.step()
+        e.record(stream)
+        e.synchronize()
+        ts.append(s.elapsed_time(e))
+    stages = {}
+    for name in ("arnr", "analysis", "recon", "lf"):
+        fn = getattr(bs, "run_" + name)
+        xs = []
+        for _ in range(3):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            torch.cuda.synchronize()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            fn()
+            e.record(stream)
+            e.synchronize()
+            xs.append(s.elapsed_time(e))
+        stages[name] = round(float(np.median(xs)), 3)
+    per_res = {}
+    for r, st in zip(pick, bs.s):
+        k = "%dx%d" % BATCH_RESOLUTIONS[int(r)]
+        d = per_res.setdefault(k, {"streams": 0, "mbs": 0})
+        d["streams"] += 1
+        d["mbs"] += st["mbs"]
+    ms = float(np.median(ts))
+    ctx.close()
+    return {"case": "batch", "metric": "MBs/s (ARNR+ME+recon+LF search), batched streams", "unit": "MB/s",
+            "value": round(bs.n_mb / (ms / 1e3), 1), "ms_per_step": round(ms, 3), "steps": args.steps,
+            "warmup": args.warmup, "streams": args.streams, "mbs_per_step": bs.n_mb, "per_resolution": per_res,
+            "stage_ms": stages, "step_ms": [round(x, 3) for x in ts],
+            "config": {"workload": "%d streams from {176x144, 640x360, 1280x720, 1920x1080, 3840x2160}: "
+                                   "P frame vs LAST/ALTREF, ARNR(5, centre), qi-44 reconstruction, LF 64x8 sweep"
+                                   % args.streams, "seed": SEED, "l2": "flushed between timed steps (256 MiB write)"}}
+
+
 def batched_predict(ctx, vp8a, torch, split):
     """vp8a_predict_inter_mb (or _split_mv) over 8 frames' worth of MBs at
     random positions of random MB-padded reference planes of the --size grid,
@@ -738,13 +922,17 @@ def main():
     ap.add_argument("--impl", default="vp8a", choices=["vp8a", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
-    ap.add_argument("--case", choices=["arnr", "analysis", "lf", "recon", "predict", "predict_mb", "predict_split"],
-                    help="profile one stage alone")
+    ap.add_argument("--case", choices=["arnr", "analysis", "lf", "recon", "predict", "predict_mb", "predict_split",
+                                       "batch"],
+                    help="profile one stage alone, or (batch) the batched many-stream path")
+    ap.add_argument("--streams", type=int, default=48, help="streams of the batch case")
     ap.add_argument("--size", default="1920x1080", help="frame size for --case")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl != "reference":
         log("note: fewer than 3 warm-up steps")
-    if args.case:
+    if args.case == "batch":
+        res = batch_arm(args)
+    elif args.case:
         res = case_arm(args)
     else:
         res = reference_arm(args) if args.impl == "reference" else gpu_arm(args)

@@ -503,6 +503,90 @@ vp8a_status vp8a_select_filter_params_sampled(vp8a_ctx* ctx, const vp8a_planes* 
                                               uint32_t sweep_sharpness, uint8_t* level_out,
                                               uint8_t* sharpness_out);
 
+/* ---------------------------------------------------- batched work lists
+ *
+ * The reference encodes each stream with its own encoder object
+ * (Vp8AltrefStreamEncoder::push_frame, src/stream.rs:2750, one
+ * encode_p_frame_multi_ref_auto_loop_filter per frame, src/encoder.rs:9373)
+ * and has no batched form. The *_frames / *_altrefs / *_sweeps entry points
+ * below take a work list of independent jobs of uneven sizes (many streams'
+ * frames) and run every job of one stage in one persistent launch; each
+ * job's results are the ones the single-job call gives. At most
+ * VP8A_MAX_BATCH_JOBS jobs per call. */
+#define VP8A_MAX_BATCH_JOBS 1024u
+
+/* One vp8a_analyse_inter_frame call's arguments. */
+typedef struct vp8a_analysis_job {
+  vp8a_i420 frame;
+  const vp8a_planes* refs;              /* n_refs MB-padded references */
+  const uint8_t* ref_ids;               /* n_refs VP8A_REF_* */
+  uint32_t n_refs;                      /* 1..3 */
+  const vp8a_mv_contexts* mv_contexts;  /* NULL = the §17.2 defaults */
+  double lambda;
+  vp8a_mb_decision* decisions;          /* mb_cols*mb_rows, raster order */
+  vp8a_ref_search* trace;               /* optional: n_refs per MB */
+} vp8a_analysis_job;
+
+/* vp8a_analyse_inter_frame for every job: the MB rows of all jobs with the
+ * same reference count form one work list over one persistent launch (each
+ * job keeps its own row-to-row wavefront; jobs with the longest wavefront
+ * start first). */
+vp8a_status vp8a_analyse_inter_frames(vp8a_ctx* ctx, const vp8a_analysis_job* jobs, uint32_t n_jobs);
+
+/* One vp8a_build_arnr_altref call's arguments. */
+typedef struct vp8a_arnr_job {
+  const vp8a_i420* frames;  /* n frames of one size */
+  uint32_t n;
+  uint32_t center;
+  uint32_t strength;
+  uint8_t* y_out;
+  uint8_t* u_out;
+  uint8_t* v_out;
+} vp8a_arnr_job;
+
+/* vp8a_build_arnr_altref for every job: one search launch over every
+ * job's (frame, strip of blocks) and one blend launch over every job's
+ * blocks. */
+vp8a_status vp8a_build_arnr_altrefs(vp8a_ctx* ctx, const vp8a_arnr_job* jobs, uint32_t n_jobs);
+
+/* One vp8a_reconstruct_inter_frame call's arguments (`recon` is written). */
+typedef struct vp8a_recon_job {
+  vp8a_i420 frame;
+  const vp8a_planes* refs;
+  const uint8_t* ref_ids;
+  uint32_t n_refs;
+  uint32_t segment_abs;
+  const vp8a_mb_decision* decisions;
+  vp8a_quant_indices quant;
+  const int8_t* mb_segment;
+  const int16_t* segment_quant;
+  uint32_t full_pixel;
+  uint32_t filter_set;
+  vp8a_planes recon;
+  int16_t* coeffs;
+  uint8_t* mb_flags;
+  vp8a_mb_lf_info* lf_info;
+} vp8a_recon_job;
+
+/* vp8a_reconstruct_inter_frame for every job: one prediction launch and one
+ * reconstruction launch over every job's MBs. */
+vp8a_status vp8a_reconstruct_inter_frames(vp8a_ctx* ctx, const vp8a_recon_job* jobs, uint32_t n_jobs);
+
+/* One vp8a_filter_sweep call's arguments. */
+typedef struct vp8a_sweep_job {
+  vp8a_planes planes;
+  const vp8a_mb_lf_info* mbs;
+  vp8a_filter_config base;
+  vp8a_source src;
+  uint32_t every_rows;
+  uint64_t* ssd_out;  /* 512 entries, level * 8 + sharpness */
+} vp8a_sweep_job;
+
+/* vp8a_filter_sweep for every job: the (job, candidate) pairs of all jobs
+ * in one launch when every job's slot rings fit in shared memory (the
+ * larger pictures otherwise run as their own launches). */
+vp8a_status vp8a_filter_sweeps(vp8a_ctx* ctx, const vp8a_sweep_job* jobs, uint32_t n_jobs);
+
 #ifdef __cplusplus
 }
 #endif

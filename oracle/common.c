@@ -69,6 +69,10 @@ size_t vo_type_size(int which) {
     case 11: return sizeof(vp8a_mb_info);
     case 12: return sizeof(vp8a_rd_inter);
     case 13: return sizeof(vp8a_quant_indices);
+    case 14: return sizeof(vp8a_analysis_job);
+    case 15: return sizeof(vp8a_arnr_job);
+    case 16: return sizeof(vp8a_recon_job);
+    case 17: return sizeof(vp8a_sweep_job);
     default: return 0;
   }
 }

@@ -28,7 +28,11 @@
 // reference's operation order; the library is built with -fmad=false so no
 // multiply-add is fused.
 #include <cooperative_groups.h>
+#include <algorithm>
 #include <cstddef>
+#include <cstring>
+#include <utility>
+#include <vector>
 
 #include "census.cuh"
 
@@ -882,9 +886,19 @@ constexpr int MAIN_THREADS = MAIN_WARPS * 32;
 __device__ __forceinline__ void main_sync() { asm volatile("bar.sync 1, %0;" ::"n"(MAIN_THREADS) : "memory"); }
 static_assert(AN_THREADS >= 16 * FN, "one thread per field task");
 
-__global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
+// Work items: one MB row each. A single frame (BATCH false) takes rows
+// 0..a0.mb_rows-1 of a0; a batch takes items[i] = job << 16 | row over the
+// job table `jobs`, ordered so that every row comes after the row above it
+// (a job's rows are consecutive). Clusters take items round-robin and all
+// are resident, so the row a wait depends on is always held by a running
+// cluster. Every job of one launch has cluster-size (n_refs) references.
+template <bool BATCH>
+__global__ void __launch_bounds__(AN_THREADS, 1)
+    analysis_kernel(AnArgs a0, const AnArgs* __restrict__ jobs, const uint32_t* __restrict__ items, int n_items) {
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
+  __shared__ AnArgs a;  // the current item's job
+  __shared__ const double* s_mvb_src;
   __shared__ RefSmem R;
   __shared__ FieldSmem F;
   __shared__ WarpTemp wt[NW];
@@ -914,30 +928,52 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
   __shared__ QuarterGeom s_qg;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int k = (int)cl.block_rank();  // the reference this CTA searches
-  const int cid = blockIdx.x / a.n_refs, n_clusters = gridDim.x / a.n_refs;
+  const int csize = (int)cl.num_blocks();
+  const int cid = blockIdx.x / csize, n_clusters = gridDim.x / csize;
   const MePlane& P = a.refs[k];
-  for (int i = tid; i < 256; i += AN_THREADS) bit_cost[i] = a.bit_cost[i];
-  for (int i = tid; i < 2 * MV_BITS_SPAN; i += AN_THREADS) mvb[i] = a.mvbits[i];
-  __syncthreads();
-  if (tid < 20) {
-    const double b = submv_ref_bits(bit_cost, c_submv_probs[tid >> 2], tid & 3);
-    sbits[tid] = b;
-    lterm[tid] = a.lambda * (b + 0.0);
-  } else if (tid < 24) {
-    pbits[tid - 20] = mv_partition_bits(bit_cost, tid - 20);
-  } else if (tid == 24) {
-    // lambda * ref_frame_tree_bits(ref, 128, 128) (src/encoder.rs:9108).
-    const double* t = bit_cost;
-    const uint8_t id = a.ref_ids[k];
-    const double rbits = id == VP8A_REF_LAST ? bb(t, 128, 0)
-                         : id == VP8A_REF_GOLDEN ? bb(t, 128, 1) + bb(t, 128, 0)
-                                                 : bb(t, 128, 1) + bb(t, 128, 1);
-    lrbits = a.lambda * rbits;
-  }
   uint32_t* dec_slot = (uint32_t*)cl.map_shared_rank(&decs[k], 0);
   const int* abort0 = cl.map_shared_rank(&s_abort, 0);
+  if (tid == 0) s_mvb_src = nullptr;
+  const int n_it = BATCH ? n_items : a0.mb_rows;
+  int cur = -1;
 
-  for (int r = cid; r < a.mb_rows; r += n_clusters) {
+  for (int it = cid; it < n_it; it += n_clusters) {
+    int r = it, job = 0;
+    if (BATCH) {
+      const uint32_t w = items[it];
+      job = (int)(w >> 16);
+      r = (int)(w & 0xffffu);
+    }
+    if (job != cur) {
+      // Load the job and its per-job constants. The barrier first: the
+      // previous MB's last writes still read the old job's pointers.
+      __syncthreads();
+      if (tid == 0) a = BATCH ? jobs[job] : a0;
+      __syncthreads();
+      for (int i = tid; i < 256; i += AN_THREADS) bit_cost[i] = a.bit_cost[i];
+      if (s_mvb_src != a.mvbits)
+        for (int i = tid; i < 2 * MV_BITS_SPAN; i += AN_THREADS) mvb[i] = a.mvbits[i];
+      __syncthreads();
+      if (tid < 20) {
+        const double b = submv_ref_bits(bit_cost, c_submv_probs[tid >> 2], tid & 3);
+        sbits[tid] = b;
+        lterm[tid] = a.lambda * (b + 0.0);
+      } else if (tid < 24) {
+        pbits[tid - 20] = mv_partition_bits(bit_cost, tid - 20);
+      } else if (tid == 24) {
+        // lambda * ref_frame_tree_bits(ref, 128, 128) (src/encoder.rs:9108).
+        const double* t = bit_cost;
+        const uint8_t id = a.ref_ids[k];
+        const double rbits = id == VP8A_REF_LAST ? bb(t, 128, 0)
+                             : id == VP8A_REF_GOLDEN ? bb(t, 128, 1) + bb(t, 128, 0)
+                                                     : bb(t, 128, 1) + bb(t, 128, 1);
+        lrbits = a.lambda * rbits;
+      } else if (tid == 32) {
+        s_mvb_src = a.mvbits;
+      }
+      __syncthreads();
+      cur = job;
+    }
     for (int c = 0; c < a.mb_cols; c++) {
       // Rank 0 waits for the row above; the cluster follows its verdict.
       if (k == 0 && tid == 0) {
@@ -1266,11 +1302,26 @@ __global__ void __launch_bounds__(AN_THREADS, 1) analysis_kernel(AnArgs a) {
 
 }  // namespace
 
-extern "C" vp8a_status vp8a_analyse_inter_frame(vp8a_ctx* ctx, const vp8a_i420* frame, const vp8a_planes* refs,
-                                                const uint8_t* ref_ids, uint32_t n_refs,
-                                                const vp8a_mv_contexts* mv_contexts, double lambda,
-                                                vp8a_mb_decision* decisions, vp8a_ref_search* trace) {
-  if (!ctx || !frame || !refs || !ref_ids || !decisions) {
+namespace {
+
+const uint8_t kDefaultMvContexts[2][19] = {
+    {162, 128, 225, 146, 172, 147, 214, 39, 156, 128, 129, 132, 75, 145, 178, 206, 239, 254, 254},
+    {164, 128, 204, 170, 119, 235, 140, 230, 228, 128, 130, 130, 74, 148, 180, 203, 236, 254, 254}};
+
+// mv_component_bits tables already built by this call, one per distinct
+// set of MV contexts.
+struct MvBitsCache {
+  std::vector<std::pair<vp8a_mv_contexts, const double*>> tables;
+};
+
+// Validate one frame's arguments and fill its kernel arguments: inputs
+// staged, scratch (census records, row progress) allocated, progress
+// counters cleared, the mv_component_bits table built or shared.
+vp8a_status prepare_job(vp8a_ctx* ctx, vp8a::Stager& st, MvBitsCache& mc, const vp8a_i420* frame,
+                        const vp8a_planes* refs, const uint8_t* ref_ids, uint32_t n_refs,
+                        const vp8a_mv_contexts* mv_contexts, double lambda, vp8a_mb_decision* decisions,
+                        vp8a_ref_search* trace, AnArgs* out) {
+  if (!frame || !refs || !ref_ids || !decisions) {
     vp8a::set_error("null argument");
     return VP8A_E_INVALID_ARGUMENT;
   }
@@ -1283,19 +1334,16 @@ extern "C" vp8a_status vp8a_analyse_inter_frame(vp8a_ctx* ctx, const vp8a_i420* 
     return VP8A_E_INVALID_ARGUMENT;
   }
   const int mb_cols = (int)((frame->width + 15) / 16), mb_rows = (int)((frame->height + 15) / 16);
-  VP8A_CUDA(cudaSetDevice(ctx->device));
-  vp8a::Stager st(ctx);
   vp8a_status s;
   // The reference ids steer host-side validation; fetch them wherever they live.
   uint8_t ids[MAX_REFS];
   if ((s = st.read_to_host(ref_ids, n_refs, ids)) != VP8A_OK) return s;
-  ref_ids = ids;
   for (uint32_t k = 0; k < n_refs; k++) {
     if ((int)refs[k].mb_cols != mb_cols || (int)refs[k].mb_rows != mb_rows) {
       vp8a::set_error("reference planes do not match the frame's MB grid");
       return VP8A_E_REFERENCE_DIMENSIONS_MISMATCH;
     }
-    if (ref_ids[k] < VP8A_REF_LAST || ref_ids[k] > VP8A_REF_ALTREF || !refs[k].y ||
+    if (ids[k] < VP8A_REF_LAST || ids[k] > VP8A_REF_ALTREF || !refs[k].y ||
         refs[k].y_stride < (uint64_t)mb_cols * 16) {
       vp8a::set_error("bad reference id, plane or stride");
       return VP8A_E_INVALID_ARGUMENT;
@@ -1319,29 +1367,30 @@ extern "C" vp8a_status vp8a_analyse_inter_frame(vp8a_ctx* ctx, const vp8a_i420* 
     a.refs[k].stride = refs[k].y_stride;
     a.refs[k].width = mb_cols * 16;
     a.refs[k].height = mb_rows * 16;
-    a.ref_ids[k] = ref_ids[k];
+    a.ref_ids[k] = ids[k];
   }
   a.n_refs = (int)n_refs;
   a.mb_cols = mb_cols;
   a.mb_rows = mb_rows;
-  if (mv_contexts) {
-    a.ctx = *mv_contexts;
-  } else {
-    static const uint8_t dflt[2][19] = {
-        {162, 128, 225, 146, 172, 147, 214, 39, 156, 128, 129, 132, 75, 145, 178, 206, 239, 254, 254},
-        {164, 128, 204, 170, 119, 235, 140, 230, 228, 128, 130, 130, 74, 148, 180, 203, 236, 254, 254}};
-    memcpy(a.ctx.p, dflt, sizeof dflt);
-  }
+  if (mv_contexts) a.ctx = *mv_contexts;
+  else memcpy(a.ctx.p, kDefaultMvContexts, sizeof kDefaultMvContexts);
   a.lambda = lambda;
   a.bit_cost = ctx->d_bit_cost;
+  a.mvbits = nullptr;
+  for (const auto& e : mc.tables)
+    if (memcmp(&e.first, &a.ctx, sizeof a.ctx) == 0) a.mvbits = e.second;
+  if (!a.mvbits) {
+    void* dmvb;
+    if ((s = st.scratch(sizeof(double) * 2 * MV_BITS_SPAN, &dmvb)) != VP8A_OK) return s;
+    mv_bits_table_kernel<<<(2 * MV_BITS_SPAN + 255) / 256, 256, 0, ctx->stream>>>(ctx->d_bit_cost, a.ctx,
+                                                                                 (double*)dmvb);
+    VP8A_CUDA(cudaGetLastError());
+    ctx->launches++;
+    a.mvbits = (const double*)dmvb;
+    mc.tables.emplace_back(a.ctx, a.mvbits);
+  }
   const size_t nmb = (size_t)mb_cols * mb_rows;
-  void *dinfo, *dprog, *ddec, *dtr = nullptr, *dmvb;
-  if ((s = st.scratch(sizeof(double) * 2 * MV_BITS_SPAN, &dmvb)) != VP8A_OK) return s;
-  mv_bits_table_kernel<<<(2 * MV_BITS_SPAN + 255) / 256, 256, 0, ctx->stream>>>(ctx->d_bit_cost, a.ctx,
-                                                                               (double*)dmvb);
-  VP8A_CUDA(cudaGetLastError());
-  ctx->launches++;
-  a.mvbits = (const double*)dmvb;
+  void *dinfo, *dprog, *ddec, *dtr = nullptr;
   if ((s = st.scratch(sizeof(MbInfoDev) * nmb, &dinfo)) != VP8A_OK) return s;
   if ((s = st.scratch(sizeof(unsigned) * mb_rows, &dprog)) != VP8A_OK) return s;
   VP8A_CUDA(cudaMemsetAsync(dprog, 0, sizeof(unsigned) * mb_rows, ctx->stream));
@@ -1356,17 +1405,27 @@ extern "C" vp8a_status vp8a_analyse_inter_frame(vp8a_ctx* ctx, const vp8a_i420* 
   a.words = 1;
   for (uint32_t k = 0; k < n_refs; k++)
     if ((uintptr_t)a.refs[k].plane % 4 != 0 || a.refs[k].stride % 4 != 0) a.words = 0;
+  *out = a;
+  return VP8A_OK;
+}
+
+// One launch over `n_items` MB rows with n_refs-CTA clusters: the frame a0
+// (batch false) or the items of the job table (batch true).
+template <bool BATCH>
+vp8a_status launch_analysis(vp8a_ctx* ctx, int n_refs, const AnArgs& a0, const AnArgs* djobs,
+                            const uint32_t* ditems, int n_items) {
   // One CTA per reference, the references of one MB row in one thread-block
   // cluster; the shared-memory request keeps one CTA per SM so that the
   // reference searches of an MB do not compete for issue slots.
+  auto kern = analysis_kernel<BATCH>;
   cudaFuncAttributes fa;
-  VP8A_CUDA(cudaFuncGetAttributes(&fa, analysis_kernel));
+  VP8A_CUDA(cudaFuncGetAttributes(&fa, kern));
   int smem_sm = 0;
   VP8A_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
   const int dyn = (int)(4 * sizeof(SplitScratch) + 2 * MV_BITS_SPAN * sizeof(double));
   const int pad = std::max(dyn, smem_sm / 2 + 1 - (int)fa.sharedSizeBytes);
-  VP8A_CUDA(cudaFuncSetAttribute(analysis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, pad));
-  VP8A_CUDA(cudaFuncSetAttribute(analysis_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 0));
+  VP8A_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, pad));
+  VP8A_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 0));
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
   attr[0].val.clusterDim.x = n_refs;
@@ -1378,20 +1437,95 @@ extern "C" vp8a_status vp8a_analyse_inter_frame(vp8a_ctx* ctx, const vp8a_i420* 
   cfg.stream = ctx->stream;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cfg.gridDim = dim3(n_refs * (unsigned)mb_rows);
+  cfg.gridDim = dim3(n_refs * (unsigned)n_items);
   int max_clusters = 0;
-  VP8A_CUDA(cudaOccupancyMaxActiveClusters(&max_clusters, analysis_kernel, &cfg));
+  VP8A_CUDA(cudaOccupancyMaxActiveClusters(&max_clusters, kern, &cfg));
   if (max_clusters < 1) {
     vp8a::set_error("analysis kernel cannot be resident");
     return VP8A_E_CUDA;
   }
-  // Every cluster must be resident at once: rows are handed out round-robin
-  // and a row waits on the one above it.
-  const int n_clusters = std::min(mb_rows, max_clusters);
+  // Every cluster must be resident at once: items are handed out
+  // round-robin and a row waits on the one above it.
+  const int n_clusters = std::min(n_items, max_clusters);
   cfg.gridDim = dim3(n_refs * (unsigned)n_clusters);
-  VP8A_CUDA(cudaLaunchKernelEx(&cfg, analysis_kernel, a));
+  VP8A_CUDA(cudaLaunchKernelEx(&cfg, kern, a0, djobs, ditems, n_items));
   VP8A_CUDA(cudaGetLastError());
   ctx->launches++;
+  return VP8A_OK;
+}
+
+}  // namespace
+
+extern "C" vp8a_status vp8a_analyse_inter_frame(vp8a_ctx* ctx, const vp8a_i420* frame, const vp8a_planes* refs,
+                                                const uint8_t* ref_ids, uint32_t n_refs,
+                                                const vp8a_mv_contexts* mv_contexts, double lambda,
+                                                vp8a_mb_decision* decisions, vp8a_ref_search* trace) {
+  if (!ctx) {
+    vp8a::set_error("null argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  MvBitsCache mc;
+  AnArgs a{};
+  vp8a_status s = prepare_job(ctx, st, mc, frame, refs, ref_ids, n_refs, mv_contexts, lambda, decisions, trace, &a);
+  if (s != VP8A_OK) return s;
+  if ((s = launch_analysis<false>(ctx, a.n_refs, a, nullptr, nullptr, a.mb_rows)) != VP8A_OK) return s;
+  if ((s = vp8a::check_device_status(ctx)) != VP8A_OK) return s;
+  return st.finish();
+}
+
+extern "C" vp8a_status vp8a_analyse_inter_frames(vp8a_ctx* ctx, const vp8a_analysis_job* jobs, uint32_t n_jobs) {
+  if (!ctx || (!jobs && n_jobs)) {
+    vp8a::set_error("null argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (n_jobs > VP8A_MAX_BATCH_JOBS) {
+    vp8a::set_error("more jobs than VP8A_MAX_BATCH_JOBS");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (n_jobs == 0) return VP8A_OK;
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  MvBitsCache mc;
+  std::vector<AnArgs> args(n_jobs);
+  vp8a_status s;
+  for (uint32_t j = 0; j < n_jobs; j++) {
+    const vp8a_analysis_job& J = jobs[j];
+    if ((s = prepare_job(ctx, st, mc, &J.frame, J.refs, J.ref_ids, J.n_refs, J.mv_contexts, J.lambda,
+                         J.decisions, J.trace, &args[j])) != VP8A_OK)
+      return s;
+  }
+  // One launch per reference count (the cluster size). Within a launch the
+  // jobs with the longest wavefront (mb_cols + 2 mb_rows MB steps) come
+  // first, so that they start while the short ones fill in behind them.
+  for (int nr = 1; nr <= MAX_REFS; nr++) {
+    std::vector<uint32_t> order;
+    for (uint32_t j = 0; j < n_jobs; j++)
+      if (args[j].n_refs == nr) order.push_back(j);
+    if (order.empty()) continue;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+      return args[x].mb_cols + 2 * args[x].mb_rows > args[y].mb_cols + 2 * args[y].mb_rows;
+    });
+    std::vector<AnArgs> table;
+    std::vector<uint32_t> items;
+    for (uint32_t j : order) {
+      const uint32_t q = (uint32_t)table.size();
+      table.push_back(args[j]);
+      for (int r = 0; r < args[j].mb_rows; r++) items.push_back(q << 16 | (uint32_t)r);
+    }
+    void *dt, *di;
+    if ((s = st.scratch(sizeof(AnArgs) * table.size(), &dt)) != VP8A_OK) return s;
+    if ((s = st.scratch(sizeof(uint32_t) * items.size(), &di)) != VP8A_OK) return s;
+    VP8A_CUDA(cudaMemcpyAsync(dt, table.data(), sizeof(AnArgs) * table.size(), cudaMemcpyHostToDevice, ctx->stream));
+    VP8A_CUDA(cudaMemcpyAsync(di, items.data(), sizeof(uint32_t) * items.size(), cudaMemcpyHostToDevice,
+                              ctx->stream));
+    // The host tables go out of scope with this iteration.
+    VP8A_CUDA(cudaStreamSynchronize(ctx->stream));
+    if ((s = launch_analysis<true>(ctx, nr, table[0], (const AnArgs*)dt, (const uint32_t*)di, (int)items.size())) !=
+        VP8A_OK)
+      return s;
+  }
   if ((s = vp8a::check_device_status(ctx)) != VP8A_OK) return s;
   return st.finish();
 }

@@ -17,7 +17,10 @@
 //    exactly one chroma block (block k covers [8k, 8k + ceil(bw/2)) and
 //    ceil((bx+bw)/2) <= ceil(w/2)), so the clamped-overhang branch of
 //    accumulate_chroma_block never adds a second contribution.
+#include <algorithm>
 #include <climits>
+#include <cstring>
+#include <vector>
 
 #include "vp8a_internal.cuh"
 
@@ -68,13 +71,13 @@ constexpr int SWW = SWS / 4;                // words per staged row
 // and its 16 source rows of the centre frame are staged once as 32-bit
 // words; warp j then runs refine_search for block j of the strip on the
 // staged window.
-__global__ void __launch_bounds__(STRIP * 32) arnr_search_kernel(SearchArgs a) {
+__device__ __forceinline__ void search_body(const SearchArgs& a, uint32_t bid) {
   __shared__ __align__(16) uint8_t win[AW * SWS + 16];
   __shared__ __align__(16) uint8_t srcs[16 * STRIP * 16];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int strips = (a.bcols + STRIP - 1) / STRIP;
-  uint32_t fi = blockIdx.x / ((uint32_t)strips * a.brows);
-  const uint32_t rest = blockIdx.x % ((uint32_t)strips * a.brows);
+  uint32_t fi = bid / ((uint32_t)strips * a.brows);
+  const uint32_t rest = bid % ((uint32_t)strips * a.brows);
   if (fi >= a.center) fi++;  // skip the centre frame
   const int brow = (int)(rest / strips), strip = (int)(rest % strips);
   const int bx0 = strip * STRIP * 16, by = brow * 16;
@@ -188,6 +191,16 @@ __global__ void __launch_bounds__(STRIP * 32) arnr_search_kernel(SearchArgs a) {
   }
 }
 
+__global__ void __launch_bounds__(STRIP * 32) arnr_search_kernel(SearchArgs a) { search_body(a, blockIdx.x); }
+
+__global__ void __launch_bounds__(STRIP * 32)
+    arnr_search_batch_kernel(const SearchArgs* __restrict__ jobs, const uint32_t* __restrict__ cta_start, int n_jobs) {
+  __shared__ SearchArgs sa;
+  __shared__ uint32_t first[2];
+  find_job(jobs, cta_start, n_jobs, &sa, first);
+  search_body(sa, blockIdx.x - first[0]);
+}
+
 struct BlendArgs {
   const ArnrFrame* frames;
   const BlockMv* mv;
@@ -237,7 +250,8 @@ __device__ __forceinline__ uint32_t udiv_small(uint32_t a, uint32_t d) {
 // past BLEND_MAX_FRAMES are read from global memory).
 constexpr int BLEND_MAX_FRAMES = 32;
 
-__global__ void __launch_bounds__(BLEND_THREADS) arnr_blend_kernel(BlendArgs a) {
+// CTA `cta` of the `ncta` that blend job `a` (grid-stride over its blocks).
+__device__ __forceinline__ void blend_body(const BlendArgs& a, uint32_t cta, uint32_t ncta) {
   __shared__ uint32_t wt[256];
   __shared__ int2 smv[BLEND_BLOCKS][BLEND_MAX_FRAMES];  // (mvx, mvy); mvx = INT_MIN: frame not used
   for (int d = threadIdx.x; d < 256; d += blockDim.x)
@@ -246,7 +260,7 @@ __global__ void __launch_bounds__(BLEND_THREADS) arnr_blend_kernel(BlendArgs a) 
   const uint32_t nblk = (uint32_t)a.bcols * a.brows;
   const ArnrFrame c = a.frames[a.center];
   const uint32_t nst = min(a.n, (uint32_t)BLEND_MAX_FRAMES);
-  for (uint32_t b0 = blockIdx.x * BLEND_BLOCKS; b0 < nblk; b0 += gridDim.x * BLEND_BLOCKS) {
+  for (uint32_t b0 = cta * BLEND_BLOCKS; b0 < nblk; b0 += ncta * BLEND_BLOCKS) {
     const uint32_t b = b0 + g;
     const int bcol = (int)(b % (uint32_t)a.bcols), brow = (int)(b / (uint32_t)a.bcols);
     // Occlusion guard: sad / (bw * bh) > 12 (BLOCK_SAD_PER_PIXEL_CUTOFF)
@@ -331,12 +345,35 @@ __global__ void __launch_bounds__(BLEND_THREADS) arnr_blend_kernel(BlendArgs a) 
   }
 }
 
+__global__ void __launch_bounds__(BLEND_THREADS) arnr_blend_kernel(BlendArgs a) {
+  blend_body(a, blockIdx.x, gridDim.x);
+}
+
+__global__ void __launch_bounds__(BLEND_THREADS)
+    arnr_blend_batch_kernel(const BlendArgs* __restrict__ jobs, const uint32_t* __restrict__ cta_start, int n_jobs) {
+  __shared__ BlendArgs sa;
+  __shared__ uint32_t first[2];
+  find_job(jobs, cta_start, n_jobs, &sa, first);
+  blend_body(sa, blockIdx.x - first[0], first[1]);
+}
+
 }  // namespace
 
-extern "C" vp8a_status vp8a_build_arnr_altref(vp8a_ctx* ctx, const vp8a_i420* frames, uint32_t n,
-                                              uint32_t center, uint32_t strength, uint8_t* y_out,
-                                              uint8_t* u_out, uint8_t* v_out) {
-  if (!ctx || !frames || !y_out || !u_out || !v_out) {
+namespace {
+
+// One ARNR job prepared: inputs staged, the kernels' arguments, and their
+// CTA counts (no search when the window does not filter).
+struct ArnrPrepared {
+  SearchArgs sa;
+  BlendArgs ba;
+  uint32_t search_ctas, blend_ctas;
+};
+
+// `hf` holds the host copy of the frame table until the call's finish().
+vp8a_status prepare_arnr(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_i420* frames, uint32_t n, uint32_t center,
+                         uint32_t strength, uint8_t* y_out, uint8_t* u_out, uint8_t* v_out,
+                         std::vector<ArnrFrame>& hf, ArnrPrepared* P) {
+  if (!frames || !y_out || !u_out || !v_out) {
     vp8a::set_error("null argument");
     return VP8A_E_INVALID_ARGUMENT;
   }
@@ -361,10 +398,8 @@ extern "C" vp8a_status vp8a_build_arnr_altref(vp8a_ctx* ctx, const vp8a_i420* fr
       vp8a::set_error("frame planes missing or stride below width");
       return VP8A_E_INVALID_ARGUMENT;
     }
-  VP8A_CUDA(cudaSetDevice(ctx->device));
-  vp8a::Stager st(ctx);
   vp8a_status s;
-  std::vector<ArnrFrame> hf(n);
+  hf.assign(n, ArnrFrame{});
   for (uint32_t i = 0; i < n; i++) {
     const void* d;
     size_t yb = frames[i].y_stride * (size_t)(h - 1) + w, cb = frames[i].uv_stride * (size_t)(ch - 1) + cw;
@@ -380,7 +415,7 @@ extern "C" vp8a_status vp8a_build_arnr_altref(vp8a_ctx* ctx, const vp8a_i420* fr
   void* dframes = nullptr;
   if ((s = st.scratch(sizeof(ArnrFrame) * n, &dframes)) != VP8A_OK) return s;
   VP8A_CUDA(cudaMemcpyAsync(dframes, hf.data(), sizeof(ArnrFrame) * n, cudaMemcpyHostToDevice, ctx->stream));
-  st.force_sync();  // hf must outlive the copy
+  st.force_sync();  // finish() waits for the copy before hf goes
   void *dy, *du, *dv;
   if ((s = st.out(y_out, (size_t)w * h, &dy)) != VP8A_OK) return s;
   if ((s = st.out(u_out, (size_t)cw * ch, &du)) != VP8A_OK) return s;
@@ -391,34 +426,108 @@ extern "C" vp8a_status vp8a_build_arnr_altref(vp8a_ctx* ctx, const vp8a_i420* fr
   const uint32_t str = strength > 6 ? 6 : strength;
   void* dmv = nullptr;
   if ((s = st.scratch(sizeof(BlockMv) * (size_t)n * bcols * brows, &dmv)) != VP8A_OK) return s;
-  if (filter) {
-    int aligned = 1;
-    for (uint32_t i = 0; i < n; i++) aligned &= (((uintptr_t)hf[i].y | hf[i].y_stride) & 3) == 0;
-    SearchArgs sa{(const ArnrFrame*)dframes, n, center, w, h, bcols, brows, aligned, (BlockMv*)dmv};
-    const size_t ctas = (size_t)((bcols + STRIP - 1) / STRIP) * brows * (n - 1);
-    arnr_search_kernel<<<(unsigned)ctas, STRIP * 32, 0, ctx->stream>>>(sa);
-    VP8A_CUDA(cudaGetLastError());
-    ctx->launches++;
-  }
+  int aligned = 1;
+  for (uint32_t i = 0; i < n; i++) aligned &= (((uintptr_t)hf[i].y | hf[i].y_stride) & 3) == 0;
+  P->sa = SearchArgs{(const ArnrFrame*)dframes, n, center, w, h, bcols, brows, aligned, (BlockMv*)dmv};
+  P->search_ctas = filter ? (uint32_t)((bcols + STRIP - 1) / STRIP) * brows * (n - 1) : 0u;
   int aligned_in = 1;
   for (uint32_t i = 0; i < n; i++)
     aligned_in &= (((uintptr_t)hf[i].y | (uintptr_t)hf[i].u | (uintptr_t)hf[i].v | hf[i].y_stride |
                      hf[i].uv_stride) & 3) == 0;
   const int aligned_out = (((uintptr_t)dy | (uintptr_t)du | (uintptr_t)dv | (uintptr_t)w | (uintptr_t)cw) & 3) == 0;
-  BlendArgs ba{(const ArnrFrame*)dframes, (const BlockMv*)dmv, filter ? n : 0u, filter ? center : 0u,
-               8u << str, w, h, cw, ch, bcols, brows, aligned_in, aligned_out,
-               (uint8_t*)dy, (uint8_t*)du, (uint8_t*)dv};
+  P->ba = BlendArgs{(const ArnrFrame*)dframes, (const BlockMv*)dmv, filter ? n : 0u, filter ? center : 0u,
+                    8u << str, w, h, cw, ch, bcols, brows, aligned_in, aligned_out,
+                    (uint8_t*)dy, (uint8_t*)du, (uint8_t*)dv};
   if (!filter) {
     // Pass-through (src/arnr.rs:527-529): the blend with no window frames
     // reproduces the centre exactly. The centre is frames[0] of a
     // one-entry view.
-    ba.frames = (const ArnrFrame*)dframes + center;
-    ba.n = 1;
-    ba.center = 0;
+    P->ba.frames = (const ArnrFrame*)dframes + center;
+    P->ba.n = 1;
+    P->ba.center = 0;
   }
   const size_t nblk = (size_t)bcols * brows;
-  unsigned grid = (unsigned)std::min<size_t>(vp8a::grid_for(nblk, BLEND_BLOCKS), (size_t)ctx->sm_count * 16);
-  arnr_blend_kernel<<<grid, BLEND_THREADS, 0, ctx->stream>>>(ba);
+  P->blend_ctas = (uint32_t)std::min<size_t>(vp8a::grid_for(nblk, BLEND_BLOCKS), (size_t)ctx->sm_count * 16);
+  return VP8A_OK;
+}
+
+}  // namespace
+
+extern "C" vp8a_status vp8a_build_arnr_altref(vp8a_ctx* ctx, const vp8a_i420* frames, uint32_t n,
+                                              uint32_t center, uint32_t strength, uint8_t* y_out,
+                                              uint8_t* u_out, uint8_t* v_out) {
+  if (!ctx) {
+    vp8a::set_error("null argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  ArnrPrepared P;
+  std::vector<ArnrFrame> hf;
+  vp8a_status s = prepare_arnr(ctx, st, frames, n, center, strength, y_out, u_out, v_out, hf, &P);
+  if (s != VP8A_OK) return s;
+  if (P.search_ctas) {
+    arnr_search_kernel<<<P.search_ctas, STRIP * 32, 0, ctx->stream>>>(P.sa);
+    VP8A_CUDA(cudaGetLastError());
+    ctx->launches++;
+  }
+  arnr_blend_kernel<<<P.blend_ctas, BLEND_THREADS, 0, ctx->stream>>>(P.ba);
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
+  return st.finish();
+}
+
+extern "C" vp8a_status vp8a_build_arnr_altrefs(vp8a_ctx* ctx, const vp8a_arnr_job* jobs, uint32_t n_jobs) {
+  if (!ctx || (!jobs && n_jobs)) {
+    vp8a::set_error("null argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (n_jobs > VP8A_MAX_BATCH_JOBS) {
+    vp8a::set_error("more jobs than VP8A_MAX_BATCH_JOBS");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (n_jobs == 0) return VP8A_OK;
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  vp8a_status s;
+  std::vector<SearchArgs> sj;
+  std::vector<BlendArgs> bj;
+  std::vector<uint32_t> s_start{0}, b_start{0};
+  std::vector<std::vector<ArnrFrame>> hf(n_jobs);
+  for (uint32_t j = 0; j < n_jobs; j++) {
+    const vp8a_arnr_job& J = jobs[j];
+    ArnrPrepared P;
+    if ((s = prepare_arnr(ctx, st, J.frames, J.n, J.center, J.strength, J.y_out, J.u_out, J.v_out, hf[j], &P)) !=
+        VP8A_OK)
+      return s;
+    if (P.search_ctas) {
+      sj.push_back(P.sa);
+      s_start.push_back(s_start.back() + P.search_ctas);
+    }
+    bj.push_back(P.ba);
+    b_start.push_back(b_start.back() + P.blend_ctas);
+  }
+  // Job tables: search args, search CTA offsets, blend args, blend CTA offsets.
+  const size_t o_ss = sizeof(SearchArgs) * sj.size(), o_ba = (o_ss + sizeof(uint32_t) * s_start.size() + 15) & ~15,
+               o_bs = o_ba + sizeof(BlendArgs) * bj.size(), total = o_bs + sizeof(uint32_t) * b_start.size();
+  std::vector<uint8_t> blob(total, 0);
+  if (!sj.empty()) memcpy(blob.data(), sj.data(), o_ss);
+  memcpy(blob.data() + o_ss, s_start.data(), sizeof(uint32_t) * s_start.size());
+  memcpy(blob.data() + o_ba, bj.data(), sizeof(BlendArgs) * bj.size());
+  memcpy(blob.data() + o_bs, b_start.data(), sizeof(uint32_t) * b_start.size());
+  void* d;
+  if ((s = st.scratch(total, &d)) != VP8A_OK) return s;
+  VP8A_CUDA(cudaMemcpyAsync(d, blob.data(), total, cudaMemcpyHostToDevice, ctx->stream));
+  VP8A_CUDA(cudaStreamSynchronize(ctx->stream));  // the host blob goes out of scope
+  const uint8_t* db = (const uint8_t*)d;
+  if (!sj.empty()) {
+    arnr_search_batch_kernel<<<s_start.back(), STRIP * 32, 0, ctx->stream>>>(
+        (const SearchArgs*)db, (const uint32_t*)(db + o_ss), (int)sj.size());
+    VP8A_CUDA(cudaGetLastError());
+    ctx->launches++;
+  }
+  arnr_blend_batch_kernel<<<b_start.back(), BLEND_THREADS, 0, ctx->stream>>>(
+      (const BlendArgs*)(db + o_ba), (const uint32_t*)(db + o_bs), (int)bj.size());
   VP8A_CUDA(cudaGetLastError());
   ctx->launches++;
   return st.finish();

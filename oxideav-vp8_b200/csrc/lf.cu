@@ -505,6 +505,8 @@ __device__ __forceinline__ void prefetch_mb(const LfArgs& a, Stage* g, int r, in
 // reconstruction and the source under the MB finished in its slot) are
 // issued together before the slot is touched.
 // SSD totals of the CTA's candidates into the table.
+// A sweep-mode level-0 candidate's SSD is stored for every sharpness
+// (level 0 scores the unfiltered planes whatever the sharpness).
 template <int NC>
 __device__ __forceinline__ void block_sums_store(const uint64_t (&v)[NC], const LfArgs& a, const int (&lv)[NC],
                                                  const int (&sh)[NC], int nc) {
@@ -523,7 +525,11 @@ __device__ __forceinline__ void block_sums_store(const uint64_t (&v)[NC], const 
     uint64_t x = lane < nwarps ? red[k][lane] : 0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(FULL, x, o);
-    if (lane == 0) a.ssd_out[lv[k] * 8 + sh[k]] = x;
+    if (lv[k] == 0 && a.level0_unfiltered) {
+      if (lane < 8) a.ssd_out[lane] = x;
+    } else if (lane == 0) {
+      a.ssd_out[lv[k] * 8 + sh[k]] = x;
+    }
   }
 }
 
@@ -533,11 +539,11 @@ __device__ __forceinline__ void block_sums_store(const uint64_t (&v)[NC], const 
 // the unfiltered reconstruction (score_filter_candidate's short cut,
 // src/loop_filter.rs:2071).
 template <int NC>
-__global__ void __launch_bounds__(1024) lf_sweep_kernel(LfArgs a) {
+__device__ __forceinline__ void sweep_body(const LfArgs& a, int cta) {
   extern __shared__ __align__(16) uint8_t smem_slots[];
   const int hw = threadIdx.x >> 4, nhw = blockDim.x >> 4, l = threadIdx.x & 15;
   const unsigned hm = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
-  const int first = blockIdx.x * NC, nc = min(NC, a.n_cands - first);
+  const int first = cta * NC, nc = min(NC, a.n_cands - first);
   int lv[NC], sh[NC];
   bool filt[NC];
   uint64_t acc[NC];
@@ -642,6 +648,21 @@ __global__ void __launch_bounds__(1024) lf_sweep_kernel(LfArgs a) {
       if (k < nc) acc[k] += finish_mb(a, slots[k], r, c, l, sw);
   }
   if (score) block_sums_store<NC>(acc, a, lv, sh, nc);
+}
+
+template <int NC>
+__global__ void __launch_bounds__(1024) lf_sweep_kernel(LfArgs a) {
+  sweep_body<NC>(a, blockIdx.x);
+}
+
+// Many pictures' sweeps in one launch: CTA offsets per job as in find_job.
+template <int NC>
+__global__ void __launch_bounds__(1024)
+    lf_sweep_batch_kernel(const LfArgs* __restrict__ jobs, const uint32_t* __restrict__ cta_start, int n_jobs) {
+  __shared__ LfArgs sa;
+  __shared__ uint32_t first[2];
+  find_job(jobs, cta_start, n_jobs, &sa, first);
+  sweep_body<NC>(sa, (int)(blockIdx.x - first[0]));
 }
 
 // Plain visible-window SSD of a reconstruction (reconstruction_ssd).
@@ -1078,9 +1099,122 @@ vp8a_status vp8a_filter_sweep(vp8a_ctx* ctx, const vp8a_planes* planes, const vp
       c.push_back((uint8_t)sh);
     }
   if ((s = launch_sweep(ctx, st, L.a, c.data(), (int)(c.size() / 2))) != VP8A_OK) return s;
-  // Level 0 scores the same for every sharpness.
-  for (int sh = 1; sh < 8; sh++)
-    VP8A_CUDA(cudaMemcpyAsync((uint64_t*)dt + sh, dt, sizeof(uint64_t), cudaMemcpyDeviceToDevice, ctx->stream));
+  st.force_sync();  // the candidate vector must outlive its async copy
+  return st.finish();
+}
+
+vp8a_status vp8a_filter_sweeps(vp8a_ctx* ctx, const vp8a_sweep_job* jobs, uint32_t n_jobs) {
+  if (!ctx || (!jobs && n_jobs)) {
+    vp8a::set_error("null argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (n_jobs > VP8A_MAX_BATCH_JOBS) {
+    vp8a::set_error("more jobs than VP8A_MAX_BATCH_JOBS");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (n_jobs == 0) return VP8A_OK;
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  vp8a_status s;
+  // The whole grid's candidates, shared by every job.
+  std::vector<uint8_t> c{0, 0};
+  for (int l = 1; l < 64; l++)
+    for (int sh = 0; sh < 8; sh++) {
+      c.push_back((uint8_t)l);
+      c.push_back((uint8_t)sh);
+    }
+  const int n_c = (int)(c.size() / 2);
+  void* dc;
+  if ((s = st.scratch(c.size(), &dc)) != VP8A_OK) return s;
+  VP8A_CUDA(cudaMemcpyAsync(dc, c.data(), c.size(), cudaMemcpyHostToDevice, ctx->stream));
+  std::vector<LfArgs> args(n_jobs);
+  for (uint32_t j = 0; j < n_jobs; j++) {
+    const vp8a_sweep_job& J = jobs[j];
+    if (!J.ssd_out) {
+      vp8a::set_error("null ssd_out");
+      return VP8A_E_INVALID_ARGUMENT;
+    }
+    LfInputs L;
+    if ((s = stage_lf(ctx, st, &J.planes, J.mbs, &J.base, &J.src, J.every_rows, false, &L)) != VP8A_OK) return s;
+    void* dt;
+    if ((s = st.out(J.ssd_out, 512 * sizeof(uint64_t), &dt)) != VP8A_OK) return s;
+    L.a.ssd_out = (uint64_t*)dt;
+    L.a.level0_unfiltered = 1;
+    L.a.cands = (const uint8_t*)dc;
+    L.a.n_cands = n_c;
+    L.a.ring_bytes = L.a.mb_rows * RING * SLOT_STRIDE;
+    args[j] = L.a;
+  }
+  // One launch for every job whose slot rings fit in shared memory (two
+  // candidates per CTA when the largest job's pair fits, else one), with
+  // the most half-warps any job needs; the rest run as their own launches.
+  int max_smem = 0;
+  VP8A_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+  cudaFuncAttributes f1, f2;
+  VP8A_CUDA(cudaFuncGetAttributes(&f1, lf_sweep_batch_kernel<1>));
+  VP8A_CUDA(cudaFuncGetAttributes(&f2, lf_sweep_batch_kernel<2>));
+  auto al = [](const void* p, uint64_t stride, unsigned k) { return ((uintptr_t)p % k == 0) && (stride % k == 0); };
+  auto threads_of = [](const LfArgs& a) { return std::min(1024, std::max(32, (16 * a.max_active + 31) / 32 * 32)); };
+  auto pre_of = [&](const LfArgs& a) {
+    return al(a.y, a.ys, 16) && al(a.u, a.cs, 8) && al(a.v, a.cs, 8) && (uintptr_t)a.mbs % 8 == 0 &&
+           al(a.sy, a.sys, 16) && al(a.su, a.scs, 8) && al(a.sv, a.scs, 8);
+  };
+  std::vector<uint32_t> group, alone;
+  int threads = 32, max_ring = 0;
+  bool pre = true;
+  for (uint32_t j = 0; j < n_jobs; j++) {
+    const int t = std::max(threads, threads_of(args[j]));
+    const int r = std::max(max_ring, args[j].ring_bytes);
+    const bool p = pre && pre_of(args[j]);
+    const size_t need = (size_t)r + (p ? (size_t)(t / 16) * sizeof(Stage) : 0) + f1.sharedSizeBytes + 1024;
+    if (need > (size_t)max_smem) {
+      alone.push_back(j);
+      continue;
+    }
+    group.push_back(j);
+    threads = t;
+    max_ring = r;
+    pre = p;
+  }
+  if (!group.empty()) {
+    const size_t stage_bytes = pre ? (size_t)(threads / 16) * sizeof(Stage) : 0;
+    const int nc = (size_t)2 * max_ring + stage_bytes + f2.sharedSizeBytes + 1024 <= (size_t)max_smem ? 2 : 1;
+    const size_t total = (size_t)nc * max_ring + stage_bytes;
+    std::vector<LfArgs> table;
+    std::vector<uint32_t> start{0};
+    for (uint32_t j : group) {
+      LfArgs a = args[j];
+      a.smem_slots = 1;
+      a.gslots = nullptr;
+      a.prefetch = pre;
+      a.stage_off = nc * a.ring_bytes;
+      table.push_back(a);
+      start.push_back(start.back() + (uint32_t)((n_c + nc - 1) / nc));
+    }
+    const size_t o_start = sizeof(LfArgs) * table.size(), bytes = o_start + sizeof(uint32_t) * start.size();
+    std::vector<uint8_t> blob(bytes);
+    memcpy(blob.data(), table.data(), o_start);
+    memcpy(blob.data() + o_start, start.data(), sizeof(uint32_t) * start.size());
+    void* d;
+    if ((s = st.scratch(bytes, &d)) != VP8A_OK) return s;
+    VP8A_CUDA(cudaMemcpyAsync(d, blob.data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
+    VP8A_CUDA(cudaStreamSynchronize(ctx->stream));  // the host tables go out of scope
+    const LfArgs* dj = (const LfArgs*)d;
+    const uint32_t* ds = (const uint32_t*)((const uint8_t*)d + o_start);
+    if (nc == 2) {
+      VP8A_CUDA(cudaFuncSetAttribute(lf_sweep_batch_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)total));
+      lf_sweep_batch_kernel<2><<<start.back(), threads, total, ctx->stream>>>(dj, ds, (int)table.size());
+    } else {
+      VP8A_CUDA(cudaFuncSetAttribute(lf_sweep_batch_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)total));
+      lf_sweep_batch_kernel<1><<<start.back(), threads, total, ctx->stream>>>(dj, ds, (int)table.size());
+    }
+    VP8A_CUDA(cudaGetLastError());
+    ctx->launches++;
+  }
+  for (uint32_t j : alone)
+    if ((s = run_sweep(ctx, args[j], n_c, &st)) != VP8A_OK) return s;
   st.force_sync();  // the candidate vector must outlive its async copy
   return st.finish();
 }

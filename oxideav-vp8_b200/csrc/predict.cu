@@ -268,8 +268,9 @@ __device__ __forceinline__ void stage_row(const Job& J, uint8_t* S, int i, const
   }
 }
 
+// CTA `cta` of the `ncta` working on `a` (grid-stride over 8-MB groups).
 template <int MODE>
-__global__ void __launch_bounds__(PR_THREADS) predict_kernel(PredArgs a) {
+__device__ __forceinline__ void predict_body(const PredArgs& a, uint32_t cta, uint32_t ncta) {
   __shared__ __align__(16) uint8_t slots[PR_MBS][SLOT_BYTES];
   __shared__ Job jobs[PR_MBS];
   __shared__ uint32_t tw[8][4][3];  // tap words: [fraction][output shift][window word]
@@ -288,7 +289,7 @@ __global__ void __launch_bounds__(PR_THREADS) predict_kernel(PredArgs a) {
     tw[f][j][q] = w;
   }
 
-  for (uint32_t g = blockIdx.x; (size_t)g * PR_MBS < a.n; g += gridDim.x) {
+  for (uint32_t g = cta; (size_t)g * PR_MBS < a.n; g += ncta) {
     // ---- (1) per-MB vectors: 16 threads per MB, thread b = luma block b.
     {
       const int s = tid >> 4, b = tid & 15;
@@ -445,6 +446,20 @@ __global__ void __launch_bounds__(PR_THREADS) predict_kernel(PredArgs a) {
   }
 }
 
+template <int MODE>
+__global__ void __launch_bounds__(PR_THREADS) predict_kernel(PredArgs a) {
+  predict_body<MODE>(a, blockIdx.x, gridDim.x);
+}
+
+// Frame prediction over a job table (one job per frame).
+__global__ void __launch_bounds__(PR_THREADS)
+    predict_frames_kernel(const PredArgs* __restrict__ jobs, const uint32_t* __restrict__ cta_start, int n_jobs) {
+  __shared__ PredArgs sa;
+  __shared__ uint32_t first[2];
+  vp8a_dev::find_job(jobs, cta_start, n_jobs, &sa, first);
+  predict_body<PRED_FRAME>(sa, blockIdx.x - first[0], first[1]);
+}
+
 int g_pred_blocks_per_sm[3] = {0, 0, 0};
 
 template <int MODE>
@@ -555,7 +570,7 @@ namespace vp8a {
 
 vp8a_status predict_frame(vp8a_ctx* ctx, Stager& st, const vp8a_planes* refs, const uint8_t* ref_ids,
                           uint32_t n_refs, const vp8a_mb_decision* decisions, uint32_t full_pixel,
-                          uint32_t filter_set, const vp8a_planes* out, FramePrediction* fp) {
+                          uint32_t filter_set, const vp8a_planes* out, FramePrediction* fp, bool defer) {
   if (!refs || !ref_ids || !decisions) {
     set_error("null argument");
     return VP8A_E_INVALID_ARGUMENT;
@@ -611,12 +626,48 @@ vp8a_status predict_frame(vp8a_ctx* ctx, Stager& st, const vp8a_planes* refs, co
   a.n = n;
   a.full_pixel = full_pixel != 0;
   a.filter_set = (int)filter_set;
-  if ((s = launch<PRED_FRAME>(ctx, a)) != VP8A_OK) return s;
+  static_assert(sizeof(PredArgs) <= sizeof(fp->args), "FramePrediction holds the launch arguments");
+  memcpy(fp->args, &a, sizeof a);
+  if (!defer && (s = launch<PRED_FRAME>(ctx, a)) != VP8A_OK) return s;
   fp->dec = a.dec;
   fp->planes = *out;
   fp->planes.y = a.oy;
   fp->planes.u = a.ou;
   fp->planes.v = a.ov;
+  return VP8A_OK;
+}
+
+vp8a_status predict_frames(vp8a_ctx* ctx, Stager& st, const FramePrediction* fps, uint32_t n) {
+  std::vector<PredArgs> table;
+  std::vector<uint32_t> start{0};
+  if (!g_pred_blocks_per_sm[PRED_FRAME]) {
+    int b = 0;
+    VP8A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, predict_kernel<PRED_FRAME>, PR_THREADS, 0));
+    g_pred_blocks_per_sm[PRED_FRAME] = std::max(b, 1);
+  }
+  for (uint32_t j = 0; j < n; j++) {
+    PredArgs a;
+    memcpy(&a, fps[j].args, sizeof a);
+    if (a.n == 0) continue;
+    const size_t groups = (a.n + PR_MBS - 1) / PR_MBS;
+    table.push_back(a);
+    start.push_back(start.back() +
+                    (uint32_t)std::min<size_t>(groups, (size_t)ctx->sm_count * g_pred_blocks_per_sm[PRED_FRAME]));
+  }
+  if (table.empty()) return VP8A_OK;
+  const size_t o_start = sizeof(PredArgs) * table.size(), total = o_start + sizeof(uint32_t) * start.size();
+  std::vector<uint8_t> blob(total);
+  memcpy(blob.data(), table.data(), o_start);
+  memcpy(blob.data() + o_start, start.data(), sizeof(uint32_t) * start.size());
+  void* d;
+  vp8a_status s;
+  if ((s = st.scratch(total, &d)) != VP8A_OK) return s;
+  VP8A_CUDA(cudaMemcpyAsync(d, blob.data(), total, cudaMemcpyHostToDevice, ctx->stream));
+  VP8A_CUDA(cudaStreamSynchronize(ctx->stream));  // the host blob goes out of scope
+  predict_frames_kernel<<<start.back(), PR_THREADS, 0, ctx->stream>>>(
+      (const PredArgs*)d, (const uint32_t*)((const uint8_t*)d + o_start), (int)table.size());
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
   return VP8A_OK;
 }
 

@@ -196,10 +196,11 @@ __device__ __forceinline__ int rdiv(int num, int den, uint32_t m) {
   return to16(num >= 0 ? (int)q : -(int)q);
 }
 
-__global__ void __launch_bounds__(RC_WARPS * 32) recon_kernel(RcArgs a) {
+// CTA `cta` of the `ncta` working on `a`: one warp per MB, grid-stride.
+__device__ __forceinline__ void recon_body(const RcArgs& a, uint32_t cta, uint32_t ncta) {
   const int lane = threadIdx.x & 31;
   const unsigned full = 0xffffffffu;
-  for (uint32_t item = blockIdx.x * RC_WARPS + (threadIdx.x >> 5); item < a.n; item += gridDim.x * RC_WARPS) {
+  for (uint32_t item = cta * RC_WARPS + (threadIdx.x >> 5); item < a.n; item += ncta * RC_WARPS) {
     const vp8a_mb_decision& d = a.dec[item];
     bool have = false;
     for (int k = 0; k < a.n_refs; k++) have |= d.ref_frame != VP8A_REF_INTRA && a.ref_ids[k] == d.ref_frame;
@@ -357,7 +358,27 @@ __global__ void __launch_bounds__(RC_WARPS * 32) recon_kernel(RcArgs a) {
   }
 }
 
+__global__ void __launch_bounds__(RC_WARPS * 32) recon_kernel(RcArgs a) { recon_body(a, blockIdx.x, gridDim.x); }
+
+__global__ void __launch_bounds__(RC_WARPS * 32)
+    recon_frames_kernel(const RcArgs* __restrict__ jobs, const uint32_t* __restrict__ cta_start, int n_jobs) {
+  __shared__ RcArgs sa;
+  __shared__ uint32_t first[2];
+  vp8a_dev::find_job(jobs, cta_start, n_jobs, &sa, first);
+  recon_body(sa, blockIdx.x - first[0], first[1]);
+}
+
 int g_rc_blocks_per_sm = 0;
+
+// Validate one frame's arguments, queue (or, with `defer`, prepare) its
+// prediction into `recon`, and fill the reconstruction kernel's arguments
+// and CTA count.
+vp8a_status prepare_recon(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_i420* frame, const vp8a_planes* refs,
+                          const uint8_t* ref_ids, uint32_t n_refs, const vp8a_mb_decision* decisions,
+                          const vp8a_quant_indices* quant, const int8_t* mb_segment, const int16_t* segment_quant,
+                          uint32_t segment_abs, uint32_t full_pixel, uint32_t filter_set, const vp8a_planes* recon,
+                          int16_t* coeffs, uint8_t* mb_flags, vp8a_mb_lf_info* lf_info, bool defer,
+                          vp8a::FramePrediction* fp, RcArgs* out, uint32_t* ctas);
 
 }  // namespace
 
@@ -371,12 +392,15 @@ void vp8a_dequant_factors(const vp8a_quant_indices* qi, uint32_t has_segment, in
   factors_from(q, qi->y_dc_delta, qi->y2_dc_delta, qi->y2_ac_delta, qi->uv_dc_delta, qi->uv_ac_delta, out);
 }
 
-vp8a_status vp8a_reconstruct_inter_frame(vp8a_ctx* ctx, const vp8a_i420* frame, const vp8a_planes* refs,
-                                         const uint8_t* ref_ids, uint32_t n_refs, const vp8a_mb_decision* decisions,
-                                         const vp8a_quant_indices* quant, const int8_t* mb_segment,
-                                         const int16_t* segment_quant, uint32_t segment_abs, uint32_t full_pixel,
-                                         uint32_t filter_set, vp8a_planes* recon, int16_t* coeffs,
-                                         uint8_t* mb_flags, vp8a_mb_lf_info* lf_info) {
+}  // extern "C"
+
+namespace {
+vp8a_status prepare_recon(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_i420* frame, const vp8a_planes* refs,
+                          const uint8_t* ref_ids, uint32_t n_refs, const vp8a_mb_decision* decisions,
+                          const vp8a_quant_indices* quant, const int8_t* mb_segment, const int16_t* segment_quant,
+                          uint32_t segment_abs, uint32_t full_pixel, uint32_t filter_set, const vp8a_planes* recon,
+                          int16_t* coeffs, uint8_t* mb_flags, vp8a_mb_lf_info* lf_info, bool defer,
+                          vp8a::FramePrediction* fp_out, RcArgs* out, uint32_t* ctas) {
   if (!ctx || !frame || !quant || !recon) {
     vp8a::set_error("null argument");
     return VP8A_E_INVALID_ARGUMENT;
@@ -398,10 +422,9 @@ vp8a_status vp8a_reconstruct_inter_frame(vp8a_ctx* ctx, const vp8a_i420* frame, 
     vp8a::set_error("reconstruction planes do not match the frame's MB grid");
     return VP8A_E_REFERENCE_DIMENSIONS_MISMATCH;
   }
-  VP8A_CUDA(cudaSetDevice(ctx->device));
-  vp8a::Stager st(ctx);
-  vp8a::FramePrediction fp;
-  vp8a_status s = vp8a::predict_frame(ctx, st, refs, ref_ids, n_refs, decisions, full_pixel, filter_set, recon, &fp);
+  vp8a::FramePrediction& fp = *fp_out;
+  vp8a_status s = vp8a::predict_frame(ctx, st, refs, ref_ids, n_refs, decisions, full_pixel, filter_set, recon, &fp,
+                                      defer);
   if (s != VP8A_OK) return s;
 
   RcArgs a{};
@@ -463,9 +486,75 @@ vp8a_status vp8a_reconstruct_inter_frame(vp8a_ctx* ctx, const vp8a_i420* frame, 
     VP8A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, recon_kernel, RC_WARPS * 32, 0));
     g_rc_blocks_per_sm = std::max(b, 1);
   }
-  const unsigned grid = (unsigned)std::min<size_t>((a.n + RC_WARPS - 1) / RC_WARPS,
-                                                   (size_t)ctx->sm_count * g_rc_blocks_per_sm);
+  *ctas = (unsigned)std::min<size_t>((a.n + RC_WARPS - 1) / RC_WARPS, (size_t)ctx->sm_count * g_rc_blocks_per_sm);
+  *out = a;
+  return VP8A_OK;
+}
+}  // namespace
+
+extern "C" {
+
+vp8a_status vp8a_reconstruct_inter_frame(vp8a_ctx* ctx, const vp8a_i420* frame, const vp8a_planes* refs,
+                                         const uint8_t* ref_ids, uint32_t n_refs, const vp8a_mb_decision* decisions,
+                                         const vp8a_quant_indices* quant, const int8_t* mb_segment,
+                                         const int16_t* segment_quant, uint32_t segment_abs, uint32_t full_pixel,
+                                         uint32_t filter_set, vp8a_planes* recon, int16_t* coeffs,
+                                         uint8_t* mb_flags, vp8a_mb_lf_info* lf_info) {
+  if (!ctx) {
+    vp8a::set_error("null argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  vp8a::FramePrediction fp;
+  RcArgs a;
+  uint32_t grid = 0;
+  vp8a_status s = prepare_recon(ctx, st, frame, refs, ref_ids, n_refs, decisions, quant, mb_segment, segment_quant,
+                                segment_abs, full_pixel, filter_set, recon, coeffs, mb_flags, lf_info, false, &fp, &a,
+                                &grid);
+  if (s != VP8A_OK) return s;
   recon_kernel<<<grid, RC_WARPS * 32, 0, ctx->stream>>>(a);
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
+  return st.finish();
+}
+
+vp8a_status vp8a_reconstruct_inter_frames(vp8a_ctx* ctx, const vp8a_recon_job* jobs, uint32_t n_jobs) {
+  if (!ctx || (!jobs && n_jobs)) {
+    vp8a::set_error("null argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (n_jobs > VP8A_MAX_BATCH_JOBS) {
+    vp8a::set_error("more jobs than VP8A_MAX_BATCH_JOBS");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (n_jobs == 0) return VP8A_OK;
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  std::vector<vp8a::FramePrediction> fps(n_jobs);
+  std::vector<RcArgs> table(n_jobs);
+  std::vector<uint32_t> start{0};
+  vp8a_status s;
+  for (uint32_t j = 0; j < n_jobs; j++) {
+    const vp8a_recon_job& J = jobs[j];
+    uint32_t ctas = 0;
+    if ((s = prepare_recon(ctx, st, &J.frame, J.refs, J.ref_ids, J.n_refs, J.decisions, &J.quant, J.mb_segment,
+                           J.segment_quant, J.segment_abs, J.full_pixel, J.filter_set, &J.recon, J.coeffs, J.mb_flags,
+                           J.lf_info, true, &fps[j], &table[j], &ctas)) != VP8A_OK)
+      return s;
+    start.push_back(start.back() + ctas);
+  }
+  if ((s = vp8a::predict_frames(ctx, st, fps.data(), n_jobs)) != VP8A_OK) return s;
+  const size_t o_start = sizeof(RcArgs) * n_jobs, total = o_start + sizeof(uint32_t) * start.size();
+  std::vector<uint8_t> blob(total);
+  memcpy(blob.data(), table.data(), o_start);
+  memcpy(blob.data() + o_start, start.data(), sizeof(uint32_t) * start.size());
+  void* d;
+  if ((s = st.scratch(total, &d)) != VP8A_OK) return s;
+  VP8A_CUDA(cudaMemcpyAsync(d, blob.data(), total, cudaMemcpyHostToDevice, ctx->stream));
+  VP8A_CUDA(cudaStreamSynchronize(ctx->stream));  // the host blob goes out of scope
+  recon_frames_kernel<<<start.back(), RC_WARPS * 32, 0, ctx->stream>>>(
+      (const RcArgs*)d, (const uint32_t*)((const uint8_t*)d + o_start), (int)n_jobs);
   VP8A_CUDA(cudaGetLastError());
   ctx->launches++;
   return st.finish();

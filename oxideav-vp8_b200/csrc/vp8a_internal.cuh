@@ -92,13 +92,19 @@ struct FramePrediction {
   vp8a_planes planes{};
   uint8_t ref_ids[3] = {0, 0, 0};
   uint32_t n_refs = 0;
+  alignas(16) unsigned char args[320];  // the prediction kernel's arguments
 };
 
 // Validates and stages the arguments of vp8a_predict_inter_frame through
-// `st` and queues the per-MB §18 prediction into `out` (predict.cu).
+// `st` and queues the per-MB §18 prediction into `out` (predict.cu); with
+// `defer` it only prepares the launch, which predict_frames then makes for
+// many frames at once.
 vp8a_status predict_frame(vp8a_ctx* ctx, Stager& st, const vp8a_planes* refs, const uint8_t* ref_ids,
                           uint32_t n_refs, const vp8a_mb_decision* decisions, uint32_t full_pixel,
-                          uint32_t filter_set, const vp8a_planes* out, FramePrediction* fp);
+                          uint32_t filter_set, const vp8a_planes* out, FramePrediction* fp, bool defer = false);
+
+// One launch predicting every deferred frame of `fps`.
+vp8a_status predict_frames(vp8a_ctx* ctx, Stager& st, const FramePrediction* fps, uint32_t n);
 
 }  // namespace vp8a
 
@@ -114,6 +120,27 @@ static __constant__ int c_sixtap[8][6] = {
     {0, -9, 93, 50, -6, 0},   {3, -16, 77, 77, -16, 3}, {0, -6, 50, 93, -9, 0},
     {1, -8, 36, 108, -11, 2}, {0, -1, 12, 123, -6, 0},
 };
+
+// A batched launch's CTA finds its job: thread 0 searches the CTA offsets
+// (cta_start[j] <= blockIdx.x < cta_start[j + 1], n_jobs + 1 entries),
+// copies the job's arguments into shared `*sa` and its first CTA and CTA
+// count into `first[0..1]`; the block then synchronises.
+template <typename Args>
+__device__ __forceinline__ void find_job(const Args* jobs, const uint32_t* cta_start, int n_jobs, Args* sa,
+                                         uint32_t* first) {
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = n_jobs - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (cta_start[mid] <= blockIdx.x) lo = mid;
+      else hi = mid - 1;
+    }
+    *sa = jobs[lo];
+    first[0] = cta_start[lo];
+    first[1] = cta_start[lo + 1] - cta_start[lo];
+  }
+  __syncthreads();
+}
 
 // interp (src/motion_comp.rs:396): dot product, (a + 64) >> 7, clamp255.
 __device__ __forceinline__ int interp6(const int* f, int s0, int s1, int s2, int s3, int s4, int s5) {

@@ -131,6 +131,41 @@ class Source(C.Structure):
     ]
 
 
+MAX_BATCH_JOBS = 1024
+
+
+class AnalysisJob(C.Structure):
+    """vp8a_analysis_job: one vp8a_analyse_inter_frame call of a batch."""
+
+    _fields_ = [("frame", I420), ("refs", C.c_void_p), ("ref_ids", C.c_void_p), ("n_refs", C.c_uint32),
+                ("mv_contexts", C.c_void_p), ("lam", C.c_double), ("decisions", C.c_void_p),
+                ("trace", C.c_void_p)]
+
+
+class ArnrJob(C.Structure):
+    """vp8a_arnr_job: one vp8a_build_arnr_altref call of a batch."""
+
+    _fields_ = [("frames", C.c_void_p), ("n", C.c_uint32), ("center", C.c_uint32), ("strength", C.c_uint32),
+                ("y_out", C.c_void_p), ("u_out", C.c_void_p), ("v_out", C.c_void_p)]
+
+
+class ReconJob(C.Structure):
+    """vp8a_recon_job: one vp8a_reconstruct_inter_frame call of a batch."""
+
+    _fields_ = [("frame", I420), ("refs", C.c_void_p), ("ref_ids", C.c_void_p), ("n_refs", C.c_uint32),
+                ("segment_abs", C.c_uint32), ("decisions", C.c_void_p), ("quant", QuantIndices),
+                ("mb_segment", C.c_void_p), ("segment_quant", C.c_void_p), ("full_pixel", C.c_uint32),
+                ("filter_set", C.c_uint32), ("recon", Planes), ("coeffs", C.c_void_p), ("mb_flags", C.c_void_p),
+                ("lf_info", C.c_void_p)]
+
+
+class SweepJob(C.Structure):
+    """vp8a_sweep_job: one vp8a_filter_sweep call of a batch."""
+
+    _fields_ = [("planes", Planes), ("mbs", C.c_void_p), ("base", FilterConfig), ("src", Source),
+                ("every_rows", C.c_uint32), ("ssd_out", C.c_void_p)]
+
+
 MV_DTYPE = np.dtype([("row", "<i2"), ("col", "<i2")])
 SEARCH_RESULT_DTYPE = np.dtype([("mv", MV_DTYPE), ("sad", "<u4")])
 MB_DECISION_DTYPE = np.dtype(
@@ -217,6 +252,10 @@ C_SIZES = {
     "vp8a_mb_info": 72,
     "vp8a_rd_inter": 56,
     "vp8a_quant_indices": 8,
+    "vp8a_analysis_job": 104,
+    "vp8a_arnr_job": 48,
+    "vp8a_recon_job": 184,
+    "vp8a_sweep_job": 152,
 }
 
 
@@ -237,6 +276,10 @@ def check_layouts():
         "vp8a_mb_info": MB_INFO_DTYPE.itemsize,
         "vp8a_rd_inter": RD_INTER_DTYPE.itemsize,
         "vp8a_quant_indices": C.sizeof(QuantIndices),
+        "vp8a_analysis_job": C.sizeof(AnalysisJob),
+        "vp8a_arnr_job": C.sizeof(ArnrJob),
+        "vp8a_recon_job": C.sizeof(ReconJob),
+        "vp8a_sweep_job": C.sizeof(SweepJob),
     }
     assert got == C_SIZES, (got, C_SIZES)
     return got

@@ -384,3 +384,98 @@ def lf_info_from_decisions(dec, has_coeffs=None):
     if has_coeffs is not None:
         m["has_coeffs"] = np.asarray(has_coeffs, np.uint8).reshape(-1)
     return m
+
+
+# ------------------------------------------------------ batched work lists
+#
+# Each *_frames / *_altrefs / *_sweeps call runs a list of independent jobs
+# (many streams' frames, of uneven sizes) as one launch per stage; every
+# job's results equal the single-job call's.
+
+
+def _batch(ctx, fn, jobs, where):
+    arr = (type(jobs[0]) * len(jobs))(*jobs) if jobs else None
+    check(getattr(ctx._lib, fn)(ctx.handle, C.cast(arr, C.c_void_p) if arr is not None else None, len(jobs)), where)
+
+
+def analyse_inter_frames(ctx, jobs):
+    """vp8a_analyse_inter_frames: `jobs` = list of dicts with the arguments
+    of analyse_inter_frame (frame, refs, ref_ids, lam, optional
+    mv_contexts). Returns each job's (mb_rows, mb_cols) decisions."""
+    keep, cj, outs = [], [], []
+    for j in jobs:
+        f = i420(*j["frame"])
+        prs = [planes(*p) for p in j["refs"]]
+        parr = (abi.Planes * len(prs))(*prs)
+        ids = np.ascontiguousarray(np.asarray(j["ref_ids"], np.uint8))
+        ctxs = j.get("mv_contexts") or abi.default_mv_contexts()
+        mbr, mbc = (f.height + 15) // 16, (f.width + 15) // 16
+        dec = np.zeros(mbr * mbc, abi.MB_DECISION_DTYPE)
+        keep += [parr, ids, ctxs]
+        cj.append(abi.AnalysisJob(f, C.cast(parr, C.c_void_p), ptr(ids), len(prs), C.cast(C.pointer(ctxs), C.c_void_p),
+                                  j["lam"], ptr(dec), None))
+        outs.append(dec.reshape(mbr, mbc))
+    _batch(ctx, "vp8a_analyse_inter_frames", cj, "vp8a_analyse_inter_frames")
+    return outs
+
+
+def build_arnr_altrefs(ctx, jobs):
+    """vp8a_build_arnr_altrefs: `jobs` = list of (frames, center, strength)
+    with frames a list of (y, u, v). Returns each job's packed (y, u, v)."""
+    keep, cj, outs = [], [], []
+    for frames, center, strength in jobs:
+        recs = [i420(*f) for f in frames]
+        arr = (abi.I420 * len(recs))(*recs)
+        h, w = frames[0][0].shape[:2]
+        ch, cw = (h + 1) // 2, (w + 1) // 2
+        y, u, v = np.zeros((h, w), np.uint8), np.zeros((ch, cw), np.uint8), np.zeros((ch, cw), np.uint8)
+        keep.append(arr)
+        cj.append(abi.ArnrJob(C.cast(arr, C.c_void_p), len(recs), center, strength, ptr(y), ptr(u), ptr(v)))
+        outs.append((y, u, v))
+    _batch(ctx, "vp8a_build_arnr_altrefs", cj, "vp8a_build_arnr_altrefs")
+    return outs
+
+
+def reconstruct_inter_frames(ctx, jobs):
+    """vp8a_reconstruct_inter_frames: `jobs` = list of dicts with the
+    arguments of reconstruct_inter_frame (frame, refs, ref_ids, decisions,
+    quant, recon, optional mb_segment, segment_quant, segment_abs,
+    full_pixel, filter_set, lf_info). `recon` is written in place. Returns
+    each job's (coeffs, flags)."""
+    keep, cj, outs = [], [], []
+    for j in jobs:
+        f = i420(*j["frame"])
+        prs = [planes(*p) for p in j["refs"]]
+        parr = (abi.Planes * len(prs))(*prs)
+        ids = np.ascontiguousarray(np.asarray(j["ref_ids"], np.uint8))
+        dec = _contig(j["decisions"])
+        op = planes(*j["recon"])
+        n = op.mb_cols * op.mb_rows
+        cf, fl = np.zeros((n, 400), np.int16), np.zeros(n, np.uint8)
+        seg = j.get("mb_segment")
+        seg = None if seg is None else np.ascontiguousarray(np.asarray(seg, np.int8))
+        sq = j.get("segment_quant")
+        sq = None if sq is None else np.ascontiguousarray(np.asarray(sq, np.int16).reshape(4))
+        keep += [parr, ids, dec, seg, sq]
+        cj.append(abi.ReconJob(f, C.cast(parr, C.c_void_p), ptr(ids), len(prs), int(bool(j.get("segment_abs"))),
+                               ptr(dec), j["quant"], ptr(seg), ptr(sq), int(bool(j.get("full_pixel"))),
+                               j.get("filter_set", abi.FILTER_SIXTAP), op, ptr(cf), ptr(fl), ptr(j.get("lf_info"))))
+        outs.append((cf, fl))
+    _batch(ctx, "vp8a_reconstruct_inter_frames", cj, "vp8a_reconstruct_inter_frames")
+    return outs
+
+
+def filter_sweeps(ctx, jobs):
+    """vp8a_filter_sweeps: `jobs` = list of (recon, mbs, base, src[,
+    every_rows]). Returns each job's (64, 8) uint64 table."""
+    keep, cj, outs = [], [], []
+    for j in jobs:
+        recon, mbs, base, src = j[:4]
+        every = j[4] if len(j) > 4 else 0
+        m = np.ascontiguousarray(mbs, abi.MB_LF_INFO_DTYPE)
+        out = np.zeros(512, np.uint64)
+        keep.append(m)
+        cj.append(abi.SweepJob(planes(*recon), ptr(m), base, source(*src), every, ptr(out)))
+        outs.append(out.reshape(64, 8))
+    _batch(ctx, "vp8a_filter_sweeps", cj, "vp8a_filter_sweeps")
+    return outs
