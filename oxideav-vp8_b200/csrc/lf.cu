@@ -58,12 +58,24 @@ struct LfArgs {
   uint64_t sys, scs;
   int width, height;
   const uint8_t* cands;    // [n][2] (level, sharpness)
+  // [n] or null: the sharpness values whose table entries candidate i's
+  // SSD fills (bit s = level * 8 + s), null = its own sharpness only.
+  const uint8_t* cand_mask;
   const int16_t* row_t0;   // per MB row: first step, -1 = row not scored
   const uint8_t* row_top;  // per MB row: has a top MB edge
   int steps;
   const int32_t* sched_off;  // [steps + 1]: rows active at step t are
   const uint16_t* sched_row; //   sched_row[sched_off[t] .. sched_off[t + 1])
   int max_active;            // most rows active at one step
+  // Ring sets: row r keeps its slots in set row_set[r] (rows whose slot
+  // lifetimes do not overlap share a set; n_sets sets). Its last RING MBs
+  // are scored at the step where they are final: the rows listed in
+  // fin_row[fin_off[t] .. fin_off[t + 1]) at step t. Null row_set: set r
+  // for row r, tails scored after the last step.
+  const uint16_t* row_set;
+  const int32_t* fin_off;
+  const uint16_t* fin_row;
+  int n_sets;
   int recon_words;           // planes and strides allow 4-byte accesses
   int source_words;
   // Next-step prefetch: each half-warp copies its next MB's reconstruction,
@@ -111,15 +123,17 @@ __device__ __forceinline__ Prm derive(int level, int sharp, bool key) {
   return p;
 }
 
+__host__ __device__ __forceinline__ int clamp63(int v) { return v < 0 ? 0 : (v > 63 ? 63 : v); }
+
 // calculate_mb_filter_level_inter (src/loop_filter.rs:1280-1331).
-__device__ __forceinline__ int mb_level(const vp8a_filter_config& c, int level0, const vp8a_mb_lf_info& m) {
+__host__ __device__ __forceinline__ int mb_level(const vp8a_filter_config& c, int level0, const vp8a_mb_lf_info& m) {
   int level = level0;
   if (c.segmentation_enabled) {
-    int seg = m.segment_id < 0 ? 0 : min((int)m.segment_id, 3);
+    int seg = m.segment_id < 0 ? 0 : (m.segment_id > 3 ? 3 : (int)m.segment_id);
     if (c.segment_abs) level = c.segment_lf_level[seg];
     else level += c.segment_lf_level[seg];
   }
-  level = clampi(level, 0, 63);
+  level = clamp63(level);
   if (c.delta_enabled) {
     int rd = m.ref_frame == VP8A_REF_LAST     ? c.ref_delta_last
              : m.ref_frame == VP8A_REF_GOLDEN ? c.ref_delta_golden
@@ -136,7 +150,19 @@ __device__ __forceinline__ int mb_level(const vp8a_filter_config& c, int level0,
       level += c.other_mv_mode_delta;
     }
   }
-  return clampi(level, 0, 63);
+  return clamp63(level);
+}
+
+// LoopFilterParams::derive's interior limit (src/loop_filter.rs:99-148):
+// with the level, it fixes every parameter of the §15 filters.
+__host__ __device__ __forceinline__ int interior_limit(int level, int sharp) {
+  int interior = level;
+  if (sharp != 0) {
+    interior >>= (sharp > 4) ? 2 : 1;
+    const int cap = 9 - sharp > 0 ? 9 - sharp : 0;
+    if (interior > cap) interior = cap;
+  }
+  return interior == 0 ? 1 : interior;
 }
 
 // The filters below work on unsigned pixels (0..255): the reference's
@@ -206,8 +232,9 @@ __device__ __forceinline__ uint32_t pack4(const int* o) {
   return (uint32_t)o[0] | ((uint32_t)o[1] << 8) | ((uint32_t)o[2] << 16) | ((uint32_t)o[3] << 24);
 }
 
-__device__ __forceinline__ uint8_t* slot_ptr(uint8_t* slots, int r, int c) {
-  return slots + ((size_t)r * RING + c % RING) * SLOT_STRIDE;
+// Slot of column c of the row using ring set `set`.
+__device__ __forceinline__ uint8_t* slot_ptr(uint8_t* slots, int set, int c) {
+  return slots + ((size_t)set * RING + c % RING) * SLOT_STRIDE;
 }
 
 // One half-warp handles one MB: lane l (0-15) owns luma row l and chroma
@@ -311,9 +338,9 @@ __device__ __forceinline__ uint32_t ssd4(uint32_t x, uint32_t y, uint32_t m) {
 
 // Finish final MB (r, c): write it back (apply mode) and return this lane's
 // share of its visible-window SSD.
-__device__ __forceinline__ uint32_t finish_mb(const LfArgs& a, const uint8_t* slots, int r, int c, int l,
+__device__ __forceinline__ uint32_t finish_mb(const LfArgs& a, const uint8_t* slots, int set, int r, int c, int l,
                                               const SrcWords& sw) {
-  const uint8_t* s = slot_ptr(const_cast<uint8_t*>(slots), r, c);
+  const uint8_t* s = slot_ptr(const_cast<uint8_t*>(slots), set, c);
   const uint32_t* sy = (const uint32_t*)(s + l * 16);
   const uint32_t* sc = (const uint32_t*)(s + (l < 8 ? 256 : 320) + (l & 7) * 8);
   if (a.oy) {
@@ -339,15 +366,16 @@ __device__ __forceinline__ uint32_t finish_mb(const LfArgs& a, const uint8_t* sl
 // Filter MB (r, c) held in its slot; neighbours in their slots. The
 // caller's half-warp (mask hm) runs this together.
 __device__ __forceinline__ void filter_mb(const LfArgs& a, const Prm* prm, const vp8a_mb_lf_info m, uint8_t* slots,
-                                          int level0, int r, int c, bool has_top, int l, unsigned hm) {
+                                          int level0, int set, int set_above, int c, bool has_top, int l,
+                                          unsigned hm) {
   const int level = mb_level(a.base, level0, m);
   if (level == 0) return;
   const Prm q = prm[level];
   const bool sub = m.y_mode_is_bpred || m.has_coeffs;
   const bool has_left = c > 0;
-  uint8_t* me = slot_ptr(slots, r, c);
-  uint8_t* left = slot_ptr(slots, r, c - 1);
-  uint8_t* above = has_top ? slot_ptr(slots, r - 1, c) : nullptr;
+  uint8_t* me = slot_ptr(slots, set, c);
+  uint8_t* left = slot_ptr(slots, set, c - 1);
+  uint8_t* above = has_top ? slot_ptr(slots, set_above, c) : nullptr;
 
   if (a.base.simple) {
     // §20.6 filter_row_simple: luma only.
@@ -509,7 +537,7 @@ __device__ __forceinline__ void prefetch_mb(const LfArgs& a, Stage* g, int r, in
 // (level 0 scores the unfiltered planes whatever the sharpness).
 template <int NC>
 __device__ __forceinline__ void block_sums_store(const uint64_t (&v)[NC], const LfArgs& a, const int (&lv)[NC],
-                                                 const int (&sh)[NC], int nc) {
+                                                 const int (&mk)[NC], int nc) {
   __shared__ unsigned long long red[NC][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -525,11 +553,7 @@ __device__ __forceinline__ void block_sums_store(const uint64_t (&v)[NC], const 
     uint64_t x = lane < nwarps ? red[k][lane] : 0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(FULL, x, o);
-    if (lv[k] == 0 && a.level0_unfiltered) {
-      if (lane < 8) a.ssd_out[lane] = x;
-    } else if (lane == 0) {
-      a.ssd_out[lv[k] * 8 + sh[k]] = x;
-    }
+    if (lane < 8 && ((mk[k] >> lane) & 1)) a.ssd_out[lv[k] * 8 + lane] = x;
   }
 }
 
@@ -544,7 +568,7 @@ __device__ __forceinline__ void sweep_body(const LfArgs& a, int cta) {
   const int hw = threadIdx.x >> 4, nhw = blockDim.x >> 4, l = threadIdx.x & 15;
   const unsigned hm = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
   const int first = cta * NC, nc = min(NC, a.n_cands - first);
-  int lv[NC], sh[NC];
+  int lv[NC], sh[NC], mk[NC];
   bool filt[NC];
   uint64_t acc[NC];
   uint8_t* slots[NC];
@@ -554,6 +578,9 @@ __device__ __forceinline__ void sweep_body(const LfArgs& a, int cta) {
     const int q = first + min(k, nc - 1);
     lv[k] = a.cands[2 * q];
     sh[k] = a.cands[2 * q + 1];
+    // A sweep-mode level-0 candidate scores the unfiltered planes, the same
+    // for every sharpness.
+    mk[k] = (lv[k] == 0 && a.level0_unfiltered) ? 0xff : (a.cand_mask ? a.cand_mask[q] : 1 << sh[k]);
     filt[k] = k < nc && !(lv[k] == 0 && a.level0_unfiltered);
     acc[k] = 0;
     slots[k] = (a.smem_slots ? smem_slots : a.gslots + (size_t)first * a.ring_bytes) + (size_t)k * a.ring_bytes;
@@ -563,6 +590,65 @@ __device__ __forceinline__ void sweep_body(const LfArgs& a, int cta) {
   const bool score = a.ssd_out != nullptr;
   __syncthreads();
   Stage* stage = a.prefetch ? (Stage*)(smem_slots + a.stage_off) + hw : nullptr;
+  // MB (r, c) of every candidate: its inputs come from the half-warp's
+  // staging area (`from_stage`, then `next()` may refill it) or straight
+  // from global memory; the MB three columns back leaves its slot scored,
+  // MB (r, c) takes the slot and is filtered.
+  auto set_of = [&](int r) -> int { return a.row_set ? (int)a.row_set[r] : r; };
+  auto do_mb = [&](int r, int c, bool from_stage, auto&& next) {
+    const int set = set_of(r), set_above = (a.row_top[r] != 0) ? set_of(r - 1) : 0;
+    MbWords rec;
+    SrcWords sw{};
+    vp8a_mb_lf_info m;
+    if (from_stage) {
+      cp_async_wait_all();
+      __syncwarp(hm);
+      const uint32_t* ry = (const uint32_t*)(stage->rec + l * 16);
+      const uint32_t* rc = (const uint32_t*)(stage->rec + (l < 8 ? 256 : 320) + (l & 7) * 8);
+#pragma unroll
+      for (int k = 0; k < 4; k++) rec.y[k] = ry[k];
+      rec.c[0] = rc[0];
+      rec.c[1] = rc[1];
+      if (score && c >= RING) {
+        const uint32_t* sy = (const uint32_t*)(stage->src + l * 16);
+        const uint32_t* sc = (const uint32_t*)(stage->src + (l < 8 ? 256 : 320) + (l & 7) * 8);
+        const int ny = r * 16 + l < a.height ? clampi(a.width - (c - RING) * 16, 0, 16) : 0;
+        const int cw = (a.width + 1) >> 1, ch = (a.height + 1) >> 1;
+        const int ncv = r * 8 + (l & 7) < ch ? clampi(cw - (c - RING) * 8, 0, 8) : 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          sw.y[k] = sy[k];
+          sw.my[k] = vis_mask(ny, k);
+        }
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+          sw.c[k] = sc[k];
+          sw.mc[k] = vis_mask(ncv, k);
+        }
+      }
+      m = stage->info;
+      __syncwarp(hm);
+      // The staging area is free again: start the next MB's copies.
+      next();
+    } else {
+      rec = fetch_recon(a, r, c, l);
+      if (score && c >= RING) sw = fetch_source(a, r, c - RING, l);
+      m = a.mbs[(size_t)r * a.mb_cols + c];
+    }
+#pragma unroll
+    for (int k = 0; k < NC; k++) {
+      if (k >= nc) break;
+      if (c >= RING) {
+        acc[k] += finish_mb(a, slots[k], set, r, c - RING, l, sw);
+        __syncwarp(hm);
+      }
+      store_slot(slot_ptr(slots[k], set, c), rec, l);
+    }
+    __syncwarp(hm);
+#pragma unroll
+    for (int k = 0; k < NC; k++)
+      if (filt[k]) filter_mb(a, prm[k], m, slots[k], lv[k], set, set_above, c, a.row_top[r] != 0, l, hm);
+  };
   // The half-warp's first MB of step t, or -1.
   auto first_mb = [&](int t) -> int {
     if (t >= a.steps) return -1;
@@ -582,72 +668,38 @@ __device__ __forceinline__ void sweep_body(const LfArgs& a, int cta) {
     bool next_issued = false;
     for (int i = b + hw; i < e; i += nhw) {
       const int r = a.sched_row[i], c = t - a.row_t0[r];
-      MbWords rec;
-      SrcWords sw{};
-      vp8a_mb_lf_info m;
-      if (staged && i == b + hw) {
-        cp_async_wait_all();
-        __syncwarp(hm);
-        const uint32_t* ry = (const uint32_t*)(stage->rec + l * 16);
-        const uint32_t* rc = (const uint32_t*)(stage->rec + (l < 8 ? 256 : 320) + (l & 7) * 8);
-#pragma unroll
-        for (int k = 0; k < 4; k++) rec.y[k] = ry[k];
-        rec.c[0] = rc[0];
-        rec.c[1] = rc[1];
-        if (score && c >= RING) {
-          const uint32_t* sy = (const uint32_t*)(stage->src + l * 16);
-          const uint32_t* sc = (const uint32_t*)(stage->src + (l < 8 ? 256 : 320) + (l & 7) * 8);
-          const int ny = r * 16 + l < a.height ? clampi(a.width - (c - RING) * 16, 0, 16) : 0;
-          const int cw = (a.width + 1) >> 1, ch = (a.height + 1) >> 1;
-          const int ncv = r * 8 + (l & 7) < ch ? clampi(cw - (c - RING) * 8, 0, 8) : 0;
-#pragma unroll
-          for (int k = 0; k < 4; k++) {
-            sw.y[k] = sy[k];
-            sw.my[k] = vis_mask(ny, k);
-          }
-#pragma unroll
-          for (int k = 0; k < 2; k++) {
-            sw.c[k] = sc[k];
-            sw.mc[k] = vis_mask(ncv, k);
-          }
-        }
-        m = stage->info;
-        __syncwarp(hm);
-        // The staging area is free again: start the next step's copies.
+      const bool from_stage = staged && i == b + hw;
+      do_mb(r, c, from_stage, [&] {
         staged = a.prefetch && issue(t + 1);
         next_issued = true;
-      } else {
-        rec = fetch_recon(a, r, c, l);
-        if (score && c >= RING) sw = fetch_source(a, r, c - RING, l);
-        m = a.mbs[(size_t)r * a.mb_cols + c];
-      }
-#pragma unroll
-      for (int k = 0; k < NC; k++) {
-        if (k >= nc) break;
-        if (c >= RING) {
-          acc[k] += finish_mb(a, slots[k], r, c - RING, l, sw);
-          __syncwarp(hm);
-        }
-        store_slot(slot_ptr(slots[k], r, c), rec, l);
-      }
-      __syncwarp(hm);
-#pragma unroll
-      for (int k = 0; k < NC; k++)
-        if (filt[k]) filter_mb(a, prm[k], m, slots[k], lv[k], r, c, a.row_top[r] != 0, l, hm);
+      });
     }
     if (a.prefetch && !next_issued) staged = issue(t + 1);
+    if (a.row_set) {
+      // Rows whose last MBs became final with the previous step.
+      const int fb = a.fin_off[t] * RING, fe = a.fin_off[t + 1] * RING;
+      for (int j = fb + hw; j < fe; j += nhw) {
+        const int r = a.fin_row[j / RING], c = a.mb_cols - RING + j % RING;
+        if (c < 0) continue;
+        const SrcWords sw = score ? fetch_source(a, r, c, l) : SrcWords{};
+        const int set = set_of(r);
+#pragma unroll
+        for (int k = 0; k < NC; k++)
+          if (k < nc) acc[k] += finish_mb(a, slots[k], set, r, c, l, sw);
+      }
+    }
     __syncthreads();
   }
-  // The last MBs of every scored row.
-  for (int i = hw; i < a.mb_rows * RING; i += nhw) {
+  // Without a tail schedule: the last MBs of every scored row.
+  for (int i = hw; !a.row_set && i < a.mb_rows * RING; i += nhw) {
     const int r = i / RING, c = a.mb_cols - RING + i % RING;
     if (c < 0 || a.row_t0[r] < 0) continue;
     const SrcWords sw = score ? fetch_source(a, r, c, l) : SrcWords{};
 #pragma unroll
     for (int k = 0; k < NC; k++)
-      if (k < nc) acc[k] += finish_mb(a, slots[k], r, c, l, sw);
+      if (k < nc) acc[k] += finish_mb(a, slots[k], r, r, c, l, sw);
   }
-  if (score) block_sums_store<NC>(acc, a, lv, sh, nc);
+  if (score) block_sums_store<NC>(acc, a, lv, mk, nc);
 }
 
 template <int NC>
@@ -789,26 +841,66 @@ vp8a_status stage_lf(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_planes* planes,
         max_t0 = std::max(max_t0, 2 * k);
       }
   }
-  // Step schedule: the rows active at step t, in increasing order.
-  const int steps = max_t0 + cols;
-  std::vector<int32_t> off(steps + 1, 0);
-  std::vector<uint16_t> sched;
+  // Tails: row r's last RING MBs are final once the scored row below it in
+  // the same band has run its last MB (else once row r has), and are scored
+  // the step after (tf[r]). Ring sets: a row takes any set whose previous
+  // row's tail was scored before the row's first step.
+  std::vector<int> tf(rows, -1);
+  int steps = 0;
+  for (int r = 0; r < rows; r++) {
+    if (t0[r] < 0) continue;
+    const bool below = r + 1 < rows && t0[r + 1] >= 0 && top[r + 1];
+    tf[r] = (below ? t0[r + 1] : t0[r]) + cols;
+    steps = std::max(steps, tf[r] + 1);
+  }
+  std::vector<uint16_t> set(rows, 0);
+  std::vector<int> set_free;  // per set: first step it may be taken again
+  std::vector<int> order;
+  for (int r = 0; r < rows; r++)
+    if (t0[r] >= 0) order.push_back(r);
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return t0[x] < t0[y]; });
+  for (int r : order) {
+    int k = -1;
+    for (int q = 0; q < (int)set_free.size() && k < 0; q++)
+      if (set_free[q] <= t0[r]) k = q;
+    if (k < 0) {
+      k = (int)set_free.size();
+      set_free.push_back(0);
+    }
+    set[r] = (uint16_t)k;
+    set_free[k] = tf[r] + 1;
+  }
+  // Step schedule: the rows active at step t, in increasing order, and the
+  // rows whose tails are scored at step t.
+  std::vector<int32_t> off(steps + 1, 0), foff(steps + 1, 0);
+  std::vector<uint16_t> sched, fin;
   int max_active = 0;
   for (int t = 0; t < steps; t++) {
     off[t] = (int32_t)sched.size();
-    for (int r = 0; r < rows; r++)
+    foff[t] = (int32_t)fin.size();
+    for (int r = 0; r < rows; r++) {
       if (t0[r] >= 0 && t >= t0[r] && t < t0[r] + cols) sched.push_back((uint16_t)r);
+      if (tf[r] == t) fin.push_back((uint16_t)r);
+    }
     max_active = std::max(max_active, (int)sched.size() - off[t]);
   }
   off[steps] = (int32_t)sched.size();
-  // One upload: t0 (int16), top (u8), offsets (int32), rows (u16).
-  const size_t o_top = sizeof(int16_t) * rows, o_off = (o_top + rows + 3) & ~(size_t)3,
-               o_row = o_off + sizeof(int32_t) * (steps + 1), total = o_row + sizeof(uint16_t) * sched.size();
+  foff[steps] = (int32_t)fin.size();
+  // One upload: t0 (int16), top (u8), offsets (int32), rows (u16), sets
+  // (u16), tail offsets (int32), tail rows (u16).
+  auto a4 = [](size_t x) { return (x + 3) & ~(size_t)3; };
+  const size_t o_top = sizeof(int16_t) * rows, o_off = a4(o_top + rows),
+               o_row = o_off + sizeof(int32_t) * (steps + 1), o_set = a4(o_row + sizeof(uint16_t) * sched.size()),
+               o_foff = a4(o_set + sizeof(uint16_t) * rows), o_fin = o_foff + sizeof(int32_t) * (steps + 1),
+               total = o_fin + sizeof(uint16_t) * fin.size();
   std::vector<uint8_t> blob(total, 0);
   memcpy(blob.data(), t0.data(), o_top);
   memcpy(blob.data() + o_top, top.data(), rows);
   memcpy(blob.data() + o_off, off.data(), sizeof(int32_t) * (steps + 1));
   if (!sched.empty()) memcpy(blob.data() + o_row, sched.data(), sizeof(uint16_t) * sched.size());
+  memcpy(blob.data() + o_set, set.data(), sizeof(uint16_t) * rows);
+  memcpy(blob.data() + o_foff, foff.data(), sizeof(int32_t) * (steps + 1));
+  if (!fin.empty()) memcpy(blob.data() + o_fin, fin.data(), sizeof(uint16_t) * fin.size());
   void* dblob;
   if ((s = st.scratch(total, &dblob)) != VP8A_OK) return s;
   VP8A_CUDA(cudaMemcpyAsync(dblob, blob.data(), total, cudaMemcpyHostToDevice, ctx->stream));
@@ -818,6 +910,10 @@ vp8a_status stage_lf(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_planes* planes,
   a.row_top = db + o_top;
   a.sched_off = (const int32_t*)(db + o_off);
   a.sched_row = (const uint16_t*)(db + o_row);
+  a.row_set = (const uint16_t*)(db + o_set);
+  a.fin_off = (const int32_t*)(db + o_foff);
+  a.fin_row = (const uint16_t*)(db + o_fin);
+  a.n_sets = (int)set_free.size();
   a.max_active = max_active;
   a.steps = steps;
   auto al4 = [](const void* p, uint64_t stride) { return ((uintptr_t)p % 4 == 0) && (stride % 4 == 0); };
@@ -827,50 +923,103 @@ vp8a_status stage_lf(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_planes* planes,
   return VP8A_OK;
 }
 
+// Launch one sweep kernel variant (NC candidates per CTA) for one picture
+// (`a`) or over a job table.
+template <int NC>
+vp8a_status launch_nc(vp8a_ctx* ctx, unsigned grid, int threads, size_t smem, const LfArgs& a, const LfArgs* dj,
+                      const uint32_t* ds, int n_jobs) {
+  if (dj) {
+    VP8A_CUDA(cudaFuncSetAttribute(lf_sweep_batch_kernel<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    lf_sweep_batch_kernel<NC><<<grid, threads, smem, ctx->stream>>>(dj, ds, n_jobs);
+  } else {
+    VP8A_CUDA(cudaFuncSetAttribute(lf_sweep_kernel<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    lf_sweep_kernel<NC><<<grid, threads, smem, ctx->stream>>>(a);
+  }
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
+  return VP8A_OK;
+}
+
+vp8a_status launch_variant(vp8a_ctx* ctx, int nc, unsigned grid, int threads, size_t smem, const LfArgs& a,
+                           const LfArgs* dj, const uint32_t* ds, int n_jobs) {
+  if (nc == 3) return launch_nc<3>(ctx, grid, threads, smem, a, dj, ds, n_jobs);
+  if (nc == 2) return launch_nc<2>(ctx, grid, threads, smem, a, dj, ds, n_jobs);
+  return launch_nc<1>(ctx, grid, threads, smem, a, dj, ds, n_jobs);
+}
+
+// Shared-memory layout of a sweep launch: NC rings of `ring` bytes, then
+// the half-warps' staging areas (prefetch). Returns the dynamic bytes.
+size_t sweep_smem(int nc, int ring, bool pre, int threads) {
+  return (size_t)nc * ring + (pre ? (size_t)(threads / 16) * sizeof(Stage) : 0);
+}
+
+// The layout a sweep of `n` candidates runs with: candidates per CTA and
+// the prefetch, among those whose shared memory fits, by an estimate of
+// the time: whole waves of CTAs over the GPU x candidates per CTA (a CTA's
+// steps carry every candidate's filtering), 15 % more without the
+// prefetch. Returns false when no layout fits.
+struct SweepLayout {
+  int nc;
+  bool pre;
+  size_t smem;
+};
+bool pick_layout(vp8a_ctx* ctx, int n, int ring, bool pre_ok, int threads, bool batch, SweepLayout* out) {
+  int max_smem = 0;
+  VP8A_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+  double best = 1e30;
+  bool found = false;
+  for (int nc = 3; nc >= 1; nc--) {
+    if (nc > 1 && n < nc) continue;
+    cudaFuncAttributes fa;
+    const void* k = batch ? (nc == 3 ? (const void*)lf_sweep_batch_kernel<3>
+                                     : nc == 2 ? (const void*)lf_sweep_batch_kernel<2>
+                                               : (const void*)lf_sweep_batch_kernel<1>)
+                          : (nc == 3 ? (const void*)lf_sweep_kernel<3>
+                                     : nc == 2 ? (const void*)lf_sweep_kernel<2> : (const void*)lf_sweep_kernel<1>);
+    if (cudaFuncGetAttributes(&fa, k) != cudaSuccess) return false;
+    for (int pre = pre_ok ? 1 : 0; pre >= 0; pre--) {
+      const size_t smem = sweep_smem(nc, ring, pre, threads);
+      if (smem + fa.sharedSizeBytes + 1024 > (size_t)max_smem) continue;
+      if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return false;
+      int per_sm = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem) != cudaSuccess) return false;
+      if (per_sm < 1) continue;
+      const long ctas = (n + nc - 1) / nc, slots = (long)ctx->sm_count * per_sm;
+      const double cost = (double)((ctas + slots - 1) / slots) * nc * (pre ? 1.0 : 1.15);
+      if (cost < best) {
+        best = cost;
+        *out = SweepLayout{nc, pre != 0, smem};
+        found = true;
+      }
+    }
+  }
+  return found;
+}
+
 // Launch the sweep over `n` candidates (pairs of level, sharpness) already
-// in device memory at a.cands. Layout, best first: two candidates per CTA
-// with the next-MB prefetch, one with the prefetch, two without, one
-// without (the slot rings and staging in shared memory); otherwise, when
-// `gslots` can provide them, the rings in global memory. The prefetch needs
-// planes whose rows allow aligned 16- and 8-byte asynchronous copies.
+// in device memory at a.cands, with the slot rings and staging in shared
+// memory (pick_layout); otherwise, when `gst` can provide them, with the
+// rings in global memory. The prefetch needs planes whose rows allow
+// aligned 16- and 8-byte asynchronous copies.
 vp8a_status run_sweep(vp8a_ctx* ctx, LfArgs a, int n, vp8a::Stager* gst) {
   if (n == 0) return VP8A_OK;
   a.n_cands = n;
-  a.ring_bytes = a.mb_rows * RING * SLOT_STRIDE;
+  a.ring_bytes = (a.row_set ? a.n_sets : a.mb_rows) * RING * SLOT_STRIDE;
   int max_smem = 0;
   VP8A_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
   const int threads = std::min(1024, std::max(32, (16 * a.max_active + 31) / 32 * 32));
   auto al = [](const void* p, uint64_t stride, unsigned k) { return ((uintptr_t)p % k == 0) && (stride % k == 0); };
   bool pre_ok = al(a.y, a.ys, 16) && al(a.u, a.cs, 8) && al(a.v, a.cs, 8) && (uintptr_t)a.mbs % 8 == 0;
   if (a.ssd_out) pre_ok = pre_ok && al(a.sy, a.sys, 16) && al(a.su, a.scs, 8) && al(a.sv, a.scs, 8);
-  const size_t stage_bytes = (size_t)(threads / 16) * sizeof(Stage);
-  cudaFuncAttributes f1, f2;
+  cudaFuncAttributes f1;
   VP8A_CUDA(cudaFuncGetAttributes(&f1, lf_sweep_kernel<1>));
-  VP8A_CUDA(cudaFuncGetAttributes(&f2, lf_sweep_kernel<2>));
-  const struct {
-    int nc;
-    bool pre;
-  } opts[4] = {{2, true}, {1, true}, {2, false}, {1, false}};
-  for (const auto& o : opts) {
-    if ((o.nc == 2 && n < 2) || (o.pre && !pre_ok)) continue;
-    const size_t rings = (size_t)o.nc * a.ring_bytes, total = rings + (o.pre ? stage_bytes : 0);
-    const size_t stat = o.nc == 2 ? f2.sharedSizeBytes : f1.sharedSizeBytes;
-    if (total + stat + 1024 > (size_t)max_smem) continue;
+  SweepLayout L;
+  if (pick_layout(ctx, n, a.ring_bytes, pre_ok, threads, false, &L)) {
     a.smem_slots = 1;
     a.gslots = nullptr;
-    a.prefetch = o.pre;
-    a.stage_off = (int)rings;
-    const int grid = (n + o.nc - 1) / o.nc;
-    if (o.nc == 2) {
-      VP8A_CUDA(cudaFuncSetAttribute(lf_sweep_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)total));
-      lf_sweep_kernel<2><<<grid, threads, total, ctx->stream>>>(a);
-    } else {
-      VP8A_CUDA(cudaFuncSetAttribute(lf_sweep_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)total));
-      lf_sweep_kernel<1><<<grid, threads, total, ctx->stream>>>(a);
-    }
-    VP8A_CUDA(cudaGetLastError());
-    ctx->launches++;
-    return VP8A_OK;
+    a.prefetch = L.pre;
+    a.stage_off = L.nc * a.ring_bytes;
+    return launch_variant(ctx, L.nc, (unsigned)((n + L.nc - 1) / L.nc), threads, L.smem, a, nullptr, nullptr, 0);
   }
   if (!gst) {
     vp8a::set_error("the MB rows' slot rings do not fit in shared memory");
@@ -882,13 +1031,78 @@ vp8a_status run_sweep(vp8a_ctx* ctx, LfArgs a, int n, vp8a::Stager* gst) {
   if ((s = gst->scratch((size_t)a.ring_bytes * n, &g)) != VP8A_OK) return s;
   a.smem_slots = 0;
   a.gslots = (uint8_t*)g;
-  a.prefetch = pre_ok && stage_bytes + f1.sharedSizeBytes + 1024 <= (size_t)max_smem;
+  a.prefetch = pre_ok && sweep_smem(0, 0, true, threads) + f1.sharedSizeBytes + 1024 <= (size_t)max_smem;
   a.stage_off = 0;
-  const size_t total = a.prefetch ? stage_bytes : 0;
-  VP8A_CUDA(cudaFuncSetAttribute(lf_sweep_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)total));
-  lf_sweep_kernel<1><<<n, threads, total, ctx->stream>>>(a);
-  VP8A_CUDA(cudaGetLastError());
-  ctx->launches++;
+  return launch_variant(ctx, 1, (unsigned)n, threads, sweep_smem(0, 0, a.prefetch, threads), a, nullptr, nullptr, 0);
+}
+
+// The whole 64 x 8 grid as distinct filter passes. Two sharpness values
+// of one level filter identically when every MB level the configuration can
+// produce from that level (each segment, reference and mode class of
+// calculate_mb_filter_level_inter) has the same interior limit under both:
+// the interior limit and the level fix every parameter of the §15 filters
+// (LoopFilterParams::derive, src/loop_filter.rs:99-148). Each pass fills the
+// table entries of its sharpness group (`masks`); level 0 is one pass for
+// all eight (score_filter_candidate's unfiltered short cut).
+void grid_candidates(const vp8a_filter_config& base, std::vector<uint8_t>& pairs, std::vector<uint8_t>& masks) {
+  pairs.assign({0, 0});
+  masks.assign({0xff});
+  std::vector<vp8a_mb_lf_info> classes;
+  const int nseg = base.segmentation_enabled ? 4 : 1;
+  for (int seg = 0; seg < nseg; seg++) {
+    vp8a_mb_lf_info m{};
+    m.segment_id = (int8_t)seg;
+    m.ref_frame = VP8A_REF_INTRA;
+    m.inter_mode = VP8A_MODE_NONE;
+    for (int bp = 0; bp < 2; bp++) {
+      m.y_mode_is_bpred = (uint8_t)bp;
+      classes.push_back(m);
+    }
+    m.y_mode_is_bpred = 0;
+    for (int ref = VP8A_REF_LAST; ref <= VP8A_REF_ALTREF; ref++)
+      for (int mode : {VP8A_MODE_ZERO, VP8A_MODE_SPLIT, VP8A_MODE_NEAREST}) {
+        m.ref_frame = (uint8_t)ref;
+        m.inter_mode = (uint8_t)mode;
+        classes.push_back(m);
+      }
+  }
+  for (int level = 1; level < 64; level++) {
+    uint8_t done = 0;
+    for (int s0 = 0; s0 < 8; s0++) {
+      if (done >> s0 & 1) continue;
+      uint8_t mask = 0;
+      for (int s1 = s0; s1 < 8; s1++) {
+        bool same = true;
+        for (const auto& m : classes) {
+          const int l = mb_level(base, level, m);
+          if (l != 0 && interior_limit(l, s0) != interior_limit(l, s1)) same = false;
+        }
+        if (same) mask |= (uint8_t)(1u << s1);
+      }
+      done |= mask;
+      pairs.push_back((uint8_t)level);
+      pairs.push_back((uint8_t)s0);
+      masks.push_back(mask);
+    }
+  }
+}
+
+// Upload a grid's candidate pairs and masks into `a`.
+vp8a_status upload_grid(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_filter_config& base, LfArgs* a) {
+  std::vector<uint8_t> pairs, masks;
+  grid_candidates(base, pairs, masks);
+  const size_t n = masks.size();
+  std::vector<uint8_t> blob(3 * n);
+  memcpy(blob.data(), pairs.data(), 2 * n);
+  memcpy(blob.data() + 2 * n, masks.data(), n);
+  void* d;
+  vp8a_status s;
+  if ((s = st.scratch(blob.size(), &d)) != VP8A_OK) return s;
+  VP8A_CUDA(cudaMemcpyAsync(d, blob.data(), blob.size(), cudaMemcpyHostToDevice, ctx->stream));
+  VP8A_CUDA(cudaStreamSynchronize(ctx->stream));  // the host blob goes out of scope
+  a->cands = (const uint8_t*)d;
+  a->cand_mask = (const uint8_t*)d + 2 * n;
+  a->n_cands = (int)n;
   return VP8A_OK;
 }
 
@@ -1088,18 +1302,8 @@ vp8a_status vp8a_filter_sweep(vp8a_ctx* ctx, const vp8a_planes* planes, const vp
   if ((s = st.out(ssd_out, 512 * sizeof(uint64_t), &dt)) != VP8A_OK) return s;
   L.a.ssd_out = (uint64_t*)dt;
   L.a.level0_unfiltered = 1;
-  // One level-0 candidate plus every (level 1..63, sharpness 0..7).
-  std::vector<uint8_t> c;
-  c.reserve(2 * 505);
-  c.push_back(0);
-  c.push_back(0);
-  for (int l = 1; l < 64; l++)
-    for (int sh = 0; sh < 8; sh++) {
-      c.push_back((uint8_t)l);
-      c.push_back((uint8_t)sh);
-    }
-  if ((s = launch_sweep(ctx, st, L.a, c.data(), (int)(c.size() / 2))) != VP8A_OK) return s;
-  st.force_sync();  // the candidate vector must outlive its async copy
+  if ((s = upload_grid(ctx, st, *base, &L.a)) != VP8A_OK) return s;
+  if ((s = run_sweep(ctx, L.a, L.a.n_cands, &st)) != VP8A_OK) return s;
   return st.finish();
 }
 
@@ -1116,17 +1320,6 @@ vp8a_status vp8a_filter_sweeps(vp8a_ctx* ctx, const vp8a_sweep_job* jobs, uint32
   VP8A_CUDA(cudaSetDevice(ctx->device));
   vp8a::Stager st(ctx);
   vp8a_status s;
-  // The whole grid's candidates, shared by every job.
-  std::vector<uint8_t> c{0, 0};
-  for (int l = 1; l < 64; l++)
-    for (int sh = 0; sh < 8; sh++) {
-      c.push_back((uint8_t)l);
-      c.push_back((uint8_t)sh);
-    }
-  const int n_c = (int)(c.size() / 2);
-  void* dc;
-  if ((s = st.scratch(c.size(), &dc)) != VP8A_OK) return s;
-  VP8A_CUDA(cudaMemcpyAsync(dc, c.data(), c.size(), cudaMemcpyHostToDevice, ctx->stream));
   std::vector<LfArgs> args(n_jobs);
   for (uint32_t j = 0; j < n_jobs; j++) {
     const vp8a_sweep_job& J = jobs[j];
@@ -1140,9 +1333,8 @@ vp8a_status vp8a_filter_sweeps(vp8a_ctx* ctx, const vp8a_sweep_job* jobs, uint32
     if ((s = st.out(J.ssd_out, 512 * sizeof(uint64_t), &dt)) != VP8A_OK) return s;
     L.a.ssd_out = (uint64_t*)dt;
     L.a.level0_unfiltered = 1;
-    L.a.cands = (const uint8_t*)dc;
-    L.a.n_cands = n_c;
-    L.a.ring_bytes = L.a.mb_rows * RING * SLOT_STRIDE;
+    if ((s = upload_grid(ctx, st, J.base, &L.a)) != VP8A_OK) return s;
+    L.a.ring_bytes = L.a.n_sets * RING * SLOT_STRIDE;
     args[j] = L.a;
   }
   // One launch for every job whose slot rings fit in shared memory (two
@@ -1166,8 +1358,7 @@ vp8a_status vp8a_filter_sweeps(vp8a_ctx* ctx, const vp8a_sweep_job* jobs, uint32
     const int t = std::max(threads, threads_of(args[j]));
     const int r = std::max(max_ring, args[j].ring_bytes);
     const bool p = pre && pre_of(args[j]);
-    const size_t need = (size_t)r + (p ? (size_t)(t / 16) * sizeof(Stage) : 0) + f1.sharedSizeBytes + 1024;
-    if (need > (size_t)max_smem) {
+    if (sweep_smem(1, r, p, t) + f1.sharedSizeBytes + 1024 > (size_t)max_smem) {
       alone.push_back(j);
       continue;
     }
@@ -1177,9 +1368,18 @@ vp8a_status vp8a_filter_sweeps(vp8a_ctx* ctx, const vp8a_sweep_job* jobs, uint32
     pre = p;
   }
   if (!group.empty()) {
-    const size_t stage_bytes = pre ? (size_t)(threads / 16) * sizeof(Stage) : 0;
-    const int nc = (size_t)2 * max_ring + stage_bytes + f2.sharedSizeBytes + 1024 <= (size_t)max_smem ? 2 : 1;
-    const size_t total = (size_t)nc * max_ring + stage_bytes;
+    // The layout for the largest job's rings and the group's candidates
+    // (each CTA takes `nc` candidates of one job).
+    long n_all = 0;
+    for (uint32_t j : group) n_all += args[j].n_cands;
+    SweepLayout L{1, pre, sweep_smem(1, max_ring, pre, threads)};
+    if (!pick_layout(ctx, (int)std::min<long>(n_all, 1 << 30), max_ring, pre, threads, true, &L)) {
+      vp8a::set_error("no sweep layout fits in shared memory");
+      return VP8A_E_CUDA;
+    }
+    const int nc = L.nc;
+    pre = L.pre;
+    const size_t total = L.smem;
     std::vector<LfArgs> table;
     std::vector<uint32_t> start{0};
     for (uint32_t j : group) {
@@ -1189,7 +1389,7 @@ vp8a_status vp8a_filter_sweeps(vp8a_ctx* ctx, const vp8a_sweep_job* jobs, uint32
       a.prefetch = pre;
       a.stage_off = nc * a.ring_bytes;
       table.push_back(a);
-      start.push_back(start.back() + (uint32_t)((n_c + nc - 1) / nc));
+      start.push_back(start.back() + (uint32_t)((a.n_cands + nc - 1) / nc));
     }
     const size_t o_start = sizeof(LfArgs) * table.size(), bytes = o_start + sizeof(uint32_t) * start.size();
     std::vector<uint8_t> blob(bytes);
@@ -1199,23 +1399,12 @@ vp8a_status vp8a_filter_sweeps(vp8a_ctx* ctx, const vp8a_sweep_job* jobs, uint32
     if ((s = st.scratch(bytes, &d)) != VP8A_OK) return s;
     VP8A_CUDA(cudaMemcpyAsync(d, blob.data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
     VP8A_CUDA(cudaStreamSynchronize(ctx->stream));  // the host tables go out of scope
-    const LfArgs* dj = (const LfArgs*)d;
-    const uint32_t* ds = (const uint32_t*)((const uint8_t*)d + o_start);
-    if (nc == 2) {
-      VP8A_CUDA(cudaFuncSetAttribute(lf_sweep_batch_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)total));
-      lf_sweep_batch_kernel<2><<<start.back(), threads, total, ctx->stream>>>(dj, ds, (int)table.size());
-    } else {
-      VP8A_CUDA(cudaFuncSetAttribute(lf_sweep_batch_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)total));
-      lf_sweep_batch_kernel<1><<<start.back(), threads, total, ctx->stream>>>(dj, ds, (int)table.size());
-    }
-    VP8A_CUDA(cudaGetLastError());
-    ctx->launches++;
+    if ((s = launch_variant(ctx, nc, start.back(), threads, total, table[0], (const LfArgs*)d,
+                            (const uint32_t*)((const uint8_t*)d + o_start), (int)table.size())) != VP8A_OK)
+      return s;
   }
   for (uint32_t j : alone)
-    if ((s = run_sweep(ctx, args[j], n_c, &st)) != VP8A_OK) return s;
-  st.force_sync();  // the candidate vector must outlive its async copy
+    if ((s = run_sweep(ctx, args[j], args[j].n_cands, &st)) != VP8A_OK) return s;
   return st.finish();
 }
 
@@ -1269,7 +1458,7 @@ vp8a_status vp8a_select_filter_params(vp8a_ctx* ctx, const vp8a_planes* planes, 
     const uint8_t zero = 0;
     if ((s = st.write_from_host(level_out, &zero, 1)) != VP8A_OK) return s;
     if ((s = st.write_from_host(sharpness_out, &bs, 1)) != VP8A_OK) return s;
-    return st.finish();
+      return st.finish();
   }
   // Stage 2: the other sharpness values at the chosen level.
   c.clear();

@@ -84,6 +84,22 @@ def test_sweep_tall_pictures(ctx, oracle, size):
     assert np.array_equal(got, want)
 
 
+@pytest.mark.parametrize("size,every_rows", [((400, 16), 0), ((4096, 64), 0), ((320, 240), 0), ((320, 240), 3),
+                                             ((1920, 96), 0)])
+def test_sweep_grid_groups_with_segments_and_deltas(ctx, oracle, size, every_rows):
+    # The sweep scores one pass per group of sharpness values whose interior
+    # limits agree at every MB level the configuration can produce, and
+    # fills the group's table entries from it. Segment and delta levels make
+    # the groups uneven; wide and short pictures take few half-warps per
+    # step; the oracle scores every (level, sharpness) on its own.
+    src, recon, m = lf_case(*size, seed=size[0] + size[1])
+    base = abi.filter_config(0, 3, segmentation_enabled=1, segment_abs=0, segment_lf_level=[-20, 4, 9, 0],
+                             delta_enabled=1, ref_delta_golden=5, split_mv_mode_delta=-4)
+    got = vp8a.filter_sweep(ctx, recon, m, base, src, every_rows)
+    want = oracle.filter_sweep(recon, m, base, src, every_rows, threads=8)
+    assert np.array_equal(got, want)
+
+
 def test_sweep_unaligned_strides(ctx, oracle):
     # Row strides that allow neither word nor asynchronous copies.
     src, recon, m = lf_case(96, 72, seed=11)
