@@ -957,7 +957,9 @@ size_t sweep_smem(int nc, int ring, bool pre, int threads) {
 // the prefetch, among those whose shared memory fits, by an estimate of
 // the time: whole waves of CTAs over the GPU x candidates per CTA (a CTA's
 // steps carry every candidate's filtering), 15 % more without the
-// prefetch. Returns false when no layout fits.
+// prefetch and 20 % less per candidate when a CTA carries several (their
+// filtering shares each step's barrier and loads) — factors measured on
+// the 1080p and 640x368 sweeps. Returns false when no layout fits.
 struct SweepLayout {
   int nc;
   bool pre;
@@ -985,7 +987,7 @@ bool pick_layout(vp8a_ctx* ctx, int n, int ring, bool pre_ok, int threads, bool 
       if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem) != cudaSuccess) return false;
       if (per_sm < 1) continue;
       const long ctas = (n + nc - 1) / nc, slots = (long)ctx->sm_count * per_sm;
-      const double cost = (double)((ctas + slots - 1) / slots) * nc * (pre ? 1.0 : 1.15);
+      const double cost = (double)((ctas + slots - 1) / slots) * nc * (pre ? 1.0 : 1.15) * (nc > 1 ? 0.8 : 1.0);
       if (cost < best) {
         best = cost;
         *out = SweepLayout{nc, pre != 0, smem};
