@@ -78,6 +78,8 @@ struct LfArgs {
   int n_sets;
   int recon_words;           // planes and strides allow 4-byte accesses
   int source_words;
+  int recon_vec;   // luma rows allow 16-byte and chroma rows 8-byte loads
+  int source_vec;
   // Next-step prefetch: each half-warp copies its next MB's reconstruction,
   // source rows and MB record into its own staging area (dynamic shared
   // memory at byte stage_off) while the current step runs (cp.async).
@@ -250,7 +252,17 @@ __device__ __forceinline__ MbWords fetch_recon(const LfArgs& a, int r, int c, in
   MbWords w;
   const uint8_t* gy = a.y + (size_t)(r * 16 + l) * a.ys + (size_t)c * 16;
   const uint8_t* gc = (l < 8 ? a.u : a.v) + (size_t)(r * 8 + (l & 7)) * a.cs + (size_t)c * 8;
-  if (a.recon_words) {
+  if (a.recon_vec) {
+    // Plain loads: apply mode writes final MBs back into these planes.
+    const uint4 y4 = *(const uint4*)gy;
+    const uint2 c2 = *(const uint2*)gc;
+    w.y[0] = y4.x;
+    w.y[1] = y4.y;
+    w.y[2] = y4.z;
+    w.y[3] = y4.w;
+    w.c[0] = c2.x;
+    w.c[1] = c2.y;
+  } else if (a.recon_words) {
 #pragma unroll
     for (int k = 0; k < 4; k++) w.y[k] = ((const uint32_t*)gy)[k];
     w.c[0] = ((const uint32_t*)gc)[0];
@@ -307,7 +319,13 @@ __device__ __forceinline__ SrcWords fetch_source(const LfArgs& a, int r, int c, 
   }
   if (ny > 0) {
     const uint8_t* p = a.sy + (size_t)yy * a.sys + x0;
-    if (ny == 16 && a.source_words) {
+    if (ny == 16 && a.source_vec) {
+      const uint4 v = __ldg((const uint4*)p);
+      w.y[0] = v.x;
+      w.y[1] = v.y;
+      w.y[2] = v.z;
+      w.y[3] = v.w;
+    } else if (ny == 16 && a.source_words) {
 #pragma unroll
       for (int k = 0; k < 4; k++) w.y[k] = ((const uint32_t*)p)[k];
     } else {
@@ -318,7 +336,11 @@ __device__ __forceinline__ SrcWords fetch_source(const LfArgs& a, int r, int c, 
   }
   if (nc > 0) {
     const uint8_t* p = (l < 8 ? a.su : a.sv) + (size_t)cy * a.scs + cx0;
-    if (nc == 8 && a.source_words) {
+    if (nc == 8 && a.source_vec) {
+      const uint2 v = __ldg((const uint2*)p);
+      w.c[0] = v.x;
+      w.c[1] = v.y;
+    } else if (nc == 8 && a.source_words) {
       w.c[0] = ((const uint32_t*)p)[0];
       w.c[1] = ((const uint32_t*)p)[1];
     } else {
@@ -919,6 +941,9 @@ vp8a_status stage_lf(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_planes* planes,
   auto al4 = [](const void* p, uint64_t stride) { return ((uintptr_t)p % 4 == 0) && (stride % 4 == 0); };
   a.recon_words = al4(a.y, a.ys) && al4(a.u, a.cs) && al4(a.v, a.cs);
   a.source_words = a.sy ? (al4(a.sy, a.sys) && al4(a.su, a.scs) && al4(a.sv, a.scs)) : 0;
+  auto alk = [](const void* p, uint64_t stride, unsigned k) { return ((uintptr_t)p % k == 0) && (stride % k == 0); };
+  a.recon_vec = alk(a.y, a.ys, 16) && alk(a.u, a.cs, 8) && alk(a.v, a.cs, 8);
+  a.source_vec = a.sy ? (alk(a.sy, a.sys, 16) && alk(a.su, a.scs, 8) && alk(a.sv, a.scs, 8)) : 0;
   L->max_steps = a.steps;
   return VP8A_OK;
 }
