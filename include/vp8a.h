@@ -303,8 +303,10 @@ vp8a_status vp8a_motion_descent(vp8a_ctx* ctx, const vp8a_luma_ref* ref,
  * `mv_contexts` NULL means the §17.2 defaults; `lambda` is the RD
  * multiplier (rd_lambda, src/encoder.rs:3742). Writes mb_cols*mb_rows
  * decisions in raster order; `trace` (optional) receives n_refs entries
- * per MB. The MB-row wavefront of the reference (row r waits for row r-1
- * to be two MBs ahead) runs on the device. */
+ * per MB. The MB-row wavefront runs on the device: MB (r, c) starts once
+ * MB (r-1, c) is decided (its census neighbours are the above, left and
+ * above-left MBs; the reference's row contract also waits for the
+ * above-right MB, which only its intra candidates read). */
 vp8a_status vp8a_analyse_inter_frame(vp8a_ctx* ctx, const vp8a_i420* frame,
                                      const vp8a_planes* refs, const uint8_t* ref_ids,
                                      uint32_t n_refs, const vp8a_mv_contexts* mv_contexts,

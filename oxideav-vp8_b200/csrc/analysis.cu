@@ -976,10 +976,17 @@ __global__ void __launch_bounds__(AN_THREADS, 1)
     }
     for (int c = 0; c < a.mb_cols; c++) {
       // Rank 0 waits for the row above; the cluster follows its verdict.
+      // MB (r, c) reads the records of its above, left and above-left
+      // neighbours only (find_near_mvs, SPLITMV LEFT/ABOVE sub-MVs), so it
+      // needs MB (r - 1, c) done. The reference's row contract waits for
+      // (r - 1, c + 1) (src/encoder/inter.rs:350-513) because its intra
+      // candidates predict from the above-right MB's reconstruction; with
+      // intra picking off nothing here reads that MB, and the decisions do
+      // not depend on the schedule.
       if (k == 0 && tid == 0) {
         int abort = 0;
         if (r > 0) {
-          const unsigned need = (unsigned)min(c + 2, a.mb_cols);
+          const unsigned need = (unsigned)(c + 1);
           unsigned long long it = 0;
           while (ld_acquire(&a.progress[r - 1]) < need) {
             if (*(volatile unsigned*)a.status != 0u || ++it > a.spin_limit) {
