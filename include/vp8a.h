@@ -589,6 +589,54 @@ typedef struct vp8a_sweep_job {
  * larger pictures otherwise run as their own launches). */
 vp8a_status vp8a_filter_sweeps(vp8a_ctx* ctx, const vp8a_sweep_job* jobs, uint32_t n_jobs);
 
+/* ------------------------------------------- learned motion proposal
+ *
+ * No counterpart in the reference: the learned proposal the survey builds
+ * beside the plain search. A 4-layer 3x3 conv net (32 channels, BF16
+ * weights and activations, FP32 accumulation on the tensor cores) maps an
+ * MB's coarse cost volume against a reference (2 x 32 x 32: at each of a
+ * 32 x 32 grid of whole-pel vectors 2 px apart, cell (i, j) = (2 (i - 16),
+ * 2 (j - 16)) px, the half-resolution SAD of the MB and the reference's
+ * texture) to scores over that grid; its best cells seed an exact local
+ * search with the plain search's SAD kernels. All buffers are
+ * device memory of the context's GPU; all calls are stream-ordered on the
+ * context stream and allocate nothing. Activations are NHWC [n][32][32][C]
+ * BF16 (uint16 bit patterns); weights [cout][9][cin] with tap
+ * (dy + 1) * 3 + (dx + 1). */
+
+/* The net's input for n MBs: item i is the MB at mb_xy[2i], mb_xy[2i+1]
+ * (column, row); out = [n][32][32][2] BF16: (32 - the mean absolute
+ * difference of the 2x2-averaged MB and reference block at the cell's
+ * vector) / 32, and (the averaged reference at the block's centre - 128) /
+ * 64. `src` and `ref` are visible luma planes of one size. */
+vp8a_status vp8a_lp_windows(vp8a_ctx* ctx, const vp8a_luma_ref* src, const vp8a_luma_ref* ref,
+                            const uint32_t* mb_xy, uint32_t n, uint16_t* out);
+
+/* One conv layer (cin -> cout in {2->32, 32->32, 32->1}) over n images,
+ * + bias, ReLU when `relu`; output BF16 `y` or FP32 `y_f32` (one of them). */
+vp8a_status vp8a_lp_conv_forward(vp8a_ctx* ctx, const uint16_t* x, uint32_t cin, const uint16_t* w,
+                                 const float* bias, uint32_t cout, uint32_t n, uint32_t relu,
+                                 uint16_t* y, float* y_f32);
+
+/* Its gradients: `dw` (cout*9*cin) and `db` (cout) FP32 are accumulated
+ * into (zero them first); `dx` (optional, BF16) = the gradient w.r.t. x,
+ * multiplied by (x > 0) when `x_relu` (x came out of a ReLU). */
+vp8a_status vp8a_lp_conv_backward(vp8a_ctx* ctx, const uint16_t* x, uint32_t cin, const uint16_t* w,
+                                  uint32_t cout, uint32_t n, const uint16_t* dy, uint32_t x_relu,
+                                  uint16_t* dx, float* dw, float* db);
+
+/* Softmax over each item's 1024 scores; with `labels` (cell index, < 0 =
+ * none): the summed cross-entropy added to `loss`, d(scores) =
+ * (softmax - onehot) / n into `dlogits` (BF16) and the label's probability
+ * into `label_prob` (each optional). */
+vp8a_status vp8a_lp_softmax_ce(vp8a_ctx* ctx, const float* logits, const int32_t* labels, uint32_t n,
+                               uint16_t* dlogits, float* loss, float* label_prob);
+
+/* One Adam step (bias-corrected for `step` >= 1) on FP32 master weights;
+ * writes their BF16 copies. */
+vp8a_status vp8a_lp_adam(vp8a_ctx* ctx, float* w, const float* grad, float* m, float* v, uint32_t n,
+                         float lr, float beta1, float beta2, float eps, uint32_t step, uint16_t* w_bf16);
+
 #ifdef __cplusplus
 }
 #endif

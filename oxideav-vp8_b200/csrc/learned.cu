@@ -1,0 +1,436 @@
+// learned.cu — the learned motion proposal: a 4-layer 3x3 conv net (BF16
+// weights and activations, FP32 accumulation) that scores a 32x32 grid of
+// whole-pel vectors (2 px apart, -32 .. +30 px) for an MB from a coarse
+// cost volume: at each grid vector, the half-resolution SAD of the MB
+// against the reference and the reference's texture there. Its top four
+// cells seed an exact local search (the plain search's SAD kernels), so
+// the net only proposes; every returned vector and SAD is exact.
+//
+// Kernels (all hand-written; the GEMM-shaped ones on the tensor cores with
+// mma.sync m16n8k16 BF16 -> FP32):
+//   lp_windows_kernel       coarse cost volumes -> NHWC [n, 32, 32, 2] BF16
+//   lp_conv_fwd_kernel      implicit-GEMM conv (+ bias, ReLU), one warp per
+//                           16 output pixels x all output channels
+//   lp_conv_bwd_data_kernel dX = conv^T(dY, W), masked by the ReLU of X
+//   lp_conv_bwd_w_kernel    dW = sum over pixels of dY x shifted X (split
+//                           over pixel chunks, FP32 atomics), db
+//   lp_softmax_ce_kernel    softmax over the 1024 cells, cross-entropy,
+//                           d(logits) = (p - onehot) / n
+//   lp_adam_kernel          Adam on FP32 master weights, BF16 copies
+// Layout: activations NHWC, 32x32 pixels per MB, channel count 2 or 32
+// (the last layer 1); weights [cout][tap][cin], tap = (dy + 1) * 3 + dx + 1.
+#include <cuda_bf16.h>
+
+#include "vp8a_internal.cuh"
+
+namespace {
+
+constexpr int LP_S = 32;          // image side
+constexpr int LP_P = LP_S * LP_S; // pixels per image
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t*>(&v);
+}
+__device__ __forceinline__ uint32_t pack_raw(uint16_t lo, uint16_t hi) { return (uint32_t)lo | ((uint32_t)hi << 16); }
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// Element (pixel q of image img shifted by (dy, dx), channel c) of an NHWC
+// BF16 tensor with C channels, 0 outside the image or past C.
+__device__ __forceinline__ uint16_t act(const uint16_t* X, int C, int img, int y, int x, int c) {
+  if (y < 0 || y >= LP_S || x < 0 || x >= LP_S || c >= C) return 0;
+  return X[((size_t)img * LP_P + y * LP_S + x) * C + c];
+}
+
+// ---------------------------------------------------------------- windows
+
+// Item i: the MB at (xy[2i], xy[2i+1]). Both pictures are averaged over
+// 2x2 (rounded) and edge-clamped: the MB to 8x8, the reference around it
+// (80x80 pixels, the MB at [32, 48)) to 40x40. Cell (i, j) is the vector
+// (2 (i - 16), 2 (j - 16)) px: channel 0 = (32 - mean |MB - reference block
+// at that vector|) / 32, channel 1 = (reference at the block's centre - 128)
+// / 64.
+__global__ void __launch_bounds__(256) lp_windows_kernel(const uint8_t* src, uint64_t ss, const uint8_t* ref,
+                                                         uint64_t rs, int w, int h, const uint32_t* xy, int n,
+                                                         uint16_t* out) {
+  __shared__ uint8_t rw[40 * 40];
+  __shared__ uint8_t mb[64];
+  const int i = blockIdx.x, t = threadIdx.x;
+  if (i >= n) return;
+  const int mx = (int)xy[2 * i] * 16, my = (int)xy[2 * i + 1] * 16;
+  auto avg2 = [&](const uint8_t* p, uint64_t st, int y, int x) -> int {
+    int s = 0;
+    for (int a = 0; a < 2; a++)
+      for (int b = 0; b < 2; b++) s += p[(size_t)min(max(y + a, 0), h - 1) * st + min(max(x + b, 0), w - 1)];
+    return (s + 2) >> 2;
+  };
+  for (int q = t; q < 40 * 40; q += blockDim.x)
+    rw[q] = (uint8_t)avg2(ref, rs, my - 32 + 2 * (q / 40), mx - 32 + 2 * (q % 40));
+  if (t < 64) mb[t] = (uint8_t)avg2(src, ss, my + 2 * (t >> 3), mx + 2 * (t & 7));
+  __syncthreads();
+  for (int q = t; q < LP_P; q += blockDim.x) {
+    const int oy = q >> 5, ox = q & 31;  // block origin in the 40x40 window
+    int sad = 0;
+#pragma unroll 8
+    for (int k = 0; k < 64; k++) {
+      const int d = (int)mb[k] - (int)rw[(oy + (k >> 3)) * 40 + ox + (k & 7)];
+      sad += d < 0 ? -d : d;
+    }
+    const float c0 = (32.0f - (float)sad * (1.0f / 64.0f)) * (1.0f / 32.0f);
+    const float c1 = ((float)rw[(oy + 4) * 40 + ox + 4] - 128.0f) * (1.0f / 64.0f);
+    *reinterpret_cast<uint32_t*>(out + ((size_t)i * LP_P + q) * 2) = pack_bf16(c0, c1);
+  }
+}
+
+// ------------------------------------------------------------ conv fwd
+
+// One warp per 16 output pixels (one half row) x COUT (NT tiles of 8).
+// A[p][k] = X[p + off(tap)][ci], k = tap * CP + ci (CP = CIN rounded up to
+// 16); B[k][n] = W[n][tap][ci].
+template <int CIN, int NT>
+__global__ void __launch_bounds__(128) lp_conv_fwd_kernel(const uint16_t* X, const uint16_t* W, const float* bias,
+                                                          int cout, int n_img, int relu, uint16_t* Y, float* Yf) {
+  constexpr int CP = (CIN + 15) / 16 * 16;
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int tile = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (tile >= n_img * (LP_P / 16)) return;
+  const int img = tile / (LP_P / 16), rem = tile % (LP_P / 16), y = rem >> 1, xb = (rem & 1) * 16;
+  float d[NT][4];
+#pragma unroll
+  for (int j = 0; j < NT; j++) d[j][0] = d[j][1] = d[j][2] = d[j][3] = 0.f;
+  for (int tap = 0; tap < 9; tap++) {
+    const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+#pragma unroll
+    for (int c0 = 0; c0 < CP; c0 += 16) {
+      uint32_t a[4];
+      const int ca = c0 + 2 * t, cb = c0 + 2 * t + 8;
+      a[0] = pack_raw(act(X, CIN, img, y + dy, xb + g + dx, ca), act(X, CIN, img, y + dy, xb + g + dx, ca + 1));
+      a[1] = pack_raw(act(X, CIN, img, y + dy, xb + g + 8 + dx, ca), act(X, CIN, img, y + dy, xb + g + 8 + dx, ca + 1));
+      a[2] = pack_raw(act(X, CIN, img, y + dy, xb + g + dx, cb), act(X, CIN, img, y + dy, xb + g + dx, cb + 1));
+      a[3] = pack_raw(act(X, CIN, img, y + dy, xb + g + 8 + dx, cb), act(X, CIN, img, y + dy, xb + g + 8 + dx, cb + 1));
+#pragma unroll
+      for (int j = 0; j < NT; j++) {
+        const int n = j * 8 + g;
+        auto wv = [&](int ci) -> uint16_t {
+          return (n < cout && ci < CIN) ? W[((size_t)n * 9 + tap) * CIN + ci] : (uint16_t)0;
+        };
+        const uint32_t b[2] = {pack_raw(wv(ca), wv(ca + 1)), pack_raw(wv(cb), wv(cb + 1))};
+        mma_bf16(d[j], a, b);
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < NT; j++) {
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int p = y * LP_S + xb + g + 8 * h;
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const int n = j * 8 + 2 * t + e;
+        if (n >= cout) continue;
+        float v = d[j][2 * h + e] + bias[n];
+        if (relu) v = fmaxf(v, 0.f);
+        const size_t o = ((size_t)img * LP_P + p) * cout + n;
+        if (Yf) Yf[o] = v;
+        else Y[o] = __bfloat16_as_ushort(__float2bfloat16_rn(v));
+      }
+    }
+  }
+}
+
+// --------------------------------------------------------- conv bwd data
+
+// dX[p][ci] = sum over taps and co of dY[p - off(tap)][co] W[co][tap][ci],
+// times (Xa[p][ci] > 0) when `mask` (the ReLU of the layer that produced X).
+template <int COUT, int NT>
+__global__ void __launch_bounds__(128) lp_conv_bwd_data_kernel(const uint16_t* dY, const uint16_t* W, int cin,
+                                                               int n_img, const uint16_t* Xa, uint16_t* dX) {
+  constexpr int KP = (COUT + 15) / 16 * 16;
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int tile = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (tile >= n_img * (LP_P / 16)) return;
+  const int img = tile / (LP_P / 16), rem = tile % (LP_P / 16), y = rem >> 1, xb = (rem & 1) * 16;
+  float d[NT][4];
+#pragma unroll
+  for (int j = 0; j < NT; j++) d[j][0] = d[j][1] = d[j][2] = d[j][3] = 0.f;
+  for (int tap = 0; tap < 9; tap++) {
+    const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+#pragma unroll
+    for (int c0 = 0; c0 < KP; c0 += 16) {
+      uint32_t a[4];
+      const int ca = c0 + 2 * t, cb = c0 + 2 * t + 8;
+      // dY at p - off: the output pixel whose tap `tap` reads p.
+      a[0] = pack_raw(act(dY, COUT, img, y - dy, xb + g - dx, ca), act(dY, COUT, img, y - dy, xb + g - dx, ca + 1));
+      a[1] = pack_raw(act(dY, COUT, img, y - dy, xb + g + 8 - dx, ca),
+                      act(dY, COUT, img, y - dy, xb + g + 8 - dx, ca + 1));
+      a[2] = pack_raw(act(dY, COUT, img, y - dy, xb + g - dx, cb), act(dY, COUT, img, y - dy, xb + g - dx, cb + 1));
+      a[3] = pack_raw(act(dY, COUT, img, y - dy, xb + g + 8 - dx, cb),
+                      act(dY, COUT, img, y - dy, xb + g + 8 - dx, cb + 1));
+#pragma unroll
+      for (int j = 0; j < NT; j++) {
+        const int n = j * 8 + g;  // ci
+        auto wv = [&](int co) -> uint16_t {
+          return (n < cin && co < COUT) ? W[((size_t)co * 9 + tap) * cin + n] : (uint16_t)0;
+        };
+        const uint32_t b[2] = {pack_raw(wv(ca), wv(ca + 1)), pack_raw(wv(cb), wv(cb + 1))};
+        mma_bf16(d[j], a, b);
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < NT; j++)
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int p = y * LP_S + xb + g + 8 * h;
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const int n = j * 8 + 2 * t + e;
+        if (n >= cin) continue;
+        const size_t o = ((size_t)img * LP_P + p) * cin + n;
+        float v = d[j][2 * h + e];
+        if (Xa && !(__bfloat162float(__ushort_as_bfloat16(Xa[o])) > 0.f)) v = 0.f;
+        dX[o] = __bfloat16_as_ushort(__float2bfloat16_rn(v));
+      }
+    }
+}
+
+// ------------------------------------------------------- conv bwd weights
+
+// dW[co][tap][ci] += sum over a chunk of pixels of dY[p][co] X[p + off][ci]:
+// M = co (16-row tiles), N = tap * CIN + ci (8-column tiles), K = pixels.
+// Block (chunk, n-tile group): 4 warps, warp w takes n-tiles w, w + 4, ...
+// of the group; each accumulates its chunk and adds it with FP32 atomics.
+constexpr int LP_WCHUNK = 512;  // pixels per block
+
+template <int CIN>
+__global__ void __launch_bounds__(128) lp_conv_bwd_w_kernel(const uint16_t* dY, const uint16_t* X, int cout,
+                                                            long n_pix, float* dW, float* db) {
+  constexpr int NTOT = (9 * CIN + 7) / 8;  // n-tiles
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3, warp = threadIdx.x >> 5;
+  const long p0 = (long)blockIdx.x * LP_WCHUNK;
+  const int mtiles = (cout + 15) / 16;
+  for (int nt = blockIdx.y * 4 + warp; nt < NTOT; nt += gridDim.y * 4) {
+    for (int mt = 0; mt < mtiles; mt++) {
+      float d[4] = {0.f, 0.f, 0.f, 0.f};
+      for (long k0 = p0; k0 < p0 + LP_WCHUNK && k0 < n_pix; k0 += 16) {
+        auto dy = [&](int co, long p) -> uint16_t { return (co < cout && p < n_pix) ? dY[p * cout + co] : (uint16_t)0; };
+        auto xs = [&](int n, long p) -> uint16_t {
+          if (p >= n_pix || n >= 9 * CIN) return 0;
+          const int tap = n / CIN, ci = n % CIN, img = (int)(p / LP_P), q = (int)(p % LP_P);
+          return act(X, CIN, img, (q >> 5) + tap / 3 - 1, (q & 31) + tap % 3 - 1, ci);
+        };
+        const int m0 = mt * 16 + g, m1 = m0 + 8;
+        const uint32_t a[4] = {pack_raw(dy(m0, k0 + 2 * t), dy(m0, k0 + 2 * t + 1)),
+                               pack_raw(dy(m1, k0 + 2 * t), dy(m1, k0 + 2 * t + 1)),
+                               pack_raw(dy(m0, k0 + 2 * t + 8), dy(m0, k0 + 2 * t + 9)),
+                               pack_raw(dy(m1, k0 + 2 * t + 8), dy(m1, k0 + 2 * t + 9))};
+        const int n = nt * 8 + g;
+        const uint32_t b[2] = {pack_raw(xs(n, k0 + 2 * t), xs(n, k0 + 2 * t + 1)),
+                               pack_raw(xs(n, k0 + 2 * t + 8), xs(n, k0 + 2 * t + 9))};
+        mma_bf16(d, a, b);
+      }
+#pragma unroll
+      for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int co = mt * 16 + g + 8 * h, n = nt * 8 + 2 * t + e;
+          if (co < cout && n < 9 * CIN) atomicAdd(&dW[(size_t)co * 9 * CIN + n], d[2 * h + e]);
+        }
+    }
+  }
+  // Bias gradient: this chunk's column sums of dY (block row 0 only).
+  if (blockIdx.y == 0)
+    for (int co = threadIdx.x; co < cout; co += blockDim.x) {
+      float s = 0.f;
+      for (long p = p0; p < p0 + LP_WCHUNK && p < n_pix; p++) s += __bfloat162float(__ushort_as_bfloat16(dY[p * cout + co]));
+      atomicAdd(&db[co], s);
+    }
+}
+
+// ------------------------------------------------------------- loss
+
+// One block per item: softmax over its 1024 logits, the cross-entropy of
+// the label cell (added to *loss), and d(logits) = (softmax - onehot) / n
+// as BF16. Labels < 0 contribute nothing (zero gradient).
+__global__ void __launch_bounds__(256) lp_softmax_ce_kernel(const float* logits, const int32_t* labels, int n,
+                                                            uint16_t* dlogits, float* loss, float* top_prob) {
+  const int i = blockIdx.x, t = threadIdx.x;
+  __shared__ float red[8];
+  const float* z = logits + (size_t)i * LP_P;
+  float m = -INFINITY;
+  for (int q = t; q < LP_P; q += 256) m = fmaxf(m, z[q]);
+  for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((t & 31) == 0) red[t >> 5] = m;
+  __syncthreads();
+  m = red[0];
+  for (int k = 1; k < 8; k++) m = fmaxf(m, red[k]);
+  __syncthreads();
+  float s = 0.f;
+  for (int q = t; q < LP_P; q += 256) s += __expf(z[q] - m);
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((t & 31) == 0) red[t >> 5] = s;
+  __syncthreads();
+  s = 0.f;
+  for (int k = 0; k < 8; k++) s += red[k];
+  const int lab = labels ? labels[i] : -1;
+  for (int q = t; q < LP_P; q += 256) {
+    const float p = __expf(z[q] - m) / s;
+    if (dlogits) {
+      const float gr = lab < 0 ? 0.f : (p - (q == lab ? 1.f : 0.f)) / (float)n;
+      dlogits[(size_t)i * LP_P + q] = __bfloat16_as_ushort(__float2bfloat16_rn(gr));
+    }
+    if (top_prob && q == lab) top_prob[i] = p;
+  }
+  if (t == 0 && loss && lab >= 0) atomicAdd(loss, -(z[lab] - m - __logf(s)));
+}
+
+// ------------------------------------------------------------- Adam
+
+__global__ void lp_adam_kernel(float* w, const float* grad, float* m, float* v, int n, float lr, float b1, float b2,
+                               float eps, float c1, float c2, uint16_t* w_bf16) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gr = grad[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gr, vi = b2 * v[i] + (1.f - b2) * gr * gr;
+  m[i] = mi;
+  v[i] = vi;
+  const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  w[i] = wi;
+  w_bf16[i] = __bfloat16_as_ushort(__float2bfloat16_rn(wi));
+}
+
+template <int CIN, int NT>
+vp8a_status conv_fwd(vp8a_ctx* ctx, const uint16_t* X, const uint16_t* W, const float* b, int cout, int n, int relu,
+                     uint16_t* Y, float* Yf) {
+  const int tiles = n * (LP_P / 16);
+  lp_conv_fwd_kernel<CIN, NT><<<(tiles + 3) / 4, 128, 0, ctx->stream>>>(X, W, b, cout, n, relu, Y, Yf);
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
+  return VP8A_OK;
+}
+
+template <int COUT, int NT>
+vp8a_status conv_bwd_data(vp8a_ctx* ctx, const uint16_t* dY, const uint16_t* W, int cin, int n, const uint16_t* Xa,
+                          uint16_t* dX) {
+  const int tiles = n * (LP_P / 16);
+  lp_conv_bwd_data_kernel<COUT, NT><<<(tiles + 3) / 4, 128, 0, ctx->stream>>>(dY, W, cin, n, Xa, dX);
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
+  return VP8A_OK;
+}
+
+template <int CIN>
+vp8a_status conv_bwd_w(vp8a_ctx* ctx, const uint16_t* dY, const uint16_t* X, int cout, int n, float* dW, float* db) {
+  const long n_pix = (long)n * LP_P;
+  constexpr int NTOT = (9 * CIN + 7) / 8;
+  const dim3 grid((unsigned)((n_pix + LP_WCHUNK - 1) / LP_WCHUNK), (unsigned)((NTOT + 3) / 4));
+  lp_conv_bwd_w_kernel<CIN><<<grid, 128, 0, ctx->stream>>>(dY, X, cout, n_pix, dW, db);
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
+  return VP8A_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+vp8a_status vp8a_lp_windows(vp8a_ctx* ctx, const vp8a_luma_ref* src, const vp8a_luma_ref* ref, const uint32_t* mb_xy,
+                            uint32_t n, uint16_t* out) {
+  if (!ctx || !src || !ref || (n && (!mb_xy || !out))) {
+    vp8a::set_error("null argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (src->width != ref->width || src->height != ref->height || !src->width || !src->height) {
+    vp8a::set_error("source and reference planes differ in size");
+    return VP8A_E_REFERENCE_DIMENSIONS_MISMATCH;
+  }
+  if (n == 0) return VP8A_OK;
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  lp_windows_kernel<<<n, 256, 0, ctx->stream>>>(src->plane, src->stride, ref->plane, ref->stride, (int)src->width,
+                                                 (int)src->height, mb_xy, (int)n, out);
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
+  return VP8A_OK;
+}
+
+vp8a_status vp8a_lp_conv_forward(vp8a_ctx* ctx, const uint16_t* x, uint32_t cin, const uint16_t* w, const float* bias,
+                                 uint32_t cout, uint32_t n, uint32_t relu, uint16_t* y, float* y_f32) {
+  if (!ctx || !x || !w || !bias || (!y && !y_f32)) {
+    vp8a::set_error("null argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  if (cin == 2 && cout == 32) return conv_fwd<2, 4>(ctx, x, w, bias, 32, (int)n, relu, y, y_f32);
+  if (cin == 32 && cout == 32) return conv_fwd<32, 4>(ctx, x, w, bias, 32, (int)n, relu, y, y_f32);
+  if (cin == 32 && cout == 1) return conv_fwd<32, 1>(ctx, x, w, bias, 1, (int)n, relu, y, y_f32);
+  vp8a::set_error("conv shape must be 2->32, 32->32 or 32->1");
+  return VP8A_E_INVALID_ARGUMENT;
+}
+
+vp8a_status vp8a_lp_conv_backward(vp8a_ctx* ctx, const uint16_t* x, uint32_t cin, const uint16_t* w, uint32_t cout,
+                                  uint32_t n, const uint16_t* dy, uint32_t x_relu, uint16_t* dx, float* dw,
+                                  float* db) {
+  if (!ctx || !x || !w || !dy || !dw || !db) {
+    vp8a::set_error("null argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a_status s;
+  const uint16_t* mask = x_relu ? x : nullptr;
+  if (cin == 2 && cout == 32) {
+    if ((s = conv_bwd_w<2>(ctx, dy, x, 32, (int)n, dw, db)) != VP8A_OK) return s;
+    if (dx) return conv_bwd_data<32, 1>(ctx, dy, w, 2, (int)n, mask, dx);
+    return VP8A_OK;
+  }
+  if (cin == 32 && cout == 32) {
+    if ((s = conv_bwd_w<32>(ctx, dy, x, 32, (int)n, dw, db)) != VP8A_OK) return s;
+    if (dx) return conv_bwd_data<32, 4>(ctx, dy, w, 32, (int)n, mask, dx);
+    return VP8A_OK;
+  }
+  if (cin == 32 && cout == 1) {
+    if ((s = conv_bwd_w<32>(ctx, dy, x, 1, (int)n, dw, db)) != VP8A_OK) return s;
+    if (dx) return conv_bwd_data<1, 4>(ctx, dy, w, 32, (int)n, mask, dx);
+    return VP8A_OK;
+  }
+  vp8a::set_error("conv shape must be 2->32, 32->32 or 32->1");
+  return VP8A_E_INVALID_ARGUMENT;
+}
+
+vp8a_status vp8a_lp_softmax_ce(vp8a_ctx* ctx, const float* logits, const int32_t* labels, uint32_t n,
+                               uint16_t* dlogits, float* loss, float* label_prob) {
+  if (!ctx || !logits) {
+    vp8a::set_error("null argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (n == 0) return VP8A_OK;
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  lp_softmax_ce_kernel<<<n, 256, 0, ctx->stream>>>(logits, labels, (int)n, dlogits, loss, label_prob);
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
+  return VP8A_OK;
+}
+
+vp8a_status vp8a_lp_adam(vp8a_ctx* ctx, float* w, const float* grad, float* m, float* v, uint32_t n, float lr,
+                         float beta1, float beta2, float eps, uint32_t step, uint16_t* w_bf16) {
+  if (!ctx || !w || !grad || !m || !v || !w_bf16 || step == 0) {
+    vp8a::set_error("null argument or step 0");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (n == 0) return VP8A_OK;
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  const float c1 = 1.f - powf(beta1, (float)step), c2 = 1.f - powf(beta2, (float)step);
+  lp_adam_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(w, grad, m, v, (int)n, lr, beta1, beta2, eps, c1, c2,
+                                                            w_bf16);
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
+  return VP8A_OK;
+}
+
+}  // extern "C"

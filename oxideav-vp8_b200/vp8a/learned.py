@@ -1,0 +1,315 @@
+"""Learned motion proposal (no counterpart in the reference).
+
+A 4-layer 3x3 conv net (2 -> 32 -> 32 -> 32 -> 1 channels, ReLU between,
+BF16 weights and activations, FP32 accumulation) scores a 32 x 32 grid of
+whole-pel vectors, 2 px apart, from an MB's coarse cost volume against a
+reference (`vp8a_lp_windows`: at each grid vector the half-resolution SAD of
+the MB and the reference's texture), so each score sees the matching cost
+of its own vector and its neighbours'. Every
+layer runs on the library's hand-written tensor-core kernels
+(`vp8a_lp_conv_forward` / `vp8a_lp_conv_backward`), the loss and the
+optimiser on its own kernels (`vp8a_lp_softmax_ce`, `vp8a_lp_adam`); torch
+only holds the device buffers. Training labels are the plain search's own
+whole-pel results (`labels_from_search`).
+
+The net only proposes: `learned_search` takes its best cells as seeds of an
+exact local search (every whole-pel position within +-2 px of each seed, the
+first smallest SAD, then the reference's half- and quarter-pel refinement),
+with the plain descent from the zero vector as the fallback for MBs whose
+refined SAD exceeds 1.25 x the frame's median. Every returned vector and SAD
+is exact; the net decides only where to look.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from .frames import luma_ref, ptr
+from .lib import check
+
+GRID = 32            # cells per side; cell (i, j) = (2 (i - 16), 2 (j - 16)) px
+
+_streams = {}
+
+
+def on_ctx_stream(ctx):
+    """A torch stream context on the library context's CUDA stream: torch
+    work inside it is ordered with the library's calls (every function here
+    runs its torch ops under it; callers building inputs with torch should
+    too)."""
+    import torch
+
+    key = ctx.stream
+    if key not in _streams:
+        _streams[key] = torch.cuda.ExternalStream(ctx.stream)
+    return torch.cuda.stream(_streams[key])
+PIX = GRID * GRID
+LAYERS = [(2, 32, True), (32, 32, True), (32, 32, True), (32, 1, False)]
+
+
+def cell_of_mv(mv_row, mv_col):
+    """Label cell of a quarter-pel vector (nearest 2-px cell), or -1 when it
+    falls outside the grid."""
+    r = np.rint(np.asarray(mv_row, np.float64) / 8.0).astype(np.int64) + 16
+    c = np.rint(np.asarray(mv_col, np.float64) / 8.0).astype(np.int64) + 16
+    ok = (r >= 0) & (r < GRID) & (c >= 0) & (c < GRID)
+    return np.where(ok, r * GRID + c, -1).astype(np.int32)
+
+
+def mv_of_cell(cell):
+    """Quarter-pel (row, col) of a cell's vector."""
+    cell = np.asarray(cell, np.int64)
+    return (cell // GRID - 16) * 8, (cell % GRID - 16) * 8
+
+
+def _ordered(fn):
+    """Run a ProposalNet method with torch on the library's stream."""
+
+    def wrapped(self, *a, **k):
+        with on_ctx_stream(self.ctx):
+            return fn(self, *a, **k)
+
+    wrapped.__doc__ = fn.__doc__
+    wrapped.__name__ = fn.__name__
+    return wrapped
+
+
+class ProposalNet:
+    """The net's parameters (FP32 master copies, BF16 working copies, Adam
+    moments) and activations, on the context's GPU."""
+
+    def __init__(self, ctx, seed=0):
+        import torch
+
+        self.torch, self.ctx, self.dev = torch, ctx, torch.device("cuda")
+        g = torch.Generator().manual_seed(seed)
+        self.layers = []
+        for cin, cout, relu in LAYERS:
+            std = (2.0 / (9 * cin)) ** 0.5 * (0.5 if not relu else 1.0)
+            w = (torch.randn(cout * 9 * cin, generator=g) * std).to(self.dev)
+            b = torch.zeros(cout, device=self.dev)
+            self.layers.append({
+                "cin": cin, "cout": cout, "relu": relu, "w": w, "b": b,
+                "wh": w.to(torch.bfloat16),
+                "mw": torch.zeros_like(w), "vw": torch.zeros_like(w),
+                "mb": torch.zeros_like(b), "vb": torch.zeros_like(b),
+                "gw": torch.zeros_like(w), "gb": torch.zeros_like(b),
+                "bh": b.to(torch.bfloat16),  # the bias stays FP32 in the forward pass
+            })
+        self.step_count = 0
+        self._acts = None
+
+    def _lib(self):
+        return self.ctx._lib
+
+    @_ordered
+    def forward(self, x, keep=False):
+        """x: [n, 32, 32, 2] bf16 device tensor. Returns FP32 scores [n, 1024]
+        (and keeps the activations for `backward` when `keep`)."""
+        torch = self.torch
+        n = x.shape[0]
+        acts = [x]
+        h = x
+        for li, L in enumerate(self.layers):
+            last = li == len(self.layers) - 1
+            if last:
+                out = torch.empty((n, PIX), dtype=torch.float32, device=self.dev)
+                y, yf = None, out
+            else:
+                out = torch.empty((n, GRID, GRID, L["cout"]), dtype=torch.bfloat16, device=self.dev)
+                y, yf = out, None
+            check(self._lib().vp8a_lp_conv_forward(self.ctx.handle, ptr(h), L["cin"], ptr(L["wh"]), ptr(L["b"]),
+                                                   L["cout"], n, int(L["relu"]), ptr(y), ptr(yf)),
+                  "vp8a_lp_conv_forward")
+            h = out
+            acts.append(out)
+        if keep:
+            self._acts = acts
+        return h
+
+    @_ordered
+    def loss_and_grad(self, logits, labels):
+        """Softmax cross-entropy of `labels` (int32 device tensor, -1 = none);
+        returns (mean loss, BF16 d(logits))."""
+        torch = self.torch
+        n = logits.shape[0]
+        d = torch.empty((n, PIX), dtype=torch.bfloat16, device=self.dev)
+        loss = torch.zeros(1, dtype=torch.float32, device=self.dev)
+        check(self._lib().vp8a_lp_softmax_ce(self.ctx.handle, ptr(logits), ptr(labels), n, ptr(d), ptr(loss), None),
+              "vp8a_lp_softmax_ce")
+        valid = max(int((labels >= 0).sum().item()), 1)
+        return loss, d, valid
+
+    @_ordered
+    def backward(self, dlogits):
+        """Accumulates every layer's gradients from d(scores)."""
+        torch = self.torch
+        acts = self._acts
+        n = acts[0].shape[0]
+        dy = dlogits.view(n, GRID, GRID, 1)
+        for li in range(len(self.layers) - 1, -1, -1):
+            L = self.layers[li]
+            x = acts[li]
+            dx = None if li == 0 else torch.empty_like(x)
+            check(self._lib().vp8a_lp_conv_backward(self.ctx.handle, ptr(x), L["cin"], ptr(L["wh"]), L["cout"], n,
+                                                    ptr(dy), int(li > 0), ptr(dx), ptr(L["gw"]), ptr(L["gb"])),
+                  "vp8a_lp_conv_backward")
+            dy = dx
+
+    @_ordered
+    def zero_grad(self):
+        for L in self.layers:
+            L["gw"].zero_()
+            L["gb"].zero_()
+
+    @_ordered
+    def adam(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8):
+        self.step_count += 1
+        for L in self.layers:
+            for w, g, m, v, wh in ((L["w"], L["gw"], L["mw"], L["vw"], L["wh"]),
+                                   (L["b"], L["gb"], L["mb"], L["vb"], L["bh"])):
+                check(self._lib().vp8a_lp_adam(self.ctx.handle, ptr(w), ptr(g), ptr(m), ptr(v), w.numel(), lr, beta1,
+                                               beta2, eps, self.step_count, ptr(wh)), "vp8a_lp_adam")
+
+    @_ordered
+    def train_step(self, x, labels, lr=1e-3):
+        """One forward / backward / Adam step on a batch; returns the mean
+        cross-entropy (a device scalar)."""
+        self.zero_grad()
+        logits = self.forward(x, keep=True)
+        loss, d, valid = self.loss_and_grad(logits, labels)
+        # d(logits) is normalised by the batch size, the loss by the labelled
+        # items.
+        self.backward(d)
+        self.adam(lr)
+        return loss / valid
+
+    @_ordered
+    def propose(self, x, k=4):
+        """Top-k cells per item, best first ([n, k] int64 device tensor)."""
+        logits = self.forward(x)
+        return self.torch.topk(logits, k, dim=1).indices
+
+
+def windows(ctx, src_y, ref_y, mb_xy):
+    """The net's input for the MBs `mb_xy` ([n, 2] uint32 device tensor of
+    (col, row)) of a source / reference luma pair (device uint8 planes of one
+    size). Returns [n, 32, 32, 2] bf16."""
+    import torch
+
+    n = mb_xy.shape[0]
+    for t, what in ((src_y, "source"), (ref_y, "reference"), (mb_xy, "mb_xy")):
+        assert t.is_cuda, f"{what} must be a CUDA tensor"
+    assert mb_xy.dim() == 2 and mb_xy.shape[1] == 2 and mb_xy.dtype == torch.int32 and mb_xy.is_contiguous()
+    with on_ctx_stream(ctx):
+        out = torch.empty((n, GRID, GRID, 2), dtype=torch.bfloat16, device=mb_xy.device)
+        s, r = luma_ref(src_y), luma_ref(ref_y)
+        check(ctx._lib.vp8a_lp_windows(ctx.handle, C.byref(s), C.byref(r), ptr(mb_xy), n, ptr(out)),
+              "vp8a_lp_windows")
+    return out
+
+
+def all_mbs(mb_cols, mb_rows, device="cuda"):
+    import torch
+
+    r, c = np.meshgrid(np.arange(mb_rows), np.arange(mb_cols), indexing="ij")
+    xy = np.stack([c.reshape(-1), r.reshape(-1)], 1).astype(np.uint32)
+    return torch.from_numpy(xy.view(np.int32)).to(device)
+
+
+def labels_from_search(ctx, frame, ref_padded, lam):
+    """Labels of one frame: the plain search's quarter-pel result against
+    `ref_padded` (the exhaustive analysis' per-reference trace, reference
+    LAST), as cells (-1 where the vector leaves the grid)."""
+    from .api import analyse_inter_frame
+
+    _, tr = analyse_inter_frame(ctx, frame, [ref_padded], [abi.REF_LAST], lam, trace=True)
+    q = tr[..., 0]["quarter"]["mv"].reshape(-1)
+    return cell_of_mv(q["row"], q["col"]), tr[..., 0]["quarter"]["sad"].reshape(-1)
+
+
+def learned_search(ctx, net, src_y, ref_y, mb_xy, k=4, radius=2, fallback=1.25, seeds=None):
+    """The learned path for one (source, reference) luma pair: proposal,
+    exact +-`radius` px whole-pel search around each of the k seeds, half-
+    and quarter-pel refinement of the best, and the plain descent from the
+    zero vector for MBs whose SAD exceeds `fallback` x the median. `seeds`
+    ([n, k] cells) replaces the net (the ablation). Returns (mv [n, 2]
+    quarter-pel int16, sad [n] uint32, fell_back [n] bool) as numpy."""
+    import torch
+
+    with on_ctx_stream(ctx):
+        return _learned_search(ctx, net, src_y, ref_y, mb_xy, k, radius, fallback, seeds)
+
+
+def _learned_search(ctx, net, src_y, ref_y, mb_xy, k, radius, fallback, seeds):
+    import torch
+
+    n = mb_xy.shape[0]
+    h, w = src_y.shape[0], src_y.shape[1]
+    if seeds is None:
+        x = windows(ctx, src_y, ref_y[:h, :w], mb_xy)
+        seeds = net.propose(x, k)
+    seeds = seeds.to(torch.int64)
+    sr = (seeds // GRID - 16) * 8
+    sc = (seeds % GRID - 16) * 8
+    d = torch.arange(-radius, radius + 1, device=seeds.device) * 4
+    dr, dc = torch.meshgrid(d, d, indexing="ij")
+    ncand = k * dr.numel()
+    cr = (sr[:, :, None] + dr.reshape(1, 1, -1)).reshape(n, ncand)
+    cc = (sc[:, :, None] + dc.reshape(1, 1, -1)).reshape(n, ncand)
+    cr = cr.clamp(-1023, 1023)
+    cc = cc.clamp(-1023, 1023)
+    mbr, mbc = (h + 15) // 16, (w + 15) // 16
+    # Source MBs (16x16 luma, edge-replicated) for every item.
+    src_mbs = _source_mbs(src_y, mb_xy, h, w)
+    rep_src = src_mbs.repeat_interleave(ncand, dim=0)
+    rep_xy = mb_xy.repeat_interleave(ncand, dim=0)
+    mvs = torch.stack([cr, cc], dim=2).reshape(-1, 2).to(torch.int16).contiguous()
+    sads = torch.empty(n * ncand, dtype=torch.int32, device=seeds.device)
+    ref = luma_ref(ref_y, width=mbc * 16, height=mbr * 16)
+    lib = ctx._lib
+    check(lib.vp8a_mb_luma_sad_at_mv(ctx.handle, C.byref(ref), ptr(rep_src), ptr(rep_xy), ptr(mvs), n * ncand,
+                                     ptr(sads)), "vp8a_mb_luma_sad_at_mv")
+    # First smallest SAD in seed order.
+    best = sads.view(n, ncand).to(torch.int64).argmin(dim=1)
+    whole = mvs.view(n, ncand, 2)[torch.arange(n, device=seeds.device), best].contiguous()
+    sr_out = torch.empty((n, 2), dtype=torch.int32, device=seeds.device)  # search_result: mv (2 x i16) + sad
+    half = torch.empty((n, 2), dtype=torch.int32, device=seeds.device)
+    check(lib.vp8a_half_pixel_refine_luma(ctx.handle, C.byref(ref), ptr(src_mbs), ptr(mb_xy), ptr(whole), n,
+                                          ptr(half)), "vp8a_half_pixel_refine_luma")
+    hmv = half[:, 0].contiguous().view(torch.int16).view(n, 2)
+    check(lib.vp8a_quarter_pixel_refine_luma(ctx.handle, C.byref(ref), ptr(src_mbs), ptr(mb_xy), ptr(hmv.contiguous()),
+                                             n, ptr(sr_out)), "vp8a_quarter_pixel_refine_luma")
+    out_mv = sr_out[:, 0].contiguous().view(torch.int16).view(n, 2).clone()
+    out_sad = sr_out[:, 1].clone()
+    # Fallback: the plain descent from the zero vector (8 rounds + sub-pel).
+    med = out_sad.to(torch.float32).median()
+    fb = out_sad.to(torch.float32) > fallback * med
+    nf = int(fb.sum().item())
+    if nf:
+        idx = torch.nonzero(fb).reshape(-1)
+        zero = torch.zeros((nf, 2), dtype=torch.int16, device=seeds.device)
+        w_o = torch.empty((nf, 2), dtype=torch.int32, device=seeds.device)
+        h_o = torch.empty_like(w_o)
+        q_o = torch.empty_like(w_o)
+        check(lib.vp8a_motion_descent(ctx.handle, C.byref(ref), ptr(src_mbs[idx].contiguous()),
+                                      ptr(mb_xy[idx].contiguous()), ptr(zero), 8, nf, ptr(w_o), ptr(h_o), ptr(q_o)),
+              "vp8a_motion_descent")
+        better = q_o[:, 1] < out_sad[idx]
+        sel = idx[better]
+        out_sad[sel] = q_o[better, 1]
+        out_mv[sel] = q_o[better, 0].contiguous().view(torch.int16).view(-1, 2)
+    ctx.synchronize()
+    return out_mv.cpu().numpy(), out_sad.cpu().numpy().astype(np.uint32), fb.cpu().numpy()
+
+
+def _source_mbs(src_y, mb_xy, h, w):
+    """[n, 256] uint8: the 16x16 luma of each listed MB, edge-replicated
+    (I420Frame::extract_mb)."""
+    import torch
+
+    xy = mb_xy.view(torch.int32).to(torch.int64)
+    oy = torch.arange(16, device=src_y.device)
+    ys = (xy[:, 1:2] * 16 + oy[None, :]).clamp(max=h - 1)
+    xs = (xy[:, 0:1] * 16 + oy[None, :]).clamp(max=w - 1)
+    return src_y[ys[:, :, None], xs[:, None, :]].reshape(-1, 256).contiguous()

@@ -1,0 +1,218 @@
+"""The learned motion proposal's kernels against an FP32 numpy reference
+(gradient check), its training, and the seeded exact search with the
+ablation (net seeds against the same search seeded at the zero vector).
+
+Reference semantics: the conv layers compute, in FP32 over BF16 inputs and
+weights, out[y][x][co] = b[co] + sum over taps and ci of
+x[y + dy][x + dx][ci] w[co][tap][ci] (zero outside the 32 x 32 image);
+their gradients are the exact sums below; the GPU's differ only by the
+FP32 accumulation order (and BF16 rounding of the activations it stores),
+which the tolerances state."""
+import numpy as np
+import pytest
+
+import vp8a
+from vp8a import abi, learned, synth
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def bf16(a):
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(torch.bfloat16).float().numpy()
+
+
+def conv_ref(x, w, b, relu):
+    n, s, _, cin = x.shape
+    cout = w.shape[0]
+    xp = np.pad(x, ((0, 0), (1, 1), (1, 1), (0, 0)))
+    out = np.zeros((n, s, s, cout), np.float64) + b
+    for tap in range(9):
+        dy, dx = tap // 3 - 1, tap % 3 - 1
+        out += np.einsum("nyxc,oc->nyxo", xp[:, 1 + dy:1 + dy + s, 1 + dx:1 + dx + s, :], w[:, tap, :])
+    return np.maximum(out, 0) if relu else out
+
+
+def conv_bwd_ref(x, w, dy_, x_relu):
+    n, s, _, cin = x.shape
+    xp = np.pad(x, ((0, 0), (1, 1), (1, 1), (0, 0)))
+    dyp = np.pad(dy_, ((0, 0), (1, 1), (1, 1), (0, 0)))
+    dw = np.zeros(w.shape, np.float64)
+    dx = np.zeros(x.shape, np.float64)
+    for tap in range(9):
+        ty, tx = tap // 3 - 1, tap % 3 - 1
+        dw[:, tap, :] = np.einsum("nyxo,nyxc->oc", dy_, xp[:, 1 + ty:1 + ty + s, 1 + tx:1 + tx + s, :])
+        dx += np.einsum("nyxo,oc->nyxc", dyp[:, 1 - ty:1 - ty + s, 1 - tx:1 - tx + s, :], w[:, tap, :])
+    if x_relu:
+        dx = dx * (x > 0)
+    return dw, dy_.sum(axis=(0, 1, 2)), dx
+
+
+def dev_bf16(a):
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(torch.bfloat16).cuda()
+
+
+@pytest.mark.parametrize("cin,cout,relu", [(2, 32, True), (32, 32, True), (32, 1, False)])
+def test_conv_forward_and_gradients_match_fp32_reference(ctx, cin, cout, relu):
+    rng = np.random.default_rng(cin * 100 + cout)
+    n = 3
+    x = bf16(rng.standard_normal((n, 32, 32, cin)))
+    if cin == 32:
+        x = np.maximum(x, 0)  # an activation out of a ReLU
+    w = bf16(rng.standard_normal((cout, 9, cin)) * 0.2)
+    b = rng.standard_normal(cout).astype(np.float32) * 0.1
+    lib = ctx._lib
+    dx_, dw_, db_ = dev_bf16(x), dev_bf16(w.reshape(-1)), torch.from_numpy(b).cuda()
+    yf = torch.empty((n, 32, 32, cout), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()  # inputs in place before the library's stream reads them
+    assert lib.vp8a_lp_conv_forward(ctx.handle, dx_.data_ptr(), cin, dw_.data_ptr(), db_.data_ptr(), cout, n,
+                                    int(relu), None, yf.data_ptr()) == abi.OK
+    ctx.synchronize()
+    want = conv_ref(x, w, b, relu)
+    got = yf.cpu().numpy()
+    # FP32 accumulation of BF16 products: the order differs, nothing else.
+    assert np.abs(got - want).max() <= 1e-4 * max(1.0, np.abs(want).max())
+    # Gradients for a BF16 upstream gradient.
+    dy = bf16(rng.standard_normal((n, 32, 32, cout)) * 0.05)
+    gw = torch.zeros(cout * 9 * cin, device="cuda")
+    gb = torch.zeros(cout, device="cuda")
+    gx = torch.empty((n, 32, 32, cin), dtype=torch.bfloat16, device="cuda")
+    x_relu = int(cin == 32)
+    ddy = dev_bf16(dy)
+    torch.cuda.synchronize()
+    assert lib.vp8a_lp_conv_backward(ctx.handle, dx_.data_ptr(), cin, dw_.data_ptr(), cout, n, ddy.data_ptr(),
+                                     x_relu, gx.data_ptr(), gw.data_ptr(), gb.data_ptr()) == abi.OK
+    ctx.synchronize()
+    rdw, rdb, rdx = conv_bwd_ref(x, w, dy, x_relu)
+    assert np.abs(gw.cpu().numpy().reshape(rdw.shape) - rdw).max() <= 1e-4 * max(1.0, np.abs(rdw).max())
+    assert np.abs(gb.cpu().numpy() - rdb).max() <= 1e-4 * max(1.0, np.abs(rdb).max())
+    # dX is stored as BF16: within half an ulp of BF16 (2^-8 relative).
+    gxn = gx.float().cpu().numpy()
+    assert np.all(np.abs(gxn - rdx) <= np.abs(rdx) * 2.0 ** -8 + 1e-6)
+
+
+def test_softmax_cross_entropy_and_adam(ctx):
+    rng = np.random.default_rng(3)
+    n = 5
+    z = (rng.standard_normal((n, 1024)) * 3).astype(np.float32)
+    lab = np.array([0, 1023, 517, -1, 44], np.int32)
+    dz = torch.from_numpy(z).cuda()
+    dl = torch.from_numpy(lab).cuda()
+    g = torch.empty((n, 1024), dtype=torch.bfloat16, device="cuda")
+    loss = torch.zeros(1, device="cuda")
+    prob = torch.zeros(n, device="cuda")
+    torch.cuda.synchronize()
+    assert ctx._lib.vp8a_lp_softmax_ce(ctx.handle, dz.data_ptr(), dl.data_ptr(), n, g.data_ptr(), loss.data_ptr(),
+                                       prob.data_ptr()) == abi.OK
+    ctx.synchronize()
+    p = np.exp(z - z.max(1, keepdims=True))
+    p /= p.sum(1, keepdims=True)
+    want_loss = -sum(np.log(p[i, lab[i]]) for i in range(n) if lab[i] >= 0)
+    assert abs(loss.item() - want_loss) <= 1e-4 * abs(want_loss)
+    onehot = np.zeros_like(p)
+    for i in range(n):
+        if lab[i] >= 0:
+            onehot[i, lab[i]] = 1
+    want_g = np.where((lab >= 0)[:, None], (p - onehot) / n, 0)
+    assert np.all(np.abs(g.float().cpu().numpy() - want_g) <= np.abs(want_g) * 2.0 ** -8 + 1e-7)
+    # Adam against its definition.
+    w = rng.standard_normal(1000).astype(np.float32)
+    gr = rng.standard_normal(1000).astype(np.float32)
+    m = np.zeros_like(w)
+    v = np.zeros_like(w)
+    dw_, dg, dm, dv = (torch.from_numpy(a.copy()).cuda() for a in (w, gr, m, v))
+    wb = torch.empty(1000, dtype=torch.bfloat16, device="cuda")
+    torch.cuda.synchronize()
+    for step in (1, 2):
+        assert ctx._lib.vp8a_lp_adam(ctx.handle, dw_.data_ptr(), dg.data_ptr(), dm.data_ptr(), dv.data_ptr(), 1000,
+                                     1e-3, 0.9, 0.999, 1e-8, step, wb.data_ptr()) == abi.OK
+        m = 0.9 * m + 0.1 * gr
+        v = 0.999 * v + 0.001 * gr * gr
+        w = w - 1e-3 * (m / (1 - 0.9 ** step)) / (np.sqrt(v / (1 - 0.999 ** step)) + 1e-8)
+    ctx.synchronize()
+    assert np.abs(dw_.cpu().numpy() - w).max() <= 1e-6
+    # The BF16 copy is the rounding of the FP32 master weights.
+    assert torch.equal(wb, dw_.to(torch.bfloat16))
+
+
+def moving_sequence(w, h, seed, n=6):
+    frames, _ = synth.make_sequence(w, h, n, seed=seed, pieces=4, occluders=3)
+    return frames
+
+
+def dataset(ctx, sizes_seeds, lam):
+    with learned.on_ctx_stream(ctx):
+        x, y = _dataset(ctx, sizes_seeds, lam)
+    ctx.synchronize()
+    return x, y
+
+
+def _dataset(ctx, sizes_seeds, lam):
+    xs, ys = [], []
+    for (w, h, seed) in sizes_seeds:
+        frames = moving_sequence(w, h, seed)
+        for k in range(1, len(frames)):
+            ref = vp8a.pad_to_mb(*frames[k - 1])
+            lab, _ = learned.labels_from_search(ctx, frames[k], ref, lam)
+            mbr, mbc = (h + 15) // 16, (w + 15) // 16
+            xy = learned.all_mbs(mbc, mbr)
+            src = torch.from_numpy(frames[k][0]).cuda()
+            refy = torch.from_numpy(ref[0]).cuda()
+            xs.append(learned.windows(ctx, src, refy[:h, :w], xy))
+            ys.append(torch.from_numpy(lab).cuda())
+    return torch.cat(xs), torch.cat(ys)
+
+
+def test_training_reduces_loss_and_finds_the_search_vectors(ctx):
+    lam = vp8a.rd_lambda(44)
+    x, y = dataset(ctx, [(320, 240, 11), (320, 240, 12), (176, 144, 13)], lam)
+    net = learned.ProposalNet(ctx, seed=1)
+    n = x.shape[0]
+    g = torch.Generator(device="cpu").manual_seed(0)
+
+    def top4(net_):
+        cells = net_.propose(x, 4)
+        with learned.on_ctx_stream(ctx):
+            return float(((cells == y[:, None].long()).any(1) & (y >= 0)).float().sum() / (y >= 0).sum())
+
+    before = top4(net)
+    losses = []
+    for it in range(150):
+        with learned.on_ctx_stream(ctx):
+            idx = torch.randint(0, n, (256,), generator=g).cuda()
+            xb, yb = x[idx].contiguous(), y[idx].contiguous()
+        losses.append(float(net.train_step(xb, yb, lr=2e-3)))
+    after = top4(net)
+    assert np.mean(losses[-20:]) < 0.7 * np.mean(losses[:10]), (losses[:10], losses[-20:])
+    assert after > before + 0.2, (before, after)
+
+
+def test_learned_search_is_exact_and_beats_zero_seeds(ctx, oracle):
+    lam = vp8a.rd_lambda(44)
+    x, y = dataset(ctx, [(320, 240, 21), (320, 240, 22)], lam)
+    net = learned.ProposalNet(ctx, seed=2)
+    g = torch.Generator(device="cpu").manual_seed(1)
+    for it in range(150):
+        with learned.on_ctx_stream(ctx):
+            idx = torch.randint(0, x.shape[0], (256,), generator=g).cuda()
+            xb, yb = x[idx].contiguous(), y[idx].contiguous()
+        net.train_step(xb, yb, lr=2e-3)
+    frames = moving_sequence(320, 240, 29)
+    ref = vp8a.pad_to_mb(*frames[2])
+    src = frames[3]
+    xy = learned.all_mbs(20, 15)
+    srcd = torch.from_numpy(src[0]).cuda()
+    refd = torch.from_numpy(ref[0]).cuda()
+    mv, sad, fb = learned.learned_search(ctx, net, srcd, refd, xy)
+    # Exact: every SAD is the plain search's SAD at the returned vector.
+    xyh = xy.cpu().numpy().view(np.uint32)
+    src_mbs = learned._source_mbs(srcd, xy, 240, 320).cpu().numpy()
+    want = oracle.mb_luma_sad_at_mv(ref[0], src_mbs, xyh, mv)
+    assert np.array_equal(sad, np.asarray(want, np.uint32))
+    # The ablation: the same search seeded at the zero vector only.
+    zero = torch.full((xy.shape[0], 4), 16 * 32 + 16, dtype=torch.int64, device="cuda")
+    _, sad0, _ = learned.learned_search(ctx, net, srcd, refd, xy, seeds=zero)
+    assert sad.mean() < sad0.mean(), (sad.mean(), sad0.mean())
+    # And the plain exhaustive search's per-MB result for reference.
+    _, plain_sad = learned.labels_from_search(ctx, src, ref, lam)
+    assert sad.mean() <= 1.15 * plain_sad.mean(), (sad.mean(), plain_sad.mean())
