@@ -887,6 +887,115 @@ def batch_arm(args):
                                    % args.streams, "seed": SEED, "l2": "flushed between timed steps (256 MiB write)"}}
 
 
+# --------------------------------------------------- learned proposal case
+
+def learned_arm(args):
+    """The learned motion proposal at 1080p (the survey's config 4): the net
+    is trained (untimed) on ~200k labels — the plain search's LAST-reference
+    vectors over 24 seeded 1080p frame pairs (gratings, noise, piecewise
+    motion, moving occluders) — with Adam, lr 1e-3, batches of 4096 MBs;
+    then, on the bench's P frame, the learned search (proposal + exact
+    +-2 px search around 4 seeds + sub-pel + descent fallback) for LAST,
+    GOLDEN and ALTREF is timed against the plain exhaustive analysis of the
+    same frame and references. Quality: mean SAD per reference against the
+    plain search's own per-reference result."""
+    import torch
+
+    import vp8a
+    from vp8a import abi, learned, synth
+
+    ctx = vp8a.Context(0)
+    lam = vp8a.rd_lambda(QI)
+    t0 = time.time()
+    xs, ys = [], []
+    with learned.on_ctx_stream(ctx):
+        for sidx in range(4):
+            frames, _ = synth.make_sequence(W, H, 7, SEED + 1000 + sidx, pieces=4, occluders=4)
+            for k in range(1, 7):
+                ref = pad_planes(frames[k - 1])
+                lab, _ = learned.labels_from_search(ctx, frames[k], ref, lam)
+                xy = learned.all_mbs(MB_COLS, MB_ROWS)
+                src = torch.from_numpy(frames[k][0]).cuda()
+                refy = torch.from_numpy(ref[0]).cuda()
+                xs.append(learned.windows(ctx, src, refy[:H, :W], xy))
+                ys.append(torch.from_numpy(lab).cuda())
+        x = torch.cat(xs)
+        y = torch.cat(ys)
+    ctx.synchronize()
+    t_labels = time.time() - t0
+    net = learned.ProposalNet(ctx, seed=7)
+    g = torch.Generator().manual_seed(5)
+    n = x.shape[0]
+    losses = []
+    t1 = time.time()
+    for it in range(args.train_steps):
+        with learned.on_ctx_stream(ctx):
+            idx = torch.randint(0, n, (4096,), generator=g).cuda()
+            xb, yb = x[idx].contiguous(), y[idx].contiguous()
+        losses.append(float(net.train_step(xb, yb, lr=1e-3)))
+    ctx.synchronize()
+    t_train = time.time() - t1
+    with learned.on_ctx_stream(ctx):
+        cells = net.propose(x[:65536], 4)
+        top4 = float(((cells == y[:65536, None].long()).any(1) & (y[:65536] >= 0)).float().sum() /
+                     (y[:65536] >= 0).sum())
+    del x, y, xs, ys
+    # The bench's P frame and references.
+    frames, _ = make_inputs(SEED)
+    gs = GpuStep(ctx, frames, vp8a.load(), torch, 0)
+    with learned.on_ctx_stream(ctx):
+        src = gs.cur[0]
+        refs = [gs.last[0], gs.golden[0], gs.alt[0]]
+        xy = learned.all_mbs(MB_COLS, MB_ROWS)
+    ctx.synchronize()
+    stream = gs.stream
+
+    def learned_step():
+        return [learned.learned_search(ctx, net, src, r, xy) for r in refs]
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        ctx.synchronize()
+        ts = []
+        for _ in range(steps):
+            torch.cuda.synchronize()
+            s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s_.record(stream)
+            fn()
+            e_.record(stream)
+            e_.synchronize()
+            ts.append(s_.elapsed_time(e_))
+        return float(np.median(ts)), ts
+
+    ms_learned, ts_l = timed(learned_step, args.steps, args.warmup)
+    ms_plain, ts_p = timed(gs.run_analysis, args.steps, args.warmup)
+    # Quality against the plain search's per-reference results (trace).
+    res = learned_step()
+    plain_sad = []
+    for rp in (gs.last, gs.golden, gs.alt):
+        planes_np = tuple(p.cpu().numpy() for p in rp)
+        _, tr = vp8a.analyse_inter_frame(ctx, frames[8], [planes_np], [abi.REF_LAST], lam, trace=True)
+        plain_sad.append(tr[..., 0]["quarter"]["sad"].reshape(-1).astype(np.float64))
+    ratio = [float(np.asarray(o[1], np.float64).mean() / ps.mean()) for o, ps in zip(res, plain_sad)]
+    fb = [float(np.mean(o[2])) for o in res]
+    ctx.close()
+    return {"case": "learned", "size": "%dx%d" % (W, H), "unit": "MB/s",
+            "learned_me_mbs_per_s": round(N_MB / (ms_learned / 1e3), 1), "learned_me_ms": round(ms_learned, 3),
+            "plain_analysis_mbs_per_s": round(N_MB / (ms_plain / 1e3), 1), "plain_analysis_ms": round(ms_plain, 3),
+            "speedup_vs_plain_analysis": round(ms_plain / ms_learned, 2),
+            "mean_sad_ratio_vs_plain_per_ref": [round(v, 4) for v in ratio],
+            "fallback_rate_per_ref": [round(v, 4) for v in fb],
+            "training": {"labels": int(n), "steps": args.train_steps, "batch": 4096, "lr": 1e-3,
+                         "first_loss": round(float(np.mean(losses[:5])), 4),
+                         "last_loss": round(float(np.mean(losses[-5:])), 4), "top4_label_hit": round(top4, 4),
+                         "label_s": round(t_labels, 1), "train_s": round(t_train, 1)},
+            "learned_ms": [round(v, 3) for v in ts_l], "plain_ms": [round(v, 3) for v in ts_p],
+            "note": "learned = proposal net + exact +-2 px search at 4 seeds + sub-pel + descent fallback, 3 refs, "
+                    "per-reference vectors; plain = the exhaustive analysis (census, SPLITMV, RD decision) of the "
+                    "same frame and references"}
+
+
 def batched_predict(ctx, vp8a, torch, split):
     """vp8a_predict_inter_mb (or _split_mv) over 8 frames' worth of MBs at
     random positions of random MB-padded reference planes of the --size grid,
@@ -923,15 +1032,18 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--case", choices=["arnr", "analysis", "lf", "recon", "predict", "predict_mb", "predict_split",
-                                       "batch"],
+                                       "batch", "learned"],
                     help="profile one stage alone, or (batch) the batched many-stream path")
     ap.add_argument("--streams", type=int, default=48, help="streams of the batch case")
+    ap.add_argument("--train-steps", type=int, default=300, help="training steps of the learned case")
     ap.add_argument("--size", default="1920x1080", help="frame size for --case")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl != "reference":
         log("note: fewer than 3 warm-up steps")
     if args.case == "batch":
         res = batch_arm(args)
+    elif args.case == "learned":
+        res = learned_arm(args)
     elif args.case:
         res = case_arm(args)
     else:
