@@ -9,8 +9,8 @@
 // Kernels (all hand-written; the GEMM-shaped ones on the tensor cores with
 // mma.sync m16n8k16 BF16 -> FP32):
 //   lp_windows_kernel       coarse cost volumes -> NHWC [n, 32, 32, 2] BF16
-//   lp_conv_fwd_kernel      implicit-GEMM conv (+ bias, ReLU), one warp per
-//                           16 output pixels x all output channels
+//   lp_conv_fwd_smem_kernel implicit-GEMM conv (+ bias, ReLU), one CTA per
+//                           image staged with its halo in shared memory
 //   lp_conv_bwd_data_kernel dX = conv^T(dY, W), masked by the ReLU of X
 //   lp_conv_bwd_w_kernel    dW = sum over pixels of dY x shifted X (split
 //                           over pixel chunks, FP32 atomics), db
@@ -91,57 +91,89 @@ __global__ void __launch_bounds__(256) lp_windows_kernel(const uint8_t* src, uin
 
 // ------------------------------------------------------------ conv fwd
 
-// One warp per 16 output pixels (one half row) x COUT (NT tiles of 8).
-// A[p][k] = X[p + off(tap)][ci], k = tap * CP + ci (CP = CIN rounded up to
-// 16); B[k][n] = W[n][tap][ci].
+// Implicit GEMM: A[p][k] = X[p + off(tap)][ci], k = tap * CP + ci (CP = CIN
+// rounded up to 16); B[k][n] = W[n][tap][ci].
+// Forward pass with the image staged: one CTA (8 warps) per image. The
+// 32x32 input gets a zero halo (34x34) in shared memory, one pixel every PS
+// halves (channels padded to CP, then 8 spare: a 16-byte-aligned row whose
+// 32-bit words fall on distinct banks for the 8 pixels x 4 channel pairs a
+// fragment reads); the weights sit beside it ([n][tap][ci], n stride
+// 9 CIN + 8). Warp w takes the 16-pixel tiles w, w + 8, ... of the image.
 template <int CIN, int NT>
-__global__ void __launch_bounds__(128) lp_conv_fwd_kernel(const uint16_t* X, const uint16_t* W, const float* bias,
-                                                          int cout, int n_img, int relu, uint16_t* Y, float* Yf) {
-  constexpr int CP = (CIN + 15) / 16 * 16;
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  const int tile = blockIdx.x * 4 + (threadIdx.x >> 5);
-  if (tile >= n_img * (LP_P / 16)) return;
-  const int img = tile / (LP_P / 16), rem = tile % (LP_P / 16), y = rem >> 1, xb = (rem & 1) * 16;
-  float d[NT][4];
-#pragma unroll
-  for (int j = 0; j < NT; j++) d[j][0] = d[j][1] = d[j][2] = d[j][3] = 0.f;
-  for (int tap = 0; tap < 9; tap++) {
-    const int dy = tap / 3 - 1, dx = tap % 3 - 1;
-#pragma unroll
-    for (int c0 = 0; c0 < CP; c0 += 16) {
-      uint32_t a[4];
-      const int ca = c0 + 2 * t, cb = c0 + 2 * t + 8;
-      a[0] = pack_raw(act(X, CIN, img, y + dy, xb + g + dx, ca), act(X, CIN, img, y + dy, xb + g + dx, ca + 1));
-      a[1] = pack_raw(act(X, CIN, img, y + dy, xb + g + 8 + dx, ca), act(X, CIN, img, y + dy, xb + g + 8 + dx, ca + 1));
-      a[2] = pack_raw(act(X, CIN, img, y + dy, xb + g + dx, cb), act(X, CIN, img, y + dy, xb + g + dx, cb + 1));
-      a[3] = pack_raw(act(X, CIN, img, y + dy, xb + g + 8 + dx, cb), act(X, CIN, img, y + dy, xb + g + 8 + dx, cb + 1));
-#pragma unroll
-      for (int j = 0; j < NT; j++) {
-        const int n = j * 8 + g;
-        auto wv = [&](int ci) -> uint16_t {
-          return (n < cout && ci < CIN) ? W[((size_t)n * 9 + tap) * CIN + ci] : (uint16_t)0;
-        };
-        const uint32_t b[2] = {pack_raw(wv(ca), wv(ca + 1)), pack_raw(wv(cb), wv(cb + 1))};
-        mma_bf16(d[j], a, b);
-      }
+__global__ void __launch_bounds__(256) lp_conv_fwd_smem_kernel(const uint16_t* X, const uint16_t* W, const float* bias,
+                                                               int cout, int relu, uint16_t* Y, float* Yf) {
+  constexpr int CP = (CIN + 15) / 16 * 16, PS = CP + 8, WS = 9 * CIN + 8, COUTP = NT * 8;
+  extern __shared__ __align__(16) uint16_t sm[];
+  uint16_t* img_s = sm;                 // 34 * 34 * PS
+  uint16_t* w_s = sm + 34 * 34 * PS;    // COUTP * WS
+  const int img = blockIdx.x, tid = threadIdx.x;
+  // Zero the halo and the channel padding, then copy the image.
+  for (int q = tid; q < 34 * 34 * PS / 2; q += blockDim.x) reinterpret_cast<uint32_t*>(img_s)[q] = 0u;
+  for (int q = tid; q < COUTP * WS / 2; q += blockDim.x) reinterpret_cast<uint32_t*>(w_s)[q] = 0u;
+  __syncthreads();
+  const uint16_t* Xi = X + (size_t)img * LP_P * CIN;
+  if (CIN % 2 == 0) {
+    for (int q = tid; q < LP_P * CIN / 2; q += blockDim.x) {
+      const int p = q / (CIN / 2), c = (q % (CIN / 2)) * 2;
+      const int sy = (p >> 5) + 1, sx = (p & 31) + 1;
+      *reinterpret_cast<uint32_t*>(img_s + (sy * 34 + sx) * PS + c) = reinterpret_cast<const uint32_t*>(Xi)[q];
     }
   }
+  for (int q = tid; q < cout * 9 * CIN; q += blockDim.x) w_s[(q / (9 * CIN)) * WS + q % (9 * CIN)] = W[q];
+  __syncthreads();
+  const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+  for (int tile = warp; tile < LP_P / 16; tile += 8) {
+    const int y = tile >> 1, xb = (tile & 1) * 16;
+    float d[NT][4];
 #pragma unroll
-  for (int j = 0; j < NT; j++) {
+    for (int j = 0; j < NT; j++) d[j][0] = d[j][1] = d[j][2] = d[j][3] = 0.f;
 #pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const int p = y * LP_S + xb + g + 8 * h;
+    for (int tap = 0; tap < 9; tap++) {
+      const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+      const uint16_t* r0 = img_s + ((y + dy + 1) * 34 + (xb + g + dx + 1)) * PS;
+      const uint16_t* r1 = r0 + 8 * PS;
 #pragma unroll
-      for (int e = 0; e < 2; e++) {
-        const int n = j * 8 + 2 * t + e;
-        if (n >= cout) continue;
-        float v = d[j][2 * h + e] + bias[n];
-        if (relu) v = fmaxf(v, 0.f);
-        const size_t o = ((size_t)img * LP_P + p) * cout + n;
-        if (Yf) Yf[o] = v;
-        else Y[o] = __bfloat16_as_ushort(__float2bfloat16_rn(v));
+      for (int c0 = 0; c0 < CP; c0 += 16) {
+        uint32_t a[4];
+        a[0] = *reinterpret_cast<const uint32_t*>(r0 + c0 + 2 * t);
+        a[1] = *reinterpret_cast<const uint32_t*>(r1 + c0 + 2 * t);
+        a[2] = *reinterpret_cast<const uint32_t*>(r0 + c0 + 2 * t + 8);
+        a[3] = *reinterpret_cast<const uint32_t*>(r1 + c0 + 2 * t + 8);
+#pragma unroll
+        for (int j = 0; j < NT; j++) {
+          const uint16_t* wr = w_s + (j * 8 + g) * WS + tap * CIN + c0 + 2 * t;
+          uint32_t b[2];
+          if (CIN >= 16) {
+            b[0] = *reinterpret_cast<const uint32_t*>(wr);
+            b[1] = *reinterpret_cast<const uint32_t*>(wr + 8);
+          } else {  // CIN = 2: channels past CIN are zero
+            b[0] = (c0 + 2 * t < CIN) ? *reinterpret_cast<const uint32_t*>(wr) : 0u;
+            b[1] = 0u;
+          }
+          mma_bf16(d[j], a, b);
+        }
       }
     }
+#pragma unroll
+    for (int j = 0; j < NT; j++)
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int p = y * LP_S + xb + g + 8 * h, n = j * 8 + 2 * t;
+        const size_t o = ((size_t)img * LP_P + p) * cout + n;
+        float v0 = d[j][2 * h] + (n < cout ? bias[n] : 0.f), v1 = d[j][2 * h + 1] + (n + 1 < cout ? bias[n + 1] : 0.f);
+        if (relu) {
+          v0 = fmaxf(v0, 0.f);
+          v1 = fmaxf(v1, 0.f);
+        }
+        if (Yf) {
+          if (n < cout) Yf[o] = v0;
+          if (n + 1 < cout) Yf[o + 1] = v1;
+        } else if (n + 1 < cout) {
+          *reinterpret_cast<uint32_t*>(Y + o) = pack_bf16(v0, v1);
+        } else if (n < cout) {
+          Y[o] = __bfloat16_as_ushort(__float2bfloat16_rn(v0));
+        }
+      }
   }
 }
 
@@ -309,8 +341,12 @@ __global__ void lp_adam_kernel(float* w, const float* grad, float* m, float* v, 
 template <int CIN, int NT>
 vp8a_status conv_fwd(vp8a_ctx* ctx, const uint16_t* X, const uint16_t* W, const float* b, int cout, int n, int relu,
                      uint16_t* Y, float* Yf) {
-  const int tiles = n * (LP_P / 16);
-  lp_conv_fwd_kernel<CIN, NT><<<(tiles + 3) / 4, 128, 0, ctx->stream>>>(X, W, b, cout, n, relu, Y, Yf);
+  if (n == 0) return VP8A_OK;
+  constexpr int CP = (CIN + 15) / 16 * 16, PS = CP + 8, WS = 9 * CIN + 8;
+  const size_t smem = sizeof(uint16_t) * (34 * 34 * PS + NT * 8 * WS);
+  VP8A_CUDA(cudaFuncSetAttribute(lp_conv_fwd_smem_kernel<CIN, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  lp_conv_fwd_smem_kernel<CIN, NT><<<n, 256, smem, ctx->stream>>>(X, W, b, cout, relu, Y, Yf);
   VP8A_CUDA(cudaGetLastError());
   ctx->launches++;
   return VP8A_OK;
