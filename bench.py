@@ -940,6 +940,32 @@ def learned_arm(args):
         top4 = float(((cells == y[:65536, None].long()).any(1) & (y[:65536] >= 0)).float().sum() /
                      (y[:65536] >= 0).sum())
     del x, y, xs, ys
+    # Loop-filter window head: the plain path's level choice on training
+    # frames at several quantisers (reconstruction + full sweep + walk).
+    head = learned.LfWindowHead(ctx, seed=3)
+    sample = learned.sample_mbs(MB_COLS, MB_ROWS, 256, seed=1)
+    lf_frames, lf_levels = [], []
+    qis = [24, 44, 64, 100]
+    for sidx in range(4):
+        frames_t, _ = synth.make_sequence(W, H, 7, SEED + 1000 + sidx, pieces=4, occluders=4)
+        for k in range(1, 7):
+            qi = qis[(sidx * 6 + k) % len(qis)]
+            ref = pad_planes(frames_t[k - 1])
+            dec = vp8a.analyse_inter_frame(ctx, frames_t[k], [ref], [abi.REF_LAST], vp8a.rd_lambda(qi))
+            rec = tuple(np.array(p_) for p_ in ref)
+            lfi = np.zeros(N_MB, abi.MB_LF_INFO_DTYPE)
+            vp8a.reconstruct_inter_frame(ctx, frames_t[k], [ref], [abi.REF_LAST], dec, abi.quant_indices(qi), rec,
+                                         lf_info=lfi)
+            tab = vp8a.filter_sweep(ctx, rec, lfi, abi.filter_config(0, 0), frames_t[k])
+            level, _ = select_full(tab.reshape(-1), 0)
+            with learned.on_ctx_stream(ctx):
+                src_t = torch.from_numpy(frames_t[k][0]).cuda()
+                ref_t = torch.from_numpy(ref[0]).cuda()
+            sums, count = head.features(net, src_t, ref_t, sample, qi)
+            lf_frames.append((sums, count, level))
+            lf_levels.append(int(level))
+    head_losses = [head.train_step(lf_frames, lr=1e-2) for _ in range(200)]
+    head_hits = sum(1 for (sm_, ct_, lv_) in lf_frames if head.window(sm_, ct_)[0] <= lv_ <= head.window(sm_, ct_)[1])
     # The bench's P frame and references.
     frames, _ = make_inputs(SEED)
     gs = GpuStep(ctx, frames, vp8a.load(), torch, 0)
@@ -970,6 +996,31 @@ def learned_arm(args):
 
     ms_learned, ts_l = timed(learned_step, args.steps, args.warmup)
     ms_plain, ts_p = timed(gs.run_analysis, args.steps, args.warmup)
+    # The full step with the learned loop-filter window: ARNR, the plain
+    # analysis and reconstruction, the head's window from 256 sampled MBs
+    # (net layers 1-3 against LAST), the sweep over level 0 and the window's
+    # 9 levels, the reference's walk over that table.
+    win_tab = torch.zeros(512, dtype=torch.int64, device="cuda")
+    choice = {}
+
+    def window_step():
+        gs.run_arnr()
+        gs.run_analysis()
+        gs.run_recon()
+        sums, count = head.features(net, src, refs[0], sample, QI)
+        lo, hi = head.window(sums, count)
+        st_ = gs.lib.vp8a_filter_sweep_window(ctx.handle, C.byref(gs.recon_planes), gs.mbs.data_ptr(),
+                                              C.byref(gs.base), C.byref(gs.src), lo, hi, win_tab.data_ptr())
+        assert st_ == 0, vp8a.load().vp8a_last_error()
+        ctx.synchronize()
+        choice["window"] = (lo, hi)
+        choice["learned"] = select_full(win_tab.cpu().numpy().view(np.uint64), 0)
+
+    def plain_step():
+        choice["plain"] = gs.step()
+
+    ms_wstep, ts_w = timed(window_step, args.steps, args.warmup)
+    ms_pstep, ts_ps = timed(plain_step, args.steps, args.warmup)
     # Quality against the plain search's per-reference results (trace).
     res = learned_step()
     plain_sad = []
@@ -991,6 +1042,14 @@ def learned_arm(args):
                          "last_loss": round(float(np.mean(losses[-5:])), 4), "top4_label_hit": round(top4, 4),
                          "label_s": round(t_labels, 1), "train_s": round(t_train, 1)},
             "learned_ms": [round(v, 3) for v in ts_l], "plain_ms": [round(v, 3) for v in ts_p],
+            "lf_window": {"step_ms_learned_window": round(ms_wstep, 3), "step_ms_plain": round(ms_pstep, 3),
+                          "step_mbs_per_s_learned_window": round(N_MB / (ms_wstep / 1e3), 1),
+                          "step_mbs_per_s_plain": round(N_MB / (ms_pstep / 1e3), 1),
+                          "speedup": round(ms_pstep / ms_wstep, 2), "window": list(choice["window"]),
+                          "choice_learned": list(choice["learned"]), "choice_plain": list(choice["plain"]),
+                          "train_frames": len(lf_frames), "train_levels": sorted(set(lf_levels)),
+                          "train_window_hits": head_hits, "head_loss_first_last": [round(head_losses[0], 4),
+                                                                                    round(head_losses[-1], 4)]},
             "note": "learned = proposal net + exact +-2 px search at 4 seeds + sub-pel + descent fallback, 3 refs, "
                     "per-reference vectors; plain = the exhaustive analysis (census, SPLITMV, RD decision) of the "
                     "same frame and references"}

@@ -484,6 +484,16 @@ vp8a_status vp8a_filter_sweep_noalloc(vp8a_ctx* ctx, const vp8a_planes* planes,
                                       const vp8a_source* src, uint32_t every_rows,
                                       uint64_t* ssd_out);
 
+/* vp8a_filter_sweep restricted to level 0 and levels lo_level..hi_level
+ * (every sharpness): ssd_out[level * 8 + sharpness] is written for those
+ * and UINT64_MAX elsewhere, so the reference's selection walk over the
+ * table stays inside the window. No counterpart in the reference: the
+ * learned proposal's loop-filter window. */
+vp8a_status vp8a_filter_sweep_window(vp8a_ctx* ctx, const vp8a_planes* planes,
+                                     const vp8a_mb_lf_info* mbs, const vp8a_filter_config* base,
+                                     const vp8a_source* src, uint32_t lo_level, uint32_t hi_level,
+                                     uint64_t* ssd_out);
+
 /* select_filter_params (src/loop_filter.rs:2047): the reference's coarse
  * grid + refine + sharpness search, replayed over the device sweep. */
 vp8a_status vp8a_select_filter_params(vp8a_ctx* ctx, const vp8a_planes* planes,
@@ -631,6 +641,18 @@ vp8a_status vp8a_lp_conv_backward(vp8a_ctx* ctx, const uint16_t* x, uint32_t cin
  * into `label_prob` (each optional). */
 vp8a_status vp8a_lp_softmax_ce(vp8a_ctx* ctx, const float* logits, const int32_t* labels, uint32_t n,
                                uint16_t* dlogits, float* loss, float* label_prob);
+
+/* Channel sums of n images' activations ([n][32][32][c] BF16, c divides
+ * 256, at most 64) added into sums[c] (FP32). */
+vp8a_status vp8a_lp_pool(vp8a_ctx* ctx, const uint16_t* x, uint32_t c, uint32_t n, float* sums);
+
+/* The loop-filter level head: features f = sums / count (c of them),
+ * scores z = w f + b over `levels` levels ([levels][c] weights), written to
+ * `logits` (optional); with label >= 0 the cross-entropy is added to `loss`
+ * (optional) and its gradients to dw, db. */
+vp8a_status vp8a_lp_lf_head(vp8a_ctx* ctx, const float* sums, float count, uint32_t c, const float* w,
+                            const float* b, uint32_t levels, int32_t label, float* logits, float* dw,
+                            float* db, float* loss);
 
 /* One Adam step (bias-corrected for `step` >= 1) on FP32 master weights;
  * writes their BF16 copies. */

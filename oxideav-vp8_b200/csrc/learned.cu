@@ -338,6 +338,54 @@ __global__ void lp_adam_kernel(float* w, const float* grad, float* m, float* v, 
   w_bf16[i] = __bfloat16_as_ushort(__float2bfloat16_rn(wi));
 }
 
+// ------------------------------------------------- loop-filter window
+
+// Channel sums of n images' activations ([n][32][32][C] BF16) into
+// out[C] (FP32, accumulated): one CTA per image.
+__global__ void __launch_bounds__(256) lp_pool_kernel(const uint16_t* X, int C, float* out) {
+  __shared__ float part[64];
+  const int img = blockIdx.x, t = threadIdx.x;
+  if (t < 64) part[t] = 0.f;
+  __syncthreads();
+  const uint16_t* Xi = X + (size_t)img * LP_P * C;
+  // Thread t sums channel t % C over pixels t / C, t / C + 256 / C, ...
+  const int c = t % C, step = 256 / C;
+  float s = 0.f;
+  if (t < step * C)
+    for (int p = t / C; p < LP_P; p += step) s += __bfloat162float(__ushort_as_bfloat16(Xi[(size_t)p * C + c]));
+  atomicAdd(&part[c], s);
+  __syncthreads();
+  if (t < C) atomicAdd(&out[t], part[t]);
+}
+
+// The head: f = sums / count (C features), z = W f + b (L levels), softmax;
+// with a label: loss += CE, dW += (p - onehot) f^T, db += p - onehot. One
+// CTA of L threads.
+__global__ void lp_lf_head_kernel(const float* sums, float count, int C, const float* W, const float* b, int L,
+                                  int label, float* logits, float* dW, float* db, float* loss) {
+  __shared__ float f[64], z[128];
+  const int t = threadIdx.x;
+  if (t < C) f[t] = sums[t] / count;
+  __syncthreads();
+  float zi = 0.f;
+  if (t < L) {
+    zi = b[t];
+    for (int c = 0; c < C; c++) zi += W[t * C + c] * f[c];
+    z[t] = zi;
+    if (logits) logits[t] = zi;
+  }
+  __syncthreads();
+  if (label < 0 || t >= L) return;
+  float m = -INFINITY;
+  for (int k = 0; k < L; k++) m = fmaxf(m, z[k]);
+  float s = 0.f;
+  for (int k = 0; k < L; k++) s += __expf(z[k] - m);
+  const float p = __expf(zi - m) / s, gz = p - (t == label ? 1.f : 0.f);
+  for (int c = 0; c < C; c++) dW[t * C + c] += gz * f[c];
+  db[t] += gz;
+  if (t == label && loss) *loss += -(zi - m - __logf(s));
+}
+
 template <int CIN, int NT>
 vp8a_status conv_fwd(vp8a_ctx* ctx, const uint16_t* X, const uint16_t* W, const float* b, int cout, int n, int relu,
                      uint16_t* Y, float* Yf) {
@@ -464,6 +512,34 @@ vp8a_status vp8a_lp_adam(vp8a_ctx* ctx, float* w, const float* grad, float* m, f
   const float c1 = 1.f - powf(beta1, (float)step), c2 = 1.f - powf(beta2, (float)step);
   lp_adam_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(w, grad, m, v, (int)n, lr, beta1, beta2, eps, c1, c2,
                                                             w_bf16);
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
+  return VP8A_OK;
+}
+
+vp8a_status vp8a_lp_pool(vp8a_ctx* ctx, const uint16_t* x, uint32_t c, uint32_t n, float* sums) {
+  if (!ctx || !sums || (n && !x) || c == 0 || c > 64 || 256 % c != 0) {
+    vp8a::set_error("null argument or channel count not a divisor of 256 up to 64");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (n == 0) return VP8A_OK;
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  lp_pool_kernel<<<n, 256, 0, ctx->stream>>>(x, (int)c, sums);
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
+  return VP8A_OK;
+}
+
+vp8a_status vp8a_lp_lf_head(vp8a_ctx* ctx, const float* sums, float count, uint32_t c, const float* w,
+                            const float* b, uint32_t levels, int32_t label, float* logits, float* dw, float* db,
+                            float* loss) {
+  if (!ctx || !sums || !w || !b || c == 0 || c > 64 || levels == 0 || levels > 128 || !(count > 0.f) ||
+      (label >= 0 && (!dw || !db || label >= (int32_t)levels))) {
+    vp8a::set_error("bad loop-filter head arguments");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  lp_lf_head_kernel<<<1, 128, 0, ctx->stream>>>(sums, count, (int)c, w, b, (int)levels, label, logits, dw, db, loss);
   VP8A_CUDA(cudaGetLastError());
   ctx->launches++;
   return VP8A_OK;

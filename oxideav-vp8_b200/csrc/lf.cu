@@ -1114,10 +1114,19 @@ void grid_candidates(const vp8a_filter_config& base, std::vector<uint8_t>& pairs
   }
 }
 
-// Upload a grid's candidate pairs and masks into `a`.
-vp8a_status upload_grid(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_filter_config& base, LfArgs* a) {
-  std::vector<uint8_t> pairs, masks;
-  grid_candidates(base, pairs, masks);
+// Upload a grid's candidate pairs and masks into `a` (level 0 and the
+// levels lo..hi).
+vp8a_status upload_grid(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_filter_config& base, LfArgs* a, int lo = 1,
+                        int hi = 63) {
+  std::vector<uint8_t> all_pairs, all_masks, pairs, masks;
+  grid_candidates(base, all_pairs, all_masks);
+  for (size_t i = 0; i < all_masks.size(); i++) {
+    const int level = all_pairs[2 * i];
+    if (level != 0 && (level < lo || level > hi)) continue;
+    pairs.push_back(all_pairs[2 * i]);
+    pairs.push_back(all_pairs[2 * i + 1]);
+    masks.push_back(all_masks[i]);
+  }
   const size_t n = masks.size();
   std::vector<uint8_t> blob(3 * n);
   memcpy(blob.data(), pairs.data(), 2 * n);
@@ -1330,6 +1339,29 @@ vp8a_status vp8a_filter_sweep(vp8a_ctx* ctx, const vp8a_planes* planes, const vp
   L.a.ssd_out = (uint64_t*)dt;
   L.a.level0_unfiltered = 1;
   if ((s = upload_grid(ctx, st, *base, &L.a)) != VP8A_OK) return s;
+  if ((s = run_sweep(ctx, L.a, L.a.n_cands, &st)) != VP8A_OK) return s;
+  return st.finish();
+}
+
+vp8a_status vp8a_filter_sweep_window(vp8a_ctx* ctx, const vp8a_planes* planes, const vp8a_mb_lf_info* mbs,
+                                     const vp8a_filter_config* base, const vp8a_source* src, uint32_t lo_level,
+                                     uint32_t hi_level, uint64_t* ssd_out) {
+  if (!ctx || !src || !ssd_out || !base) return VP8A_E_INVALID_ARGUMENT;
+  if (lo_level > hi_level || hi_level > 63) {
+    vp8a::set_error("window levels must satisfy lo <= hi <= 63");
+    return VP8A_E_LOOP_FILTER_LEVEL_OUT_OF_RANGE;
+  }
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  LfInputs L;
+  vp8a_status s = stage_lf(ctx, st, planes, mbs, base, src, 0, false, &L);
+  if (s != VP8A_OK) return s;
+  void* dt;
+  if ((s = st.out(ssd_out, 512 * sizeof(uint64_t), &dt)) != VP8A_OK) return s;
+  VP8A_CUDA(cudaMemsetAsync(dt, 0xff, 512 * sizeof(uint64_t), ctx->stream));
+  L.a.ssd_out = (uint64_t*)dt;
+  L.a.level0_unfiltered = 1;
+  if ((s = upload_grid(ctx, st, *base, &L.a, (int)std::max(1u, lo_level), (int)hi_level)) != VP8A_OK) return s;
   if ((s = run_sweep(ctx, L.a, L.a.n_cands, &st)) != VP8A_OK) return s;
   return st.finish();
 }

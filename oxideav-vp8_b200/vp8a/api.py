@@ -332,6 +332,17 @@ def filter_sweep(ctx, recon, mbs, base, src, every_rows=0):
     return out.reshape(64, 8)
 
 
+def filter_sweep_window(ctx, recon, mbs, base, src, lo_level, hi_level):
+    """vp8a_filter_sweep_window: the sweep table for level 0 and levels
+    lo..hi only (UINT64_MAX elsewhere); a (64, 8) uint64 table."""
+    p, s = planes(*recon), source(*src)
+    m = np.ascontiguousarray(mbs, abi.MB_LF_INFO_DTYPE)
+    out = np.zeros(512, np.uint64)
+    check(ctx._lib.vp8a_filter_sweep_window(ctx.handle, C.byref(p), ptr(m), C.byref(base), C.byref(s), lo_level,
+                                            hi_level, ptr(out)), "vp8a_filter_sweep_window")
+    return out.reshape(64, 8)
+
+
 def select_filter_params(ctx, recon, mbs, base, src):
     """select_filter_params (src/loop_filter.rs:2047) -> (level, sharpness)."""
     p, s = planes(*recon), source(*src)

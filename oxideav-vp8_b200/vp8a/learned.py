@@ -313,3 +313,85 @@ def _source_mbs(src_y, mb_xy, h, w):
     ys = (xy[:, 1:2] * 16 + oy[None, :]).clamp(max=h - 1)
     xs = (xy[:, 0:1] * 16 + oy[None, :]).clamp(max=w - 1)
     return src_y[ys[:, :, None], xs[:, None, :]].reshape(-1, 256).contiguous()
+
+
+LF_LEVELS = 64
+LF_WINDOW = 9
+
+
+class LfWindowHead:
+    """The proposal's loop-filter level window: a linear head over the
+    net's layer-3 features averaged over a sample of the frame's MBs, plus
+    the frame's quantiser index (qi / 127), scoring the 64 levels; the
+    window is the 9 levels around the best score. Trained with the frame's
+    level chosen by the plain search (vp8a_lp_lf_head, Adam)."""
+
+    C = 33  # 32 pooled channels + qi
+
+    def __init__(self, ctx, seed=0):
+        import torch
+
+        self.torch, self.ctx = torch, ctx
+        g = torch.Generator().manual_seed(seed)
+        self.w = (torch.randn(LF_LEVELS * self.C, generator=g) * 0.05).cuda()
+        self.b = torch.zeros(LF_LEVELS, device="cuda")
+        self.state = {k: torch.zeros_like(v) for k, v in (("mw", self.w), ("vw", self.w), ("mb", self.b),
+                                                          ("vb", self.b), ("gw", self.w), ("gb", self.b))}
+        self.wh = self.w.to(torch.bfloat16)
+        self.bh = self.b.to(torch.bfloat16)
+        self.steps = 0
+
+    def features(self, net, src_y, ref_y, mb_xy, qi):
+        """(sums [33] FP32 device tensor, count) of one frame: the layer-3
+        channel sums over the sampled MBs' 32x32 maps, and qi / 127 x count."""
+        torch = self.torch
+        with on_ctx_stream(self.ctx):
+            h, w = src_y.shape[0], src_y.shape[1]
+            x = windows(self.ctx, src_y, ref_y[:h, :w], mb_xy)
+            net.forward(x, keep=True)
+            a3 = net._acts[3]
+            sums = torch.zeros(self.C, dtype=torch.float32, device="cuda")
+            check(self.ctx._lib.vp8a_lp_pool(self.ctx.handle, ptr(a3), 32, a3.shape[0], ptr(sums)), "vp8a_lp_pool")
+            count = float(a3.shape[0] * PIX)
+            sums[32] = qi / 127.0 * count
+        return sums, count
+
+    def train_step(self, frames, lr=1e-2):
+        """frames: list of (sums, count, level). Returns the summed loss."""
+        torch = self.torch
+        with on_ctx_stream(self.ctx):
+            self.state["gw"].zero_()
+            self.state["gb"].zero_()
+            loss = torch.zeros(1, device="cuda")
+            for sums, count, level in frames:
+                check(self.ctx._lib.vp8a_lp_lf_head(self.ctx.handle, ptr(sums), count, self.C, ptr(self.w),
+                                                    ptr(self.b), LF_LEVELS, int(level), None, ptr(self.state["gw"]),
+                                                    ptr(self.state["gb"]), ptr(loss)), "vp8a_lp_lf_head")
+            self.steps += 1
+            for w, g, m, v, wh in ((self.w, self.state["gw"], self.state["mw"], self.state["vw"], self.wh),
+                                   (self.b, self.state["gb"], self.state["mb"], self.state["vb"], self.bh)):
+                check(self.ctx._lib.vp8a_lp_adam(self.ctx.handle, ptr(w), ptr(g), ptr(m), ptr(v), w.numel(), lr, 0.9,
+                                                 0.999, 1e-8, self.steps, ptr(wh)), "vp8a_lp_adam")
+            return float(loss.item())
+
+    def window(self, sums, count):
+        """(lo, hi): the 9 levels around the best-scored level, inside 0..63."""
+        torch = self.torch
+        with on_ctx_stream(self.ctx):
+            z = torch.empty(LF_LEVELS, device="cuda")
+            check(self.ctx._lib.vp8a_lp_lf_head(self.ctx.handle, ptr(sums), count, self.C, ptr(self.w), ptr(self.b),
+                                                LF_LEVELS, -1, ptr(z), None, None, None), "vp8a_lp_lf_head")
+            c = int(torch.argmax(z).item())
+        lo = max(0, min(c - LF_WINDOW // 2, LF_LEVELS - LF_WINDOW))
+        return lo, lo + LF_WINDOW - 1
+
+
+def sample_mbs(mb_cols, mb_rows, n=256, seed=0, device="cuda"):
+    """n MB positions spread over the frame (seeded)."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    total = mb_cols * mb_rows
+    idx = np.sort(rng.choice(total, size=min(n, total), replace=False))
+    xy = np.stack([idx % mb_cols, idx // mb_cols], 1).astype(np.uint32)
+    return torch.from_numpy(xy.view(np.int32)).to(device)

@@ -42,6 +42,9 @@ PROTOTYPES = {
     "vp8a_lp_conv_backward": (C.c_int, [P, P, U32, P, U32, U32, P, U32, P, P, P]),
     "vp8a_lp_softmax_ce": (C.c_int, [P, P, P, U32, P, P, P]),
     "vp8a_lp_adam": (C.c_int, [P, P, P, P, P, U32, C.c_float, C.c_float, C.c_float, C.c_float, U32, P]),
+    "vp8a_lp_pool": (C.c_int, [P, P, U32, U32, P]),
+    "vp8a_lp_lf_head": (C.c_int, [P, P, C.c_float, U32, P, P, U32, C.c_int32, P, P, P, P]),
+    "vp8a_filter_sweep_window": (C.c_int, [P, P, P, P, P, U32, U32, P]),
     "vp8a_rd_inter_search": (
         C.c_int,
         [P, C.POINTER(abi.I420), P, P, U32, C.POINTER(abi.MvContexts), C.c_double, U32, U32, P, P],

@@ -216,3 +216,45 @@ def test_learned_search_is_exact_and_beats_zero_seeds(ctx, oracle):
     # And the plain exhaustive search's per-MB result for reference.
     _, plain_sad = learned.labels_from_search(ctx, src, ref, lam)
     assert sad.mean() <= 1.15 * plain_sad.mean(), (sad.mean(), plain_sad.mean())
+
+
+def test_filter_sweep_window_matches_the_full_table(ctx, oracle):
+    from test_gpu_lf import lf_case
+
+    src, recon, m = lf_case(160, 96, seed=4)
+    base = abi.filter_config(0, 2, delta_enabled=1, ref_delta_last=3)
+    full = vp8a.filter_sweep(ctx, recon, m, base, src)
+    win = vp8a.filter_sweep_window(ctx, recon, m, base, src, 20, 28)
+    inside = np.zeros((64, 8), bool)
+    inside[0] = True
+    inside[20:29] = True
+    assert np.array_equal(win[inside], full[inside])
+    assert (win[~inside] == np.uint64(2 ** 64 - 1)).all()
+
+
+def test_lf_head_matches_its_definition(ctx):
+    rng = np.random.default_rng(8)
+    c, levels = 33, 64
+    sums = (rng.standard_normal(c) * 100).astype(np.float32)
+    count = 50.0
+    w = (rng.standard_normal(levels * c) * 0.1).astype(np.float32)
+    b = (rng.standard_normal(levels) * 0.1).astype(np.float32)
+    d = {k: torch.from_numpy(v).cuda() for k, v in (("s", sums), ("w", w), ("b", b))}
+    z = torch.empty(levels, device="cuda")
+    gw = torch.zeros(levels * c, device="cuda")
+    gb = torch.zeros(levels, device="cuda")
+    loss = torch.zeros(1, device="cuda")
+    torch.cuda.synchronize()
+    assert ctx._lib.vp8a_lp_lf_head(ctx.handle, d["s"].data_ptr(), count, c, d["w"].data_ptr(), d["b"].data_ptr(),
+                                    levels, 17, z.data_ptr(), gw.data_ptr(), gb.data_ptr(), loss.data_ptr()) == abi.OK
+    ctx.synchronize()
+    f = sums / count
+    zz = w.reshape(levels, c) @ f + b
+    p = np.exp(zz - zz.max())
+    p /= p.sum()
+    g = p.copy()
+    g[17] -= 1
+    assert np.allclose(z.cpu().numpy(), zz, rtol=1e-5, atol=1e-5)
+    assert np.allclose(gb.cpu().numpy(), g, rtol=1e-4, atol=1e-6)
+    assert np.allclose(gw.cpu().numpy().reshape(levels, c), np.outer(g, f), rtol=1e-4, atol=1e-6)
+    assert abs(loss.item() + np.log(p[17])) < 1e-4
