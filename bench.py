@@ -361,6 +361,22 @@ class HostStep:
         return select_full(self.table.numpy().view(np.uint64), 0)
 
 
+def max_over_ranks(values, dist, device):
+    """Every rank's timing scalars replaced by their maximum over the ranks
+    (the slowest rank sets the job's time)."""
+    import torch
+
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def whole_job_rate(units_per_rank_step, steps, world, ms):
+    """Units per second of the whole job: every rank's units over the
+    slowest rank's time (replicas: each rank processes its own frames)."""
+    return units_per_rank_step * steps * world / (ms / 1000.0)
+
+
 class PipelineStep:
     """The step as a user of the library runs it on a frame stream: the
     step's inputs — the 7 lookahead frames, the P frame and the MB-padded
@@ -479,14 +495,12 @@ def gpu_arm(args):
         e_times.append(s.elapsed_time(e))
     e_ms = float(np.sum(e_times))
     if world > 1:
-        t = torch.tensor([ms, e_ms, e_ms_call], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e_ms, e_ms_call = float(t[0]), float(t[1]), float(t[2])
+        ms, e_ms, e_ms_call = max_over_ranks([ms, e_ms, e_ms_call], dist, dev)
     result = None
     if rank == 0:
-        value = N_MB * args.steps * world / (ms / 1000.0)
-        e2e = N_MB * args.steps * world / (e_ms / 1000.0)
-        e2e_call = N_MB * args.steps * world / (e_ms_call / 1000.0)
+        value = whole_job_rate(N_MB, args.steps, world, ms)
+        e2e = whole_job_rate(N_MB, args.steps, world, e_ms)
+        e2e_call = whole_job_rate(N_MB, args.steps, world, e_ms_call)
         peak, peak_kind = peaks()
         dom = max((k for k in stage if k not in EXTRA_STAGES), key=lambda k: stage[k]["ms"])
         d = stage[dom]
