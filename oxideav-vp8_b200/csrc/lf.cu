@@ -1426,6 +1426,11 @@ vp8a_status vp8a_filter_sweeps(vp8a_ctx* ctx, const vp8a_sweep_job* jobs, uint32
     max_ring = r;
     pre = p;
   }
+  // Largest pictures first: their CTAs run longest, so they start first
+  // and the short ones fill in behind them.
+  std::stable_sort(group.begin(), group.end(), [&](uint32_t x, uint32_t y) {
+    return (long)args[x].mb_cols * args[x].mb_rows > (long)args[y].mb_cols * args[y].mb_rows;
+  });
   if (!group.empty()) {
     // The layout for the largest job's rings and the group's candidates
     // (each CTA takes `nc` candidates of one job).
