@@ -122,23 +122,31 @@ __global__ void __launch_bounds__(256) lp_conv_fwd_smem_kernel(const uint16_t* X
   for (int q = tid; q < cout * 9 * CIN; q += blockDim.x) w_s[(q / (9 * CIN)) * WS + q % (9 * CIN)] = W[q];
   __syncthreads();
   const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
-  for (int tile = warp; tile < LP_P / 16; tile += 8) {
-    const int y = tile >> 1, xb = (tile & 1) * 16;
-    float d[NT][4];
+  // Warp w takes tiles w, w + 8, ..., four at a time, so each weight
+  // fragment loaded from shared memory feeds four MMAs.
+  constexpr int TG = 4;
+  for (int t0 = warp; t0 < LP_P / 16; t0 += 8 * TG) {
+    float d[TG][NT][4];
 #pragma unroll
-    for (int j = 0; j < NT; j++) d[j][0] = d[j][1] = d[j][2] = d[j][3] = 0.f;
+    for (int u = 0; u < TG; u++)
+#pragma unroll
+      for (int j = 0; j < NT; j++) d[u][j][0] = d[u][j][1] = d[u][j][2] = d[u][j][3] = 0.f;
 #pragma unroll
     for (int tap = 0; tap < 9; tap++) {
       const int dy = tap / 3 - 1, dx = tap % 3 - 1;
-      const uint16_t* r0 = img_s + ((y + dy + 1) * 34 + (xb + g + dx + 1)) * PS;
-      const uint16_t* r1 = r0 + 8 * PS;
 #pragma unroll
       for (int c0 = 0; c0 < CP; c0 += 16) {
-        uint32_t a[4];
-        a[0] = *reinterpret_cast<const uint32_t*>(r0 + c0 + 2 * t);
-        a[1] = *reinterpret_cast<const uint32_t*>(r1 + c0 + 2 * t);
-        a[2] = *reinterpret_cast<const uint32_t*>(r0 + c0 + 2 * t + 8);
-        a[3] = *reinterpret_cast<const uint32_t*>(r1 + c0 + 2 * t + 8);
+        uint32_t a[TG][4];
+#pragma unroll
+        for (int u = 0; u < TG; u++) {
+          const int tile = t0 + 8 * u, y = tile >> 1, xb = (tile & 1) * 16;
+          const uint16_t* r0 = img_s + ((y + dy + 1) * 34 + (xb + g + dx + 1)) * PS;
+          const uint16_t* r1 = r0 + 8 * PS;
+          a[u][0] = *reinterpret_cast<const uint32_t*>(r0 + c0 + 2 * t);
+          a[u][1] = *reinterpret_cast<const uint32_t*>(r1 + c0 + 2 * t);
+          a[u][2] = *reinterpret_cast<const uint32_t*>(r0 + c0 + 2 * t + 8);
+          a[u][3] = *reinterpret_cast<const uint32_t*>(r1 + c0 + 2 * t + 8);
+        }
 #pragma unroll
         for (int j = 0; j < NT; j++) {
           const uint16_t* wr = w_s + (j * 8 + g) * WS + tap * CIN + c0 + 2 * t;
@@ -150,30 +158,36 @@ __global__ void __launch_bounds__(256) lp_conv_fwd_smem_kernel(const uint16_t* X
             b[0] = (c0 + 2 * t < CIN) ? *reinterpret_cast<const uint32_t*>(wr) : 0u;
             b[1] = 0u;
           }
-          mma_bf16(d[j], a, b);
+#pragma unroll
+          for (int u = 0; u < TG; u++) mma_bf16(d[u][j], a[u], b);
         }
       }
     }
 #pragma unroll
-    for (int j = 0; j < NT; j++)
+    for (int u = 0; u < TG; u++) {
+      const int tile = t0 + 8 * u, y = tile >> 1, xb = (tile & 1) * 16;
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const int p = y * LP_S + xb + g + 8 * h, n = j * 8 + 2 * t;
-        const size_t o = ((size_t)img * LP_P + p) * cout + n;
-        float v0 = d[j][2 * h] + (n < cout ? bias[n] : 0.f), v1 = d[j][2 * h + 1] + (n + 1 < cout ? bias[n + 1] : 0.f);
-        if (relu) {
-          v0 = fmaxf(v0, 0.f);
-          v1 = fmaxf(v1, 0.f);
+      for (int j = 0; j < NT; j++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int p = y * LP_S + xb + g + 8 * h, n = j * 8 + 2 * t;
+          const size_t o = ((size_t)img * LP_P + p) * cout + n;
+          float v0 = d[u][j][2 * h] + (n < cout ? bias[n] : 0.f);
+          float v1 = d[u][j][2 * h + 1] + (n + 1 < cout ? bias[n + 1] : 0.f);
+          if (relu) {
+            v0 = fmaxf(v0, 0.f);
+            v1 = fmaxf(v1, 0.f);
+          }
+          if (Yf) {
+            if (n < cout) Yf[o] = v0;
+            if (n + 1 < cout) Yf[o + 1] = v1;
+          } else if (n + 1 < cout) {
+            *reinterpret_cast<uint32_t*>(Y + o) = pack_bf16(v0, v1);
+          } else if (n < cout) {
+            Y[o] = __bfloat16_as_ushort(__float2bfloat16_rn(v0));
+          }
         }
-        if (Yf) {
-          if (n < cout) Yf[o] = v0;
-          if (n + 1 < cout) Yf[o + 1] = v1;
-        } else if (n + 1 < cout) {
-          *reinterpret_cast<uint32_t*>(Y + o) = pack_bf16(v0, v1);
-        } else if (n < cout) {
-          Y[o] = __bfloat16_as_ushort(__float2bfloat16_rn(v0));
-        }
-      }
+    }
   }
 }
 
