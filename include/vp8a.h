@@ -55,7 +55,17 @@ typedef enum vp8a_status {
    * advanced); the context stays usable. */
   VP8A_E_DEVICE_TIMEOUT = 8,
   VP8A_E_OUT_OF_MEMORY = 9,
-  VP8A_E_NO_DEVICE = 10
+  VP8A_E_NO_DEVICE = 10,
+  /* EncodeError::InvalidDctPartitionCount (not 1, 2, 4 or 8). */
+  VP8A_E_INVALID_DCT_PARTITION_COUNT = 11,
+  /* EncodeError::FirstPartitionTooLarge (> 0x7FFFF bytes). */
+  VP8A_E_FIRST_PARTITION_TOO_LARGE = 12,
+  /* EncodeError::Token(CoefficientOutOfRange): |coefficient| > 2114. */
+  VP8A_E_COEFFICIENT_OUT_OF_RANGE = 13,
+  /* EncodeError::InvalidCopyBufferSelector. */
+  VP8A_E_INVALID_COPY_BUFFER_SELECTOR = 14,
+  /* EncodeError::LoopFilterDeltaOutOfRange (|delta| > 63). */
+  VP8A_E_LOOP_FILTER_DELTA_OUT_OF_RANGE = 15
 } vp8a_status;
 
 /* ------------------------------------------------------------------ types */
@@ -658,6 +668,68 @@ vp8a_status vp8a_lp_lf_head(vp8a_ctx* ctx, const float* sums, float count, uint3
  * writes their BF16 copies. */
 vp8a_status vp8a_lp_adam(vp8a_ctx* ctx, float* w, const float* grad, float* m, float* v, uint32_t n,
                          float lr, float beta1, float beta2, float eps, uint32_t step, uint16_t* w_bf16);
+
+/* ------------------------------------------- P-frame bitstream (§19.2) */
+
+/* The frame-level choices an inter frame's header carries: KeyframeParams
+ * (y_ac_qi, filter_type, levels, nbr_of_dct_partitions), RefreshControls
+ * (src/encoder.rs:9174), LoopFilterDeltas (:771) and the segmentation layer
+ * (InterSegmentationConfig) of encode_p_frame_multi_ref_inner_driven
+ * (src/encoder.rs:10739). */
+typedef struct vp8a_frame_header {
+  uint32_t width;                   /* visible size, 1..0x3FFF */
+  uint32_t height;
+  vp8a_quant_indices quant;         /* y_ac_qi; a delta of 0 is not sent */
+  uint8_t filter_type;              /* 0 = normal (§15.3), 1 = simple (§15.2) */
+  uint8_t loop_filter_level;        /* 0..63 */
+  uint8_t sharpness_level;          /* 0..7 */
+  uint8_t n_partitions;             /* token partitions: 1, 2, 4 or 8 */
+  uint8_t refresh_golden_frame;
+  uint8_t refresh_alternate_frame;
+  uint8_t copy_buffer_to_golden;    /* 0..2, sent when !refresh_golden_frame */
+  uint8_t copy_buffer_to_alternate; /* 0..2, sent when !refresh_alternate_frame */
+  uint8_t refresh_last;
+  uint8_t pick_intra;               /* 1: prob_intra fitted to the MB counts (the
+                                       auto-LF entry point); 0: prob_intra 255 */
+  uint8_t fit_skip_prob;            /* 1: prob_skip_false fitted to the skips (the
+                                       reduced search); 0: 128 (exhaustive) */
+  uint8_t lf_delta_enabled;         /* loop_filter_adj_enable */
+  uint8_t lf_delta_update;          /* mode_ref_lf_delta_update */
+  uint8_t lf_ref_delta_present;     /* bit k: ref_frame_delta[k] is sent */
+  uint8_t lf_mode_delta_present;    /* bit k: mode_delta[k] is sent */
+  int8_t lf_ref_delta[4];           /* INTRA, LAST, GOLDEN, ALTREF; |v| <= 63 */
+  int8_t lf_mode_delta[4];          /* B_PRED, ZEROMV, other MV, SPLITMV */
+  uint8_t segmentation;             /* 1: update_segmentation with the MB map */
+  uint8_t segment_lf_present;       /* 1: the per-segment filter deltas are sent */
+  int8_t segment_quant[4];          /* §10 quantiser deltas per segment */
+  int8_t segment_lf[4];             /* §10 filter-level deltas per segment */
+  uint8_t reserved[2];
+} vp8a_frame_header;
+
+/* The inter-frame bitstream encode_p_frame_multi_ref_inner_driven writes
+ * (src/encoder.rs:11214-11720): the §9.1 frame tag, the first partition
+ * (§19.2 header; per MB the segment id, mb_skip_coeff, is_inter_mb, the
+ * §16.2 ref_frame and mv_ref_tree walk against the §16.3 census
+ * probabilities, NEWMV and NEW4X4 §17.2 differentials against the default
+ * MV contexts, SPLITMV partition and sub_mv_ref modes) and the §13 token
+ * partitions (MB row r in partition r % n, encode_coeff_block_into
+ * src/encoder.rs:1915, skipped MBs clear their contexts,
+ * clear_skip_ctx :7369). `decisions` are the analysis's (inter MBs only),
+ * `coeffs` the quantised coefficients of vp8a_reconstruct_inter_frame (400
+ * per MB, MbCoeffs order), `mb_segment` one id per MB when the header
+ * enables segmentation (-1 = segment 0), `token_prob_updates` NULL or 1056
+ * entries in [4][8][3][11] order (0 = keep the §13.5 default, else the new
+ * probability, sent as a §13.4 update and coded against). mb_skip_coeff is
+ * derived from the coefficients as the reference does (src/encoder.rs:8746).
+ * Writes the frame to `out` and its size to `out_size`; when `out` is NULL
+ * or `out_capacity` is short, returns VP8A_E_INVALID_ARGUMENT with
+ * `out_size` set to the size needed. Host memory only; runs on the host
+ * (the boolean coder is a serial chain) with one thread per token
+ * partition, and needs no context. */
+vp8a_status vp8a_write_inter_frame(const vp8a_frame_header* header,
+                                   const vp8a_mb_decision* decisions, const int16_t* coeffs,
+                                   const int8_t* mb_segment, const uint8_t* token_prob_updates,
+                                   uint8_t* out, uint64_t out_capacity, uint64_t* out_size);
 
 #ifdef __cplusplus
 }

@@ -73,6 +73,7 @@ size_t vo_type_size(int which) {
     case 15: return sizeof(vp8a_arnr_job);
     case 16: return sizeof(vp8a_recon_job);
     case 17: return sizeof(vp8a_sweep_job);
+    case 18: return sizeof(vp8a_frame_header);
     default: return 0;
   }
 }

@@ -186,6 +186,36 @@ void vo_vp8_decoder_free(vo_vp8_decoder* d) {
   free(d);
 }
 
+static int alloc_slots(vo_vp8_decoder* d);
+
+/* Test hook: install `refs` (LAST, GOLDEN, ALTREF x (y, u, v), MB-padded
+ * planes of a width x height picture) as the three reference slots, with
+ * the entropy state a key frame without probability updates leaves
+ * (default coefficient, MV and mode probabilities, no sign bias, no loop
+ * filter deltas). Inter frames written against arbitrary references then
+ * decode as they would after such a key frame. Returns 0, or -1 for a bad
+ * size or an allocation failure. */
+int vo_vp8_decoder_prime(vo_vp8_decoder* d, uint32_t width, uint32_t height, const uint8_t* const* refs) {
+  if (!d || !width || !height || width > 0x3fff || height > 0x3fff) return -1;
+  d->width = width;
+  d->height = height;
+  d->mb_cols = (width + 15) / 16;
+  d->mb_rows = (height + 15) / 16;
+  if (alloc_slots(d)) return -1;
+  const size_t ly = (size_t)d->mb_cols * 16 * d->mb_rows * 16;
+  for (int s = 0; s < 3; s++)
+    for (int p = 0; p < 3; p++) memcpy(d->slot[s][p], refs[3 * s + p], p ? ly / 4 : ly);
+  memcpy(d->coef, VO_DEFAULT_COEF_PROBS, sizeof d->coef);
+  memcpy(d->ymode_prob, IF_YMODE_PROB_DEFAULTS, 4);
+  memcpy(d->uvmode_prob, IF_UV_MODE_PROB_DEFAULTS, 3);
+  memcpy(d->mvc, DEFAULT_MV_CONTEXT, sizeof d->mvc);
+  d->sign_bias_golden = d->sign_bias_altref = 0;
+  memset(d->ref_lf_deltas, 0, sizeof d->ref_lf_deltas);
+  memset(d->mode_lf_deltas, 0, sizeof d->mode_lf_deltas);
+  d->have_key = 1;
+  return 0;
+}
+
 /* ---------------------------------------------------------------- headers */
 
 typedef struct {

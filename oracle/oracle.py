@@ -89,6 +89,7 @@ def load():
         "vo_vp8_decoder_new": (P, []),
         "vo_vp8_decoder_free": (None, [P]),
         "vo_vp8_decoder_capture": (None, [P, P]),
+        "vo_vp8_decoder_prime": (C.c_int, [P, U32, U32, P]),
         "vo_vp8_decode_frame": (C.c_int, [P, P, C.c_size_t, P, C.POINTER(U32), C.POINTER(U32),
                                           C.POINTER(C.c_int)]),
         "vo_segment_factors": (None, [C.POINTER(abi.QuantIndices), C.c_int, C.c_int32, C.c_int, P]),
@@ -131,7 +132,7 @@ def type_sizes():
     names = ["vp8a_mv", "vp8a_search_result", "vp8a_luma_ref", "vp8a_i420", "vp8a_planes", "vp8a_mv_contexts",
              "vp8a_mb_decision", "vp8a_ref_search", "vp8a_mb_lf_info", "vp8a_filter_config", "vp8a_source",
              "vp8a_mb_info", "vp8a_rd_inter", "vp8a_quant_indices", "vp8a_analysis_job", "vp8a_arnr_job",
-             "vp8a_recon_job", "vp8a_sweep_job"]
+             "vp8a_recon_job", "vp8a_sweep_job", "vp8a_frame_header"]
     return {n: int(lib.vo_type_size(i)) for i, n in enumerate(names)}
 
 
@@ -600,39 +601,64 @@ class _Capture(C.Structure):
                 ("filtered", C.c_int32), ("mb_cols", C.c_int32), ("mb_rows", C.c_int32), ("captured", C.c_int32)]
 
 
-def decode_ivf_captured(data):
-    """Decode an IVF stream with the restated decoder, yielding per frame a
-    dict of its intermediate state (MB-padded planes as (y, u, v)): `refs`
-    (LAST, GOLDEN, ALTREF in force), `pred` (inter MBs' prediction, intra
-    MBs 0), `dec` (MB_DECISION_DTYPE; ref_frame INTRA for intra MBs),
-    `pre` / `post` (reconstruction before / after the loop filter), `lf`
+class CapturingDecoder(Vp8Decoder):
+    """A decoder of width x height frames that records each decoded frame's
+    intermediate state (MB-padded planes as (y, u, v)): `refs` (LAST,
+    GOLDEN, ALTREF in force), `pred` (inter MBs' prediction, intra MBs 0),
+    `dec` (MB_DECISION_DTYPE; ref_frame INTRA for intra MBs), `pre` /
+    `post` (reconstruction before / after the loop filter), `lf`
     (MB_LF_INFO_DTYPE), `cfg` (abi.FilterConfig), `key`, `version`,
     `filtered`, and the visible `picture`."""
-    w, h = int.from_bytes(data[12:14], "little"), int.from_bytes(data[14:16], "little")
-    mbc, mbr = (w + 15) // 16, (h + 15) // 16
-    shapes = [(mbr * 16, mbc * 16), (mbr * 8, mbc * 8), (mbr * 8, mbc * 8)]
-    new = lambda: [np.zeros(s, np.uint8) for s in shapes]  # noqa: E731
-    refs, pred, pre, post = [new() for _ in range(3)], new(), new(), new()
-    dec = np.zeros(mbc * mbr, abi.MB_DECISION_DTYPE)
-    lf = np.zeros(mbc * mbr, abi.MB_LF_INFO_DTYPE)
-    cfg = abi.FilterConfig()
-    cap = _Capture()
-    for s in range(3):
+
+    def __init__(self, width, height):
+        super().__init__()
+        self.width, self.height = width, height
+        mbc, mbr = (width + 15) // 16, (height + 15) // 16
+        shapes = [(mbr * 16, mbc * 16), (mbr * 8, mbc * 8), (mbr * 8, mbc * 8)]
+        new = lambda: [np.zeros(s, np.uint8) for s in shapes]  # noqa: E731
+        self.refs, self.pred, self.pre, self.post = [new() for _ in range(3)], new(), new(), new()
+        self.dec = np.zeros(mbc * mbr, abi.MB_DECISION_DTYPE)
+        self.lf = np.zeros(mbc * mbr, abi.MB_LF_INFO_DTYPE)
+        self.cfg = abi.FilterConfig()
+        cap = self.cap = _Capture()
+        for s in range(3):
+            for p in range(3):
+                cap.refs[s][p] = ptr(self.refs[s][p])
         for p in range(3):
-            cap.refs[s][p] = ptr(refs[s][p])
-    for p in range(3):
-        cap.pred[p], cap.pre[p], cap.post[p] = ptr(pred[p]), ptr(pre[p]), ptr(post[p])
-    cap.dec, cap.lf, cap.cfg = ptr(dec), ptr(lf), C.pointer(cfg)
-    cap.mb_cols, cap.mb_rows = mbc, mbr
-    dec_obj = Vp8Decoder()
-    dec_obj.lib.vo_vp8_decoder_capture(dec_obj.h, C.byref(cap))
+            cap.pred[p], cap.pre[p], cap.post[p] = ptr(self.pred[p]), ptr(self.pre[p]), ptr(self.post[p])
+        cap.dec, cap.lf, cap.cfg = ptr(self.dec), ptr(self.lf), C.pointer(self.cfg)
+        cap.mb_cols, cap.mb_rows = mbc, mbr
+        self.lib.vo_vp8_decoder_capture(self.h, C.byref(cap))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.vo_vp8_decoder_capture(self.h, None)
+        super().__del__()
+
+    def prime(self, refs):
+        """Install `refs` (LAST, GOLDEN, ALTREF as MB-padded (y, u, v)) with
+        a key frame's default entropy state (vo_vp8_decoder_prime)."""
+        planes = [np.ascontiguousarray(p, np.uint8) for r in refs for p in r]
+        arr = (P * 9)(*[ptr(p) for p in planes])
+        if self.lib.vo_vp8_decoder_prime(self.h, self.width, self.height, arr) != 0:
+            raise RuntimeError("vo_vp8_decoder_prime failed")
+
+    def decode(self, frame):
+        self.cap.captured = 0
+        picture, shown = self.decode_into(frame)
+        if not self.cap.captured:
+            raise ValueError("frame size differs from the decoder's; capture needs a fixed size")
+        return {"refs": [tuple(p.copy() for p in r) for r in self.refs], "pred": tuple(p.copy() for p in self.pred),
+                "pre": tuple(p.copy() for p in self.pre), "post": tuple(p.copy() for p in self.post),
+                "dec": self.dec.copy(), "lf": self.lf.copy(), "cfg": abi.FilterConfig.from_buffer_copy(self.cfg),
+                "key": bool(self.cap.key), "version": int(self.cap.version), "filtered": bool(self.cap.filtered),
+                "picture": picture, "shown": shown}
+
+
+def decode_ivf_captured(data):
+    """Decode an IVF stream with the restated decoder, yielding per frame
+    the state CapturingDecoder.decode records."""
+    w, h = int.from_bytes(data[12:14], "little"), int.from_bytes(data[14:16], "little")
+    dec = CapturingDecoder(w, h)
     for frame in ivf_frames(data):
-        cap.captured = 0
-        picture, shown = dec_obj.decode_into(frame)
-        if not cap.captured:
-            raise ValueError("frame size differs from the IVF header's; capture needs a fixed size")
-        yield {"refs": [tuple(p.copy() for p in r) for r in refs], "pred": tuple(p.copy() for p in pred),
-               "pre": tuple(p.copy() for p in pre), "post": tuple(p.copy() for p in post), "dec": dec.copy(),
-               "lf": lf.copy(), "cfg": abi.FilterConfig.from_buffer_copy(cfg), "key": bool(cap.key),
-               "version": int(cap.version), "filtered": bool(cap.filtered), "picture": picture, "shown": shown}
-    dec_obj.lib.vo_vp8_decoder_capture(dec_obj.h, None)
+        yield dec.decode(frame)

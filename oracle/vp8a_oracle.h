@@ -191,6 +191,7 @@ typedef struct vo_vp8_capture {
 vo_vp8_decoder* vo_vp8_decoder_new(void);
 void vo_vp8_decoder_free(vo_vp8_decoder* d);
 void vo_vp8_decoder_capture(vo_vp8_decoder* d, vo_vp8_capture* cap);
+int vo_vp8_decoder_prime(vo_vp8_decoder* d, uint32_t width, uint32_t height, const uint8_t* const* refs);
 int vo_vp8_decode_frame(vo_vp8_decoder* d, const uint8_t* data, size_t size, uint8_t* out,
                         uint32_t* width, uint32_t* height, int* shown);
 

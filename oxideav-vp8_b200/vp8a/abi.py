@@ -21,6 +21,11 @@ E_CUDA = 7
 E_DEVICE_TIMEOUT = 8
 E_OUT_OF_MEMORY = 9
 E_NO_DEVICE = 10
+E_INVALID_DCT_PARTITION_COUNT = 11
+E_FIRST_PARTITION_TOO_LARGE = 12
+E_COEFFICIENT_OUT_OF_RANGE = 13
+E_INVALID_COPY_BUFFER_SELECTOR = 14
+E_LOOP_FILTER_DELTA_OUT_OF_RANGE = 15
 
 STATUS_NAMES = {
     0: "OK",
@@ -34,6 +39,11 @@ STATUS_NAMES = {
     8: "DeviceTimeout",
     9: "OutOfMemory",
     10: "NoDevice",
+    11: "InvalidDctPartitionCount",
+    12: "FirstPartitionTooLarge",
+    13: "CoefficientOutOfRange",
+    14: "InvalidCopyBufferSelector",
+    15: "LoopFilterDeltaOutOfRange",
 }
 
 REF_INTRA, REF_LAST, REF_GOLDEN, REF_ALTREF = 0, 1, 2, 3
@@ -117,6 +127,58 @@ def quant_indices(y_ac_qi, y_dc=0, y2_dc=0, y2_ac=0, uv_dc=0, uv_ac=0):
 
 
 MB_SKIP, MB_HAS_COEFFS = 1, 2
+
+
+class FrameHeader(C.Structure):
+    """vp8a_frame_header: the frame-level choices of an inter frame's
+    header (KeyframeParams, RefreshControls src/encoder.rs:9174,
+    LoopFilterDeltas :771, the segmentation layer)."""
+
+    _fields_ = [
+        ("width", C.c_uint32),
+        ("height", C.c_uint32),
+        ("quant", QuantIndices),
+        ("filter_type", C.c_uint8),
+        ("loop_filter_level", C.c_uint8),
+        ("sharpness_level", C.c_uint8),
+        ("n_partitions", C.c_uint8),
+        ("refresh_golden_frame", C.c_uint8),
+        ("refresh_alternate_frame", C.c_uint8),
+        ("copy_buffer_to_golden", C.c_uint8),
+        ("copy_buffer_to_alternate", C.c_uint8),
+        ("refresh_last", C.c_uint8),
+        ("pick_intra", C.c_uint8),
+        ("fit_skip_prob", C.c_uint8),
+        ("lf_delta_enabled", C.c_uint8),
+        ("lf_delta_update", C.c_uint8),
+        ("lf_ref_delta_present", C.c_uint8),
+        ("lf_mode_delta_present", C.c_uint8),
+        ("lf_ref_delta", C.c_int8 * 4),
+        ("lf_mode_delta", C.c_int8 * 4),
+        ("segmentation", C.c_uint8),
+        ("segment_lf_present", C.c_uint8),
+        ("segment_quant", C.c_int8 * 4),
+        ("segment_lf", C.c_int8 * 4),
+        ("reserved", C.c_uint8 * 2),
+    ]
+
+
+def frame_header(width, height, quant, n_partitions=1, refresh_last=True, pick_intra=True, **kw):
+    """A vp8a_frame_header with the defaults of the auto-LF P-frame entry
+    point (encode_p_frame_multi_ref_auto_loop_filter, src/encoder.rs:9373:
+    RefreshControls::default, no deltas, intra picking on) and keyword
+    overrides; list-valued fields take sequences."""
+    h = FrameHeader()
+    h.width, h.height, h.quant = width, height, quant
+    h.n_partitions, h.refresh_last, h.pick_intra = n_partitions, int(refresh_last), int(pick_intra)
+    for k, v in kw.items():
+        if isinstance(v, (list, tuple)):
+            arr = getattr(h, k)
+            for i, x in enumerate(v):
+                arr[i] = x
+        else:
+            setattr(h, k, int(v))
+    return h
 
 
 class Source(C.Structure):
@@ -256,6 +318,7 @@ C_SIZES = {
     "vp8a_arnr_job": 48,
     "vp8a_recon_job": 184,
     "vp8a_sweep_job": 152,
+    "vp8a_frame_header": 52,
 }
 
 
@@ -280,6 +343,7 @@ def check_layouts():
         "vp8a_arnr_job": C.sizeof(ArnrJob),
         "vp8a_recon_job": C.sizeof(ReconJob),
         "vp8a_sweep_job": C.sizeof(SweepJob),
+        "vp8a_frame_header": C.sizeof(FrameHeader),
     }
     assert got == C_SIZES, (got, C_SIZES)
     return got

@@ -253,6 +253,69 @@ def dequant_factors(quant, segment_quant=None, absolute=False):
     return tuple(int(x) for x in out)
 
 
+def write_inter_frame(header, decisions, coeffs, mb_segment=None, token_prob_updates=None):
+    """The inter-frame bitstream of encode_p_frame_multi_ref_inner_driven
+    (src/encoder.rs:11214-11720) as bytes: `header` an abi.FrameHeader,
+    `decisions` the analysis's MB_DECISION_DTYPE records (raster order),
+    `coeffs` (n_mbs, 400) int16 quantised coefficients as
+    reconstruct_inter_frame returns them, `mb_segment` one int8 per MB when
+    the header enables segmentation, `token_prob_updates` None or 1056
+    probabilities in [4][8][3][11] order (0 = keep the default). Host
+    memory; no context needed."""
+    lib = load()
+    dec = np.ascontiguousarray(decisions).reshape(-1)
+    cf = np.ascontiguousarray(coeffs, np.int16)
+    if cf.size != dec.size * 400:
+        raise ValueError("coeffs must hold 400 int16 per MB")
+    seg = None if mb_segment is None else np.ascontiguousarray(np.asarray(mb_segment, np.int8).reshape(-1))
+    upd = None
+    if token_prob_updates is not None:
+        upd = np.ascontiguousarray(np.asarray(token_prob_updates, np.uint8).reshape(-1))
+        if upd.size != 1056:
+            raise ValueError("token_prob_updates must hold 1056 entries")
+    size = C.c_uint64(0)
+    cap = 1024 + 600 * dec.size
+    while True:
+        out = np.zeros(cap, np.uint8)
+        st = lib.vp8a_write_inter_frame(C.byref(header), ptr(dec), ptr(cf), ptr(seg), ptr(upd), ptr(out), cap,
+                                        C.byref(size))
+        if st == abi.E_INVALID_ARGUMENT and size.value > cap:
+            cap = size.value
+            continue
+        check(st, "vp8a_write_inter_frame")
+        return out[:size.value].tobytes()
+
+
+def encode_p_frame(ctx, frame, refs, ref_ids, y_ac_qi, loop_filter_level=0, sharpness_level=0, simple=False,
+                   n_partitions=1, auto_lf=True, refresh_last=True):
+    """encode_p_frame_multi_ref_auto_loop_filter (src/encoder.rs:9373) with
+    intra picking off and the trellis off: the exhaustive analysis, the §14
+    reconstruction of the chosen modes, the §9.4 (level, sharpness) search
+    (select_filter_params, when `auto_lf`), the §15 filter pass and the
+    bitstream. `frame` = visible (y, u, v); `refs` = MB-padded (y, u, v)
+    with ids `ref_ids` (VP8A_REF_*). Returns (frame bytes, the filtered
+    reconstruction as MB-padded (y, u, v), details dict with the decisions,
+    coefficients, flags, the loop-filter records and the chosen level and
+    sharpness)."""
+    dec = analyse_inter_frame(ctx, frame, refs, ref_ids, rd_lambda(y_ac_qi)).reshape(-1)
+    quant = abi.quant_indices(y_ac_qi)
+    recon = tuple(np.zeros_like(p) for p in refs[0])
+    lf = np.zeros(dec.size, abi.MB_LF_INFO_DTYPE)
+    cf, fl = reconstruct_inter_frame(ctx, frame, refs, ref_ids, dec, quant, recon, lf_info=lf)
+    level, sharp = loop_filter_level, sharpness_level
+    if auto_lf:
+        base = abi.filter_config(level=0, sharpness=sharpness_level, simple=simple)
+        level, sharp = select_filter_params(ctx, recon, lf, base, frame)
+    cfg = abi.filter_config(level=level, sharpness=sharp, simple=simple)
+    out = filter_frame(ctx, recon, lf, cfg) if level else recon
+    hdr = abi.frame_header(frame[0].shape[1], frame[0].shape[0], quant, n_partitions=n_partitions,
+                           refresh_last=refresh_last, filter_type=int(simple), loop_filter_level=level,
+                           sharpness_level=sharp)
+    bits = write_inter_frame(hdr, dec, cf)
+    return bits, out, dict(decisions=dec, coeffs=cf, flags=fl, lf_info=lf, recon=recon, level=level,
+                           sharpness=sharp)
+
+
 def reconstruct_inter_frame(ctx, frame, refs, ref_ids, decisions, quant, recon, mb_segment=None,
                             segment_quant=None, segment_abs=False, full_pixel=False, filter_set=abi.FILTER_SIXTAP,
                             coeffs=True, flags=True, lf_info=None):

@@ -2,7 +2,7 @@
 
     python oxideav-vp8_b200/vp8a/build.py [--force]
 
-Compiles every csrc/*.cu with nvcc into vp8a/libvp8a.so. The library is built
+Compiles every csrc/*.cu (and the host-only csrc/*.cpp) with nvcc into vp8a/libvp8a.so. The library is built
 with -fmad=false: the RD costs of the inter analysis are f64 expressions that
 must round exactly like the reference's unfused arithmetic.
 """
@@ -31,11 +31,12 @@ NVCC_FLAGS = [
 
 
 def sources():
-    return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
 
 
 def deps():
-    return sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h"))
+    return (sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) +
+            glob.glob(os.path.join(INCLUDE, "*.h")))
 
 
 def up_to_date():

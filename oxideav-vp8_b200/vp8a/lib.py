@@ -53,6 +53,8 @@ PROTOTYPES = {
     "vp8a_predict_split_mv": (C.c_int, [P, C.POINTER(abi.Planes), P, P, U32, U32, U32, P]),
     "vp8a_predict_inter_frame": (C.c_int, [P, P, P, U32, P, U32, U32, C.POINTER(abi.Planes)]),
     "vp8a_dequant_factors": (None, [C.POINTER(abi.QuantIndices), U32, C.c_int32, U32, P]),
+    "vp8a_write_inter_frame": (C.c_int, [C.POINTER(abi.FrameHeader), P, P, P, P, P, C.c_uint64,
+                                         C.POINTER(C.c_uint64)]),
     "vp8a_reconstruct_inter_frame": (
         C.c_int,
         [P, C.POINTER(abi.I420), P, P, U32, P, C.POINTER(abi.QuantIndices), P, P, U32, U32, U32,
