@@ -42,14 +42,11 @@ struct BoolWriter {
   }
   void put(int prob, bool bit) {
     const uint32_t split = 1 + (((range - 1) * (uint32_t)prob) >> 8);
-    if (bit) {
-      bottom += split;
-      range -= split;
-    } else {
-      range = split;
-    }
+    // Branch-free choice of the sub-interval: the bit is data, not control.
+    const uint32_t m = 0u - (uint32_t)bit;
+    bottom += split & m;
+    range = split + ((range - 2 * split) & m);
     const int shift = __builtin_clz(range) - 24;  // range in [1, 255]
-    if (shift == 0) return;
     range <<= shift;
     if (shift < pending) {
       bottom <<= shift;
@@ -321,10 +318,13 @@ int mb_blocks(const int16_t* mb, bool has_y2, BlockRef* out) {
   return n;
 }
 
+// Whether the block has a nonzero coefficient it codes (raster and scan
+// order hold the same set past the DC): four 64-bit ORs.
 bool block_nonzero(const BlockRef& b) {
-  for (int i = b.first; i < 16; i++)
-    if (b.c[i] != 0) return true;  // raster and scan hold the same set past DC
-  return false;
+  uint64_t w[4];
+  std::memcpy(w, b.c, sizeof w);
+  if (b.first) w[0] &= ~(uint64_t)0xFFFF;
+  return (w[0] | w[1] | w[2] | w[3]) != 0;
 }
 
 }  // namespace
@@ -376,6 +376,7 @@ extern "C" vp8a_status vp8a_write_inter_frame(const vp8a_frame_header* h, const 
   // Per MB: the wire segment, skip flag (no nonzero block among those the
   // MB codes, src/encoder.rs:8746-8769) and the per-block nonzero flags.
   std::vector<uint8_t> skip(n_mbs), seg(n_mbs, 0);
+  std::vector<uint32_t> nzmask(n_mbs);  // bit b: coding-order block b has a coded nonzero
   uint32_t n_skip = 0, n_ref[4] = {0, 0, 0, 0}, seg_count[4] = {0, 0, 0, 0};
   for (size_t i = 0; i < n_mbs; i++) {
     const vp8a_mb_decision& d = decisions[i];
@@ -384,13 +385,15 @@ extern "C" vp8a_status vp8a_write_inter_frame(const vp8a_frame_header* h, const 
     if (d.mode == VP8A_MODE_SPLIT && d.partition > VP8A_PART_MV16) return VP8A_E_INVALID_ARGUMENT;
     BlockRef blk[25];
     const int nb = mb_blocks(coeffs + 400 * i, d.mode != VP8A_MODE_SPLIT, blk);
-    bool any = false;
+    uint32_t mask = 0;
     for (int b = 0; b < nb; b++) {
+      if (!block_nonzero(blk[b])) continue;
+      mask |= 1u << b;
       for (int k = blk[b].first; k < 16; k++)
         if (std::abs((int)blk[b].c[k]) > 2114) return VP8A_E_COEFFICIENT_OUT_OF_RANGE;
-      any = any || block_nonzero(blk[b]);
     }
-    skip[i] = !any;
+    nzmask[i] = mask;
+    skip[i] = mask == 0;
     n_skip += skip[i];
     n_ref[d.ref_frame]++;
     if (h->segmentation) {
@@ -573,7 +576,7 @@ extern "C" vp8a_status vp8a_write_inter_frame(const vp8a_frame_header* h, const 
         for (int b = 0; b < nb; b++) {
           ctx_in[(i * 25 + b) * 2] = a[blk[b].slot_above];
           ctx_in[(i * 25 + b) * 2 + 1] = left_nz[blk[b].slot_left];
-          const uint8_t nz = block_nonzero(blk[b]);
+          const uint8_t nz = (nzmask[i] >> b) & 1;
           a[blk[b].slot_above] = nz;
           left_nz[blk[b].slot_left] = nz;
         }
@@ -589,9 +592,13 @@ extern "C" vp8a_status vp8a_write_inter_frame(const vp8a_frame_header* h, const 
         if (skip[i]) continue;
         BlockRef blk[25];
         const int nb = mb_blocks(coeffs + 400 * i, decisions[i].mode != VP8A_MODE_SPLIT, blk);
-        for (int b = 0; b < nb; b++)
-          code_block(w, probs, blk[b].plane, blk[b].first,
-                     ctx_in[(i * 25 + b) * 2] + ctx_in[(i * 25 + b) * 2 + 1], blk[b].c);
+        for (int b = 0; b < nb; b++) {
+          const int ctx = ctx_in[(i * 25 + b) * 2] + ctx_in[(i * 25 + b) * 2 + 1];
+          if ((nzmask[i] >> b) & 1)
+            code_block(w, probs, blk[b].plane, blk[b].first, ctx, blk[b].c);
+          else  // an empty block is its EOB alone
+            w.put(probs[blk[b].plane][kBands[blk[b].first]][ctx][0], false);
+        }
       }
     parts[p] = w.finish();
   };
