@@ -254,6 +254,8 @@ vp8a_status vp8a_ctx_create(int device, vp8a_ctx** out);
 vp8a_status vp8a_ctx_destroy(vp8a_ctx* ctx);
 /* The context's cudaStream_t, as an opaque pointer. */
 void* vp8a_ctx_stream(vp8a_ctx* ctx);
+/* Wait for the context stream; returns VP8A_E_DEVICE_TIMEOUT when a bounded
+ * device wait of an asynchronous call ran out since the last check. */
 vp8a_status vp8a_ctx_synchronize(vp8a_ctx* ctx);
 /* Kernel launches issued by this context since creation. */
 uint64_t vp8a_ctx_launch_count(const vp8a_ctx* ctx);

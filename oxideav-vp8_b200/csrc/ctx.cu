@@ -250,8 +250,9 @@ void* vp8a_ctx_stream(vp8a_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr
 
 vp8a_status vp8a_ctx_synchronize(vp8a_ctx* ctx) {
   if (!ctx) return VP8A_E_INVALID_ARGUMENT;
-  VP8A_CUDA(cudaStreamSynchronize(ctx->stream));
-  return VP8A_OK;
+  // Waits for the stream and reports a bounded device wait that ran out in
+  // an asynchronous call since the last check.
+  return check_device_status(ctx);
 }
 
 uint64_t vp8a_ctx_launch_count(const vp8a_ctx* ctx) { return ctx ? ctx->launches : 0; }

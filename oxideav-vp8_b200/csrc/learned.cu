@@ -400,6 +400,171 @@ __global__ void lp_lf_head_kernel(const float* sums, float count, int C, const f
   if (t == label && loss) *loss += -(zi - m - __logf(s));
 }
 
+// ------------------------------------------- tcgen05 forward, 32 -> 32
+// The 32 -> 32 layers on the 5th-generation tensor cores: one CTA per
+// image, the 3x3 convolution as an implicit GEMM D[pixel][n] = sum over
+// (tap, ci) of A[pixel + tap offset][ci] * W[n][tap][ci]. The image sits in
+// shared memory with a zero halo on a 34-pixel row pitch, channel-group
+// major (group g of 8 channels: 16 bytes per halo pixel), so that 8
+// consecutive "virtual" output pixels v = y * 34 + x form one 8 x 16-byte
+// core matrix of the K-major, unswizzled canonical layout and a tap
+// (dy, dx) is only a base-address shift of (dy + 1) * 34 + dx + 1 pixels.
+// The virtual grid computes 2 discarded columns per row (x = 32, 33) and
+// is covered by 9 M = 128 tiles; each tile takes 18 MMAs of K = 16 (9 taps
+// x 2 channel halves) into a 32-column FP32 accumulator in tensor memory.
+// The weights sit as [k-group of 8][n][8] (k = tap * 32 + ci). One thread
+// issues the MMAs of up to four tiles, one commit signals an mbarrier, and
+// the 8 warps read the accumulators back (warp w: lanes 32 (w % 4) .. +31,
+// columns 16 (w / 4) .. +15 of each tile), add the bias, apply the ReLU and
+// store BF16.
+namespace lptc {
+constexpr int NV = 1224;                    // halo pixels per channel group (>= 1151 + 70 + 1)
+constexpr int REGION = NV * 16;             // bytes per channel group
+constexpr int IMG_BYTES = 4 * REGION;
+constexpr int W_BYTES = 36 * 32 * 16;       // 36 k-groups x 32 n x 16 bytes
+constexpr int SMEM = IMG_BYTES + W_BYTES + 16;
+constexpr int TILES = 9;                    // ceil(32 * 34 / 128)
+constexpr uint32_t TMEM_COLS = 128;         // four 32-column accumulators
+// Instruction descriptor (kind::f16): D FP32, A and B BF16, both K-major,
+// N = 32, M = 128.
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr int WAIT_LIMIT = 1 << 22;
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  // Unswizzled K-major shared-memory matrix descriptor: start address,
+  // leading (K) and stride (M/N) byte offsets in 16-byte units, version 1.
+  return (uint64_t)((addr & 0x3FFFF) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+}  // namespace lptc
+
+__global__ void __launch_bounds__(256, 2) lp_conv_fwd_tc_kernel(const uint16_t* X, const uint16_t* W,
+                                                                 const float* bias, int relu, uint16_t* Y,
+                                                                 uint32_t* status) {
+  using namespace lptc;
+  extern __shared__ __align__(128) uint8_t smt[];
+  uint8_t* img_s = smt;
+  uint8_t* w_s = smt + IMG_BYTES;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smt + IMG_BYTES + W_BYTES);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smt + IMG_BYTES + W_BYTES + 8);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const size_t im = blockIdx.x;
+  const uint32_t img_a = (uint32_t)__cvta_generic_to_shared(img_s);
+  const uint32_t w_a = (uint32_t)__cvta_generic_to_shared(w_s);
+  const uint32_t bar_a = (uint32_t)__cvta_generic_to_shared(mbar);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(tmem_slot)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_a), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  // Zero image (halo and tail), then the 1024 pixels and the weights.
+  for (int q = tid; q < IMG_BYTES / 16; q += 256) reinterpret_cast<uint4*>(img_s)[q] = make_uint4(0, 0, 0, 0);
+  __syncthreads();
+  const uint4* Xi = reinterpret_cast<const uint4*>(X + im * LP_P * 32);
+  for (int q = tid; q < LP_P * 4; q += 256) {
+    const int p = q >> 2, g = q & 3;
+    const int h = ((p >> 5) + 1) * 34 + (p & 31) + 1;
+    *reinterpret_cast<uint4*>(img_s + g * REGION + h * 16) = Xi[q];
+  }
+  for (int q = tid; q < 32 * 36; q += 256) {
+    const int n = q / 36, kg = q % 36;
+    *reinterpret_cast<uint4*>(w_s + (kg * 32 + n) * 16) = *reinterpret_cast<const uint4*>(W + n * 288 + kg * 8);
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  uint32_t phase = 0;
+  bool failed = false;
+  for (int t0 = 0; t0 < TILES && !failed; t0 += 4) {
+    const int nt = TILES - t0 < 4 ? TILES - t0 : 4;
+    if (tid == 0) {
+      for (int u = 0; u < nt; u++) {
+        const int v0 = (t0 + u) * 128;
+        const uint32_t d = tmem + (uint32_t)(u * 32);
+        for (int ks = 0; ks < 18; ks++) {
+          const int tap = ks >> 1, hh = ks & 1;
+          const int off = (tap / 3) * 34 + tap % 3;
+          const uint64_t ad = smem_desc(img_a + (uint32_t)(2 * hh * REGION + (v0 + off) * 16), REGION, 128);
+          const uint64_t bd = smem_desc(w_a + (uint32_t)((tap * 4 + 2 * hh) * 32 * 16), 512, 128);
+          const uint32_t acc = ks > 0 ? 1u : 0u;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\t"
+              "setp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+              "l"(ad), "l"(bd), "r"(IDESC), "r"(acc));
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_a)
+                   : "memory");
+    }
+    // Bounded wait for the commit; a timeout is reported, not waited out.
+    uint32_t done = 0;
+    for (int it = 0; it < WAIT_LIMIT && !done; it++) {
+      asm volatile(
+          "{\n\t.reg .pred P1;\n\t"
+          "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+          "selp.b32 %0, 1, 0, P1;\n\t}\n"
+          : "=r"(done)
+          : "r"(bar_a), "r"(phase)
+          : "memory");
+    }
+    phase ^= 1u;
+    failed = __syncthreads_or(!done);
+    if (failed) {
+      if (tid == 0) atomicExch(status, 1u);  // DEV_TIMEOUT
+      break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int lq = warp & 3, half = warp >> 2;
+    for (int u = 0; u < nt; u++) {
+      uint32_t r[16];
+      const uint32_t ta = tmem + ((uint32_t)(32 * lq) << 16) + (uint32_t)(u * 32 + half * 16);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+          "%14, %15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(ta));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      const int v = (t0 + u) * 128 + 32 * lq + lane, y = v / 34, x = v % 34;
+      if (y < 32 && x < 32) {
+        uint32_t o[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          const int n = half * 16 + 2 * j;
+          float a = __uint_as_float(r[2 * j]) + __ldg(bias + n);
+          float b = __uint_as_float(r[2 * j + 1]) + __ldg(bias + n + 1);
+          if (relu) {
+            a = fmaxf(a, 0.f);
+            b = fmaxf(b, 0.f);
+          }
+          o[j] = pack_bf16(a, b);
+        }
+        uint4* dst = reinterpret_cast<uint4*>(Y + (im * LP_P + y * 32 + x) * 32 + half * 16);
+        dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
+        dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+  }
+}
+
 template <int CIN, int NT>
 vp8a_status conv_fwd(vp8a_ctx* ctx, const uint16_t* X, const uint16_t* W, const float* b, int cout, int n, int relu,
                      uint16_t* Y, float* Yf) {
@@ -466,6 +631,18 @@ vp8a_status vp8a_lp_conv_forward(vp8a_ctx* ctx, const uint16_t* x, uint32_t cin,
   }
   VP8A_CUDA(cudaSetDevice(ctx->device));
   if (cin == 2 && cout == 32) return conv_fwd<2, 4>(ctx, x, w, bias, 32, (int)n, relu, y, y_f32);
+  if (cin == 32 && cout == 32 && y && !y_f32 && n > 0) {
+    // The tensor-core path: 16-byte aligned activations and weights.
+    if (((uintptr_t)x | (uintptr_t)w | (uintptr_t)y) & 15) {
+      vp8a::set_error("tensor-core conv needs 16-byte aligned buffers");
+      return VP8A_E_INVALID_ARGUMENT;
+    }
+    VP8A_CUDA(cudaFuncSetAttribute(lp_conv_fwd_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lptc::SMEM));
+    lp_conv_fwd_tc_kernel<<<n, 256, lptc::SMEM, ctx->stream>>>(x, w, bias, (int)relu, y, ctx->d_status);
+    VP8A_CUDA(cudaGetLastError());
+    ctx->launches++;
+    return VP8A_OK;
+  }
   if (cin == 32 && cout == 32) return conv_fwd<32, 4>(ctx, x, w, bias, 32, (int)n, relu, y, y_f32);
   if (cin == 32 && cout == 1) return conv_fwd<32, 1>(ctx, x, w, bias, 1, (int)n, relu, y, y_f32);
   vp8a::set_error("conv shape must be 2->32, 32->32 or 32->1");

@@ -91,6 +91,31 @@ def test_conv_forward_and_gradients_match_fp32_reference(ctx, cin, cout, relu):
     assert np.all(np.abs(gxn - rdx) <= np.abs(rdx) * 2.0 ** -8 + 1e-6)
 
 
+@pytest.mark.parametrize("relu", [True, False])
+def test_tensor_core_conv_32_to_32_matches_fp32_reference(ctx, relu):
+    # BF16 output of a 32 -> 32 layer: the tcgen05 path (TMEM accumulators,
+    # shared-memory descriptors). FP32 accumulation in another order, then
+    # one BF16 rounding: within half a BF16 ulp of the FP32 reference plus
+    # the accumulation slack.
+    rng = np.random.default_rng(77 + relu)
+    n = 7
+    x = np.maximum(bf16(rng.standard_normal((n, 32, 32, 32))), 0)
+    w = bf16(rng.standard_normal((32, 9, 32)) * 0.2)
+    b = rng.standard_normal(32).astype(np.float32) * 0.1
+    lib = ctx._lib
+    dx_, dw_, db_ = dev_bf16(x), dev_bf16(w.reshape(-1)), torch.from_numpy(b).cuda()
+    y = torch.full((n, 32, 32, 32), float("nan"), dtype=torch.bfloat16, device="cuda")
+    torch.cuda.synchronize()
+    assert lib.vp8a_lp_conv_forward(ctx.handle, dx_.data_ptr(), 32, dw_.data_ptr(), db_.data_ptr(), 32, n,
+                                    int(relu), y.data_ptr(), None) == abi.OK
+    assert lib.vp8a_ctx_synchronize(ctx.handle) == abi.OK
+    want = conv_ref(x, w, b, relu)
+    got = y.float().cpu().numpy()
+    assert np.isfinite(got).all()
+    slack = 1e-4 * max(1.0, np.abs(want).max())
+    assert np.all(np.abs(got - want) <= np.abs(want) * 2.0 ** -8 + slack)
+
+
 def test_softmax_cross_entropy_and_adam(ctx):
     rng = np.random.default_rng(3)
     n = 5
