@@ -1162,6 +1162,52 @@ def batched_predict(ctx, vp8a, torch, split):
     return fn
 
 
+def lp_conv_arm(args):
+    """One 32 -> 32 layer of the proposal net over `--images` 32 x 32 maps
+    (8160 = one reference of a 1080p frame) through vp8a_lp_conv_forward:
+    the tcgen05 path (BF16 out) beside the mma.sync path (FP32 out), CUDA
+    events on the context stream, inputs larger than L2."""
+    import torch
+
+    import vp8a
+
+    ctx = vp8a.Context(0)
+    lib = ctx._lib
+    n = args.images
+    g = torch.Generator(device="cuda").manual_seed(5)
+    x = torch.relu(torch.randn(n, 32, 32, 32, device="cuda", generator=g)).to(torch.bfloat16)
+    w = (torch.randn(32 * 9 * 32, device="cuda", generator=g) * 0.2).to(torch.bfloat16)
+    b = torch.randn(32, device="cuda", generator=g) * 0.1
+    y = torch.empty(n, 32, 32, 32, dtype=torch.bfloat16, device="cuda")
+    yf = torch.empty(n, 32, 32, 32, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    out = {}
+    for name, yb, yff in (("tcgen05_bf16_out", y.data_ptr(), None), ("mma_sync_f32_out", None, yf.data_ptr())):
+        call = lambda: lib.vp8a_lp_conv_forward(ctx.handle, x.data_ptr(), 32, w.data_ptr(), b.data_ptr(), 32, n,  # noqa: E731
+                                                1, yb, yff)
+        for _ in range(args.warmup):
+            assert call() == 0
+        assert lib.vp8a_ctx_synchronize(ctx.handle) == 0
+        ts = []
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            assert call() == 0
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        assert lib.vp8a_ctx_synchronize(ctx.handle) == 0
+        ms = sorted(ts)[len(ts) // 2]
+        flops = 2.0 * n * 1024 * 32 * 288
+        out[name] = {"ms": round(ms, 4), "tflops": round(flops / ms / 1e9, 1),
+                     "gbs_in_out": round(n * 1024 * 32 * (2 + (2 if yb else 4)) / ms / 1e6, 1)}
+    out["max_abs_diff"] = float((y.float() - yf).abs().max())
+    del x, y, yf, w, b, stream
+    ctx.close()
+    return {"case": "lp_conv", "images": n, "layer": "3x3 conv 32 -> 32 on 32 x 32 maps", **out}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1171,11 +1217,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--case", choices=["arnr", "analysis", "lf", "recon", "predict", "predict_mb", "predict_split",
-                                       "batch", "learned"],
+                                       "batch", "learned", "lp_conv"],
                     help="profile one stage alone, or (batch) the batched many-stream path")
     ap.add_argument("--streams", type=int, default=48, help="streams of the batch case")
     ap.add_argument("--train-steps", type=int, default=300, help="training steps of the learned case")
     ap.add_argument("--size", default="1920x1080", help="frame size for --case")
+    ap.add_argument("--images", type=int, default=8160, help="32 x 32 maps of the lp_conv case")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl != "reference":
         log("note: fewer than 3 warm-up steps")
@@ -1183,6 +1230,8 @@ def main():
         res = batch_arm(args)
     elif args.case == "learned":
         res = learned_arm(args)
+    elif args.case == "lp_conv":
+        res = lp_conv_arm(args)
     elif args.case:
         res = case_arm(args)
     else:

@@ -463,19 +463,29 @@ __global__ void __launch_bounds__(256, 2) lp_conv_fwd_tc_kernel(const uint16_t* 
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_a), "r"(1));
     asm volatile("fence.mbarrier_init.release.cluster;");
   }
-  // Zero image (halo and tail), then the 1024 pixels and the weights.
-  for (int q = tid; q < IMG_BYTES / 16; q += 256) reinterpret_cast<uint4*>(img_s)[q] = make_uint4(0, 0, 0, 0);
-  __syncthreads();
+  // The 1024 pixels and the weights by 16-byte asynchronous copies (all in
+  // flight at once), and zeros into the halo ring and the tail only, which
+  // no copy touches.
   const uint4* Xi = reinterpret_cast<const uint4*>(X + im * LP_P * 32);
   for (int q = tid; q < LP_P * 4; q += 256) {
     const int p = q >> 2, g = q & 3;
     const int h = ((p >> 5) + 1) * 34 + (p & 31) + 1;
-    *reinterpret_cast<uint4*>(img_s + g * REGION + h * 16) = Xi[q];
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(img_a + (uint32_t)(g * REGION + h * 16)),
+                 "l"(Xi + q)
+                 : "memory");
   }
   for (int q = tid; q < 32 * 36; q += 256) {
     const int n = q / 36, kg = q % 36;
-    *reinterpret_cast<uint4*>(w_s + (kg * 32 + n) * 16) = *reinterpret_cast<const uint4*>(W + n * 288 + kg * 8);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(w_a + (uint32_t)((kg * 32 + n) * 16)),
+                 "l"(W + n * 288 + kg * 8)
+                 : "memory");
   }
+  for (int q = tid; q < 4 * NV; q += 256) {
+    const int h = q % NV, hy = h / 34, hx = h % 34;
+    if (h >= 34 * 34 || hy == 0 || hy == 33 || hx == 0 || hx == 33)
+      reinterpret_cast<uint4*>(img_s)[q] = make_uint4(0, 0, 0, 0);
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
