@@ -10,7 +10,7 @@
 
 #include "../../include/vp8a.h"
 
-#define VP8A_ABI_VERSION ((1u << 16) | 0u)
+#define VP8A_ABI_VERSION ((1u << 16) | 1u)  /* 1.1: the bitstream writer */
 
 // ----------------------------------------------------------------- context
 struct vp8a_ctx {
