@@ -12,8 +12,10 @@
 //   lp_conv_fwd_smem_kernel implicit-GEMM conv (+ bias, ReLU), one CTA per
 //                           image staged with its halo in shared memory
 //   lp_conv_bwd_data_kernel dX = conv^T(dY, W), masked by the ReLU of X
-//   lp_conv_bwd_w_kernel    dW = sum over pixels of dY x shifted X (split
-//                           over pixel chunks, FP32 atomics), db
+//   lp_conv_fwd_tc_kernel   the 32 -> 32 forward layers on tcgen05 tensor
+//                           cores (TMEM accumulators)
+//   lp_conv_bwd_w_smem_kernel dW = sum over pixels of dY x shifted X (16
+//                           staged chunks per CTA, one atomic per weight), db
 //   lp_softmax_ce_kernel    softmax over the 1024 cells, cross-entropy,
 //                           d(logits) = (p - onehot) / n
 //   lp_adam_kernel          Adam on FP32 master weights, BF16 copies
@@ -251,54 +253,8 @@ __global__ void __launch_bounds__(128) lp_conv_bwd_data_kernel(const uint16_t* d
 
 // dW[co][tap][ci] += sum over a chunk of pixels of dY[p][co] X[p + off][ci]:
 // M = co (16-row tiles), N = tap * CIN + ci (8-column tiles), K = pixels.
-// Block (chunk, n-tile group): 4 warps, warp w takes n-tiles w, w + 4, ...
-// of the group; each accumulates its chunk and adds it with FP32 atomics.
-constexpr int LP_WCHUNK = 512;  // pixels per block
+constexpr int LP_WCHUNK = 512;  // pixels per staged chunk (half an image)
 
-template <int CIN>
-__global__ void __launch_bounds__(128) lp_conv_bwd_w_kernel(const uint16_t* dY, const uint16_t* X, int cout,
-                                                            long n_pix, float* dW, float* db) {
-  constexpr int NTOT = (9 * CIN + 7) / 8;  // n-tiles
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3, warp = threadIdx.x >> 5;
-  const long p0 = (long)blockIdx.x * LP_WCHUNK;
-  const int mtiles = (cout + 15) / 16;
-  for (int nt = blockIdx.y * 4 + warp; nt < NTOT; nt += gridDim.y * 4) {
-    for (int mt = 0; mt < mtiles; mt++) {
-      float d[4] = {0.f, 0.f, 0.f, 0.f};
-      for (long k0 = p0; k0 < p0 + LP_WCHUNK && k0 < n_pix; k0 += 16) {
-        auto dy = [&](int co, long p) -> uint16_t { return (co < cout && p < n_pix) ? dY[p * cout + co] : (uint16_t)0; };
-        auto xs = [&](int n, long p) -> uint16_t {
-          if (p >= n_pix || n >= 9 * CIN) return 0;
-          const int tap = n / CIN, ci = n % CIN, img = (int)(p / LP_P), q = (int)(p % LP_P);
-          return act(X, CIN, img, (q >> 5) + tap / 3 - 1, (q & 31) + tap % 3 - 1, ci);
-        };
-        const int m0 = mt * 16 + g, m1 = m0 + 8;
-        const uint32_t a[4] = {pack_raw(dy(m0, k0 + 2 * t), dy(m0, k0 + 2 * t + 1)),
-                               pack_raw(dy(m1, k0 + 2 * t), dy(m1, k0 + 2 * t + 1)),
-                               pack_raw(dy(m0, k0 + 2 * t + 8), dy(m0, k0 + 2 * t + 9)),
-                               pack_raw(dy(m1, k0 + 2 * t + 8), dy(m1, k0 + 2 * t + 9))};
-        const int n = nt * 8 + g;
-        const uint32_t b[2] = {pack_raw(xs(n, k0 + 2 * t), xs(n, k0 + 2 * t + 1)),
-                               pack_raw(xs(n, k0 + 2 * t + 8), xs(n, k0 + 2 * t + 9))};
-        mma_bf16(d, a, b);
-      }
-#pragma unroll
-      for (int h = 0; h < 2; h++)
-#pragma unroll
-        for (int e = 0; e < 2; e++) {
-          const int co = mt * 16 + g + 8 * h, n = nt * 8 + 2 * t + e;
-          if (co < cout && n < 9 * CIN) atomicAdd(&dW[(size_t)co * 9 * CIN + n], d[2 * h + e]);
-        }
-    }
-  }
-  // Bias gradient: this chunk's column sums of dY (block row 0 only).
-  if (blockIdx.y == 0)
-    for (int co = threadIdx.x; co < cout; co += blockDim.x) {
-      float s = 0.f;
-      for (long p = p0; p < p0 + LP_WCHUNK && p < n_pix; p++) s += __bfloat162float(__ushort_as_bfloat16(dY[p * cout + co]));
-      atomicAdd(&db[co], s);
-    }
-}
 
 // ------------------------------------------------------------- loss
 
@@ -599,12 +555,106 @@ vp8a_status conv_bwd_data(vp8a_ctx* ctx, const uint16_t* dY, const uint16_t* W, 
   return VP8A_OK;
 }
 
+// Weight gradient with staged chunks: each CTA walks LP_WCPB chunks of 512
+// pixels (half an image each), staging the chunk's dY ([pixel][co], co
+// padded to 16 * MT) and its 18 input rows with a zero halo ([row][col][ci])
+// in shared memory; warp w accumulates the n-tiles w, w + 4, ... of
+// dW = dY^T x im2col(X) in registers across all its chunks, and the CTA
+// adds its partial sums with one atomic per weight at the end.
+constexpr int LP_WCPB = 16;
+template <int CIN, int MT>
+__global__ void __launch_bounds__(128) lp_conv_bwd_w_smem_kernel(const uint16_t* dY, const uint16_t* X, int cout,
+                                                                 long n_chunks, float* dW, float* db) {
+  constexpr int NTOT = (9 * CIN + 7) / 8, NPW = (NTOT + 3) / 4;
+  constexpr int DS = 16 * MT + 8, PS = CIN + (CIN >= 16 ? 8 : 0) + (CIN < 16 ? 2 : 0);
+  extern __shared__ __align__(16) uint16_t smw[];
+  uint16_t* dy_s = smw;                        // 512 * DS
+  uint16_t* x_s = smw + LP_WCHUNK * DS;        // 18 * 34 * PS
+  const int tid = threadIdx.x, lane = tid & 31, g = lane >> 2, t = lane & 3, warp = tid >> 5;
+  float d[NPW][MT][4];
+#pragma unroll
+  for (int a = 0; a < NPW; a++)
+#pragma unroll
+    for (int m = 0; m < MT; m++) d[a][m][0] = d[a][m][1] = d[a][m][2] = d[a][m][3] = 0.f;
+  float bsum = 0.f;
+  for (long ch = (long)blockIdx.x * LP_WCPB; ch < n_chunks && ch < (long)(blockIdx.x + 1) * LP_WCPB; ch++) {
+    const long p0 = ch * LP_WCHUNK;
+    const int img = (int)(p0 / LP_P), row0 = (int)(p0 % LP_P) / 32;
+    __syncthreads();  // the previous chunk's fragments are read
+    for (int q = tid; q < LP_WCHUNK * DS; q += 128) {
+      const int pp = q / DS, co = q % DS;
+      dy_s[q] = co < cout ? dY[(p0 + pp) * cout + co] : (uint16_t)0;
+    }
+    for (int q = tid; q < 18 * 34 * PS; q += 128) {
+      const int ci = q % PS, c = (q / PS) % 34, r = q / (PS * 34);
+      const int y = row0 + r - 1, x = c - 1;
+      x_s[q] = (ci < CIN && y >= 0 && y < 32 && x >= 0 && x < 32)
+                   ? X[((size_t)img * LP_P + y * 32 + x) * CIN + ci]
+                   : (uint16_t)0;
+    }
+    __syncthreads();
+    if (tid < cout)
+      for (int pp = 0; pp < LP_WCHUNK; pp++) bsum += __bfloat162float(__ushort_as_bfloat16(dy_s[pp * DS + tid]));
+#pragma unroll
+    for (int a = 0; a < NPW; a++) {
+      const int nt = warp + 4 * a;
+      if (nt >= NTOT) break;
+      const int n = nt * 8 + g;
+      const bool nv = n < 9 * CIN;
+      const int tap = nv ? n / CIN : 0, ci = nv ? n % CIN : 0, oy = tap / 3, ox = tap % 3;
+      for (int k0 = 0; k0 < LP_WCHUNK; k0 += 16) {
+        auto xv = [&](int pp) -> uint32_t {
+          return nv ? x_s[(((pp >> 5) + oy) * 34 + (pp & 31) + ox) * PS + ci] : 0u;
+        };
+        const uint32_t b[2] = {xv(k0 + 2 * t) | (xv(k0 + 2 * t + 1) << 16),
+                               xv(k0 + 2 * t + 8) | (xv(k0 + 2 * t + 9) << 16)};
+#pragma unroll
+        for (int m = 0; m < MT; m++) {
+          const int m0 = m * 16 + g, m1 = m0 + 8;
+          auto dv = [&](int co, int pp) -> uint32_t { return dy_s[pp * DS + co]; };
+          const uint32_t av[4] = {dv(m0, k0 + 2 * t) | (dv(m0, k0 + 2 * t + 1) << 16),
+                                  dv(m1, k0 + 2 * t) | (dv(m1, k0 + 2 * t + 1) << 16),
+                                  dv(m0, k0 + 2 * t + 8) | (dv(m0, k0 + 2 * t + 9) << 16),
+                                  dv(m1, k0 + 2 * t + 8) | (dv(m1, k0 + 2 * t + 9) << 16)};
+          mma_bf16(d[a][m], av, b);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < NPW; a++) {
+    const int nt = warp + 4 * a;
+    if (nt >= NTOT) break;
+#pragma unroll
+    for (int m = 0; m < MT; m++)
+#pragma unroll
+      for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int co = m * 16 + g + 8 * h, n = nt * 8 + 2 * t + e;
+          if (co < cout && n < 9 * CIN) atomicAdd(&dW[(size_t)co * 9 * CIN + n], d[a][m][2 * h + e]);
+        }
+  }
+  if (tid < cout) atomicAdd(&db[tid], bsum);
+}
+
 template <int CIN>
 vp8a_status conv_bwd_w(vp8a_ctx* ctx, const uint16_t* dY, const uint16_t* X, int cout, int n, float* dW, float* db) {
-  const long n_pix = (long)n * LP_P;
-  constexpr int NTOT = (9 * CIN + 7) / 8;
-  const dim3 grid((unsigned)((n_pix + LP_WCHUNK - 1) / LP_WCHUNK), (unsigned)((NTOT + 3) / 4));
-  lp_conv_bwd_w_kernel<CIN><<<grid, 128, 0, ctx->stream>>>(dY, X, cout, n_pix, dW, db);
+  const long n_chunks = (long)n * LP_P / LP_WCHUNK;
+  const unsigned grid = (unsigned)((n_chunks + LP_WCPB - 1) / LP_WCPB);
+  if (grid == 0) return VP8A_OK;
+  constexpr int PS = CIN + (CIN >= 16 ? 8 : 0) + (CIN < 16 ? 2 : 0);
+  if (cout > 16) {
+    const size_t smem = sizeof(uint16_t) * (LP_WCHUNK * (32 + 8) + 18 * 34 * PS);
+    VP8A_CUDA(cudaFuncSetAttribute(lp_conv_bwd_w_smem_kernel<CIN, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+    lp_conv_bwd_w_smem_kernel<CIN, 2><<<grid, 128, smem, ctx->stream>>>(dY, X, cout, n_chunks, dW, db);
+  } else {
+    const size_t smem = sizeof(uint16_t) * (LP_WCHUNK * (16 + 8) + 18 * 34 * PS);
+    VP8A_CUDA(cudaFuncSetAttribute(lp_conv_bwd_w_smem_kernel<CIN, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+    lp_conv_bwd_w_smem_kernel<CIN, 1><<<grid, 128, smem, ctx->stream>>>(dY, X, cout, n_chunks, dW, db);
+  }
   VP8A_CUDA(cudaGetLastError());
   ctx->launches++;
   return VP8A_OK;
