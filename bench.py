@@ -489,11 +489,13 @@ def gpu_arm(args):
         torch.cuda.synchronize(dev)
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record(stream)
-        ps.step()
+        choice = ps.step()
         e.record(stream)
         e.synchronize()
         e_times.append(s.elapsed_time(e))
     e_ms = float(np.sum(e_times))
+    # The device step's outputs of its last run, for the parity check.
+    got = gpu_step_outputs(gs, choice)
     if world > 1:
         ms, e_ms, e_ms_call = max_over_ranks([ms, e_ms, e_ms_call], dist, dev)
     result = None
@@ -562,8 +564,20 @@ def gpu_arm(args):
             "e2e_per_call_step_ms": [round(x, 3) for x in e_times_call],
             "clocks": clk.summary(),
         }
+        want = None
         if args.gpus == 1 and world == 1 and not args.no_cpu_baseline:
-            result["cpu_baseline"] = cpu_baseline(frames, budget_s=args.cpu_budget)
+            result["cpu_baseline"], want = cpu_baseline(frames, budget_s=args.cpu_budget)
+        if not args.no_parity:
+            if want is None:
+                sys.path.insert(0, os.path.join(ROOT, "oracle"))
+                import oracle
+
+                oracle.build()
+                want = cpu_step(oracle, frames, os.cpu_count() or 1)
+            ok, detail = step_parity(got, want)
+            result["parity"] = ok
+            result["parity_detail"] = {**detail, "against": "the oracle (C restatement of the reference) on the "
+                                                            "same inputs; rank 0's frames"}
     # Pinned buffers copied on the library's stream are released while that
     # stream still exists (their release records an event on it).
     ctx.synchronize()
@@ -660,6 +674,10 @@ def stage_times(gs, stream, torch, flush, reps=3):
 
 
 def cpu_step(oracle, frames, threads):
+    """The step on the CPU by the oracle. Returns every output the device
+    step produces: the MB-padded ALTREF anchor, the MB decisions, the qi-44
+    reconstruction, the MBs' loop-filter records, the 64 x 8 candidate table
+    and the walk's (level, sharpness)."""
     import vp8a
 
     anchor = oracle.build_arnr_altref([frames[9 + i] for i in range(LOOKAHEAD)], 3, 3, threads=threads)
@@ -671,10 +689,44 @@ def cpu_step(oracle, frames, threads):
     oracle.reconstruct_inter_frame(frames[8], refs, [1, 2, 3], dec, vp8a.abi.quant_indices(QI), recon, lf_info=mbs,
                                    threads=threads)
     table = oracle.filter_sweep(recon, mbs, vp8a.abi.filter_config(0, 0), frames[8], 0, threads=threads)
-    return select_full(table.reshape(-1), 0)
+    return {"altref": refs[2], "decisions": dec.reshape(-1), "recon": recon, "lf_info": mbs,
+            "lf_table": table.reshape(-1), "lf_choice": select_full(table.reshape(-1), 0)}
+
+
+def gpu_step_outputs(gs, choice):
+    """The device step's outputs read back after its last run (same keys as
+    cpu_step's)."""
+    gs.ctx.synchronize()
+    gs.torch.cuda.synchronize()
+    abi = gs.abi
+    return {"altref": tuple(p.cpu().numpy() for p in gs.alt),
+            "decisions": np.frombuffer(gs.dec.cpu().numpy().tobytes(), abi.MB_DECISION_DTYPE),
+            "recon": tuple(p.cpu().numpy() for p in gs.recon),
+            "lf_info": np.frombuffer(gs.mbs.cpu().numpy().tobytes(), abi.MB_LF_INFO_DTYPE),
+            "lf_table": gs.table.cpu().numpy().view(np.uint64).copy(), "lf_choice": tuple(choice)}
+
+
+def step_parity(got, want):
+    """Exact equality of the device step's outputs with the oracle's, per
+    output: ALTREF planes, every decision field, the reconstruction planes,
+    the loop-filter records, all 512 table entries (505 distinct candidates)
+    and the selected (level, sharpness)."""
+    dec_fields = [f for f in got["decisions"].dtype.names if f != "reserved"]
+    lf_fields = [f for f in got["lf_info"].dtype.names if f != "reserved"]
+    out = {
+        "altref": all(np.array_equal(a, b) for a, b in zip(got["altref"], want["altref"])),
+        "decisions": all(np.array_equal(got["decisions"][f], want["decisions"][f]) for f in dec_fields),
+        "recon": all(np.array_equal(a, b) for a, b in zip(got["recon"], want["recon"])),
+        "lf_info": all(np.array_equal(got["lf_info"][f], want["lf_info"][f]) for f in lf_fields),
+        "lf_table": bool(np.array_equal(got["lf_table"], want["lf_table"])),
+        "lf_choice": tuple(got["lf_choice"]) == tuple(want["lf_choice"]),
+    }
+    return all(out.values()), out
 
 
 def cpu_baseline(frames, budget_s=30.0):
+    """Times the oracle's step on all host threads (a bounded sample) and
+    returns (baseline record, the first step's outputs)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
@@ -682,8 +734,10 @@ def cpu_baseline(frames, budget_s=30.0):
     threads = os.cpu_count() or 1
     t0 = time.perf_counter()
     n = 0
+    first = None
     while True:
-        cpu_step(oracle, frames, threads)
+        out = cpu_step(oracle, frames, threads)
+        first = first or out
         n += 1
         if time.perf_counter() - t0 > min(budget_s, 30.0) or n >= 3:
             break
@@ -691,7 +745,9 @@ def cpu_baseline(frames, budget_s=30.0):
     return {"value": round(N_MB * n / dt, 1), "unit": "MB/s", "cores": threads, "kind": "port",
             "sample": f"{n} full 1080p step(s) (ARNR + 3-ref analysis + qi-44 reconstruction + 505-candidate "
                       f"LF sweep) by the C oracle on {threads} threads in {dt:.2f} s",
-            "cpu_model": cpu_model()}
+            "note": "a scalar C restatement of the reference's algorithm on the 64x8 grid (505 candidates); the "
+                    "reference's own walk scores ~24 candidates and its nightly SIMD kernels are not in the port",
+            "cpu_model": cpu_model()}, first
 
 
 def cpu_model():
@@ -1012,7 +1068,7 @@ def learned_arm(args):
         with learned.on_ctx_stream(ctx):
             idx = torch.randint(0, n, (4096,), generator=g).cuda()
             xb, yb = x[idx].contiguous(), y[idx].contiguous()
-        losses.append(float(net.train_step(xb, yb, lr=1e-3)))
+        losses.append(net.train_step(xb, yb, lr=1e-3))
     ctx.synchronize()
     t_train = time.time() - t1
     with learned.on_ctx_stream(ctx):
@@ -1215,6 +1271,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="vp8a", choices=["vp8a", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the step's parity check against the oracle")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--case", choices=["arnr", "analysis", "lf", "recon", "predict", "predict_mb", "predict_split",
                                        "batch", "learned", "lp_conv"],

@@ -259,6 +259,14 @@ void* vp8a_ctx_stream(vp8a_ctx* ctx);
 vp8a_status vp8a_ctx_synchronize(vp8a_ctx* ctx);
 /* Kernel launches issued by this context since creation. */
 uint64_t vp8a_ctx_launch_count(const vp8a_ctx* ctx);
+/* No counterpart in the reference (its threads join instead of polling).
+ * Sets how many times a wavefront wait of the inter analysis (an MB row
+ * waiting for the row above it) may poll before it gives up: the call then
+ * returns VP8A_E_DEVICE_TIMEOUT, every CTA leaves, and the context stays
+ * usable. Default 2^24 polls (seconds). 0 gives up at the first poll that
+ * finds the row above behind, which makes the timeout path testable without
+ * hanging or faulting anything. Applies to calls issued after it. */
+vp8a_status vp8a_ctx_set_wait_limit(vp8a_ctx* ctx, uint64_t polls);
 /* Text of the last error on this thread ("" if none). */
 const char* vp8a_last_error(void);
 /* ABI version of this header (major << 16 | minor). */

@@ -1412,7 +1412,7 @@ vp8a_status prepare_job(vp8a_ctx* ctx, vp8a::Stager& st, MvBitsCache& mc, const 
   a.status = ctx->d_status;
   a.dec = (vp8a_mb_decision*)ddec;
   a.trace = (vp8a_ref_search*)dtr;
-  a.spin_limit = 1ull << 24;
+  a.spin_limit = ctx->wait_limit;
   a.words = 1;
   for (uint32_t k = 0; k < n_refs; k++)
     if ((uintptr_t)a.refs[k].plane % 4 != 0 || a.refs[k].stride % 4 != 0) a.words = 0;

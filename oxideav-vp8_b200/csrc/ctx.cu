@@ -257,6 +257,12 @@ vp8a_status vp8a_ctx_synchronize(vp8a_ctx* ctx) {
 
 uint64_t vp8a_ctx_launch_count(const vp8a_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+vp8a_status vp8a_ctx_set_wait_limit(vp8a_ctx* ctx, uint64_t polls) {
+  if (!ctx) return VP8A_E_INVALID_ARGUMENT;
+  ctx->wait_limit = polls;
+  return VP8A_OK;
+}
+
 const char* vp8a_last_error(void) { return g_last_error.c_str(); }
 
 uint32_t vp8a_abi_version(void) { return VP8A_ABI_VERSION; }

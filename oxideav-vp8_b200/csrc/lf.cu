@@ -1071,10 +1071,14 @@ vp8a_status run_sweep(vp8a_ctx* ctx, LfArgs a, int n, vp8a::Stager* gst) {
 // (LoopFilterParams::derive, src/loop_filter.rs:99-148). Each pass fills the
 // table entries of its sharpness group (`masks`); level 0 is one pass for
 // all eight (score_filter_candidate's unfiltered short cut).
-void grid_candidates(const vp8a_filter_config& base, std::vector<uint8_t>& pairs, std::vector<uint8_t>& masks) {
-  pairs.assign({0, 0});
-  masks.assign({0xff});
-  std::vector<vp8a_mb_lf_info> classes;
+// Writes the passes into `pairs` (2 per pass) and `masks` (1 per pass;
+// room for 1 + 63 * 8 passes) and returns their number. No heap memory.
+int grid_passes(const vp8a_filter_config& base, uint8_t* pairs, uint8_t* masks) {
+  int n = 0;
+  pairs[0] = pairs[1] = 0;
+  masks[n++] = 0xff;
+  vp8a_mb_lf_info classes[4 * 11];
+  int nc = 0;
   const int nseg = base.segmentation_enabled ? 4 : 1;
   for (int seg = 0; seg < nseg; seg++) {
     vp8a_mb_lf_info m{};
@@ -1083,14 +1087,14 @@ void grid_candidates(const vp8a_filter_config& base, std::vector<uint8_t>& pairs
     m.inter_mode = VP8A_MODE_NONE;
     for (int bp = 0; bp < 2; bp++) {
       m.y_mode_is_bpred = (uint8_t)bp;
-      classes.push_back(m);
+      classes[nc++] = m;
     }
     m.y_mode_is_bpred = 0;
     for (int ref = VP8A_REF_LAST; ref <= VP8A_REF_ALTREF; ref++)
       for (int mode : {VP8A_MODE_ZERO, VP8A_MODE_SPLIT, VP8A_MODE_NEAREST}) {
         m.ref_frame = (uint8_t)ref;
         m.inter_mode = (uint8_t)mode;
-        classes.push_back(m);
+        classes[nc++] = m;
       }
   }
   for (int level = 1; level < 64; level++) {
@@ -1100,18 +1104,27 @@ void grid_candidates(const vp8a_filter_config& base, std::vector<uint8_t>& pairs
       uint8_t mask = 0;
       for (int s1 = s0; s1 < 8; s1++) {
         bool same = true;
-        for (const auto& m : classes) {
-          const int l = mb_level(base, level, m);
+        for (int c = 0; c < nc; c++) {
+          const int l = mb_level(base, level, classes[c]);
           if (l != 0 && interior_limit(l, s0) != interior_limit(l, s1)) same = false;
         }
         if (same) mask |= (uint8_t)(1u << s1);
       }
       done |= mask;
-      pairs.push_back((uint8_t)level);
-      pairs.push_back((uint8_t)s0);
-      masks.push_back(mask);
+      pairs[2 * n] = (uint8_t)level;
+      pairs[2 * n + 1] = (uint8_t)s0;
+      masks[n++] = mask;
     }
   }
+  return n;
+}
+
+void grid_candidates(const vp8a_filter_config& base, std::vector<uint8_t>& pairs, std::vector<uint8_t>& masks) {
+  pairs.resize(2 * (1 + 63 * 8));
+  masks.resize(1 + 63 * 8);
+  const int n = grid_passes(base, pairs.data(), masks.data());
+  pairs.resize(2 * n);
+  masks.resize(n);
 }
 
 // Upload a grid's candidate pairs and masks into `a` (level 0 and the
@@ -1177,10 +1190,22 @@ constexpr int NA_CANDIDATES = 1 + 63 * 8;
 constexpr size_t NA_CANDS = 0;                                              // (level, sharpness) pairs
 constexpr size_t NA_T0 = 1024;                                              // int16 per MB row
 constexpr size_t NA_TOP = NA_T0 + 2 * NA_MAX_MB_ROWS;                       // u8 per MB row
-constexpr size_t NA_OFF = 1536;                                             // int32 per step + 1
+constexpr size_t NA_MASK = 1440;                                            // u8 sharpness mask per pass
+constexpr size_t NA_OFF = 2048;                                             // int32 per step + 1
 constexpr size_t NA_ROWS = (NA_OFF + 4 * (NA_MAX_STEPS + 1) + 15) & ~(size_t)15;  // u16 per scored MB
 constexpr size_t NA_BYTES = NA_ROWS + 2 * (size_t)NA_MAX_MB_ROWS * NA_MAX_MB_COLS;
-static_assert(2 * NA_CANDIDATES <= NA_T0 && NA_TOP + NA_MAX_MB_ROWS <= NA_OFF, "scratch layout");
+static_assert(2 * NA_CANDIDATES <= NA_T0 && NA_TOP + NA_MAX_MB_ROWS <= NA_MASK &&
+                  NA_MASK + NA_CANDIDATES <= NA_OFF, "scratch layout");
+
+// The grid's filter passes (grid_candidates: level 0, then one pass per
+// group of sharpness values that filter identically), passed to the
+// schedule kernel by value (1.5 KB of kernel parameters) so that no host
+// buffer has to be staged.
+struct NaGrid {
+  int n;
+  uint8_t pairs[2 * NA_CANDIDATES];
+  uint8_t masks[NA_CANDIDATES];
+};
 
 // The library's only copy; every call on a device shares it (about 72 KiB,
 // held by each device that loads the library until the process exits).
@@ -1190,19 +1215,21 @@ static __device__ __align__(256) uint8_t g_sweep_scratch[NA_BYTES];
 // stage_lf and vp8a_filter_sweep), written on the device. One CTA of 1024
 // threads: steps <= NA_MAX_STEPS < 1024.
 __global__ void __launch_bounds__(1024) sweep_schedule_kernel(uint8_t* scr, int rows, int cols, int every_rows,
-                                                              int steps) {
+                                                              int steps, const __grid_constant__ NaGrid grid) {
   __shared__ int16_t st0[NA_MAX_MB_ROWS];
   __shared__ int cnt[NA_MAX_STEPS];
   uint8_t* cands = scr + NA_CANDS;
+  uint8_t* masks = scr + NA_MASK;
   int16_t* t0 = (int16_t*)(scr + NA_T0);
   uint8_t* top = scr + NA_TOP;
   int32_t* off = (int32_t*)(scr + NA_OFF);
   uint16_t* srow = (uint16_t*)(scr + NA_ROWS);
   const int tid = threadIdx.x;
-  // One level-0 candidate, then every (level 1..63, sharpness 0..7).
-  for (int i = tid; i < NA_CANDIDATES; i += blockDim.x) {
-    cands[2 * i] = (uint8_t)(i == 0 ? 0 : 1 + (i - 1) / 8);
-    cands[2 * i + 1] = (uint8_t)(i == 0 ? 0 : (i - 1) % 8);
+  // The grid's passes and the table entries each one fills.
+  for (int i = tid; i < grid.n; i += blockDim.x) {
+    cands[2 * i] = grid.pairs[2 * i];
+    cands[2 * i + 1] = grid.pairs[2 * i + 1];
+    masks[i] = grid.masks[i];
   }
   for (int r = tid; r < rows; r += blockDim.x) {
     int v, t;
@@ -1678,7 +1705,9 @@ vp8a_status vp8a_filter_sweep_noalloc(vp8a_ctx* ctx, const vp8a_planes* planes, 
     }
     max_active = std::max(max_active, n);
   }
-  sweep_schedule_kernel<<<1, 1024, 0, ctx->stream>>>(scr, rows, cols, (int)every_rows, steps);
+  NaGrid grid{};
+  grid.n = grid_passes(*base, grid.pairs, grid.masks);  // <= NA_CANDIDATES
+  sweep_schedule_kernel<<<1, 1024, 0, ctx->stream>>>(scr, rows, cols, (int)every_rows, steps, grid);
   VP8A_CUDA(cudaGetLastError());
   ctx->launches++;
 
@@ -1700,6 +1729,7 @@ vp8a_status vp8a_filter_sweep_noalloc(vp8a_ctx* ctx, const vp8a_planes* planes, 
   a.width = (int)src->width;
   a.height = (int)src->height;
   a.cands = scr + NA_CANDS;
+  a.cand_mask = scr + NA_MASK;
   a.row_t0 = (const int16_t*)(scr + NA_T0);
   a.row_top = scr + NA_TOP;
   a.sched_off = (const int32_t*)(scr + NA_OFF);
@@ -1713,11 +1743,8 @@ vp8a_status vp8a_filter_sweep_noalloc(vp8a_ctx* ctx, const vp8a_planes* planes, 
   a.level0_unfiltered = 1;
   a.smem_slots = 1;
   a.gslots = nullptr;
-  if ((s = run_sweep(ctx, a, NA_CANDIDATES, nullptr)) != VP8A_OK) return s;
-  // Level 0 scores the same for every sharpness.
-  for (int sh = 1; sh < 8; sh++)
-    VP8A_CUDA(cudaMemcpyAsync(ssd_out + sh, ssd_out, sizeof(uint64_t), cudaMemcpyDeviceToDevice, ctx->stream));
-  return VP8A_OK;
+  // The level-0 pass writes all eight sharpness entries itself.
+  return run_sweep(ctx, a, grid.n, nullptr);
 }
 
 }  // extern "C"

@@ -20,6 +20,8 @@ struct vp8a_ctx {
   uint64_t launches = 0;
   // Device-resident status word shared by kernels with bounded waits.
   uint32_t* d_status = nullptr;
+  // Poll budget of the analysis wavefront waits (vp8a_ctx_set_wait_limit).
+  uint64_t wait_limit = 1ull << 24;
   // Device copy of the 256-entry -log2(p/256) bit-cost table (f64).
   double* d_bit_cost = nullptr;
 };

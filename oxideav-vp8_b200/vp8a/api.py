@@ -54,6 +54,10 @@ class Context:
     def synchronize(self):
         check(self._lib.vp8a_ctx_synchronize(self.handle), "vp8a_ctx_synchronize")
 
+    def set_wait_limit(self, polls):
+        """Poll budget of the analysis wavefront waits (default 2**24)."""
+        check(self._lib.vp8a_ctx_set_wait_limit(self.handle, int(polls)), "vp8a_ctx_set_wait_limit")
+
 
 def _mvs(a):
     a = np.ascontiguousarray(a)

@@ -174,7 +174,9 @@ class ProposalNet:
     @_ordered
     def train_step(self, x, labels, lr=1e-3):
         """One forward / backward / Adam step on a batch; returns the mean
-        cross-entropy (a device scalar)."""
+        cross-entropy over the batch's labelled items (of the forward pass
+        before the update) as a Python float. The loss is read back on the
+        library's stream, after the kernel that wrote it."""
         self.zero_grad()
         logits = self.forward(x, keep=True)
         loss, d, valid = self.loss_and_grad(logits, labels)
@@ -182,7 +184,7 @@ class ProposalNet:
         # items.
         self.backward(d)
         self.adam(lr)
-        return loss / valid
+        return float((loss / valid).item())
 
     @_ordered
     def propose(self, x, k=4):

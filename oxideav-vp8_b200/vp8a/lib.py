@@ -21,6 +21,7 @@ PROTOTYPES = {
     "vp8a_ctx_stream": (P, [P]),
     "vp8a_ctx_synchronize": (C.c_int, [P]),
     "vp8a_ctx_launch_count": (C.c_uint64, [P]),
+    "vp8a_ctx_set_wait_limit": (C.c_int, [P, C.c_uint64]),
     "vp8a_last_error": (C.c_char_p, []),
     "vp8a_abi_version": (U32, []),
     "vp8a_mb_luma_sad_at_mv": (C.c_int, [P, C.POINTER(abi.LumaRef), P, P, P, U32, P]),

@@ -3,7 +3,10 @@ oxideav-vp8: libvpx-encoded IVF streams with the libvpx-decoded I420
 output, public conformance vectors) into tests/golden/vp8_fixtures/, so the
 decoder restatement's tests run without the reference tree.
 
-    python tests/golden/copy_vp8_fixtures.py [reference_root]
+    python tests/golden/copy_vp8_fixtures.py <reference_root>
+
+`reference_root` is the root of an oxideav-vp8 checkout (the directory that
+holds its tests/fixtures/).
 """
 import os
 import shutil
@@ -13,7 +16,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def main():
-    src_root = os.path.join(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", "tests", "fixtures")
+    if len(sys.argv) != 2:
+        sys.exit("usage: copy_vp8_fixtures.py <reference_root>")
+    src_root = os.path.join(sys.argv[1], "tests", "fixtures")
     dst_root = os.path.join(HERE, "vp8_fixtures")
     names = sorted(n for n in os.listdir(src_root) if os.path.isdir(os.path.join(src_root, n)))
     for name in names:

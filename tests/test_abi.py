@@ -29,6 +29,11 @@ def test_library_exports_every_declared_symbol():
     assert lib.vp8a_abi_version() >> 16 == 1
 
 
+def test_wait_limit_needs_a_context():
+    # Host-side argument check only: no device work without a context.
+    assert vp8a.load().vp8a_ctx_set_wait_limit(None, 5) == abi.E_INVALID_ARGUMENT
+
+
 def test_record_layouts_match_c(oracle):
     assert abi.check_layouts() == oracle.type_sizes()
 

@@ -202,12 +202,30 @@ def test_training_reduces_loss_and_finds_the_search_vectors(ctx):
 
     before = top4(net)
     losses = []
+    first_ref = None
     for it in range(150):
         with learned.on_ctx_stream(ctx):
             idx = torch.randint(0, n, (256,), generator=g).cuda()
             xb, yb = x[idx].contiguous(), y[idx].contiguous()
-        losses.append(float(net.train_step(xb, yb, lr=2e-3)))
+        if it == 0:
+            # The definition on this batch, in float64 numpy from the net's
+            # own FP32 scores: mean over labelled items of
+            # logsumexp(scores) - scores[label].
+            scores = net.forward(xb)
+            with learned.on_ctx_stream(ctx):
+                sc = scores.double().cpu().numpy()
+                lab = yb.cpu().numpy()
+            keep = lab >= 0
+            m = sc.max(1, keepdims=True)
+            lse = (m[:, 0] + np.log(np.exp(sc - m).sum(1)))
+            first_ref = float(np.mean((lse - sc[np.arange(sc.shape[0]), np.maximum(lab, 0)])[keep]))
+        losses.append(net.train_step(xb, yb, lr=2e-3))
     after = top4(net)
+    # A fresh net's scores are near-uniform over the 1024 cells: the first
+    # loss is close to ln 1024 and equals the definition on its batch.
+    assert abs(losses[0] - first_ref) <= 1e-3 * first_ref, (losses[0], first_ref)
+    assert 0.5 * np.log(1024) < losses[0] < 2.0 * np.log(1024), losses[0]
+    assert all(v > 0.0 for v in losses), min(losses)
     assert np.mean(losses[-20:]) < 0.7 * np.mean(losses[:10]), (losses[:10], losses[-20:])
     assert after > before + 0.2, (before, after)
 

@@ -47,7 +47,30 @@ def noalloc_sweep(ctx, drecon, dmbs, base, dsrc, every_rows, dout):
                                              every_rows, ptr(dout))
 
 
-@pytest.mark.parametrize("size", [(640, 368), (320, 240)])
+def pool_high_water_reset():
+    """Resets the high-water mark of the device's default memory pool (the
+    pool the library's stream-ordered staging draws from) and returns a
+    function that reads it back."""
+    from cuda.bindings import driver as drv
+
+    import torch
+
+    dev = torch.cuda.current_device()
+    err, pool = drv.cuDeviceGetDefaultMemPool(dev)
+    assert err == drv.CUresult.CUDA_SUCCESS, err
+    attr = drv.CUmemPool_attribute.CU_MEMPOOL_ATTR_USED_MEM_HIGH
+    (err,) = drv.cuMemPoolSetAttribute(pool, attr, drv.cuuint64_t(0))
+    assert err == drv.CUresult.CUDA_SUCCESS, err
+
+    def read():
+        e, v = drv.cuMemPoolGetAttribute(pool, attr)
+        assert e == drv.CUresult.CUDA_SUCCESS, e
+        return int(v)
+
+    return read
+
+
+@pytest.mark.parametrize("size", [(640, 368), (320, 240), (4096, 2176)])
 def test_noalloc_sweep_matches_filter_sweep_twice(ctx, size):
     import torch
 
@@ -56,14 +79,24 @@ def test_noalloc_sweep_matches_filter_sweep_twice(ctx, size):
     dsrc, drecon = on_device(src), on_device(recon)
     dmbs = torch.from_numpy(m.view(np.uint8).copy()).cuda()
     dout = torch.zeros(512, dtype=torch.int64, device="cuda")
+    wants = {er: vp8a.filter_sweep(ctx, recon, m, base, src, every_rows=er) for er in (0, 3)}
+    # A first call loads the kernels and looks the scratch address up; the
+    # calls after it must take no device memory at all: the default pool's
+    # high-water mark stays at zero and the GPU's free memory is unchanged.
+    assert noalloc_sweep(ctx, drecon, dmbs, base, dsrc, 0, dout) == abi.OK
+    assert ctx._lib.vp8a_ctx_synchronize(ctx.handle) == abi.OK
+    torch.cuda.synchronize()
+    high = pool_high_water_reset()
+    free0 = torch.cuda.mem_get_info()[0]
     for every_rows in (0, 0, 3):  # two whole-frame calls in a row, then a sampled one
-        want = vp8a.filter_sweep(ctx, recon, m, base, src, every_rows=every_rows)
         dout.fill_(-1)
         torch.cuda.synchronize()
         assert noalloc_sweep(ctx, drecon, dmbs, base, dsrc, every_rows, dout) == abi.OK
         assert ctx._lib.vp8a_ctx_synchronize(ctx.handle) == abi.OK
         got = dout.cpu().numpy().view(np.uint64).reshape(64, 8)
-        assert np.array_equal(got, want), every_rows
+        assert np.array_equal(got, wants[every_rows]), every_rows
+    assert high() == 0
+    assert torch.cuda.mem_get_info()[0] == free0
 
 
 def test_noalloc_sweep_refuses_host_buffers_and_oversized_grids(ctx):
@@ -84,5 +117,13 @@ def test_noalloc_sweep_refuses_host_buffers_and_oversized_grids(ctx):
     dmbs = torch.zeros(257 * abi.MB_LF_INFO_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
     dout = torch.zeros(512, dtype=torch.int64, device="cuda")
     st = noalloc_sweep(ctx, wide, dmbs, base, wide, 0, dout)
+    assert st == abi.E_INVALID_DIMENSIONS
+    assert b"4096x2176" in ctx._lib.vp8a_last_error()
+    # 2192 pixels tall is one MB row more than the scratch holds.
+    tall = [torch.zeros((2192, 16), dtype=torch.uint8, device="cuda"),
+            torch.zeros((1096, 8), dtype=torch.uint8, device="cuda"),
+            torch.zeros((1096, 8), dtype=torch.uint8, device="cuda")]
+    dmbs = torch.zeros(137 * abi.MB_LF_INFO_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    st = noalloc_sweep(ctx, tall, dmbs, base, tall, 0, dout)
     assert st == abi.E_INVALID_DIMENSIONS
     assert b"4096x2176" in ctx._lib.vp8a_last_error()
