@@ -211,6 +211,9 @@ class GpuStep:
         self.ids = torch.tensor([1, 2, 3], dtype=torch.uint8, device=dev)
         self.ctxs = abi.default_mv_contexts()
         self.base = abi.filter_config(0, 0)
+        self.i420_window = (abi.I420 * LOOKAHEAD)(*[vp8a.i420(*f) for f in self.window])
+        self.alt_planes = vp8a.planes(*self.alt)
+        self.host_ids = np.array([1, 2, 3], np.uint8)
         torch.cuda.synchronize(dev)  # uploads (torch stream) before library calls
         # Per-MB loop-filter side information from the frame's decisions.
         self.run_arnr()
@@ -220,7 +223,6 @@ class GpuStep:
         dec = np.frombuffer(self.dec.cpu().numpy().tobytes(), abi.MB_DECISION_DTYPE)
         self.decisions = dec
         torch.cuda.synchronize(dev)
-        self.i420_window = (abi.I420 * LOOKAHEAD)(*[vp8a.i420(*f) for f in self.window])
         self.i420_cur = vp8a.i420(*self.cur)
         self.planes = (abi.Planes * 3)(vp8a.planes(*self.last), vp8a.planes(*self.golden), vp8a.planes(*self.alt))
         self.recon_planes = vp8a.planes(*self.recon)
@@ -229,29 +231,22 @@ class GpuStep:
         # the analysis; timed as its own stage, outside the metric's step).
         self.pred = [torch.zeros_like(p) for p in self.last]
         self.pred_planes = vp8a.planes(*self.pred)
-        self.host_ids = np.array([1, 2, 3], np.uint8)
         self.run_recon()
         ctx.synchronize()
 
     def run_arnr(self):
-        v = self.vp8a
-        win = (self.abi.I420 * LOOKAHEAD)(*[v.i420(*f) for f in self.window])
-        st = self.lib.vp8a_build_arnr_altref(self.ctx.handle, C.cast(win, C.c_void_p), LOOKAHEAD, 3, 3,
-                                             self.alt[0].data_ptr(), self.alt[1].data_ptr(), self.alt[2].data_ptr())
-        assert st == 0, v.load().vp8a_last_error()
-        # Edge-replicate the anchor into the MB-padded ALTREF planes.
-        with self.torch.cuda.stream(self.stream):
-            self.alt[0][H:] = self.alt[0][H - 1]
-            ch = (H + 1) // 2
-            self.alt[1][ch:] = self.alt[1][ch - 1]
-            self.alt[2][ch:] = self.alt[2][ch - 1]
+        # The anchor goes straight into the MB-padded ALTREF planes (the
+        # blend kernel writes the edge-replicated padding).
+        st = self.lib.vp8a_build_arnr_altref_planes(self.ctx.handle, C.cast(self.i420_window, C.c_void_p), LOOKAHEAD,
+                                                    3, 3, C.byref(self.alt_planes))
+        assert st == 0, self.vp8a.load().vp8a_last_error()
 
     def run_analysis(self):
         v = self.vp8a
         f = v.i420(*self.cur)
         pl = (self.abi.Planes * 3)(v.planes(*self.last), v.planes(*self.golden), v.planes(*self.alt))
         st = self.lib.vp8a_analyse_inter_frame(self.ctx.handle, C.byref(f), C.cast(pl, C.c_void_p),
-                                               self.ids.data_ptr(), 3, C.byref(self.ctxs), self.lam,
+                                               self.host_ids.ctypes.data, 3, C.byref(self.ctxs), self.lam,
                                                self.dec.data_ptr(), None)
         assert st == 0, v.load().vp8a_last_error()
 
@@ -331,19 +326,14 @@ class HostStep:
                     self.golden[0].numel() + self.alt[0].numel() +
                     nb(self.cur) + refs + nb([self.dec]) + nb(self.recon) + nb([self.mbs]) +
                     nb(self.recon) + nb([self.mbs]) + nb(self.cur))
-        self.d2h = nb(self.alt) - (self.alt[0][H:].numel() + 2 * self.alt[1][(H + 1) // 2:].numel()) + \
-            nb([self.dec]) + nb(self.recon) + nb([self.mbs]) + nb([self.table])
+        self.d2h = nb(self.alt) + nb([self.dec]) + nb(self.recon) + nb([self.mbs]) + nb([self.table])
 
     def step(self):
         gs, v, abi, lib = self.gs, self.gs.vp8a, self.gs.abi, self.gs.lib
         win = (abi.I420 * LOOKAHEAD)(*[v.i420(*f) for f in self.window])
-        st = lib.vp8a_build_arnr_altref(gs.ctx.handle, C.cast(win, C.c_void_p), LOOKAHEAD, 3, 3,
-                                        self.alt[0].data_ptr(), self.alt[1].data_ptr(), self.alt[2].data_ptr())
+        ap = v.planes(*self.alt)
+        st = lib.vp8a_build_arnr_altref_planes(gs.ctx.handle, C.cast(win, C.c_void_p), LOOKAHEAD, 3, 3, C.byref(ap))
         assert st == 0
-        self.alt[0][H:] = self.alt[0][H - 1]
-        ch = (H + 1) // 2
-        self.alt[1][ch:] = self.alt[1][ch - 1]
-        self.alt[2][ch:] = self.alt[2][ch - 1]
         f = v.i420(*self.cur)
         pl = (abi.Planes * 3)(v.planes(*self.last), v.planes(*self.golden), v.planes(*self.alt))
         st = lib.vp8a_analyse_inter_frame(gs.ctx.handle, C.byref(f), C.cast(pl, C.c_void_p),
@@ -457,6 +447,7 @@ def gpu_arm(args):
         torch.cuda.synchronize(dev)
     barrier()
     launches = ctx.launches - launches0
+    lf_layout = ctx.last_sweep_layout()
     ms = float(np.sum(times))
     step_ms = [round(x, 3) for x in times]
     # Per-kernel-stage timing for the roofline (separate, after the timed run).
@@ -542,6 +533,10 @@ def gpu_arm(args):
                 "l2": "flushed between timed steps (256 MiB write)",
                 "parallelism": f"replicas x{world}",
                 "lf_choice": list(choice),
+                "lf_layout": {"passes_per_cta": lf_layout[0], "threads_per_cta": lf_layout[1],
+                              "prefetch": bool(lf_layout[2]), "ctas_per_sm": lf_layout[3],
+                              "chosen_by": "autotune (timed on the first sweep of this picture shape)"},
+                "analysis_subpel": "16 sub-pel planes per reference precomputed per frame",
             },
             "e2e": {"value": round(e2e, 1), "unit": "MB/s", "h2d_bytes_per_step": int(ps.h2d),
                     "d2h_bytes_per_step": int(ps.d2h),
@@ -851,7 +846,7 @@ class BatchStep:
     ALTREF (the ARNR anchor of a 5-frame lookahead, centre anchor), its
     qi-44 reconstruction and the 64 x 8 loop-filter sweep over it. Each
     stage of all streams is one call of the batched entry points
-    (vp8a_build_arnr_altrefs, vp8a_analyse_inter_frames,
+    (vp8a_build_arnr_altrefs_planes, vp8a_analyse_inter_frames,
     vp8a_reconstruct_inter_frames, vp8a_filter_sweeps) on device-resident
     buffers."""
 
@@ -886,9 +881,8 @@ class BatchStep:
             win = (abi.I420 * BATCH_LOOKAHEAD)(*[vp8a.i420(*f) for f in st["win"]])
             refs = (abi.Planes * 2)(vp8a.planes(*st["last"]), vp8a.planes(*st["alt"]))
             self.keep += [win, refs]
-            a = st["alt"]
-            aj.append(abi.ArnrJob(C.cast(win, C.c_void_p), BATCH_LOOKAHEAD, BATCH_LOOKAHEAD // 2, 3,
-                                  a[0].data_ptr(), a[1].data_ptr(), a[2].data_ptr()))
+            aj.append(abi.ArnrPlanesJob(C.cast(win, C.c_void_p), BATCH_LOOKAHEAD, BATCH_LOOKAHEAD // 2, 3,
+                                        vp8a.planes(*st["alt"])))
             cur = vp8a.i420(*st["cur"])
             anj.append(abi.AnalysisJob(cur, C.cast(refs, C.c_void_p), ids.ctypes.data, 2,
                                        C.cast(C.pointer(self.ctxs), C.c_void_p), lam, st["dec"].data_ptr(), None))
@@ -908,17 +902,8 @@ class BatchStep:
         assert st == 0, self.vp8a.load().vp8a_last_error()
 
     def run_arnr(self):
-        self._call("vp8a_build_arnr_altrefs", "arnr")
-        # Edge-replicate each anchor into its MB-padded ALTREF planes.
-        with self.torch.cuda.stream(self.stream):
-            for st in self.s:
-                h, ch = st["h"], (st["h"] + 1) // 2
-                a = st["alt"]
-                if a[0].shape[0] > h:
-                    a[0][h:] = a[0][h - 1]
-                if a[1].shape[0] > ch:
-                    a[1][ch:] = a[1][ch - 1]
-                    a[2][ch:] = a[2][ch - 1]
+        # Every stream's anchor straight into its MB-padded ALTREF planes.
+        self._call("vp8a_build_arnr_altrefs_planes", "arnr")
 
     def run_analysis(self):
         self._call("vp8a_analyse_inter_frames", "analysis")
@@ -1191,6 +1176,77 @@ def learned_arm(args):
                     "same frame and references"}
 
 
+def rd_arm(args):
+    """The RD-effort inter search (decide_mb_rd's search, the stream
+    encoder's per-MB inter search) over the bench's 1080p P frame against
+    LAST / GOLDEN / ALTREF, census neighbours from the plain analysis's
+    decisions, qi 44: device time per effort level (CUDA events on the
+    context stream, every buffer device-resident, L2 flushed between
+    calls) and MB/s."""
+    import torch
+
+    import vp8a
+    from vp8a import abi
+
+    ctx = vp8a.Context(0)
+    frames, _ = make_inputs(SEED)
+    gs = GpuStep(ctx, frames, vp8a.load(), torch, 0)
+    ctx.synchronize()
+    dec = np.frombuffer(gs.dec.cpu().numpy().tobytes(), abi.MB_DECISION_DTYPE).reshape(MB_ROWS, MB_COLS)
+    nb = vp8a.neighbours_from_decisions(dec)
+    with torch.cuda.stream(gs.stream):
+        dnb = torch.from_numpy(nb.view(np.uint8).copy()).cuda()
+        out = torch.zeros(N_MB * abi.RD_INTER_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    ctx.synchronize()
+    y1_ac = vp8a.dequant_factors(gs.quant)[1]
+    f = vp8a.i420(*gs.cur)
+    pl = (abi.Planes * 3)(vp8a.planes(*gs.last), vp8a.planes(*gs.golden), vp8a.planes(*gs.alt))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    res = {}
+    for effort, name in enumerate(("fastest", "fast", "balanced", "thorough")):
+        def call():
+            st = ctx._lib.vp8a_rd_inter_search(ctx.handle, C.byref(f), C.cast(pl, C.c_void_p), gs.host_ids.ctypes.data,
+                                               3, C.byref(gs.ctxs), gs.lam, y1_ac, effort, dnb.data_ptr(),
+                                               out.data_ptr())
+            assert st == 0, vp8a.load().vp8a_last_error()
+        for _ in range(args.warmup):
+            call()
+        ctx.synchronize()
+        ts = []
+        for _ in range(args.steps):
+            with torch.cuda.stream(gs.stream):
+                flush.fill_(1)
+            s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s_.record(gs.stream)
+            call()
+            e_.record(gs.stream)
+            e_.synchronize()
+            ts.append(s_.elapsed_time(e_))
+        ms = float(np.median(ts))
+        o = np.frombuffer(out.cpu().numpy().tobytes(), abi.RD_INTER_DTYPE)
+        res[name] = {"ms": round(ms, 4), "mbs_per_s": round(N_MB / (ms / 1e3), 1),
+                     "mean_refs_searched": round(float(o["n_searched"].mean()), 3),
+                     "mean_sad": round(float(o["sad"].mean()), 1)}
+    ms_plain = None
+    ts = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(gs.stream):
+            flush.fill_(1)
+        s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s_.record(gs.stream)
+        gs.run_analysis()
+        e_.record(gs.stream)
+        e_.synchronize()
+        ts.append(s_.elapsed_time(e_))
+    ms_plain = float(np.median(ts))
+    del out, dnb, flush
+    ctx.close()
+    return {"case": "rd", "size": "%dx%d" % (W, H), "unit": "MB/s", "qi": QI, "y1_ac": int(y1_ac), "refs": 3,
+            "efforts": res, "exhaustive_analysis_ms": round(ms_plain, 4),
+            "note": "RD-effort inter search per MB given its census neighbours (one warp per MB, no wavefront); "
+                    "the exhaustive analysis (the metric's search) timed beside it"}
+
+
 def batched_predict(ctx, vp8a, torch, split):
     """vp8a_predict_inter_mb (or _split_mv) over 8 frames' worth of MBs at
     random positions of random MB-padded reference planes of the --size grid,
@@ -1274,7 +1330,7 @@ def main():
     ap.add_argument("--no-parity", action="store_true", help="skip the step's parity check against the oracle")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--case", choices=["arnr", "analysis", "lf", "recon", "predict", "predict_mb", "predict_split",
-                                       "batch", "learned", "lp_conv"],
+                                       "batch", "learned", "lp_conv", "rd"],
                     help="profile one stage alone, or (batch) the batched many-stream path")
     ap.add_argument("--streams", type=int, default=48, help="streams of the batch case")
     ap.add_argument("--train-steps", type=int, default=300, help="training steps of the learned case")
@@ -1289,6 +1345,8 @@ def main():
         res = learned_arm(args)
     elif args.case == "lp_conv":
         res = lp_conv_arm(args)
+    elif args.case == "rd":
+        res = rd_arm(args)
     elif args.case:
         res = case_arm(args)
     else:

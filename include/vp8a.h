@@ -267,6 +267,29 @@ uint64_t vp8a_ctx_launch_count(const vp8a_ctx* ctx);
  * finds the row above behind, which makes the timeout path testable without
  * hanging or faulting anything. Applies to calls issued after it. */
 vp8a_status vp8a_ctx_set_wait_limit(vp8a_ctx* ctx, uint64_t polls);
+/* No counterpart in the reference (launch shapes of the device kernels).
+ * With autotune on (the default) the loop-filter sweep times every launch
+ * shape that fits — passes per CTA, threads per CTA, next-MB prefetch — on
+ * the first scored sweep of each picture shape and keeps the fastest for
+ * that shape in the context (the first call takes longer); off, a cost
+ * model picks. Results never depend on the shape. */
+vp8a_status vp8a_ctx_set_autotune(vp8a_ctx* ctx, uint32_t on);
+/* No counterpart in the reference. On (the default), the inter analysis
+ * first builds each reference's 16 quarter-pel sub-pel planes (every
+ * §18.3 sample at even eighth-pel fractions, over the MB-padded plane plus
+ * a 32-pixel border) in a parallel pass, and its half- and quarter-pel
+ * refinements read their predictions from them; off, it synthesises each
+ * candidate's prediction inside the wavefront. The results are the same;
+ * on costs 16 planes of device scratch per reference during the call. */
+vp8a_status vp8a_ctx_set_subpel_planes(vp8a_ctx* ctx, uint32_t on);
+/* Forces the loop-filter sweep's launch shape (for tests): `passes` per
+ * CTA (1-3; 0 = back to automatic), `threads` per CTA, `prefetch` 0/1. A
+ * sweep whose picture the shape does not fit returns
+ * VP8A_E_INVALID_ARGUMENT. */
+vp8a_status vp8a_ctx_force_sweep_layout(vp8a_ctx* ctx, uint32_t passes, uint32_t threads, uint32_t prefetch);
+/* The last sweep's launch shape: out[0] passes per CTA, out[1] threads per
+ * CTA, out[2] prefetch, out[3] CTAs per SM (0: rings in global memory). */
+vp8a_status vp8a_ctx_last_sweep_layout(const vp8a_ctx* ctx, uint32_t out[4]);
 /* Text of the last error on this thread ("" if none). */
 const char* vp8a_last_error(void);
 /* ABI version of this header (major << 16 | minor). */
@@ -326,7 +349,11 @@ vp8a_status vp8a_motion_descent(vp8a_ctx* ctx, const vp8a_luma_ref* ref,
  * per MB. The MB-row wavefront runs on the device: MB (r, c) starts once
  * MB (r-1, c) is decided (its census neighbours are the above, left and
  * above-left MBs; the reference's row contract also waits for the
- * above-right MB, which only its intra candidates read). */
+ * above-right MB, which only its intra candidates read). A row's wait for
+ * the row above is bounded (vp8a_ctx_set_wait_limit); when it runs out the
+ * call returns VP8A_E_DEVICE_TIMEOUT if any buffer was host memory (the call
+ * then waits for its kernel anyway), and otherwise stays asynchronous and
+ * the next vp8a_ctx_synchronize returns it. */
 vp8a_status vp8a_analyse_inter_frame(vp8a_ctx* ctx, const vp8a_i420* frame,
                                      const vp8a_planes* refs, const uint8_t* ref_ids,
                                      uint32_t n_refs, const vp8a_mv_contexts* mv_contexts,
@@ -455,6 +482,16 @@ vp8a_status vp8a_build_arnr_altref(vp8a_ctx* ctx, const vp8a_i420* frames, uint3
                                    uint32_t center, uint32_t strength, uint8_t* y_out,
                                    uint8_t* u_out, uint8_t* v_out);
 
+/* build_arnr_altref (src/arnr.rs:476) written straight into MB-padded
+ * planes, the KeyframePlanes layout (src/frame.rs:123) an encoder keeps its
+ * ALTREF reference in: `out` has mb_cols = ceil(w/16), mb_rows = ceil(h/16)
+ * and its own row pitches; the visible anchor is the one
+ * vp8a_build_arnr_altref returns, and the padding columns and rows repeat
+ * the last visible column and row (the edge replication of an MB-padded
+ * reference). The blend kernel writes the padding itself. */
+vp8a_status vp8a_build_arnr_altref_planes(vp8a_ctx* ctx, const vp8a_i420* frames, uint32_t n,
+                                          uint32_t center, uint32_t strength, const vp8a_planes* out);
+
 /* ------------------------------------------------------- §15 loop filter */
 
 /* filter_inter_frame_flags (src/loop_filter.rs:1364) / filter_frame_flags
@@ -580,6 +617,19 @@ typedef struct vp8a_arnr_job {
  * job's (frame, strip of blocks) and one blend launch over every job's
  * blocks. */
 vp8a_status vp8a_build_arnr_altrefs(vp8a_ctx* ctx, const vp8a_arnr_job* jobs, uint32_t n_jobs);
+
+/* One vp8a_build_arnr_altref_planes call's arguments. */
+typedef struct vp8a_arnr_planes_job {
+  const vp8a_i420* frames;  /* n frames of one size */
+  uint32_t n;
+  uint32_t center;
+  uint32_t strength;
+  vp8a_planes out;          /* MB-padded output planes (written) */
+} vp8a_arnr_planes_job;
+
+/* vp8a_build_arnr_altref_planes for every job (launches as
+ * vp8a_build_arnr_altrefs). */
+vp8a_status vp8a_build_arnr_altrefs_planes(vp8a_ctx* ctx, const vp8a_arnr_planes_job* jobs, uint32_t n_jobs);
 
 /* One vp8a_reconstruct_inter_frame call's arguments (`recon` is written). */
 typedef struct vp8a_recon_job {

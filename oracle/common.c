@@ -74,6 +74,7 @@ size_t vo_type_size(int which) {
     case 16: return sizeof(vp8a_recon_job);
     case 17: return sizeof(vp8a_sweep_job);
     case 18: return sizeof(vp8a_frame_header);
+    case 19: return sizeof(vp8a_arnr_planes_job);
     default: return 0;
   }
 }

@@ -132,7 +132,7 @@ def type_sizes():
     names = ["vp8a_mv", "vp8a_search_result", "vp8a_luma_ref", "vp8a_i420", "vp8a_planes", "vp8a_mv_contexts",
              "vp8a_mb_decision", "vp8a_ref_search", "vp8a_mb_lf_info", "vp8a_filter_config", "vp8a_source",
              "vp8a_mb_info", "vp8a_rd_inter", "vp8a_quant_indices", "vp8a_analysis_job", "vp8a_arnr_job",
-             "vp8a_recon_job", "vp8a_sweep_job", "vp8a_frame_header"]
+             "vp8a_recon_job", "vp8a_sweep_job", "vp8a_frame_header", "vp8a_arnr_planes_job"]
     return {n: int(lib.vo_type_size(i)) for i, n in enumerate(names)}
 
 

@@ -61,6 +61,11 @@ struct AnArgs {
   vp8a_ref_search* trace;
   unsigned long long spin_limit;
   int words;  // reference planes allow 32-bit loads (4-byte aligned base and stride)
+  // The 16 sub-pel planes of each reference (subpel_planes_kernel), or
+  // null: plane (fx, fy) of reference k starts at spl[k] + (fy / 2 * 4 +
+  // fx / 2) * sp_plane, pixel (x, y) at ((y + SPB) * sp_pitch + x + SPB).
+  const uint8_t* spl[MAX_REFS];
+  uint64_t sp_pitch, sp_plane;
 };
 
 // ------------------------------------------------------------- staging
@@ -723,6 +728,103 @@ __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// ------------------------------------------------------ sub-pel planes
+//
+// The §18.3 sub-pel sample at integer position (x, y) with eighth-pel
+// fraction (fx, fy) depends only on the edge-clamped reference around it:
+// a horizontal six-tap pass over rows y - 2 .. y + 3 (skipped when fx is
+// 0), the 8-bit intermediate, then a vertical pass (skipped when fy is 0)
+// — the two-pass listing of sixtap_mb_luma (src/motion_comp.rs:1018-1057)
+// with its identity elision, whatever block the sample belongs to. The
+// luma vectors of the analysis have even eighth-pel fractions, so 16
+// planes (fx, fy in {0, 2, 4, 6}) hold every sample its half- and
+// quarter-pel refinements read. A parallel pre-pass builds them over the
+// MB-padded plane plus a border of SPB pixels; the wavefront's refinement
+// steps then read each candidate's 16 x 16 prediction as plain bytes
+// instead of synthesising it in the per-MB critical path. Candidates whose
+// block leaves the border keep the in-kernel synthesis.
+constexpr int SPB = 32;                  // border around the MB-padded plane
+constexpr int SP_TW = 64, SP_TH = 32;    // pre-pass output tile
+
+struct SubpelArgs {
+  const uint8_t* ref;
+  uint64_t stride;
+  int pw, ph;  // MB-padded plane (the clamp bounds)
+  uint8_t* out;
+  uint64_t pitch, plane;
+};
+
+// One CTA per 64 x 32 output tile of all 16 planes of one reference.
+__global__ void __launch_bounds__(256) subpel_planes_kernel(SubpelArgs a) {
+  __shared__ uint8_t E[SP_TH + 5][SP_TW + 8];
+  __shared__ __align__(4) uint8_t Hs[SP_TH + 5][SP_TW];
+  const int tid = threadIdx.x;
+  const int tx0 = (int)blockIdx.x * SP_TW - SPB, ty0 = (int)blockIdx.y * SP_TH - SPB;
+  // The edge-clamped reference under the tile and its six-tap reach.
+  for (int i = tid; i < (SP_TH + 5) * (SP_TW + 5); i += 256) {
+    const int r = i / (SP_TW + 5), c = i - r * (SP_TW + 5);
+    const int y = clampi(ty0 - 2 + r, 0, a.ph - 1), x = clampi(tx0 - 2 + c, 0, a.pw - 1);
+    E[r][c] = __ldg(a.ref + (size_t)y * a.stride + x);
+  }
+  __syncthreads();
+  for (int fxi = 0; fxi < 4; fxi++) {
+    const int* fh = c_sixtap[2 * fxi];
+    for (int i = tid; i < (SP_TH + 5) * SP_TW; i += 256) {
+      const int r = i / SP_TW, c = i - r * SP_TW;
+      const uint8_t* p = &E[r][c];
+      Hs[r][c] = fxi ? (uint8_t)interp6(fh, p[0], p[1], p[2], p[3], p[4], p[5]) : p[2];
+    }
+    __syncthreads();
+    for (int fyi = 0; fyi < 4; fyi++) {
+      const int* fv = c_sixtap[2 * fyi];
+      uint8_t* op = a.out + (size_t)(fyi * 4 + fxi) * a.plane + (size_t)(ty0 + SPB) * a.pitch + (tx0 + SPB);
+      for (int w = tid; w < SP_TH * SP_TW / 4; w += 256) {
+        const int r = w / (SP_TW / 4), c = 4 * (w - r * (SP_TW / 4));
+        uint32_t o = 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const int v = fyi ? interp6(fv, Hs[r][c + j], Hs[r + 1][c + j], Hs[r + 2][c + j], Hs[r + 3][c + j],
+                                      Hs[r + 4][c + j], Hs[r + 5][c + j])
+                            : Hs[r + 2][c + j];
+          o |= (uint32_t)v << (8 * j);
+        }
+        *reinterpret_cast<uint32_t*>(op + (size_t)r * a.pitch + c) = o;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Sub-pel plane geometry of a reference: row pitch and plane size in bytes
+// (whole pre-pass tiles, so the kernel needs no bounds checks).
+__host__ __device__ inline uint64_t sp_pitch_of(int pw) { return (uint64_t)((pw + 2 * SPB + SP_TW - 1) / SP_TW * SP_TW); }
+__host__ __device__ inline int sp_rows_of(int ph) { return (ph + 2 * SPB + SP_TH - 1) / SP_TH * SP_TH; }
+
+// Whether a 16 x 16 block at (ix, iy) lies inside the planes' extent.
+__device__ __forceinline__ bool sp_inside(const MePlane& P, int ix, int iy) {
+  return ix >= -SPB && iy >= -SPB && ix + 16 <= P.width + SPB && iy + 16 <= P.height + SPB;
+}
+
+// Row `row` of the 16 x 16 block at (ix, iy) of a sub-pel plane against the
+// source row, summed over the half-warp (every lane of it gets the SAD).
+// The five aligned words cover the sixteen bytes; the plane's row pitch
+// leaves at least SPB bytes after the last block, so they stay inside it.
+__device__ __forceinline__ uint32_t sp_block_sad(const uint8_t* plane, uint64_t pitch, int ix, int iy,
+                                                 const uint8_t* src, int row) {
+  const uint8_t* p = plane + (size_t)(iy + SPB + row) * pitch + (ix + SPB);
+  const uintptr_t ad = (uintptr_t)p;
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(ad & ~(uintptr_t)3);
+  const unsigned sh = (unsigned)(ad & 3) * 8u;
+  const uint32_t w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2), w3 = __ldg(w + 3), w4 = __ldg(w + 4);
+  const uint32_t* s = reinterpret_cast<const uint32_t*>(src + row * 16);
+  uint32_t sad = __vsadu4(__funnelshift_r(w0, w1, sh), s[0]) + __vsadu4(__funnelshift_r(w1, w2, sh), s[1]) +
+                 __vsadu4(__funnelshift_r(w2, w3, sh), s[2]) + __vsadu4(__funnelshift_r(w3, w4, sh), s[3]);
+  const unsigned hm = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
+#pragma unroll
+  for (int o = 8; o >= 1; o >>= 1) sad += __shfl_xor_sync(hm, sad, o);
+  return sad;
+}
+
 // ------------------------------------------------------ sub-pel stages
 
 // Offsets (row, col) of the eight refinement candidates in the reference's
@@ -1115,17 +1217,31 @@ __global__ void __launch_bounds__(AN_THREADS, 2)
         // candidate is clamped.
         const vp8a_mv hc = mo.whole.mv;
         const int hbx = mbx + hc.col / 4 - plan.wx0, hby = mby + hc.row / 4 - plan.wy0;
-        const bool planes = hc.row >= -1020 && hc.row <= 1020 && hc.col >= -1020 && hc.col <= 1020 &&
-                            !(hc.row & 3) && !(hc.col & 3) && hbx >= 3 && hby >= 3 && hbx + 19 <= WS &&
-                            hby + 19 <= WS;
-        if (planes) {
-          half_planes_hv(R.ws, hbx, hby, mt, MAIN_THREADS);
-          main_sync();
-          half_planes_d(R.ws, mt, MAIN_THREADS);
-          main_sync();
-          for (int q = slot; q < 8; q += MAIN_WARPS) {
-            const uint32_t sv = half_cand_sad(R.ws, q, src, lane);
-            if (lane == 0) cand_sad[q] = sv;
+        const bool whole_c = hc.row >= -1020 && hc.row <= 1020 && hc.col >= -1020 && hc.col <= 1020 &&
+                             !(hc.row & 3) && !(hc.col & 3);
+        const uint8_t* spb = a.spl[k];
+        const int hix = mbx + hc.col / 4, hiy = mby + hc.row / 4;
+        const bool gplanes = spb != nullptr && whole_c && sp_inside(P, hix - 1, hiy - 1) && sp_inside(P, hix, hiy);
+        const bool planes = whole_c && hbx >= 3 && hby >= 3 && hbx + 19 <= WS && hby + 19 <= WS;
+        if (gplanes || planes) {
+          if (gplanes) {
+            // Candidate q's prediction is a block of the precomputed plane
+            // (fx, fy) = (4 if dc, 4 if dr), one block row per thread.
+            if (mt < 128) {
+              const int q = mt >> 4, dr = cand_dr(q), dc = cand_dc(q);
+              const uint32_t sv = sp_block_sad(spb + (size_t)((dr ? 8 : 0) + (dc ? 2 : 0)) * a.sp_plane, a.sp_pitch,
+                                               hix + (dc < 0 ? -1 : 0), hiy + (dr < 0 ? -1 : 0), src, mt & 15);
+              if ((mt & 15) == 0) cand_sad[q] = sv;
+            }
+          } else {
+            half_planes_hv(R.ws, hbx, hby, mt, MAIN_THREADS);
+            main_sync();
+            half_planes_d(R.ws, mt, MAIN_THREADS);
+            main_sync();
+            for (int q = slot; q < 8; q += MAIN_WARPS) {
+              const uint32_t sv = half_cand_sad(R.ws, q, src, lane);
+              if (lane == 0) cand_sad[q] = sv;
+            }
           }
           main_sync();
           if (mt == 0) {
@@ -1151,7 +1267,22 @@ __global__ void __launch_bounds__(AN_THREADS, 2)
         // quarter_pixel_refine_luma around the half-pel result; the centre's
         // SAD is the half-pel result's.
         const vp8a_mv qc = mo.half.mv;
-        if (s_qok) {
+        // The eight candidates' blocks span the integer offsets of the
+        // columns qc.col - 1 .. qc.col + 1 and rows qc.row - 1 .. qc.row + 1.
+        const bool gq = spb != nullptr &&
+                        sp_inside(P, mbx + (eighth(clamp_component(qc.col - 1)) >> 3),
+                                  mby + (eighth(clamp_component(qc.row - 1)) >> 3)) &&
+                        sp_inside(P, mbx + (eighth(clamp_component(qc.col + 1)) >> 3),
+                                  mby + (eighth(clamp_component(qc.row + 1)) >> 3));
+        if (gq) {
+          if (mt < 128) {
+            const int q = mt >> 4;
+            const int er = eighth(clamp_component(qc.row + cand_dr(q))), ec = eighth(clamp_component(qc.col + cand_dc(q)));
+            const uint32_t sv = sp_block_sad(spb + (size_t)((er & 7) / 2 * 4 + (ec & 7) / 2) * a.sp_plane, a.sp_pitch,
+                                             mbx + (ec >> 3), mby + (er >> 3), src, mt & 15);
+            if ((mt & 15) == 0) cand_sad[q] = sv;
+          }
+        } else if (s_qok) {
           uint8_t* qh = R.ws.temp;  // the six-tap scratch and half planes are free now
           quarter_planes_h(R.ws.win, qh, s_qg, mt, MAIN_THREADS);
           main_sync();
@@ -1413,6 +1544,23 @@ vp8a_status prepare_job(vp8a_ctx* ctx, vp8a::Stager& st, MvBitsCache& mc, const 
   a.dec = (vp8a_mb_decision*)ddec;
   a.trace = (vp8a_ref_search*)dtr;
   a.spin_limit = ctx->wait_limit;
+  // The references' sub-pel planes, built before the wavefront starts.
+  if (ctx->subpel_planes) {
+    const int pw = mb_cols * 16, ph = mb_rows * 16;
+    a.sp_pitch = sp_pitch_of(pw);
+    a.sp_plane = a.sp_pitch * (uint64_t)sp_rows_of(ph);
+    void* dsp;
+    if ((s = st.scratch(16 * a.sp_plane * n_refs, &dsp)) != VP8A_OK) return s;
+    for (uint32_t k = 0; k < n_refs; k++) {
+      uint8_t* o = (uint8_t*)dsp + 16 * a.sp_plane * k;
+      const SubpelArgs sa{a.refs[k].plane, a.refs[k].stride, pw, ph, o, a.sp_pitch, a.sp_plane};
+      subpel_planes_kernel<<<dim3((unsigned)(a.sp_pitch / SP_TW), (unsigned)(sp_rows_of(ph) / SP_TH)), 256, 0,
+                             ctx->stream>>>(sa);
+      VP8A_CUDA(cudaGetLastError());
+      ctx->launches++;
+      a.spl[k] = o;
+    }
+  }
   a.words = 1;
   for (uint32_t k = 0; k < n_refs; k++)
     if ((uintptr_t)a.refs[k].plane % 4 != 0 || a.refs[k].stride % 4 != 0) a.words = 0;
@@ -1465,6 +1613,16 @@ vp8a_status launch_analysis(vp8a_ctx* ctx, int n_refs, const AnArgs& a0, const A
   return VP8A_OK;
 }
 
+// Ends an analysis call. With host buffers the call has waited for its
+// kernels (to copy the decisions back), so a wavefront wait that ran out is
+// reported now; with device buffers the call stays asynchronous and the
+// next vp8a_ctx_synchronize reports it.
+vp8a_status finish_analysis(vp8a_ctx* ctx, vp8a::Stager& st) {
+  vp8a_status s = st.finish();
+  if (s != VP8A_OK) return s;
+  return st.touched_host() ? vp8a::check_device_status(ctx) : VP8A_OK;
+}
+
 }  // namespace
 
 extern "C" vp8a_status vp8a_analyse_inter_frame(vp8a_ctx* ctx, const vp8a_i420* frame, const vp8a_planes* refs,
@@ -1482,8 +1640,7 @@ extern "C" vp8a_status vp8a_analyse_inter_frame(vp8a_ctx* ctx, const vp8a_i420* 
   vp8a_status s = prepare_job(ctx, st, mc, frame, refs, ref_ids, n_refs, mv_contexts, lambda, decisions, trace, &a);
   if (s != VP8A_OK) return s;
   if ((s = launch_analysis<false>(ctx, a.n_refs, a, nullptr, nullptr, a.mb_rows)) != VP8A_OK) return s;
-  if ((s = vp8a::check_device_status(ctx)) != VP8A_OK) return s;
-  return st.finish();
+  return finish_analysis(ctx, st);
 }
 
 extern "C" vp8a_status vp8a_analyse_inter_frames(vp8a_ctx* ctx, const vp8a_analysis_job* jobs, uint32_t n_jobs) {
@@ -1526,17 +1683,11 @@ extern "C" vp8a_status vp8a_analyse_inter_frames(vp8a_ctx* ctx, const vp8a_analy
       for (int r = 0; r < args[j].mb_rows; r++) items.push_back(q << 16 | (uint32_t)r);
     }
     void *dt, *di;
-    if ((s = st.scratch(sizeof(AnArgs) * table.size(), &dt)) != VP8A_OK) return s;
-    if ((s = st.scratch(sizeof(uint32_t) * items.size(), &di)) != VP8A_OK) return s;
-    VP8A_CUDA(cudaMemcpyAsync(dt, table.data(), sizeof(AnArgs) * table.size(), cudaMemcpyHostToDevice, ctx->stream));
-    VP8A_CUDA(cudaMemcpyAsync(di, items.data(), sizeof(uint32_t) * items.size(), cudaMemcpyHostToDevice,
-                              ctx->stream));
-    // The host tables go out of scope with this iteration.
-    VP8A_CUDA(cudaStreamSynchronize(ctx->stream));
+    if ((s = st.upload(table.data(), sizeof(AnArgs) * table.size(), &dt)) != VP8A_OK) return s;
+    if ((s = st.upload(items.data(), sizeof(uint32_t) * items.size(), &di)) != VP8A_OK) return s;
     if ((s = launch_analysis<true>(ctx, nr, table[0], (const AnArgs*)dt, (const uint32_t*)di, (int)items.size())) !=
         VP8A_OK)
       return s;
   }
-  if ((s = vp8a::check_device_status(ctx)) != VP8A_OK) return s;
-  return st.finish();
+  return finish_analysis(ctx, st);
 }

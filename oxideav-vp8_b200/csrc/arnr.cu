@@ -211,6 +211,9 @@ struct BlendArgs {
   uint8_t* y_out;
   uint8_t* u_out;
   uint8_t* v_out;
+  uint64_t ys, cs;  // output row pitches
+  int ow, oh;       // output luma extent (w x h, or the MB-padded size)
+  int ocw, och;     // output chroma extent
 };
 
 constexpr int BLEND_BLOCKS = 2;                 // 16x16 blocks per CTA step
@@ -336,11 +339,23 @@ __device__ __forceinline__ void blend_body(const BlendArgs& a, uint32_t cta, uin
     uint32_t o = 0;
 #pragma unroll
     for (int j = 0; j < 4; j++) o |= udiv_small(acc[j] + ws[j] / 2, ws[j]) << (8 * j);
-    uint8_t* op = plane == 0 ? a.y_out + (size_t)y * a.w : (plane == 1 ? a.u_out : a.v_out) + (size_t)y * a.cw;
-    if (nvalid == 4 && a.aligned_out) {
-      *reinterpret_cast<uint32_t*>(op + x) = o;
-    } else {
-      for (int j = 0; j < nvalid; j++) op[x + j] = (uint8_t)(o >> (8 * j));
+    uint8_t* const base = plane == 0 ? a.y_out : (plane == 1 ? a.u_out : a.v_out);
+    const uint64_t os = plane == 0 ? a.ys : a.cs;
+    const int opw = plane == 0 ? a.ow : a.ocw, oph = plane == 0 ? a.oh : a.och;
+    const uint8_t last = (uint8_t)(o >> (8 * (nvalid - 1)));
+    // The visible pixels, then (MB-padded output) the edge replication of
+    // the last column into the padding columns and of the last row into the
+    // padding rows, as the MB-padded reference planes hold them.
+    const int rows = y == ph - 1 ? oph - y : 1;
+    for (int rr = 0; rr < rows; rr++) {
+      uint8_t* op = base + (size_t)(y + rr) * os;
+      if (nvalid == 4 && a.aligned_out) {
+        *reinterpret_cast<uint32_t*>(op + x) = o;
+      } else {
+        for (int j = 0; j < nvalid; j++) op[x + j] = (uint8_t)(o >> (8 * j));
+      }
+      if (x + nvalid == pw)
+        for (int c = pw; c < opw; c++) op[c] = last;
     }
   }
 }
@@ -369,11 +384,21 @@ struct ArnrPrepared {
   uint32_t search_ctas, blend_ctas;
 };
 
-// `hf` holds the host copy of the frame table until the call's finish().
+// Where an anchor goes: packed visible planes (row pitch = width, the
+// ArnrPicture layout), or MB-padded planes with their own pitches (the
+// KeyframePlanes layout of a reference, padding edge-replicated).
+struct ArnrOut {
+  uint8_t* y;
+  uint8_t* u;
+  uint8_t* v;
+  uint64_t ys, cs;        // 0: packed
+  uint32_t mb_cols, mb_rows;  // MB-padded output grid (0: packed)
+};
+
+// `hf` is the host copy of the frame table (uploaded before this returns).
 vp8a_status prepare_arnr(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_i420* frames, uint32_t n, uint32_t center,
-                         uint32_t strength, uint8_t* y_out, uint8_t* u_out, uint8_t* v_out,
-                         std::vector<ArnrFrame>& hf, ArnrPrepared* P) {
-  if (!frames || !y_out || !u_out || !v_out) {
+                         uint32_t strength, const ArnrOut& out, std::vector<ArnrFrame>& hf, ArnrPrepared* P) {
+  if (!frames || !out.y || !out.u || !out.v) {
     vp8a::set_error("null argument");
     return VP8A_E_INVALID_ARGUMENT;
   }
@@ -413,13 +438,23 @@ vp8a_status prepare_arnr(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_i420* frame
     hf[i].uv_stride = frames[i].uv_stride;
   }
   void* dframes = nullptr;
-  if ((s = st.scratch(sizeof(ArnrFrame) * n, &dframes)) != VP8A_OK) return s;
-  VP8A_CUDA(cudaMemcpyAsync(dframes, hf.data(), sizeof(ArnrFrame) * n, cudaMemcpyHostToDevice, ctx->stream));
-  st.force_sync();  // finish() waits for the copy before hf goes
+  if ((s = st.upload(hf.data(), sizeof(ArnrFrame) * n, &dframes)) != VP8A_OK) return s;
+  const bool padded = out.mb_cols != 0;
+  const int ow = padded ? (int)out.mb_cols * 16 : w, oh = padded ? (int)out.mb_rows * 16 : h;
+  const int ocw = padded ? (int)out.mb_cols * 8 : cw, och = padded ? (int)out.mb_rows * 8 : ch;
+  const uint64_t ys = padded ? out.ys : (uint64_t)w, cs = padded ? out.cs : (uint64_t)cw;
+  if (padded && ((int)out.mb_cols != (w + 15) / 16 || (int)out.mb_rows != (h + 15) / 16)) {
+    vp8a::set_error("output planes do not match the frames' MB grid");
+    return VP8A_E_REFERENCE_DIMENSIONS_MISMATCH;
+  }
+  if (padded && (ys < (uint64_t)ow || cs < (uint64_t)ocw)) {
+    vp8a::set_error("output stride below the MB-padded width");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
   void *dy, *du, *dv;
-  if ((s = st.out(y_out, (size_t)w * h, &dy)) != VP8A_OK) return s;
-  if ((s = st.out(u_out, (size_t)cw * ch, &du)) != VP8A_OK) return s;
-  if ((s = st.out(v_out, (size_t)cw * ch, &dv)) != VP8A_OK) return s;
+  if ((s = st.out(out.y, ys * (size_t)(oh - 1) + ow, &dy)) != VP8A_OK) return s;
+  if ((s = st.out(out.u, cs * (size_t)(och - 1) + ocw, &du)) != VP8A_OK) return s;
+  if ((s = st.out(out.v, cs * (size_t)(och - 1) + ocw, &dv)) != VP8A_OK) return s;
 
   const int bcols = (w + 15) / 16, brows = (h + 15) / 16;
   const bool filter = strength != 0 && n >= 2;
@@ -434,10 +469,10 @@ vp8a_status prepare_arnr(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_i420* frame
   for (uint32_t i = 0; i < n; i++)
     aligned_in &= (((uintptr_t)hf[i].y | (uintptr_t)hf[i].u | (uintptr_t)hf[i].v | hf[i].y_stride |
                      hf[i].uv_stride) & 3) == 0;
-  const int aligned_out = (((uintptr_t)dy | (uintptr_t)du | (uintptr_t)dv | (uintptr_t)w | (uintptr_t)cw) & 3) == 0;
+  const int aligned_out = (((uintptr_t)dy | (uintptr_t)du | (uintptr_t)dv | (uintptr_t)ys | (uintptr_t)cs) & 3) == 0;
   P->ba = BlendArgs{(const ArnrFrame*)dframes, (const BlockMv*)dmv, filter ? n : 0u, filter ? center : 0u,
                     8u << str, w, h, cw, ch, bcols, brows, aligned_in, aligned_out,
-                    (uint8_t*)dy, (uint8_t*)du, (uint8_t*)dv};
+                    (uint8_t*)dy, (uint8_t*)du, (uint8_t*)dv, ys, cs, ow, oh, ocw, och};
   if (!filter) {
     // Pass-through (src/arnr.rs:527-529): the blend with no window frames
     // reproduces the centre exactly. The centre is frames[0] of a
@@ -453,9 +488,10 @@ vp8a_status prepare_arnr(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_i420* frame
 
 }  // namespace
 
-extern "C" vp8a_status vp8a_build_arnr_altref(vp8a_ctx* ctx, const vp8a_i420* frames, uint32_t n,
-                                              uint32_t center, uint32_t strength, uint8_t* y_out,
-                                              uint8_t* u_out, uint8_t* v_out) {
+namespace {
+
+vp8a_status build_one(vp8a_ctx* ctx, const vp8a_i420* frames, uint32_t n, uint32_t center, uint32_t strength,
+                      const ArnrOut& out) {
   if (!ctx) {
     vp8a::set_error("null argument");
     return VP8A_E_INVALID_ARGUMENT;
@@ -464,7 +500,7 @@ extern "C" vp8a_status vp8a_build_arnr_altref(vp8a_ctx* ctx, const vp8a_i420* fr
   vp8a::Stager st(ctx);
   ArnrPrepared P;
   std::vector<ArnrFrame> hf;
-  vp8a_status s = prepare_arnr(ctx, st, frames, n, center, strength, y_out, u_out, v_out, hf, &P);
+  vp8a_status s = prepare_arnr(ctx, st, frames, n, center, strength, out, hf, &P);
   if (s != VP8A_OK) return s;
   if (P.search_ctas) {
     arnr_search_kernel<<<P.search_ctas, STRIP * 32, 0, ctx->stream>>>(P.sa);
@@ -477,7 +513,33 @@ extern "C" vp8a_status vp8a_build_arnr_altref(vp8a_ctx* ctx, const vp8a_i420* fr
   return st.finish();
 }
 
-extern "C" vp8a_status vp8a_build_arnr_altrefs(vp8a_ctx* ctx, const vp8a_arnr_job* jobs, uint32_t n_jobs) {
+ArnrOut planes_out(const vp8a_planes* p) {
+  return ArnrOut{(uint8_t*)p->y, (uint8_t*)p->u, (uint8_t*)p->v, p->y_stride, p->uv_stride, p->mb_cols, p->mb_rows};
+}
+
+}  // namespace
+
+extern "C" vp8a_status vp8a_build_arnr_altref(vp8a_ctx* ctx, const vp8a_i420* frames, uint32_t n,
+                                              uint32_t center, uint32_t strength, uint8_t* y_out,
+                                              uint8_t* u_out, uint8_t* v_out) {
+  return build_one(ctx, frames, n, center, strength, ArnrOut{y_out, u_out, v_out, 0, 0, 0, 0});
+}
+
+extern "C" vp8a_status vp8a_build_arnr_altref_planes(vp8a_ctx* ctx, const vp8a_i420* frames, uint32_t n,
+                                                     uint32_t center, uint32_t strength, const vp8a_planes* out) {
+  if (!out || out->mb_cols == 0 || out->mb_rows == 0) {
+    vp8a::set_error("null or empty output planes");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  return build_one(ctx, frames, n, center, strength, planes_out(out));
+}
+
+namespace {
+
+// Every job's search in one launch and every job's blend in another; `job`
+// gives job j's (frames, n, center, strength) and output.
+template <class Job, class OutOf>
+vp8a_status build_batch(vp8a_ctx* ctx, const Job* jobs, uint32_t n_jobs, OutOf out_of) {
   if (!ctx || (!jobs && n_jobs)) {
     vp8a::set_error("null argument");
     return VP8A_E_INVALID_ARGUMENT;
@@ -495,11 +557,9 @@ extern "C" vp8a_status vp8a_build_arnr_altrefs(vp8a_ctx* ctx, const vp8a_arnr_jo
   std::vector<uint32_t> s_start{0}, b_start{0};
   std::vector<std::vector<ArnrFrame>> hf(n_jobs);
   for (uint32_t j = 0; j < n_jobs; j++) {
-    const vp8a_arnr_job& J = jobs[j];
+    const Job& J = jobs[j];
     ArnrPrepared P;
-    if ((s = prepare_arnr(ctx, st, J.frames, J.n, J.center, J.strength, J.y_out, J.u_out, J.v_out, hf[j], &P)) !=
-        VP8A_OK)
-      return s;
+    if ((s = prepare_arnr(ctx, st, J.frames, J.n, J.center, J.strength, out_of(J), hf[j], &P)) != VP8A_OK) return s;
     if (P.search_ctas) {
       sj.push_back(P.sa);
       s_start.push_back(s_start.back() + P.search_ctas);
@@ -516,9 +576,7 @@ extern "C" vp8a_status vp8a_build_arnr_altrefs(vp8a_ctx* ctx, const vp8a_arnr_jo
   memcpy(blob.data() + o_ba, bj.data(), sizeof(BlendArgs) * bj.size());
   memcpy(blob.data() + o_bs, b_start.data(), sizeof(uint32_t) * b_start.size());
   void* d;
-  if ((s = st.scratch(total, &d)) != VP8A_OK) return s;
-  VP8A_CUDA(cudaMemcpyAsync(d, blob.data(), total, cudaMemcpyHostToDevice, ctx->stream));
-  VP8A_CUDA(cudaStreamSynchronize(ctx->stream));  // the host blob goes out of scope
+  if ((s = st.upload(blob.data(), total, &d)) != VP8A_OK) return s;
   const uint8_t* db = (const uint8_t*)d;
   if (!sj.empty()) {
     arnr_search_batch_kernel<<<s_start.back(), STRIP * 32, 0, ctx->stream>>>(
@@ -531,4 +589,21 @@ extern "C" vp8a_status vp8a_build_arnr_altrefs(vp8a_ctx* ctx, const vp8a_arnr_jo
   VP8A_CUDA(cudaGetLastError());
   ctx->launches++;
   return st.finish();
+}
+
+}  // namespace
+
+extern "C" vp8a_status vp8a_build_arnr_altrefs(vp8a_ctx* ctx, const vp8a_arnr_job* jobs, uint32_t n_jobs) {
+  return build_batch(ctx, jobs, n_jobs,
+                     [](const vp8a_arnr_job& J) { return ArnrOut{J.y_out, J.u_out, J.v_out, 0, 0, 0, 0}; });
+}
+
+extern "C" vp8a_status vp8a_build_arnr_altrefs_planes(vp8a_ctx* ctx, const vp8a_arnr_planes_job* jobs,
+                                                      uint32_t n_jobs) {
+  for (uint32_t j = 0; jobs && j < n_jobs; j++)
+    if (jobs[j].out.mb_cols == 0 || jobs[j].out.mb_rows == 0) {
+      vp8a::set_error("empty output planes");
+      return VP8A_E_INVALID_ARGUMENT;
+    }
+  return build_batch(ctx, jobs, n_jobs, [](const vp8a_arnr_planes_job& J) { return planes_out(&J.out); });
 }

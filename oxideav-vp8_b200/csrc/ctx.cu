@@ -56,6 +56,24 @@ vp8a_status Stager::scratch(size_t bytes, void** dev) {
   return VP8A_OK;
 }
 
+vp8a_status Stager::upload(const void* host, size_t bytes, void** dev) {
+  vp8a_status st = scratch(bytes, dev);
+  if (st != VP8A_OK || bytes == 0) return st;
+  if (!ctx_->up_host || bytes > vp8a_ctx::UP_SLOT_BYTES) {
+    // Pageable source: the call waits for the copy before it returns.
+    VP8A_CUDA(cudaMemcpyAsync(*dev, host, bytes, cudaMemcpyHostToDevice, ctx_->stream));
+    VP8A_CUDA(cudaStreamSynchronize(ctx_->stream));
+    return VP8A_OK;
+  }
+  const unsigned k = ctx_->up_next++ % vp8a_ctx::UP_SLOTS;
+  VP8A_CUDA(cudaEventSynchronize(ctx_->up_ev[k]));  // that slot's previous upload is done
+  uint8_t* slot = ctx_->up_host + (size_t)k * vp8a_ctx::UP_SLOT_BYTES;
+  memcpy(slot, host, bytes);
+  VP8A_CUDA(cudaMemcpyAsync(*dev, slot, bytes, cudaMemcpyHostToDevice, ctx_->stream));
+  VP8A_CUDA(cudaEventRecord(ctx_->up_ev[k], ctx_->stream));
+  return VP8A_OK;
+}
+
 vp8a_status Stager::read_to_host(const void* p, size_t bytes, void* host_dst) {
   if (!p) {
     set_error("null input buffer");
@@ -231,6 +249,17 @@ vp8a_status vp8a_ctx_create(int device, vp8a_ctx** out) {
     vp8a_ctx_destroy(c);
     return cuda_fail(se, "context buffers");
   }
+  if ((se = cudaHostAlloc((void**)&c->up_host, vp8a_ctx::UP_SLOTS * vp8a_ctx::UP_SLOT_BYTES,
+                          cudaHostAllocDefault)) != cudaSuccess) {
+    c->up_host = nullptr;
+    vp8a_ctx_destroy(c);
+    return cuda_fail(se, "pinned upload ring");
+  }
+  for (int k = 0; k < vp8a_ctx::UP_SLOTS; k++)
+    if ((se = cudaEventCreateWithFlags(&c->up_ev[k], cudaEventDisableTiming)) != cudaSuccess) {
+      vp8a_ctx_destroy(c);
+      return cuda_fail(se, "upload events");
+    }
   *out = c;
   return VP8A_OK;
 }
@@ -241,6 +270,9 @@ vp8a_status vp8a_ctx_destroy(vp8a_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->d_bit_cost) cudaFree(ctx->d_bit_cost);
+  for (int k = 0; k < vp8a_ctx::UP_SLOTS; k++)
+    if (ctx->up_ev[k]) cudaEventDestroy(ctx->up_ev[k]);
+  if (ctx->up_host) cudaFreeHost(ctx->up_host);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return VP8A_OK;
@@ -260,6 +292,35 @@ uint64_t vp8a_ctx_launch_count(const vp8a_ctx* ctx) { return ctx ? ctx->launches
 vp8a_status vp8a_ctx_set_wait_limit(vp8a_ctx* ctx, uint64_t polls) {
   if (!ctx) return VP8A_E_INVALID_ARGUMENT;
   ctx->wait_limit = polls;
+  return VP8A_OK;
+}
+
+vp8a_status vp8a_ctx_set_subpel_planes(vp8a_ctx* ctx, uint32_t on) {
+  if (!ctx) return VP8A_E_INVALID_ARGUMENT;
+  ctx->subpel_planes = on != 0;
+  return VP8A_OK;
+}
+
+vp8a_status vp8a_ctx_set_autotune(vp8a_ctx* ctx, uint32_t on) {
+  if (!ctx) return VP8A_E_INVALID_ARGUMENT;
+  ctx->autotune = on != 0;
+  return VP8A_OK;
+}
+
+vp8a_status vp8a_ctx_force_sweep_layout(vp8a_ctx* ctx, uint32_t passes, uint32_t threads, uint32_t prefetch) {
+  if (!ctx || passes > 3 || (passes && (threads < 32 || threads > 1024 || threads % 32 != 0))) {
+    set_error("passes must be 0-3 and threads a multiple of 32 in 32..1024");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  ctx->force_layout[0] = (int)passes;
+  ctx->force_layout[1] = (int)threads;
+  ctx->force_layout[2] = prefetch != 0;
+  return VP8A_OK;
+}
+
+vp8a_status vp8a_ctx_last_sweep_layout(const vp8a_ctx* ctx, uint32_t out[4]) {
+  if (!ctx || !out) return VP8A_E_INVALID_ARGUMENT;
+  for (int i = 0; i < 4; i++) out[i] = (uint32_t)ctx->last_layout[i];
   return VP8A_OK;
 }
 

@@ -924,9 +924,7 @@ vp8a_status stage_lf(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_planes* planes,
   memcpy(blob.data() + o_foff, foff.data(), sizeof(int32_t) * (steps + 1));
   if (!fin.empty()) memcpy(blob.data() + o_fin, fin.data(), sizeof(uint16_t) * fin.size());
   void* dblob;
-  if ((s = st.scratch(total, &dblob)) != VP8A_OK) return s;
-  VP8A_CUDA(cudaMemcpyAsync(dblob, blob.data(), total, cudaMemcpyHostToDevice, ctx->stream));
-  VP8A_CUDA(cudaStreamSynchronize(ctx->stream));  // the host blob goes out of scope
+  if ((s = st.upload(blob.data(), total, &dblob)) != VP8A_OK) return s;
   const uint8_t* db = (const uint8_t*)dblob;
   a.row_t0 = (const int16_t*)db;
   a.row_top = db + o_top;
@@ -978,75 +976,169 @@ size_t sweep_smem(int nc, int ring, bool pre, int threads) {
   return (size_t)nc * ring + (pre ? (size_t)(threads / 16) * sizeof(Stage) : 0);
 }
 
-// The layout a sweep of `n` candidates runs with: candidates per CTA and
-// the prefetch, among those whose shared memory fits, by an estimate of
-// the time: whole waves of CTAs over the GPU x candidates per CTA (a CTA's
-// steps carry every candidate's filtering), 15 % more without the
-// prefetch and 20 % less per candidate when a CTA carries several (their
-// filtering shares each step's barrier and loads) — factors measured on
-// the 1080p and 640x368 sweeps. Returns false when no layout fits.
+// The layouts a sweep of `n` candidates can run with: candidates (passes)
+// per CTA, threads per CTA and the prefetch, among those whose shared
+// memory fits and that can be resident. A CTA's steps carry every one of
+// its candidates' filtering, and a half-warp takes several MBs of a step
+// when the CTA has fewer half-warps than the step has MBs; fewer threads
+// per CTA let more CTAs share an SM, so one CTA's step barrier is covered
+// by the others' work.
 struct SweepLayout {
   int nc;
   bool pre;
   size_t smem;
+  int threads;
+  int per_sm;
 };
-bool pick_layout(vp8a_ctx* ctx, int n, int ring, bool pre_ok, int threads, bool batch, SweepLayout* out) {
+
+const void* sweep_kernel_of(int nc, bool batch) {
+  return batch ? (nc == 3 ? (const void*)lf_sweep_batch_kernel<3>
+                          : nc == 2 ? (const void*)lf_sweep_batch_kernel<2> : (const void*)lf_sweep_batch_kernel<1>)
+               : (nc == 3 ? (const void*)lf_sweep_kernel<3>
+                          : nc == 2 ? (const void*)lf_sweep_kernel<2> : (const void*)lf_sweep_kernel<1>);
+}
+
+vp8a_status sweep_layouts(vp8a_ctx* ctx, int n, int ring, bool pre_ok, int threads_full, bool batch,
+                          std::vector<SweepLayout>* out) {
+  out->clear();
   int max_smem = 0;
   VP8A_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-  double best = 1e30;
-  bool found = false;
+  const int tcands[] = {1024, 768, 512, 384, 352, 256, 192, 128};
   for (int nc = 3; nc >= 1; nc--) {
     if (nc > 1 && n < nc) continue;
+    const void* k = sweep_kernel_of(nc, batch);
     cudaFuncAttributes fa;
-    const void* k = batch ? (nc == 3 ? (const void*)lf_sweep_batch_kernel<3>
-                                     : nc == 2 ? (const void*)lf_sweep_batch_kernel<2>
-                                               : (const void*)lf_sweep_batch_kernel<1>)
-                          : (nc == 3 ? (const void*)lf_sweep_kernel<3>
-                                     : nc == 2 ? (const void*)lf_sweep_kernel<2> : (const void*)lf_sweep_kernel<1>);
-    if (cudaFuncGetAttributes(&fa, k) != cudaSuccess) return false;
+    VP8A_CUDA(cudaFuncGetAttributes(&fa, k));
     for (int pre = pre_ok ? 1 : 0; pre >= 0; pre--) {
-      const size_t smem = sweep_smem(nc, ring, pre, threads);
-      if (smem + fa.sharedSizeBytes + 1024 > (size_t)max_smem) continue;
-      if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return false;
-      int per_sm = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem) != cudaSuccess) return false;
-      if (per_sm < 1) continue;
-      const long ctas = (n + nc - 1) / nc, slots = (long)ctx->sm_count * per_sm;
-      const double cost = (double)((ctas + slots - 1) / slots) * nc * (pre ? 1.0 : 1.15) * (nc > 1 ? 0.8 : 1.0);
-      if (cost < best) {
-        best = cost;
-        *out = SweepLayout{nc, pre != 0, smem};
-        found = true;
+      int last_per_sm = 0;
+      for (int ti = 0; ti < (int)(sizeof tcands / sizeof tcands[0]); ti++) {
+        const int t = ti == 0 ? threads_full : std::min(threads_full, tcands[ti]);
+        if (ti > 0 && t >= threads_full) continue;
+        const size_t smem = sweep_smem(nc, ring, pre, t);
+        if (smem + fa.sharedSizeBytes + 1024 > (size_t)max_smem) continue;
+        VP8A_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        VP8A_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, t, smem));
+        if (per_sm < 1) continue;
+        // Fewer threads only pay when more CTAs share an SM.
+        if (ti > 0 && per_sm <= last_per_sm) continue;
+        last_per_sm = per_sm;
+        out->push_back(SweepLayout{nc, pre != 0, smem, t, per_sm});
       }
+    }
+  }
+  return VP8A_OK;
+}
+
+// The cost model's pick among `ls` (full thread count only): whole waves of
+// CTAs over the GPU x candidates per CTA, 15 % more without the prefetch
+// and 20 % less per candidate when a CTA carries several (their filtering
+// shares each step's barrier and loads) — factors measured on the 1080p
+// and 640x368 sweeps.
+bool model_layout(vp8a_ctx* ctx, int n, int threads_full, const std::vector<SweepLayout>& ls, SweepLayout* out) {
+  double best = 1e30;
+  bool found = false;
+  for (const SweepLayout& L : ls) {
+    if (L.threads != threads_full) continue;
+    const long ctas = (n + L.nc - 1) / L.nc, slots = (long)ctx->sm_count * L.per_sm;
+    const double cost =
+        (double)((ctas + slots - 1) / slots) * L.nc * (L.pre ? 1.0 : 1.15) * (L.nc > 1 ? 0.8 : 1.0);
+    if (cost < best) {
+      best = cost;
+      *out = L;
+      found = true;
     }
   }
   return found;
 }
 
+bool pick_layout(vp8a_ctx* ctx, int n, int ring, bool pre_ok, int threads, bool batch, SweepLayout* out) {
+  std::vector<SweepLayout> ls;
+  if (sweep_layouts(ctx, n, ring, pre_ok, threads, batch, &ls) != VP8A_OK) return false;
+  return model_layout(ctx, n, threads, ls, out);
+}
+
 // Launch the sweep over `n` candidates (pairs of level, sharpness) already
 // in device memory at a.cands, with the slot rings and staging in shared
-// memory (pick_layout); otherwise, when `gst` can provide them, with the
-// rings in global memory. The prefetch needs planes whose rows allow
-// aligned 16- and 8-byte asynchronous copies.
+// memory (a layout of sweep_layouts: forced, measured or modelled);
+// otherwise, when `gst` can provide them, with the rings in global memory.
+// The prefetch needs planes whose rows allow aligned 16- and 8-byte
+// asynchronous copies.
 vp8a_status run_sweep(vp8a_ctx* ctx, LfArgs a, int n, vp8a::Stager* gst) {
   if (n == 0) return VP8A_OK;
   a.n_cands = n;
   a.ring_bytes = (a.row_set ? a.n_sets : a.mb_rows) * RING * SLOT_STRIDE;
   int max_smem = 0;
   VP8A_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-  const int threads = std::min(1024, std::max(32, (16 * a.max_active + 31) / 32 * 32));
+  const int threads_full = std::min(1024, std::max(32, (16 * a.max_active + 31) / 32 * 32));
   auto al = [](const void* p, uint64_t stride, unsigned k) { return ((uintptr_t)p % k == 0) && (stride % k == 0); };
   bool pre_ok = al(a.y, a.ys, 16) && al(a.u, a.cs, 8) && al(a.v, a.cs, 8) && (uintptr_t)a.mbs % 8 == 0;
   if (a.ssd_out) pre_ok = pre_ok && al(a.sy, a.sys, 16) && al(a.su, a.scs, 8) && al(a.sv, a.scs, 8);
   cudaFuncAttributes f1;
   VP8A_CUDA(cudaFuncGetAttributes(&f1, lf_sweep_kernel<1>));
-  SweepLayout L;
-  if (pick_layout(ctx, n, a.ring_bytes, pre_ok, threads, false, &L)) {
-    a.smem_slots = 1;
-    a.gslots = nullptr;
-    a.prefetch = L.pre;
-    a.stage_off = L.nc * a.ring_bytes;
-    return launch_variant(ctx, L.nc, (unsigned)((n + L.nc - 1) / L.nc), threads, L.smem, a, nullptr, nullptr, 0);
+  std::vector<SweepLayout> ls;
+  vp8a_status s = sweep_layouts(ctx, n, a.ring_bytes, pre_ok, threads_full, false, &ls);
+  if (s != VP8A_OK) return s;
+  auto launch = [&](const SweepLayout& L) {
+    LfArgs b = a;
+    b.smem_slots = 1;
+    b.gslots = nullptr;
+    b.prefetch = L.pre;
+    b.stage_off = L.nc * a.ring_bytes;
+    ctx->last_layout[0] = L.nc;
+    ctx->last_layout[1] = L.threads;
+    ctx->last_layout[2] = L.pre;
+    ctx->last_layout[3] = L.per_sm;
+    return launch_variant(ctx, L.nc, (unsigned)((n + L.nc - 1) / L.nc), L.threads, L.smem, b, nullptr, nullptr, 0);
+  };
+  if (!ls.empty()) {
+    if (ctx->force_layout[0]) {
+      // A forced layout (tests): it must be one of the feasible ones.
+      for (const SweepLayout& x : ls)
+        if (x.nc == ctx->force_layout[0] && x.threads == ctx->force_layout[1] && (int)x.pre == ctx->force_layout[2])
+          return launch(x);
+      vp8a::set_error("the forced sweep layout does not fit this picture");
+      return VP8A_E_INVALID_ARGUMENT;
+    }
+    SweepLayout L = ls[0];
+    // Filtering into the planes (apply mode) or a handful of candidates:
+    // the model; a scored sweep: the measured choice for this shape.
+    if (!ctx->autotune || !a.ssd_out || n < 16 || ls.size() == 1) {
+      model_layout(ctx, n, threads_full, ls, &L);
+      return launch(L);
+    }
+    const std::array<int64_t, 6> key{a.mb_cols, a.mb_rows, n, a.steps, (int64_t)pre_ok, a.row_set != nullptr};
+    auto it = ctx->lf_tuned.find(key);
+    if (it == ctx->lf_tuned.end()) {
+      // Time every feasible layout on this call's own inputs (a scored
+      // sweep only writes its table, so repeating it changes nothing) and
+      // keep the fastest.
+      cudaEvent_t e0, e1;
+      VP8A_CUDA(cudaEventCreate(&e0));
+      VP8A_CUDA(cudaEventCreate(&e1));
+      float best = 1e30f;
+      std::array<int, 3> pick{ls[0].nc, ls[0].threads, (int)ls[0].pre};
+      for (const SweepLayout& x : ls) {
+        if ((s = launch(x)) != VP8A_OK) break;  // warm
+        if ((s = vp8a::cuda_ok(cudaEventRecord(e0, ctx->stream), "cudaEventRecord")) != VP8A_OK) break;
+        if ((s = launch(x)) != VP8A_OK) break;
+        if ((s = vp8a::cuda_ok(cudaEventRecord(e1, ctx->stream), "cudaEventRecord")) != VP8A_OK) break;
+        if ((s = vp8a::cuda_ok(cudaEventSynchronize(e1), "cudaEventSynchronize")) != VP8A_OK) break;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) {
+          best = ms;
+          pick = {x.nc, x.threads, (int)x.pre};
+        }
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      if (s != VP8A_OK) return s;
+      it = ctx->lf_tuned.emplace(key, pick).first;
+    }
+    for (const SweepLayout& x : ls)
+      if (x.nc == it->second[0] && x.threads == it->second[1] && (int)x.pre == it->second[2]) L = x;
+    return launch(L);
   }
   if (!gst) {
     vp8a::set_error("the MB rows' slot rings do not fit in shared memory");
@@ -1054,13 +1146,17 @@ vp8a_status run_sweep(vp8a_ctx* ctx, LfArgs a, int n, vp8a::Stager* gst) {
   }
   // Rings in global memory, one set per candidate; staging still shared.
   void* g;
-  vp8a_status s;
   if ((s = gst->scratch((size_t)a.ring_bytes * n, &g)) != VP8A_OK) return s;
   a.smem_slots = 0;
   a.gslots = (uint8_t*)g;
-  a.prefetch = pre_ok && sweep_smem(0, 0, true, threads) + f1.sharedSizeBytes + 1024 <= (size_t)max_smem;
+  a.prefetch = pre_ok && sweep_smem(0, 0, true, threads_full) + f1.sharedSizeBytes + 1024 <= (size_t)max_smem;
   a.stage_off = 0;
-  return launch_variant(ctx, 1, (unsigned)n, threads, sweep_smem(0, 0, a.prefetch, threads), a, nullptr, nullptr, 0);
+  ctx->last_layout[0] = 1;
+  ctx->last_layout[1] = threads_full;
+  ctx->last_layout[2] = a.prefetch;
+  ctx->last_layout[3] = 0;
+  return launch_variant(ctx, 1, (unsigned)n, threads_full, sweep_smem(0, 0, a.prefetch, threads_full), a, nullptr,
+                        nullptr, 0);
 }
 
 // The whole 64 x 8 grid as distinct filter passes. Two sharpness values
@@ -1146,9 +1242,7 @@ vp8a_status upload_grid(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_filter_confi
   memcpy(blob.data() + 2 * n, masks.data(), n);
   void* d;
   vp8a_status s;
-  if ((s = st.scratch(blob.size(), &d)) != VP8A_OK) return s;
-  VP8A_CUDA(cudaMemcpyAsync(d, blob.data(), blob.size(), cudaMemcpyHostToDevice, ctx->stream));
-  VP8A_CUDA(cudaStreamSynchronize(ctx->stream));  // the host blob goes out of scope
+  if ((s = st.upload(blob.data(), blob.size(), &d)) != VP8A_OK) return s;
   a->cands = (const uint8_t*)d;
   a->cand_mask = (const uint8_t*)d + 2 * n;
   a->n_cands = (int)n;
@@ -1159,8 +1253,7 @@ vp8a_status launch_sweep(vp8a_ctx* ctx, vp8a::Stager& st, LfArgs a, const uint8_
   if (n == 0) return VP8A_OK;
   void* dc;
   vp8a_status s;
-  if ((s = st.scratch((size_t)n * 2, &dc)) != VP8A_OK) return s;
-  VP8A_CUDA(cudaMemcpyAsync(dc, cands, (size_t)n * 2, cudaMemcpyHostToDevice, ctx->stream));
+  if ((s = st.upload(cands, (size_t)n * 2, &dc)) != VP8A_OK) return s;
   a.cands = (const uint8_t*)dc;
   return run_sweep(ctx, a, n, &st);
 }
@@ -1315,7 +1408,6 @@ vp8a_status vp8a_filter_frame(vp8a_ctx* ctx, vp8a_planes* planes, const vp8a_mb_
   const uint8_t cand[2] = {config->loop_filter_level, config->sharpness_level};
   L.a.level0_unfiltered = 0;
   if ((s = launch_sweep(ctx, st, L.a, cand, 1)) != VP8A_OK) return s;
-  st.force_sync();  // `cand` must outlive its async copy
   return st.finish();
 }
 
@@ -1463,7 +1555,7 @@ vp8a_status vp8a_filter_sweeps(vp8a_ctx* ctx, const vp8a_sweep_job* jobs, uint32
     // (each CTA takes `nc` candidates of one job).
     long n_all = 0;
     for (uint32_t j : group) n_all += args[j].n_cands;
-    SweepLayout L{1, pre, sweep_smem(1, max_ring, pre, threads)};
+    SweepLayout L{1, pre, sweep_smem(1, max_ring, pre, threads), threads, 1};
     if (!pick_layout(ctx, (int)std::min<long>(n_all, 1 << 30), max_ring, pre, threads, true, &L)) {
       vp8a::set_error("no sweep layout fits in shared memory");
       return VP8A_E_CUDA;
@@ -1487,9 +1579,7 @@ vp8a_status vp8a_filter_sweeps(vp8a_ctx* ctx, const vp8a_sweep_job* jobs, uint32
     memcpy(blob.data(), table.data(), o_start);
     memcpy(blob.data() + o_start, start.data(), sizeof(uint32_t) * start.size());
     void* d;
-    if ((s = st.scratch(bytes, &d)) != VP8A_OK) return s;
-    VP8A_CUDA(cudaMemcpyAsync(d, blob.data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
-    VP8A_CUDA(cudaStreamSynchronize(ctx->stream));  // the host tables go out of scope
+    if ((s = st.upload(blob.data(), bytes, &d)) != VP8A_OK) return s;
     if ((s = launch_variant(ctx, nc, start.back(), threads, total, table[0], (const LfArgs*)d,
                             (const uint32_t*)((const uint8_t*)d + o_start), (int)table.size())) != VP8A_OK)
       return s;

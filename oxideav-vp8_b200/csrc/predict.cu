@@ -661,9 +661,7 @@ vp8a_status predict_frames(vp8a_ctx* ctx, Stager& st, const FramePrediction* fps
   memcpy(blob.data() + o_start, start.data(), sizeof(uint32_t) * start.size());
   void* d;
   vp8a_status s;
-  if ((s = st.scratch(total, &d)) != VP8A_OK) return s;
-  VP8A_CUDA(cudaMemcpyAsync(d, blob.data(), total, cudaMemcpyHostToDevice, ctx->stream));
-  VP8A_CUDA(cudaStreamSynchronize(ctx->stream));  // the host blob goes out of scope
+  if ((s = st.upload(blob.data(), total, &d)) != VP8A_OK) return s;
   predict_frames_kernel<<<start.back(), PR_THREADS, 0, ctx->stream>>>(
       (const PredArgs*)d, (const uint32_t*)((const uint8_t*)d + o_start), (int)table.size());
   VP8A_CUDA(cudaGetLastError());

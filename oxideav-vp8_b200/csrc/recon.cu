@@ -550,9 +550,7 @@ vp8a_status vp8a_reconstruct_inter_frames(vp8a_ctx* ctx, const vp8a_recon_job* j
   memcpy(blob.data(), table.data(), o_start);
   memcpy(blob.data() + o_start, start.data(), sizeof(uint32_t) * start.size());
   void* d;
-  if ((s = st.scratch(total, &d)) != VP8A_OK) return s;
-  VP8A_CUDA(cudaMemcpyAsync(d, blob.data(), total, cudaMemcpyHostToDevice, ctx->stream));
-  VP8A_CUDA(cudaStreamSynchronize(ctx->stream));  // the host blob goes out of scope
+  if ((s = st.upload(blob.data(), total, &d)) != VP8A_OK) return s;
   recon_frames_kernel<<<start.back(), RC_WARPS * 32, 0, ctx->stream>>>(
       (const RcArgs*)d, (const uint32_t*)((const uint8_t*)d + o_start), (int)n_jobs);
   VP8A_CUDA(cudaGetLastError());

@@ -3,8 +3,10 @@
 
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cstdint>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -24,12 +26,35 @@ struct vp8a_ctx {
   uint64_t wait_limit = 1ull << 24;
   // Device copy of the 256-entry -log2(p/256) bit-cost table (f64).
   double* d_bit_cost = nullptr;
+  // Pinned host ring for the small tables a call builds on the host
+  // (schedules, job tables, candidate lists): a table is copied into slot k
+  // and uploaded asynchronously, so the call never waits for the GPU to
+  // take it; slot k is reused only once the event recorded behind its last
+  // upload has completed.
+  static constexpr int UP_SLOTS = 16;
+  static constexpr size_t UP_SLOT_BYTES = 256 << 10;
+  uint8_t* up_host = nullptr;
+  cudaEvent_t up_ev[UP_SLOTS] = {};
+  unsigned up_next = 0;
+  // Launch-shape choice of the loop-filter sweep: measured on first use
+  // per picture shape (autotune) or by the cost model; a forced layout
+  // (tests) overrides both. Cache: shape key -> (passes per CTA, threads,
+  // prefetch). last_layout: the last sweep's (passes, threads, prefetch,
+  // CTAs per SM).
+  bool autotune = true;
+  // The analysis reads its half- and quarter-pel predictions from planes
+  // precomputed per call (vp8a_ctx_set_subpel_planes).
+  bool subpel_planes = true;
+  int force_layout[3] = {0, 0, 0};
+  std::map<std::array<int64_t, 6>, std::array<int, 3>> lf_tuned;
+  int last_layout[4] = {0, 0, 0, 0};
 };
 
 namespace vp8a {
 
 void set_error(const std::string& msg);
 vp8a_status cuda_fail(cudaError_t e, const char* what);
+inline vp8a_status cuda_ok(cudaError_t e, const char* what) { return e == cudaSuccess ? VP8A_OK : cuda_fail(e, what); }
 
 #define VP8A_CUDA(call)                                        \
   do {                                                         \
@@ -54,6 +79,10 @@ class Stager {
   vp8a_status inout(void* p, size_t bytes, void** dev);
   // Scratch device memory owned by this call.
   vp8a_status scratch(size_t bytes, void** dev);
+  // Scratch device memory holding a copy of `bytes` host bytes (a table the
+  // call built). The host buffer may go away once this returns; the copy
+  // is stream-ordered and the call does not wait for it.
+  vp8a_status upload(const void* host, size_t bytes, void** dev);
   // Host copy of a small buffer that may be host or device memory (for
   // metadata the host logic itself reads, e.g. reference ids).
   vp8a_status read_to_host(const void* p, size_t bytes, void* host_dst);

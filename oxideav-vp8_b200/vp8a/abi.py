@@ -211,6 +211,13 @@ class ArnrJob(C.Structure):
                 ("y_out", C.c_void_p), ("u_out", C.c_void_p), ("v_out", C.c_void_p)]
 
 
+class ArnrPlanesJob(C.Structure):
+    """vp8a_arnr_planes_job: one vp8a_build_arnr_altref_planes call of a batch."""
+
+    _fields_ = [("frames", C.c_void_p), ("n", C.c_uint32), ("center", C.c_uint32), ("strength", C.c_uint32),
+                ("out", Planes)]
+
+
 class ReconJob(C.Structure):
     """vp8a_recon_job: one vp8a_reconstruct_inter_frame call of a batch."""
 
@@ -319,6 +326,7 @@ C_SIZES = {
     "vp8a_recon_job": 184,
     "vp8a_sweep_job": 152,
     "vp8a_frame_header": 52,
+    "vp8a_arnr_planes_job": 72,
 }
 
 
@@ -344,6 +352,7 @@ def check_layouts():
         "vp8a_recon_job": C.sizeof(ReconJob),
         "vp8a_sweep_job": C.sizeof(SweepJob),
         "vp8a_frame_header": C.sizeof(FrameHeader),
+        "vp8a_arnr_planes_job": C.sizeof(ArnrPlanesJob),
     }
     assert got == C_SIZES, (got, C_SIZES)
     return got

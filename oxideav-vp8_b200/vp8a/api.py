@@ -54,6 +54,25 @@ class Context:
     def synchronize(self):
         check(self._lib.vp8a_ctx_synchronize(self.handle), "vp8a_ctx_synchronize")
 
+    def set_subpel_planes(self, on):
+        """Precomputed sub-pel planes for the analysis refinements (default on)."""
+        check(self._lib.vp8a_ctx_set_subpel_planes(self.handle, int(bool(on))), "vp8a_ctx_set_subpel_planes")
+
+    def set_autotune(self, on):
+        """Measured (True, the default) or modelled launch shapes."""
+        check(self._lib.vp8a_ctx_set_autotune(self.handle, int(bool(on))), "vp8a_ctx_set_autotune")
+
+    def force_sweep_layout(self, passes, threads=0, prefetch=0):
+        """Force the loop-filter sweep's launch shape (passes 0 = automatic)."""
+        check(self._lib.vp8a_ctx_force_sweep_layout(self.handle, passes, threads, prefetch),
+              "vp8a_ctx_force_sweep_layout")
+
+    def last_sweep_layout(self):
+        """(passes per CTA, threads per CTA, prefetch, CTAs per SM) of the last sweep."""
+        out = (C.c_uint32 * 4)()
+        check(self._lib.vp8a_ctx_last_sweep_layout(self.handle, out), "vp8a_ctx_last_sweep_layout")
+        return tuple(int(x) for x in out)
+
     def set_wait_limit(self, polls):
         """Poll budget of the analysis wavefront waits (default 2**24)."""
         check(self._lib.vp8a_ctx_set_wait_limit(self.handle, int(polls)), "vp8a_ctx_set_wait_limit")
@@ -369,6 +388,25 @@ def build_arnr_altref(ctx, frames, center, strength=3):
     return y, u, v
 
 
+def build_arnr_altref_planes(ctx, frames, center, strength=3, out=None):
+    """build_arnr_altref (src/arnr.rs:476) into MB-padded planes
+    (vp8a_build_arnr_altref_planes): the anchor with its padding
+    edge-replicated, the layout of a reference. `out` = MB-padded (y, u, v)
+    to write (numpy or torch CUDA), else new numpy planes. Returns `out`."""
+    recs = [i420(*f) for f in frames]
+    arr = (abi.I420 * len(recs))(*recs)
+    shape_src = frames[center] if 0 <= center < len(frames) else frames[0]
+    h, w = shape_src[0].shape[0], shape_src[0].shape[1]
+    if out is None:
+        mbr, mbc = (h + 15) // 16, (w + 15) // 16
+        out = (np.zeros((mbr * 16, mbc * 16), np.uint8), np.zeros((mbr * 8, mbc * 8), np.uint8),
+               np.zeros((mbr * 8, mbc * 8), np.uint8))
+    p = planes(*out)
+    check(ctx._lib.vp8a_build_arnr_altref_planes(ctx.handle, C.cast(arr, C.c_void_p), len(recs), center, strength,
+                                                 C.byref(p)), "vp8a_build_arnr_altref_planes")
+    return out
+
+
 def filter_frame(ctx, recon, mbs, config):
     """filter_inter_frame_flags / filter_frame_flags
     (src/loop_filter.rs:1364, :2506) on a copy of `recon` (MB-padded
@@ -511,6 +549,24 @@ def build_arnr_altrefs(ctx, jobs):
         cj.append(abi.ArnrJob(C.cast(arr, C.c_void_p), len(recs), center, strength, ptr(y), ptr(u), ptr(v)))
         outs.append((y, u, v))
     _batch(ctx, "vp8a_build_arnr_altrefs", cj, "vp8a_build_arnr_altrefs")
+    return outs
+
+
+def build_arnr_altrefs_planes(ctx, jobs):
+    """vp8a_build_arnr_altrefs_planes: `jobs` = list of (frames, center,
+    strength). Returns each job's MB-padded (y, u, v) anchor."""
+    keep, cj, outs = [], [], []
+    for frames, center, strength in jobs:
+        recs = [i420(*f) for f in frames]
+        arr = (abi.I420 * len(recs))(*recs)
+        h, w = frames[0][0].shape[:2]
+        mbr, mbc = (h + 15) // 16, (w + 15) // 16
+        out = (np.zeros((mbr * 16, mbc * 16), np.uint8), np.zeros((mbr * 8, mbc * 8), np.uint8),
+               np.zeros((mbr * 8, mbc * 8), np.uint8))
+        keep.append(arr)
+        cj.append(abi.ArnrPlanesJob(C.cast(arr, C.c_void_p), len(recs), center, strength, planes(*out)))
+        outs.append(out)
+    _batch(ctx, "vp8a_build_arnr_altrefs_planes", cj, "vp8a_build_arnr_altrefs_planes")
     return outs
 
 

@@ -57,14 +57,45 @@ def nvcc():
 
 
 def build(force=False, verbose=False):
+    """Compiles each source to an object in parallel (objects under
+    vp8a/_build/, rebuilt only when a source or header is newer), then links
+    libvp8a.so."""
     if not force and up_to_date():
         return OUT
-    cmd = [nvcc()] + NVCC_FLAGS + ["-o", OUT + ".tmp"] + sources()
+    import concurrent.futures as cf
+
+    obj_dir = os.path.join(HERE, "_build")
+    os.makedirs(obj_dir, exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    headers = [p for p in deps() if p not in sources()]
+    newest_header = max((os.path.getmtime(p) for p in headers), default=0.0)
+    exe = nvcc()
+
+    def compile_one(src):
+        obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
+        if (not force and os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(src) and
+                os.path.getmtime(obj) >= newest_header):
+            return obj, None
+        cmd = [exe] + compile_flags + ["-c", "-o", obj + ".tmp", src]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            return obj, r.stdout + r.stderr
+        os.replace(obj + ".tmp", obj)
+        return obj, None
+
+    with cf.ThreadPoolExecutor(max_workers=max(1, min(len(sources()), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(compile_one, sources()))
+    errors = [e for _, e in results if e]
+    if errors:
+        raise RuntimeError("nvcc failed:\n" + "\n".join(errors))
+    cmd = [exe] + NVCC_FLAGS + ["-o", OUT + ".tmp"] + [o for o, _ in results]
     if verbose:
         print(" ".join(cmd))
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+        raise RuntimeError("nvcc link failed:\n" + r.stdout + r.stderr)
     os.replace(OUT + ".tmp", OUT)
     return OUT
 

@@ -22,6 +22,10 @@ PROTOTYPES = {
     "vp8a_ctx_synchronize": (C.c_int, [P]),
     "vp8a_ctx_launch_count": (C.c_uint64, [P]),
     "vp8a_ctx_set_wait_limit": (C.c_int, [P, C.c_uint64]),
+    "vp8a_ctx_set_autotune": (C.c_int, [P, U32]),
+    "vp8a_ctx_set_subpel_planes": (C.c_int, [P, U32]),
+    "vp8a_ctx_force_sweep_layout": (C.c_int, [P, U32, U32, U32]),
+    "vp8a_ctx_last_sweep_layout": (C.c_int, [P, P]),
     "vp8a_last_error": (C.c_char_p, []),
     "vp8a_abi_version": (U32, []),
     "vp8a_mb_luma_sad_at_mv": (C.c_int, [P, C.POINTER(abi.LumaRef), P, P, P, U32, P]),
@@ -36,6 +40,7 @@ PROTOTYPES = {
     "vp8a_rd_lambda": (C.c_double, [U32]),
     "vp8a_analyse_inter_frames": (C.c_int, [P, P, U32]),
     "vp8a_build_arnr_altrefs": (C.c_int, [P, P, U32]),
+    "vp8a_build_arnr_altrefs_planes": (C.c_int, [P, P, U32]),
     "vp8a_reconstruct_inter_frames": (C.c_int, [P, P, U32]),
     "vp8a_filter_sweeps": (C.c_int, [P, P, U32]),
     "vp8a_lp_windows": (C.c_int, [P, C.POINTER(abi.LumaRef), C.POINTER(abi.LumaRef), P, U32, P]),
@@ -62,6 +67,7 @@ PROTOTYPES = {
          C.POINTER(abi.Planes), P, P, P],
     ),
     "vp8a_build_arnr_altref": (C.c_int, [P, P, U32, U32, U32, P, P, P]),
+    "vp8a_build_arnr_altref_planes": (C.c_int, [P, P, U32, U32, U32, C.POINTER(abi.Planes)]),
     "vp8a_filter_frame": (C.c_int, [P, C.POINTER(abi.Planes), P, C.POINTER(abi.FilterConfig)]),
     "vp8a_reconstruction_ssd": (C.c_int, [P, C.POINTER(abi.Planes), C.POINTER(abi.Source), P]),
     "vp8a_filter_sweep": (

@@ -120,3 +120,21 @@ def test_analysis_and_lf_device_resident(ctx, oracle):
     assert st == 0, lib.vp8a_last_error()
     ctx.synchronize()
     assert (int(lv.item()), int(sh.item())) == want
+
+
+@pytest.mark.parametrize("planes", [True, False])
+def test_analysis_with_and_without_subpel_planes(oracle, planes):
+    # The half- and quarter-pel refinements read precomputed sub-pel planes
+    # (default) or synthesise each candidate in the wavefront; both give the
+    # oracle's decisions and traces. GOLDEN is four frames back (up to 32
+    # px of motion), which puts vectors near the frame edges.
+    frames, _ = synth.make_sequence(320, 240, 7, seed=57, pieces=6, occluders=5)
+    refs = refs_for(frames, 4)
+    ids = [abi.REF_LAST, abi.REF_GOLDEN, abi.REF_ALTREF]
+    lam = vp8a.rd_lambda(30)
+    want, wtr = oracle.analyse_inter_frame(frames[4], refs, ids, lam, trace=True)
+    with vp8a.Context(0) as c:
+        c.set_subpel_planes(planes)
+        got, gtr = vp8a.analyse_inter_frame(c, frames[4], refs, ids, lam, trace=True)
+    assert np.array_equal(gtr, wtr)
+    assert_same(got, want)

@@ -67,3 +67,36 @@ def test_arnr_errors(ctx):
 def test_arnr_1080p_lookahead7(ctx, oracle):
     frames, _ = synth.make_sequence(1920, 1080, 7, seed=5)
     assert same(vp8a.build_arnr_altref(ctx, frames, 3, 3), oracle.build_arnr_altref(frames, 3, 3, threads=8))
+
+
+@pytest.mark.parametrize("w,h", [(320, 240), (17, 9), (47, 33), (100, 18), (1920, 1080)])
+def test_arnr_into_mb_padded_planes(ctx, oracle, w, h):
+    # vp8a_build_arnr_altref_planes: the oracle's anchor, edge-replicated
+    # into the MB-padded layout of a reference (pad_to_mb), written by the
+    # blend kernel itself; planes with a row pitch wider than the padded
+    # width keep their extra bytes.
+    frames, _ = synth.make_sequence(w, h, 5, seed=w * 7 + h)
+    want = vp8a.pad_to_mb(*oracle.build_arnr_altref(frames, 2, 3, threads=8))
+    got = vp8a.build_arnr_altref_planes(ctx, frames, 2, 3)
+    assert same(got, want)
+    wide = [np.full((p.shape[0], p.shape[1] + 12), 7, np.uint8) for p in want]
+    vp8a.build_arnr_altref_planes(ctx, frames, 2, 3, out=[x[:, : p.shape[1]] for x, p in zip(wide, want)])
+    assert same([x[:, : p.shape[1]] for x, p in zip(wide, want)], want)
+    assert all((x[:, p.shape[1]:] == 7).all() for x, p in zip(wide, want))
+
+
+def test_arnr_batched_into_mb_padded_planes(ctx, oracle):
+    jobs = []
+    for i, (w, h) in enumerate([(176, 144), (64, 48), (47, 33)]):
+        frames, _ = synth.make_sequence(w, h, 5, seed=90 + i)
+        jobs.append((frames, 2 if i != 1 else 4, 3))
+    got = vp8a.build_arnr_altrefs_planes(ctx, jobs)
+    for (frames, center, strength), g in zip(jobs, got):
+        assert same(g, vp8a.pad_to_mb(*oracle.build_arnr_altref(frames, center, strength)))
+
+
+def test_arnr_planes_grid_mismatch(ctx):
+    frames, _ = synth.make_sequence(64, 48, 3, seed=4)
+    bad = (np.zeros((64, 64), np.uint8), np.zeros((32, 32), np.uint8), np.zeros((32, 32), np.uint8))
+    with pytest.raises(vp8a.Vp8aError, match="ReferenceDimensionsMismatch"):
+        vp8a.build_arnr_altref_planes(ctx, frames, 1, 3, out=bad)

@@ -183,3 +183,34 @@ def test_key_frame_auto_lf(ctx, oracle, size):
             oracle.select_filter_params_sampled(recon, m, base, src, er, sw, threads=8)
         assert vp8a.select_filter_params_key_frame(ctx, recon, m, base, src, sampled=False) == \
             oracle.select_filter_params(recon, m, base, src, threads=8)
+
+
+@pytest.mark.parametrize("size", [(640, 368), (1920, 1080)])
+def test_sweep_every_launch_shape_gives_the_same_table(oracle, size):
+    # The sweep's launch shape (passes per CTA, threads per CTA, prefetch) is
+    # picked by measurement or by the cost model; every shape must give the
+    # oracle's table.
+    src, recon, m = lf_case(*size, seed=size[0] // 8)
+    base = abi.filter_config(0, 0)
+    want = oracle.filter_sweep(recon, m, base, src, 0, threads=8)
+    ran = set()
+    with vp8a.Context(0) as c:
+        assert np.array_equal(vp8a.filter_sweep(c, recon, m, base, src, 0), want)
+        tuned = c.last_sweep_layout()
+        assert tuned[0] in (1, 2, 3) and tuned[3] >= 1
+        for passes in (1, 2, 3):
+            for threads in (1024, 768, 512, 384, 352, 256, 192, 128):
+                for pre in (0, 1):
+                    c.force_sweep_layout(passes, threads, pre)
+                    try:
+                        got = vp8a.filter_sweep(c, recon, m, base, src, 0)
+                    except vp8a.Vp8aError as e:
+                        assert e.status == abi.E_INVALID_ARGUMENT
+                        continue
+                    assert c.last_sweep_layout()[:3] == (passes, threads, pre)
+                    assert np.array_equal(got, want), (passes, threads, pre)
+                    ran.add((passes, threads, pre))
+        c.force_sweep_layout(0)
+        c.set_autotune(False)
+        assert np.array_equal(vp8a.filter_sweep(c, recon, m, base, src, 0), want)
+    assert len(ran) >= 4, ran

@@ -58,3 +58,24 @@ def test_rd_search_1080p_balanced(ctx, oracle):
     got = vp8a.rd_inter_search(ctx, frames[3], refs, [1, 2, 3], lam, 48, abi.EFFORT_BALANCED, nb)
     want = oracle.rd_inter_search(frames[3], refs, [1, 2, 3], lam, 48, abi.EFFORT_BALANCED, nb, threads=8)
     check(got, want)
+
+
+# The hand-derived known-answer cases (rd_kat_cases; their values are
+# asserted on the oracle in test_oracle_rd_search_kat.py) on the device:
+# every output field equal to the oracle's, and the key answers directly.
+@pytest.mark.parametrize("effort", [0, 1, 2, 3])
+def test_rd_search_known_answers_on_device(ctx, oracle, effort):
+    import rd_kat_cases as K
+
+    src, ref = K.ramp_case()
+    nb = K.intra_neighbours(K.RAMP_W // 16, K.RAMP_H // 16)
+    got = vp8a.rd_inter_search(ctx, src, [ref, ref], [1, 2], 0.5, 8, effort, nb)
+    check(got, oracle.rd_inter_search(src, [ref, ref], [1, 2], 0.5, 8, effort, nb))
+    f = K.mb_of(got, K.RAMP_MB)["found"][0]
+    assert (int(f["mv"]["col"]), int(f["sad"])) == K.RAMP_WHOLE[effort]
+    for half in (False, True):
+        fsrc, fref, fnb = K.far_case(5 if half else 3, half_pel_source=half)
+        got = vp8a.rd_inter_search(ctx, fsrc, [fref], [1], 0.5, 8, effort, fnb)
+        check(got, oracle.rd_inter_search(fsrc, [fref], [1], 0.5, 8, effort, fnb))
+        o = K.mb_of(got, K.FAR_MB)
+        assert int(o["found"][0]["mv"]["col"]) == 1020 and int(o["mv"]["col"]) != 1022

@@ -46,6 +46,40 @@ def test_analysis_wait_runs_out_and_the_context_recovers(oracle):
         assert same(got, want)
 
 
+def test_device_resident_analysis_reports_the_timeout_at_synchronize(oracle):
+    # With every buffer on the device the call is asynchronous: it returns
+    # OK and the next synchronize reports the wait that ran out.
+    import ctypes as C
+
+    import torch
+
+    frame, refs, ids, lam = case()
+    want = oracle.analyse_inter_frame(frame, refs, ids, lam, threads=4)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    cur = [d(p) for p in frame]
+    drefs = [[d(p) for p in r] for r in refs]
+    n = want.size
+    out = torch.zeros(n * abi.MB_DECISION_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    host_ids = np.array(ids, np.uint8)
+    torch.cuda.synchronize()
+    with vp8a.Context(0) as c:
+        lib = c._lib
+        f = vp8a.i420(*cur)
+        pl = (abi.Planes * 2)(*[vp8a.planes(*r) for r in drefs])
+        ctxs = abi.default_mv_contexts()
+        call = lambda: lib.vp8a_analyse_inter_frame(c.handle, C.byref(f), C.cast(pl, C.c_void_p),  # noqa: E731
+                                                    host_ids.ctypes.data, 2, C.byref(ctxs), lam, out.data_ptr(),
+                                                    None)
+        c.set_wait_limit(0)
+        assert call() == abi.OK
+        assert lib.vp8a_ctx_synchronize(c.handle) == abi.E_DEVICE_TIMEOUT
+        c.set_wait_limit(1 << 24)
+        assert call() == abi.OK
+        assert lib.vp8a_ctx_synchronize(c.handle) == abi.OK
+        got = np.frombuffer(out.cpu().numpy().tobytes(), abi.MB_DECISION_DTYPE).reshape(want.shape)
+        assert same(got, want)
+
+
 def test_batched_analysis_wait_runs_out_and_the_context_recovers(oracle):
     frame, refs, ids, lam = case()
     want = oracle.analyse_inter_frame(frame, refs, ids, lam, threads=4)
