@@ -669,6 +669,16 @@ typedef struct vp8a_sweep_job {
  * larger pictures otherwise run as their own launches). */
 vp8a_status vp8a_filter_sweeps(vp8a_ctx* ctx, const vp8a_sweep_job* jobs, uint32_t n_jobs);
 
+/* select_filter_params (src/loop_filter.rs:2047) for every job: the
+ * reference's walk — the coarse grid 0, 4, ..., 60, 63 at the base
+ * sharpness, the +-3 refine around its winner, the other sharpness values
+ * at a non-zero chosen level — with each stage of all jobs in one batched
+ * sweep launch. Whole frames only (every_rows 0); the jobs' ssd_out is not
+ * used (the walk keeps its tables in scratch). level_out[j] and
+ * sharpness_out[j] (host memory) receive job j's pair. */
+vp8a_status vp8a_select_filter_params_batch(vp8a_ctx* ctx, const vp8a_sweep_job* jobs, uint32_t n_jobs,
+                                            uint8_t* level_out, uint8_t* sharpness_out);
+
 /* ------------------------------------------- learned motion proposal
  *
  * No counterpart in the reference: the learned proposal the survey builds

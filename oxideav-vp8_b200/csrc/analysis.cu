@@ -796,8 +796,12 @@ __global__ void __launch_bounds__(256) subpel_planes_kernel(SubpelArgs a) {
 }
 
 // Sub-pel plane geometry of a reference: row pitch and plane size in bytes
-// (whole pre-pass tiles, so the kernel needs no bounds checks).
-__host__ __device__ inline uint64_t sp_pitch_of(int pw) { return (uint64_t)((pw + 2 * SPB + SP_TW - 1) / SP_TW * SP_TW); }
+// (whole pre-pass tiles, so the kernel needs no bounds checks). The pitch
+// keeps at least 16 bytes after the extent's last column, where the
+// aligned word reads of a block at the right edge end.
+__host__ __device__ inline uint64_t sp_pitch_of(int pw) {
+  return (uint64_t)((pw + 2 * SPB + 16 + SP_TW - 1) / SP_TW * SP_TW);
+}
 __host__ __device__ inline int sp_rows_of(int ph) { return (ph + 2 * SPB + SP_TH - 1) / SP_TH * SP_TH; }
 
 // Whether a 16 x 16 block at (ix, iy) lies inside the planes' extent.
@@ -807,8 +811,9 @@ __device__ __forceinline__ bool sp_inside(const MePlane& P, int ix, int iy) {
 
 // Row `row` of the 16 x 16 block at (ix, iy) of a sub-pel plane against the
 // source row, summed over the half-warp (every lane of it gets the SAD).
-// The five aligned words cover the sixteen bytes; the plane's row pitch
-// leaves at least SPB bytes after the last block, so they stay inside it.
+// The five aligned words cover the sixteen bytes and end at most 19 bytes
+// after the block's first column; the pitch's 16 spare bytes keep them
+// inside the row.
 __device__ __forceinline__ uint32_t sp_block_sad(const uint8_t* plane, uint64_t pitch, int ix, int iy,
                                                  const uint8_t* src, int row) {
   const uint8_t* p = plane + (size_t)(iy + SPB + row) * pitch + (ix + SPB);

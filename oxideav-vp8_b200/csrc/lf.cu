@@ -1485,36 +1485,12 @@ vp8a_status vp8a_filter_sweep_window(vp8a_ctx* ctx, const vp8a_planes* planes, c
   return st.finish();
 }
 
-vp8a_status vp8a_filter_sweeps(vp8a_ctx* ctx, const vp8a_sweep_job* jobs, uint32_t n_jobs) {
-  if (!ctx || (!jobs && n_jobs)) {
-    vp8a::set_error("null argument");
-    return VP8A_E_INVALID_ARGUMENT;
-  }
-  if (n_jobs > VP8A_MAX_BATCH_JOBS) {
-    vp8a::set_error("more jobs than VP8A_MAX_BATCH_JOBS");
-    return VP8A_E_INVALID_ARGUMENT;
-  }
-  if (n_jobs == 0) return VP8A_OK;
-  VP8A_CUDA(cudaSetDevice(ctx->device));
-  vp8a::Stager st(ctx);
+// Every job's candidates (a.cands / a.cand_mask / a.n_cands set, rings
+// sized) as one batched launch where their slot rings fit in shared memory
+// together, the rest as launches of their own.
+vp8a_status run_batch(vp8a_ctx* ctx, vp8a::Stager& st, std::vector<LfArgs>& args) {
+  const uint32_t n_jobs = (uint32_t)args.size();
   vp8a_status s;
-  std::vector<LfArgs> args(n_jobs);
-  for (uint32_t j = 0; j < n_jobs; j++) {
-    const vp8a_sweep_job& J = jobs[j];
-    if (!J.ssd_out) {
-      vp8a::set_error("null ssd_out");
-      return VP8A_E_INVALID_ARGUMENT;
-    }
-    LfInputs L;
-    if ((s = stage_lf(ctx, st, &J.planes, J.mbs, &J.base, &J.src, J.every_rows, false, &L)) != VP8A_OK) return s;
-    void* dt;
-    if ((s = st.out(J.ssd_out, 512 * sizeof(uint64_t), &dt)) != VP8A_OK) return s;
-    L.a.ssd_out = (uint64_t*)dt;
-    L.a.level0_unfiltered = 1;
-    if ((s = upload_grid(ctx, st, J.base, &L.a)) != VP8A_OK) return s;
-    L.a.ring_bytes = L.a.n_sets * RING * SLOT_STRIDE;
-    args[j] = L.a;
-  }
   // One launch for every job whose slot rings fit in shared memory (two
   // candidates per CTA when the largest job's pair fits, else one), with
   // the most half-warps any job needs; the rest run as their own launches.
@@ -1586,6 +1562,150 @@ vp8a_status vp8a_filter_sweeps(vp8a_ctx* ctx, const vp8a_sweep_job* jobs, uint32
   }
   for (uint32_t j : alone)
     if ((s = run_sweep(ctx, args[j], args[j].n_cands, &st)) != VP8A_OK) return s;
+  return VP8A_OK;
+}
+
+vp8a_status vp8a_filter_sweeps(vp8a_ctx* ctx, const vp8a_sweep_job* jobs, uint32_t n_jobs) {
+  if (!ctx || (!jobs && n_jobs)) {
+    vp8a::set_error("null argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (n_jobs > VP8A_MAX_BATCH_JOBS) {
+    vp8a::set_error("more jobs than VP8A_MAX_BATCH_JOBS");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (n_jobs == 0) return VP8A_OK;
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  vp8a_status s;
+  std::vector<LfArgs> args(n_jobs);
+  for (uint32_t j = 0; j < n_jobs; j++) {
+    const vp8a_sweep_job& J = jobs[j];
+    if (!J.ssd_out) {
+      vp8a::set_error("null ssd_out");
+      return VP8A_E_INVALID_ARGUMENT;
+    }
+    LfInputs L;
+    if ((s = stage_lf(ctx, st, &J.planes, J.mbs, &J.base, &J.src, J.every_rows, false, &L)) != VP8A_OK) return s;
+    void* dt;
+    if ((s = st.out(J.ssd_out, 512 * sizeof(uint64_t), &dt)) != VP8A_OK) return s;
+    L.a.ssd_out = (uint64_t*)dt;
+    L.a.level0_unfiltered = 1;
+    if ((s = upload_grid(ctx, st, J.base, &L.a)) != VP8A_OK) return s;
+    L.a.ring_bytes = L.a.n_sets * RING * SLOT_STRIDE;
+    args[j] = L.a;
+  }
+  if ((s = run_batch(ctx, st, args)) != VP8A_OK) return s;
+  return st.finish();
+}
+
+vp8a_status vp8a_select_filter_params_batch(vp8a_ctx* ctx, const vp8a_sweep_job* jobs, uint32_t n_jobs,
+                                            uint8_t* level_out, uint8_t* sharpness_out) {
+  if (!ctx || (!jobs && n_jobs) || (n_jobs && (!level_out || !sharpness_out))) {
+    vp8a::set_error("null argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (n_jobs > VP8A_MAX_BATCH_JOBS) {
+    vp8a::set_error("more jobs than VP8A_MAX_BATCH_JOBS");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (n_jobs == 0) return VP8A_OK;
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  vp8a_status s;
+  std::vector<LfArgs> base_args(n_jobs);
+  void* dt;
+  if ((s = st.scratch(512 * sizeof(uint64_t) * n_jobs, &dt)) != VP8A_OK) return s;
+  VP8A_CUDA(cudaMemsetAsync(dt, 0, 512 * sizeof(uint64_t) * n_jobs, ctx->stream));
+  std::vector<uint8_t> bs(n_jobs), best_level(n_jobs, 0), best_sharp(n_jobs);
+  std::vector<uint64_t> best(n_jobs), t((size_t)512 * n_jobs, 0);
+  for (uint32_t j = 0; j < n_jobs; j++) {
+    const vp8a_sweep_job& J = jobs[j];
+    if (J.every_rows != 0) {
+      vp8a::set_error("vp8a_select_filter_params_batch scores whole frames (every_rows must be 0)");
+      return VP8A_E_INVALID_ARGUMENT;
+    }
+    LfInputs Li;
+    if ((s = stage_lf(ctx, st, &J.planes, J.mbs, &J.base, &J.src, 0, false, &Li)) != VP8A_OK) return s;
+    Li.a.ssd_out = (uint64_t*)dt + (size_t)512 * j;
+    Li.a.level0_unfiltered = 1;
+    Li.a.cand_mask = nullptr;
+    Li.a.ring_bytes = Li.a.n_sets * RING * SLOT_STRIDE;
+    base_args[j] = Li.a;
+    bs[j] = J.base.sharpness_level > 7 ? 7 : J.base.sharpness_level;
+    best_sharp[j] = bs[j];
+  }
+  // One stage of the walk: job j scores the (level, sharpness) pairs in
+  // cands[j] (none: the job sits the stage out); the tables come back.
+  auto stage = [&](const std::vector<std::vector<uint8_t>>& cands) -> vp8a_status {
+    std::vector<LfArgs> args;
+    for (uint32_t j = 0; j < n_jobs; j++) {
+      if (cands[j].empty()) continue;
+      LfArgs a = base_args[j];
+      void* dc;
+      vp8a_status e = st.upload(cands[j].data(), cands[j].size(), &dc);
+      if (e != VP8A_OK) return e;
+      a.cands = (const uint8_t*)dc;
+      a.n_cands = (int)(cands[j].size() / 2);
+      args.push_back(a);
+    }
+    if (args.empty()) return VP8A_OK;
+    vp8a_status e = run_batch(ctx, st, args);
+    if (e != VP8A_OK) return e;
+    VP8A_CUDA(cudaMemcpyAsync(t.data(), dt, t.size() * sizeof(uint64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    VP8A_CUDA(cudaStreamSynchronize(ctx->stream));
+    return VP8A_OK;
+  };
+  std::vector<std::vector<uint8_t>> c(n_jobs);
+  // Stage 1: grid 0, 4, ..., 60, 63 at the base sharpness.
+  for (uint32_t j = 0; j < n_jobs; j++) {
+    for (int l = 0; l <= 60; l += 4) c[j].insert(c[j].end(), {(uint8_t)l, bs[j]});
+    c[j].insert(c[j].end(), {63, bs[j]});
+  }
+  if ((s = stage(c)) != VP8A_OK) return s;
+  for (uint32_t j = 0; j < n_jobs; j++) {
+    const uint64_t* tj = t.data() + (size_t)512 * j;
+    best[j] = tj[0 * 8 + bs[j]];
+    for (size_t i = 2; i < c[j].size(); i += 2)
+      if (tj[c[j][i] * 8 + bs[j]] < best[j]) {
+        best[j] = tj[c[j][i] * 8 + bs[j]];
+        best_level[j] = c[j][i];
+      }
+  }
+  // Refine +/-3 around each grid winner, excluding it.
+  for (uint32_t j = 0; j < n_jobs; j++) {
+    c[j].clear();
+    const int lo = best_level[j] >= 3 ? best_level[j] - 3 : 0, hi = std::min(63, best_level[j] + 3);
+    for (int l = lo; l <= hi; l++)
+      if (l != best_level[j]) c[j].insert(c[j].end(), {(uint8_t)l, bs[j]});
+  }
+  if ((s = stage(c)) != VP8A_OK) return s;
+  for (uint32_t j = 0; j < n_jobs; j++) {
+    const uint64_t* tj = t.data() + (size_t)512 * j;
+    for (size_t i = 0; i < c[j].size(); i += 2)
+      if (tj[c[j][i] * 8 + bs[j]] < best[j]) {
+        best[j] = tj[c[j][i] * 8 + bs[j]];
+        best_level[j] = c[j][i];
+      }
+  }
+  // Stage 2: the other sharpness values at each chosen non-zero level.
+  for (uint32_t j = 0; j < n_jobs; j++) {
+    c[j].clear();
+    if (best_level[j] == 0) continue;
+    for (int sh = 0; sh < 8; sh++)
+      if (sh != bs[j]) c[j].insert(c[j].end(), {best_level[j], (uint8_t)sh});
+  }
+  if ((s = stage(c)) != VP8A_OK) return s;
+  for (uint32_t j = 0; j < n_jobs; j++) {
+    const uint64_t* tj = t.data() + (size_t)512 * j;
+    for (size_t i = 0; i < c[j].size(); i += 2)
+      if (tj[best_level[j] * 8 + c[j][i + 1]] < best[j]) {
+        best[j] = tj[best_level[j] * 8 + c[j][i + 1]];
+        best_sharp[j] = c[j][i + 1];
+      }
+    level_out[j] = best_level[j];
+    sharpness_out[j] = best_sharp[j];
+  }
   return st.finish();
 }
 

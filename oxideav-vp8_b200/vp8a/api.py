@@ -613,3 +613,21 @@ def filter_sweeps(ctx, jobs):
         outs.append(out.reshape(64, 8))
     _batch(ctx, "vp8a_filter_sweeps", cj, "vp8a_filter_sweeps")
     return outs
+
+
+def select_filter_params_batch(ctx, jobs):
+    """vp8a_select_filter_params_batch: select_filter_params
+    (src/loop_filter.rs:2047) for every job of `jobs` = list of (recon, mbs,
+    base, src); each stage of the walk runs all jobs in one launch. Returns
+    each job's (level, sharpness)."""
+    keep, cj = [], []
+    for recon, mbs, base, src in jobs:
+        m = mbs if hasattr(mbs, "data_ptr") else np.ascontiguousarray(mbs, abi.MB_LF_INFO_DTYPE)
+        keep.append(m)
+        cj.append(abi.SweepJob(planes(*recon), ptr(m), base, source(*src), 0, None))
+    arr = (abi.SweepJob * len(cj))(*cj)
+    lv = np.zeros(len(cj), np.uint8)
+    sh = np.zeros(len(cj), np.uint8)
+    check(ctx._lib.vp8a_select_filter_params_batch(ctx.handle, C.cast(arr, C.c_void_p), len(cj), ptr(lv), ptr(sh)),
+          "vp8a_select_filter_params_batch")
+    return [(int(a), int(b)) for a, b in zip(lv, sh)]

@@ -23,6 +23,7 @@ PROTOTYPES = {
     "vp8a_ctx_launch_count": (C.c_uint64, [P]),
     "vp8a_ctx_set_wait_limit": (C.c_int, [P, C.c_uint64]),
     "vp8a_ctx_set_autotune": (C.c_int, [P, U32]),
+    "vp8a_select_filter_params_batch": (C.c_int, [P, P, U32, P, P]),
     "vp8a_ctx_set_subpel_planes": (C.c_int, [P, U32]),
     "vp8a_ctx_force_sweep_layout": (C.c_int, [P, U32, U32, U32]),
     "vp8a_ctx_last_sweep_layout": (C.c_int, [P, P]),
