@@ -167,3 +167,21 @@ def test_batch_empty_and_errors(ctx):
     got = vp8a.analyse_inter_frames(ctx, [good])
     want = vp8a.analyse_inter_frame(ctx, good["frame"], good["refs"], good["ref_ids"], good["lam"])
     assert np.array_equal(got[0].view(np.uint8), want.view(np.uint8))
+
+
+def test_select_filter_params_batch_matches_single_walks(ctx, oracle):
+    # The reference's walk (grid, refine, sharpness) for several pictures of
+    # different sizes and configurations, every stage of all of them in one
+    # batched launch: each job's pair equals the oracle's own walk.
+    from test_gpu_lf import lf_case
+
+    jobs = []
+    for i, (size, cfg) in enumerate([((320, 240), dict(sharpness=0)), ((176, 144), dict(sharpness=3)),
+                                     ((72, 40), dict(sharpness=0, key_frame=True)),
+                                     ((640, 368), dict(sharpness=5, delta_enabled=1, ref_delta_last=4))]):
+        src, recon, m = lf_case(*size, seed=300 + i)
+        jobs.append((recon, m, abi.filter_config(0, **cfg), src))
+    got = vp8a.select_filter_params_batch(ctx, jobs)
+    want = [oracle.select_filter_params(r, m, b, s, threads=8) for r, m, b, s in jobs]
+    assert got == want
+    assert any(lv != 0 for lv, _ in want)
