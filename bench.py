@@ -1176,6 +1176,81 @@ def learned_arm(args):
                     "same frame and references"}
 
 
+STREAM_SIZES = [(3840, 2160)] * 8 + [(1280, 720)] * 8
+STREAM_GROUP = 15
+
+
+def stream_arm(args):
+    """The lagged altref stream path of the survey's config 5: 8 streams at
+    3840x2160 and 8 at 1280x720 in lockstep, 15-frame lookahead groups, each
+    group an invisible ARNR anchor (centre = the group's last frame) coded
+    against LAST / GOLDEN / ALTREF and then its P frames, all with the
+    automatic loop-filter pick and the filtered pictures as the next
+    references (vp8a.stream.AltrefStreams: every stage of all 16 streams one
+    batched call). Timed: groups after the first (the first opens the
+    streams), device time per group with inputs resident; MB/s counts every
+    coded MB (anchors and P frames). Bytes and PSNR come from one further
+    group with the host bitstream writer on, untimed."""
+    import torch
+
+    import vp8a
+    from vp8a import synth
+    from vp8a.stream import AltrefStreams
+
+    sizes = STREAM_SIZES[: args.streams] if args.streams < len(STREAM_SIZES) else STREAM_SIZES
+    g = STREAM_GROUP
+    n_groups = 2 + args.steps
+    need = g * n_groups
+    seqs = {}
+    for (w, h) in sorted(set(sizes)):
+        seqs[(w, h)], _ = synth.make_sequence(w, h, need + 7, SEED + w, pieces=4, occluders=4)
+    ctx = vp8a.Context(0)
+    dev = torch.device("cuda", 0)
+    frames = []
+    for i, (w, h) in enumerate(sizes):
+        off = i % 8
+        frames.append([tuple(torch.from_numpy(np.ascontiguousarray(p)).to(dev) for p in f)
+                       for f in seqs[(w, h)][off:off + need]])
+    torch.cuda.synchronize()
+    streams = AltrefStreams(ctx, sizes, qi=QI, strength=3, write=False)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    mbs_group = sum(((w + 15) // 16) * ((h + 15) // 16) for w, h in sizes) * g  # anchor + (g - 1) P frames
+    ts = []
+    for gi in range(n_groups - 1):
+        grp = [f[gi * g:(gi + 1) * g] for f in frames]
+        ctx.synchronize()
+        s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s_.record(stream)
+        streams.encode_group(grp)
+        e_.record(stream)
+        e_.synchronize()
+        ts.append(s_.elapsed_time(e_))
+    timed = ts[1:]  # the first group opens the streams (no anchor context before it)
+    ms = float(np.median(timed))
+    # Bytes and luma PSNR of one more group, writer on.
+    streams.write = True
+    gi = n_groups - 1
+    grp = [f[gi * g:(gi + 1) * g] for f in frames]
+    packets = streams.encode_group(grp)
+    by_res = {}
+    for (w, h), pk in zip(sizes, packets):
+        d = by_res.setdefault("%dx%d" % (w, h), {"streams": 0, "bytes_per_group": 0, "levels": []})
+        d["streams"] += 1
+        d["bytes_per_group"] += sum(len(p["bytes"]) for p in pk if p["bytes"] is not None)
+        d["levels"] += [p["level"] for p in pk]
+    for d in by_res.values():
+        d["bytes_per_group"] //= d["streams"]
+        d["mean_level"] = round(float(np.mean(d.pop("levels"))), 2)
+    ctx.close()
+    return {"case": "stream", "unit": "MB/s", "streams": len(sizes), "sizes": sorted(set("%dx%d" % s for s in sizes)),
+            "group": g, "qi": QI, "value": round(mbs_group / (ms / 1e3), 1), "ms_per_group": round(ms, 2),
+            "mbs_per_group": mbs_group, "group_ms": [round(x, 2) for x in ts], "per_resolution": by_res,
+            "config": {"workload": "8x3840x2160 + 8x1280x720 altref streams, 15-frame groups: ARNR anchor + 14 P "
+                                   "frames per group, exhaustive 3-ref analysis, qi-44 reconstruction, auto-LF "
+                                   "(reference walk) and filter on every coded frame", "seed": SEED,
+                       "timed": "device time per group after the first, inputs resident"}}
+
+
 def rd_arm(args):
     """The RD-effort inter search (decide_mb_rd's search, the stream
     encoder's per-MB inter search) over the bench's 1080p P frame against
@@ -1330,7 +1405,7 @@ def main():
     ap.add_argument("--no-parity", action="store_true", help="skip the step's parity check against the oracle")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--case", choices=["arnr", "analysis", "lf", "recon", "predict", "predict_mb", "predict_split",
-                                       "batch", "learned", "lp_conv", "rd"],
+                                       "batch", "learned", "lp_conv", "rd", "stream"],
                     help="profile one stage alone, or (batch) the batched many-stream path")
     ap.add_argument("--streams", type=int, default=48, help="streams of the batch case")
     ap.add_argument("--train-steps", type=int, default=300, help="training steps of the learned case")
@@ -1347,6 +1422,8 @@ def main():
         res = lp_conv_arm(args)
     elif args.case == "rd":
         res = rd_arm(args)
+    elif args.case == "stream":
+        res = stream_arm(args)
     elif args.case:
         res = case_arm(args)
     else:

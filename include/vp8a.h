@@ -584,6 +584,20 @@ vp8a_status vp8a_select_filter_params_sampled(vp8a_ctx* ctx, const vp8a_planes* 
  * VP8A_MAX_BATCH_JOBS jobs per call. */
 #define VP8A_MAX_BATCH_JOBS 1024u
 
+/* No counterpart in the reference: vp8a_analyse_inter_frame with one
+ * proposed vector per (MB, reference) — `proposals` holds n_refs vectors
+ * per MB in raster order, e.g. the learned proposal's refined seeds — as a
+ * second NEWMV candidate beside the searched one: its exact SAD is computed
+ * here and it costs what a searched vector costs (SAD + lambda * (NEWMV
+ * mode bits + differential bits)); it replaces the searched vector when
+ * strictly cheaper. A zero vector or one beyond +-1023 quarter-pels is not
+ * a candidate. Everything else is vp8a_analyse_inter_frame's decision. */
+vp8a_status vp8a_analyse_inter_frame_proposals(vp8a_ctx* ctx, const vp8a_i420* frame,
+                                               const vp8a_planes* refs, const uint8_t* ref_ids,
+                                               uint32_t n_refs, const vp8a_mv_contexts* mv_contexts,
+                                               double lambda, const vp8a_mv* proposals,
+                                               vp8a_mb_decision* decisions, vp8a_ref_search* trace);
+
 /* One vp8a_analyse_inter_frame call's arguments. */
 typedef struct vp8a_analysis_job {
   vp8a_i420 frame;

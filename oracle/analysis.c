@@ -442,7 +442,7 @@ static void pick_mb_for_ref(uint8_t ref_id, const vp8a_luma_ref* r, const uint8_
                             const vo_mb_info* above, const vo_mb_info* left,
                             const vo_mb_info* aboveleft, int mb_col, int mb_row, int mb_cols,
                             int mb_rows, const vp8a_mv_contexts* ctx, double lambda,
-                            ref_pick* out, vp8a_ref_search* trace) {
+                            const vp8a_mv* prop, ref_pick* out, vp8a_ref_search* trace) {
   vp8a_mv near[3];
   int32_t cnt[4];
   vo_find_near_mvs(above, left, aboveleft, ref_id, near, cnt);
@@ -479,6 +479,25 @@ static void pick_mb_for_ref(uint8_t ref_id, const vp8a_luma_ref* r, const uint8_
   int nearest_eligible = !mv_zero(nearest_mv);
   int near_eligible = !mv_zero(near_mv);
   int new_eligible = diff_in_range && !mv_zero(search.mv);
+  vp8a_mv new_mv = search.mv;
+  /* A proposed vector (the learned proposal's, for this reference) is a
+   * second NEWMV candidate: its exact SAD and the same cost terms; it
+   * replaces the searched vector when strictly cheaper (or when that one
+   * is not eligible). Proposals beyond +-1023 are ignored. */
+  if (prop && prop->row >= -1023 && prop->row <= 1023 && prop->col >= -1023 && prop->col <= 1023 &&
+      !mv_zero(*prop)) {
+    int32_t pr = (int32_t)prop->row - best_predictor.row, pc = (int32_t)prop->col - best_predictor.col;
+    if (pr >= -1023 && pr <= 1023 && pc >= -1023 && pc <= 1023) {
+      uint32_t sad_p = vo_mb_luma_sad_at_mv(r, mb_col, mb_row, src_y, *prop);
+      double j_p = (double)sad_p + lambda * (bits_mode_new + (vo_mv_component_bits(ctx->p[0], pr) +
+                                                               vo_mv_component_bits(ctx->p[1], pc)));
+      if (!new_eligible || j_p < j_new) {
+        new_mv = *prop;
+        j_new = j_p;
+        new_eligible = 1;
+      }
+    }
+  }
 
   out->mode = VP8A_MODE_ZERO;
   out->mv = MV0;
@@ -496,7 +515,7 @@ static void pick_mb_for_ref(uint8_t ref_id, const vp8a_luma_ref* r, const uint8_
   }
   if (new_eligible && j_new < chosen_j) {
     out->mode = VP8A_MODE_NEW;
-    out->mv = search.mv;
+    out->mv = new_mv;
     chosen_j = j_new;
   }
 
@@ -578,6 +597,7 @@ typedef struct {
   double lambda;
   vp8a_mb_decision* dec;
   vp8a_ref_search* trace;
+  const vp8a_mv* props; /* n_refs proposed vectors per MB, or NULL */
   vo_mb_info* infos;
   int mb_cols, mb_rows;
   atomic_int* progress; /* per row: MBs done */
@@ -603,7 +623,8 @@ static void analyse_mb(analyse_job* j, int mb_row, int mb_col) {
                         j->refs[k].mb_rows * 16};
     ref_pick pk;
     pick_mb_for_ref(j->ref_ids[k], &lr, src_y, above, left, aboveleft, mb_col, mb_row,
-                    j->mb_cols, j->mb_rows, j->ctx, j->lambda, &pk,
+                    j->mb_cols, j->mb_rows, j->ctx, j->lambda, j->props ? &j->props[idx * j->n_refs + k] : NULL,
+                    &pk,
                     j->trace ? &j->trace[idx * j->n_refs + k] : NULL);
     double total = pk.j + j->lambda * ref_tree_bits(j->ref_ids[k]);
     if (total < best_total) {
@@ -651,11 +672,29 @@ static void analyse_row_task(void* arg, uint32_t row) {
   }
 }
 
+int vo_analyse_inter_frame_proposals(const vp8a_i420* frame, const vp8a_planes* refs,
+                                     const uint8_t* ref_ids, uint32_t n_refs,
+                                     const vp8a_mv_contexts* mv_contexts, double lambda,
+                                     const vp8a_mv* proposals, vp8a_mb_decision* decisions,
+                                     vp8a_ref_search* trace, uint32_t threads);
+
 int vo_analyse_inter_frame(const vp8a_i420* frame, const vp8a_planes* refs,
                            const uint8_t* ref_ids, uint32_t n_refs,
                            const vp8a_mv_contexts* mv_contexts, double lambda,
                            vp8a_mb_decision* decisions, vp8a_ref_search* trace,
                            uint32_t threads) {
+  return vo_analyse_inter_frame_proposals(frame, refs, ref_ids, n_refs, mv_contexts, lambda, NULL,
+                                          decisions, trace, threads);
+}
+
+/* vo_analyse_inter_frame with one proposed vector per (MB, reference) as a
+ * second NEWMV candidate (the learned proposal's seeds into the exhaustive
+ * decision; no counterpart in the reference). */
+int vo_analyse_inter_frame_proposals(const vp8a_i420* frame, const vp8a_planes* refs,
+                                     const uint8_t* ref_ids, uint32_t n_refs,
+                                     const vp8a_mv_contexts* mv_contexts, double lambda,
+                                     const vp8a_mv* proposals, vp8a_mb_decision* decisions,
+                                     vp8a_ref_search* trace, uint32_t threads) {
   if (!frame || !decisions || (n_refs > 0 && (!refs || !ref_ids))) return VP8A_E_INVALID_ARGUMENT;
   if (frame->width == 0 || frame->height == 0 || frame->width > 0x3FFF || frame->height > 0x3FFF)
     return VP8A_E_INVALID_DIMENSIONS;
@@ -679,6 +718,7 @@ int vo_analyse_inter_frame(const vp8a_i420* frame, const vp8a_planes* refs,
   j.lambda = lambda;
   j.dec = decisions;
   j.trace = trace;
+  j.props = proposals;
   j.mb_cols = mb_cols;
   j.mb_rows = mb_rows;
   j.infos = (vo_mb_info*)calloc((size_t)mb_cols * mb_rows, sizeof(vo_mb_info));

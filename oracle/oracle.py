@@ -59,6 +59,8 @@ def load():
         "vo_rd_lambda": (C.c_double, [U32]),
         "vo_analyse_inter_frame": (C.c_int, [C.POINTER(abi.I420), P, P, U32, C.POINTER(abi.MvContexts),
                                              C.c_double, P, P, U32]),
+        "vo_analyse_inter_frame_proposals": (C.c_int, [C.POINTER(abi.I420), P, P, U32, C.POINTER(abi.MvContexts),
+                                                       C.c_double, P, P, P, U32]),
         "vo_build_arnr_altref": (C.c_int, [P, U32, U32, U32, P, P, P, U32]),
         "vo_lf_derive": (None, [C.c_uint8, C.c_uint8, C.c_int, P]),
         "vo_common_adjust": (C.c_int32, [C.c_int, P]),
@@ -209,7 +211,9 @@ def _check(status, where):
         raise RuntimeError(f"{where}: {abi.STATUS_NAMES.get(status, status)}")
 
 
-def analyse_inter_frame(frame, refs, ref_ids, lam, mv_contexts=None, trace=False, threads=1):
+def analyse_inter_frame(frame, refs, ref_ids, lam, mv_contexts=None, trace=False, threads=1, proposals=None):
+    """The exhaustive analysis; `proposals` (optional, (mb_rows * mb_cols,
+    n_refs) MV_DTYPE) adds one proposed NEWMV vector per MB and reference."""
     f = i420(*frame)
     prs = [planes(*p) for p in refs]
     parr = (abi.Planes * len(prs))(*prs)
@@ -218,8 +222,14 @@ def analyse_inter_frame(frame, refs, ref_ids, lam, mv_contexts=None, trace=False
     dec = np.zeros(mbr * mbc, abi.MB_DECISION_DTYPE)
     tr = np.zeros(mbr * mbc * len(prs), abi.REF_SEARCH_DTYPE) if trace else None
     ctxs = mv_contexts if mv_contexts is not None else abi.default_mv_contexts()
-    st = load().vo_analyse_inter_frame(C.byref(f), C.cast(parr, C.c_void_p), ptr(ids), len(prs), C.byref(ctxs), lam,
-                                       ptr(dec), ptr(tr), threads)
+    if proposals is None:
+        st = load().vo_analyse_inter_frame(C.byref(f), C.cast(parr, C.c_void_p), ptr(ids), len(prs), C.byref(ctxs),
+                                           lam, ptr(dec), ptr(tr), threads)
+    else:
+        pr = np.ascontiguousarray(proposals, abi.MV_DTYPE).reshape(-1)
+        assert pr.size == mbr * mbc * len(prs)
+        st = load().vo_analyse_inter_frame_proposals(C.byref(f), C.cast(parr, C.c_void_p), ptr(ids), len(prs),
+                                                     C.byref(ctxs), lam, ptr(pr), ptr(dec), ptr(tr), threads)
     _check(st, "vo_analyse_inter_frame")
     dec = dec.reshape(mbr, mbc)
     if trace:

@@ -88,6 +88,13 @@ int vo_analyse_inter_frame(const vp8a_i420* frame, const vp8a_planes* refs,
                            const vp8a_mv_contexts* mv_contexts, double lambda,
                            vp8a_mb_decision* decisions, vp8a_ref_search* trace,
                            uint32_t threads);
+/* vo_analyse_inter_frame with `proposals` (n_refs vectors per MB, raster
+ * order) as second NEWMV candidates. */
+int vo_analyse_inter_frame_proposals(const vp8a_i420* frame, const vp8a_planes* refs,
+                                     const uint8_t* ref_ids, uint32_t n_refs,
+                                     const vp8a_mv_contexts* mv_contexts, double lambda,
+                                     const vp8a_mv* proposals, vp8a_mb_decision* decisions,
+                                     vp8a_ref_search* trace, uint32_t threads);
 
 /* The RD-effort inter search (decide_mb_rd's search part,
  * src/encoder/inter_search.rs:198-552, :846-1060) for every MB given its

@@ -66,6 +66,9 @@ struct AnArgs {
   // fx / 2) * sp_plane, pixel (x, y) at ((y + SPB) * sp_pitch + x + SPB).
   const uint8_t* spl[MAX_REFS];
   uint64_t sp_pitch, sp_plane;
+  // One proposed vector per (MB, reference), n_refs per MB in raster
+  // order, or null: a second NEWMV candidate (the learned proposal's).
+  const vp8a_mv* props;
 };
 
 // ------------------------------------------------------------- staging
@@ -1032,6 +1035,9 @@ __global__ void __launch_bounds__(AN_THREADS, 2)
   __shared__ Census cen;
   __shared__ Plan plan;
   __shared__ int s_abort, s_qok;
+  __shared__ vp8a_mv s_prop_mv;
+  __shared__ uint32_t s_prop_sad;
+  __shared__ int s_prop_ok;
   // Per-MB cost terms of the mode decision (from the census probabilities),
   // filled during the search by warp 7; per-CTA constants below.
   __shared__ double dz, dnearest, dnear, dnew_bits, dsplit;
@@ -1205,6 +1211,20 @@ __global__ void __launch_bounds__(AN_THREADS, 2)
           const int er = eighth(cen.near_.row), ec = eighth(cen.near_.col);
           const uint32_t sv = subpel_sad(R.halo_near, HS, ec & 7, er & 7, src, wt[6].temp, lane);
           if (lane == 0) mo.sad_near = sv;
+        } else if (warp == 8) {
+          // The proposed vector's exact SAD (a second NEWMV candidate).
+          vp8a_mv pv = {0, 0};
+          if (a.props) pv = a.props[((size_t)r * a.mb_cols + c) * a.n_refs + k];
+          const bool ok = a.props && !mv_zero(pv) && pv.row >= -1023 && pv.row <= 1023 && pv.col >= -1023 &&
+                          pv.col <= 1023;
+          uint32_t sv = 0;
+          if (ok) sv = sad_at_mv(P, R.ws.win, wt[8].temp, wt[8].halo, plan.wx0, plan.wy0, mbx, mby, pv.row, pv.col,
+                                 src, lane);
+          if (lane == 0) {
+            s_prop_ok = ok;
+            s_prop_mv = pv;
+            s_prop_sad = sv;
+          }
         } else if (warp == 7 && lane == 0) {
           // The mode tree's bits under this MB's census probabilities.
           const double* t = bit_cost;
@@ -1331,7 +1351,23 @@ __global__ void __launch_bounds__(AN_THREADS, 2)
         const double j_zero = (double)m.sad_zero + dz;
         const double j_nearest = (double)m.sad_nearest + dnearest;
         const double j_near = (double)m.sad_near + dnear;
-        const double j_new = (double)m.quarter.sad + lambda * (dnew_bits + bits_mv);
+        double j_new = (double)m.quarter.sad + lambda * (dnew_bits + bits_mv);
+        bool new_ok = in_range && !mv_zero(m.quarter.mv);
+        vp8a_mv new_mv = m.quarter.mv;
+        if (s_prop_ok) {
+          // The proposal replaces the searched vector when strictly cheaper
+          // (or when that one is not eligible).
+          const int pr = (int)s_prop_mv.row - bp.row, pc = (int)s_prop_mv.col - bp.col;
+          if (pr >= -1023 && pr <= 1023 && pc >= -1023 && pc <= 1023) {
+            const double j_p =
+                (double)s_prop_sad + lambda * (dnew_bits + (mvb[pr + 1023] + mvb[MV_BITS_SPAN + pc + 1023]));
+            if (!new_ok || j_p < j_new) {
+              j_new = j_p;
+              new_mv = s_prop_mv;
+              new_ok = true;
+            }
+          }
+        }
         int mode = VP8A_MODE_ZERO, pid = VP8A_PART_NONE;
         vp8a_mv mv = {0, 0};
         double cj = j_zero;
@@ -1345,9 +1381,9 @@ __global__ void __launch_bounds__(AN_THREADS, 2)
           mv = cen.near_;
           cj = j_near;
         }
-        if (in_range && !mv_zero(m.quarter.mv) && j_new < cj) {
+        if (new_ok && j_new < cj) {
           mode = VP8A_MODE_NEW;
-          mv = m.quarter.mv;
+          mv = new_mv;
           cj = j_new;
         }
         int have = 0, sp = -1;
@@ -1467,7 +1503,7 @@ struct MvBitsCache {
 vp8a_status prepare_job(vp8a_ctx* ctx, vp8a::Stager& st, MvBitsCache& mc, const vp8a_i420* frame,
                         const vp8a_planes* refs, const uint8_t* ref_ids, uint32_t n_refs,
                         const vp8a_mv_contexts* mv_contexts, double lambda, vp8a_mb_decision* decisions,
-                        vp8a_ref_search* trace, AnArgs* out) {
+                        vp8a_ref_search* trace, AnArgs* out, const vp8a_mv* proposals = nullptr) {
   if (!frame || !refs || !ref_ids || !decisions) {
     vp8a::set_error("null argument");
     return VP8A_E_INVALID_ARGUMENT;
@@ -1549,6 +1585,11 @@ vp8a_status prepare_job(vp8a_ctx* ctx, vp8a::Stager& st, MvBitsCache& mc, const 
   a.dec = (vp8a_mb_decision*)ddec;
   a.trace = (vp8a_ref_search*)dtr;
   a.spin_limit = ctx->wait_limit;
+  if (proposals) {
+    const void* dp;
+    if ((s = st.in(proposals, sizeof(vp8a_mv) * nmb * n_refs, &dp)) != VP8A_OK) return s;
+    a.props = (const vp8a_mv*)dp;
+  }
   // The references' sub-pel planes, built before the wavefront starts.
   if (ctx->subpel_planes) {
     const int pw = mb_cols * 16, ph = mb_rows * 16;
@@ -1643,6 +1684,26 @@ extern "C" vp8a_status vp8a_analyse_inter_frame(vp8a_ctx* ctx, const vp8a_i420* 
   MvBitsCache mc;
   AnArgs a{};
   vp8a_status s = prepare_job(ctx, st, mc, frame, refs, ref_ids, n_refs, mv_contexts, lambda, decisions, trace, &a);
+  if (s != VP8A_OK) return s;
+  if ((s = launch_analysis<false>(ctx, a.n_refs, a, nullptr, nullptr, a.mb_rows)) != VP8A_OK) return s;
+  return finish_analysis(ctx, st);
+}
+
+extern "C" vp8a_status vp8a_analyse_inter_frame_proposals(vp8a_ctx* ctx, const vp8a_i420* frame,
+                                                          const vp8a_planes* refs, const uint8_t* ref_ids,
+                                                          uint32_t n_refs, const vp8a_mv_contexts* mv_contexts,
+                                                          double lambda, const vp8a_mv* proposals,
+                                                          vp8a_mb_decision* decisions, vp8a_ref_search* trace) {
+  if (!ctx || !proposals) {
+    vp8a::set_error("null argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  vp8a::Stager st(ctx);
+  MvBitsCache mc;
+  AnArgs a{};
+  vp8a_status s =
+      prepare_job(ctx, st, mc, frame, refs, ref_ids, n_refs, mv_contexts, lambda, decisions, trace, &a, proposals);
   if (s != VP8A_OK) return s;
   if ((s = launch_analysis<false>(ctx, a.n_refs, a, nullptr, nullptr, a.mb_rows)) != VP8A_OK) return s;
   return finish_analysis(ctx, st);

@@ -152,12 +152,14 @@ def rd_lambda(y_ac_qi):
     return load().vp8a_rd_lambda(y_ac_qi)
 
 
-def analyse_inter_frame(ctx, frame, refs, ref_ids, lam, mv_contexts=None, trace=False):
+def analyse_inter_frame(ctx, frame, refs, ref_ids, lam, mv_contexts=None, trace=False, proposals=None):
     """The exhaustive inter analysis (analyse_inter_frame,
     src/encoder/inter.rs:263, intra picking off). `frame` = (y, u, v)
     visible planes; `refs` = list of MB-padded (y, u, v). Returns the
     decisions as a (mb_rows, mb_cols) structured array (and the per-ref
-    search trace when `trace`)."""
+    search trace when `trace`). `proposals` (optional: n_refs MV_DTYPE
+    vectors per MB, raster order, numpy or a device tensor) adds each as a
+    second NEWMV candidate (vp8a_analyse_inter_frame_proposals)."""
     f = i420(*frame)
     prs = [planes(*p) for p in refs]
     parr = (abi.Planes * len(prs))(*prs)
@@ -166,8 +168,14 @@ def analyse_inter_frame(ctx, frame, refs, ref_ids, lam, mv_contexts=None, trace=
     dec = np.zeros(mbr * mbc, abi.MB_DECISION_DTYPE)
     tr = np.zeros(mbr * mbc * len(prs), abi.REF_SEARCH_DTYPE) if trace else None
     ctxs = mv_contexts if mv_contexts is not None else abi.default_mv_contexts()
-    check(ctx._lib.vp8a_analyse_inter_frame(ctx.handle, C.byref(f), C.cast(parr, C.c_void_p), ptr(ids), len(prs),
-                                            C.byref(ctxs), lam, ptr(dec), ptr(tr)), "vp8a_analyse_inter_frame")
+    if proposals is None:
+        check(ctx._lib.vp8a_analyse_inter_frame(ctx.handle, C.byref(f), C.cast(parr, C.c_void_p), ptr(ids), len(prs),
+                                                C.byref(ctxs), lam, ptr(dec), ptr(tr)), "vp8a_analyse_inter_frame")
+    else:
+        pr = proposals if hasattr(proposals, "data_ptr") else np.ascontiguousarray(proposals, abi.MV_DTYPE)
+        check(ctx._lib.vp8a_analyse_inter_frame_proposals(ctx.handle, C.byref(f), C.cast(parr, C.c_void_p), ptr(ids),
+                                                          len(prs), C.byref(ctxs), lam, ptr(pr), ptr(dec), ptr(tr)),
+              "vp8a_analyse_inter_frame_proposals")
     dec = dec.reshape(mbr, mbc)
     if trace:
         return dec, tr.reshape(mbr, mbc, len(prs))

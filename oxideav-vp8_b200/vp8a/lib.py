@@ -38,6 +38,10 @@ PROTOTYPES = {
         C.c_int,
         [P, C.POINTER(abi.I420), P, P, U32, C.POINTER(abi.MvContexts), C.c_double, P, P],
     ),
+    "vp8a_analyse_inter_frame_proposals": (
+        C.c_int,
+        [P, C.POINTER(abi.I420), P, P, U32, C.POINTER(abi.MvContexts), C.c_double, P, P, P],
+    ),
     "vp8a_rd_lambda": (C.c_double, [U32]),
     "vp8a_analyse_inter_frames": (C.c_int, [P, P, U32]),
     "vp8a_build_arnr_altrefs": (C.c_int, [P, P, U32]),

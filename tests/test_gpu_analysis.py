@@ -138,3 +138,28 @@ def test_analysis_with_and_without_subpel_planes(oracle, planes):
         got, gtr = vp8a.analyse_inter_frame(c, frames[4], refs, ids, lam, trace=True)
     assert np.array_equal(gtr, wtr)
     assert_same(got, want)
+
+
+def test_analysis_with_proposals(ctx, oracle):
+    # A proposed vector per (MB, reference) is a second NEWMV candidate:
+    # random vectors (some zero, some beyond +-1023, some close to the true
+    # motion) give exactly the oracle's decisions, and good ones are taken.
+    frames, _ = synth.make_sequence(320, 240, 7, seed=31, pieces=5, occluders=4)
+    refs = refs_for(frames, 3)
+    ids = [abi.REF_LAST, abi.REF_GOLDEN, abi.REF_ALTREF]
+    lam = vp8a.rd_lambda(44)
+    rng = np.random.default_rng(5)
+    n = 20 * 15
+    prop = np.zeros((n, 3), abi.MV_DTYPE)
+    prop["row"] = rng.integers(-40, 41, (n, 3))
+    prop["col"] = rng.integers(-40, 41, (n, 3))
+    prop[rng.random((n, 3)) < 0.1] = (0, 0)
+    far = rng.random((n, 3)) < 0.05
+    prop["col"][far] = 1100
+    want = oracle.analyse_inter_frame(frames[3], refs, ids, lam, proposals=prop, threads=8)
+    got = vp8a.analyse_inter_frame(ctx, frames[3], refs, ids, lam, proposals=prop)
+    assert_same(got, want)
+    plain = oracle.analyse_inter_frame(frames[3], refs, ids, lam, threads=8)
+    taken = (want["mode"] == abi.MODE_NEW) & ((want["mv"]["row"] != plain["mv"]["row"]) |
+                                              (want["mv"]["col"] != plain["mv"]["col"]))
+    assert taken.any()
