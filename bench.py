@@ -1151,6 +1151,7 @@ def learned_arm(args):
         plain_sad.append(tr[..., 0]["quarter"]["sad"].reshape(-1).astype(np.float64))
     ratio = [float(np.asarray(o[1], np.float64).mean() / ps.mean()) for o, ps in zip(res, plain_sad)]
     fb = [float(np.mean(o[2])) for o in res]
+    rd = learned_rd(ctx, net, head, sample)
     ctx.close()
     return {"case": "learned", "size": "%dx%d" % (W, H), "unit": "MB/s",
             "learned_me_mbs_per_s": round(N_MB / (ms_learned / 1e3), 1), "learned_me_ms": round(ms_learned, 3),
@@ -1171,6 +1172,7 @@ def learned_arm(args):
                           "train_frames": len(lf_frames), "train_levels": sorted(set(lf_levels)),
                           "train_window_hits": head_hits, "head_loss_first_last": [round(head_losses[0], 4),
                                                                                     round(head_losses[-1], 4)]},
+            "rd": rd,
             "note": "learned = proposal net + exact +-2 px search at 4 seeds + sub-pel + descent fallback, 3 refs, "
                     "per-reference vectors; plain = the exhaustive analysis (census, SPLITMV, RD decision) of the "
                     "same frame and references"}
@@ -1320,6 +1322,77 @@ def rd_arm(args):
             "efforts": res, "exhaustive_analysis_ms": round(ms_plain, 4),
             "note": "RD-effort inter search per MB given its census neighbours (one warp per MB, no wavefront); "
                     "the exhaustive analysis (the metric's search) timed beside it"}
+
+
+def psnr_y(a, b):
+    d = a.astype(np.float64) - b.astype(np.float64)
+    mse = float(np.mean(d * d))
+    return 99.0 if mse == 0 else 10.0 * np.log10(255.0 * 255.0 / mse)
+
+
+def learned_rd(ctx, net, head, sample, n_seq=2):
+    """Bytes and PSNR of whole P-frame encodes (analysis, qi reconstruction,
+    automatic loop filter, bitstream) with and without the learned
+    proposals, on held-out 1080p frames (seeds not used in training: frame
+    8 against LAST = 7, GOLDEN = 0 and the ARNR anchor of frames 9-15) at
+    qi 24 / 44 / 64. "learned" passes each reference's learned-search vector
+    as a second NEWMV candidate to the exhaustive decision. Also: whether
+    the learned loop-filter window holds the plain path's level on those
+    frames, counting the frames whose plain level is not 0."""
+    import torch
+
+    import vp8a
+    from vp8a import abi, learned, synth
+
+    held = []
+    for sidx in range(n_seq):
+        fr, _ = synth.make_sequence(W, H, 16, SEED + 5000 + sidx, pieces=4, occluders=4)
+        anchor = vp8a.build_arnr_altref_planes(ctx, [fr[9 + i] for i in range(LOOKAHEAD)], 3, 3)
+        held.append((fr[8], [pad_planes(fr[7]), pad_planes(fr[0]), anchor]))
+    xy = learned.all_mbs(MB_COLS, MB_ROWS)
+    props, t_learn = [], []
+    for cur, refs in held:
+        with learned.on_ctx_stream(ctx):
+            src = torch.from_numpy(cur[0]).cuda()
+            rts = [torch.from_numpy(r[0]).cuda() for r in refs]
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        res = [learned.learned_search(ctx, net, src, r, xy) for r in rts]
+        t_learn.append(time.perf_counter() - t0)
+        p = np.zeros((N_MB, 3), abi.MV_DTYPE)
+        for k, (mv, _, _) in enumerate(res):
+            p["row"][:, k] = mv[:, 0]
+            p["col"][:, k] = mv[:, 1]
+        props.append(p)
+    out = {}
+    window_hits, window_n = 0, 0
+    for qi in (24, 44, 64):
+        acc = {m: {"bytes": 0, "psnr": [], "levels": []} for m in ("plain", "learned")}
+        for (cur, refs), p in zip(held, props):
+            for mode, pr in (("plain", None), ("learned", p)):
+                bits, filt, det = vp8a.encode_p_frame(ctx, cur, refs, [1, 2, 3], qi, proposals=pr)
+                acc[mode]["bytes"] += len(bits)
+                acc[mode]["psnr"].append(psnr_y(filt[0][:H, :W], cur[0]))
+                acc[mode]["levels"].append(int(det["level"]))
+                if mode == "plain" and det["level"] != 0:
+                    with learned.on_ctx_stream(ctx):
+                        s_t = torch.from_numpy(cur[0]).cuda()
+                        r_t = torch.from_numpy(refs[0][0]).cuda()
+                    sums, count = head.features(net, s_t, r_t, sample, qi)
+                    lo, hi = head.window(sums, count)
+                    window_n += 1
+                    window_hits += int(lo <= det["level"] <= hi)
+        pb, lb = acc["plain"]["bytes"], acc["learned"]["bytes"]
+        out["qi%d" % qi] = {
+            "plain_bytes": pb, "learned_bytes": lb, "byte_delta_pct": round(100.0 * (lb - pb) / pb, 3),
+            "plain_psnr_y": round(float(np.mean(acc["plain"]["psnr"])), 3),
+            "learned_psnr_y": round(float(np.mean(acc["learned"]["psnr"])), 3),
+            "psnr_delta_db": round(float(np.mean(acc["learned"]["psnr"]) - np.mean(acc["plain"]["psnr"])), 3),
+            "levels_plain": acc["plain"]["levels"], "levels_learned": acc["learned"]["levels"]}
+    out["frames"] = len(held)
+    out["learned_search_s_per_frame"] = round(float(np.mean(t_learn)), 4)
+    out["lf_window_hits_on_nonzero_plain_levels"] = [window_hits, window_n]
+    return out
 
 
 def batched_predict(ctx, vp8a, torch, split):

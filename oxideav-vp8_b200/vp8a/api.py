@@ -318,7 +318,7 @@ def write_inter_frame(header, decisions, coeffs, mb_segment=None, token_prob_upd
 
 
 def encode_p_frame(ctx, frame, refs, ref_ids, y_ac_qi, loop_filter_level=0, sharpness_level=0, simple=False,
-                   n_partitions=1, auto_lf=True, refresh_last=True):
+                   n_partitions=1, auto_lf=True, refresh_last=True, proposals=None):
     """encode_p_frame_multi_ref_auto_loop_filter (src/encoder.rs:9373) with
     intra picking off and the trellis off: the exhaustive analysis, the §14
     reconstruction of the chosen modes, the §9.4 (level, sharpness) search
@@ -327,8 +327,9 @@ def encode_p_frame(ctx, frame, refs, ref_ids, y_ac_qi, loop_filter_level=0, shar
     with ids `ref_ids` (VP8A_REF_*). Returns (frame bytes, the filtered
     reconstruction as MB-padded (y, u, v), details dict with the decisions,
     coefficients, flags, the loop-filter records and the chosen level and
-    sharpness)."""
-    dec = analyse_inter_frame(ctx, frame, refs, ref_ids, rd_lambda(y_ac_qi)).reshape(-1)
+    sharpness). `proposals` (optional) are second NEWMV candidates for the
+    analysis (vp8a_analyse_inter_frame_proposals)."""
+    dec = analyse_inter_frame(ctx, frame, refs, ref_ids, rd_lambda(y_ac_qi), proposals=proposals).reshape(-1)
     quant = abi.quant_indices(y_ac_qi)
     recon = tuple(np.zeros_like(p) for p in refs[0])
     lf = np.zeros(dec.size, abi.MB_LF_INFO_DTYPE)
