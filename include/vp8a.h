@@ -282,6 +282,15 @@ vp8a_status vp8a_ctx_set_autotune(vp8a_ctx* ctx, uint32_t on);
  * candidate's prediction inside the wavefront. The results are the same;
  * on costs 16 planes of device scratch per reference during the call. */
 vp8a_status vp8a_ctx_set_subpel_planes(vp8a_ctx* ctx, uint32_t on);
+/* TrellisStrength (src/encoder.rs:2669-2711) of this context's inter
+ * reconstructions (vp8a_reconstruct_inter_frame[s]): 0 (the default here)
+ * quantises by plain rounding, TrellisStrength::OFF; > 0 runs the §13
+ * trellis quantiser (trellis_quantize_block, src/encoder.rs:3095) on every
+ * block at lambda = rd_lambda(factors) * strength * 0.04 against the §13.5
+ * default coefficient probabilities, as the reference's inter path does with
+ * KeyframeParams::trellis_strength (whose default is 1.0). Clamped to 0..=8;
+ * NaN means 1.0. Applies to calls issued after it. */
+vp8a_status vp8a_ctx_set_trellis_strength(vp8a_ctx* ctx, double strength);
 /* Forces the loop-filter sweep's launch shape (for tests): `passes` per
  * CTA (1-3; 0 = back to automatic), `threads` per CTA, `prefetch` 0/1. A
  * sweep whose picture the shape does not fit returns

@@ -134,16 +134,11 @@ static const uint8_t DEFAULT_MV_CONTEXT[2][19] = {
     {162, 128, 225, 146, 172, 147, 214, 39, 156, 128, 129, 132, 75, 145, 178, 206, 239, 254, 254},
     {164, 128, 204, 170, 119, 235, 140, 230, 228, 128, 130, 130, 74, 148, 180, 203, 236, 254, 254}};
 static const int8_t SMALL_MVTREE[14] = {2, 8, 4, 6, 0, -1, -2, -3, 10, 12, -4, -5, -6, -7};
-static const uint8_t COEFF_BANDS[16] = {0, 1, 2, 3, 6, 4, 5, 6, 6, 6, 6, 6, 6, 6, 6, 7};
-static const uint8_t ZIGZAG[16] = {0, 1, 4, 8, 5, 2, 3, 6, 9, 12, 13, 10, 7, 11, 14, 15};
-static const uint8_t PCAT[6][11] = {{159},
-                                    {165, 145},
-                                    {173, 148, 140},
-                                    {176, 155, 140, 135},
-                                    {180, 157, 141, 134, 130},
-                                    {254, 254, 243, 230, 196, 177, 153, 140, 133, 130, 129}};
-static const uint8_t PCAT_LEN[6] = {1, 2, 3, 4, 5, 11};
-static const uint16_t CAT_BASE[6] = {5, 7, 11, 19, 35, 67};
+#define COEFF_BANDS VO_COEFF_BANDS
+#define ZIGZAG VO_ZIGZAG
+#define PCAT VO_PCAT
+#define PCAT_LEN VO_PCAT_LEN
+#define CAT_BASE VO_CAT_BASE
 static const uint8_t LEFT_CTX[25] = {0, 0, 0, 0, 1, 1, 1, 1, 2, 2, 2, 2, 3, 3, 3, 3,
                                      4, 4, 5, 5, 6, 6, 7, 7, 8};
 static const uint8_t ABOVE_CTX[25] = {0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3,

@@ -101,8 +101,17 @@ def load():
         "vo_inverse_wht_4x4": (None, [P, P]),
         "vo_enc_quantize_block": (None, [P, C.c_int16, C.c_int16]),
         "vo_reconstruct_inter_mb": (C.c_int, [P, P, P, C.c_int, P]),
+        "vo_reconstruct_inter_mb_trellis": (C.c_int, [P, P, P, C.c_int, P, C.c_double]),
         "vo_reconstruct_inter_frame": (C.c_int, [C.POINTER(abi.I420), P, P, U32, P, C.POINTER(abi.QuantIndices), P, P,
                                                  C.c_int, C.c_int, C.c_int, C.POINTER(abi.Planes), P, P, P, U32]),
+        "vo_reconstruct_inter_frame_trellis": (C.c_int, [C.POINTER(abi.I420), P, P, U32, P,
+                                                         C.POINTER(abi.QuantIndices), P, P, C.c_int, C.c_int, C.c_int,
+                                                         C.POINTER(abi.Planes), P, P, P, C.c_double, U32]),
+        "vo_trellis_quantize_block": (None, [P, C.c_int16, C.c_int16, C.c_int, C.c_int, C.c_int, C.c_double]),
+        "vo_coeff_token_bits": (C.c_double, [C.c_int, C.c_int, C.c_int, C.c_int, U32]),
+        "vo_eob_token_bits": (C.c_double, [C.c_int, C.c_int, C.c_int]),
+        "vo_trellis_lambda": (C.c_double, [C.c_int16, C.c_double]),
+        "vo_idct_basis_norm_sq": (P, []),
         "vo_rd_inter_search": (C.c_int, [C.POINTER(abi.I420), P, P, U32, C.POINTER(abi.MvContexts), C.c_double,
                                          U32, U32, P, P, U32]),
     }
@@ -517,22 +526,49 @@ def enc_quantize_block(block, dc, ac):
     return a
 
 
-def reconstruct_inter_mb(src384, pred384, factors, split):
-    """The §14 half of the chosen-mode step for one MB: returns
-    (recon 384 B, quantised coeffs (400,) int16, flags)."""
+def reconstruct_inter_mb(src384, pred384, factors, split, tlambda=0.0):
+    """The §14 half of the chosen-mode step for one MB (with the §13
+    trellis at `tlambda` when > 0): returns (recon 384 B, quantised coeffs
+    (400,) int16, flags)."""
     src = np.ascontiguousarray(np.asarray(src384, np.uint8).reshape(384))
     rec = np.ascontiguousarray(np.asarray(pred384, np.uint8).reshape(384)).copy()
     f = np.ascontiguousarray(np.asarray(factors, np.int16).reshape(6))
     cf = np.zeros(400, np.int16)
-    fl = load().vo_reconstruct_inter_mb(ptr(src), ptr(rec), ptr(f), int(bool(split)), ptr(cf))
+    fl = load().vo_reconstruct_inter_mb_trellis(ptr(src), ptr(rec), ptr(f), int(bool(split)), ptr(cf), tlambda)
     return rec, cf, fl
+
+
+def trellis_quantize_block(block, dc, ac, first_coeff, plane, lam, entry_ctx3=0):
+    """trellis_quantize_block (src/encoder.rs:3095) on one raster block;
+    returns the chosen levels (16,) int16."""
+    b = np.ascontiguousarray(np.asarray(block, np.int16).reshape(16)).copy()
+    load().vo_trellis_quantize_block(ptr(b), dc, ac, first_coeff, entry_ctx3, plane, lam)
+    return b
+
+
+def coeff_token_bits(plane, i, ctx3, prev_was_zero, level):
+    return load().vo_coeff_token_bits(plane, i, ctx3, int(bool(prev_was_zero)), level)
+
+
+def eob_token_bits(plane, i, ctx3):
+    return load().vo_eob_token_bits(plane, i, ctx3)
+
+
+def trellis_lambda(y1_ac, strength):
+    return load().vo_trellis_lambda(y1_ac, strength)
+
+
+def idct_basis_norm_sq():
+    p = load().vo_idct_basis_norm_sq()
+    return np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_double)), shape=(16,)).copy()
 
 
 def reconstruct_inter_frame(frame, refs, ref_ids, decisions, quant, out, mb_segment=None, segment_quant=None,
                             segment_abs=False, full_pixel=False, filter_set=abi.FILTER_SIXTAP, lf_info=None,
-                            threads=1):
-    """pick_mb_for_ref's chosen-mode §18 + §14 step (trellis off) for a
-    frame into the MB-padded planes `out` in place. Returns
+                            threads=1, trellis_strength=0.0):
+    """pick_mb_for_ref's chosen-mode §18 + §14 step (with the §13 trellis at
+    TrellisStrength `trellis_strength`; 0 = off) for a frame into the
+    MB-padded planes `out` in place. Returns
     (coeffs (mb_rows*mb_cols, 400) int16, flags (mb_rows*mb_cols,) uint8,
     number of MBs left untouched); `lf_info` (optional MB_LF_INFO_DTYPE
     array) receives the §15 side information."""
@@ -547,10 +583,11 @@ def reconstruct_inter_frame(frame, refs, ref_ids, decisions, quant, out, mb_segm
     fl = np.zeros(n, np.uint8)
     seg = None if mb_segment is None else np.ascontiguousarray(np.asarray(mb_segment, np.int8).reshape(-1))
     sq = None if segment_quant is None else np.ascontiguousarray(np.asarray(segment_quant, np.int16).reshape(4))
-    skipped = load().vo_reconstruct_inter_frame(C.byref(f), C.cast(parr, C.c_void_p), ptr(ids), len(prs), ptr(dec),
-                                                C.byref(quant), ptr(seg), ptr(sq), int(bool(segment_abs)),
-                                                int(bool(full_pixel)), filter_set, C.byref(op), ptr(cf), ptr(fl),
-                                                ptr(lf_info), threads)
+    skipped = load().vo_reconstruct_inter_frame_trellis(C.byref(f), C.cast(parr, C.c_void_p), ptr(ids), len(prs),
+                                                        ptr(dec), C.byref(quant), ptr(seg), ptr(sq),
+                                                        int(bool(segment_abs)), int(bool(full_pixel)), filter_set,
+                                                        C.byref(op), ptr(cf), ptr(fl), ptr(lf_info),
+                                                        float(trellis_strength), threads)
     return cf, fl, skipped
 
 

@@ -266,8 +266,29 @@ static void idct_add(const int16_t* dq, uint8_t* plane, int n, int bi, int bj) {
  * u 64, v 64) and receives the reconstruction. coeffs gets the quantised
  * MbCoeffs (y2[16], y[16][16], u[4][16], v[4][16]); returns bit 0 = the
  * §11.1 mb_skip_coeff, bit 1 = mb_has_coeffs. */
+void vo_trellis_quantize_block(int16_t* block, int16_t dc, int16_t ac, int first_coeff, int entry_ctx3, int plane,
+                               double lambda);
+
+/* Quantise one block: plain rounding, or the §13 trellis when tlambda > 0
+ * (every inter call site uses entry context 0; planes are BlockType
+ * indices: 0 YAfterY2, 1 Y2, 2 UV, 3 YNoY2). */
+static void quantize(int16_t* blk, int16_t dc, int16_t ac, int first_coeff, int plane, double tlambda) {
+  if (tlambda > 0.0) vo_trellis_quantize_block(blk, dc, ac, first_coeff, 0, plane, tlambda);
+  else vo_enc_quantize_block(blk, dc, ac);
+}
+
+int vo_reconstruct_inter_mb_trellis(const uint8_t* src384, uint8_t* pred, const int16_t* f, int split,
+                                    int16_t* coeffs, double tlambda);
+
 int vo_reconstruct_inter_mb(const uint8_t* src384, uint8_t* pred, const int16_t* f, int split,
                             int16_t* coeffs) {
+  return vo_reconstruct_inter_mb_trellis(src384, pred, f, split, coeffs, 0.0);
+}
+
+/* vo_reconstruct_inter_mb with the §13 trellis at `tlambda`
+ * (MbRdCtx::trellis_lambda; 0 = plain rounding). */
+int vo_reconstruct_inter_mb_trellis(const uint8_t* src384, uint8_t* pred, const int16_t* f, int split,
+                                    int16_t* coeffs, double tlambda) {
   int16_t* y2 = coeffs;
   int16_t* y = coeffs + 16;
   int16_t* u = coeffs + 272;
@@ -287,9 +308,9 @@ int vo_reconstruct_inter_mb(const uint8_t* src384, uint8_t* pred, const int16_t*
       y[b * 16] = 0;
     }
     vo_forward_wht_4x4(dcs, y2);
-    vo_enc_quantize_block(y2, f[2], f[3]);
+    quantize(y2, f[2], f[3], 0, 1, tlambda);
   }
-  for (int b = 0; b < 16; b++) vo_enc_quantize_block(y + b * 16, f[0], f[1]);
+  for (int b = 0; b < 16; b++) quantize(y + b * 16, f[0], f[1], split ? 0 : 1, split ? 3 : 0, tlambda);
   /* transform_chroma_plane_rd, U then V */
   for (int p = 0; p < 2; p++) {
     int16_t* dst = p ? v : u;
@@ -298,7 +319,7 @@ int vo_reconstruct_inter_mb(const uint8_t* src384, uint8_t* pred, const int16_t*
         int16_t res[16];
         residual_4x4(src384 + 256 + 64 * p, pred + 256 + 64 * p, 8, i, j, res);
         vo_forward_dct_4x4(res, dst + (i * 2 + j) * 16);
-        vo_enc_quantize_block(dst + (i * 2 + j) * 16, f[4], f[5]);
+        quantize(dst + (i * 2 + j) * 16, f[4], f[5], 0, 2, tlambda);
       }
   }
   /* §11.1 skip detection (src/encoder.rs:8745-8769) */
@@ -352,6 +373,7 @@ typedef struct {
   const vp8a_mb_decision* dec;
   const int8_t* mb_segment;
   int16_t fset[5][6];
+  double tlambda[5];
   int full_pixel, filter_set;
   vp8a_planes* out;
   int16_t* coeffs;
@@ -384,7 +406,8 @@ static void recon_row(void* arg, uint32_t row) {
     extract_mb(j->frame, row, col, src, src + 256, src + 320);
     const int seg = j->mb_segment ? j->mb_segment[idx] : -1;
     const int16_t* f = j->fset[(seg >= 0 && seg < 4) ? 1 + seg : 0];
-    const int fl = vo_reconstruct_inter_mb(src, mb, f, split, cf);
+    const int fl = vo_reconstruct_inter_mb_trellis(src, mb, f, split, cf,
+                                                   j->tlambda[(seg >= 0 && seg < 4) ? 1 + seg : 0]);
     if (j->flags) j->flags[idx] = (uint8_t)fl;
     if (j->lf) {
       /* The §15 side information of the MB (SPLITMV as B_PRED,
@@ -406,6 +429,16 @@ static void recon_row(void* arg, uint32_t row) {
   }
 }
 
+double vo_trellis_lambda(int16_t y1_ac, double strength);
+
+int vo_reconstruct_inter_frame_trellis(const vp8a_i420* frame, const vp8a_planes* refs,
+                                       const uint8_t* ref_ids, uint32_t n_refs,
+                                       const vp8a_mb_decision* dec, const vp8a_quant_indices* qi,
+                                       const int8_t* mb_segment, const int16_t* segment_quant,
+                                       int segment_abs, int full_pixel, int filter_set,
+                                       vp8a_planes* out, int16_t* coeffs, uint8_t* flags,
+                                       vp8a_mb_lf_info* lf, double trellis_strength, uint32_t threads);
+
 int vo_reconstruct_inter_frame(const vp8a_i420* frame, const vp8a_planes* refs,
                                const uint8_t* ref_ids, uint32_t n_refs,
                                const vp8a_mb_decision* dec, const vp8a_quant_indices* qi,
@@ -413,6 +446,21 @@ int vo_reconstruct_inter_frame(const vp8a_i420* frame, const vp8a_planes* refs,
                                int segment_abs, int full_pixel, int filter_set,
                                vp8a_planes* out, int16_t* coeffs, uint8_t* flags,
                                vp8a_mb_lf_info* lf, uint32_t threads) {
+  return vo_reconstruct_inter_frame_trellis(frame, refs, ref_ids, n_refs, dec, qi, mb_segment, segment_quant,
+                                            segment_abs, full_pixel, filter_set, out, coeffs, flags, lf, 0.0,
+                                            threads);
+}
+
+/* vo_reconstruct_inter_frame with the §13 trellis at TrellisStrength
+ * `trellis_strength` (clamped to 0..=8, NaN = 1.0; 0 = off): each factor
+ * set's trellis lambda is rd_lambda(factors) * strength * 0.04. */
+int vo_reconstruct_inter_frame_trellis(const vp8a_i420* frame, const vp8a_planes* refs,
+                                       const uint8_t* ref_ids, uint32_t n_refs,
+                                       const vp8a_mb_decision* dec, const vp8a_quant_indices* qi,
+                                       const int8_t* mb_segment, const int16_t* segment_quant,
+                                       int segment_abs, int full_pixel, int filter_set,
+                                       vp8a_planes* out, int16_t* coeffs, uint8_t* flags,
+                                       vp8a_mb_lf_info* lf, double trellis_strength, uint32_t threads) {
   recon_job j;
   memset(&j, 0, sizeof j);
   j.frame = frame;
@@ -424,6 +472,9 @@ int vo_reconstruct_inter_frame(const vp8a_i420* frame, const vp8a_planes* refs,
   vo_segment_factors(qi, 0, 0, 0, j.fset[0]);
   for (int k = 0; k < 4; k++)
     vo_segment_factors(qi, 1, segment_quant ? segment_quant[k] : 0, segment_abs, j.fset[1 + k]);
+  double s = trellis_strength != trellis_strength ? 1.0 : trellis_strength;
+  s = s < 0.0 ? 0.0 : (s > 8.0 ? 8.0 : s);
+  for (int k = 0; k < 5; k++) j.tlambda[k] = vo_trellis_lambda(j.fset[k][1], s);
   j.full_pixel = full_pixel;
   j.filter_set = filter_set;
   j.out = out;

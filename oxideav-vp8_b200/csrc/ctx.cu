@@ -295,6 +295,14 @@ vp8a_status vp8a_ctx_set_wait_limit(vp8a_ctx* ctx, uint64_t polls) {
   return VP8A_OK;
 }
 
+vp8a_status vp8a_ctx_set_trellis_strength(vp8a_ctx* ctx, double strength) {
+  if (!ctx) return VP8A_E_INVALID_ARGUMENT;
+  // TrellisStrength::new (src/encoder.rs:2686-2692): NaN is the default,
+  // the rest is clamped to 0..=8.
+  ctx->trellis_strength = strength != strength ? 1.0 : (strength < 0.0 ? 0.0 : (strength > 8.0 ? 8.0 : strength));
+  return VP8A_OK;
+}
+
 vp8a_status vp8a_ctx_set_subpel_planes(vp8a_ctx* ctx, uint32_t on) {
   if (!ctx) return VP8A_E_INVALID_ARGUMENT;
   ctx->subpel_planes = on != 0;

@@ -16,7 +16,9 @@
 // prediction. All arithmetic is the reference's integer listing: the
 // forward transforms in int, the inverse DCT in wrapping 32-bit int.
 #include <algorithm>
+#include <mutex>
 
+#include "coeff_tables.h"
 #include "vp8a_internal.cuh"
 
 namespace {
@@ -76,6 +78,11 @@ struct RcArgs {
   int16_t* coeffs;
   uint8_t* flags;
   vp8a_mb_lf_info* lf;
+  // §13 trellis: lambda per factor set (0 = plain rounding), the
+  // bool_bits cost table and the IDCT basis norms by scan position.
+  double tl[5];
+  const double* bit_cost;
+  double norm[16];
 };
 
 __device__ __forceinline__ int cmul(int i) { return i + ((i * COS8) >> 16); }
@@ -84,7 +91,7 @@ __device__ __forceinline__ int rdiv2(int v) {
   const int r = v >= 0 ? (v + 1) >> 1 : -((-v + 1) >> 1);
   return r < -32768 ? -32768 : (r > 32767 ? 32767 : r);
 }
-__device__ __forceinline__ int to16(int v) { return (int)(short)v; }
+__host__ __device__ __forceinline__ int to16(int v) { return (int)(short)v; }
 
 // forward_dct_4x4_scalar (src/forward_transform.rs:486-604), in place.
 __device__ __forceinline__ void fdct4x4(int* b) {
@@ -154,12 +161,12 @@ __device__ __forceinline__ void iwht4x4(int* b) {
 }
 
 // Two's-complement 32-bit arithmetic (the reference's wrapping_* ops).
-__device__ __forceinline__ int wa(int a, int b) { return (int)((unsigned)a + (unsigned)b); }
-__device__ __forceinline__ int ws(int a, int b) { return (int)((unsigned)a - (unsigned)b); }
-__device__ __forceinline__ int wm(int a, int b) { return (int)((unsigned)a * (unsigned)b); }
+__host__ __device__ __forceinline__ int wa(int a, int b) { return (int)((unsigned)a + (unsigned)b); }
+__host__ __device__ __forceinline__ int ws(int a, int b) { return (int)((unsigned)a - (unsigned)b); }
+__host__ __device__ __forceinline__ int wm(int a, int b) { return (int)((unsigned)a * (unsigned)b); }
 
 // inverse_dct_4x4_scalar (src/inverse_transform.rs:609-712), in place.
-__device__ __forceinline__ void idct4x4(int* b) {
+__host__ __device__ __forceinline__ void idct4x4(int* b) {
   int t[16];
 #pragma unroll
   for (int col = 0; col < 4; col++) {
@@ -194,6 +201,182 @@ __device__ __forceinline__ void idct4x4(int* b) {
 __device__ __forceinline__ int rdiv(int num, int den, uint32_t m) {
   const uint32_t q = __umulhi((uint32_t)abs(num) + (uint32_t)(den >> 1), m);
   return to16(num >= 0 ? (int)q : -(int)q);
+}
+
+// ---------------------------------------------- §13 trellis quantiser
+//
+// trellis_quantize_block with the direct scan (src/encoder.rs:3095-3129,
+// :3468-3582), one block per lane: a Viterbi pass over the scan positions
+// up to the last one whose rounded level is non-zero, the survivors keyed
+// by the carried §13.3 context (0 / 1 / >= 2), candidates round, round - 1
+// and 0, cost = distortion (IDCT basis norm x transform-domain error^2) +
+// lambda x token bits (coeff_token_bits, :2789-2817, priced against the
+// §13.5 default probabilities through bool_bits), and the end of the block
+// chosen among the positions that hold a non-zero level. Every f64
+// expression keeps the reference's operation order (the library is built
+// without fused multiply-adds). Every inter call site uses entry
+// context 0.
+static __constant__ uint8_t c_tprobs[4][8][3][11] = VP8A_DEFAULT_COEFF_PROBS_INIT;
+static __constant__ uint8_t c_tbands[16] = {0, 1, 2, 3, 6, 4, 5, 6, 6, 6, 6, 6, 6, 6, 6, 7};
+static __constant__ uint8_t c_zigzag[16] = {0, 1, 4, 8, 5, 2, 3, 6, 9, 12, 13, 10, 7, 11, 14, 15};
+// Each token's (probability index, bit) path through the §13.2 coefficient
+// tree from the root (DCT_0..DCT_4, cat1..cat6); the first step is the "not
+// EOB" branch, skipped after a DCT_0.
+static __constant__ uint8_t c_tpath_len[11] = {2, 3, 5, 6, 6, 6, 6, 7, 7, 7, 7};
+static __constant__ uint8_t c_tpath[11][7][2] = {
+    {{0, 1}, {1, 0}},
+    {{0, 1}, {1, 1}, {2, 0}},
+    {{0, 1}, {1, 1}, {2, 1}, {3, 0}, {4, 0}},
+    {{0, 1}, {1, 1}, {2, 1}, {3, 0}, {4, 1}, {5, 0}},
+    {{0, 1}, {1, 1}, {2, 1}, {3, 0}, {4, 1}, {5, 1}},
+    {{0, 1}, {1, 1}, {2, 1}, {3, 1}, {6, 0}, {7, 0}},
+    {{0, 1}, {1, 1}, {2, 1}, {3, 1}, {6, 0}, {7, 1}},
+    {{0, 1}, {1, 1}, {2, 1}, {3, 1}, {6, 1}, {8, 0}, {9, 0}},
+    {{0, 1}, {1, 1}, {2, 1}, {3, 1}, {6, 1}, {8, 0}, {9, 1}},
+    {{0, 1}, {1, 1}, {2, 1}, {3, 1}, {6, 1}, {8, 1}, {10, 0}},
+    {{0, 1}, {1, 1}, {2, 1}, {3, 1}, {6, 1}, {8, 1}, {10, 1}},
+};
+// DCT_extra categories: extra-bit probabilities, their count, base values.
+static __constant__ uint8_t c_pcat[6][11] = {{159},
+                                             {165, 145},
+                                             {173, 148, 140},
+                                             {176, 155, 140, 135},
+                                             {180, 157, 141, 134, 130},
+                                             {254, 254, 243, 230, 196, 177, 153, 140, 133, 130, 129}};
+static __constant__ uint8_t c_pcat_len[6] = {1, 2, 3, 4, 5, 11};
+static __constant__ uint16_t c_cat_base[6] = {5, 7, 11, 19, 35, 67};
+
+// bool_bits (src/encoder.rs:2229).
+__device__ __forceinline__ double tbb(const double* t, int prob, int v) {
+  if (v) {
+    const int idx = 256 - prob;
+    return t[idx > 255 ? 255 : idx];
+  }
+  return t[prob];
+}
+
+// coeff_token_bits (src/encoder.rs:2789-2817).
+__device__ double token_bits(const double* t, int plane, int i, int ctx3, bool pwz, uint32_t level) {
+  const uint8_t* probs = c_tprobs[plane][c_tbands[i]][ctx3];
+  const int token = level <= 4 ? (int)level
+                               : (level <= 6 ? 5 : (level <= 10 ? 6 : (level <= 18 ? 7 : (level <= 34 ? 8 : (level <= 66 ? 9 : 10)))));
+  double bits = 0.0;
+  for (int s = pwz ? 1 : 0; s < c_tpath_len[token]; s++)
+    bits += tbb(t, probs[c_tpath[token][s][0]], c_tpath[token][s][1]);
+  if (token >= 5) {
+    const int cat = token - 5, n = c_pcat_len[cat];
+    const uint32_t extra = level - c_cat_base[cat];
+    for (int j = 0; j < n; j++) bits += tbb(t, c_pcat[cat][j], (int)((extra >> (n - 1 - j)) & 1u));
+  }
+  if (level != 0) bits += tbb(t, 128, 0);
+  return bits;
+}
+
+// eob_token_bits (src/encoder.rs:2825-2831).
+__device__ __forceinline__ double eob_bits(const double* t, int plane, int i, int ctx3) {
+  return tbb(t, c_tprobs[plane][c_tbands[i]][ctx3][0], 0);
+}
+
+// The trellis on one raster block `b` (the transform's output; replaced by
+// the chosen levels).
+__device__ void trellis_block(int* b, int dc, int ac, int first, int plane, double lambda, const RcArgs& a) {
+  const double* t = a.bit_cost;
+  const uint32_t dc_q = (uint32_t)dc, ac_q = (uint32_t)ac;
+  uint32_t ax[16], mr[16];
+  double zd[16], suffix[17];
+  unsigned negative = 0;
+  int last = -1;
+  suffix[16] = 0.0;
+#pragma unroll
+  for (int k = 15; k >= 0; k--) {
+    if (k < first) {
+      suffix[k] = 0.0;
+      ax[k] = mr[k] = 0;
+      zd[k] = 0.0;
+      continue;
+    }
+    const int x = b[c_zigzag[k]];
+    const uint32_t q = k == 0 ? dc_q : ac_q;
+    ax[k] = (uint32_t)(x < 0 ? -x : x);
+    if (x < 0) negative |= 1u << k;
+    mr[k] = (ax[k] + q / 2) / q;  // rounded_level (:3608-3615)
+    if (mr[k] != 0 && last < 0) last = k;
+    zd[k] = a.norm[k] * (double)((unsigned long long)ax[k] * ax[k]);
+    suffix[k] = suffix[k + 1] + zd[k];
+  }
+#pragma unroll
+  for (int k = 0; k < 16; k++) b[k] = 0;
+  if (last < 0) return;
+  const double INF = __longlong_as_double(0x7ff0000000000000LL);
+  double sc[3] = {0.0, INF, INF};  // entry context 0
+  bool sp[3] = {false, false, false};
+  uint16_t cl[16][3];
+  uint8_t cp[16][3];
+  double best_term = 0.0 + lambda * eob_bits(t, plane, first, 0) + suffix[first];
+  int best_pos = -1, best_ctx = 0;
+  for (int k = first; k <= last; k++) {
+    const uint32_t m = mr[k];
+    const uint32_t q = k == 0 ? dc_q : ac_q;
+    const uint32_t cands[3] = {m, m > 0 ? m - 1 : 0u, 0u};
+    const int ncand = (int)(m < 2 ? m : 2) + 1;
+    double cd[3];
+    for (int c = 0; c < ncand; c++) {
+      if (cands[c] == 0) {
+        cd[c] = zd[k];
+      } else {
+        const long long err = (long long)ax[k] - (long long)cands[c] * (long long)q;
+        cd[c] = a.norm[k] * (double)(err * err);
+      }
+    }
+    double nc[3] = {INF, INF, INF};
+    bool np[3] = {false, false, false};
+    uint16_t nl[3] = {0, 0, 0};
+    uint8_t npv[3] = {0, 0, 0};
+    for (int in_ctx = 0; in_ctx < 3; in_ctx++) {
+      const double base = sc[in_ctx];
+      if (base >= INF) continue;
+      for (int c = 0; c < ncand; c++) {
+        const uint32_t level = cands[c];
+        const double r = token_bits(t, plane, k, in_ctx, sp[in_ctx], level);
+        const double cost = base + cd[c] + lambda * r;
+        const int out = level == 0 ? 0 : (level == 1 ? 1 : 2);
+        if (cost < nc[out]) {
+          nc[out] = cost;
+          np[out] = level == 0;
+          nl[out] = (uint16_t)level;
+          npv[out] = (uint8_t)in_ctx;
+        }
+      }
+    }
+    for (int c = 0; c < 3; c++) {
+      cl[k][c] = nl[c];
+      cp[k][c] = npv[c];
+    }
+    for (int out = 1; out < 3; out++) {
+      const double cost = nc[out];
+      if (cost >= INF) continue;
+      const double term = k + 1 < 16 ? cost + lambda * eob_bits(t, plane, k + 1, out) + suffix[k + 1] : cost;
+      if (term < best_term) {
+        best_term = term;
+        best_pos = k;
+        best_ctx = out;
+      }
+    }
+    for (int c = 0; c < 3; c++) {
+      sc[c] = nc[c];
+      sp[c] = np[c];
+    }
+  }
+  if (best_pos >= 0) {
+    int k = best_pos, ctx = best_ctx;
+    for (;;) {
+      const int level = cl[k][ctx];
+      b[c_zigzag[k]] = (negative >> k & 1u) ? -level : level;
+      if (k == first) break;
+      ctx = cp[k][ctx];
+      k--;
+    }
+  }
 }
 
 // CTA `cta` of the `ncta` working on `a`: one warp per MB, grid-stride.
@@ -290,9 +473,17 @@ __device__ __forceinline__ void recon_body(const RcArgs& a, uint32_t cta, uint32
     const bool active = luma || chroma || (lane == 24 && !split);
     int nz = 0;
     if (active) {
-      blk[0] = rdiv(blk[0], qdc, mdc);
+      const double tl = a.tl[fs];
+      if (tl > 0.0) {
+        // BlockType planes: 0 YAfterY2 (from coefficient 1), 1 Y2, 2 UV,
+        // 3 YNoY2 (SPLITMV luma).
+        trellis_block(blk, qdc, qac, (luma && !split) ? 1 : 0, lane == 24 ? 1 : (chroma ? 2 : (split ? 3 : 0)), tl,
+                      a);
+      } else {
+        blk[0] = rdiv(blk[0], qdc, mdc);
 #pragma unroll
-      for (int k = 1; k < 16; k++) blk[k] = rdiv(blk[k], qac, mac);
+        for (int k = 1; k < 16; k++) blk[k] = rdiv(blk[k], qac, mac);
+      }
 #pragma unroll
       for (int k = 0; k < 16; k++) nz |= blk[k];
     }
@@ -369,6 +560,26 @@ __global__ void __launch_bounds__(RC_WARPS * 32)
 }
 
 int g_rc_blocks_per_sm = 0;
+
+// IDCT_BASIS_NORM_SQ (src/encoder.rs:2763-2777): the energy of the §14.4
+// inverse DCT of a 256 impulse at each scan position's raster index, over
+// 256^2 (exact in f64).
+const double* idct_basis_norms() {
+  static double norms[16];
+  static std::once_flag once;
+  std::call_once(once, [] {
+    static const int zz[16] = {0, 1, 4, 8, 5, 2, 3, 6, 9, 12, 13, 10, 7, 11, 14, 15};
+    for (int k = 0; k < 16; k++) {
+      int b[16] = {0};
+      b[zz[k]] = 256;
+      idct4x4(b);
+      double e = 0.0;
+      for (int i = 0; i < 16; i++) e += (double)b[i] * (double)b[i];
+      norms[k] = e / (256.0 * 256.0);
+    }
+  });
+  return norms;
+}
 
 // Validate one frame's arguments, queue (or, with `defer`, prepare) its
 // prediction into `recon`, and fill the reconstruction kernel's arguments
@@ -459,6 +670,15 @@ vp8a_status prepare_recon(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_i420* fram
   for (int k = 0; k < 4; k++) vp8a_dequant_factors(quant, 1, sq[k], segment_abs, a.f[1 + k]);
   for (int k = 0; k < 5; k++)
     for (int i = 0; i < 6; i++) a.m[k][i] = (uint32_t)((((uint64_t)1 << 32) + a.f[k][i] - 1) / a.f[k][i]);
+  // The trellis price per factor set: MbRdCtx::trellis_lambda, rd_lambda
+  // (y1_ac^2 / 32, src/encoder.rs:3742) x strength x TRELLIS_LAMBDA_SCALE.
+  for (int k = 0; k < 5; k++) {
+    const double q = (double)a.f[k][1];
+    const double lambda = q * q / 32.0;
+    a.tl[k] = ctx->trellis_strength > 0.0 ? lambda * (ctx->trellis_strength * 0.04) : 0.0;
+  }
+  a.bit_cost = ctx->d_bit_cost;
+  memcpy(a.norm, idct_basis_norms(), sizeof a.norm);
   if (mb_segment) {
     if ((s = st.in(mb_segment, a.n, &d)) != VP8A_OK) return s;
     a.mb_segment = (const int8_t*)d;

@@ -45,6 +45,9 @@ struct vp8a_ctx {
   // The analysis reads its half- and quarter-pel predictions from planes
   // precomputed per call (vp8a_ctx_set_subpel_planes).
   bool subpel_planes = true;
+  // TrellisStrength of the reconstructions (vp8a_ctx_set_trellis_strength;
+  // 0 = plain rounding).
+  double trellis_strength = 0.0;
   int force_layout[3] = {0, 0, 0};
   std::map<std::array<int64_t, 6>, std::array<int, 3>> lf_tuned;
   int last_layout[4] = {0, 0, 0, 0};

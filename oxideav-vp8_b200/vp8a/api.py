@@ -54,6 +54,10 @@ class Context:
     def synchronize(self):
         check(self._lib.vp8a_ctx_synchronize(self.handle), "vp8a_ctx_synchronize")
 
+    def set_trellis_strength(self, strength):
+        """TrellisStrength of this context's reconstructions (0 = plain rounding)."""
+        check(self._lib.vp8a_ctx_set_trellis_strength(self.handle, float(strength)), "vp8a_ctx_set_trellis_strength")
+
     def set_subpel_planes(self, on):
         """Precomputed sub-pel planes for the analysis refinements (default on)."""
         check(self._lib.vp8a_ctx_set_subpel_planes(self.handle, int(bool(on))), "vp8a_ctx_set_subpel_planes")

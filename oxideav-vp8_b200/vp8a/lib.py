@@ -25,6 +25,7 @@ PROTOTYPES = {
     "vp8a_ctx_set_autotune": (C.c_int, [P, U32]),
     "vp8a_select_filter_params_batch": (C.c_int, [P, P, U32, P, P]),
     "vp8a_ctx_set_subpel_planes": (C.c_int, [P, U32]),
+    "vp8a_ctx_set_trellis_strength": (C.c_int, [P, C.c_double]),
     "vp8a_ctx_force_sweep_layout": (C.c_int, [P, U32, U32, U32]),
     "vp8a_ctx_last_sweep_layout": (C.c_int, [P, P]),
     "vp8a_last_error": (C.c_char_p, []),

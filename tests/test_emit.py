@@ -23,7 +23,8 @@ def analysed(w, h, seed, qi=40, n_refs=3, segments=None):
 
 
 def encode_and_decode(oracle, w, h, seed, qi=40, n_refs=3, n_partitions=1, level=20, sharpness=2, simple=False,
-                      segment_quant=None, segment_lf=None, token_updates=None, fit_skip=False, lf_deltas=None):
+                      segment_quant=None, segment_lf=None, token_updates=None, fit_skip=False, lf_deltas=None,
+                      trellis_strength=0.0):
     frames, refs, src = analysed(w, h, seed, n_refs=n_refs)
     ids = IDS[:n_refs]
     dec = np.asarray(oracle.analyse_inter_frame(src, refs, ids, vp8a.rd_lambda(qi))).reshape(-1)
@@ -35,7 +36,8 @@ def encode_and_decode(oracle, w, h, seed, qi=40, n_refs=3, n_partitions=1, level
         seg = np.random.default_rng(seed).integers(0, 4, n).astype(np.int8)
     lf_info = np.zeros(n, abi.MB_LF_INFO_DTYPE)
     cf, fl, _ = oracle.reconstruct_inter_frame(src, refs, ids, dec, quant, recon, mb_segment=seg,
-                                               segment_quant=segment_quant, lf_info=lf_info)
+                                               segment_quant=segment_quant, lf_info=lf_info,
+                                               trellis_strength=trellis_strength)
     kw = {}
     if segment_quant is not None:
         kw.update(segmentation=1, segment_quant=list(segment_quant))
@@ -148,3 +150,16 @@ def test_header_errors():
     assert e.value.status == abi.E_INVALID_ARGUMENT
     # An all-ZEROMV, all-skip frame is a few bytes.
     assert len(vp8a.write_inter_frame(abi.frame_header(32, 32, q), dec, cf)) < 80
+
+
+@pytest.mark.parametrize("strength,segments", [(1.0, False), (3.0, True), (8.0, False)])
+def test_trellis_frames_decode_in_lockstep(oracle, strength, segments):
+    # The §13 trellis chooses other levels than plain rounding; the frame
+    # written from them must still decode to the same reconstruction, and it
+    # costs fewer bytes.
+    kw = dict(segment_quant=[-6, 0, 9, 20]) if segments else {}
+    r = encode_and_decode(oracle, 176, 144, 11, qi=44, trellis_strength=strength, **kw)
+    check_lockstep(r, oracle)
+    plain = encode_and_decode(oracle, 176, 144, 11, qi=44, **kw)
+    assert not np.array_equal(r["cf"], plain["cf"])
+    assert len(r["bits"]) < len(plain["bits"])

@@ -64,3 +64,27 @@ def test_encode_p_frame_fixed_level_and_simple_filter(ctx, oracle):
     assert got["cfg"].simple == 1
     for a, b in zip(got["post"], filtered):
         assert np.array_equal(a, b)
+
+
+def test_device_trellis_frame_decodes_in_lockstep(oracle):
+    # A P frame reconstructed with the device trellis (TrellisStrength 1.0,
+    # the reference's default) is written and decoded by the decoder
+    # restatement primed with the references: same decisions and
+    # reconstruction, and fewer bytes than with plain rounding.
+    from vp8a import abi, synth
+
+    frames, _ = synth.make_sequence(176, 144, 5, seed=23, pieces=3, occluders=2)
+    refs = [vp8a.pad_to_mb(*frames[k]) for k in (2, 0, 4)]
+    ids = [abi.REF_LAST, abi.REF_GOLDEN, abi.REF_ALTREF]
+    sizes = {}
+    with vp8a.Context(0) as c:
+        for strength in (0.0, 1.0):
+            c.set_trellis_strength(strength)
+            bits, filt, det = vp8a.encode_p_frame(c, frames[3], refs, ids, 44)
+            d = oracle.CapturingDecoder(176, 144)
+            d.prime(refs)
+            back = d.decode(bits)
+            assert np.array_equal(back["dec"]["mode"], det["decisions"]["mode"])
+            assert all(np.array_equal(a, b) for a, b in zip(back["pre"], det["recon"]))
+            sizes[strength] = len(bits)
+    assert sizes[1.0] < sizes[0.0]

@@ -137,3 +137,35 @@ def test_reconstruct_errors(ctx):
         vp8a.reconstruct_inter_frame(ctx, small, refs, [1, 2], dec, abi.quant_indices(40), rec)
     assert e.value.status == abi.E_REFERENCE_DIMENSIONS_MISMATCH
 
+
+
+@pytest.mark.parametrize("strength,qi,segments", [(1.0, 44, False), (1.0, 10, False), (3.5, 80, True),
+                                                  (8.0, 44, False), (0.5, 127, True)])
+def test_reconstruct_with_the_trellis(oracle, strength, qi, segments):
+    # The §13 trellis (TrellisStrength > 0) on every block: the device's
+    # levels, reconstruction and flags equal the oracle's, whole-MB and
+    # SPLITMV MBs alike, with segment quantisers (each its own lambda).
+    frame, refs = frame_case(320, 240, 31)
+    ids = [abi.REF_LAST, abi.REF_GOLDEN, abi.REF_ALTREF]
+    kw = {}
+    if segments:
+        kw = dict(mb_segment=np.random.default_rng(qi).integers(-1, 4, 300).astype(np.int8),
+                  segment_quant=[-10, 0, 7, 25])
+    with vp8a.Context(0) as c:
+        dec = vp8a.analyse_inter_frame(c, frame, refs, ids, vp8a.rd_lambda(qi))
+        assert (dec["mode"] == abi.MODE_SPLIT).any()
+        plain_cf, _ = vp8a.reconstruct_inter_frame(c, frame, refs, ids, dec, abi.quant_indices(qi),
+                                                   tuple(np.zeros_like(p) for p in refs[0]), **kw)
+        c.set_trellis_strength(strength)
+        got = tuple(np.full(p.shape, 7, np.uint8) for p in refs[0])
+        want = tuple(np.full(p.shape, 7, np.uint8) for p in refs[0])
+        gcf, gfl = vp8a.reconstruct_inter_frame(c, frame, refs, ids, dec, abi.quant_indices(qi), got, **kw)
+    wcf, wfl, _ = oracle.reconstruct_inter_frame(frame, refs, ids, dec, abi.quant_indices(qi), want,
+                                                 trellis_strength=strength, threads=8, **kw)
+    bad = np.argwhere((gcf != wcf).any(axis=1)).reshape(-1)
+    assert bad.size == 0, f"coefficients differ in {bad.size} MBs, first {bad[:5]}"
+    assert np.array_equal(gfl, wfl)
+    for g, w in zip(got, want):
+        assert np.array_equal(g, w)
+    assert not np.array_equal(gcf, plain_cf)
+    assert np.count_nonzero(gcf) < np.count_nonzero(plain_cf)
