@@ -25,10 +25,11 @@ back.
 What the device path does not do, as in the rest of this library: the key
 frame that opens a stream is intra coding, so the first group's first
 frame stands in as its own reconstruction (LAST = GOLDEN = ALTREF = that
-frame, MB-padded) and is not coded; intra picking is off and the trellis
-off (the caveat of encode_p_frame). Rate control, scene cuts and golden
-promotion are control plane and keep their defaults (fixed quantiser, no
-promotion).
+frame, MB-padded) and is not coded; intra picking is off. The §13 trellis
+runs at `trellis_strength` (the reference's KeyframeParams default, 1.0,
+unless given; it is set on the context). Rate control, scene cuts and
+golden promotion are control plane and keep their defaults (fixed
+quantiser, no promotion).
 """
 import ctypes as C
 
@@ -83,7 +84,7 @@ class AltrefStreams:
     index, `strength` the ARNR strength. With `write` the frames'
     bitstreams are produced (host writer) and returned."""
 
-    def __init__(self, ctx, sizes, qi=44, strength=3, write=True, n_partitions=1):
+    def __init__(self, ctx, sizes, qi=44, strength=3, write=True, n_partitions=1, trellis_strength=1.0):
         import torch
 
         from .api import rd_lambda
@@ -96,6 +97,7 @@ class AltrefStreams:
         self.lam = rd_lambda(qi)
         self.ctxs = abi.default_mv_contexts()
         self.ids = np.array(REF_IDS, np.uint8)
+        ctx.set_trellis_strength(trellis_strength)
         with torch.cuda.stream(self.stream):
             self.s = [_Stream(torch, w, h, self.dev) for w, h in sizes]
         self.keep = []

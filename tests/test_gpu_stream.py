@@ -15,6 +15,7 @@ pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
 QI, STRENGTH = 44, 3
+TRELLIS = 1.0
 
 
 class OracleStream:
@@ -31,7 +32,7 @@ class OracleStream:
         recon = tuple(np.zeros_like(p) for p in self.refs[0])
         lf = np.zeros(dec.size, abi.MB_LF_INFO_DTYPE)
         cf, fl, _ = o.reconstruct_inter_frame(frame, self.refs, [1, 2, 3], dec, abi.quant_indices(QI), recon,
-                                              lf_info=lf, threads=8)
+                                              lf_info=lf, threads=8, trellis_strength=TRELLIS)
         level, sharp = o.select_filter_params(recon, lf, abi.filter_config(0, 0), frame, threads=8)
         out = o.filter_frame(recon, lf, abi.filter_config(level, sharp)) if level else recon
         h, w = frame[0].shape
@@ -60,13 +61,14 @@ class OracleStream:
         return packets
 
 
-def test_altref_streams_match_the_oracle_walk(ctx, oracle):
+def test_altref_streams_match_the_oracle_walk(oracle):
+    ctx = vp8a.Context(0)  # its own context: the pipeline sets the trellis strength on it
     sizes = [(96, 64), (64, 48), (80, 40)]
     group, n_groups = 4, 2
     seqs = [synth.make_sequence(w, h, group * n_groups, seed=70 + i, pieces=3, occluders=2)[0]
             for i, (w, h) in enumerate(sizes)]
     dev = lambda f: tuple(torch.from_numpy(np.ascontiguousarray(p)).cuda() for p in f)  # noqa: E731
-    streams = AltrefStreams(ctx, sizes, qi=QI, strength=STRENGTH)
+    streams = AltrefStreams(ctx, sizes, qi=QI, strength=STRENGTH, trellis_strength=TRELLIS)
     oracles = [OracleStream(oracle) for _ in sizes]
     kinds_seen, levels_seen = set(), set()
     for gi in range(n_groups):
@@ -84,5 +86,6 @@ def test_altref_streams_match_the_oracle_walk(ctx, oracle):
             ctx.synchronize()
             for dref, oref in zip(streams.references(k), orc.refs):
                 assert all(np.array_equal(d.cpu().numpy(), o) for d, o in zip(dref, oref)), (gi, k)
+    ctx.close()
     assert kinds_seen == {"key", "altref", "inter"}
     assert len(levels_seen) > 1
