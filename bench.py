@@ -797,6 +797,59 @@ def reference_arm(args):
     }
 
 
+def extra_case(ctx, gs, torch, case):
+    """Single-kernel cases over the frame of a GpuStep: `me` (the batched
+    motion descent, vp8a_motion_descent, every MB against LAST from the zero
+    vector: diamond + half + quarter), `lp_windows` (the proposal's cost
+    volumes of every MB against LAST) and `lp_bwd` (one 32 -> 32 conv layer's
+    data and weight gradients over every MB's 32 x 32 map)."""
+    import vp8a
+    from vp8a import abi, learned
+    from vp8a.frames import luma_ref
+
+    lib = ctx._lib
+    with torch.cuda.stream(gs.stream):
+        xy = learned.all_mbs(MB_COLS, MB_ROWS)
+        n = xy.shape[0]
+        if case == "me":
+            src = learned._source_mbs(gs.cur[0], xy, H, W)
+            zero = torch.zeros((n, 2), dtype=torch.int16, device="cuda")
+            outs = [torch.empty((n, 2), dtype=torch.int32, device="cuda") for _ in range(3)]
+            ref = luma_ref(gs.last[0])
+
+            def fn():
+                st = lib.vp8a_motion_descent(ctx.handle, C.byref(ref), src.data_ptr(), xy.data_ptr(), zero.data_ptr(),
+                                             8, n, outs[0].data_ptr(), outs[1].data_ptr(), outs[2].data_ptr())
+                assert st == 0, vp8a.load().vp8a_last_error()
+            fn.keep = (src, zero, outs, ref)
+        elif case == "lp_windows":
+            out = torch.empty((n, 32, 32, 2), dtype=torch.bfloat16, device="cuda")
+            s, r = luma_ref(gs.cur[0]), luma_ref(gs.last[0][:H, :W])
+
+            def fn():
+                st = lib.vp8a_lp_windows(ctx.handle, C.byref(s), C.byref(r), xy.data_ptr(), n, out.data_ptr())
+                assert st == 0, vp8a.load().vp8a_last_error()
+            fn.keep = (out, s, r)
+        elif case == "lp_bwd":
+            g = torch.Generator(device="cuda").manual_seed(5)
+            x = torch.relu(torch.randn(n, 32, 32, 32, device="cuda", generator=g)).to(torch.bfloat16)
+            wt = (torch.randn(32 * 9 * 32, device="cuda", generator=g) * 0.2).to(torch.bfloat16)
+            dy = (torch.randn(n, 32, 32, 32, device="cuda", generator=g) * 0.01).to(torch.bfloat16)
+            dx = torch.empty_like(x)
+            gw = torch.zeros(32 * 9 * 32, device="cuda")
+            gb = torch.zeros(32, device="cuda")
+
+            def fn():
+                st = lib.vp8a_lp_conv_backward(ctx.handle, x.data_ptr(), 32, wt.data_ptr(), 32, n, dy.data_ptr(), 1,
+                                               dx.data_ptr(), gw.data_ptr(), gb.data_ptr())
+                assert st == 0, vp8a.load().vp8a_last_error()
+            fn.keep = (x, wt, dy, dx, gw, gb)
+        else:
+            raise ValueError(case)
+    ctx.synchronize()
+    return fn
+
+
 def case_arm(args):
     """One stage alone on a WxH frame, for profiling captures: runs
     `--warmup` + `--steps` calls of the stage and prints its mean device ms."""
@@ -816,8 +869,10 @@ def case_arm(args):
     else:
         frames, _ = synth.make_sequence(w, h, 16, SEED, pieces=4, occluders=4)
         gs = GpuStep(ctx, frames, vp8a.load(), torch, 0)
+        if args.case == "trellis":
+            ctx.set_trellis_strength(1.0)
         fn = {"arnr": gs.run_arnr, "analysis": gs.run_analysis, "lf": gs.run_lf, "predict": gs.run_predict,
-              "recon": gs.run_recon}[args.case]
+              "recon": gs.run_recon, "trellis": gs.run_recon}.get(args.case) or extra_case(ctx, gs, torch, args.case)
     stream = torch.cuda.ExternalStream(ctx.stream)
     for _ in range(args.warmup):
         fn()
@@ -1478,7 +1533,8 @@ def main():
     ap.add_argument("--no-parity", action="store_true", help="skip the step's parity check against the oracle")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--case", choices=["arnr", "analysis", "lf", "recon", "predict", "predict_mb", "predict_split",
-                                       "batch", "learned", "lp_conv", "rd", "stream"],
+                                       "batch", "learned", "lp_conv", "rd", "stream", "trellis", "me", "lp_windows",
+                                       "lp_bwd"],
                     help="profile one stage alone, or (batch) the batched many-stream path")
     ap.add_argument("--streams", type=int, default=48, help="streams of the batch case")
     ap.add_argument("--train-steps", type=int, default=300, help="training steps of the learned case")
