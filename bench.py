@@ -864,6 +864,7 @@ def case_arm(args):
     MB_COLS, MB_ROWS = (w + 15) // 16, (h + 15) // 16
     N_MB = MB_COLS * MB_ROWS
     ctx = vp8a.Context(0)
+    ctx.set_subpel_planes(args.subpel_planes)
     if args.case in ("predict_mb", "predict_split"):
         fn = batched_predict(ctx, vp8a, torch, args.case == "predict_split")
     else:
@@ -1540,6 +1541,7 @@ def main():
     ap.add_argument("--train-steps", type=int, default=300, help="training steps of the learned case")
     ap.add_argument("--size", default="1920x1080", help="frame size for --case")
     ap.add_argument("--images", type=int, default=8160, help="32 x 32 maps of the lp_conv case")
+    ap.add_argument("--subpel-planes", type=int, default=1, help="analysis sub-pel planes on/off (single-stage cases)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl != "reference":
         log("note: fewer than 3 warm-up steps")

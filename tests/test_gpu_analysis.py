@@ -159,7 +159,16 @@ def test_analysis_with_proposals(ctx, oracle):
     want = oracle.analyse_inter_frame(frames[3], refs, ids, lam, proposals=prop, threads=8)
     got = vp8a.analyse_inter_frame(ctx, frames[3], refs, ids, lam, proposals=prop)
     assert_same(got, want)
-    plain = oracle.analyse_inter_frame(frames[3], refs, ids, lam, threads=8)
-    taken = (want["mode"] == abi.MODE_NEW) & ((want["mv"]["row"] != plain["mv"]["row"]) |
-                                              (want["mv"]["col"] != plain["mv"]["col"]))
-    assert taken.any()
+    # Proposals the search cannot reach are taken: the frame is the
+    # reference moved 30 px right, and every MB proposes that vector.
+    frames, _ = synth.make_sequence(128, 96, 1, seed=4)
+    ref = vp8a.pad_to_mb(*frames[0])
+    y = frames[0][0]
+    cur = (np.ascontiguousarray(np.concatenate([y[:, 30:], np.repeat(y[:, -1:], 30, axis=1)], axis=1)),
+           frames[0][1], frames[0][2])
+    prop = np.zeros((48, 1), abi.MV_DTYPE)
+    prop["col"] = 120
+    want = oracle.analyse_inter_frame(cur, [ref], [1], lam, proposals=prop)
+    got = vp8a.analyse_inter_frame(ctx, cur, [ref], [1], lam, proposals=prop)
+    assert_same(got, want)
+    assert ((want["mode"] == abi.MODE_NEW) & (want["mv"]["col"] == 120)).any()
