@@ -865,6 +865,8 @@ def case_arm(args):
     N_MB = MB_COLS * MB_ROWS
     ctx = vp8a.Context(0)
     ctx.set_subpel_planes(args.subpel_planes)
+    if args.lf_layout:
+        ctx.force_sweep_layout(*(int(v) for v in args.lf_layout.split(",")))
     if args.case in ("predict_mb", "predict_split"):
         fn = batched_predict(ctx, vp8a, torch, args.case == "predict_split")
     else:
@@ -1542,6 +1544,7 @@ def main():
     ap.add_argument("--size", default="1920x1080", help="frame size for --case")
     ap.add_argument("--images", type=int, default=8160, help="32 x 32 maps of the lp_conv case")
     ap.add_argument("--subpel-planes", type=int, default=1, help="analysis sub-pel planes on/off (single-stage cases)")
+    ap.add_argument("--lf-layout", default="", help="passes,threads,prefetch: force the sweep's launch shape (cases)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl != "reference":
         log("note: fewer than 3 warm-up steps")
