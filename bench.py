@@ -536,7 +536,6 @@ def gpu_arm(args):
                 "lf_layout": {"passes_per_cta": lf_layout[0], "threads_per_cta": lf_layout[1],
                               "prefetch": bool(lf_layout[2]), "ctas_per_sm": lf_layout[3],
                               "chosen_by": "autotune (timed on the first sweep of this picture shape)"},
-                "analysis_subpel": "16 sub-pel planes per reference precomputed per frame",
             },
             "e2e": {"value": round(e2e, 1), "unit": "MB/s", "h2d_bytes_per_step": int(ps.h2d),
                     "d2h_bytes_per_step": int(ps.d2h),
@@ -1543,7 +1542,7 @@ def main():
     ap.add_argument("--train-steps", type=int, default=300, help="training steps of the learned case")
     ap.add_argument("--size", default="1920x1080", help="frame size for --case")
     ap.add_argument("--images", type=int, default=8160, help="32 x 32 maps of the lp_conv case")
-    ap.add_argument("--subpel-planes", type=int, default=1, help="analysis sub-pel planes on/off (single-stage cases)")
+    ap.add_argument("--subpel-planes", type=int, default=0, help="analysis sub-pel planes on/off (single-stage cases)")
     ap.add_argument("--lf-layout", default="", help="passes,threads,prefetch: force the sweep's launch shape (cases)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl != "reference":

@@ -452,9 +452,12 @@ vp8a_status prepare_arnr(vp8a_ctx* ctx, vp8a::Stager& st, const vp8a_i420* frame
     return VP8A_E_INVALID_ARGUMENT;
   }
   void *dy, *du, *dv;
-  if ((s = st.out(out.y, ys * (size_t)(oh - 1) + ow, &dy)) != VP8A_OK) return s;
-  if ((s = st.out(out.u, cs * (size_t)(och - 1) + ocw, &du)) != VP8A_OK) return s;
-  if ((s = st.out(out.v, cs * (size_t)(och - 1) + ocw, &dv)) != VP8A_OK) return s;
+  // Padded host planes may have a pitch wider than their rows: staged
+  // in and out, so the bytes between rows come back unchanged.
+  auto stage_out = [&](void* p, size_t bytes, void** d) { return padded ? st.inout(p, bytes, d) : st.out(p, bytes, d); };
+  if ((s = stage_out(out.y, ys * (size_t)(oh - 1) + ow, &dy)) != VP8A_OK) return s;
+  if ((s = stage_out(out.u, cs * (size_t)(och - 1) + ocw, &du)) != VP8A_OK) return s;
+  if ((s = stage_out(out.v, cs * (size_t)(och - 1) + ocw, &dv)) != VP8A_OK) return s;
 
   const int bcols = (w + 15) / 16, brows = (h + 15) / 16;
   const bool filter = strength != 0 && n >= 2;

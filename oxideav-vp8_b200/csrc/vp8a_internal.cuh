@@ -43,8 +43,9 @@ struct vp8a_ctx {
   // CTAs per SM).
   bool autotune = true;
   // The analysis reads its half- and quarter-pel predictions from planes
-  // precomputed per call (vp8a_ctx_set_subpel_planes).
-  bool subpel_planes = true;
+  // precomputed per call (vp8a_ctx_set_subpel_planes; off by default: the
+  // SPLITMV warps, not the refinements, bound each MB's latency).
+  bool subpel_planes = false;
   // TrellisStrength of the reconstructions (vp8a_ctx_set_trellis_strength;
   // 0 = plain rounding).
   double trellis_strength = 0.0;

@@ -213,4 +213,6 @@ def test_sweep_every_launch_shape_gives_the_same_table(oracle, size):
         c.force_sweep_layout(0)
         c.set_autotune(False)
         assert np.array_equal(vp8a.filter_sweep(c, recon, m, base, src, 0), want)
-    assert len(ran) >= 4, ran
+    # 1080p's slot rings leave room for one pass per CTA only; smaller
+    # pictures fit more shapes.
+    assert len(ran) >= (3 if size[0] > 1000 else 6), ran
