@@ -1048,17 +1048,66 @@ def batch_arm(args):
             e.synchronize()
             xs.append(s.elapsed_time(e))
         stages[name] = round(float(np.median(xs)), 3)
-    per_res = {}
-    for r, st in zip(pick, bs.s):
-        k = "%dx%d" % BATCH_RESOLUTIONS[int(r)]
-        d = per_res.setdefault(k, {"streams": 0, "mbs": 0})
-        d["streams"] += 1
-        d["mbs"] += st["mbs"]
+    mixed_layout = ctx.last_sweep_layout()
     ms = float(np.median(ts))
+    n_mb = bs.n_mb
+    # Each resolution's streams as a batch of their own: MB/s and each
+    # stage's algorithmic GB/s (per MB: ARNR 6 frames x 384 B in + 384 out;
+    # analysis source 256 + 2 refs x 256 + decision 104; reconstruction
+    # 1264; LF sweep 774 read once), with the launch shape the sweep's
+    # autotuner picked for that batch.
+    per_alg = {"arnr": (BATCH_LOOKAHEAD + 1) * 384, "analysis": 256 + 2 * 256 + 104, "recon": 1264, "lf": 774}
+    per_res = {}
+    del bs
+    for r in sorted(set(int(x) for x in pick)):
+        sub = [s_ for s_, p_ in zip(streams, pick) if int(p_) == r]
+        rb = BatchStep(ctx, sub, torch)
+        for _ in range(args.warmup):
+            rb.step()
+        ctx.synchronize()
+        rts = []
+        for _ in range(max(3, args.steps // 2)):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            torch.cuda.synchronize()
+            s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s_.record(stream)
+            rb.step()
+            e_.record(stream)
+            e_.synchronize()
+            rts.append(s_.elapsed_time(e_))
+        st_ms = {}
+        for name in ("arnr", "analysis", "recon", "lf"):
+            fn = getattr(rb, "run_" + name)
+            xs = []
+            for _ in range(3):
+                with torch.cuda.stream(stream):
+                    flush.fill_(1)
+                torch.cuda.synchronize()
+                s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s_.record(stream)
+                fn()
+                e_.record(stream)
+                e_.synchronize()
+                xs.append(s_.elapsed_time(e_))
+            st_ms[name] = float(np.median(xs))
+        rms = float(np.median(rts))
+        lay = ctx.last_sweep_layout()
+        per_res["%dx%d" % BATCH_RESOLUTIONS[r]] = {
+            "streams": len(sub), "mbs": rb.n_mb, "ms_per_step": round(rms, 3),
+            "mbs_per_s": round(rb.n_mb / (rms / 1e3), 1),
+            "stage_ms": {k: round(v, 3) for k, v in st_ms.items()},
+            "stage_gbs": {k: round(rb.n_mb * per_alg[k] / (v / 1e3) / 1e9, 2) for k, v in st_ms.items()},
+            "lf_layout": {"passes_per_cta": lay[0], "threads_per_cta": lay[1], "prefetch": bool(lay[2]),
+                          "ctas_per_sm": lay[3]}}
+        del rb
     ctx.close()
     return {"case": "batch", "metric": "MBs/s (ARNR+ME+recon+LF search), batched streams", "unit": "MB/s",
-            "value": round(bs.n_mb / (ms / 1e3), 1), "ms_per_step": round(ms, 3), "steps": args.steps,
-            "warmup": args.warmup, "streams": args.streams, "mbs_per_step": bs.n_mb, "per_resolution": per_res,
+            "value": round(n_mb / (ms / 1e3), 1), "ms_per_step": round(ms, 3), "steps": args.steps,
+            "warmup": args.warmup, "streams": args.streams, "mbs_per_step": n_mb, "per_resolution": per_res,
+            "lf_layout_mixed": {"passes_per_cta": mixed_layout[0], "threads_per_cta": mixed_layout[1],
+                                "prefetch": bool(mixed_layout[2]), "ctas_per_sm": mixed_layout[3],
+                                "chosen_by": "autotune (timed on the first batch of these picture shapes)"},
             "stage_ms": stages, "step_ms": [round(x, 3) for x in ts],
             "config": {"workload": "%d streams from {176x144, 640x360, 1280x720, 1920x1080, 3840x2160}: "
                                    "P frame vs LAST/ALTREF, ARNR(5, centre), qi-44 reconstruction, LF 64x8 sweep"

@@ -1528,37 +1528,82 @@ vp8a_status run_batch(vp8a_ctx* ctx, vp8a::Stager& st, std::vector<LfArgs>& args
   });
   if (!group.empty()) {
     // The layout for the largest job's rings and the group's candidates
-    // (each CTA takes `nc` candidates of one job).
+    // (each CTA takes `nc` candidates of one job): measured on the first
+    // batch of these picture shapes (autotune), else the cost model.
     long n_all = 0;
     for (uint32_t j : group) n_all += args[j].n_cands;
-    SweepLayout L{1, pre, sweep_smem(1, max_ring, pre, threads), threads, 1};
-    if (!pick_layout(ctx, (int)std::min<long>(n_all, 1 << 30), max_ring, pre, threads, true, &L)) {
+    std::vector<SweepLayout> ls;
+    if ((s = sweep_layouts(ctx, (int)std::min<long>(n_all, 1 << 30), max_ring, pre, threads, true, &ls)) != VP8A_OK)
+      return s;
+    if (ls.empty()) {
       vp8a::set_error("no sweep layout fits in shared memory");
       return VP8A_E_CUDA;
     }
-    const int nc = L.nc;
-    pre = L.pre;
-    const size_t total = L.smem;
-    std::vector<LfArgs> table;
-    std::vector<uint32_t> start{0};
-    for (uint32_t j : group) {
-      LfArgs a = args[j];
-      a.smem_slots = 1;
-      a.gslots = nullptr;
-      a.prefetch = pre;
-      a.stage_off = nc * a.ring_bytes;
-      table.push_back(a);
-      start.push_back(start.back() + (uint32_t)((a.n_cands + nc - 1) / nc));
+    auto launch_group = [&](const SweepLayout& L) -> vp8a_status {
+      const int nc = L.nc;
+      std::vector<LfArgs> table;
+      std::vector<uint32_t> start{0};
+      for (uint32_t j : group) {
+        LfArgs a = args[j];
+        a.smem_slots = 1;
+        a.gslots = nullptr;
+        a.prefetch = L.pre;
+        a.stage_off = nc * a.ring_bytes;
+        table.push_back(a);
+        start.push_back(start.back() + (uint32_t)((a.n_cands + nc - 1) / nc));
+      }
+      const size_t o_start = sizeof(LfArgs) * table.size(), bytes = o_start + sizeof(uint32_t) * start.size();
+      std::vector<uint8_t> blob(bytes);
+      memcpy(blob.data(), table.data(), o_start);
+      memcpy(blob.data() + o_start, start.data(), sizeof(uint32_t) * start.size());
+      void* d;
+      vp8a_status e = st.upload(blob.data(), bytes, &d);
+      if (e != VP8A_OK) return e;
+      ctx->last_layout[0] = L.nc;
+      ctx->last_layout[1] = L.threads;
+      ctx->last_layout[2] = L.pre;
+      ctx->last_layout[3] = L.per_sm;
+      return launch_variant(ctx, nc, start.back(), L.threads, L.smem, table[0], (const LfArgs*)d,
+                            (const uint32_t*)((const uint8_t*)d + o_start), (int)table.size());
+    };
+    SweepLayout L = ls[0];
+    model_layout(ctx, (int)std::min<long>(n_all, 1 << 30), threads, ls, &L);
+    bool scored = true;
+    for (uint32_t j : group) scored = scored && args[j].ssd_out != nullptr;
+    if (ctx->autotune && scored && ls.size() > 1) {
+      std::vector<int64_t> key{(int64_t)pre};
+      for (uint32_t j : group) key.insert(key.end(), {args[j].mb_cols, args[j].mb_rows, args[j].n_cands, args[j].steps});
+      auto it = ctx->lf_tuned_batch.find(key);
+      if (it == ctx->lf_tuned_batch.end()) {
+        // Time every feasible layout on this batch (scored sweeps only
+        // write their tables, so repeating one changes nothing).
+        cudaEvent_t e0, e1;
+        VP8A_CUDA(cudaEventCreate(&e0));
+        VP8A_CUDA(cudaEventCreate(&e1));
+        float best = 1e30f;
+        std::array<int, 3> pick{L.nc, L.threads, (int)L.pre};
+        for (const SweepLayout& x : ls) {
+          if ((s = launch_group(x)) != VP8A_OK) break;  // warm
+          if ((s = vp8a::cuda_ok(cudaEventRecord(e0, ctx->stream), "cudaEventRecord")) != VP8A_OK) break;
+          if ((s = launch_group(x)) != VP8A_OK) break;
+          if ((s = vp8a::cuda_ok(cudaEventRecord(e1, ctx->stream), "cudaEventRecord")) != VP8A_OK) break;
+          if ((s = vp8a::cuda_ok(cudaEventSynchronize(e1), "cudaEventSynchronize")) != VP8A_OK) break;
+          float ms = 0.f;
+          cudaEventElapsedTime(&ms, e0, e1);
+          if (ms < best) {
+            best = ms;
+            pick = {x.nc, x.threads, (int)x.pre};
+          }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (s != VP8A_OK) return s;
+        it = ctx->lf_tuned_batch.emplace(key, pick).first;
+      }
+      for (const SweepLayout& x : ls)
+        if (x.nc == it->second[0] && x.threads == it->second[1] && (int)x.pre == it->second[2]) L = x;
     }
-    const size_t o_start = sizeof(LfArgs) * table.size(), bytes = o_start + sizeof(uint32_t) * start.size();
-    std::vector<uint8_t> blob(bytes);
-    memcpy(blob.data(), table.data(), o_start);
-    memcpy(blob.data() + o_start, start.data(), sizeof(uint32_t) * start.size());
-    void* d;
-    if ((s = st.upload(blob.data(), bytes, &d)) != VP8A_OK) return s;
-    if ((s = launch_variant(ctx, nc, start.back(), threads, total, table[0], (const LfArgs*)d,
-                            (const uint32_t*)((const uint8_t*)d + o_start), (int)table.size())) != VP8A_OK)
-      return s;
+    if ((s = launch_group(L)) != VP8A_OK) return s;
   }
   for (uint32_t j : alone)
     if ((s = run_sweep(ctx, args[j], args[j].n_cands, &st)) != VP8A_OK) return s;

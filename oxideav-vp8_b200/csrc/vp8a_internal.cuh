@@ -51,6 +51,7 @@ struct vp8a_ctx {
   double trellis_strength = 0.0;
   int force_layout[3] = {0, 0, 0};
   std::map<std::array<int64_t, 6>, std::array<int, 3>> lf_tuned;
+  std::map<std::vector<int64_t>, std::array<int, 3>> lf_tuned_batch;  // batched sweeps: job shapes -> layout
   int last_layout[4] = {0, 0, 0, 0};
 };
 
