@@ -355,7 +355,8 @@ vp8a_status vp8a_motion_descent(vp8a_ctx* ctx, const vp8a_luma_ref* ref,
  * src/encoder.rs:7573-8246). `refs[k]` (k < n_refs) are MB-padded
  * reference planes in scoring order with ids `ref_ids[k]` (VP8A_REF_*);
  * `mv_contexts` NULL means the §17.2 defaults; `lambda` is the RD
- * multiplier (rd_lambda, src/encoder.rs:3742). Writes mb_cols*mb_rows
+ * multiplier (rd_lambda, src/encoder.rs:3742): finite and >= 0, else
+ * VP8A_E_INVALID_ARGUMENT. Writes mb_cols*mb_rows
  * decisions in raster order; `trace` (optional) receives n_refs entries
  * per MB. The MB-row wavefront runs on the device: MB (r, c) starts once
  * MB (r-1, c) is decided (its census neighbours are the above, left and

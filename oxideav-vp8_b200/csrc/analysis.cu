@@ -125,21 +125,15 @@ struct SplitOut {
 // SPLITMV scratch of one warp. Candidate column layout (fixed, no
 // de-duplication): 0 = ZERO, 1..4 = LEFT vectors of the MB's left column
 // anchors 0/4/8/12, 5..8 = ABOVE vectors of the top-row anchors 0..3,
-// 9..24 = the NEW4X4 result of group 0..15.
-struct SplitScratch {
-  double table[16 * 9];       // group g's SAD at staged column m < 9 (exact in f64): table[g * 9 + m]
+// 9..24 = the NEW4X4 result of group 0..15. Aligned to 16 bytes with a
+// size that is a multiple of 16: every warp's copy moves table columns as
+// 16-byte vectors.
+struct __align__(16) SplitScratch {
+  uint32_t table[CMAX * 16];  // group g's SAD at column m: table[m * 16 + g], needed columns only
   double new_cost[16 * 5];    // lambda * (NEW4X4 mode bits of context x + group g's vector bits)
-  double new_bits[16];        // NEW4X4 vector bits of group g (when new_ok)
-  double bits_a[16];          // group g's sub-MV reference bits
   vp8a_mv cmv[CMAX];
-  uint32_t new_sad[16];
-  uint32_t sad[16];           // group g's SAD at its chosen vector
-  uint8_t new_ok[16];         // group g's NEW differential lies in [-1023, 1023]
-  uint8_t chosen[16];         // column each group chose
-  uint8_t is_new[16];         // group g chose NEW4X4 (adds new_bits[g])
-  uint8_t bad[16];            // group g had no finite choice
-  int colpos[CMAX];           // column m < 9: staged block index; m >= 9: field position or -1
 };
+static_assert(sizeof(SplitScratch) % 16 == 0, "SplitScratch copies stay 16-byte aligned");
 struct Plan {
   int wx0, wy0;        // window origin (plane pixels)
   int hn_x, hn_y;      // NEAREST halo origin
@@ -506,6 +500,10 @@ __device__ void split_partition(const AnArgs& a, const double* pbits, const doub
                                 SplitOut* out, int lane) {
   const int G = pid == 3 ? 16 : (pid == 2 ? 4 : 2);
   const int goff = pid == 0 ? 0 : (pid == 1 ? 2 : 4);
+  // Group `lane`'s NEW4X4 result (lanes < G).
+  bool my_new_ok = false;
+  uint32_t my_new_sad = 0;
+  double my_new_bits = 0.0;
   if (lane < G) {
     // group_small_diamond_search (src/encoder.rs:7812-7879): snap then
     // clamp the centre; N, S, W, E clamped, not snapped; four rounds. Every
@@ -586,12 +584,12 @@ __device__ void split_partition(const AnArgs& a, const double* pbits, const doub
       if (!improved) break;
     }
     W.cmv[9 + g] = best;
-    W.new_sad[g] = bs;
     const int dr = (int)best.row - bp.row, dc = (int)best.col - bp.col;
     const bool ok = dr >= -1023 && dr <= 1023 && dc >= -1023 && dc <= 1023;
     const double nb = ok ? mvb[dr + 1023] + mvb[MV_BITS_SPAN + dc + 1023] : 0.0;
-    W.new_ok[g] = ok;
-    W.new_bits[g] = nb;
+    my_new_ok = ok;
+    my_new_sad = bs;
+    my_new_bits = nb;
 #pragma unroll
     for (int x = 0; x < 5; x++) W.new_cost[g * 5 + x] = a.lambda * (sbits[x * 4 + VP8A_SUBMV_NEW] + nb);
   }
@@ -600,59 +598,75 @@ __device__ void split_partition(const AnArgs& a, const double* pbits, const doub
   if (lane < 9)
     W.cmv[lane] = lane == 0 ? vp8a_mv{0, 0} : (lane < 5 ? ext_left(left, 4 * (lane - 1)) : ext_above(above, lane - 5));
   __syncwarp();
-  // Candidate SADs. Columns 0-8 (ZERO and the neighbours' vectors) are the
-  // staged blocks: their group SADs are tabled, (group, column) pairs over
-  // the lanes. Columns 9+ (the groups' NEW results) lie in the field and
-  // are read from it when the chain needs them.
+  // Lane m < 9 + G holds column m's vector, packed (equal vectors, equal
+  // words; the zero vector is 0).
+  const int ncol = 9 + G;
+  const vp8a_mv mvm = lane < ncol ? W.cmv[lane] : vp8a_mv{0, 0};
+  const uint32_t cvec = (uint32_t)(uint16_t)mvm.row | ((uint32_t)(uint16_t)mvm.col << 16);
+  // The candidate table: lane m fills column m for every group. Columns
+  // 0-8 (ZERO and the neighbours' vectors) are staged blocks; columns 9+
+  // (the groups' NEW results) lie in the field, or, beyond it, are summed
+  // from the plane. Only the columns the partition's choice can reach.
   const uint32_t need = c_need_cols[pid];
-  if (lane < 9 + G && ((need >> lane) & 1u)) {
-    const vp8a_mv mv = W.cmv[lane];
-    const int x = fv.mbx + int_off(mv.col), y = fv.mby + int_off(mv.row);
-    W.colpos[lane] = lane < 9 ? fv.pl->colblk[lane] : fpos(x - fv.cxp, y - fv.cyp);
+  if (lane < ncol && ((need >> lane) & 1u)) {
+    const int x = fv.mbx + int_off(mvm.col), y = fv.mby + int_off(mvm.row);
+    const int cp = lane < 9 ? fv.pl->colblk[lane] : fpos(x - fv.cxp, y - fv.cyp);
+    uint32_t* col = W.table + lane * 16;
+    if (pid == 3 && (lane < 9 || cp >= 0)) {
+      // The 16 block SADs of a staged block or a field position are one
+      // 32-byte row.
+      const uint4* row = lane < 9 ? (const uint4*)fv.xs[cp] : (const uint4*)fv.F->blk[cp];
+      const uint4 lo = row[0], hi = row[1];
+      const uint32_t w[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        ((uint4*)col)[q] = make_uint4(w[2 * q] & 0xffffu, w[2 * q] >> 16, w[2 * q + 1] & 0xffffu, w[2 * q + 1] >> 16);
+    } else {
+      for (int g = 0; g < G; g++) {
+        uint32_t v;
+        if (lane < 9) v = pid == 3 ? fv.xs[cp][g] : group_sum(fv.xs[cp], pid, g);
+        else if (cp >= 0) v = pid == 3 ? fv.F->blk[cp][g] : fv.F->grp[cp][goff + g];
+        else v = direct_group_sad(P, src, x, y, pid, g);
+        col[g] = v;
+      }
+    }
   }
   __syncwarp();
-  for (int q = lane; q < G * 9; q += 32) {
-    const int g = q / 9, m = q - g * 9;
-    if (!((need >> m) & 1u)) continue;
-    const int j = W.colpos[m];  // always staged: the plan stages every one of these vectors
-    W.table[q] = (double)(pid == 3 ? fv.xs[j][g] : group_sum(fv.xs[j], pid, g));
-  }
-  __syncwarp();
-  // Group g's SAD at column m.
-  auto cand = [&](int g, int m) -> double {
-    if (m < 9) return W.table[g * 9 + m];
-    const int p = W.colpos[m];
-    if (p >= 0) return (double)(pid == 3 ? fv.F->blk[p][g] : fv.F->grp[p][goff + g]);
-    const vp8a_mv mv = W.cmv[m];
-    return (double)direct_group_sad(P, src, fv.mbx + int_off(mv.col), fv.mby + int_off(mv.row), pid, g);
-  };
-  // The sub-MV choice. A group's LEFT/ABOVE come from the group to its left
-  // and above, so the groups of one anti-diagonal of the partition's group
-  // grid are independent: step s decides them in parallel, one lane each.
+  // The sub-MV choice. Lane g decides group g. A group's LEFT/ABOVE come
+  // from the group to its left and above, so the groups of one
+  // anti-diagonal of the partition's group grid are independent: step s
+  // decides them in parallel. The columns the neighbouring groups chose
+  // and the vectors they stand for travel by shuffles.
   const int gh = pid == 1 ? 1 : (pid == 3 ? 4 : 2), gw = pid == 0 ? 1 : (pid == 3 ? 4 : 2);
+  const int gr = lane / gw, gc = lane - gr * gw;
+  // The group's top-left block; the blocks left of and above it belong to
+  // the groups (gr, gc - 1) and (gr - 1, gc), or lie outside the MB.
+  const int anchor = gr * (4 / gh) * 4 + gc * (4 / gw);
+  int chosen = 0, mode = VP8A_SUBMV_ZERO, my_ctx = 0;
+  uint32_t my_sad = 0;
+  bool my_bad = false;
   for (int st = 0; st < gh + gw - 1; st++) {
-    const int gr = max(0, st - (gw - 1)) + lane, gc = st - gr;
-    if (gr <= min(gh - 1, st) && gc >= 0) {
-      const int gg = gr * gw + gc;
-      // The group's top-left block; the blocks left of and above it belong
-      // to the groups (gr, gc - 1) and (gr - 1, gc), or lie outside the MB.
-      const int anchor = gr * (4 / gh) * 4 + gc * (4 / gw);
-      const int lidx = gc == 0 ? 1 + (anchor >> 2) : W.chosen[gg - 1];
-      const int aidx = gr == 0 ? 5 + anchor : W.chosen[gg - gw];
-      const vp8a_mv lmv = W.cmv[lidx], amv = W.cmv[aidx];
-      const bool lez = mv_zero(lmv), aez = mv_zero(amv), lea = mv_eq(lmv, amv);
+    const int lch = __shfl_sync(FULL, chosen, gc == 0 ? lane : lane - 1);
+    const int ach = __shfl_sync(FULL, chosen, gr == 0 ? lane : lane - gw);
+    const int lidx = gc == 0 ? 1 + (anchor >> 2) : lch;
+    const int aidx = gr == 0 ? 5 + anchor : ach;
+    const uint32_t lv = __shfl_sync(FULL, cvec, lidx & 31), av = __shfl_sync(FULL, cvec, aidx & 31);
+    if (lane < G && gr + gc == st) {
+      const bool lez = lv == 0u, aez = av == 0u, lea = lv == av;
       const int ctxi = (lea && lez) ? 4 : (lea ? 3 : (aez ? 2 : (lez ? 1 : 0)));
       const double* lt = lterm + ctxi * 4;
-      const double tl = cand(gg, lidx), ta = cand(gg, aidx), tz = W.table[gg * 9];
+      const uint32_t tl = W.table[lidx * 16 + lane], ta = W.table[aidx * 16 + lane], tz = W.table[lane];
       // LEFT, ABOVE, ZERO, then NEW (sad + lambda * (mode bits + vector
       // bits), the vector bits 0 for the first three); strict '<' keeps the
-      // first minimum.
-      const double j0 = tl + lt[0];
-      const double j1 = ta + lt[1];
-      const double j2 = tz + lt[2];
-      double best_j = __longlong_as_double(0x7ff0000000000000LL);
+      // first minimum. Every J is a sum of non-negative finite terms, or
+      // +inf before the first, so J order is the order of the doubles' bit
+      // patterns as unsigned integers.
+      const uint64_t j0 = (uint64_t)__double_as_longlong((double)tl + lt[0]);
+      const uint64_t j1 = (uint64_t)__double_as_longlong((double)ta + lt[1]);
+      const uint64_t j2 = (uint64_t)__double_as_longlong((double)tz + lt[2]);
+      uint64_t best_j = 0x7ff0000000000000ull;
       int best_mode = VP8A_SUBMV_ZERO, best_col = 0;
-      double best_sad = tz;
+      uint32_t best_sad = tz;
       if (j0 < best_j) {
         best_j = j0;
         best_mode = VP8A_SUBMV_LEFT;
@@ -671,33 +685,32 @@ __device__ void split_partition(const AnArgs& a, const double* pbits, const doub
         best_col = 0;
         best_sad = tz;
       }
-      if (W.new_ok[gg]) {
-        const double jn = (double)W.new_sad[gg] + W.new_cost[gg * 5 + ctxi];
+      if (my_new_ok) {
+        const uint64_t jn = (uint64_t)__double_as_longlong((double)my_new_sad + W.new_cost[lane * 5 + ctxi]);
         if (jn < best_j) {
           best_j = jn;
           best_mode = VP8A_SUBMV_NEW;
-          best_col = 9 + gg;
-          best_sad = (double)W.new_sad[gg];
+          best_col = 9 + lane;
+          best_sad = my_new_sad;
         }
       }
-      W.chosen[gg] = (uint8_t)best_col;
-      W.bad[gg] = !isfinite(best_j);
-      W.sad[gg] = (uint32_t)best_sad;
-      W.bits_a[gg] = sbits[ctxi * 4 + best_mode];
-      W.is_new[gg] = best_mode == VP8A_SUBMV_NEW;
-      out->modes[gg] = (uint8_t)best_mode;
+      chosen = best_col;
+      mode = best_mode;
+      my_ctx = ctxi;
+      my_sad = best_sad;
+      my_bad = best_j >= 0x7ff0000000000000ull;
     }
-    __syncwarp();
   }
+  if (lane < G) out->modes[lane] = (uint8_t)mode;
   // Totals in the reference's group order (the f64 sum is order-sensitive):
   // lane g holds group g's terms, every lane sums them in order.
   const bool mine = lane < G;
-  const double ba = mine ? W.bits_a[lane] : 0.0;
-  const double bn = mine && W.is_new[lane] ? W.new_bits[lane] : 0.0;
-  const int isn = mine ? W.is_new[lane] : 0, bad = mine ? W.bad[lane] : 0;
-  const uint32_t sd = mine ? W.sad[lane] : 0u;
+  const bool isn = mine && mode == VP8A_SUBMV_NEW;
+  const double ba = mine ? sbits[my_ctx * 4 + mode] : 0.0;
+  const double bn = isn ? my_new_bits : 0.0;
+  const uint32_t sd = mine ? my_sad : 0u;
   const uint32_t total_sad = __reduce_add_sync(FULL, sd);
-  const unsigned any_bad = __ballot_sync(FULL, bad != 0), news = __ballot_sync(FULL, isn != 0);
+  const unsigned any_bad = __ballot_sync(FULL, mine && my_bad), news = __ballot_sync(FULL, isn);
   double xa[16], xn[16];
 #pragma unroll
   for (int gg = 0; gg < 16; gg++) {
@@ -719,7 +732,11 @@ __device__ void split_partition(const AnArgs& a, const double* pbits, const doub
       for (int i = G; i < 16; i++) out->modes[i] = VP8A_SUBMV_ZERO;
     }
   }
-  if (lane < 16) out->split_mvs[lane] = W.cmv[W.chosen[((lane >> 2) / (4 / gh)) * gw + (lane & 3) / (4 / gw)]];
+  // Block b's vector: the column its group chose.
+  const int gb = lane < 16 ? ((lane >> 2) / (4 / gh)) * gw + (lane & 3) / (4 / gw) : 0;
+  const int cb = __shfl_sync(FULL, chosen, gb);
+  const uint32_t vb = __shfl_sync(FULL, cvec, cb);
+  if (lane < 16) out->split_mvs[lane] = vp8a_mv{(int16_t)(vb & 0xffffu), (int16_t)(vb >> 16)};
 }
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
@@ -1514,6 +1531,12 @@ vp8a_status prepare_job(vp8a_ctx* ctx, vp8a::Stager& st, MvBitsCache& mc, const 
   }
   if (n_refs == 0 || n_refs > (uint32_t)MAX_REFS) {
     vp8a::set_error("n_refs must be 1..3");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  // rd_lambda is finite and non-negative; the SPLITMV choice compares its
+  // costs (sums of non-negative terms) by their bit patterns.
+  if (!(lambda >= 0.0) || lambda > 1.0e300) {
+    vp8a::set_error("lambda must be a finite, non-negative RD multiplier");
     return VP8A_E_INVALID_ARGUMENT;
   }
   const int mb_cols = (int)((frame->width + 15) / 16), mb_rows = (int)((frame->height + 15) / 16);

@@ -79,6 +79,10 @@ def test_analysis_errors(ctx):
         vp8a.analyse_inter_frame(ctx, frames[1], [bad], [1], 72.0)
     with pytest.raises(vp8a.Vp8aError, match="InvalidArgument"):
         vp8a.analyse_inter_frame(ctx, frames[1], [vp8a.pad_to_mb(*frames[0])], [7], 72.0)
+    # rd_lambda is finite and non-negative.
+    for lam in (-1.0, float("nan"), float("inf")):
+        with pytest.raises(vp8a.Vp8aError, match="InvalidArgument"):
+            vp8a.analyse_inter_frame(ctx, frames[1], [vp8a.pad_to_mb(*frames[0])], [1], lam)
 
 
 def test_analysis_and_lf_device_resident(ctx, oracle):
