@@ -131,6 +131,7 @@ struct SplitOut {
 struct __align__(16) SplitScratch {
   uint32_t table[CMAX * 16];  // group g's SAD at column m: table[m * 16 + g], needed columns only
   double new_cost[16 * 5];    // lambda * (NEW4X4 mode bits of context x + group g's vector bits)
+  double terms[32];           // group g's reference bits [g] and NEW vector bits [16 + g], for the total
   vp8a_mv cmv[CMAX];
 };
 static_assert(sizeof(SplitScratch) % 16 == 0, "SplitScratch copies stay 16-byte aligned");
@@ -637,105 +638,91 @@ __device__ void split_partition(const AnArgs& a, const double* pbits, const doub
   // anti-diagonal of the partition's group grid are independent: step s
   // decides them in parallel. The columns the neighbouring groups chose
   // and the vectors they stand for travel by shuffles.
-  const int gh = pid == 1 ? 1 : (pid == 3 ? 4 : 2), gw = pid == 0 ? 1 : (pid == 3 ? 4 : 2);
-  const int gr = lane / gw, gc = lane - gr * gw;
+  // The group grid is gh x gw = 2^lgh x 2^lgw groups of (4 >> lgh) x
+  // (4 >> lgw) blocks.
+  const int lgh = pid == 1 ? 0 : (pid == 3 ? 2 : 1), lgw = pid == 0 ? 0 : (pid == 3 ? 2 : 1);
+  const int gh = 1 << lgh, gw = 1 << lgw;
+  const int gr = lane >> lgw, gc = lane & (gw - 1);
   // The group's top-left block; the blocks left of and above it belong to
   // the groups (gr, gc - 1) and (gr - 1, gc), or lie outside the MB.
-  const int anchor = gr * (4 / gh) * 4 + gc * (4 / gw);
+  const int anchor = ((gr << (2 - lgh)) << 2) + (gc << (2 - lgw));
+  // A group on the MB's left or top edge takes its LEFT or ABOVE vector
+  // from the neighbour MB's column; lane g's NEW result is column 9 + g.
+  const int ext_l = 1 + (anchor >> 2), ext_a = 5 + anchor;
+  const uint32_t ext_lv = __shfl_sync(FULL, cvec, ext_l & 31), ext_av = __shfl_sync(FULL, cvec, ext_a & 31);
+  const uint32_t new_vec = __shfl_sync(FULL, cvec, (9 + lane) & 31);
+  // The group's choice: its column and that column's vector.
   int chosen = 0, mode = VP8A_SUBMV_ZERO, my_ctx = 0;
-  uint32_t my_sad = 0;
+  uint32_t chosen_vec = 0, my_sad = 0;
   bool my_bad = false;
   for (int st = 0; st < gh + gw - 1; st++) {
-    const int lch = __shfl_sync(FULL, chosen, gc == 0 ? lane : lane - 1);
-    const int ach = __shfl_sync(FULL, chosen, gr == 0 ? lane : lane - gw);
-    const int lidx = gc == 0 ? 1 + (anchor >> 2) : lch;
-    const int aidx = gr == 0 ? 5 + anchor : ach;
-    const uint32_t lv = __shfl_sync(FULL, cvec, lidx & 31), av = __shfl_sync(FULL, cvec, aidx & 31);
+    const int lsrc = gc == 0 ? lane : lane - 1, asrc = gr == 0 ? lane : lane - gw;
+    const int lch = __shfl_sync(FULL, chosen, lsrc), ach = __shfl_sync(FULL, chosen, asrc);
+    const uint32_t lchv = __shfl_sync(FULL, chosen_vec, lsrc), achv = __shfl_sync(FULL, chosen_vec, asrc);
     if (lane < G && gr + gc == st) {
+      const int lidx = gc == 0 ? ext_l : lch, aidx = gr == 0 ? ext_a : ach;
+      const uint32_t lv = gc == 0 ? ext_lv : lchv, av = gr == 0 ? ext_av : achv;
       const bool lez = lv == 0u, aez = av == 0u, lea = lv == av;
       const int ctxi = (lea && lez) ? 4 : (lea ? 3 : (aez ? 2 : (lez ? 1 : 0)));
       const double* lt = lterm + ctxi * 4;
       const uint32_t tl = W.table[lidx * 16 + lane], ta = W.table[aidx * 16 + lane], tz = W.table[lane];
       // LEFT, ABOVE, ZERO, then NEW (sad + lambda * (mode bits + vector
-      // bits), the vector bits 0 for the first three); strict '<' keeps the
-      // first minimum. Every J is a sum of non-negative finite terms, or
-      // +inf before the first, so J order is the order of the doubles' bit
-      // patterns as unsigned integers.
+      // bits), the vector bits 0 for the first three); the reference keeps
+      // the first strict minimum in that order. Every J here is a finite sum
+      // of non-negative terms, so J order is the order of the doubles' bit
+      // patterns as unsigned integers, and the first minimum of the four is
+      // the first minimum of the first minima of (LEFT, ABOVE) and (ZERO,
+      // NEW).
       const uint64_t j0 = (uint64_t)__double_as_longlong((double)tl + lt[0]);
       const uint64_t j1 = (uint64_t)__double_as_longlong((double)ta + lt[1]);
       const uint64_t j2 = (uint64_t)__double_as_longlong((double)tz + lt[2]);
-      uint64_t best_j = 0x7ff0000000000000ull;
-      int best_mode = VP8A_SUBMV_ZERO, best_col = 0;
-      uint32_t best_sad = tz;
-      if (j0 < best_j) {
-        best_j = j0;
-        best_mode = VP8A_SUBMV_LEFT;
-        best_col = lidx;
-        best_sad = tl;
-      }
-      if (j1 < best_j) {
-        best_j = j1;
-        best_mode = VP8A_SUBMV_ABOVE;
-        best_col = aidx;
-        best_sad = ta;
-      }
-      if (j2 < best_j) {
-        best_j = j2;
-        best_mode = VP8A_SUBMV_ZERO;
-        best_col = 0;
-        best_sad = tz;
-      }
-      if (my_new_ok) {
-        const uint64_t jn = (uint64_t)__double_as_longlong((double)my_new_sad + W.new_cost[lane * 5 + ctxi]);
-        if (jn < best_j) {
-          best_j = jn;
-          best_mode = VP8A_SUBMV_NEW;
-          best_col = 9 + lane;
-          best_sad = my_new_sad;
-        }
-      }
-      chosen = best_col;
-      mode = best_mode;
+      const uint64_t jn = my_new_ok ? (uint64_t)__double_as_longlong((double)my_new_sad + W.new_cost[lane * 5 + ctxi])
+                                    : 0xffffffffffffffffull;
+      const bool above_first = j1 < j0, new_second = jn < j2;
+      const uint64_t v01 = above_first ? j1 : j0, v2n = new_second ? jn : j2;
+      const bool second = v2n < v01;
+      const uint64_t best_j = second ? v2n : v01;
+      mode = second ? (new_second ? VP8A_SUBMV_NEW : VP8A_SUBMV_ZERO)
+                    : (above_first ? VP8A_SUBMV_ABOVE : VP8A_SUBMV_LEFT);
+      chosen = second ? (new_second ? 9 + lane : 0) : (above_first ? aidx : lidx);
+      chosen_vec = second ? (new_second ? new_vec : 0u) : (above_first ? av : lv);
+      my_sad = second ? (new_second ? my_new_sad : tz) : (above_first ? ta : tl);
       my_ctx = ctxi;
-      my_sad = best_sad;
       my_bad = best_j >= 0x7ff0000000000000ull;
     }
   }
   if (lane < G) out->modes[lane] = (uint8_t)mode;
   // Totals in the reference's group order (the f64 sum is order-sensitive):
-  // lane g holds group g's terms, every lane sums them in order.
+  // the groups' terms go through shared memory and lane 0 sums them in
+  // order.
   const bool mine = lane < G;
   const bool isn = mine && mode == VP8A_SUBMV_NEW;
-  const double ba = mine ? sbits[my_ctx * 4 + mode] : 0.0;
-  const double bn = isn ? my_new_bits : 0.0;
-  const uint32_t sd = mine ? my_sad : 0u;
-  const uint32_t total_sad = __reduce_add_sync(FULL, sd);
+  if (mine) {
+    W.terms[lane] = sbits[my_ctx * 4 + mode];
+    W.terms[16 + lane] = my_new_bits;
+  }
+  const uint32_t total_sad = __reduce_add_sync(FULL, mine ? my_sad : 0u);
   const unsigned any_bad = __ballot_sync(FULL, mine && my_bad), news = __ballot_sync(FULL, isn);
-  double xa[16], xn[16];
-#pragma unroll
-  for (int gg = 0; gg < 16; gg++) {
-    xa[gg] = __shfl_sync(FULL, ba, gg);
-    xn[gg] = __shfl_sync(FULL, bn, gg);
-  }
-  double total_bits = 0.0;
-#pragma unroll
-  for (int gg = 0; gg < 16; gg++) {
-    if (gg >= G) break;
-    total_bits += xa[gg];
-    if ((news >> gg) & 1u) total_bits += xn[gg];
-  }
+  __syncwarp();
   if (lane == 0) {
     // The reference stops at the first group without a finite choice.
     out->valid = any_bad == 0u;
     if (any_bad == 0u) {
+      double total_bits = 0.0;
+#pragma unroll
+      for (int gg = 0; gg < 16; gg++) {
+        if (gg < G) {
+          total_bits += W.terms[gg];
+          if ((news >> gg) & 1u) total_bits += W.terms[16 + gg];
+        }
+      }
       out->j = (double)total_sad + a.lambda * (pbits[pid] + total_bits);
       for (int i = G; i < 16; i++) out->modes[i] = VP8A_SUBMV_ZERO;
     }
   }
   // Block b's vector: the column its group chose.
-  const int gb = lane < 16 ? ((lane >> 2) / (4 / gh)) * gw + (lane & 3) / (4 / gw) : 0;
-  const int cb = __shfl_sync(FULL, chosen, gb);
-  const uint32_t vb = __shfl_sync(FULL, cvec, cb);
+  const int gb = lane < 16 ? (((lane >> 2) >> (2 - lgh)) << lgw) + ((lane & 3) >> (2 - lgw)) : 0;
+  const uint32_t vb = __shfl_sync(FULL, chosen_vec, gb);
   if (lane < 16) out->split_mvs[lane] = vp8a_mv{(int16_t)(vb & 0xffffu), (int16_t)(vb >> 16)};
 }
 
@@ -852,6 +839,11 @@ __device__ __forceinline__ uint32_t sp_block_sad(const uint8_t* plane, uint64_t 
 
 // ------------------------------------------------------ sub-pel stages
 
+constexpr int NW = 9;                 // warps per CTA (one reference)
+constexpr int AN_THREADS = NW * 32;
+constexpr int MAIN_WARPS = 5;         // warps 0 and 5-8: the MB search chain
+constexpr int MAIN_THREADS = MAIN_WARPS * 32;
+
 // Offsets (row, col) of the eight refinement candidates in the reference's
 // order: (-1,-1) (-1,0) (-1,1) (0,-1) (0,1) (1,-1) (1,0) (1,1).
 __device__ __forceinline__ int cand_dr(int k) { return (k < 3) ? -1 : (k < 5 ? 0 : 1); }
@@ -859,29 +851,36 @@ __device__ __forceinline__ int cand_dc(int k) { return (k == 0 || k == 3 || k ==
 
 // The H, V and D half-pel planes around a whole-pel centre whose block
 // origin in the window is (bx, by) (the planes of half_plane_sads, filled
-// by several warps): H and V first, then D from H.
-__device__ __forceinline__ void half_planes_hv(WarpScratch& S, int bx, int by, int tid, int nthreads) {
-  const int* f = c_sixtap[4];
-  for (int o = tid; o < 22 * 17 + 17 * 16; o += nthreads) {
-    if (o < 22 * 17) {
+// by the main group's MAIN_THREADS threads): H and V first, then D from H.
+// Each thread's outputs are independent; the loops are unrolled so that
+// all of a thread's window reads are in flight together.
+__device__ __forceinline__ void half_planes_hv(WarpScratch& S, int bx, int by, int tid) {
+  constexpr int NH = 22 * 17, NO = NH + 17 * 16;
+#pragma unroll
+  for (int it = 0; it < (NO + MAIN_THREADS - 1) / MAIN_THREADS; it++) {
+    const int o = tid + it * MAIN_THREADS;
+    if (o < NH) {
       const int r = o / 17, i = o - r * 17;
       const uint8_t* p = S.win + (by - 3 + r) * WS + bx + i - 3;
-      S.hp[o] = (uint8_t)interp6(f, p[0], p[1], p[2], p[3], p[4], p[5]);
-    } else {
-      const int q = o - 22 * 17, r = q >> 4, c = q & 15;
+      S.hp[o] = (uint8_t)interp6_half(p[0], p[1], p[2], p[3], p[4], p[5]);
+    } else if (o < NO) {
+      const int q = o - NH, r = q >> 4, c = q & 15;
       const uint8_t* p = S.win + (by + r - 3) * WS + bx + c;
-      S.vp[q] = (uint8_t)interp6(f, p[0], p[WS], p[2 * WS], p[3 * WS], p[4 * WS], p[5 * WS]);
+      S.vp[q] = (uint8_t)interp6_half(p[0], p[WS], p[2 * WS], p[3 * WS], p[4 * WS], p[5 * WS]);
     }
   }
 }
 
 // The D plane, from H (after H is complete).
-__device__ __forceinline__ void half_planes_d(WarpScratch& S, int tid, int nthreads) {
-  const int* f = c_sixtap[4];
-  for (int o = tid; o < 17 * 17; o += nthreads) {
-    const int r = o / 17, i = o - r * 17;
-    const uint8_t* p = S.hp + r * 17 + i;
-    S.dp[o] = (uint8_t)interp6(f, p[0], p[17], p[34], p[51], p[68], p[85]);
+__device__ __forceinline__ void half_planes_d(WarpScratch& S, int tid) {
+#pragma unroll
+  for (int it = 0; it < (17 * 17 + MAIN_THREADS - 1) / MAIN_THREADS; it++) {
+    const int o = tid + it * MAIN_THREADS;
+    if (o < 17 * 17) {
+      const int r = o / 17, i = o - r * 17;
+      const uint8_t* p = S.hp + r * 17 + i;
+      S.dp[o] = (uint8_t)interp6_half(p[0], p[17], p[34], p[51], p[68], p[85]);
+    }
   }
 }
 
@@ -943,19 +942,24 @@ __device__ __forceinline__ bool quarter_geom(vp8a_mv qc, int mbx, int mby, int w
   return xmin >= 2 && xmax + 19 <= WS && ymin >= 2 && ymin + 20 <= WS && ymax - ymin <= 1;
 }
 
-// Horizontal planes: qh[k * 352 + rr * 16 + c], rr = 0..21 from window row iy0.
-__device__ __forceinline__ void quarter_planes_h(const uint8_t* win, uint8_t* qh, const QuarterGeom& q, int t, int n) {
-  for (int o = t; o < 3 * 22 * 16; o += n) {
-    const int k = o / 352, rem = o - k * 352, rr = rem >> 4, c = rem & 15;
-    const uint8_t* p = win + (q.iy0 + rr) * WS + q.ix[k] + c;
-    int v;
-    if (q.fx[k]) {
-      const int* f = c_sixtap[q.fx[k]];
-      v = interp6(f, p[-2], p[-1], p[0], p[1], p[2], p[3]);
-    } else {
-      v = p[0];
+// Horizontal planes: qh[k * 352 + rr * 16 + c], rr = 0..21 from window row
+// iy0 (filled by the main group; unrolled, as the half-pel planes).
+__device__ __forceinline__ void quarter_planes_h(const uint8_t* win, uint8_t* qh, const QuarterGeom& q, int t) {
+#pragma unroll
+  for (int it = 0; it < (3 * 22 * 16 + MAIN_THREADS - 1) / MAIN_THREADS; it++) {
+    const int o = t + it * MAIN_THREADS;
+    if (o < 3 * 22 * 16) {
+      const int k = o / 352, rem = o - k * 352, rr = rem >> 4, c = rem & 15;
+      const uint8_t* p = win + (q.iy0 + rr) * WS + q.ix[k] + c;
+      int v;
+      if (q.fx[k]) {
+        const int* f = c_sixtap[q.fx[k]];
+        v = interp6(f, p[-2], p[-1], p[0], p[1], p[2], p[3]);
+      } else {
+        v = p[0];
+      }
+      qh[o] = (uint8_t)v;
     }
-    qh[o] = (uint8_t)v;
   }
 }
 
@@ -1004,10 +1008,6 @@ struct __align__(16) WarpTemp {
 
 // -------------------------------------------------------------- kernel
 
-constexpr int NW = 9;                 // warps per CTA (one reference)
-constexpr int AN_THREADS = NW * 32;
-constexpr int MAIN_WARPS = 5;         // warps 0 and 5-8: the MB search chain
-constexpr int MAIN_THREADS = MAIN_WARPS * 32;
 
 // Barrier 1: the main group only.
 __device__ __forceinline__ void main_sync() { asm volatile("bar.sync 1, %0;" ::"n"(MAIN_THREADS) : "memory"); }
@@ -1276,9 +1276,9 @@ __global__ void __launch_bounds__(AN_THREADS, 2)
               if ((mt & 15) == 0) cand_sad[q] = sv;
             }
           } else {
-            half_planes_hv(R.ws, hbx, hby, mt, MAIN_THREADS);
+            half_planes_hv(R.ws, hbx, hby, mt);
             main_sync();
-            half_planes_d(R.ws, mt, MAIN_THREADS);
+            half_planes_d(R.ws, mt);
             main_sync();
             for (int q = slot; q < 8; q += MAIN_WARPS) {
               const uint32_t sv = half_cand_sad(R.ws, q, src, lane);
@@ -1286,17 +1286,22 @@ __global__ void __launch_bounds__(AN_THREADS, 2)
             }
           }
           main_sync();
-          if (mt == 0) {
-            vp8a_mv best = hc;
-            uint32_t best_sad = mo.whole.sad;
-            for (int q = 0; q < 8; q++)
-              if (cand_sad[q] < best_sad) {
-                best_sad = cand_sad[q];
+          if (warp == 0) {
+            // The first strictly better candidate in order = the smallest
+            // (SAD, index) if its SAD beats the centre's.
+            const uint32_t m = __reduce_min_sync(FULL, lane < 8 ? (cand_sad[lane] << 3) | (uint32_t)lane : ~0u);
+            if (lane == 0) {
+              vp8a_mv best = hc;
+              uint32_t best_sad = mo.whole.sad;
+              const int q = (int)(m & 7u);
+              if ((m >> 3) < best_sad) {
+                best_sad = m >> 3;
                 best.row = (int16_t)(hc.row + 2 * cand_dr(q));
                 best.col = (int16_t)(hc.col + 2 * cand_dc(q));
               }
-            mo.half = vp8a_search_result{best, best_sad};
-            s_qok = quarter_geom(best, mbx, mby, plan.wx0, plan.wy0, s_qg);
+              mo.half = vp8a_search_result{best, best_sad};
+              s_qok = quarter_geom(best, mbx, mby, plan.wx0, plan.wy0, s_qg);
+            }
           }
         } else if (warp == 0) {
           const vp8a_search_result h = refine(P, R.ws, plan.wx0, plan.wy0, mbx, mby, hc, 2, src, lane, mo.whole.sad);
@@ -1326,7 +1331,7 @@ __global__ void __launch_bounds__(AN_THREADS, 2)
           }
         } else if (s_qok) {
           uint8_t* qh = R.ws.temp;  // the six-tap scratch and half planes are free now
-          quarter_planes_h(R.ws.win, qh, s_qg, mt, MAIN_THREADS);
+          quarter_planes_h(R.ws.win, qh, s_qg, mt);
           main_sync();
           if (mt < 128) {
             const uint32_t sv = quarter_vsad(qh, s_qg, src, mt);
@@ -1341,16 +1346,19 @@ __global__ void __launch_bounds__(AN_THREADS, 2)
           }
         }
         main_sync();
-        if (mt == 0) {
-          vp8a_mv best = qc;
-          uint32_t best_sad = mo.half.sad;
-          for (int q = 0; q < 8; q++)
-            if (cand_sad[q] < best_sad) {
-              best_sad = cand_sad[q];
+        if (warp == 0) {
+          const uint32_t m = __reduce_min_sync(FULL, lane < 8 ? (cand_sad[lane] << 3) | (uint32_t)lane : ~0u);
+          if (lane == 0) {
+            vp8a_mv best = qc;
+            uint32_t best_sad = mo.half.sad;
+            const int q = (int)(m & 7u);
+            if ((m >> 3) < best_sad) {
+              best_sad = m >> 3;
               best.row = clamp_component(qc.row + cand_dr(q));
               best.col = clamp_component(qc.col + cand_dc(q));
             }
-          mo.quarter = vp8a_search_result{best, best_sad};
+            mo.quarter = vp8a_search_result{best, best_sad};
+          }
         }
       }
       __syncthreads();

@@ -291,25 +291,24 @@ __device__ __forceinline__ bool half_plane_sads(WarpScratch& S, int wx0, int wy0
   if ((center.row & 3) || (center.col & 3)) return false;
   const int bx = mbx + center.col / 4 - wx0, by = mby + center.row / 4 - wy0;  // block origin in window
   if (bx < 3 || by < 3 || bx + 19 > WS || by + 19 > WS) return false;
-  const int* f = c_sixtap[4];
   // H: 22 rows (window rows by-3 .. by+18), 17 outputs at x = bx + i - 0.5.
   for (int o = lane; o < 22 * 17; o += 32) {
     const int r = o / 17, i = o - r * 17;
     const uint8_t* p = S.win + (by - 3 + r) * WS + bx + i - 3;
-    S.hp[o] = (uint8_t)interp6(f, p[0], p[1], p[2], p[3], p[4], p[5]);
+    S.hp[o] = (uint8_t)interp6_half(p[0], p[1], p[2], p[3], p[4], p[5]);
   }
   // V: 17 rows at y = by + r - 0.5, 16 columns.
   for (int o = lane; o < 17 * 16; o += 32) {
     const int r = o >> 4, c = o & 15;
     const uint8_t* p = S.win + (by + r - 3) * WS + bx + c;
-    S.vp[o] = (uint8_t)interp6(f, p[0], p[WS], p[2 * WS], p[3 * WS], p[4 * WS], p[5 * WS]);
+    S.vp[o] = (uint8_t)interp6_half(p[0], p[WS], p[2 * WS], p[3 * WS], p[4 * WS], p[5 * WS]);
   }
   __syncwarp();
   // D: vertical half-pel over H (rows r..r+5 of H), 17 x 17.
   for (int o = lane; o < 17 * 17; o += 32) {
     const int r = o / 17, i = o - r * 17;
     const uint8_t* p = S.hp + r * 17 + i;
-    S.dp[o] = (uint8_t)interp6(f, p[0], p[17], p[34], p[51], p[68], p[85]);
+    S.dp[o] = (uint8_t)interp6_half(p[0], p[17], p[34], p[51], p[68], p[85]);
   }
   __syncwarp();
   const int c = lane & 15, r0 = (lane >> 4) * 8;

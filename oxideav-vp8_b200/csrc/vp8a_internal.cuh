@@ -184,4 +184,11 @@ __device__ __forceinline__ int interp6(const int* f, int s0, int s1, int s2, int
   return clampi((a + 64) >> 7, 0, 255);
 }
 
+// interp with the half-pel taps (row 4: 3, -16, 77, 77, -16, 3) as
+// literals; the integer dot product is the same.
+__device__ __forceinline__ int interp6_half(int s0, int s1, int s2, int s3, int s4, int s5) {
+  const int a = 3 * (s0 + s5) - 16 * (s1 + s4) + 77 * (s2 + s3);
+  return clampi((a + 64) >> 7, 0, 255);
+}
+
 }  // namespace vp8a_dev
