@@ -441,6 +441,57 @@ __device__ __forceinline__ void filter_mb(const LfArgs& a, const Prm* prm, const
   }
 
   const int pl = l < 8 ? 256 : 320, cl = l & 7;  // this lane's chroma plane offset and row/column
+  // MBs without inner edges (no coefficients, not B_PRED) filter only their
+  // left and top MB edges: eight taps per lane and direction. When no MB of
+  // the warp's converged lanes has inner edges, the warp takes that narrow
+  // path (both half-warps run the same instructions); otherwise every MB
+  // runs the full rows and columns below, filtering inner edges only where
+  // it has them.
+  if (__ballot_sync(__activemask(), sub) == 0u) {
+    if (has_left) {
+      int p[8];
+      uint32_t* lw = (uint32_t*)(left + l * 16 + 12);
+      uint32_t* rw = (uint32_t*)(me + l * 16);
+      unpack4(*lw, p);
+      unpack4(*rw, p + 4);
+      mb_filter<0>(p, q);
+      *lw = pack4(p);
+      *rw = pack4(p + 4);
+      uint32_t* lc = (uint32_t*)(left + pl + cl * 8 + 4);
+      uint32_t* rc = (uint32_t*)(me + pl + cl * 8);
+      unpack4(*lc, p);
+      unpack4(*rc, p + 4);
+      mb_filter<0>(p, q);
+      *lc = pack4(p);
+      *rc = pack4(p + 4);
+    }
+    __syncwarp(hm);
+    if (has_top) {
+      // The last four rows of the MB above and the first four here; the
+      // filter changes the last three above and the first three here.
+      int p[8];
+#pragma unroll
+      for (int k = 0; k < 4; k++) p[k] = (int)above[(12 + k) * 16 + l];
+#pragma unroll
+      for (int k = 0; k < 4; k++) p[4 + k] = (int)me[k * 16 + l];
+      mb_filter<0>(p, q);
+#pragma unroll
+      for (int k = 1; k < 4; k++) above[(12 + k) * 16 + l] = (uint8_t)p[k];
+#pragma unroll
+      for (int k = 0; k < 3; k++) me[k * 16 + l] = (uint8_t)p[4 + k];
+#pragma unroll
+      for (int k = 0; k < 4; k++) p[k] = (int)above[pl + (4 + k) * 8 + cl];
+#pragma unroll
+      for (int k = 0; k < 4; k++) p[4 + k] = (int)me[pl + k * 8 + cl];
+      mb_filter<0>(p, q);
+#pragma unroll
+      for (int k = 1; k < 4; k++) above[pl + (4 + k) * 8 + cl] = (uint8_t)p[k];
+#pragma unroll
+      for (int k = 0; k < 3; k++) me[pl + k * 8 + cl] = (uint8_t)p[4 + k];
+    }
+    __syncwarp(hm);
+    return;
+  }
   // ---- vertical edges (steps 1 and 2): luma row l, then chroma row cl ----
   {
     uint32_t* rw = (uint32_t*)(me + l * 16);
