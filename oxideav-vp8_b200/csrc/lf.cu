@@ -1054,7 +1054,7 @@ vp8a_status sweep_layouts(vp8a_ctx* ctx, int n, int ring, bool pre_ok, int threa
   out->clear();
   int max_smem = 0;
   VP8A_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-  const int tcands[] = {1024, 768, 512, 384, 352, 320, 256, 192, 128};
+  const int tcands[] = {1024, 768, 512, 384, 352, 256, 192, 128};
   for (int nc = 3; nc >= 1; nc--) {
     if (nc > 1 && n < nc) continue;
     const void* k = sweep_kernel_of(nc, batch);
