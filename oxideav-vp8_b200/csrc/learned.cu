@@ -21,7 +21,10 @@
 //   lp_adam_kernel          Adam on FP32 master weights, BF16 copies
 // Layout: activations NHWC, 32x32 pixels per MB, channel count 2 or 32
 // (the last layer 1); weights [cout][tap][cin], tap = (dy + 1) * 3 + dx + 1.
+#include <cuda.h>
 #include <cuda_bf16.h>
+
+#include <mutex>
 
 #include "vp8a_internal.cuh"
 
@@ -361,7 +364,11 @@ __global__ void lp_lf_head_kernel(const float* sums, float count, int C, const f
 // image, the 3x3 convolution as an implicit GEMM D[pixel][n] = sum over
 // (tap, ci) of A[pixel + tap offset][ci] * W[n][tap][ci]. The image sits in
 // shared memory with a zero halo on a 34-pixel row pitch, channel-group
-// major (group g of 8 channels: 16 bytes per halo pixel), so that 8
+// major (group g of 8 channels: 16 bytes per halo pixel). Four TMA tile
+// loads bring it in: the activations as a 4-D tensor (channel, x, y,
+// image), a box of 8 channels x 34 x 34 pixels x 1 image per channel
+// group, started at (8 g, -1, -1, image), so the box lands in exactly that
+// layout and the halo ring is the loads' out-of-bounds zero fill. So that 8
 // consecutive "virtual" output pixels v = y * 34 + x form one 8 x 16-byte
 // core matrix of the K-major, unswizzled canonical layout and a tap
 // (dy, dx) is only a base-address shift of (dy + 1) * 34 + dx + 1 pixels.
@@ -378,7 +385,9 @@ constexpr int NV = 1224;                    // halo pixels per channel group (>=
 constexpr int REGION = NV * 16;             // bytes per channel group
 constexpr int IMG_BYTES = 4 * REGION;
 constexpr int W_BYTES = 36 * 32 * 16;       // 36 k-groups x 32 n x 16 bytes
-constexpr int SMEM = IMG_BYTES + W_BYTES + 16;
+constexpr int SMEM = IMG_BYTES + W_BYTES + 32;
+constexpr uint32_t BOX_BYTES = 8 * 34 * 34 * 2;  // one channel group's TMA box
+static_assert(REGION % 128 == 0, "TMA destinations are 128-byte aligned");
 constexpr int TILES = 9;                    // ceil(32 * 34 / 128)
 constexpr uint32_t TMEM_COLS = 128;         // four 32-column accumulators
 // Instruction descriptor (kind::f16): D FP32, A and B BF16, both K-major,
@@ -394,20 +403,37 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
 }
 }  // namespace lptc
 
-__global__ void __launch_bounds__(256, 2) lp_conv_fwd_tc_kernel(const uint16_t* X, const uint16_t* W,
-                                                                 const float* bias, int relu, uint16_t* Y,
-                                                                 uint32_t* status) {
+// Bounded wait for phase `phase` of the mbarrier at shared address `bar`;
+// true when it completed.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, int limit) {
+  uint32_t done = 0;
+  for (int it = 0; it < limit && !done; it++) {
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(phase)
+        : "memory");
+  }
+  return done != 0;
+}
+
+__global__ void __launch_bounds__(256, 2) lp_conv_fwd_tc_kernel(const __grid_constant__ CUtensorMap tmx,
+                                                                 const uint16_t* W, const float* bias, int relu,
+                                                                 uint16_t* Y, uint32_t* status) {
   using namespace lptc;
   extern __shared__ __align__(128) uint8_t smt[];
   uint8_t* img_s = smt;
   uint8_t* w_s = smt + IMG_BYTES;
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smt + IMG_BYTES + W_BYTES);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smt + IMG_BYTES + W_BYTES + 8);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smt + IMG_BYTES + W_BYTES + 16);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const size_t im = blockIdx.x;
   const uint32_t img_a = (uint32_t)__cvta_generic_to_shared(img_s);
   const uint32_t w_a = (uint32_t)__cvta_generic_to_shared(w_s);
   const uint32_t bar_a = (uint32_t)__cvta_generic_to_shared(mbar);
+  const uint32_t bar_t = bar_a + 8;  // the image loads' mbarrier
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -417,39 +443,46 @@ __global__ void __launch_bounds__(256, 2) lp_conv_fwd_tc_kernel(const uint16_t* 
   }
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_a), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_t), "r"(1));
     asm volatile("fence.mbarrier_init.release.cluster;");
-  }
-  // The 1024 pixels and the weights by 16-byte asynchronous copies (all in
-  // flight at once), and zeros into the halo ring and the tail only, which
-  // no copy touches.
-  const uint4* Xi = reinterpret_cast<const uint4*>(X + im * LP_P * 32);
-  for (int q = tid; q < LP_P * 4; q += 256) {
-    const int p = q >> 2, g = q & 3;
-    const int h = ((p >> 5) + 1) * 34 + (p & 31) + 1;
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(img_a + (uint32_t)(g * REGION + h * 16)),
-                 "l"(Xi + q)
+    // The image: four TMA tile loads (one per channel group, the halo ring
+    // from their out-of-bounds fill) completing on bar_t.
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_t), "r"(4 * BOX_BYTES)
                  : "memory");
+    const uint64_t tm = reinterpret_cast<uint64_t>(&tmx);
+    for (int g = 0; g < 4; g++)
+      asm volatile(
+          "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+          "[%6];" ::"r"(img_a + (uint32_t)(g * REGION)),
+          "l"(tm), "r"(8 * g), "r"(-1), "r"(-1), "r"((int)im), "r"(bar_t)
+          : "memory");
   }
+  // The weights by 16-byte asynchronous copies, and zeros into each
+  // channel group's tail past the 34 x 34 box, which no load touches.
   for (int q = tid; q < 32 * 36; q += 256) {
     const int n = q / 36, kg = q % 36;
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(w_a + (uint32_t)((kg * 32 + n) * 16)),
                  "l"(W + n * 288 + kg * 8)
                  : "memory");
   }
-  for (int q = tid; q < 4 * NV; q += 256) {
-    const int h = q % NV, hy = h / 34, hx = h % 34;
-    if (h >= 34 * 34 || hy == 0 || hy == 33 || hx == 0 || hx == 33)
-      reinterpret_cast<uint4*>(img_s)[q] = make_uint4(0, 0, 0, 0);
-  }
+  constexpr int TAIL = NV - 34 * 34;
+  for (int q = tid; q < 4 * TAIL; q += 256)
+    reinterpret_cast<uint4*>(img_s + (q / TAIL) * REGION)[34 * 34 + q % TAIL] = make_uint4(0, 0, 0, 0);
   asm volatile("cp.async.wait_all;" ::: "memory");
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
+  __syncthreads();  // the mbarrier inits are visible from here on
+  // Bounded wait for the image; a load that never lands is reported, and
+  // the CTA waits once more (bounded) for it before leaving.
+  bool failed = __syncthreads_or(!mbar_wait(bar_t, 0, WAIT_LIMIT));
+  if (failed) {
+    if (tid == 0) atomicExch(status, 1u);  // DEV_TIMEOUT
+    mbar_wait(bar_t, 0, WAIT_LIMIT);
+  }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
   uint32_t phase = 0;
-  bool failed = false;
   for (int t0 = 0; t0 < TILES && !failed; t0 += 4) {
     const int nt = TILES - t0 < 4 ? TILES - t0 : 4;
     if (tid == 0) {
@@ -473,16 +506,7 @@ __global__ void __launch_bounds__(256, 2) lp_conv_fwd_tc_kernel(const uint16_t* 
                    : "memory");
     }
     // Bounded wait for the commit; a timeout is reported, not waited out.
-    uint32_t done = 0;
-    for (int it = 0; it < WAIT_LIMIT && !done; it++) {
-      asm volatile(
-          "{\n\t.reg .pred P1;\n\t"
-          "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-          "selp.b32 %0, 1, 0, P1;\n\t}\n"
-          : "=r"(done)
-          : "r"(bar_a), "r"(phase)
-          : "memory");
-    }
+    const bool done = mbar_wait(bar_a, phase, WAIT_LIMIT);
     phase ^= 1u;
     failed = __syncthreads_or(!done);
     if (failed) {
@@ -529,6 +553,46 @@ __global__ void __launch_bounds__(256, 2) lp_conv_fwd_tc_kernel(const uint16_t* 
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
   }
+}
+
+// cuTensorMapEncodeTiled, taken from the driver once.
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
+
+// The TMA map of n NHWC [32][32][32] BF16 images for the tcgen05 conv: a
+// 4-D tensor (channel, x, y, image) with boxes of 8 channels x 34 x 34 x 1.
+vp8a_status conv_image_map(const uint16_t* x, uint32_t n, CUtensorMap* tm) {
+  const EncodeTiledFn enc = encode_tiled();
+  if (!enc) {
+    vp8a::set_error("the driver does not provide cuTensorMapEncodeTiled");
+    return VP8A_E_CUDA;
+  }
+  const cuuint64_t gdim[4] = {32, 32, 32, (cuuint64_t)n};
+  const cuuint64_t gstride[3] = {32 * 2, 32 * 32 * 2, 32 * 32 * 32 * 2};  // bytes, dims 1..3
+  const cuuint32_t box[4] = {8, 34, 34, 1}, estride[4] = {1, 1, 1, 1};
+  const CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<uint16_t*>(x), gdim, gstride, box, estride,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    vp8a::set_error("cuTensorMapEncodeTiled rejected the activation map (error " + std::to_string((int)r) + ")");
+    return VP8A_E_CUDA;
+  }
+  return VP8A_OK;
 }
 
 template <int CIN, int NT>
@@ -697,8 +761,11 @@ vp8a_status vp8a_lp_conv_forward(vp8a_ctx* ctx, const uint16_t* x, uint32_t cin,
       vp8a::set_error("tensor-core conv needs 16-byte aligned buffers");
       return VP8A_E_INVALID_ARGUMENT;
     }
+    CUtensorMap tm;
+    const vp8a_status s = conv_image_map(x, n, &tm);
+    if (s != VP8A_OK) return s;
     VP8A_CUDA(cudaFuncSetAttribute(lp_conv_fwd_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lptc::SMEM));
-    lp_conv_fwd_tc_kernel<<<n, 256, lptc::SMEM, ctx->stream>>>(x, w, bias, (int)relu, y, ctx->d_status);
+    lp_conv_fwd_tc_kernel<<<n, 256, lptc::SMEM, ctx->stream>>>(tm, w, bias, (int)relu, y, ctx->d_status);
     VP8A_CUDA(cudaGetLastError());
     ctx->launches++;
     return VP8A_OK;
