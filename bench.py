@@ -1149,23 +1149,16 @@ def batch_arm(args):
 
 # --------------------------------------------------- learned proposal case
 
-def learned_arm(args):
-    """The learned motion proposal at 1080p (the survey's config 4): the net
-    is trained (untimed) on ~200k labels — the plain search's LAST-reference
-    vectors over 24 seeded 1080p frame pairs (gratings, noise, piecewise
-    motion, moving occluders) — with Adam, lr 1e-3, batches of 4096 MBs;
-    then, on the bench's P frame, the learned search (proposal + exact
-    +-2 px search around 4 seeds + sub-pel + descent fallback) for LAST,
-    GOLDEN and ALTREF is timed against the plain exhaustive analysis of the
-    same frame and references. Quality: mean SAD per reference against the
-    plain search's own per-reference result."""
+def train_proposal_net(ctx, train_steps):
+    """The learned proposal's net, trained (untimed) on ~200k labels: the
+    plain search's LAST-reference vectors over 24 seeded 1080p frame pairs
+    (gratings, noise, piecewise motion, moving occluders), Adam, lr 1e-3,
+    batches of 4096 MBs. Returns (net, stats)."""
     import torch
 
-    import vp8a
-    from vp8a import abi, learned, synth
+    from vp8a import learned, synth
 
-    ctx = vp8a.Context(0)
-    lam = vp8a.rd_lambda(QI)
+    lam = __import__("vp8a").rd_lambda(QI)
     t0 = time.time()
     xs, ys = [], []
     with learned.on_ctx_stream(ctx):
@@ -1188,7 +1181,7 @@ def learned_arm(args):
     n = x.shape[0]
     losses = []
     t1 = time.time()
-    for it in range(args.train_steps):
+    for it in range(train_steps):
         with learned.on_ctx_stream(ctx):
             idx = torch.randint(0, n, (4096,), generator=g).cuda()
             xb, yb = x[idx].contiguous(), y[idx].contiguous()
@@ -1200,6 +1193,29 @@ def learned_arm(args):
         top4 = float(((cells == y[:65536, None].long()).any(1) & (y[:65536] >= 0)).float().sum() /
                      (y[:65536] >= 0).sum())
     del x, y, xs, ys
+    return net, {"labels": int(n), "losses": losses, "top4": top4, "label_s": t_labels, "train_s": t_train}
+
+
+def learned_arm(args):
+    """The learned motion proposal at 1080p (the survey's config 4): the net
+    is trained (untimed) on ~200k labels — the plain search's LAST-reference
+    vectors over 24 seeded 1080p frame pairs (gratings, noise, piecewise
+    motion, moving occluders) — with Adam, lr 1e-3, batches of 4096 MBs;
+    then, on the bench's P frame, the learned search (proposal + exact
+    +-2 px search around 4 seeds + sub-pel + descent fallback) for LAST,
+    GOLDEN and ALTREF is timed against the plain exhaustive analysis of the
+    same frame and references. Quality: mean SAD per reference against the
+    plain search's own per-reference result."""
+    import torch
+
+    import vp8a
+    from vp8a import abi, learned, synth
+
+    ctx = vp8a.Context(0)
+    lam = vp8a.rd_lambda(QI)
+    net, tstats = train_proposal_net(ctx, args.train_steps)
+    n, losses, top4 = tstats["labels"], tstats["losses"], tstats["top4"]
+    t_labels, t_train = tstats["label_s"], tstats["train_s"]
     # Loop-filter window head: the plain path's level choice on training
     # frames at several quantisers (reconstruction + full sweep + walk).
     head = learned.LfWindowHead(ctx, seed=3)
@@ -1321,6 +1337,77 @@ STREAM_SIZES = [(3840, 2160)] * 8 + [(1280, 720)] * 8
 STREAM_GROUP = 15
 
 
+def stream_learned(ctx, torch, sizes, frames, g, train_steps):
+    """The learned proposal on the altref stream path (the survey's config
+    5): every coded frame of every stream gets, per reference, the learned
+    search's vector (net proposal, exact +-2 px search around 4 seeds,
+    sub-pel, descent fallback) as a second NEWMV candidate of the batched
+    exhaustive analysis; the plain path is the same pipeline without it.
+    One group after the opening one, on the same inputs for both: wall time
+    per group with the bitstream writer off (the learned searches run one
+    frame and reference at a time), then bytes and luma PSNR per resolution
+    with the writer on, and the fallback rate of the learned searches."""
+    from vp8a import abi, learned
+    from vp8a.stream import AltrefStreams
+
+    net, tstats = train_proposal_net(ctx, train_steps)
+    xy_cache, fbs = {}, []
+
+    def proposer(streams, srcs):
+        out = []
+        for st, src in zip(streams.s, srcs):
+            key = (st.mb_cols, st.mb_rows)
+            if key not in xy_cache:
+                xy_cache[key] = learned.all_mbs(st.mb_cols, st.mb_rows)
+            p = np.zeros((st.n_mb, 3), abi.MV_DTYPE)
+            for k, ref in enumerate((st.last, st.golden, st.altref)):
+                mv, _, fb = learned.learned_search(ctx, net, src[0], ref[0], xy_cache[key])
+                p["row"][:, k] = mv[:, 0]
+                p["col"][:, k] = mv[:, 1]
+                fbs.append(float(fb.mean()))
+            out.append(p)
+        return out
+
+    mbs_group = sum(((w + 15) // 16) * ((h + 15) // 16) for w, h in sizes) * g
+    res = {}
+    for mode in ("plain", "learned"):
+        prop = proposer if mode == "learned" else None
+        for write in (False, True):
+            streams = AltrefStreams(ctx, sizes, qi=QI, strength=3, write=write)
+            for gi in range(2):  # the first group opens the streams
+                grp = [f[gi * g:(gi + 1) * g] for f in frames]
+                ctx.synchronize()
+                t = time.perf_counter()
+                pk = streams.encode_group(grp, proposer=prop, psnr=write)
+                ctx.synchronize()
+                dt = time.perf_counter() - t
+            if not write:
+                res[mode] = {"group_s": round(dt, 3), "mbs_per_s_wall": round(mbs_group / dt, 1)}
+                continue
+            by_res = {}
+            for (w, h), packets in zip(sizes, pk):
+                d = by_res.setdefault("%dx%d" % (w, h), {"bytes": 0, "psnr": []})
+                d["bytes"] += sum(len(q["bytes"]) for q in packets if q["bytes"] is not None)
+                d["psnr"] += [q["psnr_y"] for q in packets if "psnr_y" in q]
+            res[mode]["by_res"] = by_res
+            del streams
+    out = {}
+    for r in res["plain"]["by_res"]:
+        a, b = res["plain"]["by_res"][r], res["learned"]["by_res"][r]
+        out[r] = {"plain_bytes": a["bytes"], "learned_bytes": b["bytes"],
+                  "byte_delta_pct": round(100.0 * (b["bytes"] - a["bytes"]) / a["bytes"], 3),
+                  "plain_psnr_y": round(float(np.mean(a["psnr"])), 3), "learned_psnr_y": round(float(np.mean(b["psnr"])), 3),
+                  "psnr_delta_db": round(float(np.mean(b["psnr"]) - np.mean(a["psnr"])), 3)}
+    return {"per_resolution": out, "plain_group_s": res["plain"]["group_s"],
+            "learned_group_s": res["learned"]["group_s"],
+            "plain_mbs_per_s_wall": res["plain"]["mbs_per_s_wall"],
+            "learned_mbs_per_s_wall": res["learned"]["mbs_per_s_wall"],
+            "fallback_rate": round(float(np.mean(fbs)), 4) if fbs else None,
+            "net": {"labels": tstats["labels"], "top4_label_hit": round(tstats["top4"], 4)},
+            "note": "one group after the opening one; wall time with the writer off; the proposals are not "
+                    "fused into the batched analysis launch (one learned search per frame and reference)"}
+
+
 def stream_arm(args):
     """The lagged altref stream path of the survey's config 5: 8 streams at
     3840x2160 and 8 at 1280x720 in lockstep, 15-frame lookahead groups, each
@@ -1382,6 +1469,7 @@ def stream_arm(args):
     for d in by_res.values():
         d["bytes_per_group"] //= d["streams"]
         d["mean_level"] = round(float(np.mean(d.pop("levels"))), 2)
+    learned_res = stream_learned(ctx, torch, sizes, frames, g, args.train_steps) if args.stream_learned else None
     ctx.close()
     return {"case": "stream", "unit": "MB/s", "streams": len(sizes), "sizes": sorted(set("%dx%d" % s for s in sizes)),
             "group": g, "qi": QI, "value": round(mbs_group / (ms / 1e3), 1), "ms_per_group": round(ms, 2),
@@ -1389,7 +1477,7 @@ def stream_arm(args):
             "config": {"workload": "8x3840x2160 + 8x1280x720 altref streams, 15-frame groups: ARNR anchor + 14 P "
                                    "frames per group, exhaustive 3-ref analysis, qi-44 reconstruction, auto-LF "
                                    "(reference walk) and filter on every coded frame", "seed": SEED,
-                       "timed": "device time per group after the first, inputs resident"}}
+                       "timed": "device time per group after the first, inputs resident"}, "learned": learned_res}
 
 
 def rd_arm(args):
@@ -1622,6 +1710,8 @@ def main():
                     help="profile one stage alone, or (batch) the batched many-stream path")
     ap.add_argument("--streams", type=int, default=48, help="streams of the batch case")
     ap.add_argument("--train-steps", type=int, default=300, help="training steps of the learned case")
+    ap.add_argument("--stream-learned", action="store_true",
+                    help="stream case: also run the learned proposal through the stream path against the plain path")
     ap.add_argument("--size", default="1920x1080", help="frame size for --case")
     ap.add_argument("--images", type=int, default=8160, help="32 x 32 maps of the lp_conv case")
     ap.add_argument("--subpel-planes", type=int, default=0, help="analysis sub-pel planes on/off (single-stage cases)")

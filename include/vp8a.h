@@ -628,6 +628,13 @@ typedef struct vp8a_analysis_job {
  * start first). */
 vp8a_status vp8a_analyse_inter_frames(vp8a_ctx* ctx, const vp8a_analysis_job* jobs, uint32_t n_jobs);
 
+/* No counterpart in the reference: vp8a_analyse_inter_frames with
+ * vp8a_analyse_inter_frame_proposals' second NEWMV candidate per job.
+ * proposals[j] holds job j's n_refs vectors per MB (raster order), or is
+ * NULL for a job without proposals. */
+vp8a_status vp8a_analyse_inter_frames_proposals(vp8a_ctx* ctx, const vp8a_analysis_job* jobs, uint32_t n_jobs,
+                                                const vp8a_mv* const* proposals);
+
 /* One vp8a_build_arnr_altref call's arguments. */
 typedef struct vp8a_arnr_job {
   const vp8a_i420* frames;  /* n frames of one size */

@@ -1740,7 +1740,10 @@ extern "C" vp8a_status vp8a_analyse_inter_frame_proposals(vp8a_ctx* ctx, const v
   return finish_analysis(ctx, st);
 }
 
-extern "C" vp8a_status vp8a_analyse_inter_frames(vp8a_ctx* ctx, const vp8a_analysis_job* jobs, uint32_t n_jobs) {
+// The work-list analysis; `proposals` (optional) holds, per job, that job's
+// proposal vectors or null.
+static vp8a_status analyse_frames(vp8a_ctx* ctx, const vp8a_analysis_job* jobs, uint32_t n_jobs,
+                                  const vp8a_mv* const* proposals) {
   if (!ctx || (!jobs && n_jobs)) {
     vp8a::set_error("null argument");
     return VP8A_E_INVALID_ARGUMENT;
@@ -1758,7 +1761,7 @@ extern "C" vp8a_status vp8a_analyse_inter_frames(vp8a_ctx* ctx, const vp8a_analy
   for (uint32_t j = 0; j < n_jobs; j++) {
     const vp8a_analysis_job& J = jobs[j];
     if ((s = prepare_job(ctx, st, mc, &J.frame, J.refs, J.ref_ids, J.n_refs, J.mv_contexts, J.lambda,
-                         J.decisions, J.trace, &args[j])) != VP8A_OK)
+                         J.decisions, J.trace, &args[j], proposals ? proposals[j] : nullptr)) != VP8A_OK)
       return s;
   }
   // One launch per reference count (the cluster size). Within a launch the
@@ -1787,4 +1790,17 @@ extern "C" vp8a_status vp8a_analyse_inter_frames(vp8a_ctx* ctx, const vp8a_analy
       return s;
   }
   return finish_analysis(ctx, st);
+}
+
+extern "C" vp8a_status vp8a_analyse_inter_frames(vp8a_ctx* ctx, const vp8a_analysis_job* jobs, uint32_t n_jobs) {
+  return analyse_frames(ctx, jobs, n_jobs, nullptr);
+}
+
+extern "C" vp8a_status vp8a_analyse_inter_frames_proposals(vp8a_ctx* ctx, const vp8a_analysis_job* jobs,
+                                                           uint32_t n_jobs, const vp8a_mv* const* proposals) {
+  if (!proposals && n_jobs) {
+    vp8a::set_error("null argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  return analyse_frames(ctx, jobs, n_jobs, proposals);
 }

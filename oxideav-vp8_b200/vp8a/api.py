@@ -530,8 +530,11 @@ def _batch(ctx, fn, jobs, where):
 def analyse_inter_frames(ctx, jobs):
     """vp8a_analyse_inter_frames: `jobs` = list of dicts with the arguments
     of analyse_inter_frame (frame, refs, ref_ids, lam, optional
-    mv_contexts). Returns each job's (mb_rows, mb_cols) decisions."""
-    keep, cj, outs = [], [], []
+    mv_contexts, optional proposals: n_refs MV_DTYPE vectors per MB, numpy
+    or a device tensor; any job with proposals makes the call
+    vp8a_analyse_inter_frames_proposals). Returns each job's (mb_rows,
+    mb_cols) decisions."""
+    keep, cj, outs, props = [], [], [], []
     for j in jobs:
         f = i420(*j["frame"])
         prs = [planes(*p) for p in j["refs"]]
@@ -544,7 +547,19 @@ def analyse_inter_frames(ctx, jobs):
         cj.append(abi.AnalysisJob(f, C.cast(parr, C.c_void_p), ptr(ids), len(prs), C.cast(C.pointer(ctxs), C.c_void_p),
                                   j["lam"], ptr(dec), None))
         outs.append(dec.reshape(mbr, mbc))
-    _batch(ctx, "vp8a_analyse_inter_frames", cj, "vp8a_analyse_inter_frames")
+        pr = j.get("proposals")
+        if pr is not None and not hasattr(pr, "data_ptr"):
+            pr = np.ascontiguousarray(pr, abi.MV_DTYPE)
+        keep.append(pr)
+        props.append(None if pr is None else (pr.data_ptr() if hasattr(pr, "data_ptr") else pr.ctypes.data))
+    if any(p is not None for p in props):
+        arr = (abi.AnalysisJob * len(cj))(*cj)
+        parr_ = (C.c_void_p * len(props))(*props)
+        check(ctx._lib.vp8a_analyse_inter_frames_proposals(ctx.handle, C.cast(arr, C.c_void_p), len(cj),
+                                                           C.cast(parr_, C.c_void_p)),
+              "vp8a_analyse_inter_frames_proposals")
+    else:
+        _batch(ctx, "vp8a_analyse_inter_frames", cj, "vp8a_analyse_inter_frames")
     return outs
 
 

@@ -45,6 +45,7 @@ PROTOTYPES = {
     ),
     "vp8a_rd_lambda": (C.c_double, [U32]),
     "vp8a_analyse_inter_frames": (C.c_int, [P, P, U32]),
+    "vp8a_analyse_inter_frames_proposals": (C.c_int, [P, P, U32, P]),
     "vp8a_build_arnr_altrefs": (C.c_int, [P, P, U32]),
     "vp8a_build_arnr_altrefs_planes": (C.c_int, [P, P, U32]),
     "vp8a_reconstruct_inter_frames": (C.c_int, [P, P, U32]),

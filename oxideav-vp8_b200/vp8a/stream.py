@@ -106,9 +106,12 @@ class AltrefStreams:
     def _frames_i420(self, frames):
         return [i420(*f) for f in frames]
 
-    def _analyse(self, srcs):
+    def _analyse(self, srcs, props=None):
         """Exhaustive analysis of srcs[k] (visible (y, u, v) device planes)
-        for stream k against its LAST / GOLDEN / ALTREF."""
+        for stream k against its LAST / GOLDEN / ALTREF; `props` (optional)
+        gives per stream its proposal vectors (3 MV_DTYPE vectors per MB, a
+        device tensor or a contiguous numpy array, or None), the second
+        NEWMV candidate of vp8a_analyse_inter_frames_proposals."""
         jobs, keep = [], []
         for st, src in zip(self.s, srcs):
             refs = (abi.Planes * 3)(planes(*st.last), planes(*st.golden), planes(*st.altref))
@@ -116,8 +119,16 @@ class AltrefStreams:
             jobs.append(abi.AnalysisJob(i420(*src), C.cast(refs, C.c_void_p), self.ids.ctypes.data, 3,
                                         C.cast(C.pointer(self.ctxs), C.c_void_p), self.lam, st.dec.data_ptr(), None))
         arr = (abi.AnalysisJob * len(jobs))(*jobs)
-        check(self.lib.vp8a_analyse_inter_frames(self.ctx.handle, C.cast(arr, C.c_void_p), len(jobs)),
-              "vp8a_analyse_inter_frames")
+        if props is not None and any(p is not None for p in props):
+            ptrs = [None if p is None else (p.data_ptr() if hasattr(p, "data_ptr") else p.ctypes.data) for p in props]
+            parr = (C.c_void_p * len(props))(*ptrs)
+            keep += [parr, props]
+            check(self.lib.vp8a_analyse_inter_frames_proposals(self.ctx.handle, C.cast(arr, C.c_void_p), len(jobs),
+                                                               C.cast(parr, C.c_void_p)),
+                  "vp8a_analyse_inter_frames_proposals")
+        else:
+            check(self.lib.vp8a_analyse_inter_frames(self.ctx.handle, C.cast(arr, C.c_void_p), len(jobs)),
+                  "vp8a_analyse_inter_frames")
         return keep
 
     def _reconstruct(self, srcs):
@@ -171,10 +182,10 @@ class AltrefStreams:
             out.append(write_inter_frame(h, dec, cf))
         return out
 
-    def _code_frame(self, srcs, levels=None, **hdr):
+    def _code_frame(self, srcs, levels=None, props=None, **hdr):
         """Analyse, reconstruct and loop-filter srcs[k] for every stream k;
         the filtered picture is left in each stream's `recon` planes."""
-        keep = self._analyse(srcs)
+        keep = self._analyse(srcs, props)
         keep += self._reconstruct(srcs)
         levels = self._loop_filter(srcs, levels)
         bits = self._bitstreams(levels, **hdr) if self.write else [None] * len(self.s)
@@ -182,14 +193,20 @@ class AltrefStreams:
         return levels, bits
 
     # ------------------------------------------------------------- group
-    def encode_group(self, groups, lf_levels=None):
+    def encode_group(self, groups, lf_levels=None, proposer=None, psnr=False):
         """`groups[k]` = the lookahead group of stream k: a list of visible
         (y, u, v) device pictures (every stream the same length). Returns
         per stream the list of packets, each a dict with `kind` ("key", the
         uncoded stand-in, "altref" or "inter"), `level`, `sharpness` and
         `bytes` (None without `write`). `lf_levels`, when given, is a
         function (stage index, streams) -> list of (level, sharpness)
-        replacing the automatic pick (the learned window's hook)."""
+        replacing the automatic pick (the learned window's hook);
+        `proposer`, when given, is a function (streams, srcs) -> per stream
+        the proposal vectors of each coded frame (see _analyse), called
+        before the frame's analysis with its references in place (the
+        learned proposal's hook). With `psnr` each inter packet also
+        carries `psnr_y`, the luma PSNR of the filtered picture against its
+        source."""
         torch = self.torch
         n = len(groups[0])
         assert all(len(g) == n for g in groups), "every stream's group must have the same length"
@@ -222,6 +239,7 @@ class AltrefStreams:
             srcs = [(st.anchor[0][:st.h, :st.w], st.anchor[1][:(st.h + 1) // 2, :(st.w + 1) // 2],
                      st.anchor[2][:(st.h + 1) // 2, :(st.w + 1) // 2]) for st in self.s]
             levels, bits = self._code_frame(srcs, lf_levels(stage, self) if lf_levels else None,
+                                            proposer(self, srcs) if proposer else None,
                                             refresh_last=0, refresh_alternate_frame=1)
             stage += 1
             for st, p, (lv, sh), b in zip(self.s, packets, levels, bits):
@@ -229,11 +247,18 @@ class AltrefStreams:
                 p.append({"kind": "altref", "level": lv, "sharpness": sh, "bytes": b})
         for j in range(first_p, n):
             srcs = [g[j] for g in groups]
-            levels, bits = self._code_frame(srcs, lf_levels(stage, self) if lf_levels else None)
+            levels, bits = self._code_frame(srcs, lf_levels(stage, self) if lf_levels else None,
+                                            proposer(self, srcs) if proposer else None)
             stage += 1
-            for st, p, (lv, sh), b in zip(self.s, packets, levels, bits):
+            for st, p, (lv, sh), b, src in zip(self.s, packets, levels, bits, srcs):
                 st.last, st.recon = st.recon, st.last
-                p.append({"kind": "inter", "level": lv, "sharpness": sh, "bytes": b})
+                pk = {"kind": "inter", "level": lv, "sharpness": sh, "bytes": b}
+                if psnr:
+                    with torch.cuda.stream(self.stream):
+                        d = st.last[0][:st.h, :st.w].float() - src[0].float()
+                        mse = float((d * d).mean())
+                    pk["psnr_y"] = 99.0 if mse == 0.0 else 10.0 * float(np.log10(255.0 * 255.0 / mse))
+                p.append(pk)
         return packets
 
     def references(self, k):

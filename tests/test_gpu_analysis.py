@@ -176,3 +176,30 @@ def test_analysis_with_proposals(ctx, oracle):
     got = vp8a.analyse_inter_frame(ctx, cur, [ref], [1], lam, proposals=prop)
     assert_same(got, want)
     assert ((want["mode"] == abi.MODE_NEW) & (want["mv"]["col"] == 120)).any()
+
+
+def test_batched_analysis_with_proposals(ctx, oracle):
+    # vp8a_analyse_inter_frames_proposals: a work list of frames of two sizes,
+    # some jobs with proposal vectors and one without, each equal to the
+    # oracle's single-frame decision with (or without) its proposals.
+    ids = [abi.REF_LAST, abi.REF_GOLDEN, abi.REF_ALTREF]
+    lam = vp8a.rd_lambda(44)
+    rng = np.random.default_rng(9)
+    jobs, wants = [], []
+    for (w, h), seed, with_props in (((320, 240), 31, True), ((176, 144), 7, False), ((176, 144), 8, True)):
+        frames, _ = synth.make_sequence(w, h, 7, seed=seed, pieces=5, occluders=4)
+        refs = refs_for(frames, 3)
+        n = ((w + 15) // 16) * ((h + 15) // 16)
+        job = dict(frame=frames[3], refs=refs, ref_ids=ids, lam=lam)
+        prop = None
+        if with_props:
+            prop = np.zeros((n, 3), abi.MV_DTYPE)
+            prop["row"] = rng.integers(-40, 41, (n, 3))
+            prop["col"] = rng.integers(-40, 41, (n, 3))
+            prop[rng.random((n, 3)) < 0.1] = (0, 0)
+            job["proposals"] = prop
+        jobs.append(job)
+        wants.append(oracle.analyse_inter_frame(frames[3], refs, ids, lam, proposals=prop, threads=8))
+    got = vp8a.analyse_inter_frames(ctx, jobs)
+    for g, w_ in zip(got, wants):
+        assert_same(g, w_)
