@@ -1272,6 +1272,13 @@ def learned_arm(args):
 
     ms_learned, ts_l = timed(learned_step, args.steps, args.warmup)
     ms_plain, ts_p = timed(gs.run_analysis, args.steps, args.warmup)
+    # Per-stage device time of one learned frame (3 references), CUDA events
+    # on the library stream: the gaps between stages (host orchestration)
+    # fall into the stage that follows them.
+    stage_ms = {}
+    for r in refs:
+        learned.learned_search(ctx, net, src, r, xy, timings=stage_ms)
+    stage_ms = {k_: round(v_, 4) for k_, v_ in stage_ms.items()}
     # The full step with the learned loop-filter window: ARNR, the plain
     # analysis and reconstruction, the head's window from 256 sampled MBs
     # (net layers 1-3 against LAST), the sweep over level 0 and the window's
@@ -1309,7 +1316,7 @@ def learned_arm(args):
     rd = learned_rd(ctx, net, head, sample)
     ctx.close()
     return {"case": "learned", "size": "%dx%d" % (W, H), "unit": "MB/s",
-            "learned_me_mbs_per_s": round(N_MB / (ms_learned / 1e3), 1), "learned_me_ms": round(ms_learned, 3),
+            "learned_me_mbs_per_s": round(N_MB / (ms_learned / 1e3), 1), "learned_me_ms": round(ms_learned, 3), "learned_stage_ms": stage_ms,
             "plain_analysis_mbs_per_s": round(N_MB / (ms_plain / 1e3), 1), "plain_analysis_ms": round(ms_plain, 3),
             "speedup_vs_plain_analysis": round(ms_plain / ms_learned, 2),
             "mean_sad_ratio_vs_plain_per_ref": [round(v, 4) for v in ratio],

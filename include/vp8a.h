@@ -735,6 +735,18 @@ vp8a_status vp8a_select_filter_params_batch(vp8a_ctx* ctx, const vp8a_sweep_job*
 vp8a_status vp8a_lp_windows(vp8a_ctx* ctx, const vp8a_luma_ref* src, const vp8a_luma_ref* ref,
                             const uint32_t* mb_xy, uint32_t n, uint16_t* out);
 
+/* The exact whole-pel search around the net's seeds for n MBs: item i is
+ * the MB at mb_xy[2i], mb_xy[2i+1] (column, row) with its 16x16 source
+ * src_mbs[i] (256 bytes) and k seed cells seeds[i*k .. i*k+k-1] (cell c
+ * stands for the vector ((c / 32 - 16) * 2, (c % 32 - 16) * 2) px). Every
+ * vector within +-radius px of each seed is scored (whole-pel SAD against
+ * the edge-clamped `ref`); out[i] = the first smallest in seed, row,
+ * column order (vector in quarter-pels, SAD). 1 <= k <= 4, radius <= 4,
+ * k * (2 radius + 1)^2 <= 128. */
+vp8a_status vp8a_lp_seeded_search(vp8a_ctx* ctx, const vp8a_luma_ref* ref, const uint8_t* src_mbs,
+                                  const uint32_t* mb_xy, const int32_t* seeds, uint32_t k, uint32_t radius,
+                                  uint32_t n, vp8a_search_result* out);
+
 /* One conv layer (cin -> cout in {2->32, 32->32, 32->1}) over n images,
  * + bias, ReLU when `relu`; output BF16 `y` or FP32 `y_f32` (one of them). */
 vp8a_status vp8a_lp_conv_forward(vp8a_ctx* ctx, const uint16_t* x, uint32_t cin, const uint16_t* w,

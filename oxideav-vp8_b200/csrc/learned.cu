@@ -94,6 +94,65 @@ __global__ void __launch_bounds__(256) lp_windows_kernel(const uint8_t* src, uin
   }
 }
 
+// ------------------------------------------------------- seeded search
+
+// The exact search around the net's seeds: one CTA per MB, thread t takes
+// candidate t = (seed s, row offset dr, column offset dc) in seed, row,
+// column order. The source MB and each seed's (16 + 2 radius)-pixel square
+// window of the reference (edge-clamped, as every whole-pel SAD reads it)
+// sit in shared memory; the first smallest (SAD, order) wins.
+constexpr int LP_SEED_MAXC = 128;  // k * (2 radius + 1)^2
+constexpr int LP_SEED_MAXW = 16 + 2 * 4;  // window side for radius <= 4
+__global__ void __launch_bounds__(LP_SEED_MAXC) lp_seeded_search_kernel(const uint8_t* ref, uint64_t rs, int rw,
+                                                                        int rh, const uint8_t* src_mbs,
+                                                                        const uint32_t* xy, const int32_t* seeds,
+                                                                        int k, int radius, vp8a_search_result* out) {
+  __shared__ uint8_t win[4][LP_SEED_MAXW * LP_SEED_MAXW];
+  __shared__ uint8_t sm[256];
+  __shared__ uint32_t best_w[LP_SEED_MAXC / 32];
+  const int i = blockIdx.x, t = threadIdx.x;
+  const int mx = (int)xy[2 * i] * 16, my = (int)xy[2 * i + 1] * 16;
+  const int side = 16 + 2 * radius, per = (2 * radius + 1) * (2 * radius + 1);
+  for (int q = t; q < 256; q += blockDim.x) sm[q] = src_mbs[(size_t)i * 256 + q];
+  for (int s = 0; s < k; s++) {
+    const int c = seeds[(size_t)i * k + s];
+    const int x0 = mx + (c % 32 - 16) * 2 - radius, y0 = my + (c / 32 - 16) * 2 - radius;
+    for (int q = t; q < side * side; q += blockDim.x) {
+      const int y = min(max(y0 + q / side, 0), rh - 1), x = min(max(x0 + q % side, 0), rw - 1);
+      win[s][q] = ref[(size_t)y * rs + x];
+    }
+  }
+  __syncthreads();
+  uint32_t key = 0xffffffffu;
+  if (t < k * per) {
+    const int s = t / per, o = t - s * per, dr = o / (2 * radius + 1), dc = o - dr * (2 * radius + 1);
+    const uint8_t* w = win[s] + dr * side + dc;
+    uint32_t sad = 0;
+    for (int r = 0; r < 16; r++) {
+#pragma unroll
+      for (int cc = 0; cc < 16; cc++) {
+        const int d = (int)w[r * side + cc] - (int)sm[r * 16 + cc];
+        sad += (uint32_t)(d < 0 ? -d : d);
+      }
+    }
+    key = (sad << 7) | (uint32_t)t;
+  }
+  key = __reduce_min_sync(0xffffffffu, key);
+  if ((t & 31) == 0) best_w[t >> 5] = key;
+  __syncthreads();
+  if (t == 0) {
+    uint32_t b = best_w[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) b = min(b, best_w[w]);
+    const int o = (int)(b & 127u), s = o / per, r = o - s * per;
+    const int c = seeds[(size_t)i * k + s];
+    vp8a_search_result res;
+    res.mv.row = (int16_t)((c / 32 - 16) * 8 + 4 * (r / (2 * radius + 1) - radius));
+    res.mv.col = (int16_t)((c % 32 - 16) * 8 + 4 * (r % (2 * radius + 1) - radius));
+    res.sad = b >> 7;
+    out[i] = res;
+  }
+}
+
 // ------------------------------------------------------------ conv fwd
 
 // Implicit GEMM: A[p][k] = X[p + off(tap)][ci], k = tap * CP + ci (CP = CIN
@@ -742,6 +801,31 @@ vp8a_status vp8a_lp_windows(vp8a_ctx* ctx, const vp8a_luma_ref* src, const vp8a_
   VP8A_CUDA(cudaSetDevice(ctx->device));
   lp_windows_kernel<<<n, 256, 0, ctx->stream>>>(src->plane, src->stride, ref->plane, ref->stride, (int)src->width,
                                                  (int)src->height, mb_xy, (int)n, out);
+  VP8A_CUDA(cudaGetLastError());
+  ctx->launches++;
+  return VP8A_OK;
+}
+
+vp8a_status vp8a_lp_seeded_search(vp8a_ctx* ctx, const vp8a_luma_ref* ref, const uint8_t* src_mbs,
+                                  const uint32_t* mb_xy, const int32_t* seeds, uint32_t k, uint32_t radius, uint32_t n,
+                                  vp8a_search_result* out) {
+  if (!ctx || !ref || (n && (!src_mbs || !mb_xy || !seeds || !out))) {
+    vp8a::set_error("null argument");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (k < 1 || k > 4 || radius > 4 || k * (2 * radius + 1) * (2 * radius + 1) > (uint32_t)LP_SEED_MAXC) {
+    vp8a::set_error("seeded search: 1 <= k <= 4, radius <= 4 and k * (2 radius + 1)^2 <= 128");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (!ref->plane || ref->width < 16 || ref->height < 16 || ref->stride < ref->width) {
+    vp8a::set_error("bad reference plane");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  if (n == 0) return VP8A_OK;
+  VP8A_CUDA(cudaSetDevice(ctx->device));
+  lp_seeded_search_kernel<<<n, LP_SEED_MAXC, 0, ctx->stream>>>(ref->plane, ref->stride, (int)ref->width,
+                                                                (int)ref->height, src_mbs, mb_xy, seeds, (int)k,
+                                                                (int)radius, out);
   VP8A_CUDA(cudaGetLastError());
   ctx->launches++;
   return VP8A_OK;

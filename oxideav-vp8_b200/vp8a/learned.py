@@ -230,51 +230,54 @@ def labels_from_search(ctx, frame, ref_padded, lam):
     return cell_of_mv(q["row"], q["col"]), tr[..., 0]["quarter"]["sad"].reshape(-1)
 
 
-def learned_search(ctx, net, src_y, ref_y, mb_xy, k=4, radius=2, fallback=1.25, seeds=None):
+def learned_search(ctx, net, src_y, ref_y, mb_xy, k=4, radius=2, fallback=1.25, seeds=None, timings=None):
     """The learned path for one (source, reference) luma pair: proposal,
     exact +-`radius` px whole-pel search around each of the k seeds, half-
     and quarter-pel refinement of the best, and the plain descent from the
     zero vector for MBs whose SAD exceeds `fallback` x the median. `seeds`
-    ([n, k] cells) replaces the net (the ablation). Returns (mv [n, 2]
-    quarter-pel int16, sad [n] uint32, fell_back [n] bool) as numpy."""
+    ([n, k] cells) replaces the net (the ablation). `timings` (a dict),
+    when given, accumulates each stage's device milliseconds (CUDA events
+    on the library stream): cost volumes, net, seeded whole-pel search,
+    sub-pel refinement, fallback. Returns (mv [n, 2] quarter-pel int16, sad
+    [n] uint32, fell_back [n] bool) as numpy."""
     import torch
 
     with on_ctx_stream(ctx):
-        return _learned_search(ctx, net, src_y, ref_y, mb_xy, k, radius, fallback, seeds)
+        return _learned_search(ctx, net, src_y, ref_y, mb_xy, k, radius, fallback, seeds, timings)
 
 
-def _learned_search(ctx, net, src_y, ref_y, mb_xy, k, radius, fallback, seeds):
+def _learned_search(ctx, net, src_y, ref_y, mb_xy, k, radius, fallback, seeds, timings=None):
     import torch
+
+    marks = []
+
+    def mark(name):
+        if timings is not None:
+            e = torch.cuda.Event(enable_timing=True)
+            e.record()
+            marks.append((name, e))
 
     n = mb_xy.shape[0]
     h, w = src_y.shape[0], src_y.shape[1]
+    mark("start")
     if seeds is None:
         x = windows(ctx, src_y, ref_y[:h, :w], mb_xy)
+        mark("cost_volumes")
         seeds = net.propose(x, k)
-    seeds = seeds.to(torch.int64)
-    sr = (seeds // GRID - 16) * 8
-    sc = (seeds % GRID - 16) * 8
-    d = torch.arange(-radius, radius + 1, device=seeds.device) * 4
-    dr, dc = torch.meshgrid(d, d, indexing="ij")
-    ncand = k * dr.numel()
-    cr = (sr[:, :, None] + dr.reshape(1, 1, -1)).reshape(n, ncand)
-    cc = (sc[:, :, None] + dc.reshape(1, 1, -1)).reshape(n, ncand)
-    cr = cr.clamp(-1023, 1023)
-    cc = cc.clamp(-1023, 1023)
+        mark("net")
     mbr, mbc = (h + 15) // 16, (w + 15) // 16
     # Source MBs (16x16 luma, edge-replicated) for every item.
     src_mbs = _source_mbs(src_y, mb_xy, h, w)
-    rep_src = src_mbs.repeat_interleave(ncand, dim=0)
-    rep_xy = mb_xy.repeat_interleave(ncand, dim=0)
-    mvs = torch.stack([cr, cc], dim=2).reshape(-1, 2).to(torch.int16).contiguous()
-    sads = torch.empty(n * ncand, dtype=torch.int32, device=seeds.device)
     ref = luma_ref(ref_y, width=mbc * 16, height=mbr * 16)
     lib = ctx._lib
-    check(lib.vp8a_mb_luma_sad_at_mv(ctx.handle, C.byref(ref), ptr(rep_src), ptr(rep_xy), ptr(mvs), n * ncand,
-                                     ptr(sads)), "vp8a_mb_luma_sad_at_mv")
-    # First smallest SAD in seed order.
-    best = sads.view(n, ncand).to(torch.int64).argmin(dim=1)
-    whole = mvs.view(n, ncand, 2)[torch.arange(n, device=seeds.device), best].contiguous()
+    # Every whole-pel vector within +-radius px of each seed, first smallest
+    # SAD in seed, row, column order (one fused kernel).
+    seeds32 = seeds.to(torch.int32).contiguous()
+    found = torch.empty((n, 2), dtype=torch.int32, device=seeds.device)  # search_result: mv (2 x i16) + sad
+    check(lib.vp8a_lp_seeded_search(ctx.handle, C.byref(ref), ptr(src_mbs), ptr(mb_xy), ptr(seeds32), k, radius, n,
+                                    ptr(found)), "vp8a_lp_seeded_search")
+    mark("seeded_search")
+    whole = found[:, 0].contiguous().view(torch.int16).view(n, 2)
     sr_out = torch.empty((n, 2), dtype=torch.int32, device=seeds.device)  # search_result: mv (2 x i16) + sad
     half = torch.empty((n, 2), dtype=torch.int32, device=seeds.device)
     check(lib.vp8a_half_pixel_refine_luma(ctx.handle, C.byref(ref), ptr(src_mbs), ptr(mb_xy), ptr(whole), n,
@@ -284,24 +287,26 @@ def _learned_search(ctx, net, src_y, ref_y, mb_xy, k, radius, fallback, seeds):
                                              n, ptr(sr_out)), "vp8a_quarter_pixel_refine_luma")
     out_mv = sr_out[:, 0].contiguous().view(torch.int16).view(n, 2).clone()
     out_sad = sr_out[:, 1].clone()
-    # Fallback: the plain descent from the zero vector (8 rounds + sub-pel).
+    mark("subpel")
+    # Fallback: the plain descent from the zero vector (8 rounds + sub-pel)
+    # for the MBs whose SAD exceeds `fallback` x the median. The descent runs
+    # for every MB (each item is independent) and is kept where it falls
+    # back and wins, so no count or index list crosses to the host.
     med = out_sad.to(torch.float32).median()
     fb = out_sad.to(torch.float32) > fallback * med
-    nf = int(fb.sum().item())
-    if nf:
-        idx = torch.nonzero(fb).reshape(-1)
-        zero = torch.zeros((nf, 2), dtype=torch.int16, device=seeds.device)
-        w_o = torch.empty((nf, 2), dtype=torch.int32, device=seeds.device)
-        h_o = torch.empty_like(w_o)
-        q_o = torch.empty_like(w_o)
-        check(lib.vp8a_motion_descent(ctx.handle, C.byref(ref), ptr(src_mbs[idx].contiguous()),
-                                      ptr(mb_xy[idx].contiguous()), ptr(zero), 8, nf, ptr(w_o), ptr(h_o), ptr(q_o)),
-              "vp8a_motion_descent")
-        better = q_o[:, 1] < out_sad[idx]
-        sel = idx[better]
-        out_sad[sel] = q_o[better, 1]
-        out_mv[sel] = q_o[better, 0].contiguous().view(torch.int16).view(-1, 2)
+    zero = torch.zeros((n, 2), dtype=torch.int16, device=seeds.device)
+    w_o = torch.empty((n, 2), dtype=torch.int32, device=seeds.device)
+    h_o = torch.empty_like(w_o)
+    q_o = torch.empty_like(w_o)
+    check(lib.vp8a_motion_descent(ctx.handle, C.byref(ref), ptr(src_mbs), ptr(mb_xy), ptr(zero), 8, n, ptr(w_o),
+                                  ptr(h_o), ptr(q_o)), "vp8a_motion_descent")
+    better = fb & (q_o[:, 1] < out_sad)
+    out_sad = torch.where(better, q_o[:, 1], out_sad)
+    out_mv = torch.where(better[:, None], q_o[:, 0].contiguous().view(torch.int16).view(n, 2), out_mv)
+    mark("fallback")
     ctx.synchronize()
+    for (_, a), (name, b) in zip(marks, marks[1:]):
+        timings[name] = timings.get(name, 0.0) + a.elapsed_time(b)
     return out_mv.cpu().numpy(), out_sad.cpu().numpy().astype(np.uint32), fb.cpu().numpy()
 
 

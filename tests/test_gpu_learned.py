@@ -261,6 +261,55 @@ def test_learned_search_is_exact_and_beats_zero_seeds(ctx, oracle):
     assert sad.mean() <= 1.15 * plain_sad.mean(), (sad.mean(), plain_sad.mean())
 
 
+@pytest.mark.parametrize("k,radius", [(4, 2), (1, 4), (3, 1)])
+def test_seeded_search_is_the_first_smallest_sad(ctx, oracle, k, radius):
+    # vp8a_lp_seeded_search against its definition: every whole-pel vector
+    # within +-radius px of each seed cell, SADs from the plain search's
+    # SAD (the oracle), first smallest in seed, row, column order. Seeds
+    # near the grid's edges put windows across the reference's border.
+    import ctypes as C
+
+    frames = moving_sequence(176, 144, 13)
+    ref = vp8a.pad_to_mb(*frames[2])
+    src = frames[3]
+    n_mb = 11 * 9
+    xy = learned.all_mbs(11, 9)
+    srcd = torch.from_numpy(src[0]).cuda()
+    refd = torch.from_numpy(np.ascontiguousarray(ref[0])).cuda()
+    src_mbs = learned._source_mbs(srcd, xy, 144, 176)
+    rng = np.random.default_rng(k * 10 + radius)
+    cells = rng.integers(0, 1024, (n_mb, k)).astype(np.int32)
+    cells[0] = 0
+    cells[1] = 1023
+    dseeds = torch.from_numpy(cells).cuda()
+    out = torch.empty((n_mb, 2), dtype=torch.int32, device="cuda")
+    lib = vp8a.load()
+    r = vp8a.frames.luma_ref(refd, width=176, height=144)
+    with learned.on_ctx_stream(ctx):
+        st = lib.vp8a_lp_seeded_search(ctx.handle, C.byref(r), src_mbs.data_ptr(), xy.data_ptr(),
+                                       dseeds.data_ptr(), k, radius, n_mb, out.data_ptr())
+    assert st == 0, lib.vp8a_last_error()
+    ctx.synchronize()
+    got = out.cpu().numpy()
+    mv = got[:, 0].copy().view(np.int16).reshape(n_mb, 2)
+    sad = got[:, 1].view(np.uint32)
+    offs = [(dr, dc) for dr in range(-radius, radius + 1) for dc in range(-radius, radius + 1)]
+    cand = np.array([[((c // 32 - 16) * 8 + 4 * dr, (c % 32 - 16) * 8 + 4 * dc) for c in row for dr, dc in offs]
+                     for row in cells], np.int16)
+    ncand = cand.shape[1]
+    xyh = np.repeat(xy.cpu().numpy().view(np.uint32), ncand, axis=0)
+    sm = np.repeat(src_mbs.cpu().numpy(), ncand, axis=0)
+    all_sad = np.asarray(oracle.mb_luma_sad_at_mv(ref[0], sm, xyh, cand.reshape(-1, 2)), np.uint32).reshape(n_mb, ncand)
+    best = all_sad.argmin(axis=1)
+    assert np.array_equal(sad, all_sad[np.arange(n_mb), best])
+    assert np.array_equal(mv, cand[np.arange(n_mb), best])
+    # Out-of-range arguments are errors.
+    with learned.on_ctx_stream(ctx):
+        st = lib.vp8a_lp_seeded_search(ctx.handle, C.byref(r), src_mbs.data_ptr(), xy.data_ptr(),
+                                       dseeds.data_ptr(), 4, 3, n_mb, out.data_ptr())
+    assert st == abi.E_INVALID_ARGUMENT
+
+
 def test_filter_sweep_window_matches_the_full_table(ctx, oracle):
     from test_gpu_lf import lf_case
 
