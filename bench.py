@@ -1702,6 +1702,60 @@ def lp_conv_arm(args):
     return {"case": "lp_conv", "images": n, "layer": "3x3 conv 32 -> 32 on 32 x 32 maps", **out}
 
 
+def lp_net_arm(args):
+    """The whole proposal net (vp8a_lp_net_propose: four layers and the top
+    4 cells in one launch) over `--images` 32 x 32 maps, beside the same net
+    layer by layer (four vp8a_lp_conv_forward launches and a torch top-k),
+    CUDA events on the context stream. 24480 maps = the three references
+    of a 1080p frame."""
+    import torch
+
+    import vp8a
+    from vp8a import learned
+
+    ctx = vp8a.Context(0)
+    n = args.images
+    net = learned.ProposalNet(ctx, seed=1)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    with learned.on_ctx_stream(ctx):
+        x = (torch.relu(torch.randn(n, 32, 32, 2, device="cuda", generator=g)) * 40).to(torch.bfloat16)
+    ctx.synchronize()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+
+    def fused():
+        return net.propose(x, 4)
+
+    def layered():
+        with learned.on_ctx_stream(ctx):
+            return torch.topk(net.forward(x), 4, dim=1).indices
+
+    out = {}
+    for name, fn in (("fused", fused), ("layered", layered)):
+        for _ in range(args.warmup):
+            fn()
+        ctx.synchronize()
+        ts = []
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        ms = sorted(ts)[len(ts) // 2]
+        # Algorithmic FLOPs of the four 3 x 3 layers over the 32 x 32 map.
+        flops = 2.0 * n * 1024 * 9 * (2 * 32 + 32 * 32 + 32 * 32 + 32 * 1)
+        sms = torch.cuda.get_device_properties(0).multi_processor_count
+        out[name] = {"ms": round(ms, 4), "tflops": round(flops / ms / 1e9, 1),
+                     "us_per_map_per_sm": round(ms * 1e3 * sms / n, 3)}
+    with learned.on_ctx_stream(ctx):
+        same = float((fused() == layered().to(torch.int32)).all(1).float().mean())
+    out["top4_rows_equal_to_layered"] = round(same, 4)
+    del x, stream, net
+    ctx.close()
+    return {"case": "lp_net", "images": n, **out}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1712,7 +1766,7 @@ def main():
     ap.add_argument("--no-parity", action="store_true", help="skip the step's parity check against the oracle")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--case", choices=["arnr", "analysis", "lf", "recon", "predict", "predict_mb", "predict_split",
-                                       "batch", "learned", "lp_conv", "rd", "stream", "trellis", "me", "lp_windows",
+                                       "batch", "learned", "lp_conv", "lp_net", "rd", "stream", "trellis", "me", "lp_windows",
                                        "lp_bwd"],
                     help="profile one stage alone, or (batch) the batched many-stream path")
     ap.add_argument("--streams", type=int, default=48, help="streams of the batch case")
@@ -1720,7 +1774,7 @@ def main():
     ap.add_argument("--stream-learned", action="store_true",
                     help="stream case: also run the learned proposal through the stream path against the plain path")
     ap.add_argument("--size", default="1920x1080", help="frame size for --case")
-    ap.add_argument("--images", type=int, default=8160, help="32 x 32 maps of the lp_conv case")
+    ap.add_argument("--images", type=int, default=8160, help="32 x 32 maps of the lp_conv and lp_net cases")
     ap.add_argument("--subpel-planes", type=int, default=0, help="analysis sub-pel planes on/off (single-stage cases)")
     ap.add_argument("--lf-layout", default="", help="passes,threads,prefetch: force the sweep's launch shape (cases)")
     args = ap.parse_args()
@@ -1732,6 +1786,8 @@ def main():
         res = learned_arm(args)
     elif args.case == "lp_conv":
         res = lp_conv_arm(args)
+    elif args.case == "lp_net":
+        res = lp_net_arm(args)
     elif args.case == "rd":
         res = rd_arm(args)
     elif args.case == "stream":

@@ -747,6 +747,18 @@ vp8a_status vp8a_lp_seeded_search(vp8a_ctx* ctx, const vp8a_luma_ref* ref, const
                                   const uint32_t* mb_xy, const int32_t* seeds, uint32_t k, uint32_t radius,
                                   uint32_t n, vp8a_search_result* out);
 
+/* The whole net (2 -> 32 -> 32 -> 32 -> 1, ReLU between) for n images in
+ * one launch, activations kept on chip: x = [n][32][32][2] BF16, weights
+ * and FP32 biases as for vp8a_lp_conv_forward's four layers. cells[i*k ..]
+ * receives image i's k highest-scoring cells, best first (the first cell
+ * among equal scores), 1 <= k <= 16; `logits` (optional, [n][1024] FP32)
+ * the scores. The same sums as the layer-by-layer calls in another FP32
+ * accumulation order. */
+vp8a_status vp8a_lp_net_propose(vp8a_ctx* ctx, const uint16_t* x, uint32_t n, const uint16_t* w1,
+                                const float* b1, const uint16_t* w2, const float* b2, const uint16_t* w3,
+                                const float* b3, const uint16_t* w4, const float* b4, uint32_t k,
+                                int32_t* cells, float* logits);
+
 /* One conv layer (cin -> cout in {2->32, 32->32, 32->1}) over n images,
  * + bias, ReLU when `relu`; output BF16 `y` or FP32 `y_f32` (one of them). */
 vp8a_status vp8a_lp_conv_forward(vp8a_ctx* ctx, const uint16_t* x, uint32_t cin, const uint16_t* w,

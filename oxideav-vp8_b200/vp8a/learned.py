@@ -187,10 +187,21 @@ class ProposalNet:
         return float((loss / valid).item())
 
     @_ordered
-    def propose(self, x, k=4):
-        """Top-k cells per item, best first ([n, k] int64 device tensor)."""
-        logits = self.forward(x)
-        return self.torch.topk(logits, k, dim=1).indices
+    def propose(self, x, k=4, logits=None):
+        """Top-k cells per item, best first ([n, k] int32 device tensor; the
+        first cell among equal scores): the whole net in one fused launch
+        (vp8a_lp_net_propose), activations on chip. `logits` (optional
+        [n, 1024] FP32 device tensor) receives the scores."""
+        torch = self.torch
+        n = x.shape[0]
+        cells = torch.empty((n, k), dtype=torch.int32, device=self.dev)
+        L = self.layers
+        check(self._lib().vp8a_lp_net_propose(self.ctx.handle, ptr(x), n, ptr(L[0]["wh"]), ptr(L[0]["b"]),
+                                              ptr(L[1]["wh"]), ptr(L[1]["b"]), ptr(L[2]["wh"]), ptr(L[2]["b"]),
+                                              ptr(L[3]["wh"]), ptr(L[3]["b"]), k, ptr(cells),
+                                              ptr(logits) if logits is not None else None),
+              "vp8a_lp_net_propose")
+        return cells
 
 
 def windows(ctx, src_y, ref_y, mb_xy):

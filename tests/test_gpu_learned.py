@@ -350,3 +350,45 @@ def test_lf_head_matches_its_definition(ctx):
     assert np.allclose(gb.cpu().numpy(), g, rtol=1e-4, atol=1e-6)
     assert np.allclose(gw.cpu().numpy().reshape(levels, c), np.outer(g, f), rtol=1e-4, atol=1e-6)
     assert abs(loss.item() + np.log(p[17])) < 1e-4
+
+
+@pytest.mark.parametrize("k", [1, 4, 16])
+def test_fused_net_matches_the_layered_net(ctx, k):
+    # vp8a_lp_net_propose (the four layers in one launch, activations on
+    # chip) against the layer-by-layer forward of the same net: the same
+    # sums over BF16 activations in another FP32 accumulation order, so an
+    # activation may round to the neighbouring BF16 value; the scores agree
+    # within 2^-6 of their range. The cells are exactly the first-index
+    # top k of the fused scores. 300 images: more than one per CTA.
+    rng = np.random.default_rng(k)
+    frames = moving_sequence(176, 144, 21)
+    srcd = torch.from_numpy(frames[3][0]).cuda()
+    refd = torch.from_numpy(frames[2][0]).cuda()
+    xw = learned.windows(ctx, srcd, refd, learned.all_mbs(11, 9))
+    xr = dev_bf16(rng.standard_normal((300 - xw.shape[0], 32, 32, 2)) * 40)
+    with learned.on_ctx_stream(ctx):
+        x = torch.cat([xw, xr]).contiguous()
+    net = learned.ProposalNet(ctx, seed=3 + k)
+    want = net.forward(x)
+    logits = torch.full((300, 1024), float("nan"), dtype=torch.float32, device="cuda")
+    cells = net.propose(x, k, logits=logits)
+    ctx.synchronize()
+    got, want, cells = logits.cpu().numpy(), want.cpu().numpy(), cells.cpu().numpy()
+    assert np.isfinite(got).all()
+    scale = np.abs(want).max(axis=1, keepdims=True) + 1e-3
+    assert np.all(np.abs(got - want) <= scale * 2.0 ** -6)
+    assert cells.dtype == np.int32 and cells.shape == (300, k)
+    assert np.array_equal(cells, np.argsort(-got, axis=1, kind="stable")[:, :k])
+
+
+def test_fused_net_arguments(ctx):
+    net = learned.ProposalNet(ctx, seed=1)
+    x = torch.zeros((2, 32, 32, 2), dtype=torch.bfloat16, device="cuda")
+    L = net.layers
+    lib = ctx._lib
+    cells = torch.zeros((2, 17), dtype=torch.int32, device="cuda")
+    args = [x.data_ptr(), 2] + [v for li in L for v in (li["wh"].data_ptr(), li["b"].data_ptr())]
+    for bad_k in (0, 17):
+        assert lib.vp8a_lp_net_propose(ctx.handle, *args, bad_k, cells.data_ptr(), None) == abi.E_INVALID_ARGUMENT
+    assert lib.vp8a_lp_net_propose(ctx.handle, x.data_ptr(), 0, *args[2:], 4, None, None) == abi.OK
+    ctx.synchronize()
