@@ -617,32 +617,30 @@ __global__ void __launch_bounds__(256, 2) lp_conv_fwd_tc_kernel(const __grid_con
 
 // ------------------------------------------ fused net inference (tcgen05)
 // The whole proposal net, one image at a time per persistent CTA (one per
-// SM, the weights staged once), warp-specialised: warp 16 issues every
-// tcgen05.mma (lane 0) into TMEM accumulators of 96 columns;
-// warps 0-15 (two groups of 8 taking alternate tiles, each with a ring of
-// two accumulators) read each one back as soon as its MMAs commit, add the
-// bias, apply the ReLU, store BF16 into the next layer's activation buffer
-// and mark the tile written. A tile u of the next layer reads the halo rows
-// of tiles u - 1 .. u + 1, so its MMAs start once those three are written,
-// while the epilogue of the later tiles runs. Two activation buffers
-// alternate: B holds the input and layer 2's output, A layers 1 and 3.
-// Layouts are the 32 -> 32 kernel's: a 34-pixel halo pitch, channel-group
-// major (8 channels = 16 bytes per pixel), each 3x3 tap a descriptor
-// offset; tiles are M = 128 rows of virtual pixels 126 apart (9 cover the
-// 32 x 34 outputs), the last two rows of a tile only feeding the shift
-// below. A tcgen05.mma of this shape costs about the same whatever its N
-// up to ~100 (its time goes to fetching the 4 KB A operand), so the
-// layers put as much as they can into N.
+// SM, the weights staged once), warp-specialised: warps 8 and 9 issue the
+// tcgen05.mma of alternate tiles (lane 0 of each) into a ring of 16 TMEM
+// accumulators of 32 columns; warps 0-7 read each accumulator back as soon
+// as its MMAs commit, add the bias, apply the ReLU, store BF16 into the
+// next layer's activation buffer and mark the (layer, tile) written. A tile
+// u of the next layer reads the halo rows of tiles u - 1 .. u + 1, so its
+// MMAs start once those three are written, while the epilogue of the later
+// tiles runs. Two activation buffers alternate: B holds the input and layer
+// 2's output, A layers 1 and 3. Layouts are the 32 -> 32 kernel's: a
+// 34-pixel halo pitch, channel-group major (8 channels = 16 bytes per
+// pixel), each 3x3 tap a descriptor offset, 9 M = 128 tiles of virtual
+// pixels.
+//
+// One thread issuing tcgen05.mma (M = 128, K = 16) sustains one per ~63
+// cycles whatever N up to 128; two issuing warps reach one per ~40 cycles
+// at N = 32. The shapes follow from that:
 //  - Layer 1 (2 -> 32): each pixel of B's first group holds the input pairs
 //    of (x - 1, x, x + 1) and two zeros, so a kernel row is one K = 8 core
 //    matrix; rows dy = -1 and 0 share one K = 16 MMA (leading byte offset
 //    34 pixels), dy = +1 shares one with a zero-weight half: 2 MMAs a tile.
-//  - Layers 2 and 3 (32 -> 32): the three horizontal taps in N = 96
-//    (n = 32 (dx + 1) + co), K = the three kernel rows x 32 channels: 6
-//    MMAs a tile give D[r][dx][co] = sum over dy of act[r + 34 (dy + 1)] .
-//    w[dy][dx][co], and the epilogue forms out[r] = D[r][-1] + D[r + 1][0]
-//    + D[r + 2][+1] with warp shuffles (rows across a warp boundary through
-//    shared memory).
+//  - Layers 2 and 3 (32 -> 32): 18 MMAs a tile (9 taps x 2 K halves), the
+//    taps as row offsets of the A descriptor, so the epilogue only adds the
+//    bias (putting taps into N instead makes the epilogue shift rows across
+//    lanes, which costs more than the MMAs it saves).
 //  - Layer 4 (32 -> 1): a 1 x 1 contraction with the 9 taps as N (= 16),
 //    z[h][t] = act[h] . w4[t], 2 MMAs a tile; the epilogue forms
 //    logit[o] = b4 + sum_t z[o + off_t][t] from a two-tile ring of z.
@@ -650,70 +648,56 @@ __global__ void __launch_bounds__(256, 2) lp_conv_fwd_tc_kernel(const __grid_con
 // runs and is repacked into B once layer 3's MMAs have completed (the
 // commit of layer 4's first tile implies it: MMAs complete in issue order).
 // The top k cells of the logits (first index on ties) are written per
-// image, and the logits themselves when asked. Every wait is bounded; a
-// wait that runs out sets the context's status word, the other warps leave
-// at their next wait, and the CTA drains its MMAs and copy before freeing
-// TMEM.
+// image, and the logits themselves when asked.
+//
+// Every slot's tiles come from one issuer (16 is even) and go to the one
+// epilogue group in order, and each (layer, tile) barrier completes once
+// an image, so no parity wait can run a phase ahead of its barrier. Every
+// wait is bounded; a wait that runs out sets the context's status word,
+// the other warps leave at their next wait, and the CTA drains its MMAs
+// and copy before freeing TMEM.
 namespace lpnet {
 constexpr int REGION = lptc::REGION;           // one channel group's halo plane (1224 pixels x 16 B)
 constexpr int BUF = 4 * REGION;                // 32 channels
 constexpr int OFF_A = 0;
 constexpr int OFF_B = OFF_A + BUF;
 constexpr int OFF_W1 = OFF_B + BUF;            // 4 k-groups x 32 n x 16 B: dy = -1, 0, +1, zeros
-constexpr int OFF_W2 = OFF_W1 + 4 * 32 * 16;   // 12 k-groups (dy, channel group) x 96 n (dx, co) x 16 B
+constexpr int OFF_W2 = OFF_W1 + 4 * 32 * 16;   // 36 k-groups (tap, channel group) x 32 n x 16 B
 constexpr int OFF_W3 = OFF_W2 + 36 * 32 * 16;
 constexpr int OFF_W4 = OFF_W3 + 36 * 32 * 16;  // 4 k-groups x 16 n (taps 0-8, zeros) x 16 B
 constexpr int OFF_STAGE = OFF_W4 + 4 * 16 * 16;  // the next image's input, 32 x 32 x 2 BF16
 constexpr int OFF_Z = OFF_STAGE + 4096;        // z ring, [2][9][128] FP32
 constexpr int OFF_LOG = OFF_Z + 2 * 9 * 128 * 4;  // 1024 FP32 logits
-constexpr int EPI_WARPS = 16;                  // two groups of 8: 4 TMEM lane quarters x 2 channel halves
-constexpr int EPI = EPI_WARPS * 32;
-constexpr int OFF_RED = OFF_LOG + 1024 * 4;    // per-warp maxima
-constexpr int OFF_EX = OFF_RED + EPI_WARPS * 8;  // shift exchange: [group][half][boundary][3][16] FP32
-constexpr int OFF_BAR = OFF_EX + 2 * 2 * 3 * 3 * 16 * 4;
-constexpr int STRIDE = 126;                    // tile pitch (rows 126, 127 only feed the shift)
-constexpr int TILES = 9;                       // 9 x 126 >= 32 x 34 outputs
-constexpr int NSLOT = 4;                       // TMEM accumulators: two per epilogue group
-constexpr int SLOT_COLS = 96;
-constexpr int BAR_FULL = 0;                    // [4] MMAs of a slot committed
-constexpr int BAR_EMPTY = BAR_FULL + NSLOT;    // [4] a slot read back (one arrival per warp of a group)
-constexpr int BAR_WRITTEN = BAR_EMPTY + NSLOT; // [9] a tile's activations stored (one per warp of a group)
-constexpr int BAR_INPUT = BAR_WRITTEN + 9;     // the image's input repacked (group 0's warps)
+constexpr int OFF_RED = OFF_LOG + 1024 * 4;    // 8 x u64 per-warp maxima
+constexpr int OFF_BAR = OFF_RED + 8 * 8;
+constexpr int TILES = 9;                       // ceil(32 * 34 / 128)
+constexpr int NSLOT = 16;                      // TMEM accumulators of 32 columns
+constexpr int ISSUERS = 2;
+constexpr int BAR_FULL = 0;                    // [16] MMAs of a slot committed
+constexpr int BAR_EMPTY = BAR_FULL + NSLOT;    // [16] a slot read back (8 warp arrivals)
+constexpr int BAR_WRITTEN = BAR_EMPTY + NSLOT; // [3][9] layer l's tile u stored (8 warp arrivals)
+constexpr int BAR_INPUT = BAR_WRITTEN + 3 * TILES;  // the image's input repacked (8 warp arrivals)
 constexpr int BAR_STAGE = BAR_INPUT + 1;       // the bulk copy landed
-constexpr int BAR_FIN = BAR_STAGE + 1;         // every MMA completed
-constexpr int NBAR = BAR_FIN + 1;
+constexpr int BAR_FIN = BAR_STAGE + 1;         // [2] an issuer's MMAs all completed
+constexpr int NBAR = BAR_FIN + ISSUERS;
 constexpr int OFF_TMEM = OFF_BAR + NBAR * 8;
 constexpr int OFF_ABORT = OFF_TMEM + 4;
 constexpr int SMEM = OFF_ABORT + 12;
-constexpr int THREADS = EPI + 32;              // the epilogue warps + the MMA warp
+constexpr int EPI = 256;                       // 8 epilogue warps
+constexpr int THREADS = EPI + 32 * ISSUERS;
 constexpr uint32_t TMEM_COLS = 512;
 constexpr int LIMIT = 1 << 22;
 constexpr uint32_t IDESC32 = lptc::IDESC;
 constexpr uint32_t IDESC16 = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
-constexpr uint32_t IDESC96 = (1u << 4) | (1u << 7) | (1u << 10) | ((96u >> 3) << 17) | ((128u >> 4) << 24);
 static_assert(SMEM <= 227 * 1024, "fits one CTA per SM");
-static_assert(EPI_WARPS == 16, "two groups of 8 warps; the group barriers count 256 threads");
-static_assert(NSLOT * SLOT_COLS <= (int)TMEM_COLS && TILES * STRIDE >= 32 * 34, "TMEM ring and tiling");
-static_assert((TILES - 1) * STRIDE + 127 + 70 < REGION / 16, "tile reads stay in a channel group");
 static_assert(OFF_STAGE % 128 == 0 && OFF_BAR % 8 == 0, "copy and barrier alignment");
+static_assert(NSLOT * 32 <= (int)TMEM_COLS && NSLOT % ISSUERS == 0, "TMEM ring; a slot's tiles from one issuer");
+static_assert((TILES - 1) * 128 + 127 + 70 < REGION / 16, "tile reads stay in a channel group");
 
 // A float's order as an unsigned key (finite values).
 __device__ __forceinline__ uint32_t fkey(float f) {
   const uint32_t u = __float_as_uint(f);
   return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
-
-// The accumulator of tile t (0-26: layers 1-3 by tile, 27-35: layer 4) of
-// the CTA's j-th image. Tiles of layers 1-3 alternate between the epilogue
-// groups, layer 4 is group 0's; each group has a ring of two slots it
-// consumes in order (23 tiles an image for group 0, 13 for group 1), so no
-// wait on a slot's barrier runs more than one phase ahead of it.
-__device__ __forceinline__ void slot_of(int j, int t, uint32_t& s, uint32_t& use) {
-  const int g = t < 27 ? (t & 1) : 0;
-  const uint32_t idx = t < 27 ? (uint32_t)(t >> 1) : 14u + (uint32_t)(t - 27);
-  const uint32_t k = (uint32_t)j * (g == 0 ? 23u : 13u) + idx;
-  s = (uint32_t)g * 2u + (k & 1u);
-  use = k >> 1;
 }
 
 __device__ __forceinline__ void mma(uint32_t d, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t acc) {
@@ -750,25 +734,24 @@ __device__ __forceinline__ void arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-// Named barrier `id` over one epilogue group's 256 threads; the OR of `p`
-// over them.
-__device__ __forceinline__ bool grp_or(uint32_t id, bool p) {
+// Named barrier 1 over the 256 epilogue threads; the OR of `p` over them.
+__device__ __forceinline__ bool epi_or(bool p) {
   uint32_t r;
   __syncwarp();
   asm volatile(
       "{\n\t.reg .pred q, r;\n\t"
       "setp.ne.b32 q, %1, 0;\n\t"
-      "bar.red.or.pred r, %2, 256, q;\n\t"
+      "bar.red.or.pred r, 1, 256, q;\n\t"
       "selp.b32 %0, 1, 0, r;\n\t}\n"
       : "=r"(r)
-      : "r"((uint32_t)p), "r"(id)
+      : "r"((uint32_t)p)
       : "memory");
   return r != 0;
 }
 
-__device__ __forceinline__ void grp_sync(uint32_t id) {
+__device__ __forceinline__ void epi_sync() {
   __syncwarp();
-  asm volatile("bar.sync %0, 256;" ::"r"(id) : "memory");
+  asm volatile("bar.sync 1, 256;" ::: "memory");
 }
 
 // 16 consecutive 32-bit TMEM columns of this warp's 32 lanes.
@@ -814,7 +797,7 @@ __global__ void __launch_bounds__(lpnet::THREADS, 1) lp_net_kernel(const uint16_
   }
   if (tid == 0) {
     for (int i = 0; i < NBAR; i++) {
-      const bool one = (i >= BAR_FULL && i < BAR_FULL + NSLOT) || i == BAR_STAGE || i == BAR_FIN;
+      const bool one = (i >= BAR_FULL && i < BAR_FULL + NSLOT) || i == BAR_STAGE || i >= BAR_FIN;
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar(i)), "r"(one ? 1 : 8));
     }
     *abort_w = 0;
@@ -833,12 +816,11 @@ __global__ void __launch_bounds__(lpnet::THREADS, 1) lp_net_kernel(const uint16_
   }
   uint16_t* w2s = reinterpret_cast<uint16_t*>(sm_ + OFF_W2);
   uint16_t* w3s = reinterpret_cast<uint16_t*>(sm_ + OFF_W3);
-  for (int q = tid; q < 12 * 96 * 8; q += THREADS) {
-    // k-group kg = 4 (dy + 1) + channel group, n = 32 (dx + 1) + co.
-    const int e = q & 7, nn = (q >> 3) % 96, kg = q / 768;
-    const int src = (nn & 31) * 288 + ((kg >> 2) * 3 + (nn >> 5)) * 32 + (kg & 3) * 8 + e;
-    w2s[q] = W2[src];
-    w3s[q] = W3[src];
+  for (int q = tid; q < 36 * 32 * 8; q += THREADS) {
+    // k-group kg = 4 tap + channel group.
+    const int e = q & 7, nn = (q >> 3) & 31, kg = q >> 8;
+    w2s[q] = W2[nn * 288 + kg * 8 + e];
+    w3s[q] = W3[nn * 288 + kg * 8 + e];
   }
   uint16_t* w4s = reinterpret_cast<uint16_t*>(sm_ + OFF_W4);
   for (int q = tid; q < 4 * 16 * 8; q += THREADS) {
@@ -853,103 +835,97 @@ __global__ void __launch_bounds__(lpnet::THREADS, 1) lp_net_kernel(const uint16_
   const uint32_t tmem = *tmem_slot;
   const int first = blockIdx.x, stride = gridDim.x;
 
-  if (warp == EPI_WARPS) {
-    // ---- the MMA warp: lane 0 issues, the whole warp waits.
+  if (warp >= EPI / 32) {
+    // ---- the MMA warps: issuer i takes the tiles t = i, i + 2, ... of the
+    // 36 an image (layers 1-4 x 9); lane 0 issues, the whole warp waits.
+    const int iss = warp - EPI / 32;
     bool ok = true;
-    int copies = 1;    // bulk copies issued
-    if (lane == 0) fetch_input(stage_a, X + (size_t)first * 2048, bar(BAR_STAGE));
+    int copies = 0;  // bulk copies issued (issuer 0)
+    if (iss == 0) {
+      if (lane == 0) fetch_input(stage_a, X + (size_t)first * 2048, bar(BAR_STAGE));
+      copies = 1;
+    }
     int j = 0;
     for (int img = first; img < n && ok; img += stride, j++) {
       ok = __all_sync(0xffffffffu, wait(bar(BAR_INPUT), (uint32_t)j & 1u, abort_w));
       if (!ok) break;
       // The stage is free again (its contents repacked): the next image's copy.
-      if (img + stride < n) {
+      if (iss == 0 && img + stride < n) {
         if (lane == 0) fetch_input(stage_a, X + (size_t)(img + stride) * 2048, bar(BAR_STAGE));
         copies++;
       }
-      for (int layer = 0; layer < 4 && ok; layer++) {
-        for (int u = 0; u < TILES; u++) {
-          bool w_ok = true;
-          if (layer > 0) {
-            // The previous layer's tiles u - 1 .. u + 1 stored (tile u - 1
-            // and u were awaited for the tiles before).
-            const uint32_t par = (uint32_t)(3 * j + layer - 1) & 1u;
-            if (u == 0) w_ok = wait(bar(BAR_WRITTEN + 0), par, abort_w) && wait(bar(BAR_WRITTEN + 1), par, abort_w);
-            else if (u + 1 < TILES) w_ok = wait(bar(BAR_WRITTEN + u + 1), par, abort_w);
-          }
-          uint32_t s, use;
-          slot_of(j, layer * TILES + u, s, use);
-          if (w_ok && use > 0) w_ok = wait(bar(BAR_EMPTY + (int)s), (use - 1) & 1u, abort_w);
-          ok = __all_sync(0xffffffffu, w_ok);
-          if (!ok) break;
-          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-          if (lane == 0) {
-            const uint32_t d = tmem + s * SLOT_COLS;
-            const uint32_t v0 = (uint32_t)(u * STRIDE);
-            if (layer == 0) {
-              // Rows dy = -1 and 0 (34 pixels apart), then dy = +1 with a
-              // zero-weight half one pixel on.
-              mma(d, lptc::smem_desc(b_a + (v0 + 1) * 16, 34 * 16, 128), lptc::smem_desc(w1_a, 512, 128), IDESC32,
-                  0u);
-              mma(d, lptc::smem_desc(b_a + (v0 + 69) * 16, 16, 128), lptc::smem_desc(w1_a + 2 * 512, 512, 128),
-                  IDESC32, 1u);
-            } else if (layer < 3) {
-              const uint32_t src = layer == 1 ? a_a : b_a, w_a = layer == 1 ? w2_a : w3_a;
-#pragma unroll
-              for (int q = 0; q < 6; q++) {
-                const int dyi = q >> 1, hh = q & 1;
-                mma(d, lptc::smem_desc(src + (uint32_t)(2 * hh * REGION) + (v0 + dyi * 34) * 16, REGION, 128),
-                    lptc::smem_desc(w_a + (uint32_t)((dyi * 4 + 2 * hh) * 1536), 1536, 128), IDESC96,
-                    q > 0 ? 1u : 0u);
-              }
-            } else {
-              // Layer 4 over A: z for the tile's 128 halo pixels.
-              mma(d, lptc::smem_desc(a_a + v0 * 16, REGION, 128), lptc::smem_desc(w4_a, 256, 128), IDESC16, 0u);
-              mma(d, lptc::smem_desc(a_a + 2 * REGION + v0 * 16, REGION, 128), lptc::smem_desc(w4_a + 512, 256, 128),
-                  IDESC16, 1u);
-            }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             bar(BAR_FULL + (int)s))
-                         : "memory");
-          }
-          __syncwarp();
+      for (int t = iss; t < 4 * TILES; t += ISSUERS) {
+        const int layer = t / TILES, u = t % TILES;
+        bool w_ok = true;
+        if (layer > 0) {
+          // The previous layer's tiles u - 1 .. u + 1 stored.
+          for (int w = u - 1; w <= u + 1 && w_ok; w++)
+            if (w >= 0 && w < TILES) w_ok = wait(bar(BAR_WRITTEN + (layer - 1) * TILES + w), (uint32_t)j & 1u, abort_w);
         }
+        const uint32_t seq = (uint32_t)j * (4u * TILES) + (uint32_t)t, s = seq % NSLOT, use = seq / NSLOT;
+        if (w_ok && use > 0) w_ok = wait(bar(BAR_EMPTY + (int)s), (use - 1) & 1u, abort_w);
+        ok = __all_sync(0xffffffffu, w_ok);
+        if (!ok) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (lane == 0) {
+          const uint32_t d = tmem + s * 32;
+          const uint32_t v0 = (uint32_t)u * 128;
+          if (layer == 0) {
+            // Rows dy = -1 and 0 (34 pixels apart), then dy = +1 with a
+            // zero-weight half one pixel on.
+            mma(d, lptc::smem_desc(b_a + (v0 + 1) * 16, 34 * 16, 128), lptc::smem_desc(w1_a, 512, 128), IDESC32, 0u);
+            mma(d, lptc::smem_desc(b_a + (v0 + 69) * 16, 16, 128), lptc::smem_desc(w1_a + 2 * 512, 512, 128), IDESC32,
+                1u);
+          } else if (layer < 3) {
+            const uint32_t src = layer == 1 ? a_a : b_a, w_a = layer == 1 ? w2_a : w3_a;
+#pragma unroll
+            for (int ks = 0; ks < 18; ks++) {
+              const int tap = ks >> 1, hh = ks & 1, off = (tap / 3) * 34 + tap % 3;
+              mma(d, lptc::smem_desc(src + (uint32_t)(2 * hh * REGION) + (v0 + off) * 16, REGION, 128),
+                  lptc::smem_desc(w_a + (uint32_t)((tap * 4 + 2 * hh) * 512), 512, 128), IDESC32, ks > 0 ? 1u : 0u);
+            }
+          } else {
+            // Layer 4 over A: z for the tile's 128 halo pixels.
+            mma(d, lptc::smem_desc(a_a + v0 * 16, REGION, 128), lptc::smem_desc(w4_a, 256, 128), IDESC16, 0u);
+            mma(d, lptc::smem_desc(a_a + 2 * REGION + v0 * 16, REGION, 128), lptc::smem_desc(w4_a + 512, 256, 128),
+                IDESC16, 1u);
+          }
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                           bar(BAR_FULL + (int)s))
+                       : "memory");
+        }
+        __syncwarp();
       }
     }
     if (!ok && lane == 0) {
       atomicExch(status, 1u);  // DEV_TIMEOUT
       *abort_w = 1;
     }
-    // Drain: every MMA issued, and the last bulk copy, complete before the
-    // CTA frees TMEM and leaves.
+    // Drain: every MMA this warp issued, and the last bulk copy, complete
+    // before the CTA frees TMEM and leaves.
     if (lane == 0)
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar(BAR_FIN))
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       bar(BAR_FIN + iss))
                    : "memory");
     __syncwarp();
-    mbar_wait(bar(BAR_FIN), 0, LIMIT);
-    mbar_wait(bar(BAR_STAGE), (uint32_t)(copies - 1) & 1u, LIMIT);
+    mbar_wait(bar(BAR_FIN + iss), 0, LIMIT);
+    if (iss == 0) mbar_wait(bar(BAR_STAGE), (uint32_t)(copies - 1) & 1u, LIMIT);
     __syncwarp();
   } else {
-    // ---- the epilogue warps: two groups of 8 take alternate tiles of
-    // layers 1-3, so two tiles are read back at once; group 0 also runs
-    // layer 4, the logits and the top k while group 1 goes on to the next
-    // image. In a group, warp w reads TMEM lanes 32 (w % 4) .. +31 and
-    // channels 16 (w / 4) .. +15 of each accumulator.
-    const int grp = warp >> 3, gw = warp & 7, lq = gw & 3, half = gw >> 2;
-    const int gtid = tid & 255;
-    const uint32_t gbar = 1u + (uint32_t)grp;
+    // ---- the epilogue warps: warp w reads TMEM lanes 32 (w % 4) .. +31,
+    // columns 16 (w / 4) .. +15 of each accumulator.
+    const int lq = warp & 3, half = warp >> 2;
     float* z = reinterpret_cast<float*>(sm_ + OFF_Z);
     float* log_s = reinterpret_cast<float*>(sm_ + OFF_LOG);
     unsigned long long* red = reinterpret_cast<unsigned long long*>(sm_ + OFF_RED);
-    float* ex = reinterpret_cast<float*>(sm_ + OFF_EX) + (grp * 2 + half) * 144;
     const float bias4 = __ldg(b4);
     bool ok = true;
-    // One image's input from the stage into B's first group (group 0):
-    // pixel (y, x) holds the pairs of (x - 1, x, x + 1) (zero outside the
-    // image) and two zeros; then the hand-over to the MMA warp.
+    // One image's input from the stage into B's first group: pixel (y, x)
+    // holds the pairs of (x - 1, x, x + 1) (zero outside the image) and two
+    // zeros; then the hand-over to the MMA warps.
     auto repack = [&]() {
       const uint32_t* st = reinterpret_cast<const uint32_t*>(sm_ + OFF_STAGE);
-      for (int p = gtid; p < 1024; p += 256) {
+      for (int p = tid; p < 1024; p += EPI) {
         const int y = p >> 5, x = p & 31;
         const uint32_t l = x > 0 ? st[p - 1] : 0u, c = st[p], r = x < 31 ? st[p + 1] : 0u;
         *reinterpret_cast<uint4*>(sm_ + OFF_B + ((y + 1) * 34 + x + 1) * 16) = make_uint4(l, c, r, 0u);
@@ -961,126 +937,68 @@ __global__ void __launch_bounds__(lpnet::THREADS, 1) lp_net_kernel(const uint16_
     // The logits of output tile t from the z ring (slots t & 1 and
     // (t + 1) & 1; halo rows past the last tile are zero).
     auto outputs = [&](int t) {
-      if (gtid < STRIDE) {
-        const int o = t * STRIDE + gtid, y = o / 34, x = o % 34;
+      if (tid < 128) {
+        const int o = t * 128 + tid, y = o / 34, x = o % 34;
         if (y < 32 && x < 32) {
           float acc = 0.f;
 #pragma unroll
           for (int tap = 0; tap < 9; tap++) {
-            const int h = o + (tap / 3) * 34 + tap % 3, th = h / STRIDE;
-            acc += th < TILES ? z[(th & 1) * 1152 + tap * 128 + (h - th * STRIDE)] : 0.f;
+            const int h = o + (tap / 3) * 34 + tap % 3, th = h >> 7;
+            acc += th < TILES ? z[(th & 1) * 1152 + tap * 128 + (h & 127)] : 0.f;
           }
           log_s[y * 32 + x] = acc + bias4;
         }
       }
     };
-    if (grp == 0) {
-      ok = !grp_or(gbar, !wait(bar(BAR_STAGE), 0u, abort_w));
-      if (ok) repack();
-    }
+    ok = !epi_or(!wait(bar(BAR_STAGE), 0u, abort_w));
+    if (ok) repack();
     int j = 0;
     for (int img = first; img < n && ok; img += stride, j++) {
-      int bias_layer = -1;
-      float bb[16];
-      for (int t = grp; t < 3 * TILES && ok; t += 2) {
-        const int layer = t / TILES, u = t % TILES;
-        if (layer != bias_layer) {
-          const float* bias = (layer == 0 ? b1 : layer == 1 ? b2 : b3) + half * 16;
+      for (int layer = 0; layer < 3 && ok; layer++) {
+        const uint32_t dst = layer == 1 ? OFF_B : OFF_A;
+        const float* bias = layer == 0 ? b1 : layer == 1 ? b2 : b3;
+        float bb[16];
 #pragma unroll
-          for (int q = 0; q < 16; q++) bb[q] = __ldg(bias + q);
-          bias_layer = layer;
-        }
-        uint32_t s, use;
-        slot_of(j, t, s, use);
-        ok = !grp_or(gbar, !wait(bar(BAR_FULL + (int)s), use & 1u, abort_w));
-        if (!ok) break;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t ta = tmem + ((uint32_t)(32 * lq) << 16) + s * SLOT_COLS + (uint32_t)(half * 16);
-        float acc[16];
-        if (layer == 0) {
+        for (int q = 0; q < 16; q++) bb[q] = __ldg(bias + half * 16 + q);
+        for (int u = 0; u < TILES; u++) {
+          const uint32_t seq = (uint32_t)j * (4u * TILES) + (uint32_t)(layer * TILES + u);
+          const uint32_t s = seq % NSLOT, use = seq / NSLOT;
+          ok = !epi_or(!wait(bar(BAR_FULL + (int)s), use & 1u, abort_w));
+          if (!ok) break;
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           uint32_t r[16];
-          tmem_ld16(ta, r);
+          tmem_ld16(tmem + ((uint32_t)(32 * lq) << 16) + s * 32 + (uint32_t)(half * 16), r);
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
           asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
           __syncwarp();
           if (lane == 0) arrive(bar(BAR_EMPTY + (int)s));
+          const int v = u * 128 + 32 * lq + lane, y = v / 34, x = v % 34;
+          if (y < 32 && x < 32) {
+            uint32_t o[8];
 #pragma unroll
-          for (int q = 0; q < 16; q++) acc[q] = __uint_as_float(r[q]);
-        } else {
-          // D[r][dx] for dx = -1, 0, +1; out[r] = D[r][-1] + D[r + 1][0] +
-          // D[r + 2][+1]. The next warp's rows 0 and 1 reach lanes 30 and
-          // 31 through the exchange (the tile's last warp has no outputs
-          // there: rows 126 and 127 are the next tile's 0 and 1). The
-          // shuffles come first, all independent (a lane branch between
-          // them would make the warp reconverge at each one), then one
-          // barrier and the two edge lanes' fix-up.
-          uint32_t dm[16], d0[16], dp[16];
-          tmem_ld16(ta, dm);
-          tmem_ld16(ta + 32, d0);
-          tmem_ld16(ta + 64, dp);
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            for (int q = 0; q < 8; q++)
+              o[q] = pack_bf16(fmaxf(__uint_as_float(r[2 * q]) + bb[2 * q], 0.f),
+                               fmaxf(__uint_as_float(r[2 * q + 1]) + bb[2 * q + 1], 0.f));
+            uint8_t* px = sm_ + dst + ((y + 1) * 34 + x + 1) * 16;
+            *reinterpret_cast<uint4*>(px + (2 * half) * REGION) = make_uint4(o[0], o[1], o[2], o[3]);
+            *reinterpret_cast<uint4*>(px + (2 * half + 1) * REGION) = make_uint4(o[4], o[5], o[6], o[7]);
+          }
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
           __syncwarp();
-          if (lane == 0) arrive(bar(BAR_EMPTY + (int)s));
-          if (lq > 0 && lane == 0) {
-            float* e_ = ex + (lq - 1) * 48;
-#pragma unroll
-            for (int q = 0; q < 16; q++) {
-              e_[q] = __uint_as_float(d0[q]);
-              e_[16 + q] = __uint_as_float(dp[q]);
-            }
-          } else if (lq > 0 && lane == 1) {
-            float* e_ = ex + (lq - 1) * 48;
-#pragma unroll
-            for (int q = 0; q < 16; q++) e_[32 + q] = __uint_as_float(dp[q]);
-          }
-          float s1[16], s2[16];
-#pragma unroll
-          for (int q = 0; q < 16; q++) {
-            s1[q] = __shfl_down_sync(0xffffffffu, __uint_as_float(d0[q]), 1);
-            s2[q] = __shfl_down_sync(0xffffffffu, __uint_as_float(dp[q]), 2);
-          }
-          grp_sync(gbar);
-          if (lq < 3 && lane == 31) {
-            const float* e_ = ex + lq * 48;
-#pragma unroll
-            for (int q = 0; q < 16; q++) {
-              s1[q] = e_[q];
-              s2[q] = e_[32 + q];
-            }
-          } else if (lq < 3 && lane == 30) {
-            const float* e_ = ex + lq * 48;
-#pragma unroll
-            for (int q = 0; q < 16; q++) s2[q] = e_[16 + q];
-          }
-#pragma unroll
-          for (int q = 0; q < 16; q++) acc[q] = __uint_as_float(dm[q]) + s1[q] + s2[q];
+          if (lane == 0) arrive(bar(BAR_WRITTEN + layer * TILES + u));
         }
-        const int m = 32 * lq + lane, v = u * STRIDE + m, y = v / 34, x = v % 34;
-        if (m < STRIDE && y < 32 && x < 32) {
-          uint32_t o[8];
-#pragma unroll
-          for (int q = 0; q < 8; q++)
-            o[q] = pack_bf16(fmaxf(acc[2 * q] + bb[2 * q], 0.f), fmaxf(acc[2 * q + 1] + bb[2 * q + 1], 0.f));
-          uint8_t* px = sm_ + (layer == 1 ? OFF_B : OFF_A) + ((y + 1) * 34 + x + 1) * 16;
-          *reinterpret_cast<uint4*>(px + (2 * half) * REGION) = make_uint4(o[0], o[1], o[2], o[3]);
-          *reinterpret_cast<uint4*>(px + (2 * half + 1) * REGION) = make_uint4(o[4], o[5], o[6], o[7]);
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncwarp();
-        if (lane == 0) arrive(bar(BAR_WRITTEN + u));
       }
-      if (!ok || grp != 0) continue;
-      // Layer 4 (group 0): z into the ring, the logits one tile behind.
+      if (!ok) break;
+      // Layer 4: z into the ring, the logits one tile behind.
       for (int u = 0; u < TILES; u++) {
-        uint32_t s, use;
-        slot_of(j, 3 * TILES + u, s, use);
-        ok = !grp_or(gbar, !wait(bar(BAR_FULL + (int)s), use & 1u, abort_w));
+        const uint32_t seq = (uint32_t)j * (4u * TILES) + (uint32_t)(3 * TILES + u);
+        const uint32_t s = seq % NSLOT, use = seq / NSLOT;
+        ok = !epi_or(!wait(bar(BAR_FULL + (int)s), use & 1u, abort_w));
         if (!ok) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         if (half == 0) {
           uint32_t r[16];
-          tmem_ld16(tmem + ((uint32_t)(32 * lq) << 16) + s * SLOT_COLS, r);
+          tmem_ld16(tmem + ((uint32_t)(32 * lq) << 16) + s * 32, r);
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
           float* zs = z + (u & 1) * 1152 + 32 * lq + lane;
 #pragma unroll
@@ -1091,24 +1009,24 @@ __global__ void __launch_bounds__(lpnet::THREADS, 1) lp_net_kernel(const uint16_
         if (lane == 0) arrive(bar(BAR_EMPTY + (int)s));
         if (u == 0 && img + stride < n) {
           // Layer 3's MMAs have completed: B's first group takes the next input.
-          ok = !grp_or(gbar, !wait(bar(BAR_STAGE), (uint32_t)(j + 1) & 1u, abort_w));
+          ok = !epi_or(!wait(bar(BAR_STAGE), (uint32_t)(j + 1) & 1u, abort_w));
           if (!ok) break;
           repack();
         }
-        grp_sync(gbar);  // z of tile u in place
+        epi_sync();  // z of tile u in place
         if (u > 0) outputs(u - 1);
-        grp_sync(gbar);  // tile u - 1's slot free for tile u + 1
+        epi_sync();  // tile u - 1's slot free for tile u + 1
       }
       if (!ok) break;
       outputs(TILES - 1);
-      grp_sync(gbar);
+      epi_sync();
       if (logits)
-        for (int q = gtid; q < 1024; q += 256) logits[(size_t)img * 1024 + q] = log_s[q];
-      grp_sync(gbar);
+        for (int q = tid; q < 1024; q += EPI) logits[(size_t)img * 1024 + q] = log_s[q];
+      epi_sync();
       // The top k cells, best first, the first index among equal scores.
       for (int round = 0; round < k; round++) {
         unsigned long long best = 0;
-        for (int q = gtid; q < 1024; q += 256) {
+        for (int q = tid; q < 1024; q += EPI) {
           const unsigned long long key = ((unsigned long long)fkey(log_s[q]) << 32) | (uint32_t)(1023 - q);
           best = key > best ? key : best;
         }
@@ -1117,19 +1035,19 @@ __global__ void __launch_bounds__(lpnet::THREADS, 1) lp_net_kernel(const uint16_
           const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
           best = other > best ? other : best;
         }
-        if (lane == 0) red[gw] = best;
-        grp_sync(gbar);
-        if (gtid == 0) {
+        if (lane == 0) red[warp] = best;
+        epi_sync();
+        if (tid == 0) {
           unsigned long long b = red[0];
           for (int w = 1; w < 8; w++) b = red[w] > b ? red[w] : b;
           const int cell = 1023 - (int)(b & 0x3ffu);
           cells[(size_t)img * k + round] = cell;
           log_s[cell] = -INFINITY;
         }
-        grp_sync(gbar);
+        epi_sync();
       }
     }
-    if (!ok && gtid == 0) {
+    if (!ok && tid == 0) {
       atomicExch(status, 1u);  // DEV_TIMEOUT
       *abort_w = 1;
     }
