@@ -617,9 +617,9 @@ __global__ void __launch_bounds__(256, 2) lp_conv_fwd_tc_kernel(const __grid_con
 
 // ------------------------------------------ fused net inference (tcgen05)
 // The whole proposal net, one image at a time per persistent CTA (one per
-// SM, the weights staged once), warp-specialised: warps 8 and 9 issue the
-// tcgen05.mma of alternate tiles (lane 0 of each) into a ring of 16 TMEM
-// accumulators of 32 columns; warps 0-7 read each accumulator back as soon
+// SM, the weights staged once), warp-specialised: the MMA warps (8 on)
+// issue the tcgen05.mma of the tiles in turn (lane 0 of each) into a ring
+// of 16 TMEM accumulators of 32 columns; warps 0-7 read each one back as soon
 // as its MMAs commit, add the bias, apply the ReLU, store BF16 into the
 // next layer's activation buffer and mark the (layer, tile) written. A tile
 // u of the next layer reads the halo rows of tiles u - 1 .. u + 1, so its
@@ -631,8 +631,11 @@ __global__ void __launch_bounds__(256, 2) lp_conv_fwd_tc_kernel(const __grid_con
 // pixels.
 //
 // One thread issuing tcgen05.mma (M = 128, K = 16) sustains one per ~63
-// cycles whatever N up to 128; two issuing warps reach one per ~40 cycles
-// at N = 32. The shapes follow from that:
+// cycles whatever N up to 128, and between a tile's commit and its next
+// tile it waits on the queue for several hundred more; the operands stream
+// from shared memory at ~128 B per cycle (4 KB of A and 1 KB of B at N =
+// 32: ~40 cycles an MMA). Several issuing warps keep the tensor pipe fed.
+// The shapes follow from that:
 //  - Layer 1 (2 -> 32): each pixel of B's first group holds the input pairs
 //    of (x - 1, x, x + 1) and two zeros, so a kernel row is one K = 8 core
 //    matrix; rows dy = -1 and 0 share one K = 16 MMA (leading byte offset
@@ -642,15 +645,20 @@ __global__ void __launch_bounds__(256, 2) lp_conv_fwd_tc_kernel(const __grid_con
 //    bias (putting taps into N instead makes the epilogue shift rows across
 //    lanes, which costs more than the MMAs it saves).
 //  - Layer 4 (32 -> 1): a 1 x 1 contraction with the 9 taps as N (= 16),
-//    z[h][t] = act[h] . w4[t], 2 MMAs a tile; the epilogue forms
-//    logit[o] = b4 + sum_t z[o + off_t][t] from a two-tile ring of z.
+//    z[h][t] = act[h] . w4[t], 2 MMAs a tile, stored into B's channel
+//    groups 1-3 (free once layer 3's MMAs are done; their halo rings and
+//    tails are zeroed again after); after the last tile the epilogue forms
+//    logit[o] = b4 + sum_t z[o + off_t][t] in one pass.
 // The next image's 4 KB input arrives by one bulk copy while this image
-// runs and is repacked into B once layer 3's MMAs have completed (the
-// commit of layer 4's first tile implies it: MMAs complete in issue order).
-// The top k cells of the logits (first index on ties) are written per
-// image, and the logits themselves when asked.
+// runs and is repacked into B's first group at layer 4's first tile. The
+// one epilogue group consumes the tiles in order, waiting on each commit,
+// so whenever it writes a buffer every MMA issued before that reads it has
+// completed, whichever warp issued it. The top k cells of the logits
+// (first index on ties) are written per image, and the logits themselves
+// when asked.
 //
-// Every slot's tiles come from one issuer (16 is even) and go to the one
+// Every slot's tiles come from one issuer (16 is a multiple of the issuer
+// count) and go to the one
 // epilogue group in order, and each (layer, tile) barrier completes once
 // an image, so no parity wait can run a phase ahead of its barrier. Every
 // wait is bounded; a wait that runs out sets the context's status word,
@@ -666,19 +674,19 @@ constexpr int OFF_W2 = OFF_W1 + 4 * 32 * 16;   // 36 k-groups (tap, channel grou
 constexpr int OFF_W3 = OFF_W2 + 36 * 32 * 16;
 constexpr int OFF_W4 = OFF_W3 + 36 * 32 * 16;  // 4 k-groups x 16 n (taps 0-8, zeros) x 16 B
 constexpr int OFF_STAGE = OFF_W4 + 4 * 16 * 16;  // the next image's input, 32 x 32 x 2 BF16
-constexpr int OFF_Z = OFF_STAGE + 4096;        // z ring, [2][9][128] FP32
-constexpr int OFF_LOG = OFF_Z + 2 * 9 * 128 * 4;  // 1024 FP32 logits
-constexpr int OFF_RED = OFF_LOG + 1024 * 4;    // 8 x u64 per-warp maxima
-constexpr int OFF_BAR = OFF_RED + 8 * 8;
+constexpr int OFF_Z = OFF_B + REGION;          // layer 4's z, [9 taps][1152 rows] FP32, in B's groups 1-3
+constexpr int OFF_LOG = OFF_STAGE + 4096;      // 1024 FP32 logits
+constexpr int OFF_RED = OFF_LOG + 1024 * 4;    // 2 x 8 u64 per-warp maxima (by round parity)
+constexpr int OFF_BAR = OFF_RED + 2 * 8 * 8;
 constexpr int TILES = 9;                       // ceil(32 * 34 / 128)
 constexpr int NSLOT = 16;                      // TMEM accumulators of 32 columns
-constexpr int ISSUERS = 2;
+constexpr int ISSUERS = 4;
 constexpr int BAR_FULL = 0;                    // [16] MMAs of a slot committed
 constexpr int BAR_EMPTY = BAR_FULL + NSLOT;    // [16] a slot read back (8 warp arrivals)
 constexpr int BAR_WRITTEN = BAR_EMPTY + NSLOT; // [3][9] layer l's tile u stored (8 warp arrivals)
 constexpr int BAR_INPUT = BAR_WRITTEN + 3 * TILES;  // the image's input repacked (8 warp arrivals)
 constexpr int BAR_STAGE = BAR_INPUT + 1;       // the bulk copy landed
-constexpr int BAR_FIN = BAR_STAGE + 1;         // [2] an issuer's MMAs all completed
+constexpr int BAR_FIN = BAR_STAGE + 1;         // [4] an issuer's MMAs all completed
 constexpr int NBAR = BAR_FIN + ISSUERS;
 constexpr int OFF_TMEM = OFF_BAR + NBAR * 8;
 constexpr int OFF_ABORT = OFF_TMEM + 4;
@@ -693,6 +701,7 @@ static_assert(SMEM <= 227 * 1024, "fits one CTA per SM");
 static_assert(OFF_STAGE % 128 == 0 && OFF_BAR % 8 == 0, "copy and barrier alignment");
 static_assert(NSLOT * 32 <= (int)TMEM_COLS && NSLOT % ISSUERS == 0, "TMEM ring; a slot's tiles from one issuer");
 static_assert((TILES - 1) * 128 + 127 + 70 < REGION / 16, "tile reads stay in a channel group");
+static_assert(9 * TILES * 128 * 4 <= 3 * REGION, "z fits B's groups 1-3");
 
 // A float's order as an unsigned key (finite values).
 __device__ __forceinline__ uint32_t fkey(float f) {
@@ -934,17 +943,16 @@ __global__ void __launch_bounds__(lpnet::THREADS, 1) lp_net_kernel(const uint16_
       __syncwarp();
       if (lane == 0) arrive(bar(BAR_INPUT));
     };
-    // The logits of output tile t from the z ring (slots t & 1 and
-    // (t + 1) & 1; halo rows past the last tile are zero).
-    auto outputs = [&](int t) {
-      if (tid < 128) {
-        const int o = t * 128 + tid, y = o / 34, x = o % 34;
-        if (y < 32 && x < 32) {
+    // The logits from z (halo rows past the last tile are zero).
+    auto outputs = [&]() {
+      for (int o = tid; o < 32 * 34; o += EPI) {
+        const int y = o / 34, x = o % 34;
+        if (x < 32) {
           float acc = 0.f;
 #pragma unroll
           for (int tap = 0; tap < 9; tap++) {
-            const int h = o + (tap / 3) * 34 + tap % 3, th = h >> 7;
-            acc += th < TILES ? z[(th & 1) * 1152 + tap * 128 + (h & 127)] : 0.f;
+            const int h = o + (tap / 3) * 34 + tap % 3;
+            acc += h < TILES * 128 ? z[tap * (TILES * 128) + h] : 0.f;
           }
           log_s[y * 32 + x] = acc + bias4;
         }
@@ -989,7 +997,7 @@ __global__ void __launch_bounds__(lpnet::THREADS, 1) lp_net_kernel(const uint16_
         }
       }
       if (!ok) break;
-      // Layer 4: z into the ring, the logits one tile behind.
+      // Layer 4: z into B's groups 1-3, then the logits in one pass.
       for (int u = 0; u < TILES; u++) {
         const uint32_t seq = (uint32_t)j * (4u * TILES) + (uint32_t)(3 * TILES + u);
         const uint32_t s = seq % NSLOT, use = seq / NSLOT;
@@ -1000,34 +1008,50 @@ __global__ void __launch_bounds__(lpnet::THREADS, 1) lp_net_kernel(const uint16_
           uint32_t r[16];
           tmem_ld16(tmem + ((uint32_t)(32 * lq) << 16) + s * 32, r);
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-          float* zs = z + (u & 1) * 1152 + 32 * lq + lane;
+          float* zs = z + u * 128 + 32 * lq + lane;
 #pragma unroll
-          for (int t = 0; t < 9; t++) zs[t * 128] = __uint_as_float(r[t]);
+          for (int t = 0; t < 9; t++) zs[t * (TILES * 128)] = __uint_as_float(r[t]);
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncwarp();
         if (lane == 0) arrive(bar(BAR_EMPTY + (int)s));
         if (u == 0 && img + stride < n) {
-          // Layer 3's MMAs have completed: B's first group takes the next input.
+          // Every layer-3 tile's MMAs are done: B's first group takes the next input.
           ok = !epi_or(!wait(bar(BAR_STAGE), (uint32_t)(j + 1) & 1u, abort_w));
           if (!ok) break;
           repack();
         }
-        epi_sync();  // z of tile u in place
-        if (u > 0) outputs(u - 1);
-        epi_sync();  // tile u - 1's slot free for tile u + 1
       }
       if (!ok) break;
-      outputs(TILES - 1);
-      epi_sync();
+      epi_sync();  // z complete
+      outputs();
+      epi_sync();  // z read: B's groups 1-3 get their zero halo rings and tails back
+      for (int q = tid; q < 3 * (34 * 34 - 32 * 32 + lptc::NV - 34 * 34); q += EPI) {
+        const int g = 1 + q / (lptc::NV - 32 * 32), r = q % (lptc::NV - 32 * 32);
+        // r-th non-interior pixel of the group: the ring (34 x 34 minus the
+        // 32 x 32 interior), then the tail past 34 x 34.
+        int h;
+        if (r < 34) h = r;                                    // top row
+        else if (r < 68) h = 33 * 34 + (r - 34);              // bottom row
+        else if (r < 68 + 64) { const int rr = r - 68; h = (1 + (rr >> 1)) * 34 + ((rr & 1) ? 33 : 0); }
+        else h = 34 * 34 + (r - 132);                          // tail
+        *reinterpret_cast<uint4*>(sm_ + OFF_B + g * REGION + h * 16) = make_uint4(0, 0, 0, 0);
+      }
       if (logits)
         for (int q = tid; q < 1024; q += EPI) logits[(size_t)img * 1024 + q] = log_s[q];
-      epi_sync();
-      // The top k cells, best first, the first index among equal scores.
+      // The top k cells, best first, the first index among equal scores:
+      // each thread keeps its four scores in registers; a round publishes
+      // the warp maxima (one barrier, the array alternating by round),
+      // every thread reduces them alike and the owner drops the chosen cell.
+      float mine[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) mine[i] = log_s[tid + EPI * i];
       for (int round = 0; round < k; round++) {
         unsigned long long best = 0;
-        for (int q = tid; q < 1024; q += EPI) {
-          const unsigned long long key = ((unsigned long long)fkey(log_s[q]) << 32) | (uint32_t)(1023 - q);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          const unsigned long long key =
+              ((unsigned long long)fkey(mine[i]) << 32) | (uint32_t)(1023 - (tid + EPI * i));
           best = key > best ? key : best;
         }
 #pragma unroll
@@ -1035,16 +1059,17 @@ __global__ void __launch_bounds__(lpnet::THREADS, 1) lp_net_kernel(const uint16_
           const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
           best = other > best ? other : best;
         }
-        if (lane == 0) red[warp] = best;
+        unsigned long long* rr = red + (round & 1) * 8;
+        if (lane == 0) rr[warp] = best;
         epi_sync();
-        if (tid == 0) {
-          unsigned long long b = red[0];
-          for (int w = 1; w < 8; w++) b = red[w] > b ? red[w] : b;
-          const int cell = 1023 - (int)(b & 0x3ffu);
-          cells[(size_t)img * k + round] = cell;
-          log_s[cell] = -INFINITY;
-        }
-        epi_sync();
+        unsigned long long b = rr[0];
+#pragma unroll
+        for (int w = 1; w < 8; w++) b = rr[w] > b ? rr[w] : b;
+        const int cell = 1023 - (int)(b & 0x3ffu);
+        if (tid == 0) cells[(size_t)img * k + round] = cell;
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+          if (cell == tid + EPI * i) mine[i] = -INFINITY;
       }
     }
     if (!ok && tid == 0) {
