@@ -731,7 +731,8 @@ vp8a_status vp8a_select_filter_params_batch(vp8a_ctx* ctx, const vp8a_sweep_job*
  * (column, row); out = [n][32][32][2] BF16: (32 - the mean absolute
  * difference of the 2x2-averaged MB and reference block at the cell's
  * vector) / 32, and (the averaged reference at the block's centre - 128) /
- * 64. `src` and `ref` are visible luma planes of one size. */
+ * 64. `src` and `ref` are visible luma planes of one size; `out` is
+ * 16-byte aligned. */
 vp8a_status vp8a_lp_windows(vp8a_ctx* ctx, const vp8a_luma_ref* src, const vp8a_luma_ref* ref,
                             const uint32_t* mb_xy, uint32_t n, uint16_t* out);
 

@@ -66,8 +66,10 @@ __device__ __forceinline__ uint16_t act(const uint16_t* X, int C, int img, int y
 __global__ void __launch_bounds__(256) lp_windows_kernel(const uint8_t* src, uint64_t ss, const uint8_t* ref,
                                                          uint64_t rs, int w, int h, const uint32_t* xy, int n,
                                                          uint16_t* out) {
-  __shared__ uint8_t rw[40 * 40];
-  __shared__ uint8_t mb[64];
+  __shared__ uint32_t rw32[40 * 40 / 4];  // the reference window at half resolution, rows of 10 words
+  __shared__ uint32_t mb32[16];           // the MB at half resolution, rows of 2 words
+  uint8_t* rw = reinterpret_cast<uint8_t*>(rw32);
+  uint8_t* mb = reinterpret_cast<uint8_t*>(mb32);
   const int i = blockIdx.x, t = threadIdx.x;
   if (i >= n) return;
   const int mx = (int)xy[2 * i] * 16, my = (int)xy[2 * i + 1] * 16;
@@ -81,18 +83,29 @@ __global__ void __launch_bounds__(256) lp_windows_kernel(const uint8_t* src, uin
     rw[q] = (uint8_t)avg2(ref, rs, my - 32 + 2 * (q / 40), mx - 32 + 2 * (q % 40));
   if (t < 64) mb[t] = (uint8_t)avg2(src, ss, my + 2 * (t >> 3), mx + 2 * (t & 7));
   __syncthreads();
-  for (int q = t; q < LP_P; q += blockDim.x) {
-    const int oy = q >> 5, ox = q & 31;  // block origin in the 40x40 window
-    int sad = 0;
-#pragma unroll 8
-    for (int k = 0; k < 64; k++) {
-      const int d = (int)mb[k] - (int)rw[(oy + (k >> 3)) * 40 + ox + (k & 7)];
-      sad += d < 0 ? -d : d;
-    }
-    const float c0 = (32.0f - (float)sad * (1.0f / 64.0f)) * (1.0f / 32.0f);
-    const float c1 = ((float)rw[(oy + 4) * 40 + ox + 4] - 128.0f) * (1.0f / 64.0f);
-    *reinterpret_cast<uint32_t*>(out + ((size_t)i * LP_P + q) * 2) = pack_bf16(c0, c1);
+  // Thread t: cells (oy, 4 j .. 4 j + 3) with oy = t / 8, j = t % 8. Per
+  // window row three words hold the 11 bytes the four 8-byte rows need; the
+  // byte-shifted rows come from byte permutes and four-byte SADs.
+  const int oy = t >> 3, ox0 = (t & 7) * 4;
+  uint32_t sad[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+  for (int r = 0; r < 8; r++) {
+    const uint32_t* row = rw32 + (oy + r) * 10 + (ox0 >> 2);
+    const uint32_t w0 = row[0], w1 = row[1], w2 = row[2];
+    const uint32_t m0 = mb32[2 * r], m1 = mb32[2 * r + 1];
+    sad[0] = __vsadu4(w0, m0) + __vsadu4(w1, m1) + sad[0];
+    sad[1] = __vsadu4(__byte_perm(w0, w1, 0x4321), m0) + __vsadu4(__byte_perm(w1, w2, 0x4321), m1) + sad[1];
+    sad[2] = __vsadu4(__byte_perm(w0, w1, 0x5432), m0) + __vsadu4(__byte_perm(w1, w2, 0x5432), m1) + sad[2];
+    sad[3] = __vsadu4(__byte_perm(w0, w1, 0x6543), m0) + __vsadu4(__byte_perm(w1, w2, 0x6543), m1) + sad[3];
   }
+  uint32_t o[4];
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    const float c0 = (32.0f - (float)sad[c] * (1.0f / 64.0f)) * (1.0f / 32.0f);
+    const float c1 = ((float)rw[(oy + 4) * 40 + ox0 + c + 4] - 128.0f) * (1.0f / 64.0f);
+    o[c] = pack_bf16(c0, c1);
+  }
+  *reinterpret_cast<uint4*>(out + ((size_t)i * LP_P + oy * 32 + ox0) * 2) = make_uint4(o[0], o[1], o[2], o[3]);
 }
 
 // ------------------------------------------------------- seeded search
@@ -1269,6 +1282,10 @@ vp8a_status vp8a_lp_windows(vp8a_ctx* ctx, const vp8a_luma_ref* src, const vp8a_
     return VP8A_E_REFERENCE_DIMENSIONS_MISMATCH;
   }
   if (n == 0) return VP8A_OK;
+  if ((uintptr_t)out & 15) {
+    vp8a::set_error("out must be 16-byte aligned");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
   VP8A_CUDA(cudaSetDevice(ctx->device));
   lp_windows_kernel<<<n, 256, 0, ctx->stream>>>(src->plane, src->stride, ref->plane, ref->stride, (int)src->width,
                                                  (int)src->height, mb_xy, (int)n, out);
