@@ -346,6 +346,17 @@ vp8a_status vp8a_motion_descent(vp8a_ctx* ctx, const vp8a_luma_ref* ref,
                                 vp8a_search_result* whole_out, vp8a_search_result* half_out,
                                 vp8a_search_result* quarter_out);
 
+/* vp8a_motion_descent for the items whose active[i] is non-zero; the other
+ * items' outputs are left as they were. No counterpart in the reference:
+ * the learned search's fallback runs the plain descent on the MBs it
+ * flags, with the flags kept on the device. */
+vp8a_status vp8a_motion_descent_masked(vp8a_ctx* ctx, const vp8a_luma_ref* ref,
+                                       const uint8_t* src_mbs, const uint32_t* mb_xy,
+                                       const vp8a_mv* centers, uint32_t max_iters, uint32_t n,
+                                       const uint8_t* active, vp8a_search_result* whole_out,
+                                       vp8a_search_result* half_out,
+                                       vp8a_search_result* quarter_out);
+
 /* ------------------------------------- exhaustive inter analysis (§16/§17) */
 
 /* The exhaustive per-MB analysis of a P frame with intra picking off:

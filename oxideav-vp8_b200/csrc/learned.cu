@@ -117,12 +117,14 @@ __global__ void __launch_bounds__(256) lp_windows_kernel(const uint8_t* src, uin
 // sit in shared memory; the first smallest (SAD, order) wins.
 constexpr int LP_SEED_MAXC = 128;  // k * (2 radius + 1)^2
 constexpr int LP_SEED_MAXW = 16 + 2 * 4;  // window side for radius <= 4
+constexpr int LP_SEED_PITCH = 28;         // window row pitch: 7 words, so a row's five words stay in it
 __global__ void __launch_bounds__(LP_SEED_MAXC) lp_seeded_search_kernel(const uint8_t* ref, uint64_t rs, int rw,
                                                                         int rh, const uint8_t* src_mbs,
                                                                         const uint32_t* xy, const int32_t* seeds,
                                                                         int k, int radius, vp8a_search_result* out) {
-  __shared__ uint8_t win[4][LP_SEED_MAXW * LP_SEED_MAXW];
-  __shared__ uint8_t sm[256];
+  __shared__ uint32_t win32[4][LP_SEED_MAXW * LP_SEED_PITCH / 4];
+  __shared__ uint32_t sm32[64];
+  uint8_t* sm = reinterpret_cast<uint8_t*>(sm32);
   __shared__ uint32_t best_w[LP_SEED_MAXC / 32];
   const int i = blockIdx.x, t = threadIdx.x;
   const int mx = (int)xy[2 * i] * 16, my = (int)xy[2 * i + 1] * 16;
@@ -131,23 +133,27 @@ __global__ void __launch_bounds__(LP_SEED_MAXC) lp_seeded_search_kernel(const ui
   for (int s = 0; s < k; s++) {
     const int c = seeds[(size_t)i * k + s];
     const int x0 = mx + (c % 32 - 16) * 2 - radius, y0 = my + (c / 32 - 16) * 2 - radius;
+    uint8_t* win = reinterpret_cast<uint8_t*>(win32[s]);
     for (int q = t; q < side * side; q += blockDim.x) {
       const int y = min(max(y0 + q / side, 0), rh - 1), x = min(max(x0 + q % side, 0), rw - 1);
-      win[s][q] = ref[(size_t)y * rs + x];
+      win[(q / side) * LP_SEED_PITCH + q % side] = ref[(size_t)y * rs + x];
     }
   }
   __syncthreads();
   uint32_t key = 0xffffffffu;
   if (t < k * per) {
     const int s = t / per, o = t - s * per, dr = o / (2 * radius + 1), dc = o - dr * (2 * radius + 1);
-    const uint8_t* w = win[s] + dr * side + dc;
+    // Row r of the candidate: bytes dc .. dc + 15 of window row dr + r, cut
+    // from five words by byte permutes, against the MB row's four words.
+    const uint32_t* w = win32[s] + dr * (LP_SEED_PITCH / 4) + (dc >> 2);
+    const uint32_t sel = 0x3210u + (uint32_t)(dc & 3) * 0x1111u;
     uint32_t sad = 0;
+#pragma unroll 4
     for (int r = 0; r < 16; r++) {
-#pragma unroll
-      for (int cc = 0; cc < 16; cc++) {
-        const int d = (int)w[r * side + cc] - (int)sm[r * 16 + cc];
-        sad += (uint32_t)(d < 0 ? -d : d);
-      }
+      const uint32_t* wr = w + r * (LP_SEED_PITCH / 4);
+      const uint32_t w0 = wr[0], w1 = wr[1], w2 = wr[2], w3 = wr[3], w4 = wr[4];
+      sad += __vsadu4(__byte_perm(w0, w1, sel), sm32[4 * r]) + __vsadu4(__byte_perm(w1, w2, sel), sm32[4 * r + 1]) +
+             __vsadu4(__byte_perm(w2, w3, sel), sm32[4 * r + 2]) + __vsadu4(__byte_perm(w3, w4, sel), sm32[4 * r + 3]);
     }
     key = (sad << 7) | (uint32_t)t;
   }

@@ -4,6 +4,7 @@
 //   vp8a_half_pixel_refine_luma     (src/motion_search.rs:564)
 //   vp8a_quarter_pixel_refine_luma  (src/motion_search.rs:666)
 //   vp8a_motion_descent             (diamond -> half -> quarter, src/encoder.rs:8576-8596)
+//   vp8a_motion_descent_masked      (the same for the items an active mask selects)
 // One warp per item, four warps per CTA; the reference window of each item
 // is staged in shared memory (me_common.cuh).
 #include "me_common.cuh"
@@ -24,6 +25,7 @@ struct MeBatch {
   vp8a_search_result* out0;
   vp8a_search_result* out1;
   vp8a_search_result* out2;
+  const uint8_t* active;  // optional: items whose byte is 0 are skipped
 };
 
 constexpr int ME_WARPS = 4;
@@ -35,6 +37,7 @@ __global__ void __launch_bounds__(ME_WARPS * 32) me_batch_kernel(MeBatch a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t item = blockIdx.x * ME_WARPS + warp;
   if (item >= a.n) return;  // warp-uniform
+  if (a.active && !a.active[item]) return;
   WarpScratch& S = scratch[warp];
   uint8_t* src = srcs[warp];
   const uint8_t* gsrc = a.src_mbs + (size_t)item * 256;
@@ -92,7 +95,7 @@ using vp8a::Stager;
 vp8a_status run_batch(vp8a_ctx* ctx, int mode, const vp8a_luma_ref* ref, const uint8_t* src_mbs,
                       const uint32_t* mb_xy, const vp8a_mv* mvs, uint32_t max_iters, uint32_t n,
                       uint32_t* sad_out, vp8a_search_result* o0, vp8a_search_result* o1,
-                      vp8a_search_result* o2) {
+                      vp8a_search_result* o2, const uint8_t* active = nullptr) {
   if (!ctx || !ref || !ref->plane) {
     vp8a::set_error("null context or reference");
     return VP8A_E_INVALID_ARGUMENT;
@@ -123,6 +126,10 @@ vp8a_status run_batch(vp8a_ctx* ctx, int mode, const vp8a_luma_ref* ref, const u
   a.mb_xy = (const uint32_t*)d;
   if ((s = st.in(mvs, (size_t)n * sizeof(vp8a_mv), &d)) != VP8A_OK) return s;
   a.mvs = (const vp8a_mv*)d;
+  if (active) {
+    if ((s = st.in(active, (size_t)n, &d)) != VP8A_OK) return s;
+    a.active = (const uint8_t*)d;
+  }
   void* o = nullptr;
   if (sad_out) {
     if ((s = st.out(sad_out, (size_t)n * 4, &o)) != VP8A_OK) return s;
@@ -132,7 +139,10 @@ vp8a_status run_batch(vp8a_ctx* ctx, int mode, const vp8a_luma_ref* ref, const u
   vp8a_search_result** douts[3] = {&a.out0, &a.out1, &a.out2};
   for (int k = 0; k < 3; k++)
     if (outs[k]) {
-      if ((s = st.out(outs[k], (size_t)n * sizeof(vp8a_search_result), &o)) != VP8A_OK) return s;
+      // With a mask, skipped items keep their values: host outputs go both ways.
+      if ((s = active ? st.inout(outs[k], (size_t)n * sizeof(vp8a_search_result), &o)
+                      : st.out(outs[k], (size_t)n * sizeof(vp8a_search_result), &o)) != VP8A_OK)
+        return s;
       *douts[k] = (vp8a_search_result*)o;
     }
   a.n = n;
@@ -191,6 +201,18 @@ vp8a_status vp8a_motion_descent(vp8a_ctx* ctx, const vp8a_luma_ref* ref, const u
                                 vp8a_search_result* quarter_out) {
   return run_batch(ctx, MODE_DESCENT, ref, src_mbs, mb_xy, centers, max_iters, n, nullptr, whole_out,
                    half_out, quarter_out);
+}
+
+vp8a_status vp8a_motion_descent_masked(vp8a_ctx* ctx, const vp8a_luma_ref* ref, const uint8_t* src_mbs,
+                                       const uint32_t* mb_xy, const vp8a_mv* centers, uint32_t max_iters,
+                                       uint32_t n, const uint8_t* active, vp8a_search_result* whole_out,
+                                       vp8a_search_result* half_out, vp8a_search_result* quarter_out) {
+  if (n && !active) {
+    vp8a::set_error("null active mask");
+    return VP8A_E_INVALID_ARGUMENT;
+  }
+  return run_batch(ctx, MODE_DESCENT, ref, src_mbs, mb_xy, centers, max_iters, n, nullptr, whole_out,
+                   half_out, quarter_out, active);
 }
 
 }  // extern "C"

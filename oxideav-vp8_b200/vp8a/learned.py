@@ -300,17 +300,19 @@ def _learned_search(ctx, net, src_y, ref_y, mb_xy, k, radius, fallback, seeds, t
     out_sad = sr_out[:, 1].clone()
     mark("subpel")
     # Fallback: the plain descent from the zero vector (8 rounds + sub-pel)
-    # for the MBs whose SAD exceeds `fallback` x the median. The descent runs
-    # for every MB (each item is independent) and is kept where it falls
-    # back and wins, so no count or index list crosses to the host.
+    # for the MBs whose SAD exceeds `fallback` x the median, kept where it
+    # wins. The flags stay on the device: the masked descent skips the other
+    # items, so no count or index list crosses to the host.
     med = out_sad.to(torch.float32).median()
     fb = out_sad.to(torch.float32) > fallback * med
     zero = torch.zeros((n, 2), dtype=torch.int16, device=seeds.device)
     w_o = torch.empty((n, 2), dtype=torch.int32, device=seeds.device)
     h_o = torch.empty_like(w_o)
-    q_o = torch.empty_like(w_o)
-    check(lib.vp8a_motion_descent(ctx.handle, C.byref(ref), ptr(src_mbs), ptr(mb_xy), ptr(zero), 8, n, ptr(w_o),
-                                  ptr(h_o), ptr(q_o)), "vp8a_motion_descent")
+    q_o = torch.zeros_like(w_o)
+    fb8 = fb.to(torch.uint8)
+    check(lib.vp8a_motion_descent_masked(ctx.handle, C.byref(ref), ptr(src_mbs), ptr(mb_xy), ptr(zero), 8, n,
+                                         ptr(fb8), ptr(w_o), ptr(h_o), ptr(q_o)),
+          "vp8a_motion_descent_masked")
     better = fb & (q_o[:, 1] < out_sad)
     out_sad = torch.where(better, q_o[:, 1], out_sad)
     out_mv = torch.where(better[:, None], q_o[:, 0].contiguous().view(torch.int16).view(n, 2), out_mv)

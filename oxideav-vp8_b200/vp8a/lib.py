@@ -51,6 +51,7 @@ PROTOTYPES = {
     "vp8a_reconstruct_inter_frames": (C.c_int, [P, P, U32]),
     "vp8a_filter_sweeps": (C.c_int, [P, P, U32]),
     "vp8a_lp_net_propose": (C.c_int, [P, P, U32, P, P, P, P, P, P, P, P, U32, P, P]),
+    "vp8a_motion_descent_masked": (C.c_int, [P, P, P, P, P, U32, U32, P, P, P, P]),
     "vp8a_lp_seeded_search": (C.c_int, [P, P, P, P, P, U32, U32, U32, P]),
     "vp8a_lp_windows": (C.c_int, [P, C.POINTER(abi.LumaRef), C.POINTER(abi.LumaRef), P, U32, P]),
     "vp8a_lp_conv_forward": (C.c_int, [P, P, U32, P, P, U32, U32, U32, P, P]),

@@ -73,6 +73,37 @@ def test_descent_parity(ctx, oracle, seq):
         assert sr_tuples(g) == sr_tuples(w)
 
 
+def test_masked_descent_runs_only_the_active_items(ctx, oracle, seq):
+    # vp8a_motion_descent_masked: the active items get the oracle's descent,
+    # the others keep what the output buffers held.
+    import ctypes as C
+
+    from vp8a import abi
+    from vp8a.frames import ptr
+
+    ref, mbs, xy = seq
+    rng = np.random.default_rng(8)
+    c = centers_for(len(mbs), rng, "small")
+    cc = np.ascontiguousarray(np.asarray(c).astype(np.int16).reshape(-1, 2))
+    xyc = np.ascontiguousarray(np.asarray(xy, dtype=np.uint32).reshape(-1, 2))
+    active = (rng.random(len(mbs)) < 0.3).astype(np.uint8)
+    active[0], active[-1] = 1, 0
+    want = oracle.motion_descent(ref, mbs, xy, c, 8)
+    outs = [np.zeros(len(mbs), abi.SEARCH_RESULT_DTYPE) for _ in range(3)]
+    for o in outs:
+        o["sad"] = 0xDEADBEEF
+    r = vp8a.luma_ref(ref)
+    lib = ctx._lib
+    assert lib.vp8a_motion_descent_masked(ctx.handle, C.byref(r), ptr(np.ascontiguousarray(mbs)), ptr(xyc), ptr(cc),
+                                          8, len(mbs), ptr(active), *[ptr(o) for o in outs]) == abi.OK
+    on = active.astype(bool)
+    for g, w in zip(outs, want):
+        assert sr_tuples(g[on]) == sr_tuples(w[on])
+        assert (g["sad"][~on] == 0xDEADBEEF).all()
+    assert lib.vp8a_motion_descent_masked(ctx.handle, C.byref(r), ptr(np.ascontiguousarray(mbs)), ptr(xyc), ptr(cc),
+                                          8, len(mbs), None, *[ptr(o) for o in outs]) == abi.E_INVALID_ARGUMENT
+
+
 @pytest.mark.parametrize("w,h", [(16, 16), (33, 17), (48, 80), (200, 24)])
 def test_odd_plane_sizes(ctx, oracle, w, h):
     rng = np.random.default_rng(w * h)
