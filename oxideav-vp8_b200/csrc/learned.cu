@@ -6,9 +6,14 @@
 // cells seed an exact local search (the plain search's SAD kernels), so
 // the net only proposes; every returned vector and SAD is exact.
 //
-// Kernels (all hand-written; the GEMM-shaped ones on the tensor cores with
-// mma.sync m16n8k16 BF16 -> FP32):
+// Kernels (all hand-written; the GEMM-shaped ones on the tensor cores, the
+// training layers with mma.sync m16n8k16 BF16 -> FP32, inference and the
+// 32 -> 32 forward layers with tcgen05 and TMEM accumulators):
 //   lp_windows_kernel       coarse cost volumes -> NHWC [n, 32, 32, 2] BF16
+//   lp_net_kernel           the whole net and the top-k cells per map in one
+//                           launch (inference), activations on chip
+//   lp_seeded_search_kernel every whole-pel vector near the seed cells,
+//                           first smallest SAD
 //   lp_conv_fwd_smem_kernel implicit-GEMM conv (+ bias, ReLU), one CTA per
 //                           image staged with its halo in shared memory
 //   lp_conv_bwd_data_kernel dX = conv^T(dY, W), masked by the ReLU of X
