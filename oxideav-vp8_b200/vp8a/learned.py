@@ -5,16 +5,18 @@ BF16 weights and activations, FP32 accumulation) scores a 32 x 32 grid of
 whole-pel vectors, 2 px apart, from an MB's coarse cost volume against a
 reference (`vp8a_lp_windows`: at each grid vector the half-resolution SAD of
 the MB and the reference's texture), so each score sees the matching cost
-of its own vector and its neighbours'. Every
-layer runs on the library's hand-written tensor-core kernels
+of its own vector and its neighbours'. Training
+runs every layer on the library's hand-written tensor-core kernels
 (`vp8a_lp_conv_forward` / `vp8a_lp_conv_backward`), the loss and the
-optimiser on its own kernels (`vp8a_lp_softmax_ce`, `vp8a_lp_adam`); torch
-only holds the device buffers. Training labels are the plain search's own
-whole-pel results (`labels_from_search`).
+optimiser on its own kernels (`vp8a_lp_softmax_ce`, `vp8a_lp_adam`);
+inference runs the whole net and the top-k in one launch
+(`vp8a_lp_net_propose`); torch only holds the device buffers. Training
+labels are the plain search's own whole-pel results (`labels_from_search`).
 
 The net only proposes: `learned_search` takes its best cells as seeds of an
-exact local search (every whole-pel position within +-2 px of each seed, the
-first smallest SAD, then the reference's half- and quarter-pel refinement),
+exact local search (`vp8a_lp_seeded_search`: every whole-pel position within
++-2 px of each seed, the first smallest SAD, then the reference's half- and
+quarter-pel refinement),
 with the plain descent from the zero vector as the fallback for MBs whose
 refined SAD exceeds 1.25 x the frame's median. Every returned vector and SAD
 is exact; the net decides only where to look.
