@@ -12,6 +12,7 @@ import numpy as np
 import pytest
 
 import vp8a
+from util import windows_ref
 from vp8a import abi, learned, synth
 
 pytestmark = pytest.mark.gpu
@@ -394,32 +395,6 @@ def test_fused_net_arguments(ctx):
     ctx.synchronize()
 
 
-def windows_ref(src, ref, xy):
-    """The cost volume by its definition, in numpy: both planes averaged 2x2
-    (rounded, coordinates clamped to the plane), the 8 x 8 half-resolution
-    MB against the 40 x 40 half-resolution window from (-32, -32) px, then
-    c0 = (32 - SAD / 64) / 32 and c1 = (window[oy + 4][ox + 4] - 128) / 64
-    in FP32, rounded to BF16."""
-    h, w = src.shape
-
-    def avg2(p, ys, xs):
-        s = sum(p[np.clip(ys + a, 0, h - 1)][:, np.clip(xs + b, 0, w - 1)].astype(np.int32)
-                for a in (0, 1) for b in (0, 1))
-        return ((s + 2) >> 2).astype(np.int32)
-
-    out = np.zeros((len(xy), 32, 32, 2), np.float32)
-    for i, (c, r) in enumerate(xy):
-        mx, my = int(c) * 16, int(r) * 16
-        win = avg2(ref, my - 32 + 2 * np.arange(40), mx - 32 + 2 * np.arange(40))
-        mb = avg2(src, my + 2 * np.arange(8), mx + 2 * np.arange(8))
-        for oy in range(32):
-            for ox in range(32):
-                sad = np.abs(win[oy:oy + 8, ox:ox + 8] - mb).sum()
-                out[i, oy, ox, 0] = (np.float32(32.0) - np.float32(sad) * np.float32(1 / 64)) * np.float32(1 / 32)
-                out[i, oy, ox, 1] = (np.float32(win[oy + 4, ox + 4]) - np.float32(128)) * np.float32(1 / 64)
-    return bf16(out)
-
-
 @pytest.mark.parametrize("w,h", [(176, 144), (72, 40)])
 def test_windows_match_their_definition(ctx, w, h):
     # vp8a_lp_windows bit for bit against the numpy definition, frames whose
@@ -431,5 +406,5 @@ def test_windows_match_their_definition(ctx, w, h):
     xy = learned.all_mbs(mbc, mbr)
     got = learned.windows(ctx, srcd, refd, xy)
     ctx.synchronize()
-    want = windows_ref(frames[3][0], frames[2][0], xy.cpu().numpy().view(np.uint32))
+    want = bf16(windows_ref(frames[3][0], frames[2][0], xy.cpu().numpy().view(np.uint32)))
     assert np.array_equal(got.float().cpu().numpy(), want)

@@ -58,3 +58,29 @@ def extract_mbs(y, mb_rows, mb_cols):
 def sr_tuples(a):
     """Structured search results -> list of (row, col, sad)."""
     return [(int(r["mv"]["row"]), int(r["mv"]["col"]), int(r["sad"])) for r in a]
+
+
+def windows_ref(src, ref, xy):
+    """The learned proposal's cost volume by its definition (FP32, before
+    the BF16 rounding vp8a_lp_windows applies): both planes averaged 2x2
+    (rounded, each coordinate clamped to the plane), the 8 x 8
+    half-resolution MB of each listed (col, row) against the 40 x 40
+    half-resolution window from (-32, -32) px; at cell (oy, ox) channel 0 is
+    (32 - SAD / 64) / 32 and channel 1 (window[oy + 4][ox + 4] - 128) / 64.
+    Returns [n, 32, 32, 2] float32."""
+    h, w = src.shape
+
+    def avg2(p, ys, xs):
+        s = sum(p[np.clip(ys + a, 0, h - 1)][:, np.clip(xs + b, 0, w - 1)].astype(np.int32)
+                for a in (0, 1) for b in (0, 1))
+        return ((s + 2) >> 2).astype(np.int32)
+
+    out = np.zeros((len(xy), 32, 32, 2), np.float32)
+    for i, (c, r) in enumerate(np.asarray(xy).reshape(-1, 2)):
+        mx, my = int(c) * 16, int(r) * 16
+        win = avg2(ref, my - 32 + 2 * np.arange(40), mx - 32 + 2 * np.arange(40))
+        mb = avg2(src, my + 2 * np.arange(8), mx + 2 * np.arange(8))
+        sad = np.abs(np.lib.stride_tricks.sliding_window_view(win, (8, 8))[:32, :32] - mb).sum(axis=(2, 3))
+        out[i, :, :, 0] = (np.float32(32.0) - sad.astype(np.float32) * np.float32(1 / 64)) * np.float32(1 / 32)
+        out[i, :, :, 1] = (win[4:36, 4:36].astype(np.float32) - np.float32(128)) * np.float32(1 / 64)
+    return out
