@@ -869,8 +869,8 @@ __global__ void __launch_bounds__(lpnet::THREADS, 1) lp_net_kernel(const uint16_
   const int first = blockIdx.x, stride = gridDim.x;
 
   if (warp >= EPI / 32) {
-    // ---- the MMA warps: issuer i takes the tiles t = i, i + 2, ... of the
-    // 36 an image (layers 1-4 x 9); lane 0 issues, the whole warp waits.
+    // ---- the MMA warps: issuer i takes the tiles t = i, i + ISSUERS, ... of
+    // the 36 an image (layers 1-4 x 9); lane 0 issues, the whole warp waits.
     const int iss = warp - EPI / 32;
     bool ok = true;
     int copies = 0;  // bulk copies issued (issuer 0)
